@@ -1,0 +1,46 @@
+"""hwyBLAS-B200: hwyBLAS's level-3 hot path on NVIDIA B200 (sm_100a).
+
+The product is the shared library ``libhwyblas_b200.so`` whose C ABI
+(``include/hwyblas_b200.h``) replaces the reference's Fortran BLAS/LAPACK and
+CBLAS entry points. This package loads it and exposes thin Python wrappers
+with the reference's routine names and argument order (Fortran convention:
+column-major, 1-based pivots, INFO returned), accepting NumPy arrays (host)
+or CUDA tensors (device, used in place). There is no CPU fallback: if the
+library is missing or cannot load, every call raises.
+"""
+import ctypes
+import os
+
+from . import _abi
+
+__all__ = [
+    "lib", "dgemm", "sgemm", "dtrsm", "dsyrk", "idamax", "dlaswp", "dgetrf",
+    "dgetrf2", "dgetrs", "dgesv", "dpotrf", "dpotrf2", "dpotrs", "dposv",
+    "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
+    "ErrorCapture", "launch_count", "set_stream",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhwyblas_b200.so")
+_lib = None
+
+
+def lib():
+    """The loaded product library (built by hwyblas_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m hwyblas_b200.build`"
+                " (there is no CPU fallback)")
+        _lib = _abi.declare(ctypes.CDLL(LIB_PATH))
+    return _lib
+
+
+from ._api import (  # noqa: E402  (needs lib())
+    dgemm, sgemm, dtrsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
+    dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
+    cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
+    CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
+    CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
+)

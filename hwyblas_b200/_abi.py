@@ -1,0 +1,55 @@
+"""ctypes prototypes of the C ABI in include/hwyblas_b200.h.
+
+EXPORTED lists every symbol the header declares; the CPU test suite checks
+that the built library exports exactly these.
+"""
+import ctypes
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+PI = ctypes.POINTER(ctypes.c_int)
+D = ctypes.c_double
+F = ctypes.c_float
+C = ctypes.c_char_p
+
+# name -> (restype, argtypes)
+PROTOTYPES = {
+    # Fortran BLAS (all arguments by pointer)
+    "dgemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]),
+    "sgemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]),
+    "dtrsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
+    "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
+    "idamax_": (I, [PI, P, PI]),
+    "xerbla_": (None, [C, PI, ctypes.c_size_t]),
+    "hwyblas_set_error_handler": (P, [P]),
+    # LAPACK
+    "dgetrf_": (None, [PI, PI, P, PI, P, PI]),
+    "dgetrf2_": (None, [PI, PI, P, PI, P, PI]),
+    "dlaswp_": (None, [PI, P, PI, PI, PI, P, PI]),
+    "dgetrs_": (None, [C, PI, PI, P, PI, P, P, PI, PI]),
+    "dgesv_": (None, [PI, PI, P, PI, P, P, PI, PI]),
+    "dpotrf_": (None, [C, PI, P, PI, PI]),
+    "dpotrf2_": (None, [C, PI, P, PI, PI]),
+    "dpotrs_": (None, [C, PI, PI, P, PI, P, PI, PI]),
+    "dposv_": (None, [C, PI, PI, P, PI, P, PI, PI]),
+    # CBLAS (by value)
+    "cblas_xerbla": (None, [I, C, C]),
+    "cblas_dgemm": (None, [I, I, I, I, I, I, D, P, I, P, I, D, P, I]),
+    "cblas_sgemm": (None, [I, I, I, I, I, I, F, P, I, P, I, F, P, I]),
+    "cblas_dtrsm": (None, [I, I, I, I, I, I, I, D, P, I, P, I]),
+    "cblas_idamax": (ctypes.c_size_t, [I, P, I]),
+    # Extensions
+    "hwyblas_set_stream": (None, [P]),
+    "hwyblas_last_cuda_error": (I, []),
+    "hwyblas_launch_count": (ctypes.c_uint64, []),
+}
+
+EXPORTED = sorted(PROTOTYPES)
+
+
+def declare(lib):
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

@@ -1,0 +1,190 @@
+"""Python wrappers with the reference's routine names and argument order.
+
+Each wrapper takes the Fortran arguments by value (characters as str, sizes
+as int, scalars as float) and buffers as NumPy arrays (host memory, copied to
+the GPU and back by the library) or CUDA tensors (device memory, used in
+place), and calls the C ABI. Matrices are column-major: pass
+``np.asfortranarray`` data or any buffer with the right leading dimension.
+LAPACK wrappers return INFO.
+"""
+import ctypes
+
+from . import lib
+
+CblasRowMajor, CblasColMajor = 101, 102
+CblasNoTrans, CblasTrans, CblasConjTrans = 111, 112, 113
+CblasUpper, CblasLower = 121, 122
+CblasNonUnit, CblasUnit = 131, 132
+CblasLeft, CblasRight = 141, 142
+
+
+def _ptr(x):
+    """Address of a NumPy array / torch tensor / integer address."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(f"unsupported buffer {type(x)}")
+
+
+def _i(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _d(v):
+    return ctypes.byref(ctypes.c_double(float(v)))
+
+
+def _f(v):
+    return ctypes.byref(ctypes.c_float(float(v)))
+
+
+def _c(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+def dgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """C := alpha*op(A)*op(B) + beta*C (reference dgemm_, src/gemm.cc:151)."""
+    lib().dgemm_(_c(transa), _c(transb), _i(m), _i(n), _i(k), _d(alpha), _ptr(a),
+                 _i(lda), _ptr(b), _i(ldb), _d(beta), _ptr(c), _i(ldc))
+
+
+def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """FP32 GEMM (reference sgemm_, src/gemm.cc:142)."""
+    lib().sgemm_(_c(transa), _c(transb), _i(m), _i(n), _i(k), _f(alpha), _ptr(a),
+                 _i(lda), _ptr(b), _i(ldb), _f(beta), _ptr(c), _i(ldc))
+
+
+def dtrsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """Triangular solve in place (reference dtrsm_, src/trsm.cc:196)."""
+    lib().dtrsm_(_c(side), _c(uplo), _c(transa), _c(diag), _i(m), _i(n),
+                 _d(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb))
+
+
+def dsyrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """Symmetric rank-k update (reference dsyrk_, src/level3.cc:416)."""
+    lib().dsyrk_(_c(uplo), _c(trans), _i(n), _i(k), _d(alpha), _ptr(a), _i(lda),
+                 _d(beta), _ptr(c), _i(ldc))
+
+
+def idamax(n, x, incx):
+    """1-based index of the first largest |x| (reference idamax_)."""
+    return lib().idamax_(_i(n), _ptr(x), _i(incx))
+
+
+def dlaswp(n, a, lda, k1, k2, ipiv, incx):
+    """Row interchanges (reference dlaswp_, src/lapack/getrf.cc:28)."""
+    lib().dlaswp_(_i(n), _ptr(a), _i(lda), _i(k1), _i(k2), _ptr(ipiv), _i(incx))
+
+
+def _info_call(fn, *args):
+    info = ctypes.c_int(0)
+    fn(*args, ctypes.byref(info))
+    return info.value
+
+
+def dgetrf(m, n, a, lda, ipiv):
+    """Blocked LU with partial pivoting; returns INFO (src/lapack/getrf.cc:216)."""
+    return _info_call(lib().dgetrf_, _i(m), _i(n), _ptr(a), _i(lda), _ptr(ipiv))
+
+
+def dgetrf2(m, n, a, lda, ipiv):
+    """Recursive LU; returns INFO (src/lapack/getrf.cc:112)."""
+    return _info_call(lib().dgetrf2_, _i(m), _i(n), _ptr(a), _i(lda), _ptr(ipiv))
+
+
+def dgetrs(trans, n, nrhs, a, lda, ipiv, b, ldb):
+    """Solve with LU factors; returns INFO (src/lapack/getrf.cc:287)."""
+    return _info_call(lib().dgetrs_, _c(trans), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(ipiv), _ptr(b), _i(ldb))
+
+
+def dgesv(n, nrhs, a, lda, ipiv, b, ldb):
+    """LU solve of A X = B; returns INFO (src/lapack/getrf.cc:348)."""
+    return _info_call(lib().dgesv_, _i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(ipiv),
+                      _ptr(b), _i(ldb))
+
+
+def dpotrf(uplo, n, a, lda):
+    """Blocked Cholesky; returns INFO (src/lapack/potrf.cc:128)."""
+    return _info_call(lib().dpotrf_, _c(uplo), _i(n), _ptr(a), _i(lda))
+
+
+def dpotrf2(uplo, n, a, lda):
+    """Recursive Cholesky; returns INFO (src/lapack/potrf.cc:48)."""
+    return _info_call(lib().dpotrf2_, _c(uplo), _i(n), _ptr(a), _i(lda))
+
+
+def dpotrs(uplo, n, nrhs, a, lda, b, ldb):
+    """Solve with the Cholesky factor; returns INFO (src/lapack/posv.cc:31)."""
+    return _info_call(lib().dpotrs_, _c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(b), _i(ldb))
+
+
+def dposv(uplo, n, nrhs, a, lda, b, ldb):
+    """Cholesky solve of A X = B; returns INFO (src/lapack/posv.cc:78)."""
+    return _info_call(lib().dposv_, _c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(b), _i(ldb))
+
+
+def cblas_dgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
+                ldc):
+    lib().cblas_dgemm(layout, transa, transb, m, n, k, alpha, _ptr(a), lda,
+                      _ptr(b), ldb, beta, _ptr(c), ldc)
+
+
+def cblas_sgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
+                ldc):
+    lib().cblas_sgemm(layout, transa, transb, m, n, k, alpha, _ptr(a), lda,
+                      _ptr(b), ldb, beta, _ptr(c), ldc)
+
+
+def cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    lib().cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, _ptr(a), lda,
+                      _ptr(b), ldb)
+
+
+def cblas_idamax(n, x, incx):
+    return lib().cblas_idamax(n, _ptr(x), incx)
+
+
+_HANDLER_T = ctypes.CFUNCTYPE(None, ctypes.c_char_p, ctypes.c_int)
+
+
+class ErrorCapture:
+    """Installs an error handler that records (name, position) instead of
+    printing, as the reference's tests do (tests/lapack/lapack_test_util.h:99)."""
+
+    def __init__(self):
+        self.errors = []
+        self._cb = _HANDLER_T(self._record)
+        self._prev = None
+
+    def _record(self, name, pos):
+        self.errors.append((name.decode(), pos))
+
+    def __enter__(self):
+        self._prev = lib().hwyblas_set_error_handler(
+            ctypes.cast(self._cb, ctypes.c_void_p))
+        return self
+
+    def __exit__(self, *exc):
+        lib().hwyblas_set_error_handler(self._prev)
+        return False
+
+
+def launch_count():
+    """Kernels launched by the library so far (all threads)."""
+    return int(lib().hwyblas_launch_count())
+
+
+def set_stream(stream):
+    """Issue the calling thread's work on `stream` (cudaStream_t as int, or a
+    torch.cuda.Stream); None restores the library's stream."""
+    if stream is not None and hasattr(stream, "cuda_stream"):
+        stream = stream.cuda_stream
+    lib().hwyblas_set_stream(stream)

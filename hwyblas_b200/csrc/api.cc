@@ -1,0 +1,840 @@
+// The C ABI: the reference's Fortran BLAS/LAPACK and CBLAS entry points
+// (argument checks with the reference's xerbla positions, quick returns),
+// the per-thread CUDA context and device workspace, and the staging of host
+// pointers. Every entry point is synchronous on return.
+//
+// Argument checks follow src/gemm.cc:73-110 (GEMM), src/trsm.cc:137-169
+// (TRSM), src/level3.cc:84-124 (SYRK), src/level1.cc:383-402 (IAMAX),
+// src/lapack/getrf.cc:112-131, 216-234, 287-309, 348-365 (GETRF2, GETRF,
+// GETRS, GESV), src/lapack/potrf.cc:48-67, 128-147 and src/lapack/posv.cc:31-54
+// (POTRF2, POTRF, POTRS, POSV); error reporting follows src/common.cc:25-84
+// and the CBLAS position maps of src/cblas.cc:121-149, 517-537, 661-691.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/hwyblas_b200.h"
+#include "internal.h"
+
+namespace hb {
+
+std::atomic<uint64_t> g_launches{0};
+
+namespace {
+
+struct WorkspaceBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct ThreadState {
+  Context ctx;
+  WorkspaceBuf ws[kNumWorkspaceSlots];
+  bool initialized = false;
+  ~ThreadState() {
+    // Device memory is released with the process; freeing here could run
+    // after the CUDA runtime has shut down.
+  }
+};
+
+thread_local ThreadState t_state;
+
+std::atomic<hwyblas_error_handler> g_handler{nullptr};
+
+struct CblasCtx {
+  const char* name;
+  const int* positions;
+};
+thread_local const CblasCtx* t_cblas = nullptr;
+
+void Init(ThreadState& st) {
+  if (st.initialized) return;
+  Context& c = st.ctx;
+  cudaGetDevice(&c.device);
+  cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device);
+  // A blocking stream: it is ordered after work on the legacy default stream,
+  // so inputs produced there (e.g. by PyTorch) are complete when we start.
+  if (Failed(cudaStreamCreate(&c.own_stream), "stream create")) return;
+  c.stream = c.own_stream;
+  if (Failed(cudaMalloc(&c.dev_status, 4096), "status alloc")) return;
+  cudaMemset(c.dev_status, 0, 4096);
+  st.initialized = true;
+}
+
+}  // namespace
+
+Context& Ctx() {
+  Init(t_state);
+  return t_state.ctx;
+}
+
+void* Workspace(int slot, size_t bytes) {
+  ThreadState& st = t_state;
+  Init(st);
+  WorkspaceBuf& w = st.ws[slot];
+  if (bytes == 0) bytes = 256;
+  if (w.bytes < bytes) {
+    if (w.ptr != nullptr) {
+      // Work in flight may still use the old buffer.
+      cudaStreamSynchronize(st.ctx.stream);
+      cudaFree(w.ptr);
+      w.ptr = nullptr;
+      w.bytes = 0;
+    }
+    const size_t want = bytes + bytes / 4;
+    if (Failed(cudaMalloc(&w.ptr, want), "workspace alloc")) return nullptr;
+    w.bytes = want;
+  }
+  return w.ptr;
+}
+
+bool Failed(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return false;
+  t_state.ctx.last_error = static_cast<int>(e);
+  fprintf(stderr, "hwyblas_b200: CUDA error in %s: %s\n", what,
+          cudaGetErrorString(e));
+  return true;
+}
+
+bool LaunchFailed(const char* what) { return Failed(cudaGetLastError(), what); }
+
+bool CheckDeviceStatus(const char* what) {
+  Context& c = Ctx();
+  int flag = 0;
+  if (Failed(cudaMemcpyAsync(&flag, c.dev_status, sizeof(int),
+                             cudaMemcpyDeviceToHost, c.stream),
+             what) ||
+      Failed(cudaStreamSynchronize(c.stream), what)) {
+    return true;
+  }
+  if (flag != 0) {
+    fprintf(stderr, "hwyblas_b200: a device wait timed out in %s\n", what);
+    cudaMemsetAsync(c.dev_status, 0, sizeof(int), c.stream);
+    t_state.ctx.last_error = static_cast<int>(cudaErrorLaunchTimeout);
+    return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Error reporting.
+
+void ReportError(const char* routine, int info) {
+  const hwyblas_error_handler h = g_handler.load(std::memory_order_acquire);
+  if (const CblasCtx* c = t_cblas) {
+    const int position = c->positions[info - 1];
+    if (h != nullptr) {
+      h(c->name, position);
+    } else {
+      cblas_xerbla(position, c->name, "");
+    }
+    return;
+  }
+  if (h != nullptr) {
+    h(routine, info);
+  } else {
+    xerbla_(routine, &info, strlen(routine));
+  }
+}
+
+namespace {
+
+class CblasScope {
+ public:
+  CblasScope(const char* name, std::initializer_list<int> positions) {
+    int i = 0;
+    for (int p : positions) pos_[i++] = p;
+    ctx_.name = name;
+    ctx_.positions = pos_;
+    t_cblas = &ctx_;
+  }
+  ~CblasScope() { t_cblas = nullptr; }
+
+ private:
+  CblasCtx ctx_;
+  int pos_[16];
+};
+
+char Up(char c) { return (c >= 'a' && c <= 'z') ? static_cast<char>(c - 32) : c; }
+bool DecodeOp(char c, bool* trans) {
+  c = Up(c);
+  *trans = (c == 'T' || c == 'C');
+  return c == 'N' || c == 'T' || c == 'C';
+}
+
+// ---------------------------------------------------------------------------
+// Host/device staging.
+
+bool IsDevicePointer(const void* p) {
+  if (p == nullptr) return false;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// A rows x cols column-major matrix (leading dimension ld) made available on
+// the device: in place if it is device memory, else copied (if `copy_in`) to
+// a compact device buffer whose leading dimension keeps 16-byte alignment.
+template <typename T>
+struct Staged {
+  T* dev = nullptr;
+  int ld = 0;
+  bool host = false;
+  T* host_ptr = nullptr;
+  int host_ld = 0, rows = 0, cols = 0;
+
+  bool In(const T* p, int ld_in, int rows_in, int cols_in, int slot,
+          bool copy_in) {
+    rows = rows_in;
+    cols = cols_in;
+    host_ptr = const_cast<T*>(p);
+    host_ld = ld_in;
+    if (IsDevicePointer(p)) {
+      dev = const_cast<T*>(p);
+      ld = ld_in;
+      host = false;
+      return true;
+    }
+    host = true;
+    ld = std::max(16, (rows + 15) / 16 * 16);
+    dev = static_cast<T*>(
+        Workspace(slot, sizeof(T) * static_cast<size_t>(ld) * std::max(cols, 1)));
+    if (dev == nullptr) return false;
+    if (copy_in && rows > 0 && cols > 0) {
+      return !Failed(cudaMemcpy2DAsync(dev, sizeof(T) * ld, p, sizeof(T) * ld_in,
+                                       sizeof(T) * rows, cols,
+                                       cudaMemcpyHostToDevice, Ctx().stream),
+                     "copy in");
+    }
+    return true;
+  }
+  void Out() {
+    if (!host || rows <= 0 || cols <= 0) return;
+    Failed(cudaMemcpy2DAsync(host_ptr, sizeof(T) * host_ld, dev, sizeof(T) * ld,
+                             sizeof(T) * rows, cols, cudaMemcpyDeviceToHost,
+                             Ctx().stream),
+           "copy out");
+  }
+};
+
+// A 1-D int array (pivots) on the device.
+struct StagedInts {
+  int* dev = nullptr;
+  int* host_ptr = nullptr;
+  int n = 0;
+  bool host = false;
+  bool In(const int* p, int count, int slot_offset_bytes, bool copy_in) {
+    n = count;
+    host_ptr = const_cast<int*>(p);
+    if (IsDevicePointer(p)) {
+      dev = const_cast<int*>(p);
+      return true;
+    }
+    host = true;
+    dev = Ctx().dev_status + 64 + slot_offset_bytes / 4;
+    if (count > 0 && count * 4 + slot_offset_bytes > 4096 - 256) {
+      dev = static_cast<int*>(Workspace(kWsStageC, sizeof(int) * count));
+    }
+    if (copy_in && count > 0) {
+      return !Failed(cudaMemcpyAsync(dev, p, sizeof(int) * count,
+                                     cudaMemcpyHostToDevice, Ctx().stream),
+                     "pivots in");
+    }
+    return true;
+  }
+  void Out() {
+    if (!host || n <= 0) return;
+    Failed(cudaMemcpyAsync(host_ptr, dev, sizeof(int) * n,
+                           cudaMemcpyDeviceToHost, Ctx().stream),
+           "pivots out");
+  }
+};
+
+void Finish(const char* what) {
+  CheckDeviceStatus(what);
+}
+
+int* DeviceInfo() { return Ctx().dev_status + 1; }
+void ResetInfo() {
+  cudaMemsetAsync(Ctx().dev_status + 1, 0, sizeof(int), Ctx().stream);
+}
+int ReadInfo() {
+  int v = 0;
+  Failed(cudaMemcpyAsync(&v, Ctx().dev_status + 1, sizeof(int),
+                         cudaMemcpyDeviceToHost, Ctx().stream),
+         "info out");
+  Failed(cudaStreamSynchronize(Ctx().stream), "sync");
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// BLAS bodies.
+
+template <typename T>
+void GemmEntry(const char* name, const char* transa, const char* transb,
+               const int* m_p, const int* n_p, const int* k_p, const T* alpha_p,
+               const T* a, const int* lda_p, const T* b, const int* ldb_p,
+               const T* beta_p, T* c, const int* ldc_p) {
+  const int m = *m_p, n = *n_p, k = *k_p, lda = *lda_p, ldb = *ldb_p,
+            ldc = *ldc_p;
+  bool ta, tb;
+  const bool va = DecodeOp(*transa, &ta), vb = DecodeOp(*transb, &tb);
+  const int rows_a = ta ? k : m, rows_b = tb ? n : k;
+  int info = 0;
+  if (!va) info = 1;
+  else if (!vb) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, m)) info = 13;
+  if (info != 0) {
+    ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p, beta = *beta_p;
+  if (m == 0 || n == 0) return;
+  if ((k == 0 || alpha == T(0)) && beta == T(1)) return;
+  const bool compute = !(k == 0 || alpha == T(0));
+  Staged<T> sa, sb, sc;
+  if (compute) {
+    if (!sa.In(a, lda, rows_a, ta ? m : k, kWsStageA, true)) return;
+    if (!sb.In(b, ldb, rows_b, tb ? k : n, kWsStageB, true)) return;
+  }
+  if (!sc.In(c, ldc, m, n, kWsStageC, beta != T(0))) return;
+  GemmFull<T>(ta, tb, m, n, k, alpha, sa.dev, sa.ld, sb.dev, sb.ld, beta, sc.dev,
+              sc.ld);
+  sc.Out();
+  Finish(name);
+}
+
+template <typename T>
+void TrsmEntry(const char* name, const char* side, const char* uplo,
+               const char* transa, const char* diag, const int* m_p,
+               const int* n_p, const T* alpha_p, const T* a, const int* lda_p,
+               T* b, const int* ldb_p) {
+  const int m = *m_p, n = *n_p, lda = *lda_p, ldb = *ldb_p;
+  const char s = Up(*side), u = Up(*uplo), d = Up(*diag);
+  bool trans;
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const bool vt = DecodeOp(*transa, &trans), vd = (d == 'U' || d == 'N');
+  const bool left = (s == 'L');
+  const int rows_a = left ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (!vt) info = 3;
+  else if (!vd) info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, rows_a)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info != 0) {
+    ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p;
+  if (m == 0 || n == 0) return;
+  Staged<T> sa, sb;
+  if (alpha != T(0) && !sa.In(a, lda, rows_a, rows_a, kWsStageA, true)) return;
+  if (!sb.In(b, ldb, m, n, kWsStageB, alpha != T(0))) return;
+  TrsmFull<T>(left, u == 'L', trans, d == 'U', m, n, alpha, sa.dev,
+              std::max(sa.ld, 1), sb.dev, sb.ld);
+  sb.Out();
+  Finish(name);
+}
+
+bool ValidLayout(const char* name, CBLAS_LAYOUT layout) {
+  if (layout == CblasRowMajor || layout == CblasColMajor) return true;
+  const hwyblas_error_handler h = g_handler.load(std::memory_order_acquire);
+  if (h != nullptr) {
+    h(name, 1);
+  } else {
+    cblas_xerbla(1, name, "Illegal layout setting, %d\n", static_cast<int>(layout));
+  }
+  return false;
+}
+char TransChar(CBLAS_TRANSPOSE t) {
+  switch (t) {
+    case CblasNoTrans: return 'N';
+    case CblasTrans: return 'T';
+    case CblasConjTrans: return 'C';
+    default: return '?';
+  }
+}
+char UploChar(CBLAS_UPLO u) {
+  return u == CblasUpper ? 'U' : u == CblasLower ? 'L' : '?';
+}
+char DiagChar(CBLAS_DIAG d) {
+  return d == CblasNonUnit ? 'N' : d == CblasUnit ? 'U' : '?';
+}
+char SideChar(CBLAS_SIDE s) {
+  return s == CblasLeft ? 'L' : s == CblasRight ? 'R' : '?';
+}
+char FlipUplo(char c) { return c == 'U' ? 'L' : c == 'L' ? 'U' : c; }
+char FlipSide(char c) { return c == 'L' ? 'R' : c == 'R' ? 'L' : c; }
+
+template <typename T>
+void CblasGemm(const char* name, CBLAS_LAYOUT layout,
+                      CBLAS_TRANSPOSE transa, CBLAS_TRANSPOSE transb, int m,
+                      int n, int k, T alpha, const T* a, int lda, const T* b,
+                      int ldb, T beta, T* c, int ldc) {
+  if (!ValidLayout(name, layout)) return;
+  const char ta = TransChar(transa), tb = TransChar(transb);
+  const char* fname = sizeof(T) == 8 ? "DGEMM" : "SGEMM";
+  if (layout == CblasColMajor) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14});
+    hb::GemmEntry<T>(fname, &ta, &tb, &m, &n, &k, &alpha, a, &lda, b, &ldb,
+                     &beta, c, &ldc);
+  } else {
+    hb::CblasScope scope(name, {3, 2, 5, 4, 6, 7, 10, 11, 8, 9, 12, 13, 14});
+    hb::GemmEntry<T>(fname, &tb, &ta, &n, &m, &k, &alpha, b, &ldb, a, &lda,
+                     &beta, c, &ldc);
+  }
+}
+
+}  // namespace
+}  // namespace hb
+
+using hb::Ctx;
+
+extern "C" {
+
+HWYBLAS_API void dgemm_(const char* transa, const char* transb,
+                        const hwyblas_int* m, const hwyblas_int* n,
+                        const hwyblas_int* k, const double* alpha,
+                        const double* a, const hwyblas_int* lda,
+                        const double* b, const hwyblas_int* ldb,
+                        const double* beta, double* c, const hwyblas_int* ldc) {
+  hb::GemmEntry<double>("DGEMM", transa, transb, m, n, k, alpha, a, lda, b, ldb,
+                        beta, c, ldc);
+}
+
+HWYBLAS_API void sgemm_(const char* transa, const char* transb,
+                        const hwyblas_int* m, const hwyblas_int* n,
+                        const hwyblas_int* k, const float* alpha,
+                        const float* a, const hwyblas_int* lda, const float* b,
+                        const hwyblas_int* ldb, const float* beta, float* c,
+                        const hwyblas_int* ldc) {
+  hb::GemmEntry<float>("SGEMM", transa, transb, m, n, k, alpha, a, lda, b, ldb,
+                       beta, c, ldc);
+}
+
+HWYBLAS_API void dtrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m,
+                        const hwyblas_int* n, const double* alpha,
+                        const double* a, const hwyblas_int* lda, double* b,
+                        const hwyblas_int* ldb) {
+  hb::TrsmEntry<double>("DTRSM", side, uplo, transa, diag, m, n, alpha, a, lda,
+                        b, ldb);
+}
+
+HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
+                        const hwyblas_int* n_p, const hwyblas_int* k_p,
+                        const double* alpha_p, const double* a,
+                        const hwyblas_int* lda_p, const double* beta_p,
+                        double* c, const hwyblas_int* ldc_p) {
+  const int n = *n_p, k = *k_p, lda = *lda_p, ldc = *ldc_p;
+  const char u = hb::Up(*uplo);
+  bool t;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool vt = hb::DecodeOp(*trans, &t);
+  const int rows_a = t ? k : n;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!vt) info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, rows_a)) info = 7;
+  else if (ldc < std::max(1, n)) info = 10;
+  if (info != 0) {
+    hb::ReportError("DSYRK", info);
+    return;
+  }
+  const double alpha = *alpha_p, beta = *beta_p;
+  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return;
+  const bool compute = !(alpha == 0.0 || k == 0);
+  hb::Staged<double> sa, sc;
+  if (compute && !sa.In(a, lda, rows_a, t ? n : k, hb::kWsStageA, true)) return;
+  // The whole square is copied so that the other triangle comes back as is.
+  if (!sc.In(c, ldc, n, n, hb::kWsStageC, true)) return;
+  hb::SyrkFull(u == 'L', t, n, k, alpha, sa.dev, std::max(sa.ld, 1), beta,
+               sc.dev, sc.ld);
+  sc.Out();
+  hb::Finish("DSYRK");
+}
+
+HWYBLAS_API hwyblas_int idamax_(const hwyblas_int* n_p, const double* x,
+                                const hwyblas_int* incx_p) {
+  const int n = *n_p, incx = *incx_p;
+  if (n < 1 || incx <= 0) return 0;
+  if (n == 1) return 1;
+  hb::Staged<double> sx;
+  const long long span = static_cast<long long>(n - 1) * incx + 1;
+  if (span > 0x7fffffff) return 0;
+  if (!sx.In(x, static_cast<int>(span), static_cast<int>(span), 1,
+             hb::kWsStageA, true))
+    return 0;
+  int* out = Ctx().dev_status + 2;
+  hb::Iamax<double>(n, sx.dev, incx, out);
+  int result = 0;
+  hb::Failed(cudaMemcpyAsync(&result, out, sizeof(int), cudaMemcpyDeviceToHost,
+                             Ctx().stream),
+             "idamax out");
+  hb::Finish("IDAMAX");
+  return result;
+}
+
+HWYBLAS_API void xerbla_(const char* srname, const hwyblas_int* info,
+                         size_t srname_len) {
+  size_t len = 0;
+  while (len < srname_len && srname[len] != '\0' && srname[len] != ' ') ++len;
+  fprintf(stderr,
+          " ** On entry to %.*s parameter number %d had an illegal value\n",
+          static_cast<int>(len), srname, static_cast<int>(*info));
+}
+
+HWYBLAS_API hwyblas_error_handler
+hwyblas_set_error_handler(hwyblas_error_handler handler) {
+  return hb::g_handler.exchange(handler, std::memory_order_acq_rel);
+}
+
+// ---------------------------------------------------------------------------
+// LAPACK.
+
+static bool CheckGetrf(const char* name, int m, int n, int lda, int* info) {
+  *info = 0;
+  if (m < 0) *info = -1;
+  else if (n < 0) *info = -2;
+  else if (lda < std::max(1, m)) *info = -4;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return false;
+  }
+  return true;
+}
+
+static void GetrfEntry(bool recursive, const hwyblas_int* m_p,
+                       const hwyblas_int* n_p, double* a,
+                       const hwyblas_int* lda_p, hwyblas_int* ipiv,
+                       hwyblas_int* info) {
+  const int m = *m_p, n = *n_p, lda = *lda_p;
+  const char* name = recursive ? "DGETRF2" : "DGETRF";
+  if (!CheckGetrf(name, m, n, lda, info)) return;
+  if (m == 0 || n == 0) return;
+  hb::Staged<double> sa;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, m, n, hb::kWsStageA, true)) return;
+  if (!sp.In(ipiv, std::min(m, n), 0, false)) return;
+  hb::ResetInfo();
+  if (recursive) {
+    hb::Getrf2<double>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  } else {
+    hb::Getrf<double>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  }
+  sa.Out();
+  sp.Out();
+  *info = hb::ReadInfo();
+  hb::Finish(name);
+}
+
+HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv,
+                         hwyblas_int* info) {
+  GetrfEntry(false, m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void dgetrf2_(const hwyblas_int* m, const hwyblas_int* n,
+                          double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
+                          hwyblas_int* info) {
+  GetrfEntry(true, m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void dlaswp_(const hwyblas_int* n_p, double* a,
+                         const hwyblas_int* lda_p, const hwyblas_int* k1_p,
+                         const hwyblas_int* k2_p, const hwyblas_int* ipiv,
+                         const hwyblas_int* incx_p) {
+  const int n = *n_p, lda = *lda_p, k1 = *k1_p, k2 = *k2_p, incx = *incx_p;
+  if (incx == 0 || n <= 0) return;
+  const int absinc = incx < 0 ? -incx : incx;
+  const int count = k1 + (k2 - k1) * absinc;  // entries ipiv(1..count)
+  if (count <= 0 || k2 < k1) return;
+  hb::Staged<double> sa;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, lda, n, hb::kWsStageA, true)) return;
+  if (!sp.In(ipiv, count, 0, true)) return;
+  hb::Laswp<double>(n, sa.dev, sa.ld, k1, k2, sp.dev, incx);
+  sa.Out();
+  hb::Finish("DLASWP");
+}
+
+HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n_p,
+                         const hwyblas_int* nrhs_p, const double* a,
+                         const hwyblas_int* lda_p, const hwyblas_int* ipiv,
+                         double* b, const hwyblas_int* ldb_p,
+                         hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  const char t = hb::Up(*trans);
+  const bool notran = (t == 'N');
+  *info = 0;
+  if (!notran && t != 'T' && t != 'C') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -8;
+  if (*info != 0) {
+    hb::ReportError("DGETRS", -*info);
+    return;
+  }
+  if (n == 0 || nrhs == 0) return;
+  hb::Staged<double> sa, sb;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sp.In(ipiv, n, 0, true)) return;
+  hb::Getrs<double>(!notran, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish("DGETRS");
+}
+
+HWYBLAS_API void dgesv_(const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
+                        double* a, const hwyblas_int* lda_p, hwyblas_int* ipiv,
+                        double* b, const hwyblas_int* ldb_p,
+                        hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  *info = 0;
+  if (n < 0) *info = -1;
+  else if (nrhs < 0) *info = -2;
+  else if (lda < std::max(1, n)) *info = -4;
+  else if (ldb < std::max(1, n)) *info = -7;
+  if (*info != 0) {
+    hb::ReportError("DGESV", -*info);
+    return;
+  }
+  if (n == 0) return;
+  hb::Staged<double> sa, sb;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sp.In(ipiv, n, 0, false)) return;
+  hb::ResetInfo();
+  hb::Getrf<double>(n, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  const int finfo = hb::ReadInfo();
+  if (finfo == 0 && nrhs > 0) {
+    hb::Getrs<double>(false, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+  }
+  sa.Out();
+  sp.Out();
+  if (finfo == 0) sb.Out();
+  *info = finfo;
+  hb::Finish("DGESV");
+}
+
+static bool CheckPotrf(const char* name, const char* uplo, int n, int lda,
+                       int* info, bool* upper) {
+  const char u = hb::Up(*uplo);
+  *upper = (u == 'U');
+  *info = 0;
+  if (!*upper && u != 'L') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (lda < std::max(1, n)) *info = -4;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return false;
+  }
+  return true;
+}
+
+static void PotrfEntry(bool recursive, const char* uplo, const hwyblas_int* n_p,
+                       double* a, const hwyblas_int* lda_p,
+                       hwyblas_int* info) {
+  const int n = *n_p, lda = *lda_p;
+  const char* name = recursive ? "DPOTRF2" : "DPOTRF";
+  bool upper;
+  if (!CheckPotrf(name, uplo, n, lda, info, &upper)) return;
+  if (n == 0) return;
+  hb::Staged<double> sa;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  hb::ResetInfo();
+  if (recursive) {
+    hb::Potrf2(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  } else {
+    hb::Potrf(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  }
+  sa.Out();
+  *info = hb::ReadInfo();
+  hb::Finish(name);
+}
+
+HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* info) {
+  PotrfEntry(false, uplo, n, a, lda, info);
+}
+
+HWYBLAS_API void dpotrf2_(const char* uplo, const hwyblas_int* n, double* a,
+                          const hwyblas_int* lda, hwyblas_int* info) {
+  PotrfEntry(true, uplo, n, a, lda, info);
+}
+
+HWYBLAS_API void dpotrs_(const char* uplo, const hwyblas_int* n_p,
+                         const hwyblas_int* nrhs_p, const double* a,
+                         const hwyblas_int* lda_p, double* b,
+                         const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  const char u = hb::Up(*uplo);
+  const bool upper = (u == 'U');
+  *info = 0;
+  if (!upper && u != 'L') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -7;
+  if (*info != 0) {
+    hb::ReportError("DPOTRS", -*info);
+    return;
+  }
+  if (n == 0 || nrhs == 0) return;
+  hb::Staged<double> sa, sb;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  hb::Potrs(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish("DPOTRS");
+}
+
+HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n_p,
+                        const hwyblas_int* nrhs_p, double* a,
+                        const hwyblas_int* lda_p, double* b,
+                        const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  const char u = hb::Up(*uplo);
+  const bool upper = (u == 'U');
+  *info = 0;
+  if (!upper && u != 'L') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -7;
+  if (*info != 0) {
+    hb::ReportError("DPOSV", -*info);
+    return;
+  }
+  if (n == 0) return;
+  hb::Staged<double> sa, sb;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  hb::ResetInfo();
+  hb::Potrf(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  const int finfo = hb::ReadInfo();
+  if (finfo == 0 && nrhs > 0) hb::Potrs(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sa.Out();
+  if (finfo == 0) sb.Out();
+  *info = finfo;
+  hb::Finish("DPOSV");
+}
+
+// ---------------------------------------------------------------------------
+// CBLAS.
+
+HWYBLAS_API void cblas_xerbla(hwyblas_int p, const char* rout, const char* form,
+                              ...) {
+  if (p != 0) {
+    fprintf(stderr, "Parameter %d to routine %s was incorrect\n",
+            static_cast<int>(p), rout);
+  }
+  if (form != nullptr && *form != '\0') {
+    va_list args;
+    va_start(args, form);
+    vfprintf(stderr, form, args);
+    va_end(args);
+  }
+}
+
+
+HWYBLAS_API void cblas_dgemm(const CBLAS_LAYOUT layout,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k,
+                             const double alpha, const double* a,
+                             const hwyblas_int lda, const double* b,
+                             const hwyblas_int ldb, const double beta,
+                             double* c, const hwyblas_int ldc) {
+  hb::CblasGemm<double>("cblas_dgemm", layout, transa, transb, m, n, k, alpha, a,
+                    lda, b, ldb, beta, c, ldc);
+}
+
+HWYBLAS_API void cblas_sgemm(const CBLAS_LAYOUT layout,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k,
+                             const float alpha, const float* a,
+                             const hwyblas_int lda, const float* b,
+                             const hwyblas_int ldb, const float beta, float* c,
+                             const hwyblas_int ldc) {
+  hb::CblasGemm<float>("cblas_sgemm", layout, transa, transb, m, n, k, alpha, a,
+                   lda, b, ldb, beta, c, ldc);
+}
+
+HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m_in,
+                             const hwyblas_int n_in, const double alpha,
+                             const double* a, const hwyblas_int lda, double* b,
+                             const hwyblas_int ldb) {
+  const char* name = "cblas_dtrsm";
+  if (!hb::ValidLayout(name, layout)) return;
+  char sc = hb::SideChar(side), uc = hb::UploChar(uplo);
+  const char tc = hb::TransChar(transa), dc = hb::DiagChar(diag);
+  int m = m_in, n = n_in;
+  const bool row = (layout == CblasRowMajor);
+  if (row) {
+    sc = hb::FlipSide(sc);
+    uc = hb::FlipUplo(uc);
+    std::swap(m, n);
+  }
+  if (row) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 7, 6, 8, 9, 10, 11, 12});
+    hb::TrsmEntry<double>("DTRSM", &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda,
+                          b, &ldb);
+  } else {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12});
+    hb::TrsmEntry<double>("DTRSM", &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda,
+                          b, &ldb);
+  }
+}
+
+HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
+                                     const hwyblas_int incx) {
+  const hwyblas_int i = idamax_(&n, x, &incx);
+  return i > 0 ? static_cast<CBLAS_INDEX>(i - 1) : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Extensions.
+
+HWYBLAS_API void hwyblas_set_stream(void* stream) {
+  hb::Context& c = Ctx();
+  c.stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : c.own_stream;
+}
+
+HWYBLAS_API int hwyblas_last_cuda_error(void) {
+  hb::Context& c = Ctx();
+  const int e = c.last_error;
+  c.last_error = 0;
+  return e;
+}
+
+HWYBLAS_API uint64_t hwyblas_launch_count(void) {
+  return hb::g_launches.load(std::memory_order_relaxed);
+}
+
+}  // extern "C"

@@ -1,0 +1,489 @@
+// Pivot search, row interchanges and the leaf factorizations of the LU and
+// Cholesky drivers, with the reference's exact operation order:
+//   IAMAX      src/level1.cc:383-402, src/level1-inl.h:343-423
+//   LASWP      src/lapack/getrf.cc:28-81
+//   GetrfLeaf  src/lapack/factor_kernels.cc:79-183
+//   PotrfLeaf  src/lapack/factor_kernels.cc:187-221
+// "lanes" is the vector length (in elements) of the reference's SIMD target:
+// AXPY columns shorter than one vector are updated as y + (alpha*x) (two
+// roundings), longer ones as fma(x, alpha, y) (factor_kernels.cc:79-118).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+#include <cstdlib>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace hb {
+
+int RefLanesDouble() {
+  static int lanes = [] {
+    const char* e = getenv("HWYBLAS_REF_LANES");
+    const int v = e ? atoi(e) : 8;
+    return v == 4 ? 4 : 8;
+  }();
+  return lanes;
+}
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T Sfmin();
+template <>
+__device__ __forceinline__ double Sfmin<double>() { return DBL_MIN; }
+template <>
+__device__ __forceinline__ float Sfmin<float>() { return FLT_MIN; }
+
+// y + alpha*x in the reference's rounding for a column of length len.
+template <typename T>
+__device__ __forceinline__ T Axpy(T y, T alpha, T x, int len, int lanes) {
+  if (len < lanes) {
+    const T p = alpha * x;
+    return y + p;
+  }
+  return fma(x, alpha, y);
+}
+
+// (value, index) candidates: larger value wins, then the smaller index.
+// value < 0 marks "no candidate" (no rows, or only NaNs).
+template <typename T>
+__device__ __forceinline__ bool Better(T v, int i, T bv, int bi) {
+  return v > bv || (v == bv && v >= T(0) && i < bi);
+}
+
+// ---------------------------------------------------------------------------
+// IAMAX: per-block candidates, then the last block to finish reduces them.
+template <typename T>
+__global__ void IamaxKernel(int n, const T* x, long long incx, T* part_v,
+                            int* part_i, unsigned int* ticket, int* out) {
+  T bv = T(-1);
+  int bi = 0x7fffffff;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+       i < n; i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const T v = fabs(x[i * incx]);
+    if (v > bv) {  // strict: NaN never wins; each thread visits i ascending
+      bv = v;
+      bi = static_cast<int>(i);
+    }
+  }
+  __shared__ T sv[32];
+  __shared__ int si[32];
+  for (int off = 16; off > 0; off >>= 1) {
+    const T ov = __shfl_down_sync(0xffffffffu, bv, off);
+    const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+    if (Better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+  }
+  if (threadIdx.x % 32 == 0) { sv[threadIdx.x / 32] = bv; si[threadIdx.x / 32] = bi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < static_cast<int>(blockDim.x / 32); ++w)
+      if (Better(sv[w], si[w], bv, bi)) { bv = sv[w]; bi = si[w]; }
+    part_v[blockIdx.x] = bv;
+    part_i[blockIdx.x] = bi;
+    __threadfence();
+    const unsigned int done = atomicAdd(ticket, 1u);
+    if (done == gridDim.x - 1) {
+      __threadfence();
+      T gv = T(-1);
+      int gi = 0x7fffffff;
+      for (unsigned int b = 0; b < gridDim.x; ++b) {
+        const T v = *(volatile T*)&part_v[b];
+        const int i = *(volatile int*)&part_i[b];
+        if (Better(v, i, gv, gi)) { gv = v; gi = i; }
+      }
+      // The reference returns index 0 when x[0] is NaN (and x[0] is the
+      // first candidate otherwise).
+      if (isnan(fabs(x[0])) || gi == 0x7fffffff) gi = 0;
+      *out = gi + 1;
+      *ticket = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// LASWP: one thread per column applies the interchanges in order.
+template <typename T>
+__global__ void LaswpKernel(int n, T* a, long long lda, int i1, int i2,
+                            int inc, int ix0, int incx, const int* ipiv,
+                            const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= n) return;
+  T* ac = a + col * lda;
+  int ix = ix0;
+  for (int i = i1; inc > 0 ? i <= i2 : i >= i2; i += inc) {
+    const int ip = ipiv[ix - 1];
+    if (ip != i) {
+      const T t = ac[i - 1];
+      ac[i - 1] = ac[ip - 1];
+      ac[ip - 1] = t;
+    }
+    ix += incx;
+  }
+}
+
+__global__ void AdjustPivotsKernel(int* ipiv, int begin, int end, int delta) {
+  const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < end) ipiv[i] += delta;
+}
+
+// ---------------------------------------------------------------------------
+// LU leaf, pivot columns: the m x w panel (w <= 16) is split by rows over P
+// co-resident CTAs (cooperative launch), each holding its rows in shared
+// memory. Per column j: every CTA publishes its best candidate (|a|, row,
+// row contents), one grid barrier, then every CTA picks the same pivot and
+// applies the swap, the scaling and the rank-1 update to its own rows.
+constexpr int kLeafThreads = 512;
+constexpr int kLeafMaxRows = 1024;  // rows per CTA
+constexpr int kLeafW = 16;
+
+template <typename T>
+struct LeafArgs {
+  int m, w, lanes;
+  T* a;
+  long long lda;
+  int* ipiv;
+  int* info;
+  int info_base;
+  T* xchg;                // [2][P][kLeafW + 2] candidates, [2][kLeafW] row j
+  unsigned int* barrier;  // zeroed before launch
+  int* timeout_flag;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kLeafThreads)
+    GetrfLeafPanelKernel(LeafArgs<T> p) {
+  extern __shared__ __align__(16) uint8_t leaf_smem[];
+  T* sp = reinterpret_cast<T*>(leaf_smem);  // column-major [w][R]
+  __shared__ T s_piv[kLeafW], s_rowj[kLeafW];
+  __shared__ T s_wv[kLeafThreads / 32];
+  __shared__ int s_wi[kLeafThreads / 32];
+  __shared__ int s_p;
+  const int P = gridDim.x, cta = blockIdx.x;
+  const int rows_per = (p.m + P - 1) / P;
+  const int r0 = cta * rows_per, r1 = min(p.m, r0 + rows_per);
+  const int R = rows_per;
+  const int w = p.w;
+  const int slot_len = kLeafW + 2;
+  T* cand = p.xchg;                       // [2][P][slot_len]
+  T* rowj_buf = p.xchg + 2 * P * slot_len;  // [2][kLeafW]
+
+  for (int idx = threadIdx.x; idx < w * R; idx += blockDim.x) {
+    const int c = idx / R, lr = idx % R;
+    if (r0 + lr < r1) sp[c * R + lr] = p.a[(r0 + lr) + c * p.lda];
+  }
+  __syncthreads();
+
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    // (a) local candidate over rows >= j.
+    T bv = T(-1);
+    int bi = 0x7fffffff;
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+      const int gi = r0 + lr;
+      if (gi < j) continue;
+      const T v = fabs(sp[j * R + lr]);
+      if (v > bv) { bv = v; bi = gi; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const T ov = __shfl_down_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (Better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    }
+    if (threadIdx.x % 32 == 0) { s_wv[threadIdx.x / 32] = bv; s_wi[threadIdx.x / 32] = bi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int q = 1; q < kLeafThreads / 32; ++q)
+        if (Better(s_wv[q], s_wi[q], bv, bi)) { bv = s_wv[q]; bi = s_wi[q]; }
+      s_p = bi;
+      s_wv[0] = bv;
+    }
+    __syncthreads();
+    // (b) publish the candidate row and, by its owner, row j.
+    {
+      T* slot = cand + (par * P + cta) * slot_len;
+      const int ci = s_p;
+      if (threadIdx.x == 0) {
+        slot[0] = s_wv[0];
+        slot[1] = static_cast<T>(ci == 0x7fffffff ? -1 : ci);
+      }
+      if (threadIdx.x < w) {
+        slot[2 + threadIdx.x] =
+            (ci != 0x7fffffff) ? sp[threadIdx.x * R + (ci - r0)] : T(0);
+        if (j >= r0 && j < r1)
+          rowj_buf[par * kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
+      }
+    }
+    if (P > 1) {
+      if (!GridBarrier(p.barrier, P, j + 1, p.timeout_flag)) return;
+    } else {
+      __syncthreads();
+    }
+    // (c) the global pivot: the reference's IAMAX over rows j..m-1.
+    if (threadIdx.x == 0) {
+      T gv = T(-1);
+      int gi = 0x7fffffff;
+      for (int q = 0; q < P; ++q) {
+        const T* slot = cand + (par * P + q) * slot_len;
+        const T v = *(volatile const T*)&slot[0];
+        const T fi = *(volatile const T*)&slot[1];
+        if (fi < T(0)) continue;
+        const int i = static_cast<int>(fi);
+        if (Better(v, i, gv, gi)) { gv = v; gi = i; }
+      }
+      const T ajj = *(volatile const T*)&rowj_buf[par * kLeafW + j];
+      if (isnan(fabs(ajj)) || gi == 0x7fffffff) gi = j;
+      s_p = gi;
+    }
+    __syncthreads();
+    const int piv = s_p;
+    if (threadIdx.x < w) {
+      const T rj = *(volatile const T*)&rowj_buf[par * kLeafW + threadIdx.x];
+      s_rowj[threadIdx.x] = rj;
+      if (piv == j) {
+        s_piv[threadIdx.x] = rj;
+      } else {
+        // The winner's slot holds row piv.
+        T val = T(0);
+        for (int q = 0; q < P; ++q) {
+          const T* slot = cand + (par * P + q) * slot_len;
+          if (static_cast<int>(*(volatile const T*)&slot[1]) == piv &&
+              *(volatile const T*)&slot[1] >= T(0)) {
+            val = *(volatile const T*)&slot[2 + threadIdx.x];
+          }
+        }
+        s_piv[threadIdx.x] = val;
+      }
+    }
+    __syncthreads();
+    const T pivot = s_piv[j];
+    if (cta == 0 && threadIdx.x == 0) {
+      p.ipiv[j] = piv + 1;
+      if (pivot == T(0) && *p.info == 0) *p.info = p.info_base + j + 1;
+    }
+    if (pivot != T(0)) {
+      // (d) interchange rows j and piv across the leaf's columns.
+      if (piv != j && threadIdx.x < w) {
+        if (piv >= r0 && piv < r1) sp[threadIdx.x * R + (piv - r0)] = s_rowj[threadIdx.x];
+        if (j >= r0 && j < r1) sp[threadIdx.x * R + (j - r0)] = s_piv[threadIdx.x];
+      }
+      __syncthreads();
+      // (e) column j below the diagonal: * (1/pivot), or / pivot if tiny.
+      const bool tiny = !(fabs(pivot) >= Sfmin<T>());
+      const T rinv = T(1) / pivot;
+      for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+        if (r0 + lr <= j) continue;
+        T& x = sp[j * R + lr];
+        x = tiny ? x / pivot : x * rinv;
+      }
+    }
+    __syncthreads();
+    // (f) rank-1 update of columns j+1..w-1 (AXPY with alpha = -a(j, k)).
+    const int len = p.m - j - 1;
+    for (int idx = threadIdx.x; idx < (w - j - 1) * (r1 - r0); idx += blockDim.x) {
+      const int k = j + 1 + idx / (r1 - r0), lr = idx % (r1 - r0);
+      if (r0 + lr <= j) continue;
+      const T alpha = -s_piv[k];
+      sp[k * R + lr] = Axpy(sp[k * R + lr], alpha, sp[j * R + lr], len, p.lanes);
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < w * R; idx += blockDim.x) {
+    const int c = idx / R, lr = idx % R;
+    if (r0 + lr < r1) p.a[(r0 + lr) + c * p.lda] = sp[c * R + lr];
+  }
+}
+
+// LU leaf, trailing columns (n > m, m <= 16): each column replays the leaf's
+// interchanges and AXPY updates on its own (columns are independent).
+template <typename T>
+__global__ void GetrfLeafTrailingKernel(int m, int w, int n, T* a,
+                                        long long lda, const int* ipiv,
+                                        int lanes) {
+  const int k = w + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  T* col = a + k * lda;
+  for (int j = 0; j < w; ++j) {
+    const int p = ipiv[j] - 1;
+    const T pivot = a[j + j * lda];  // a(j, j) after the interchange
+    if (pivot != T(0) && p != j) {
+      const T t = col[j];
+      col[j] = col[p];
+      col[p] = t;
+    }
+    const T alpha = -col[j];
+    const int len = m - j - 1;
+    for (int i = j + 1; i < m; ++i) col[i] = Axpy(col[i], alpha, a[i + j * lda], len, lanes);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cholesky leaf (n <= 64) in one CTA, the block in shared memory.
+__global__ void __launch_bounds__(256)
+    PotrfLeafKernel(int upper, int n, double* a, long long lda, int* info,
+                    int info_base, int lanes, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ double s[64][65];  // s[i][j] = A(i, j)
+  __shared__ double row[64];
+  __shared__ int stop;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    const bool ref = upper ? (i <= j) : (i >= j);
+    s[i][j] = ref ? a[i + j * lda] : 0.0;
+  }
+  if (threadIdx.x == 0) stop = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      const double ajj = s[j][j];
+      if (ajj <= 0.0 || isnan(ajj)) {
+        stop = 1;
+        if (*info == 0) *info = info_base + j + 1;
+      } else {
+        const double r = sqrt(ajj);
+        s[j][j] = r;
+        row[j] = 1.0 / r;  // rinv
+      }
+    }
+    __syncthreads();
+    if (stop) break;
+    const double rinv = row[j];
+    __syncthreads();
+    if (upper) {
+      for (int k = j + 1 + threadIdx.x; k < n; k += blockDim.x) {
+        s[j][k] = s[j][k] * rinv;
+        row[k] = s[j][k];
+      }
+      __syncthreads();
+      // Column k, rows j+1..k: y += (-U(j,k)) * row, length k - j.
+      for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, k = idx / n;
+        if (k <= j || i <= j || i > k) continue;
+        s[i][k] = Axpy(s[i][k], -s[j][k], row[i], k - j, lanes);
+      }
+    } else {
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) s[i][j] = s[i][j] * rinv;
+      __syncthreads();
+      // Column k, rows k..n-1: y += (-L(k,j)) * L(k:n, j), length n - k.
+      for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, k = idx / n;
+        if (k <= j || i < k) continue;
+        s[i][k] = Axpy(s[i][k], -s[k][j], s[i][j], n - k, lanes);
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    const bool ref = upper ? (i <= j) : (i >= j);
+    if (ref) a[i + j * lda] = s[i][j];
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void Iamax(int n, const T* x, int incx, int* out) {
+  Context& ctx = Ctx();
+  const int blocks = static_cast<int>(std::min<long long>((n + 1023) / 1024, 296));
+  T* pv = static_cast<T*>(Workspace(kWsLeaf, 296 * (sizeof(T) + sizeof(int))));
+  int* pi = reinterpret_cast<int*>(pv + 296);
+  unsigned int* ticket = reinterpret_cast<unsigned int*>(ctx.dev_status + 8);
+  IamaxKernel<T><<<std::max(blocks, 1), 1024, 0, ctx.stream>>>(n, x, incx, pv,
+                                                                pi, ticket, out);
+  CountLaunch();
+  LaunchFailed("iamax");
+}
+template void Iamax<double>(int, const double*, int, int*);
+template void Iamax<float>(int, const float*, int, int*);
+
+template <typename T>
+void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
+  if (n <= 0 || incx == 0) return;
+  int i1, i2, inc, ix0;
+  if (incx > 0) {
+    ix0 = k1; i1 = k1; i2 = k2; inc = 1;
+  } else {
+    ix0 = k1 + (k1 - k2) * incx; i1 = k2; i2 = k1; inc = -1;
+  }
+  if (inc > 0 ? i1 > i2 : i1 < i2) return;
+  LaswpKernel<T><<<(n + 127) / 128, 128, 0, Ctx().stream>>>(
+      n, a, lda, i1, i2, inc, ix0, incx, ipiv, Ctx().guard);
+  CountLaunch();
+  LaunchFailed("laswp");
+}
+template void Laswp<double>(int, double*, int, int, int, const int*, int);
+template void Laswp<float>(int, float*, int, int, int, const int*, int);
+
+void AdjustPivots(int* ipiv, int begin, int end, int delta) {
+  if (end <= begin || delta == 0) return;
+  AdjustPivotsKernel<<<(end - begin + 255) / 256, 256, 0, Ctx().stream>>>(
+      ipiv, begin, end, delta);
+  CountLaunch();
+  LaunchFailed("adjust pivots");
+}
+
+template <typename T>
+void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
+               int info_base) {
+  Context& ctx = Ctx();
+  const int w = std::min(m, n);
+  const int lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  const int P = (m + kLeafMaxRows - 1) / kLeafMaxRows;
+  const int R = (m + P - 1) / P;
+  const size_t smem = static_cast<size_t>(w) * R * sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kLeafW * kLeafMaxRows * static_cast<int>(sizeof(T)));
+    configured = true;
+  }
+  LeafArgs<T> args;
+  args.m = m;
+  args.w = w;
+  args.lanes = lanes;
+  args.a = a;
+  args.lda = lda;
+  args.ipiv = ipiv;
+  args.info = info;
+  args.info_base = info_base;
+  args.xchg = static_cast<T*>(
+      Workspace(kWsLeaf, sizeof(T) * (2 * P * (kLeafW + 2) + 2 * kLeafW)));
+  args.barrier = reinterpret_cast<unsigned int*>(ctx.dev_status + 16);
+  args.timeout_flag = ctx.dev_status;
+  if (P > 1) {
+    cudaMemsetAsync(args.barrier, 0, sizeof(unsigned int), ctx.stream);
+    void* kargs[] = {&args};
+    Failed(cudaLaunchCooperativeKernel(
+               reinterpret_cast<void*>(GetrfLeafPanelKernel<T>), P,
+               kLeafThreads, kargs, smem, ctx.stream),
+           "getrf leaf (cooperative)");
+  } else {
+    GetrfLeafPanelKernel<T><<<1, kLeafThreads, smem, ctx.stream>>>(args);
+  }
+  CountLaunch();
+  LaunchFailed("getrf leaf");
+  if (n > w) {
+    GetrfLeafTrailingKernel<T><<<(n - w + 127) / 128, 128, 0, ctx.stream>>>(
+        m, w, n, a, lda, ipiv, lanes);
+    CountLaunch();
+    LaunchFailed("getrf leaf trailing");
+  }
+}
+template void GetrfLeaf<double>(int, int, double*, int, int*, int*, int);
+template void GetrfLeaf<float>(int, int, float*, int, int*, int*, int);
+
+void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base) {
+  PotrfLeafKernel<<<1, 256, 0, Ctx().stream>>>(upper ? 1 : 0, n, a, lda, info,
+                                               info_base, RefLanesDouble(),
+                                               Ctx().guard);
+  CountLaunch();
+  LaunchFailed("potrf leaf");
+}
+
+}  // namespace hb

@@ -1,0 +1,427 @@
+// FP64 GEMM on the FP64 tensor pipe (DMMA), bit-identical to the reference.
+//
+// The reference computes every C element as a sequential FMA chain over k,
+// restarted from 0 every KC = 256 (src/gemm_kernel-inl.h:72, 161-176;
+// src/gemm-inl.h:176-178), and merges each chunk as r = alpha*acc, then
+// C = r + C (beta 1), fma(C, beta, r) (other beta, first chunk only) or r
+// (beta 0, C not read) (src/gemm_kernel-inl.h:182-224). Tiles of a triangular
+// C that cross the diagonal are merged as r + beta*C instead
+// (src/gemm-inl.h:110-130, 219-225).
+//
+// mma.sync.m16n8k8.f64 accumulates its 8 products in ascending k as a chain
+// of correctly rounded FMAs starting from the C operand (measured on B200 on
+// random operands spanning 2^-20..2^20: 38400 of 38400 outputs identical to
+// the sequential chain), so chaining the MMAs in ascending k and restarting
+// the accumulator every 256 reproduces the reference bit for bit.
+//
+// Tiling: a CTA computes a 128 x 64 tile of C with 8 consumer warps (32 x 32
+// each: 2 x 4 MMAs per k8 step) and one producer warp that streams 16-deep k
+// slices of op(A) (128 x 16, M-contiguous) and op(B) (16 x 64, K-contiguous,
+// 128-byte swizzle) into a 4-stage shared-memory ring with TMA and mbarriers.
+// Rows of each 16-row MMA block are interleaved (MMA row g <-> tile row 2g,
+// g+8 <-> 2g+1) so that each thread's A fragment is one 16-byte shared load
+// and every shared load is bank-conflict free.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace hb {
+namespace {
+
+constexpr int kBM = 128, kBN = 64, kBK = 16, kStages = 4;
+constexpr int kConsumerWarps = 8;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
+constexpr int kTileABytes = kBM * kBK * 8;
+constexpr int kTileBBytes = kBN * kBK * 8;
+constexpr int kStageBytes = kTileABytes + kTileBBytes;
+constexpr int kKtPerChunk = 256 / kBK;  // k-slices per reference KC chunk
+constexpr int kSmemBytes = kStages * kStageBytes + 2 * kStages * 8 + 1024;
+
+struct GemmParams {
+  int m, n, k;
+  double alpha, beta;
+  double* c;
+  long long ldc;
+  int part;
+  int* timeout_flag;
+  const int* guard;
+};
+
+// Whether C(i, j) lies in a micro-tile of the reference's AVX-512 double
+// kernel (MR 16, NR 12, MC 96, NC 4080) that crosses the diagonal
+// (src/gemm-inl.h:93-106; src/gemm_kernel-inl.h:64-74).
+__device__ __forceinline__ bool InCrossingTile(int part, int m, int n, int i,
+                                               int j) {
+  constexpr int MR = 16, NR = 12, MC = 96, NC = 4080;
+  const int ic = i / MC * MC, mcb = min(MC, m - ic);
+  const int ir = (i - ic) / MR * MR, mr = min(MR, mcb - ir);
+  const int jc = j / NC * NC, ncb = min(NC, n - jc);
+  const int jr = (j - jc) / NR * NR, nr = min(NR, ncb - jr);
+  const int i0 = ic + ir, j0 = jc + jr;
+  if (part == kLower) return !(i0 > j0 + nr - 1);
+  return !(i0 + mr - 1 < j0);
+}
+
+__device__ __forceinline__ bool InPart(const GemmParams& p, int i, int j) {
+  if (i >= p.m || j >= p.n) return false;
+  if (p.part == kLower) return i >= j;
+  if (p.part == kUpper) return i <= j;
+  return true;
+}
+
+__device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
+                                     double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+}
+
+template <bool kMulti>
+__global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
+    DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
+                    const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  const int tiles_m = (p.m + kBM - 1) / kBM;
+  const int m0 = (blockIdx.x % tiles_m) * kBM;
+  const int n0 = (blockIdx.x / tiles_m) * kBN;
+  if (p.part == kLower && m0 + kBM - 1 < n0) return;
+  if (p.part == kUpper && m0 > n0 + kBN - 1) return;
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024 - (SmemAddr(smem_raw) & 1023)) & 1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      MbarInit(&full[s], 1);
+      MbarInit(&empty[s], kConsumerWarps);
+    }
+    FenceBarrierInit();
+  }
+  __syncthreads();
+  const int kt_total = (p.k + kBK - 1) / kBK;
+
+  if (warp == kConsumerWarps) {
+    // Producer warp: one lane streams the k-slices through the ring.
+    if (lane == 0) {
+      PrefetchTmap(&tm_a);
+      PrefetchTmap(&tm_b);
+      for (int kt = 0; kt < kt_total; ++kt) {
+        const int s = kt % kStages, round = kt / kStages;
+        if (round > 0 && !MbarWait(&empty[s], (round - 1) & 1, p.timeout_flag))
+          break;
+        uint8_t* st = smem + s * kStageBytes;
+        MbarArriveExpectTx(&full[s], kStageBytes);
+        TmaLoad2d(st, &tm_a, m0, kt * kBK, &full[s]);
+        TmaLoad2d(st + kTileABytes, &tm_b, kt * kBK, n0, &full[s]);
+      }
+    }
+    return;
+  }
+
+  const int wm = warp % 4, wn = warp / 4;
+  const int g = lane >> 2, t = lane & 3;
+  // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1), col0 + nb*8 + (e & 1)).
+  const int row0 = m0 + wm * 32 + 2 * g, col0 = n0 + wn * 32 + 2 * t;
+  double acc[2][4][4];
+  double cacc[2][4][4];  // kMulti: C_in, then the running merged value
+  uint32_t in_part = 0, crossing = 0;
+#pragma unroll
+  for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+    for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int bit = (mb * 4 + nb) * 4 + e;
+        const int i = row0 + mb * 16 + (e >> 1), j = col0 + nb * 8 + (e & 1);
+        acc[mb][nb][e] = 0.0;
+        const bool inside = InPart(p, i, j);
+        if (inside) in_part |= 1u << bit;
+        if (inside && p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j))
+          crossing |= 1u << bit;
+        if constexpr (kMulti) {
+          cacc[mb][nb][e] =
+              (inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
+        }
+      }
+
+  for (int kt = 0; kt < kt_total; ++kt) {
+    const int s = kt % kStages, round = kt / kStages;
+    if (!MbarWait(&full[s], round & 1, p.timeout_flag)) return;
+    const double* sa = reinterpret_cast<const double*>(smem + s * kStageBytes);
+    const uint8_t* sb = smem + s * kStageBytes + kTileABytes;
+#pragma unroll
+    for (int ks = 0; ks < kBK / 8; ++ks) {
+      double af[2][4];
+#pragma unroll
+      for (int mb = 0; mb < 2; ++mb) {
+        const int row = wm * 32 + mb * 16 + 2 * g;
+        const double2 lo =
+            *reinterpret_cast<const double2*>(sa + (ks * 8 + t) * kBM + row);
+        const double2 hi = *reinterpret_cast<const double2*>(
+            sa + (ks * 8 + t + 4) * kBM + row);
+        af[mb][0] = lo.x;
+        af[mb][1] = lo.y;
+        af[mb][2] = hi.x;
+        af[mb][3] = hi.y;
+      }
+#pragma unroll
+      for (int nb = 0; nb < 4; ++nb) {
+        const int r = wn * 32 + nb * 8 + g;
+        const int k0 = ks * 8 + t, k1 = k0 + 4;
+        const double b0 = *reinterpret_cast<const double*>(
+            sb + r * 128 + (((k0 >> 1) ^ (r & 7)) << 4) + ((k0 & 1) << 3));
+        const double b1 = *reinterpret_cast<const double*>(
+            sb + r * 128 + (((k1 >> 1) ^ (r & 7)) << 4) + ((k1 & 1) << 3));
+        Dmma(acc[0][nb], af[0], b0, b1);
+        Dmma(acc[1][nb], af[1], b0, b1);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) MbarArrive(&empty[s]);
+
+    if constexpr (kMulti) {
+      // End of a reference KC chunk: merge into the running C value.
+      if ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_total) {
+        const bool first = (kt < kKtPerChunk);
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+          for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int bit = (mb * 4 + nb) * 4 + e;
+              const double r = p.alpha * acc[mb][nb][e];
+              double& cv = cacc[mb][nb][e];
+              if (!first || p.beta == 1.0) {
+                cv = r + cv;
+              } else if (p.beta == 0.0) {
+                cv = r;
+              } else if ((crossing >> bit) & 1u) {
+                const double bc = p.beta * cv;
+                cv = r + bc;
+              } else {
+                cv = fma(cv, p.beta, r);
+              }
+              acc[mb][nb][e] = 0.0;
+            }
+      }
+    }
+  }
+
+  // Epilogue: write C.
+#pragma unroll
+  for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+    for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int bit = (mb * 4 + nb) * 4 + e;
+        if (!((in_part >> bit) & 1u)) continue;
+        const int i = row0 + mb * 16 + (e >> 1), j = col0 + nb * 8 + (e & 1);
+        double v;
+        if constexpr (kMulti) {
+          v = cacc[mb][nb][e];
+        } else {
+          const double r = p.alpha * acc[mb][nb][e];
+          if (p.beta == 0.0) {
+            v = r;
+          } else {
+            const double cin = p.c[i + j * p.ldc];
+            if ((crossing >> bit) & 1u) {
+              const double bc = p.beta * cin;
+              v = r + bc;
+            } else if (p.beta == 1.0) {
+              v = r + cin;
+            } else {
+              v = fma(cin, p.beta, r);
+            }
+          }
+        }
+        p.c[i + j * p.ldc] = v;
+      }
+}
+
+// Copies op(X) (rows x cols, strided view) into a dense column-major buffer
+// with leading dimension ld, through a 32 x 32 shared tile so that both the
+// read (along X's contiguous dimension) and the write are coalesced.
+template <typename T>
+__global__ void CanonicalCopyKernel(View<T> x, int rows, int cols, T* dst,
+                                    long long ld) {
+  __shared__ T tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const bool trans = x.rs != 1;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    // Untransposed: threadIdx.x runs along i (contiguous); else along j.
+    const int i = trans ? i0 + r : i0 + threadIdx.x;
+    const int j = trans ? j0 + threadIdx.x : j0 + r;
+    if (i < rows && j < cols) {
+      const T v = x.data[i * x.rs + j * x.cs];
+      if (trans) tile[threadIdx.x][r] = v; else tile[r][threadIdx.x] = v;
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + threadIdx.x, j = j0 + r;
+    if (i < rows && j < cols) dst[i + j * ld] = tile[r][threadIdx.x];
+  }
+}
+
+template <typename T>
+__global__ void ScaleKernel(int m, int n, T beta, T* c, long long ldc,
+                            int part, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  const long long total = static_cast<long long>(m) * n;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) +
+                       threadIdx.x;
+       idx < total; idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(idx % m), j = static_cast<int>(idx / m);
+    if (part == kLower && i < j) continue;
+    if (part == kUpper && i > j) continue;
+    T* cij = c + i + j * ldc;
+    *cij = (beta == T(0)) ? T(0) : *cij * beta;
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
+                                   void*, const cuuint64_t*, const cuuint64_t*,
+                                   const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+EncodeTiledFn Encoder() {
+  static EncodeTiledFn fn = [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr,
+                                cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      fprintf(stderr, "hwyblas_b200: cuTensorMapEncodeTiled unavailable\n");
+      return static_cast<EncodeTiledFn>(nullptr);
+    }
+    return reinterpret_cast<EncodeTiledFn>(ptr);
+  }();
+  return fn;
+}
+
+}  // namespace
+
+// 2-D tensor map over a column-major matrix (inner dimension `rows`).
+bool MakeTensorMap2d(CUtensorMap* map, CUtensorMapDataType dtype, int elem,
+                     const void* base, long long rows, long long cols,
+                     long long ld, int box_rows, int box_cols,
+                     CUtensorMapSwizzle swizzle) {
+  const EncodeTiledFn enc = Encoder();
+  if (enc == nullptr) return false;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(rows),
+                              static_cast<cuuint64_t>(cols)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * elem)};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_rows),
+                             static_cast<cuuint32_t>(box_cols)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r =
+      enc(map, dtype, 2, const_cast<void*>(base), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    fprintf(stderr, "hwyblas_b200: cuTensorMapEncodeTiled failed (%d)\n",
+            static_cast<int>(r));
+    return false;
+  }
+  return true;
+}
+
+// Whether a column-major operand can be read by TMA in place: 16-byte
+// aligned base and leading dimension.
+static bool TmaReady(const void* p, long long ld, int elem) {
+  return (reinterpret_cast<uintptr_t>(p) % 16 == 0) && ((ld * elem) % 16 == 0);
+}
+
+template <typename T>
+const T* Canonical(View<T> x, int rows, int cols, int slot, long long* ld_out) {
+  if (!x.trans() && TmaReady(x.data, x.ld(), sizeof(T))) {
+    *ld_out = x.ld();
+    return x.data;
+  }
+  const long long ld = (rows + 15) / 16 * 16;
+  T* dst = static_cast<T*>(Workspace(slot, sizeof(T) * ld * cols));
+  const dim3 grid((rows + 31) / 32, (cols + 31) / 32);
+  CanonicalCopyKernel<T><<<grid, dim3(32, 8), 0, Ctx().stream>>>(x, rows, cols,
+                                                                  dst, ld);
+  CountLaunch();
+  LaunchFailed("canonical copy");
+  *ld_out = ld;
+  return dst;
+}
+template const double* Canonical(View<double>, int, int, int, long long*);
+template const float* Canonical(View<float>, int, int, int, long long*);
+
+void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
+           double beta, double* c, int ldc, Part part) {
+  Context& ctx = Ctx();
+  long long lda, ldb;
+  const double* ca = Canonical(a, m, k, kWsPackA, &lda);
+  const double* cb = Canonical(b, k, n, kWsPackB, &ldb);
+  CUtensorMap ma, mb;
+  if (!MakeTensorMap2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ca, m, k, lda,
+                       kBM, kBK, CU_TENSOR_MAP_SWIZZLE_NONE) ||
+      !MakeTensorMap2d(&mb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, cb, k, n, ldb,
+                       kBK, kBN, CU_TENSOR_MAP_SWIZZLE_128B)) {
+    Failed(cudaErrorInvalidValue, "dgemm tensor map");
+    return;
+  }
+  GemmParams p;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.c = c;
+  p.ldc = ldc;
+  p.part = part;
+  p.timeout_flag = ctx.dev_status;
+  p.guard = ctx.guard;
+  const long long tiles =
+      static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(DgemmDmmaKernel<true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    cudaFuncSetAttribute(DgemmDmmaKernel<false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    configured = true;
+  }
+  if (k > 256) {
+    DgemmDmmaKernel<true><<<static_cast<unsigned>(tiles), kThreads, kSmemBytes,
+                            ctx.stream>>>(ma, mb, p);
+  } else {
+    DgemmDmmaKernel<false><<<static_cast<unsigned>(tiles), kThreads, kSmemBytes,
+                             ctx.stream>>>(ma, mb, p);
+  }
+  CountLaunch();
+  LaunchFailed("dgemm");
+}
+
+template <typename T>
+void ScaleMatrix(int m, int n, T beta, T* c, int ldc, Part part) {
+  if (m <= 0 || n <= 0) return;
+  const long long total = static_cast<long long>(m) * n;
+  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 8));
+  ScaleKernel<T><<<blocks, 256, 0, Ctx().stream>>>(m, n, beta, c, ldc, part,
+                                                   Ctx().guard);
+  CountLaunch();
+  LaunchFailed("scale");
+}
+template void ScaleMatrix<double>(int, int, double, double*, int, Part);
+template void ScaleMatrix<float>(int, int, float, float*, int, Part);
+
+}  // namespace hb

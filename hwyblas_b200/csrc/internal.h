@@ -1,0 +1,152 @@
+// Internal interfaces of libhwyblas_b200: per-thread context (stream, device
+// workspace, error state) and the device-level routines. Device-level
+// routines take device pointers, column-major with leading dimensions, and
+// only enqueue work on the context's stream; the C ABI (api.cc) validates
+// arguments, stages host memory and synchronises.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+
+namespace hb {
+
+// Which part of C a product updates (the reference's Part, src/gemm.h:39).
+enum Part : int { kAll = 0, kLower = 1, kUpper = 2 };
+
+// A strided view of op(X): element (i, p) is data[i * rs + p * cs], with one
+// of rs, cs equal to 1 (column-major storage, possibly transposed). This is
+// the reference's Operand (src/gemm.h:28-36) for general matrices.
+template <typename T>
+struct View {
+  const T* data = nullptr;
+  long long rs = 1, cs = 1;
+  View sub(long long i0, long long j0) const {
+    View v = *this;
+    v.data += i0 * rs + j0 * cs;
+    return v;
+  }
+  bool trans() const { return rs != 1; }
+  long long ld() const { return rs != 1 ? rs : cs; }
+};
+template <typename T>
+inline View<T> ColMajor(const T* p, long long ld, bool trans = false) {
+  View<T> v;
+  v.data = p;
+  v.rs = trans ? ld : 1;
+  v.cs = trans ? 1 : ld;
+  return v;
+}
+
+struct Context {
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int device = -1;
+  int num_sms = 148;
+  // Device status words: [0] wait-timeout flag written by kernels whose
+  // bounded waits gave up; [1] LAPACK INFO of the running driver; the rest
+  // are grid-barrier counters and scratch ints.
+  int* dev_status = nullptr;
+  // If non-null, kernels return at once while *guard != 0 (used by drivers
+  // that must stop after a failure, e.g. Cholesky's non-positive minor).
+  const int* guard = nullptr;
+  int last_error = 0;
+};
+
+// The calling thread's context on the current device (created on first use).
+Context& Ctx();
+// Grows and returns slot `slot` of the thread's device workspace (at least
+// `bytes`, 256-byte aligned). Valid until the next call with the same slot.
+void* Workspace(int slot, size_t bytes);
+enum WorkspaceSlot : int {
+  kWsStageA = 0,   // host-pointer staging
+  kWsStageB = 1,
+  kWsStageC = 2,
+  kWsPackA = 3,    // canonical (transposed / realigned) GEMM operands
+  kWsPackB = 4,
+  kWsLeaf = 5,     // LU panel exchange buffers
+  kWsEmul = 6,     // emulated-GEMM slices
+  kWsEmulAcc = 7,
+  kWsMixed = 8,    // mixed-precision solver buffers
+  kWsMixed2 = 9,
+  kWsMixed3 = 10,
+  kWsBatch = 11,
+  kNumWorkspaceSlots = 12
+};
+
+// Records a CUDA error on the context and prints it; returns true if `e` is
+// an error.
+bool Failed(cudaError_t e, const char* what);
+// Checks the last launch.
+bool LaunchFailed(const char* what);
+
+extern std::atomic<uint64_t> g_launches;
+inline void CountLaunch(uint64_t n = 1) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+// ---------------------------------------------------------------------------
+// Device-level routines (device pointers; stream-ordered on Ctx().stream).
+
+// C := alpha*op(A)*op(B) + beta*C on `part` of C; requires m, n, k > 0 and
+// alpha != 0. Bit-identical to the reference's GEMM (double: chunks of 256).
+void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
+           double beta, double* c, int ldc, Part part = kAll);
+// FP32 (chunks of 384), FFMA on the CUDA cores.
+void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
+           float beta, float* c, int ldc);
+// C := beta*C on `part` (beta == 0 writes zeros without reading C).
+template <typename T>
+void ScaleMatrix(int m, int n, T beta, T* c, int ldc, Part part = kAll);
+// Solves X*T = B (right) or T*X = B (left) for an r x r triangular op(A)
+// `tri` (lower/unit as given for op(A)); B is r x other (left) or other x r.
+template <typename T>
+void TrsmSolve(bool left, View<T> tri, bool lower, bool unit, int r,
+               int other, T* b, int ldb);
+// Device IAMAX: writes the 1-based index to *out (device int).
+template <typename T>
+void Iamax(int n, const T* x, int incx, int* out);
+// LASWP on device data; ipiv is a device array (1-based, Fortran k1/k2/incx).
+template <typename T>
+void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx);
+// ipiv[i] += delta for i in [begin, end) (device).
+void AdjustPivots(int* ipiv, int begin, int end, int delta);
+// GetrfLeaf on device: m x n, min(m, n) <= 16; ipiv (device, leaf-relative,
+// 1-based); *info (device) set to info_base + j + 1 at the first zero pivot
+// if it is still 0.
+template <typename T>
+void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base);
+// PotrfLeaf on device: n <= 64; sets *info to info_base + j + 1 and stops at
+// the first non-positive (or NaN) diagonal, if *info is still 0.
+void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base);
+
+// LAPACK drivers on device data (ipiv, info: device pointers).
+template <typename T>
+void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info);
+template <typename T>
+void Getrf2(int m, int n, T* a, int lda, int* ipiv, int* info);
+template <typename T>
+void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
+           T* b, int ldb);
+void Potrf(bool upper, int n, double* a, int lda, int* info);
+void Potrf2(bool upper, int n, double* a, int lda, int* info);
+void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
+           int ldb);
+
+// Level-3 with reference semantics (quick returns, alpha scaling).
+template <typename T>
+void TrsmFull(bool left, bool lower, bool trans, bool unit, int m, int n,
+              T alpha, const T* a, int lda, T* b, int ldb);
+void SyrkFull(bool lower, bool trans, int n, int k, double alpha,
+              const double* a, int lda, double beta, double* c, int ldc);
+template <typename T>
+void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
+              int lda, const T* b, int ldb, T beta, T* c, int ldc);
+
+// Host-side wait-timeout check: returns true (and reports) if any kernel on
+// the context set the timeout flag since the last check. Synchronises.
+bool CheckDeviceStatus(const char* what);
+
+}  // namespace hb

@@ -1,0 +1,305 @@
+// Level-3 routines around the GEMM kernels: the FP32 GEMM (FFMA on the CUDA
+// cores, the reference's FP32 order with KC = 384), the recursive TRSM with
+// its base substitution kernel, SYRK, and the reference-semantics wrappers
+// (argument-independent quick returns and alpha scaling).
+#include <algorithm>
+#include <cstdio>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace hb {
+namespace {
+
+// ---------------------------------------------------------------------------
+// FP32 GEMM: 64 x 64 tile per 256-thread CTA, 4 x 4 outputs per thread, each
+// a sequential FFMA chain over k restarted every 384 (src/gemm_kernel-inl.h:72).
+constexpr int kSB = 64, kSK = 16;
+
+__global__ void __launch_bounds__(256)
+    SgemmKernel(int m, int n, int k, float alpha, View<float> a, View<float> b,
+                float beta, float* c, long long ldc, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ float sa[kSK][kSB + 4];
+  __shared__ float sb[kSK][kSB + 4];
+  const int m0 = blockIdx.x * kSB, n0 = blockIdx.y * kSB;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  float acc[4][4] = {}, cacc[4][4] = {};
+  const int kchunk = 384;
+  for (int k0 = 0; k0 < k; k0 += kSK) {
+    for (int idx = threadIdx.x; idx < kSK * kSB; idx += 256) {
+      const int kk = idx / kSB, mm = idx % kSB;
+      const int gi = m0 + mm, gk = k0 + kk;
+      sa[kk][mm] = (gi < m && gk < k) ? a.data[gi * a.rs + gk * a.cs] : 0.f;
+      const int gj = n0 + mm;
+      sb[kk][mm] = (gj < n && gk < k) ? b.data[gk * b.rs + gj * b.cs] : 0.f;
+    }
+    __syncthreads();
+    const int kend = min(kSK, k - k0);
+    for (int kk = 0; kk < kend; ++kk) {
+      float av[4], bv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) av[r] = sa[kk][tx + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bv[q] = sb[kk][ty + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[r][q] = fmaf(av[r], bv[q], acc[r][q]);
+      const int kg = k0 + kk;
+      if ((kg + 1) % kchunk == 0 || kg + 1 == k) {
+        const bool first = kg < kchunk;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
+            const float rr = alpha * acc[r][q];
+            if (first) {
+              if (i < m && j < n) {
+                if (beta == 0.f) {
+                  cacc[r][q] = rr;
+                } else {
+                  const float cin = c[i + j * ldc];
+                  cacc[r][q] = (beta == 1.f) ? rr + cin : fmaf(cin, beta, rr);
+                }
+              }
+            } else {
+              cacc[r][q] = rr + cacc[r][q];
+            }
+            acc[r][q] = 0.f;
+          }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
+      if (i < m && j < n) c[i + j * ldc] = cacc[r][q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// TRSM base: solves X*T = B for independent rows of X (src/trsm-inl.h:107-174)
+// with T (r x r, r <= 32) read from a strided view. Columns are solved in
+// "solve order" s = 0..r-1 (column r-1-s for lower, s for upper), two per
+// pass: b_j0 -= x_q t(q, j0) and b_j1 -= x_q t(q, j1) as fma(-x_q, t, b) for
+// every solved q; x_j0 = b_j0 * (1/t(j0, j0)); b_j1 = fma(-x_j0, t(j0, j1), b_j1);
+// x_j1 = b_j1 * (1/t(j1, j1)). One thread owns one row of X; the row is kept
+// in registers indexed in solve order so all register indices are static.
+// Element (row, col q) of X is x[row * xs_row + q * xs_col].
+template <typename T>
+__global__ void __launch_bounds__(128)
+    TrsmBaseKernel(View<T> tri, int lower, int unit, int r, int rows, T* x,
+                   long long xs_row, long long xs_col, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ T st[32][33];  // st[s][u] = T(col(s), col(u)) in solve order
+  __shared__ T sinv[32];
+  for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+    const int s = idx / 32, u = idx % 32;
+    T v = T(0);
+    if (s < r && u < r) {
+      const int q = lower ? r - 1 - s : s, j = lower ? r - 1 - u : u;
+      // Only the triangle's solved-before part (s < u) and the diagonal are
+      // referenced.
+      if (s < u || (s == u && !unit)) v = tri.data[q * tri.rs + j * tri.cs];
+    }
+    st[s][u] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int s = threadIdx.x;
+    sinv[s] = (s < r && !unit) ? T(1) / st[s][s] : T(1);
+  }
+  __syncthreads();
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  T* xr = x + row * xs_row;
+  T y[32];
+#pragma unroll
+  for (int s = 0; s < 32; ++s) {
+    if (s < r) y[s] = xr[(lower ? r - 1 - s : s) * xs_col];
+  }
+#pragma unroll
+  for (int step = 0; step + 1 < 32; step += 2) {
+    if (step + 2 <= r) {
+      T acc0 = y[step], acc1 = y[step + 1];
+#pragma unroll
+      for (int s = 0; s < step; ++s) {
+        acc0 = fma(-y[s], st[s][step], acc0);
+        acc1 = fma(-y[s], st[s][step + 1], acc1);
+      }
+      if (!unit) acc0 = acc0 * sinv[step];
+      y[step] = acc0;
+      acc1 = fma(-acc0, st[step][step + 1], acc1);
+      if (!unit) acc1 = acc1 * sinv[step + 1];
+      y[step + 1] = acc1;
+    } else if (step < r) {  // odd r: the last column alone
+      T acc = y[step];
+#pragma unroll
+      for (int s = 0; s < step; ++s) acc = fma(-y[s], st[s][step], acc);
+      if (!unit) acc = acc * sinv[step];
+      y[step] = acc;
+    }
+  }
+  if (r == 32) {
+    // step 30/31 handled above; nothing left.
+  }
+#pragma unroll
+  for (int s = 0; s < 32; ++s) {
+    if (s < r) xr[(lower ? r - 1 - s : s) * xs_col] = y[s];
+  }
+}
+
+template <typename T>
+void LaunchGemm(int m, int n, int k, T alpha, View<T> a, View<T> b, T beta,
+                T* c, int ldc);
+template <>
+void LaunchGemm<double>(int m, int n, int k, double alpha, View<double> a,
+                        View<double> b, double beta, double* c, int ldc) {
+  Dgemm(m, n, k, alpha, a, b, beta, c, ldc, kAll);
+}
+template <>
+void LaunchGemm<float>(int m, int n, int k, float alpha, View<float> a,
+                       View<float> b, float beta, float* c, int ldc) {
+  Sgemm(m, n, k, alpha, a, b, beta, c, ldc);
+}
+
+// TrsmRecursive (src/trsm.cc:87-135): split at max(32, (r/2)/32*32).
+template <typename T>
+void TrsmRec(bool left, View<T> tri, bool lower, bool unit, int r, int other,
+             T* b, int ldb) {
+  if (r <= 32) {
+    TrsmSolve<T>(left, tri, lower, unit, r, other, b, ldb);
+    return;
+  }
+  const int r1 = std::max(32, (r / 2) / 32 * 32);
+  const int r2 = r - r1;
+  const View<T> t11 = tri;
+  const View<T> t22 = tri.sub(r1, r1);
+  const View<T> toff = lower ? tri.sub(r1, 0) : tri.sub(0, r1);
+  const auto cm = [&](T* p) { return ColMajor<T>(p, ldb); };
+  if (left) {
+    T* b1 = b;
+    T* b2 = b + r1;
+    if (lower) {
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+      LaunchGemm<T>(r2, other, r1, T(-1), toff, cm(b1), T(1), b2, ldb);
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+    } else {
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+      LaunchGemm<T>(r1, other, r2, T(-1), toff, cm(b2), T(1), b1, ldb);
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+    }
+  } else {
+    T* b1 = b;
+    T* b2 = b + static_cast<long long>(r1) * ldb;
+    if (lower) {
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+      LaunchGemm<T>(other, r1, r2, T(-1), cm(b2), toff, T(1), b1, ldb);
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+    } else {
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+      LaunchGemm<T>(other, r2, r1, T(-1), cm(b1), toff, T(1), b2, ldb);
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+    }
+  }
+}
+
+}  // namespace
+
+void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
+           float beta, float* c, int ldc) {
+  const dim3 grid((m + kSB - 1) / kSB, (n + kSB - 1) / kSB);
+  SgemmKernel<<<grid, 256, 0, Ctx().stream>>>(m, n, k, alpha, a, b, beta, c,
+                                              ldc, Ctx().guard);
+  CountLaunch();
+  LaunchFailed("sgemm");
+}
+
+template <typename T>
+void TrsmSolve(bool left, View<T> tri, bool lower, bool unit, int r, int other,
+               T* b, int ldb) {
+  if (r <= 0 || other <= 0) return;
+  View<T> t = tri;
+  bool lo = lower;
+  long long xs_row, xs_col;
+  if (left) {
+    // T X = B  <=>  X^T T^T = B^T (src/trsm-inl.h:306-324): rows of X^T are
+    // the columns of B.
+    t.rs = tri.cs;
+    t.cs = tri.rs;
+    lo = !lower;
+    xs_row = ldb;
+    xs_col = 1;
+  } else {
+    xs_row = 1;
+    xs_col = ldb;
+  }
+  const int threads = 128;
+  TrsmBaseKernel<T><<<(other + threads - 1) / threads, threads, 0,
+                      Ctx().stream>>>(t, lo ? 1 : 0, unit ? 1 : 0, r, other, b,
+                                      xs_row, xs_col, Ctx().guard);
+  CountLaunch();
+  LaunchFailed("trsm base");
+}
+template void TrsmSolve<double>(bool, View<double>, bool, bool, int, int,
+                                double*, int);
+template void TrsmSolve<float>(bool, View<float>, bool, bool, int, int, float*,
+                               int);
+
+// Trsm (src/trsm.cc:137-180) after argument checks: B := alpha*B first
+// (alpha != 1), zero B and return for alpha == 0, then the recursion on
+// op(A) (strides swapped and triangle flipped when transposed).
+template <typename T>
+void TrsmFull(bool left, bool lower, bool trans, bool unit, int m, int n,
+              T alpha, const T* a, int lda, T* b, int ldb) {
+  if (m == 0 || n == 0) return;
+  if (alpha != T(1)) ScaleMatrix<T>(m, n, alpha, b, ldb, kAll);
+  if (alpha == T(0)) return;
+  const View<T> tri = ColMajor<T>(a, lda, trans);
+  const bool op_lower = trans ? !lower : lower;
+  TrsmRec<T>(left, tri, op_lower, unit, left ? m : n, left ? n : m, b, ldb);
+}
+template void TrsmFull<double>(bool, bool, bool, bool, int, int, double,
+                               const double*, int, double*, int);
+template void TrsmFull<float>(bool, bool, bool, bool, int, int, float,
+                              const float*, int, float*, int);
+
+// Syrk (src/level3.cc:84-139), real: C := alpha*op(A)*op(A)^T + beta*C on one
+// triangle, as a GEMM with a triangular C part.
+void SyrkFull(bool lower, bool trans, int n, int k, double alpha,
+              const double* a, int lda, double beta, double* c, int ldc) {
+  const Part part = lower ? kLower : kUpper;
+  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return;
+  if (alpha == 0.0 || k == 0) {
+    ScaleMatrix<double>(n, n, beta, c, ldc, part);
+    return;
+  }
+  Dgemm(n, n, k, alpha, ColMajor<double>(a, lda, trans),
+        ColMajor<double>(a, lda, !trans), beta, c, ldc, part);
+}
+
+// Gemm (src/gemm.cc:114-131) after argument checks.
+template <typename T>
+void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
+              int lda, const T* b, int ldb, T beta, T* c, int ldc) {
+  if (m == 0 || n == 0) return;
+  if ((k == 0 || alpha == T(0)) && beta == T(1)) return;
+  if (k == 0 || alpha == T(0)) {
+    ScaleMatrix<T>(m, n, beta, c, ldc, kAll);
+    return;
+  }
+  LaunchGemm<T>(m, n, k, alpha, ColMajor<T>(a, lda, ta), ColMajor<T>(b, ldb, tb),
+                beta, c, ldc);
+}
+template void GemmFull<double>(bool, bool, int, int, int, double,
+                               const double*, int, const double*, int, double,
+                               double*, int);
+template void GemmFull<float>(bool, bool, int, int, int, float, const float*,
+                              int, const float*, int, float, float*, int);
+
+}  // namespace hb

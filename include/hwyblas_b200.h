@@ -1,0 +1,207 @@
+/*
+ * hwyBLAS-B200: the level-3 hot path of hwyBLAS (GEMM, TRSM, SYRK, I?AMAX and
+ * the LU / Cholesky drivers built on them) as hand-written CUDA kernels for
+ * NVIDIA B200 (sm_100a), behind the reference's own C ABI.
+ *
+ * Calling convention (as the reference, include/hwyblas/hwyblas.h:1-16):
+ * Fortran-77 style, every argument by pointer, column-major, 32-bit integers,
+ * only the first character of CHARACTER arguments is read (case-insensitive)
+ * and the hidden length arguments are neither declared nor read.
+ *
+ * Memory: every matrix or vector pointer may be host memory (pageable or
+ * pinned; the library copies it to the GPU and back) or device / managed
+ * memory of the current CUDA device (used in place). All calls are
+ * synchronous on return, as BLAS requires. Work is issued on the library's
+ * per-thread stream, or on the stream set with hwyblas_set_stream.
+ *
+ * Errors: an invalid argument calls xerbla_ (or the handler installed with
+ * hwyblas_set_error_handler) with the reference's Fortran argument position
+ * and returns without side effects; LAPACK routines return INFO < 0 / > 0 as
+ * the reference does. A CUDA failure is reported through
+ * hwyblas_last_cuda_error() and a message on stderr; there is no CPU fallback.
+ */
+#ifndef HWYBLAS_B200_H_
+#define HWYBLAS_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#define HWYBLAS_API __attribute__((visibility("default")))
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int hwyblas_int;
+
+/* ------------------------------------------------------------------------ */
+/* Fortran BLAS                                                             */
+
+/* C := alpha*op(A)*op(B) + beta*C. Replaces dgemm_
+ * (include/hwyblas/hwyblas.h:570, src/gemm.cc:151-158). Per element the
+ * result is bit-identical to the reference: sequential FMA over k in chunks
+ * of 256, merged as alpha*acc (+ C, or fma(C, beta, .)). */
+HWYBLAS_API void dgemm_(const char* transa, const char* transb,
+                        const hwyblas_int* m, const hwyblas_int* n,
+                        const hwyblas_int* k, const double* alpha,
+                        const double* a, const hwyblas_int* lda,
+                        const double* b, const hwyblas_int* ldb,
+                        const double* beta, double* c, const hwyblas_int* ldc);
+/* Replaces sgemm_ (include/hwyblas/hwyblas.h:564, src/gemm.cc:142-149);
+ * chunks of 384. */
+HWYBLAS_API void sgemm_(const char* transa, const char* transb,
+                        const hwyblas_int* m, const hwyblas_int* n,
+                        const hwyblas_int* k, const float* alpha,
+                        const float* a, const hwyblas_int* lda, const float* b,
+                        const hwyblas_int* ldb, const float* beta, float* c,
+                        const hwyblas_int* ldc);
+/* Solves op(A)*X = alpha*B or X*op(A) = alpha*B in place. Replaces dtrsm_
+ * (include/hwyblas/hwyblas.h:792, src/trsm.cc:196-201). */
+HWYBLAS_API void dtrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m,
+                        const hwyblas_int* n, const double* alpha,
+                        const double* a, const hwyblas_int* lda, double* b,
+                        const hwyblas_int* ldb);
+/* C := alpha*A*A**T + beta*C (trans N) or alpha*A**T*A + beta*C on one
+ * triangle. Replaces dsyrk_ (include/hwyblas/hwyblas.h:637,
+ * src/level3.cc:416-421). */
+HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
+                        const hwyblas_int* n, const hwyblas_int* k,
+                        const double* alpha, const double* a,
+                        const hwyblas_int* lda, const double* beta, double* c,
+                        const hwyblas_int* ldc);
+/* 1-based index of the first element of largest |x| (0 if n < 1 or
+ * incx <= 0). Replaces idamax_ (include/hwyblas/hwyblas.h:169,
+ * src/level1.cc:895-897). */
+HWYBLAS_API hwyblas_int idamax_(const hwyblas_int* n, const double* x,
+                                const hwyblas_int* incx);
+
+/* Prints " ** On entry to NAME parameter number I had an illegal value" and
+ * returns (does not stop the program). Replaces xerbla_
+ * (include/hwyblas/hwyblas.h:888, src/common.cc:68-79). */
+HWYBLAS_API void xerbla_(const char* srname, const hwyblas_int* info,
+                         size_t srname_len);
+
+/* Error handler called instead of xerbla_/cblas_xerbla; returns the previous
+ * one, NULL restores the default. Replaces hwyblas_set_error_handler
+ * (include/hwyblas/hwyblas.h:895-903, src/common.cc:81-84). */
+typedef void (*hwyblas_error_handler)(const char* name, hwyblas_int position);
+HWYBLAS_API hwyblas_error_handler
+hwyblas_set_error_handler(hwyblas_error_handler handler);
+
+/* ------------------------------------------------------------------------ */
+/* LAPACK                                                                   */
+
+/* A = P*L*U, blocked right-looking with nb = 64 (include/hwyblas/lapack.h:93,
+ * src/lapack/getrf.cc:216-280, 508-512). ipiv is 1-based and global; INFO is
+ * the first exactly-zero pivot. Same pivots as the reference. */
+HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv,
+                         hwyblas_int* info);
+/* Recursive LU (include/hwyblas/lapack.h:105, src/lapack/getrf.cc:112-207). */
+HWYBLAS_API void dgetrf2_(const hwyblas_int* m, const hwyblas_int* n,
+                          double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
+                          hwyblas_int* info);
+/* Row interchanges (include/hwyblas/lapack.h:120, src/lapack/getrf.cc:28-81). */
+HWYBLAS_API void dlaswp_(const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, const hwyblas_int* k1,
+                         const hwyblas_int* k2, const hwyblas_int* ipiv,
+                         const hwyblas_int* incx);
+/* Solve with the LU factors (include/hwyblas/lapack.h:139,
+ * src/lapack/getrf.cc:287-339). */
+HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const double* a,
+                         const hwyblas_int* lda, const hwyblas_int* ipiv,
+                         double* b, const hwyblas_int* ldb, hwyblas_int* info);
+/* LU and solve (include/hwyblas/lapack.h:158, src/lapack/getrf.cc:348-374). */
+HWYBLAS_API void dgesv_(const hwyblas_int* n, const hwyblas_int* nrhs,
+                        double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
+                        double* b, const hwyblas_int* ldb, hwyblas_int* info);
+/* Cholesky, blocked with nb = 64 (include/hwyblas/lapack.h:663,
+ * src/lapack/potrf.cc:128-199, 747-751). */
+HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+/* Recursive Cholesky (include/hwyblas/lapack.h:671,
+ * src/lapack/potrf.cc:48-119). */
+HWYBLAS_API void dpotrf2_(const char* uplo, const hwyblas_int* n, double* a,
+                          const hwyblas_int* lda, hwyblas_int* info);
+/* Solve with the Cholesky factor (include/hwyblas/lapack.h:726,
+ * src/lapack/posv.cc:31-76). */
+HWYBLAS_API void dpotrs_(const char* uplo, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const double* a,
+                         const hwyblas_int* lda, double* b,
+                         const hwyblas_int* ldb, hwyblas_int* info);
+/* Cholesky and solve (include/hwyblas/lapack.h:746, src/lapack/posv.cc:78-114). */
+HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n,
+                        const hwyblas_int* nrhs, double* a,
+                        const hwyblas_int* lda, double* b,
+                        const hwyblas_int* ldb, hwyblas_int* info);
+
+/* ------------------------------------------------------------------------ */
+/* CBLAS (include/hwyblas/cblas.h:20-45)                                    */
+
+#define CBLAS_INDEX size_t
+typedef enum CBLAS_LAYOUT { CblasRowMajor = 101, CblasColMajor = 102 } CBLAS_LAYOUT;
+typedef enum CBLAS_TRANSPOSE {
+  CblasNoTrans = 111,
+  CblasTrans = 112,
+  CblasConjTrans = 113,
+  CblasConjNoTrans = 114
+} CBLAS_TRANSPOSE;
+typedef enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 } CBLAS_UPLO;
+typedef enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 } CBLAS_DIAG;
+typedef enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 } CBLAS_SIDE;
+
+/* Replaces cblas_xerbla (include/hwyblas/cblas.h:45). */
+HWYBLAS_API void cblas_xerbla(hwyblas_int p, const char* rout, const char* form,
+                              ...);
+/* Row-major as the column-major product with A and B swapped
+ * (include/hwyblas/cblas.h:615, src/cblas.cc:517-537, 1596). */
+HWYBLAS_API void cblas_dgemm(const CBLAS_LAYOUT layout,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k,
+                             const double alpha, const double* a,
+                             const hwyblas_int lda, const double* b,
+                             const hwyblas_int ldb, const double beta,
+                             double* c, const hwyblas_int ldc);
+/* include/hwyblas/cblas.h:607, src/cblas.cc:1585. */
+HWYBLAS_API void cblas_sgemm(const CBLAS_LAYOUT layout,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k,
+                             const float alpha, const float* a,
+                             const hwyblas_int lda, const float* b,
+                             const hwyblas_int ldb, const float beta, float* c,
+                             const hwyblas_int ldc);
+/* Row-major: other side and triangle (include/hwyblas/cblas.h:865,
+ * src/cblas.cc:661-691, 1960). */
+HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m,
+                             const hwyblas_int n, const double alpha,
+                             const double* a, const hwyblas_int lda, double* b,
+                             const hwyblas_int ldb);
+/* 0-based (include/hwyblas/cblas.h:128, src/cblas.cc:845). */
+HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
+                                     const hwyblas_int incx);
+
+/* ------------------------------------------------------------------------ */
+/* Extensions (hwyblas_ prefix, as the reference's own additions)           */
+
+/* Stream for subsequent calls of the calling thread (a cudaStream_t; NULL
+ * restores the library's per-thread stream). No counterpart in the
+ * reference, which has no device. */
+HWYBLAS_API void hwyblas_set_stream(void* stream);
+/* Last CUDA error seen by the library on the calling thread (cudaError_t as
+ * int; 0 if none), cleared by the read. No counterpart in the reference. */
+HWYBLAS_API int hwyblas_last_cuda_error(void);
+/* Number of kernels the library has launched (all threads). No counterpart
+ * in the reference; used to count launches inside timed regions. */
+HWYBLAS_API uint64_t hwyblas_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HWYBLAS_B200_H_ */

@@ -1,0 +1,70 @@
+/* Oracle for the parity tests: a CPU restatement of hwyBLAS's level-3 hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker: tests/, the smoke
+ * check in __graft_entry__.py and the CPU-baseline legs of bench.py may load
+ * it; the product library (hwyblas_b200/) never links, loads or calls it.
+ *
+ * Every routine follows the reference's per-element operation order exactly
+ * (sequential FMA over k in chunks of KC, alpha/beta merge order, recursion
+ * split points, pivot choice), so results are bit-identical to the reference
+ * built for a target with `lanes` doubles per vector (8 = AVX-512, 4 = AVX2;
+ * the lane count only changes the rounding of short AXPY columns in the LU and
+ * Cholesky leaves and the micro-tile geometry of triangular-C SYRK).
+ *
+ * Argument errors are returned as the 1-based Fortran position (BLAS) or
+ * -position (LAPACK INFO), and nothing is printed.
+ */
+#ifndef HWYBLAS_ORACLE_H_
+#define HWYBLAS_ORACLE_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void orc_set_lanes(int lanes);
+int orc_get_lanes(void);
+void orc_set_threads(int threads);
+
+/* BLAS. Return 0 or the Fortran position of the first invalid argument. */
+int orc_dgemm(char transa, char transb, int m, int n, int k, double alpha,
+              const double* a, int lda, const double* b, int ldb, double beta,
+              double* c, int ldc);
+int orc_sgemm(char transa, char transb, int m, int n, int k, float alpha,
+              const float* a, int lda, const float* b, int ldb, float beta,
+              float* c, int ldc);
+int orc_dtrsm(char side, char uplo, char transa, char diag, int m, int n,
+              double alpha, const double* a, int lda, double* b, int ldb);
+int orc_strsm(char side, char uplo, char transa, char diag, int m, int n,
+              float alpha, const float* a, int lda, float* b, int ldb);
+int orc_dsyrk(char uplo, char trans, int n, int k, double alpha,
+              const double* a, int lda, double beta, double* c, int ldc);
+int orc_idamax(int n, const double* x, int incx);
+int orc_isamax(int n, const float* x, int incx);
+
+/* LAPACK. Return INFO as the reference does. */
+void orc_dlaswp(int n, double* a, int lda, int k1, int k2, const int* ipiv,
+                int incx);
+int orc_dgetrf(int m, int n, double* a, int lda, int* ipiv);
+int orc_dgetrf2(int m, int n, double* a, int lda, int* ipiv);
+int orc_sgetrf(int m, int n, float* a, int lda, int* ipiv);
+int orc_dgetrs(char trans, int n, int nrhs, const double* a, int lda,
+               const int* ipiv, double* b, int ldb);
+int orc_sgetrs(char trans, int n, int nrhs, const float* a, int lda,
+               const int* ipiv, float* b, int ldb);
+int orc_dgesv(int n, int nrhs, double* a, int lda, int* ipiv, double* b,
+              int ldb);
+int orc_dpotrf(char uplo, int n, double* a, int lda);
+int orc_dpotrf2(char uplo, int n, double* a, int lda);
+int orc_dpotrs(char uplo, int n, int nrhs, const double* a, int lda, double* b,
+               int ldb);
+int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
+              int ldb);
+
+/* Leaves, exposed for the known-answer tests. */
+int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv);
+int orc_dpotrf_leaf(int upper, int n, double* a, int lda);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HWYBLAS_ORACLE_H_ */

@@ -1,0 +1,503 @@
+// Oracle BLAS (TEST INFRASTRUCTURE ONLY; the product never loads this file's
+// library). CPU restatement of the reference's level-3 BLAS hot path with the
+// reference's exact per-element rounding:
+//
+//   GEMM   src/gemm-inl.h:153-232 (KC chunks, beta only on the first chunk),
+//          src/gemm_kernel-inl.h:161-176 (acc = fma(a, b, acc) over k),
+//          src/gemm_kernel-inl.h:182-224 (r = alpha*acc; r + C, or fma(C, beta, r))
+//          src/gemm-inl.h:91-130 (triangular C: tiles crossing the diagonal
+//          are merged element-wise as v + beta*C, two roundings)
+//          src/gemm.cc:73-132 (argument checks and quick returns)
+//   TRSM   src/trsm.cc:87-180 (recursive split at max(32, (r/2)/32*32))
+//          src/trsm-inl.h:43-71, 107-174, 277-325 (base solve, dot form,
+//          two columns per pass, reciprocal diagonal)
+//   SYRK   src/level3.cc:84-139
+//   IAMAX  src/level1.cc:383-402, src/level1-inl.h:343-423
+//
+// The restatement is vectorised with AVX2 along M only (each lane owns one C
+// element, so the per-element order is the reference's) and threaded over
+// column blocks of C (std::thread), which also leaves every element's order unchanged.
+#include <immintrin.h>
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+
+#include "oracle.h"
+#include "oracle_internal.h"
+
+namespace orc {
+
+int g_lanes = 8;
+int g_threads = 1;
+
+// ---------------------------------------------------------------------------
+// Vector helpers (AVX2 + FMA): one register of T.
+template <typename T>
+struct Vec;
+template <>
+struct Vec<double> {
+  using V = __m256d;
+  static constexpr int kL = 4;
+  static V zero() { return _mm256_setzero_pd(); }
+  static V load(const double* p) { return _mm256_loadu_pd(p); }
+  static V set(double x) { return _mm256_set1_pd(x); }
+  static V fma(V a, V b, V c) { return _mm256_fmadd_pd(a, b, c); }
+  static void store(double* p, V v) { _mm256_storeu_pd(p, v); }
+};
+template <>
+struct Vec<float> {
+  using V = __m256;
+  static constexpr int kL = 8;
+  static V zero() { return _mm256_setzero_ps(); }
+  static V load(const float* p) { return _mm256_loadu_ps(p); }
+  static V set(float x) { return _mm256_set1_ps(x); }
+  static V fma(V a, V b, V c) { return _mm256_fmadd_ps(a, b, c); }
+  static void store(float* p, V v) { _mm256_storeu_ps(p, v); }
+};
+
+// ---------------------------------------------------------------------------
+// Reference micro-tile geometry for triangular C (SYRK): MR = 2 * lanes rows,
+// NR = 12 columns with 32 vector registers (AVX-512) or 6 with 16 (AVX2);
+// MC = 96 (double) / 144 (float) rounded to MR, NC = 4080 rounded to NR
+// (src/gemm_kernel-inl.h:64-74).
+template <typename T>
+struct RefTiles {
+  size_t mr, nr, mc, nc;
+  RefTiles() {
+    const size_t lanes = sizeof(T) == 8 ? g_lanes : 2 * g_lanes;
+    mr = 2 * lanes;
+    nr = g_lanes >= 8 ? 12 : 6;
+    mc = (sizeof(T) == 4 ? 144 : 96) / mr * mr;
+    nc = 4080 / nr * nr;
+  }
+};
+
+// Whether element (i, j) of an m x n triangular C lies in a reference
+// micro-tile that crosses the diagonal (src/gemm-inl.h:93-106, 195-199).
+template <typename T>
+static bool InCrossingTile(const RefTiles<T>& t, Part part, size_t m, size_t n,
+                           size_t i, size_t j) {
+  const size_t ic = i / t.mc * t.mc, mcb = std::min(t.mc, m - ic);
+  const size_t ir = (i - ic) / t.mr * t.mr, mr = std::min(t.mr, mcb - ir);
+  const size_t jc = j / t.nc * t.nc, ncb = std::min(t.nc, n - jc);
+  const size_t jr = (j - jc) / t.nr * t.nr, nr = std::min(t.nr, ncb - jr);
+  const size_t i0 = ic + ir, j0 = jc + jr;
+  const size_t i_last = i0 + mr - 1, j_last = j0 + nr - 1;
+  if (part == kLower) return !(i0 > j_last);
+  return !(i_last < j0);
+}
+
+// One KC chunk's contribution merged into C(i, j): `first` selects beta.
+// Inside tiles: r = alpha*acc, then C = r (beta 0), r + C (beta 1) or
+// fma(C, beta, r). Crossing tiles: v = alpha*acc, then v + beta*C.
+template <typename T>
+static inline T Merge(T acc, T alpha, T beta, T c, bool crossing) {
+  const T r = alpha * acc;
+  if (beta == T(0)) return r;
+  if (crossing) {
+    const T bc = beta * c;
+    return r + bc;
+  }
+  if (beta == T(1)) return r + c;
+  return std::fma(c, beta, r);
+}
+
+template <typename T>
+constexpr size_t KcOf() {
+  return sizeof(T) == 4 ? 384 : 256;
+}
+
+// C := alpha * op(A) * op(B) + beta * C (or one triangle of it). Requires
+// m, n, k > 0 (callers handle trivial cases, as RunGemm's callers do).
+template <typename T>
+void Gemm(size_t m, size_t n, size_t k, T alpha, Opnd<T> a, Opnd<T> b, T beta,
+          T* c, size_t ldc, Part part) {
+  using VT = Vec<T>;
+  using V = typename VT::V;
+  constexpr size_t L = VT::kL;
+  constexpr size_t MR = 2 * L, NR = 6;
+  constexpr size_t KC = KcOf<T>();
+  constexpr size_t MC = 96 / MR * MR * (sizeof(T) == 4 ? 2 : 1);
+  constexpr size_t NCB = 96;  // columns per parallel block
+  const RefTiles<T> tiles;
+  const size_t nblocks = (n + NCB - 1) / NCB;
+
+  const auto run_block = [&](size_t blk) {
+    const size_t jc = blk * NCB, nc = std::min(NCB, n - jc);
+    std::vector<T> pa(MC * KC + MR), pb(((nc + NR - 1) / NR) * NR * KC + NR);
+    T tmp[MR * NR];
+    for (size_t pc = 0; pc < k; pc += KC) {
+      const size_t kc = std::min(KC, k - pc);
+      const bool first = (pc == 0);
+      // Pack op(B)[pc:pc+kc, jc:jc+nc] into NR-column panels (k-major).
+      for (size_t c0 = 0; c0 < nc; c0 += NR) {
+        T* dst = pb.data() + c0 * kc;
+        for (size_t p = 0; p < kc; ++p)
+          for (size_t cc = 0; cc < NR; ++cc)
+            dst[p * NR + cc] =
+                (c0 + cc < nc) ? b.at(pc + p, jc + c0 + cc) : T(0);
+      }
+      for (size_t ic = 0; ic < m; ic += MC) {
+        const size_t mc = std::min(MC, m - ic);
+        // Skip row blocks entirely outside the triangle.
+        if (part == kLower && ic + mc - 1 < jc) continue;
+        if (part == kUpper && ic > jc + nc - 1) continue;
+        for (size_t r0 = 0; r0 < mc; r0 += MR) {
+          T* dst = pa.data() + r0 * kc;
+          for (size_t p = 0; p < kc; ++p)
+            for (size_t rr = 0; rr < MR; ++rr)
+              dst[p * MR + rr] =
+                  (r0 + rr < mc) ? a.at(ic + r0 + rr, pc + p) : T(0);
+        }
+        for (size_t c0 = 0; c0 < nc; c0 += NR) {
+          const size_t ncols = std::min(NR, nc - c0);
+          for (size_t r0 = 0; r0 < mc; r0 += MR) {
+            const size_t nrows = std::min(MR, mc - r0);
+            const size_t gi0 = ic + r0, gj0 = jc + c0;
+            if (part == kLower && gi0 + nrows - 1 < gj0) continue;
+            if (part == kUpper && gi0 > gj0 + ncols - 1) continue;
+            const T* ap = pa.data() + r0 * kc;
+            const T* bp = pb.data() + c0 * kc;
+            V acc[NR][2];
+            for (size_t cc = 0; cc < NR; ++cc) acc[cc][0] = acc[cc][1] = VT::zero();
+            for (size_t p = 0; p < kc; ++p) {
+              const V a0 = VT::load(ap + p * MR), a1 = VT::load(ap + p * MR + L);
+              for (size_t cc = 0; cc < NR; ++cc) {
+                const V bv = VT::set(bp[p * NR + cc]);
+                acc[cc][0] = VT::fma(a0, bv, acc[cc][0]);
+                acc[cc][1] = VT::fma(a1, bv, acc[cc][1]);
+              }
+            }
+            for (size_t cc = 0; cc < NR; ++cc) {
+              VT::store(tmp + cc * MR, acc[cc][0]);
+              VT::store(tmp + cc * MR + L, acc[cc][1]);
+            }
+            const T beta_eff = first ? beta : T(1);
+            for (size_t cc = 0; cc < ncols; ++cc) {
+              const size_t gj = gj0 + cc;
+              T* cj = c + gj * ldc;
+              for (size_t rr = 0; rr < nrows; ++rr) {
+                const size_t gi = gi0 + rr;
+                bool crossing = false;
+                if (part != kAll) {
+                  if (part == kLower ? (gi < gj) : (gi > gj)) continue;
+                  crossing = InCrossingTile(tiles, part, m, n, gi, gj);
+                }
+                cj[gi] = Merge(tmp[cc * MR + rr], alpha, beta_eff,
+                               beta_eff == T(0) ? T(0) : cj[gi], crossing);
+              }
+            }
+          }
+        }
+      }
+    }
+  };
+  // Column blocks of C are independent; threads take them in turn.
+  const size_t nthreads = std::min<size_t>(g_threads, nblocks);
+  if (nthreads <= 1 || m * n * k < (size_t(1) << 21)) {
+    for (size_t blk = 0; blk < nblocks; ++blk) run_block(blk);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> pool;
+  for (size_t t = 0; t < nthreads; ++t) {
+    pool.emplace_back([&] {
+      for (size_t blk; (blk = next.fetch_add(1)) < nblocks;) run_block(blk);
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
+template <typename T>
+void ScaleMatrix(size_t m, size_t n, T beta, T* c, size_t ldc, Part part) {
+  for (size_t j = 0; j < n; ++j) {
+    T* cj = c + j * ldc;
+    const size_t begin = (part == kLower) ? std::min(j, m) : 0;
+    const size_t end = (part == kUpper) ? std::min(j + 1, m) : m;
+    if (beta == T(0)) {
+      for (size_t i = begin; i < end; ++i) cj[i] = T(0);
+    } else {
+      for (size_t i = begin; i < end; ++i) cj[i] *= beta;
+    }
+  }
+}
+
+static char Up(char ch) { return (ch >= 'a' && ch <= 'z') ? ch - 32 : ch; }
+bool DecodeOp(char ch, bool* trans) {
+  ch = Up(ch);
+  *trans = (ch == 'T' || ch == 'C');
+  return ch == 'N' || ch == 'T' || ch == 'C';
+}
+
+template <typename T>
+Opnd<T> General(bool trans, const T* x, int ld) {
+  Opnd<T> o;
+  o.data = x;
+  o.rs = trans ? ld : 1;
+  o.cs = trans ? 1 : ld;
+  return o;
+}
+
+template <typename T>
+int GemmF(char transa, char transb, int m, int n, int k, T alpha, const T* a,
+          int lda, const T* b, int ldb, T beta, T* c, int ldc) {
+  bool ta, tb;
+  const bool va = DecodeOp(transa, &ta), vb = DecodeOp(transb, &tb);
+  const int rows_a = ta ? k : m, rows_b = tb ? n : k;
+  int info = 0;
+  if (!va) info = 1;
+  else if (!vb) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, m)) info = 13;
+  if (info) return info;
+  if (m == 0 || n == 0) return 0;
+  if ((k == 0 || alpha == T(0)) && beta == T(1)) return 0;
+  if (k == 0 || alpha == T(0)) {
+    ScaleMatrix<T>(m, n, beta, c, ldc, kAll);
+    return 0;
+  }
+  Gemm<T>(m, n, k, alpha, General(ta, a, lda), General(tb, b, ldb), beta, c,
+          ldc, kAll);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// TRSM (src/trsm.cc, src/trsm-inl.h).
+
+// Solves X T = B for `rows` independent rows. Element (row i, column q) of B
+// is at b[i * xs_row + q * xs_col]; T(q, j) is tri.at(q, j).
+template <typename T>
+static void SolveBase(const Opnd<T>& tri, bool lower, bool unit, size_t r,
+                      size_t rows, T* b, ptrdiff_t xs_row, ptrdiff_t xs_col) {
+  T inv[32];
+  for (size_t j = 0; j < r; ++j) inv[j] = unit ? T(1) : T(1) / tri.at(j, j);
+  const auto col = [&](size_t s) { return lower ? r - 1 - s : s; };
+  for (size_t i = 0; i < rows; ++i) {
+    T* bi = b + static_cast<ptrdiff_t>(i) * xs_row;
+    const auto X = [&](size_t q) -> T& {
+      return bi[static_cast<ptrdiff_t>(q) * xs_col];
+    };
+    size_t step = 0;
+    for (; step + 2 <= r; step += 2) {
+      const size_t j0 = col(step), j1 = col(step + 1);
+      T acc0 = X(j0), acc1 = X(j1);
+      for (size_t s = 0; s < step; ++s) {
+        const size_t q = col(s);
+        const T x = X(q);
+        acc0 = std::fma(-x, tri.at(q, j0), acc0);
+        acc1 = std::fma(-x, tri.at(q, j1), acc1);
+      }
+      if (!unit) acc0 = acc0 * inv[j0];
+      X(j0) = acc0;
+      acc1 = std::fma(-acc0, tri.at(j0, j1), acc1);
+      if (!unit) acc1 = acc1 * inv[j1];
+      X(j1) = acc1;
+    }
+    if (step < r) {
+      const size_t j = col(step);
+      T acc = X(j);
+      for (size_t s = 0; s < step; ++s) {
+        const size_t q = col(s);
+        acc = std::fma(-X(q), tri.at(q, j), acc);
+      }
+      if (!unit) acc = acc * inv[j];
+      X(j) = acc;
+    }
+  }
+}
+
+template <typename T>
+static void TrsmRec(bool left, const Opnd<T>& tri, bool lower, bool unit,
+                    size_t r, size_t other, T* b, size_t ldb) {
+  if (r <= 32) {
+    if (!left) {
+      SolveBase(tri, lower, unit, r, other, b, 1, static_cast<ptrdiff_t>(ldb));
+    } else {
+      // T X = B  <=>  X^T T^T = B^T (src/trsm-inl.h:306-324).
+      Opnd<T> tt = tri;
+      tt.rs = tri.cs;
+      tt.cs = tri.rs;
+      SolveBase(tt, !lower, unit, r, other, b, static_cast<ptrdiff_t>(ldb), 1);
+    }
+    return;
+  }
+  const size_t r1 = std::max<size_t>(32, (r / 2) / 32 * 32);
+  const size_t r2 = r - r1;
+  const Opnd<T> t11 = tri;
+  const Opnd<T> t22 = tri.sub(r1, r1);
+  const Opnd<T> toff = lower ? tri.sub(r1, 0) : tri.sub(0, r1);
+  const auto colmajor = [&](T* blk) {
+    Opnd<T> o;
+    o.data = blk;
+    o.rs = 1;
+    o.cs = static_cast<ptrdiff_t>(ldb);
+    return o;
+  };
+  const T minus1 = T(-1), one = T(1);
+  if (left) {
+    T* b1 = b;
+    T* b2 = b + r1;
+    if (lower) {
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+      Gemm<T>(r2, other, r1, minus1, toff, colmajor(b1), one, b2, ldb, kAll);
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+    } else {
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+      Gemm<T>(r1, other, r2, minus1, toff, colmajor(b2), one, b1, ldb, kAll);
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+    }
+  } else {
+    T* b1 = b;
+    T* b2 = b + r1 * ldb;
+    if (lower) {
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+      Gemm<T>(other, r1, r2, minus1, colmajor(b2), toff, one, b1, ldb, kAll);
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+    } else {
+      TrsmRec(left, t11, lower, unit, r1, other, b1, ldb);
+      Gemm<T>(other, r2, r1, minus1, colmajor(b1), toff, one, b2, ldb, kAll);
+      TrsmRec(left, t22, lower, unit, r2, other, b2, ldb);
+    }
+  }
+}
+
+template <typename T>
+int TrsmF(char side, char uplo, char transa, char diag, int m, int n, T alpha,
+          const T* a, int lda, T* b, int ldb) {
+  const char s = Up(side), u = Up(uplo), d = Up(diag);
+  bool trans;
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const bool vt = DecodeOp(transa, &trans), vd = (d == 'U' || d == 'N');
+  const bool left = (s == 'L'), lower = (u == 'L'), unit = (d == 'U');
+  const int rows_a = left ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (!vt) info = 3;
+  else if (!vd) info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, rows_a)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info) return info;
+  if (m == 0 || n == 0) return 0;
+  if (alpha != T(1)) ScaleMatrix<T>(m, n, alpha, b, ldb, kAll);
+  if (alpha == T(0)) return 0;
+  const Opnd<T> tri = General(trans, a, lda);
+  const bool op_lower = trans ? !lower : lower;
+  TrsmRec<T>(left, tri, op_lower, unit, left ? m : n, left ? n : m, b, ldb);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// SYRK (src/level3.cc:84-139), real only.
+int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a,
+          int lda, double beta, double* c, int ldc) {
+  const char u = Up(uplo);
+  bool t;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool vt = DecodeOp(trans, &t);
+  const int rows_a = t ? k : n;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!vt) info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, rows_a)) info = 7;
+  else if (ldc < std::max(1, n)) info = 10;
+  if (info) return info;
+  const Part part = (u == 'L') ? kLower : kUpper;
+  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return 0;
+  if (alpha == 0.0 || k == 0) {
+    ScaleMatrix<double>(n, n, beta, c, ldc, part);
+    return 0;
+  }
+  Gemm<double>(n, n, k, alpha, General(t, a, lda), General(!t, a, lda), beta,
+               c, ldc, part);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// IAMAX (src/level1.cc:383-402; src/level1-inl.h:343-423): 1-based index of
+// the first element of largest |x|; NaNs never compare larger, so one is only
+// returned when it is x[0].
+template <typename T>
+int Iamax(int n, const T* x, int incx) {
+  if (n < 1 || incx <= 0) return 0;
+  if (n == 1) return 1;
+  int best = 1;
+  T bv = std::fabs(x[0]);
+  if (std::isnan(bv)) return 1;
+  for (int i = 1; i < n; ++i) {
+    const T v = std::fabs(x[static_cast<ptrdiff_t>(i) * incx]);
+    if (v > bv) {
+      best = i + 1;
+      bv = v;
+    }
+  }
+  return best;
+}
+
+template void Gemm<double>(size_t, size_t, size_t, double, Opnd<double>,
+                           Opnd<double>, double, double*, size_t, Part);
+template void Gemm<float>(size_t, size_t, size_t, float, Opnd<float>,
+                          Opnd<float>, float, float*, size_t, Part);
+template int GemmF<double>(char, char, int, int, int, double, const double*,
+                           int, const double*, int, double, double*, int);
+template int GemmF<float>(char, char, int, int, int, float, const float*, int,
+                          const float*, int, float, float*, int);
+template int TrsmF<double>(char, char, char, char, int, int, double,
+                           const double*, int, double*, int);
+template int TrsmF<float>(char, char, char, char, int, int, float,
+                          const float*, int, float*, int);
+template int Iamax<double>(int, const double*, int);
+template int Iamax<float>(int, const float*, int);
+
+}  // namespace orc
+
+extern "C" {
+void orc_set_lanes(int lanes) { orc::g_lanes = (lanes >= 8) ? 8 : 4; }
+int orc_get_lanes(void) { return orc::g_lanes; }
+void orc_set_threads(int threads) { orc::g_threads = threads < 1 ? 1 : threads; }
+
+int orc_dgemm(char ta, char tb, int m, int n, int k, double alpha,
+              const double* a, int lda, const double* b, int ldb, double beta,
+              double* c, int ldc) {
+  return orc::GemmF<double>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c,
+                            ldc);
+}
+int orc_sgemm(char ta, char tb, int m, int n, int k, float alpha,
+              const float* a, int lda, const float* b, int ldb, float beta,
+              float* c, int ldc) {
+  return orc::GemmF<float>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c,
+                           ldc);
+}
+int orc_dtrsm(char side, char uplo, char transa, char diag, int m, int n,
+              double alpha, const double* a, int lda, double* b, int ldb) {
+  return orc::TrsmF<double>(side, uplo, transa, diag, m, n, alpha, a, lda, b,
+                            ldb);
+}
+int orc_strsm(char side, char uplo, char transa, char diag, int m, int n,
+              float alpha, const float* a, int lda, float* b, int ldb) {
+  return orc::TrsmF<float>(side, uplo, transa, diag, m, n, alpha, a, lda, b,
+                           ldb);
+}
+int orc_dsyrk(char uplo, char trans, int n, int k, double alpha,
+              const double* a, int lda, double beta, double* c, int ldc) {
+  return orc::SyrkD(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int orc_idamax(int n, const double* x, int incx) {
+  return orc::Iamax<double>(n, x, incx);
+}
+int orc_isamax(int n, const float* x, int incx) {
+  return orc::Iamax<float>(n, x, incx);
+}
+}  // extern "C"

@@ -1,0 +1,359 @@
+// Oracle LAPACK (TEST INFRASTRUCTURE ONLY; the product never loads this
+// file's library). CPU restatement of the reference's LU and Cholesky drivers
+// on top of the oracle BLAS, with the reference's operation order:
+//
+//   GetrfLeaf  src/lapack/factor_kernels.cc:79-183 (pivot as IAMAX, row swap
+//              across the leaf, 1/pivot unless |pivot| < sfmin, AXPY updates;
+//              columns shorter than one vector use y + alpha*x with two
+//              roundings, longer ones fma(x, alpha, y))
+//   PotrfLeaf  src/lapack/factor_kernels.cc:187-221
+//   Laswp      src/lapack/getrf.cc:28-81
+//   Getrf2     src/lapack/getrf.cc:112-207 (leaf at min(m, n) <= 16)
+//   Getrf      src/lapack/getrf.cc:216-280 (nb = 64, src/lapack/environment.cc:86-88)
+//   Getrs/Gesv src/lapack/getrf.cc:287-374
+//   Potrf2     src/lapack/potrf.cc:48-119 (leaf at n <= 32)
+//   Potrf      src/lapack/potrf.cc:128-199 (nb = 64, environment.cc:110-111)
+//   Potrs/Posv src/lapack/posv.cc:31-114
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <utility>
+
+#include "oracle.h"
+#include "oracle_internal.h"
+
+namespace orc {
+
+template <typename T>
+static T Sfmin() {
+  return sizeof(T) == 8 ? static_cast<T>(DBL_MIN) : static_cast<T>(FLT_MIN);
+}
+
+// Lanes of the reference's vectors of T.
+template <typename T>
+static size_t LanesOf() {
+  return sizeof(T) == 8 ? g_lanes : 2 * g_lanes;
+}
+
+// y[0:n] += alpha * x[0:n] (src/lapack/factor_kernels.cc:79-118).
+template <typename T>
+static void AxpyColumn(size_t n, T alpha, const T* x, T* y) {
+  if (n < LanesOf<T>()) {
+    for (size_t i = 0; i < n; ++i) {
+      const T p = alpha * x[i];
+      y[i] = y[i] + p;
+    }
+    return;
+  }
+  for (size_t i = 0; i < n; ++i) y[i] = std::fma(x[i], alpha, y[i]);
+}
+
+template <typename T>
+int GetrfLeaf(int m_, int n_, T* a, int lda, int* ipiv) {
+  const size_t m = m_, n = n_;
+  const auto at = [&](size_t i, size_t j) -> T& { return a[i + j * lda]; };
+  const T sfmin = Sfmin<T>();
+  int info = 0;
+  for (size_t j = 0; j < std::min(m, n); ++j) {
+    const size_t p = j + static_cast<size_t>(Iamax<T>(m - j, &at(j, j), 1) - 1);
+    ipiv[j] = static_cast<int>(p + 1);
+    const T pivot = at(p, j);
+    if (pivot != T(0)) {
+      if (p != j) {
+        for (size_t k = 0; k < n; ++k) std::swap(at(j, k), at(p, k));
+      }
+      if (std::fabs(pivot) >= sfmin) {
+        const T r = T(1) / pivot;
+        for (size_t i = j + 1; i < m; ++i) at(i, j) = at(i, j) * r;
+      } else {
+        for (size_t i = j + 1; i < m; ++i) at(i, j) = at(i, j) / pivot;
+      }
+    } else if (info == 0) {
+      info = static_cast<int>(j + 1);
+    }
+    for (size_t k = j + 1; k < n; ++k) {
+      AxpyColumn(m - j - 1, -at(j, k), &at(j + 1, j), &at(j + 1, k));
+    }
+  }
+  return info;
+}
+
+template <typename T>
+int PotrfLeaf(bool upper, int n_, T* a, int lda) {
+  const size_t n = n_;
+  const auto at = [&](size_t i, size_t j) -> T& { return a[i + j * lda]; };
+  T row[64];
+  for (size_t j = 0; j < n; ++j) {
+    T ajj = at(j, j);
+    if (ajj <= T(0) || std::isnan(ajj)) return static_cast<int>(j + 1);
+    ajj = std::sqrt(ajj);
+    at(j, j) = ajj;
+    const T rinv = T(1) / ajj;
+    if (upper) {
+      for (size_t k = j + 1; k < n; ++k) {
+        at(j, k) = at(j, k) * rinv;
+        row[k] = at(j, k);
+      }
+      for (size_t k = j + 1; k < n; ++k) {
+        AxpyColumn(k - j, -at(j, k), &row[j + 1], &at(j + 1, k));
+      }
+    } else {
+      for (size_t i = j + 1; i < n; ++i) at(i, j) = at(i, j) * rinv;
+      for (size_t k = j + 1; k < n; ++k) {
+        AxpyColumn(n - k, -at(k, j), &at(k, j), &at(k, k));
+      }
+    }
+  }
+  return 0;
+}
+
+// Row interchanges, 1-based k1..k2 and ipiv (src/lapack/getrf.cc:28-81).
+// Blocking by columns does not change any column's result, so this applies
+// the interchanges column by column.
+template <typename T>
+void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
+  int i1, i2, inc, ix0;
+  if (incx > 0) {
+    ix0 = k1; i1 = k1; i2 = k2; inc = 1;
+  } else if (incx < 0) {
+    ix0 = k1 + (k1 - k2) * incx; i1 = k2; i2 = k1; inc = -1;
+  } else {
+    return;
+  }
+  for (int col = 0; col < n; ++col) {
+    T* ac = a + static_cast<ptrdiff_t>(col) * lda;
+    int ix = ix0;
+    for (int i = i1; inc > 0 ? i <= i2 : i >= i2; i += inc) {
+      const int ip = ipiv[ix - 1];
+      if (ip != i) std::swap(ac[i - 1], ac[ip - 1]);
+      ix += incx;
+    }
+  }
+}
+
+template <typename T>
+int Getrf2(int m, int n, T* a, int lda, int* ipiv) {
+  if (m < 0) return -1;
+  if (n < 0) return -2;
+  if (lda < std::max(1, m)) return -4;
+  if (m == 0 || n == 0) return 0;
+  if (std::min(m, n) <= 16) return GetrfLeaf<T>(m, n, a, lda, ipiv);
+  int info = 0;
+  const int n1 = std::min(m, n) / 2;
+  const int n2 = n - n1;
+  const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
+  int iinfo = Getrf2<T>(m, n1, a, lda, ipiv);
+  if (info == 0 && iinfo > 0) info = iinfo;
+  Laswp<T>(n2, A(0, n1), lda, 1, n1, ipiv, 1);
+  TrsmF<T>('L', 'L', 'N', 'U', n1, n2, T(1), a, lda, A(0, n1), lda);
+  GemmF<T>('N', 'N', m - n1, n2, n1, T(-1), A(n1, 0), lda, A(0, n1), lda, T(1),
+           A(n1, n1), lda);
+  iinfo = Getrf2<T>(m - n1, n2, A(n1, n1), lda, ipiv + n1);
+  if (info == 0 && iinfo > 0) info = iinfo + n1;
+  for (int i = n1; i < std::min(m, n); ++i) ipiv[i] += n1;
+  Laswp<T>(n1, a, lda, n1 + 1, std::min(m, n), ipiv, 1);
+  return info;
+}
+
+template <typename T>
+int Getrf(int m, int n, T* a, int lda, int* ipiv) {
+  if (m < 0) return -1;
+  if (n < 0) return -2;
+  if (lda < std::max(1, m)) return -4;
+  if (m == 0 || n == 0) return 0;
+  const int nb = 64;
+  const int mn = std::min(m, n);
+  if (nb >= mn) return Getrf2<T>(m, n, a, lda, ipiv);
+  const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
+  int info = 0;
+  for (int j = 0; j < mn; j += nb) {
+    const int jb = std::min(mn - j, nb);
+    const int iinfo = Getrf2<T>(m - j, jb, A(j, j), lda, ipiv + j);
+    if (info == 0 && iinfo > 0) info = iinfo + j;
+    for (int i = j; i < std::min(m, j + jb); ++i) ipiv[i] += j;
+    Laswp<T>(j, a, lda, j + 1, j + jb, ipiv, 1);
+    if (j + jb < n) {
+      Laswp<T>(n - j - jb, A(0, j + jb), lda, j + 1, j + jb, ipiv, 1);
+      TrsmF<T>('L', 'L', 'N', 'U', jb, n - j - jb, T(1), A(j, j), lda,
+               A(j, j + jb), lda);
+      if (j + jb < m) {
+        GemmF<T>('N', 'N', m - j - jb, n - j - jb, jb, T(-1), A(j + jb, j),
+                 lda, A(j, j + jb), lda, T(1), A(j + jb, j + jb), lda);
+      }
+    }
+  }
+  return info;
+}
+
+template <typename T>
+int Getrs(char trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
+          T* b, int ldb) {
+  const char t = (trans >= 'a' && trans <= 'z') ? trans - 32 : trans;
+  const bool notran = (t == 'N');
+  if (!notran && t != 'T' && t != 'C') return -1;
+  if (n < 0) return -2;
+  if (nrhs < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (ldb < std::max(1, n)) return -8;
+  if (n == 0 || nrhs == 0) return 0;
+  if (notran) {
+    Laswp<T>(nrhs, b, ldb, 1, n, ipiv, 1);
+    TrsmF<T>('L', 'L', 'N', 'U', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmF<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
+  } else {
+    TrsmF<T>('L', 'U', t, 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmF<T>('L', 'L', t, 'U', n, nrhs, T(1), a, lda, b, ldb);
+    Laswp<T>(nrhs, b, ldb, 1, n, ipiv, -1);
+  }
+  return 0;
+}
+
+int Potrf2D(char uplo, int n, double* a, int lda) {
+  const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
+  const bool upper = (u == 'U');
+  if (!upper && u != 'L') return -1;
+  if (n < 0) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (n == 0) return 0;
+  if (n <= 32) return PotrfLeaf<double>(upper, n, a, lda);
+  const int n1 = n / 2, n2 = n - n1;
+  const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
+  int iinfo = Potrf2D(uplo, n1, a, lda);
+  if (iinfo != 0) return iinfo;
+  if (upper) {
+    TrsmF<double>('L', 'U', 'C', 'N', n1, n2, 1.0, a, lda, A(0, n1), lda);
+    SyrkD('U', 'C', n2, n1, -1.0, A(0, n1), lda, 1.0, A(n1, n1), lda);
+  } else {
+    TrsmF<double>('R', 'L', 'C', 'N', n2, n1, 1.0, a, lda, A(n1, 0), lda);
+    SyrkD('L', 'N', n2, n1, -1.0, A(n1, 0), lda, 1.0, A(n1, n1), lda);
+  }
+  iinfo = Potrf2D(uplo, n2, A(n1, n1), lda);
+  if (iinfo != 0) return iinfo + n1;
+  return 0;
+}
+
+int PotrfD(char uplo, int n, double* a, int lda) {
+  const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
+  const bool upper = (u == 'U');
+  if (!upper && u != 'L') return -1;
+  if (n < 0) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (n == 0) return 0;
+  const int nb = 64;
+  if (nb >= n) return Potrf2D(uplo, n, a, lda);
+  const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
+  for (int j = 0; j < n; j += nb) {
+    const int jb = std::min(nb, n - j);
+    if (upper) {
+      SyrkD('U', 'C', jb, j, -1.0, A(0, j), lda, 1.0, A(j, j), lda);
+      const int info = Potrf2D('U', jb, A(j, j), lda);
+      if (info != 0) return info + j;
+      if (j + jb < n) {
+        GemmF<double>('C', 'N', jb, n - j - jb, j, -1.0, A(0, j), lda,
+                      A(0, j + jb), lda, 1.0, A(j, j + jb), lda);
+        TrsmF<double>('L', 'U', 'C', 'N', jb, n - j - jb, 1.0, A(j, j), lda,
+                      A(j, j + jb), lda);
+      }
+    } else {
+      SyrkD('L', 'N', jb, j, -1.0, A(j, 0), lda, 1.0, A(j, j), lda);
+      const int info = Potrf2D('L', jb, A(j, j), lda);
+      if (info != 0) return info + j;
+      if (j + jb < n) {
+        GemmF<double>('N', 'C', n - j - jb, jb, j, -1.0, A(j + jb, 0), lda,
+                      A(j, 0), lda, 1.0, A(j + jb, j), lda);
+        TrsmF<double>('R', 'L', 'C', 'N', n - j - jb, jb, 1.0, A(j, j), lda,
+                      A(j + jb, j), lda);
+      }
+    }
+  }
+  return 0;
+}
+
+int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b,
+           int ldb) {
+  const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
+  const bool upper = (u == 'U');
+  if (!upper && u != 'L') return -1;
+  if (n < 0) return -2;
+  if (nrhs < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (ldb < std::max(1, n)) return -7;
+  if (n == 0 || nrhs == 0) return 0;
+  if (upper) {
+    TrsmF<double>('L', 'U', 'C', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmF<double>('L', 'U', 'N', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+  } else {
+    TrsmF<double>('L', 'L', 'N', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmF<double>('L', 'L', 'C', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+  }
+  return 0;
+}
+
+template int GetrfLeaf<double>(int, int, double*, int, int*);
+template int GetrfLeaf<float>(int, int, float*, int, int*);
+template int PotrfLeaf<double>(bool, int, double*, int);
+template int PotrfLeaf<float>(bool, int, float*, int);
+
+}  // namespace orc
+
+extern "C" {
+void orc_dlaswp(int n, double* a, int lda, int k1, int k2, const int* ipiv,
+                int incx) {
+  orc::Laswp<double>(n, a, lda, k1, k2, ipiv, incx);
+}
+int orc_dgetrf(int m, int n, double* a, int lda, int* ipiv) {
+  return orc::Getrf<double>(m, n, a, lda, ipiv);
+}
+int orc_dgetrf2(int m, int n, double* a, int lda, int* ipiv) {
+  return orc::Getrf2<double>(m, n, a, lda, ipiv);
+}
+int orc_sgetrf(int m, int n, float* a, int lda, int* ipiv) {
+  return orc::Getrf<float>(m, n, a, lda, ipiv);
+}
+int orc_dgetrs(char trans, int n, int nrhs, const double* a, int lda,
+               const int* ipiv, double* b, int ldb) {
+  return orc::Getrs<double>(trans, n, nrhs, a, lda, ipiv, b, ldb);
+}
+int orc_sgetrs(char trans, int n, int nrhs, const float* a, int lda,
+               const int* ipiv, float* b, int ldb) {
+  return orc::Getrs<float>(trans, n, nrhs, a, lda, ipiv, b, ldb);
+}
+int orc_dgesv(int n, int nrhs, double* a, int lda, int* ipiv, double* b,
+              int ldb) {
+  if (n < 0) return -1;
+  if (nrhs < 0) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (ldb < std::max(1, n)) return -7;
+  int info = orc::Getrf<double>(n, n, a, lda, ipiv);
+  if (info == 0) info = orc::Getrs<double>('N', n, nrhs, a, lda, ipiv, b, ldb);
+  return info;
+}
+int orc_dpotrf(char uplo, int n, double* a, int lda) {
+  return orc::PotrfD(uplo, n, a, lda);
+}
+int orc_dpotrf2(char uplo, int n, double* a, int lda) {
+  return orc::Potrf2D(uplo, n, a, lda);
+}
+int orc_dpotrs(char uplo, int n, int nrhs, const double* a, int lda, double* b,
+               int ldb) {
+  return orc::PotrsD(uplo, n, nrhs, a, lda, b, ldb);
+}
+int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
+              int ldb) {
+  const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
+  if (u != 'U' && u != 'L') return -1;
+  if (n < 0) return -2;
+  if (nrhs < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (ldb < std::max(1, n)) return -7;
+  int info = orc::PotrfD(uplo, n, a, lda);
+  if (info == 0) info = orc::PotrsD(uplo, n, nrhs, a, lda, b, ldb);
+  return info;
+}
+int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv) {
+  return orc::GetrfLeaf<double>(m, n, a, lda, ipiv);
+}
+int orc_dpotrf_leaf(int upper, int n, double* a, int lda) {
+  return orc::PotrfLeaf<double>(upper != 0, n, a, lda);
+}
+}  // extern "C"

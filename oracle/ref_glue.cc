@@ -1,0 +1,136 @@
+// Glue for building the reference's own LU/Cholesky drivers (TEST
+// INFRASTRUCTURE ONLY). The reference's src/lapack/getrf.cc, potrf.cc and
+// environment.cc compile without Highway; they reach BLAS through the exported
+// Fortran symbols (src/lapack/blas.h:48-79, 338-352) and their leaves through
+// hwyblas::lapack::GetrfLeaf/PotrfLeaf (src/lapack/factor_kernels.h:34-40).
+// The Highway-based BLAS itself cannot be built here (Highway is absent), so
+// this file supplies those symbols from the oracle's restatement. Linking the
+// reference drivers to them lets the tests check the oracle's own LAPACK
+// restatement against the reference's driver code, bit for bit.
+//
+// Routines the hot path never reaches (complex types, xGETRI's helpers) abort;
+// the Fortran ones are in ref_stubs.c.
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+
+#include "src/common.h"
+#include "src/lapack/factor_kernels.h"
+#include "oracle_internal.h"
+
+namespace {
+[[noreturn]] void Unreached(const char* name) {
+  fprintf(stderr, "oracle/_ref: %s is not part of the checked path\n", name);
+  abort();
+}
+int g_last_error_pos = 0;
+char g_last_error_name[16] = {0};
+}  // namespace
+
+namespace hwyblas {
+void ReportError(const char* routine, blasint info) {
+  g_last_error_pos = info;
+  snprintf(g_last_error_name, sizeof(g_last_error_name), "%s", routine);
+}
+
+namespace lapack {
+template <typename T>
+blasint GetrfLeaf(blasint m, blasint n, T* a, blasint lda, blasint* ipiv) {
+  if constexpr (std::is_floating_point_v<T>) {
+    return orc::GetrfLeaf<T>(m, n, a, lda, ipiv);
+  } else {
+    Unreached("complex GetrfLeaf");
+  }
+}
+template <typename T>
+blasint PotrfLeaf(bool upper, blasint n, T* a, blasint lda) {
+  if constexpr (std::is_floating_point_v<T>) {
+    return orc::PotrfLeaf<T>(upper, n, a, lda);
+  } else {
+    Unreached("complex PotrfLeaf");
+  }
+}
+template <typename T>
+blasint Trtri(char, char, blasint, T*, blasint) {
+  Unreached("Trtri");
+}
+template <typename T>
+void Lacgv(blasint, T*, blasint) {
+  Unreached("Lacgv");
+}
+#define ORC_INST(T)                                                   \
+  template blasint GetrfLeaf<T>(blasint, blasint, T*, blasint, blasint*); \
+  template blasint PotrfLeaf<T>(bool, blasint, T*, blasint);          \
+  template blasint Trtri<T>(char, char, blasint, T*, blasint);        \
+  template void Lacgv<T>(blasint, T*, blasint);
+ORC_INST(float)
+ORC_INST(double)
+ORC_INST(std::complex<float>)
+ORC_INST(std::complex<double>)
+#undef ORC_INST
+}  // namespace lapack
+}  // namespace hwyblas
+
+using hwyblas::blasint;
+
+extern "C" {
+int orc_ref_last_error(char* name, int len) {
+  if (name && len > 0) snprintf(name, len, "%s", g_last_error_name);
+  const int p = g_last_error_pos;
+  g_last_error_pos = 0;
+  return p;
+}
+
+void dgemm_(const char* ta, const char* tb, const blasint* m, const blasint* n,
+            const blasint* k, const double* alpha, const double* a,
+            const blasint* lda, const double* b, const blasint* ldb,
+            const double* beta, double* c, const blasint* ldc) {
+  const int info = orc::GemmF<double>(*ta, *tb, *m, *n, *k, *alpha, a, *lda, b,
+                                      *ldb, *beta, c, *ldc);
+  if (info) hwyblas::ReportError("DGEMM", info);
+}
+void sgemm_(const char* ta, const char* tb, const blasint* m, const blasint* n,
+            const blasint* k, const float* alpha, const float* a,
+            const blasint* lda, const float* b, const blasint* ldb,
+            const float* beta, float* c, const blasint* ldc) {
+  const int info = orc::GemmF<float>(*ta, *tb, *m, *n, *k, *alpha, a, *lda, b,
+                                     *ldb, *beta, c, *ldc);
+  if (info) hwyblas::ReportError("SGEMM", info);
+}
+void dtrsm_(const char* s, const char* u, const char* t, const char* d,
+            const blasint* m, const blasint* n, const double* alpha,
+            const double* a, const blasint* lda, double* b,
+            const blasint* ldb) {
+  const int info =
+      orc::TrsmF<double>(*s, *u, *t, *d, *m, *n, *alpha, a, *lda, b, *ldb);
+  if (info) hwyblas::ReportError("DTRSM", info);
+}
+void strsm_(const char* s, const char* u, const char* t, const char* d,
+            const blasint* m, const blasint* n, const float* alpha,
+            const float* a, const blasint* lda, float* b, const blasint* ldb) {
+  const int info =
+      orc::TrsmF<float>(*s, *u, *t, *d, *m, *n, *alpha, a, *lda, b, *ldb);
+  if (info) hwyblas::ReportError("STRSM", info);
+}
+void dsyrk_(const char* u, const char* t, const blasint* n, const blasint* k,
+            const double* alpha, const double* a, const blasint* lda,
+            const double* beta, double* c, const blasint* ldc) {
+  const int info = orc::SyrkD(*u, *t, *n, *k, *alpha, a, *lda, *beta, c, *ldc);
+  if (info) hwyblas::ReportError("DSYRK", info);
+}
+blasint idamax_(const blasint* n, const double* x, const blasint* incx) {
+  return orc::Iamax<double>(*n, x, *incx);
+}
+blasint isamax_(const blasint* n, const float* x, const blasint* incx) {
+  return orc::Iamax<float>(*n, x, *incx);
+}
+void dscal_(const blasint* n, const double* a, double* x, const blasint* incx) {
+  if (*n <= 0 || *incx <= 0) return;
+  for (blasint i = 0; i < *n; ++i) x[i * *incx] *= *a;
+}
+void sscal_(const blasint* n, const float* a, float* x, const blasint* incx) {
+  if (*n <= 0 || *incx <= 0) return;
+  for (blasint i = 0; i < *n; ++i) x[i * *incx] *= *a;
+}
+
+}  // extern "C"

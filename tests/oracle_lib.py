@@ -1,0 +1,173 @@
+"""ctypes bindings of the oracle (oracle/liboracle.so) for the tests.
+
+The oracle is the checker: a CPU restatement of the reference's hot path with
+its exact rounding. Only the tests, the smoke check and the CPU-baseline legs
+of bench.py use it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_LIB = os.path.join(ORACLE_DIR, "_ref", "libhwyref.so")
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+D = ctypes.c_double
+F = ctypes.c_float
+CH = ctypes.c_char
+
+
+def build_oracle():
+    if not os.path.exists(ORACLE_LIB):
+        subprocess.run(["make", "-C", ORACLE_DIR, "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return ORACLE_LIB
+
+
+def load_ref():
+    if not os.path.exists(REF_LIB):
+        return None
+    lib = ctypes.CDLL(REF_LIB)
+    lib.dgetrf_.argtypes = [P] * 6
+    lib.dgetrf2_.argtypes = [P] * 6
+    lib.dpotrf_.argtypes = [P] * 5
+    lib.dpotrf2_.argtypes = [P] * 5
+    lib.dgetrs_.argtypes = [P] * 9
+    lib.dgesv_.argtypes = [P] * 8
+    return lib
+
+
+def ptr(a):
+    return a.ctypes.data_as(P) if a is not None else None
+
+
+def _b(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+class Oracle:
+    def __init__(self):
+        self.lib = ctypes.CDLL(build_oracle())
+        L = self.lib
+        L.orc_set_lanes.argtypes = [I]
+        L.orc_set_threads.argtypes = [I]
+        L.orc_dgemm.argtypes = [CH, CH, I, I, I, D, P, I, P, I, D, P, I]
+        L.orc_sgemm.argtypes = [CH, CH, I, I, I, F, P, I, P, I, F, P, I]
+        L.orc_dtrsm.argtypes = [CH, CH, CH, CH, I, I, D, P, I, P, I]
+        L.orc_dsyrk.argtypes = [CH, CH, I, I, D, P, I, D, P, I]
+        L.orc_idamax.argtypes = [I, P, I]
+        L.orc_dlaswp.argtypes = [I, P, I, I, I, P, I]
+        L.orc_dgetrf.argtypes = [I, I, P, I, P]
+        L.orc_dgetrf2.argtypes = [I, I, P, I, P]
+        L.orc_sgetrf.argtypes = [I, I, P, I, P]
+        L.orc_dgetrs.argtypes = [CH, I, I, P, I, P, P, I]
+        L.orc_sgetrs.argtypes = [CH, I, I, P, I, P, P, I]
+        L.orc_dgesv.argtypes = [I, I, P, I, P, P, I]
+        L.orc_dpotrf.argtypes = [CH, I, P, I]
+        L.orc_dpotrf2.argtypes = [CH, I, P, I]
+        L.orc_dpotrs.argtypes = [CH, I, I, P, I, P, I]
+        L.orc_dposv.argtypes = [CH, I, I, P, I, P, I]
+        L.orc_set_lanes(8)
+
+    def set_threads(self, n):
+        self.lib.orc_set_threads(int(n))
+
+    def dgemm(self, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+        return self.lib.orc_dgemm(_b(ta), _b(tb), m, n, k, alpha, ptr(a), lda, ptr(b),
+                                  ldb, beta, ptr(c), ldc)
+
+    def sgemm(self, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+        return self.lib.orc_sgemm(_b(ta), _b(tb), m, n, k, alpha, ptr(a), lda, ptr(b),
+                                  ldb, beta, ptr(c), ldc)
+
+    def dtrsm(self, side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+        return self.lib.orc_dtrsm(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha,
+                                  ptr(a), lda, ptr(b), ldb)
+
+    def dsyrk(self, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+        return self.lib.orc_dsyrk(_b(uplo), _b(trans), n, k, alpha, ptr(a), lda, beta,
+                                  ptr(c), ldc)
+
+    def idamax(self, n, x, incx):
+        return self.lib.orc_idamax(n, ptr(x), incx)
+
+    def dlaswp(self, n, a, lda, k1, k2, ipiv, incx):
+        self.lib.orc_dlaswp(n, ptr(a), lda, k1, k2, ptr(ipiv), incx)
+
+    def dgetrf(self, m, n, a, lda, ipiv):
+        return self.lib.orc_dgetrf(m, n, ptr(a), lda, ptr(ipiv))
+
+    def dgetrf2(self, m, n, a, lda, ipiv):
+        return self.lib.orc_dgetrf2(m, n, ptr(a), lda, ptr(ipiv))
+
+    def sgetrf(self, m, n, a, lda, ipiv):
+        return self.lib.orc_sgetrf(m, n, ptr(a), lda, ptr(ipiv))
+
+    def dgetrs(self, trans, n, nrhs, a, lda, ipiv, b, ldb):
+        return self.lib.orc_dgetrs(_b(trans), n, nrhs, ptr(a), lda, ptr(ipiv), ptr(b), ldb)
+
+    def dgesv(self, n, nrhs, a, lda, ipiv, b, ldb):
+        return self.lib.orc_dgesv(n, nrhs, ptr(a), lda, ptr(ipiv), ptr(b), ldb)
+
+    def dpotrf(self, uplo, n, a, lda):
+        return self.lib.orc_dpotrf(_b(uplo), n, ptr(a), lda)
+
+    def dpotrf2(self, uplo, n, a, lda):
+        return self.lib.orc_dpotrf2(_b(uplo), n, ptr(a), lda)
+
+    def dpotrs(self, uplo, n, nrhs, a, lda, b, ldb):
+        return self.lib.orc_dpotrs(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
+
+    def dposv(self, uplo, n, nrhs, a, lda, b, ldb):
+        return self.lib.orc_dposv(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
+
+
+def ref_call_getrf(lib, recursive, m, n, a, lda, ipiv):
+    info = ctypes.c_int(0)
+    args = [ctypes.byref(ctypes.c_int(m)), ctypes.byref(ctypes.c_int(n)), ptr(a),
+            ctypes.byref(ctypes.c_int(lda)), ptr(ipiv), ctypes.byref(info)]
+    (lib.dgetrf2_ if recursive else lib.dgetrf_)(*args)
+    return info.value
+
+
+def ref_call_potrf(lib, recursive, uplo, n, a, lda):
+    info = ctypes.c_int(0)
+    args = [ctypes.c_char_p(_b(uplo)), ctypes.byref(ctypes.c_int(n)), ptr(a),
+            ctypes.byref(ctypes.c_int(lda)), ctypes.byref(info)]
+    (lib.dpotrf2_ if recursive else lib.dpotrf_)(*args)
+    return info.value
+
+
+def rand(rng, rows, cols, dtype=np.float64):
+    """Column-major uniform[-1, 1] matrix (the reference tests' Random<T>)."""
+    return np.asfortranarray(rng.uniform(-1.0, 1.0, (rows, cols)).astype(dtype))
+
+
+def same_bits(x, y):
+    """Bitwise equality, treating any two NaNs as equal."""
+    x = np.asarray(x)
+    y = np.asarray(y)
+    if x.shape != y.shape:
+        return False
+    nx, ny = np.isnan(x), np.isnan(y)
+    if not np.array_equal(nx, ny):
+        return False
+    ix = x.view(np.uint64 if x.dtype == np.float64 else np.uint32)
+    iy = y.view(np.uint64 if y.dtype == np.float64 else np.uint32)
+    return bool(np.all((ix == iy) | nx))
+
+
+def first_diff(x, y):
+    x = np.asarray(x).ravel(order="F")
+    y = np.asarray(y).ravel(order="F")
+    bad = ~((x == y) | (np.isnan(x) & np.isnan(y)))
+    idx = np.flatnonzero(bad)
+    if idx.size == 0:
+        return None
+    i = idx[0]
+    return f"{idx.size} differ; first at flat {i}: {x[i]!r} vs {y[i]!r}"
