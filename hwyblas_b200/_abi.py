@@ -42,6 +42,7 @@ PROTOTYPES = {
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),
+    "hwyblas_fp64_peak_tflops": (ctypes.c_double, []),
 }
 
 EXPORTED = sorted(PROTOTYPES)

@@ -16,9 +16,11 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhwyblas_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
+# -fmad=false: no contraction of a*b + c into an FMA (the reference builds
+# with -ffp-contract=off); every FMA in the kernels is an explicit fma().
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
     "-Xcompiler", "-fPIC,-fvisibility=hidden",
     "-Wno-deprecated-gpu-targets",
 ]

@@ -297,8 +297,12 @@ __global__ void __launch_bounds__(kLeafThreads)
   }
 }
 
-// LU leaf, trailing columns (n > m, m <= 16): each column replays the leaf's
-// interchanges and AXPY updates on its own (columns are independent).
+// LU leaf, trailing columns (n > m, m <= 16). In the reference, step j swaps
+// rows j and p_j of every column and then updates rows i > j of column k as
+// x_i += (-x_j) * l_ij. Later swaps only exchange rows > j, in the L columns
+// and in column k alike, so each multiplier stays on the row it updates: the
+// same arithmetic is all swaps first, then the updates with the final L.
+// Columns are independent: one thread per column.
 template <typename T>
 __global__ void GetrfLeafTrailingKernel(int m, int w, int n, T* a,
                                         long long lda, const int* ipiv,
@@ -307,13 +311,15 @@ __global__ void GetrfLeafTrailingKernel(int m, int w, int n, T* a,
   if (k >= n) return;
   T* col = a + k * lda;
   for (int j = 0; j < w; ++j) {
+    // A zero pivot has p == j (its column is all zeros), so no swap.
     const int p = ipiv[j] - 1;
-    const T pivot = a[j + j * lda];  // a(j, j) after the interchange
-    if (pivot != T(0) && p != j) {
+    if (p != j) {
       const T t = col[j];
       col[j] = col[p];
       col[p] = t;
     }
+  }
+  for (int j = 0; j < w; ++j) {
     const T alpha = -col[j];
     const int len = m - j - 1;
     for (int i = j + 1; i < m; ++i) col[i] = Axpy(col[i], alpha, a[i + j * lda], len, lanes);

@@ -200,6 +200,10 @@ HWYBLAS_API int hwyblas_last_cuda_error(void);
 /* Number of kernels the library has launched (all threads). No counterpart
  * in the reference; used to count launches inside timed regions. */
 HWYBLAS_API uint64_t hwyblas_launch_count(void);
+/* Measured FP64 tensor-pipe throughput of the current device (TFLOP/s), from
+ * a DMMA issue-rate loop; the FP64 roofline denominator. No counterpart in
+ * the reference. */
+HWYBLAS_API double hwyblas_fp64_peak_tflops(void);
 
 #ifdef __cplusplus
 }

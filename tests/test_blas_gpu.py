@@ -31,8 +31,8 @@ def run_gemm(hb, orc, ta, tb, m, n, k, alpha, beta, pad=0, seed=0, poison_beta0=
     c_gpu, c_orc = c.copy(order="F"), c.copy(order="F")
     hb.dgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c_gpu, ldc)
     orc.dgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c_orc, ldc)
-    assert same_bits(c_gpu, c_orc), (ta, tb, m, n, k, alpha, beta, pad,
-                                     first_diff(c_gpu, c_orc))
+    assert same_bits(c_gpu, c_orc), (first_diff(c_gpu, c_orc), ta, tb, m, n, k, alpha,
+                                     beta, pad)
 
 
 @pytest.mark.parametrize("ta", ["N", "T"])
