@@ -16,11 +16,16 @@
 //
 // Tiling: a CTA computes a 128 x 64 tile of C with 8 consumer warps (32 x 32
 // each: 2 x 4 MMAs per k8 step) and one producer warp that streams 16-deep k
-// slices of op(A) (128 x 16, M-contiguous) and op(B) (16 x 64, K-contiguous,
-// 128-byte swizzle) into a 4-stage shared-memory ring with TMA and mbarriers.
-// Rows of each 16-row MMA block are interleaved (MMA row g <-> tile row 2g,
-// g+8 <-> 2g+1) so that each thread's A fragment is one 16-byte shared load
-// and every shared load is bank-conflict free.
+// slices of op(A) (eight 16 x 16 boxes, M-contiguous) and op(B) (16 x 64,
+// K-contiguous) into a 4-stage shared-memory ring with TMA (128-byte swizzle:
+// the 16-byte chunk c of row r lands at chunk c ^ (r & 7)) and mbarriers.
+// Which tile row/column each MMA row/column computes is a free choice, made so
+// that every shared load is conflict free: MMA rows g and g+8 of a 16-row
+// block take the adjacent tile rows 2c(g), 2c(g)+1 with c = [0,4,1,5,2,6,3,7]
+// (one 16-byte load per A fragment pair; the 8 lanes of each 128-bit load
+// phase hit 8 distinct chunks), and MMA column g takes tile column
+// [0,2,4,6,1,3,5,7][g] of its 8-column block (the 16 lanes of each 64-bit
+// load phase hit 16 distinct 8-byte slots).
 #include <cuda.h>
 
 #include <algorithm>
@@ -35,7 +40,8 @@ namespace {
 constexpr int kBM = 128, kBN = 64, kBK = 16, kStages = 4;
 constexpr int kConsumerWarps = 8;
 constexpr int kThreads = (kConsumerWarps + 1) * 32;
-constexpr int kTileABytes = kBM * kBK * 8;
+constexpr int kTileABytes = kBM * kBK * 8;  // 8 boxes of 16 (m) x 16 (k)
+constexpr int kABoxBytes = 16 * kBK * 8;
 constexpr int kTileBBytes = kBN * kBK * 8;
 constexpr int kStageBytes = kTileABytes + kTileBBytes;
 constexpr int kKtPerChunk = 256 / kBK;  // k-slices per reference KC chunk
@@ -119,7 +125,9 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
           break;
         uint8_t* st = smem + s * kStageBytes;
         MbarArriveExpectTx(&full[s], kStageBytes);
-        TmaLoad2d(st, &tm_a, m0, kt * kBK, &full[s]);
+#pragma unroll
+        for (int b = 0; b < kBM / 16; ++b)
+          TmaLoad2d(st + b * kABoxBytes, &tm_a, m0 + 16 * b, kt * kBK, &full[s]);
         TmaLoad2d(st + kTileABytes, &tm_b, kt * kBK, n0, &full[s]);
       }
     }
@@ -128,8 +136,15 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
 
   const int wm = warp % 4, wn = warp / 4;
   const int g = lane >> 2, t = lane & 3;
-  // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1), col0 + nb*8 + (e & 1)).
-  const int row0 = m0 + wm * 32 + 2 * g, col0 = n0 + wn * 32 + 2 * t;
+  // Tile-row pair of MMA rows (g, g+8) and tile columns of MMA columns 2t,
+  // 2t+1 (see the file comment).
+  const int cg = (g >> 1) + 4 * (g & 1);
+  const int ccol0 = 2 * ((2 * t) & 3) + ((2 * t) >> 2);
+  const int ccol1 = 2 * ((2 * t + 1) & 3) + ((2 * t + 1) >> 2);
+  const int bcol = 2 * (g & 3) + (g >> 2);  // tile column of this lane's B
+  // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
+  // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
+  const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
   double acc[2][4][4];
   double cacc[2][4][4];  // kMulti: C_in, then the running merged value
   uint32_t in_part = 0, crossing = 0;
@@ -140,7 +155,8 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int bit = (mb * 4 + nb) * 4 + e;
-        const int i = row0 + mb * 16 + (e >> 1), j = col0 + nb * 8 + (e & 1);
+        const int i = row0 + mb * 16 + (e >> 1);
+        const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
         acc[mb][nb][e] = 0.0;
         const bool inside = InPart(p, i, j);
         if (inside) in_part |= 1u << bit;
@@ -160,13 +176,15 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
 #pragma unroll
     for (int ks = 0; ks < kBK / 8; ++ks) {
       double af[2][4];
+      const int klo = ks * 8 + t, khi = klo + 4;
 #pragma unroll
       for (int mb = 0; mb < 2; ++mb) {
-        const int row = wm * 32 + mb * 16 + 2 * g;
-        const double2 lo =
-            *reinterpret_cast<const double2*>(sa + (ks * 8 + t) * kBM + row);
+        const uint8_t* box = reinterpret_cast<const uint8_t*>(sa) +
+                             (wm * 2 + mb) * kABoxBytes;
+        const double2 lo = *reinterpret_cast<const double2*>(
+            box + klo * 128 + ((cg ^ (klo & 7)) << 4));
         const double2 hi = *reinterpret_cast<const double2*>(
-            sa + (ks * 8 + t + 4) * kBM + row);
+            box + khi * 128 + ((cg ^ (khi & 7)) << 4));
         af[mb][0] = lo.x;
         af[mb][1] = lo.y;
         af[mb][2] = hi.x;
@@ -174,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
       }
 #pragma unroll
       for (int nb = 0; nb < 4; ++nb) {
-        const int r = wn * 32 + nb * 8 + g;
+        const int r = wn * 32 + nb * 8 + bcol;
         const int k0 = ks * 8 + t, k1 = k0 + 4;
         const double b0 = *reinterpret_cast<const double*>(
             sb + r * 128 + (((k0 >> 1) ^ (r & 7)) << 4) + ((k0 & 1) << 3));
@@ -225,7 +243,8 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
       for (int e = 0; e < 4; ++e) {
         const int bit = (mb * 4 + nb) * 4 + e;
         if (!((in_part >> bit) & 1u)) continue;
-        const int i = row0 + mb * 16 + (e >> 1), j = col0 + nb * 8 + (e & 1);
+        const int i = row0 + mb * 16 + (e >> 1);
+        const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
         double v;
         if constexpr (kMulti) {
           v = cacc[mb][nb][e];
@@ -373,7 +392,7 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const double* cb = Canonical(b, k, n, kWsPackB, &ldb);
   CUtensorMap ma, mb;
   if (!MakeTensorMap2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ca, m, k, lda,
-                       kBM, kBK, CU_TENSOR_MAP_SWIZZLE_NONE) ||
+                       16, kBK, CU_TENSOR_MAP_SWIZZLE_128B) ||
       !MakeTensorMap2d(&mb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, cb, k, n, ldb,
                        kBK, kBN, CU_TENSOR_MAP_SWIZZLE_128B)) {
     Failed(cudaErrorInvalidValue, "dgemm tensor map");
