@@ -224,6 +224,7 @@ def run_ours(args):
     B = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     C0 = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     C = C0.clone()
+    torch.cuda.synchronize()  # inputs come from torch's stream
     stream = torch.cuda.Stream()
     hb.set_stream(stream)
     peak = float(lib.hwyblas_fp64_peak_tflops())

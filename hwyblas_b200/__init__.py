@@ -17,7 +17,7 @@ __all__ = [
     "lib", "dgemm", "sgemm", "dtrsm", "dsyrk", "idamax", "dlaswp", "dgetrf",
     "dgetrf2", "dgetrs", "dgesv", "dpotrf", "dpotrf2", "dpotrs", "dposv",
     "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
-    "ErrorCapture", "launch_count", "set_stream",
+    "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -41,6 +41,7 @@ from ._api import (  # noqa: E402  (needs lib())
     dgemm, sgemm, dtrsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
     dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
     cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
+    dgemm_emulated, dgemm_ddref,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

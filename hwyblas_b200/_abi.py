@@ -39,6 +39,8 @@ PROTOTYPES = {
     "cblas_dtrsm": (None, [I, I, I, I, I, I, I, D, P, I, P, I]),
     "cblas_idamax": (ctypes.c_size_t, [I, P, I]),
     # Extensions
+    "hwyblas_dgemm_emulated": (I, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI, PI]),
+    "hwyblas_dgemm_ddref": (None, [C, C, PI, PI, PI, P, PI, P, PI, PI, P, P, PI]),
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),

@@ -131,6 +131,22 @@ def dposv(uplo, n, nrhs, a, lda, b, ldb):
                       _ptr(b), _i(ldb))
 
 
+def dgemm_emulated(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                   slices=0):
+    """FP64-accurate GEMM on INT8 tensor cores (Ozaki slices; 0 = auto).
+    Returns the slice count used."""
+    return lib().hwyblas_dgemm_emulated(_c(transa), _c(transb), _i(m), _i(n), _i(k),
+                                        _d(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb),
+                                        _d(beta), _ptr(c), _i(ldc), _i(slices))
+
+
+def dgemm_ddref(transa, transb, m, k, a, lda, b, ldb, n, cols, out, ldo):
+    """out[:, jj] = op(A) op(B)[:, cols[jj]] in double-double (error reference)."""
+    lib().hwyblas_dgemm_ddref(_c(transa), _c(transb), _i(m), _i(len(cols)), _i(k),
+                              _ptr(a), _i(lda), _ptr(b), _i(ldb), _i(n), _ptr(cols),
+                              _ptr(out), _i(ldo))
+
+
 def cblas_dgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
                 ldc):
     lib().cblas_dgemm(layout, transa, transb, m, n, k, alpha, _ptr(a), lda,

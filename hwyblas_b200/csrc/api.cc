@@ -821,6 +821,86 @@ HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
 // ---------------------------------------------------------------------------
 // Extensions.
 
+// Slice count for the emulated GEMM when the caller passes 0 (auto).
+static int AutoSlices(int k) { return k <= 2048 ? 7 : 8; }
+
+HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
+    const char* transa, const char* transb, const hwyblas_int* m_p,
+    const hwyblas_int* n_p, const hwyblas_int* k_p, const double* alpha_p,
+    const double* a, const hwyblas_int* lda_p, const double* b,
+    const hwyblas_int* ldb_p, const double* beta_p, double* c,
+    const hwyblas_int* ldc_p, const hwyblas_int* slices_p) {
+  const int m = *m_p, n = *n_p, k = *k_p, lda = *lda_p, ldb = *ldb_p,
+            ldc = *ldc_p, slices = *slices_p;
+  bool ta, tb;
+  const bool va = hb::DecodeOp(*transa, &ta), vb = hb::DecodeOp(*transb, &tb);
+  const int rows_a = ta ? k : m, rows_b = tb ? n : k;
+  int info = 0;
+  if (!va) info = 1;
+  else if (!vb) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, m)) info = 13;
+  else if (slices < 0 || slices > 8) info = 14;
+  if (info != 0) {
+    hb::ReportError("DGEMM_EMULATED", info);
+    return -1;
+  }
+  const double alpha = *alpha_p, beta = *beta_p;
+  if (m == 0 || n == 0) return 0;
+  if ((k == 0 || alpha == 0.0) && beta == 1.0) return 0;
+  hb::Staged<double> sa, sb, sc;
+  const bool compute = !(k == 0 || alpha == 0.0);
+  if (compute) {
+    if (!sa.In(a, lda, rows_a, ta ? m : k, hb::kWsStageA, true)) return -1;
+    if (!sb.In(b, ldb, rows_b, tb ? k : n, hb::kWsStageB, true)) return -1;
+  }
+  if (!sc.In(c, ldc, m, n, hb::kWsStageC, beta != 0.0)) return -1;
+  int used = 0;
+  if (!compute) {
+    hb::ScaleMatrix<double>(m, n, beta, sc.dev, sc.ld, hb::kAll);
+  } else {
+    const int S = slices == 0 ? AutoSlices(k) : slices;
+    used = hb::DgemmEmulated(m, n, k, alpha, hb::ColMajor<double>(sa.dev, sa.ld, ta),
+                             hb::ColMajor<double>(sb.dev, sb.ld, tb), beta, sc.dev,
+                             sc.ld, S);
+  }
+  sc.Out();
+  hb::Finish("DGEMM_EMULATED");
+  return used;
+}
+
+HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
+                                     const hwyblas_int* m_p,
+                                     const hwyblas_int* ncols_p,
+                                     const hwyblas_int* k_p, const double* a,
+                                     const hwyblas_int* lda_p, const double* b,
+                                     const hwyblas_int* ldb_p,
+                                     const hwyblas_int* n_p,
+                                     const hwyblas_int* cols, double* out,
+                                     const hwyblas_int* ldo_p) {
+  const int m = *m_p, ncols = *ncols_p, k = *k_p, lda = *lda_p, ldb = *ldb_p,
+            n = *n_p, ldo = *ldo_p;
+  bool ta, tb;
+  hb::DecodeOp(*transa, &ta);
+  hb::DecodeOp(*transb, &tb);
+  if (m <= 0 || ncols <= 0 || k <= 0 || n <= 0) return;
+  hb::Staged<double> sa, sb, so;
+  hb::StagedInts sj;
+  if (!sa.In(a, lda, ta ? k : m, ta ? m : k, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, tb ? n : k, tb ? k : n, hb::kWsStageB, true)) return;
+  if (!so.In(out, ldo, m, ncols, hb::kWsStageC, false)) return;
+  if (!sj.In(cols, ncols, 0, true)) return;
+  hb::DgemmDoubleDouble(m, ncols, k, hb::ColMajor<double>(sa.dev, sa.ld, ta),
+                        hb::ColMajor<double>(sb.dev, sb.ld, tb), sj.dev, so.dev,
+                        so.ld);
+  so.Out();
+  hb::Finish("DGEMM_DDREF");
+}
+
 HWYBLAS_API void hwyblas_set_stream(void* stream) {
   hb::Context& c = Ctx();
   c.stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : c.own_stream;

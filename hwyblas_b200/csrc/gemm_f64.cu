@@ -93,9 +93,15 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
   if (p.guard != nullptr && *p.guard != 0) return;
-  const int tiles_m = (p.m + kBM - 1) / kBM;
-  const int m0 = (blockIdx.x % tiles_m) * kBM;
-  const int n0 = (blockIdx.x / tiles_m) * kBN;
+  // Tiles in groups of 16 tile rows, so that a wave of CTAs covers a compact
+  // block of C and shares its A and B tiles in L2.
+  const int tiles_m = (p.m + kBM - 1) / kBM, tiles_n = (p.n + kBN - 1) / kBN;
+  const int per_group = 16 * tiles_n;
+  const int first_m = (static_cast<int>(blockIdx.x) / per_group) * 16;
+  const int gm = min(tiles_m - first_m, 16);
+  const int in_group = static_cast<int>(blockIdx.x) % per_group;
+  const int m0 = (first_m + in_group % gm) * kBM;
+  const int n0 = (in_group / gm) * kBN;
   if (p.part == kLower && m0 + kBM - 1 < n0) return;
   if (p.part == kUpper && m0 > n0 + kBN - 1) return;
 

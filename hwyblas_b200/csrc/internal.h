@@ -73,7 +73,8 @@ enum WorkspaceSlot : int {
   kWsMixed2 = 9,
   kWsMixed3 = 10,
   kWsBatch = 11,
-  kNumWorkspaceSlots = 12
+  kWsEmulW = 12,   // emulated-GEMM FP64 partial sums between passes
+  kNumWorkspaceSlots = 13
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -144,6 +145,16 @@ void SyrkFull(bool lower, bool trans, int n, int k, double alpha,
 template <typename T>
 void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
               int lda, const T* b, int ldb, T beta, T* c, int ldc);
+
+// FP64-accurate GEMM on INT8 tensor cores with `slices` slices (1..8);
+// returns the slice count used, 0 if non-finite inputs sent it to Dgemm, -1
+// on a CUDA error.
+int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
+                  View<double> b, double beta, double* c, int ldc, int slices);
+int OzakiMaxK(int S);
+// out(:, jj) = op(A) op(B)(:, cols[jj]) in double-double (error reference).
+void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,
+                       const int* cols, double* out, int ldo);
 
 // Host-side wait-timeout check: returns true (and reports) if any kernel on
 // the context set the timeout flag since the last check. Synchronises.

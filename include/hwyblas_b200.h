@@ -190,6 +190,34 @@ HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
 /* ------------------------------------------------------------------------ */
 /* Extensions (hwyblas_ prefix, as the reference's own additions)           */
 
+/* FP64-accurate GEMM on the INT8 tensor cores (Ozaki scheme): each row of
+ * op(A) and column of op(B) is scaled by a power of two and cut into `slices`
+ * 7-bit integer slices (1..8; 0 = chosen from K), the slice products with
+ * index sum below `slices` run as exact INT32 tensor-core GEMMs, and the
+ * levels are recombined in FP64 with compensated summation. Arguments and
+ * errors as dgemm_ (position 14: slices). Returns the slice count used (0:
+ * non-finite inputs, computed by the plain FP64 path instead; -1: error).
+ * No counterpart in the reference (a north-star extension). */
+HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
+    const char* transa, const char* transb, const hwyblas_int* m,
+    const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+    const double* a, const hwyblas_int* lda, const double* b,
+    const hwyblas_int* ldb, const double* beta, double* c,
+    const hwyblas_int* ldc, const hwyblas_int* slices);
+/* out(:, jj) = op(A) * op(B)(:, cols[jj] - 0) for jj < ncols (0-based column
+ * indices into the n columns of op(B)), accumulated in double-double and
+ * rounded once: the higher-precision reference against which the error of
+ * every FP64 path is stated. No counterpart in the reference. */
+HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
+                                     const hwyblas_int* m,
+                                     const hwyblas_int* ncols,
+                                     const hwyblas_int* k, const double* a,
+                                     const hwyblas_int* lda, const double* b,
+                                     const hwyblas_int* ldb,
+                                     const hwyblas_int* n,
+                                     const hwyblas_int* cols, double* out,
+                                     const hwyblas_int* ldo);
+
 /* Stream for subsequent calls of the calling thread (a cudaStream_t; NULL
  * restores the library's per-thread stream). No counterpart in the
  * reference, which has no device. */
