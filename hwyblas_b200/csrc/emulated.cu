@@ -548,7 +548,7 @@ bool LaunchOzaki(const CUtensorMap& ma, const CUtensorMap& mb,
 // k-block bytes of each pass: the stage of the slices it loads must leave
 // room for at least two stages (KB = 32 for the 8-slice pass: 64 KB).
 constexpr int KbSingle(int S) { return S <= 2 ? 128 : 64; }
-constexpr int kKbHigh = 32, kKbLow = 32;
+constexpr int kKbHigh = 32, kKbLow = 64;
 
 // One slice-product pass: the maps cover `slices` slices of op(A) / op(B)
 // with k blocks of `kb` bytes.

@@ -125,6 +125,82 @@ __global__ void LaswpKernel(int n, T* a, long long lda, int i1, int i2,
   }
 }
 
+// LASWP for incx = 1 and at most 64 interchanges: the interchanges only move
+// data among the rows k1..k2 and their partners, so their net effect is one
+// permutation of at most 128 rows. Warp 0 of every block replays the
+// interchanges on a table of (row, row whose data it holds) in shared memory;
+// then the block's threads gather the permuted rows of their 32 columns in
+// one parallel pass (the values moved, and so the result, are the same).
+constexpr int kSwapMax = 64;
+template <typename T>
+__global__ void __launch_bounds__(256)
+    LaswpPermKernel(int n, T* a, long long lda, int k1, int k2,
+                    const int* ipiv, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ int pos[2 * kSwapMax], src[2 * kSwapMax], piv[kSwapMax];
+  __shared__ int cnt;
+  __shared__ T tile[2 * kSwapMax][33];
+  const int nb = k2 - k1 + 1;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int t = lane; t < nb; t += 32) {
+      pos[t] = k1 + t;
+      src[t] = k1 + t;
+      piv[t] = ipiv[k1 - 1 + t];
+    }
+    int c = nb;
+    __syncwarp();
+    for (int i = k1; i <= k2; ++i) {
+      const int p = piv[i - k1];
+      if (p == i) continue;
+      int sp;
+      if (p >= k1 && p <= k2) {
+        sp = p - k1;
+      } else {
+        // Partner outside k1..k2: find it among the extra slots, or add it.
+        sp = -1;
+        for (int t0 = nb; t0 < c; t0 += 32) {
+          const int t = t0 + lane;
+          const unsigned hit = __ballot_sync(0xffffffffu, t < c && pos[t] == p);
+          if (hit != 0u) {
+            sp = t0 + __ffs(hit) - 1;
+            break;
+          }
+        }
+        if (sp < 0) {
+          sp = c;
+          if (lane == 0) {
+            pos[c] = p;
+            src[c] = p;
+          }
+          ++c;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        const int si = i - k1;
+        const int t = src[si];
+        src[si] = src[sp];
+        src[sp] = t;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) cnt = c;
+  }
+  __syncthreads();
+  const int c = cnt;
+  const int col0 = blockIdx.x * 32;
+  for (int idx = threadIdx.x; idx < c * 32; idx += blockDim.x) {
+    const int t = idx / 32, cc = idx % 32;
+    if (col0 + cc < n) tile[t][cc] = a[(src[t] - 1) + (col0 + cc) * lda];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < c * 32; idx += blockDim.x) {
+    const int t = idx / 32, cc = idx % 32;
+    if (col0 + cc < n) a[(pos[t] - 1) + (col0 + cc) * lda] = tile[t][cc];
+  }
+}
+
 __global__ void AdjustPivotsKernel(int* ipiv, int begin, int end, int delta) {
   const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
   if (i < end) ipiv[i] += delta;
@@ -138,6 +214,7 @@ __global__ void AdjustPivotsKernel(int* ipiv, int begin, int end, int delta) {
 // applies the swap, the scaling and the rank-1 update to its own rows.
 constexpr int kLeafThreads = 512;
 constexpr int kLeafMaxRows = 1024;  // rows per CTA
+constexpr int kLeafMaxP = 64;       // CTAs per panel (m <= 65536)
 constexpr int kLeafW = 16;
 
 template <typename T>
@@ -148,8 +225,8 @@ struct LeafArgs {
   int* ipiv;
   int* info;
   int info_base;
-  T* xchg;                // [2][P][kLeafW + 2] candidates, [2][kLeafW] row j
-  unsigned int* barrier;  // zeroed before launch
+  T* xchg;                // [2][P][2 kLeafW + 2] candidate slots
+  unsigned int* tags;     // [2][P] slot tags, zeroed before launch
   int* timeout_flag;
 };
 
@@ -159,22 +236,23 @@ __global__ void __launch_bounds__(kLeafThreads)
   extern __shared__ __align__(16) uint8_t leaf_smem[];
   T* sp = reinterpret_cast<T*>(leaf_smem);  // column-major [w][R]
   __shared__ T s_piv[kLeafW], s_rowj[kLeafW];
+  __shared__ T s_cand[kLeafMaxP * (2 * kLeafW + 2)];
   __shared__ T s_wv[kLeafThreads / 32];
   __shared__ int s_wi[kLeafThreads / 32];
-  __shared__ int s_p;
+  __shared__ int s_p, s_abort;
   const int P = gridDim.x, cta = blockIdx.x;
   const int rows_per = (p.m + P - 1) / P;
   const int r0 = cta * rows_per, r1 = min(p.m, r0 + rows_per);
   const int R = rows_per;
   const int w = p.w;
-  const int slot_len = kLeafW + 2;
-  T* cand = p.xchg;                       // [2][P][slot_len]
-  T* rowj_buf = p.xchg + 2 * P * slot_len;  // [2][kLeafW]
+  const int slot_len = 2 * kLeafW + 2;
+  T* cand = p.xchg;  // [2][P][slot_len]
+  unsigned int* tags = p.tags;
 
-  for (int idx = threadIdx.x; idx < w * R; idx += blockDim.x) {
-    const int c = idx / R, lr = idx % R;
-    if (r0 + lr < r1) sp[c * R + lr] = p.a[(r0 + lr) + c * p.lda];
-  }
+  if (threadIdx.x == 0) s_abort = 0;
+  for (int c = 0; c < w; ++c)
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x)
+      sp[c * R + lr] = p.a[(r0 + lr) + c * p.lda];
   __syncthreads();
 
   for (int j = 0; j < w; ++j) {
@@ -202,10 +280,27 @@ __global__ void __launch_bounds__(kLeafThreads)
       s_wv[0] = bv;
     }
     __syncthreads();
-    // (b) publish the candidate row and, by its owner, row j.
-    {
+    // (b) exchange the candidates. A CTA holding the whole panel keeps them in
+    // shared memory. Otherwise every CTA writes its slot for this step's
+    // parity (|a|, row, row contents, and row j if it owns it), fences and
+    // release-stores the step number as the slot's tag; each CTA polls the P
+    // tags (one thread per slot, bounded) and copies all slots in one parallel
+    // round trip. A CTA can only overwrite a parity after every CTA has
+    // published the next step, i.e. after all have read this one.
+    const int ci = s_p;
+    if (P == 1) {
+      if (threadIdx.x == 0) {
+        s_cand[0] = s_wv[0];
+        s_cand[1] = static_cast<T>(ci == 0x7fffffff ? -1 : ci);
+      }
+      if (threadIdx.x < w) {
+        s_cand[2 + threadIdx.x] =
+            (ci != 0x7fffffff) ? sp[threadIdx.x * R + ci] : T(0);
+        s_rowj[threadIdx.x] = sp[threadIdx.x * R + j];
+      }
+      __syncthreads();
+    } else {
       T* slot = cand + (par * P + cta) * slot_len;
-      const int ci = s_p;
       if (threadIdx.x == 0) {
         slot[0] = s_wv[0];
         slot[1] = static_cast<T>(ci == 0x7fffffff ? -1 : ci);
@@ -214,46 +309,76 @@ __global__ void __launch_bounds__(kLeafThreads)
         slot[2 + threadIdx.x] =
             (ci != 0x7fffffff) ? sp[threadIdx.x * R + (ci - r0)] : T(0);
         if (j >= r0 && j < r1)
-          rowj_buf[par * kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
+          slot[2 + kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
       }
-    }
-    if (P > 1) {
-      if (!GridBarrier(p.barrier, P, j + 1, p.timeout_flag)) return;
-    } else {
       __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(tags + par * P + cta),
+                     "r"(static_cast<unsigned>(j + 1))
+                     : "memory");
+      }
+      if (threadIdx.x < P) {
+        uint32_t polls = 0;
+        while (true) {
+          unsigned v;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                       : "=r"(v)
+                       : "l"(tags + par * P + threadIdx.x)
+                       : "memory");
+          if (v >= static_cast<unsigned>(j + 1)) break;
+          if (++polls >= kMaxPolls) {
+            atomicExch(p.timeout_flag, 1);
+            s_abort = 1;
+            break;
+          }
+        }
+      }
+      __syncthreads();
+      if (s_abort) return;
+      for (int idx = threadIdx.x; idx < P * slot_len; idx += blockDim.x)
+        s_cand[idx] = *(volatile const T*)&cand[par * P * slot_len + idx];
+      __syncthreads();
+      if (threadIdx.x < w)
+        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + kLeafW + threadIdx.x];
     }
-    // (c) the global pivot: the reference's IAMAX over rows j..m-1.
-    if (threadIdx.x == 0) {
+    // (c) the global pivot: the reference's IAMAX over rows j..m-1; warp 0
+    // picks the winner among the candidates.
+    __syncthreads();
+    if (threadIdx.x < 32) {
       T gv = T(-1);
       int gi = 0x7fffffff;
-      for (int q = 0; q < P; ++q) {
-        const T* slot = cand + (par * P + q) * slot_len;
-        const T v = *(volatile const T*)&slot[0];
-        const T fi = *(volatile const T*)&slot[1];
+      for (int q = threadIdx.x; q < P; q += 32) {
+        const T fi = s_cand[q * slot_len + 1];
         if (fi < T(0)) continue;
+        const T v = s_cand[q * slot_len];
         const int i = static_cast<int>(fi);
         if (Better(v, i, gv, gi)) { gv = v; gi = i; }
       }
-      const T ajj = *(volatile const T*)&rowj_buf[par * kLeafW + j];
-      if (isnan(fabs(ajj)) || gi == 0x7fffffff) gi = j;
-      s_p = gi;
+      int wq = (gi == 0x7fffffff) ? -1 : static_cast<int>(threadIdx.x);
+      for (int off = 16; off > 0; off >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, gv, off);
+        const int oi = __shfl_down_sync(0xffffffffu, gi, off);
+        const int oq = __shfl_down_sync(0xffffffffu, wq, off);
+        if (Better(ov, oi, gv, gi)) { gv = ov; gi = oi; wq = oq; }
+      }
+      if (threadIdx.x == 0) {
+        const T ajj = s_rowj[j];
+        if (isnan(fabs(ajj)) || gi == 0x7fffffff) gi = j;
+        s_p = gi;
+      }
     }
     __syncthreads();
     const int piv = s_p;
     if (threadIdx.x < w) {
-      const T rj = *(volatile const T*)&rowj_buf[par * kLeafW + threadIdx.x];
-      s_rowj[threadIdx.x] = rj;
       if (piv == j) {
-        s_piv[threadIdx.x] = rj;
+        s_piv[threadIdx.x] = s_rowj[threadIdx.x];
       } else {
         // The winner's slot holds row piv.
         T val = T(0);
         for (int q = 0; q < P; ++q) {
-          const T* slot = cand + (par * P + q) * slot_len;
-          if (static_cast<int>(*(volatile const T*)&slot[1]) == piv &&
-              *(volatile const T*)&slot[1] >= T(0)) {
-            val = *(volatile const T*)&slot[2 + threadIdx.x];
-          }
+          const T fi = s_cand[q * slot_len + 1];
+          if (fi >= T(0) && static_cast<int>(fi) == piv) val = s_cand[q * slot_len + 2 + threadIdx.x];
         }
         s_piv[threadIdx.x] = val;
       }
@@ -282,19 +407,19 @@ __global__ void __launch_bounds__(kLeafThreads)
     }
     __syncthreads();
     // (f) rank-1 update of columns j+1..w-1 (AXPY with alpha = -a(j, k)).
+    // Each thread owns rows; the column loop carries no index arithmetic.
     const int len = p.m - j - 1;
-    for (int idx = threadIdx.x; idx < (w - j - 1) * (r1 - r0); idx += blockDim.x) {
-      const int k = j + 1 + idx / (r1 - r0), lr = idx % (r1 - r0);
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
       if (r0 + lr <= j) continue;
-      const T alpha = -s_piv[k];
-      sp[k * R + lr] = Axpy(sp[k * R + lr], alpha, sp[j * R + lr], len, p.lanes);
+      const T x = sp[j * R + lr];
+      for (int k = j + 1; k < w; ++k)
+        sp[k * R + lr] = Axpy(sp[k * R + lr], -s_piv[k], x, len, p.lanes);
     }
     __syncthreads();
   }
-  for (int idx = threadIdx.x; idx < w * R; idx += blockDim.x) {
-    const int c = idx / R, lr = idx % R;
-    if (r0 + lr < r1) p.a[(r0 + lr) + c * p.lda] = sp[c * R + lr];
-  }
+  for (int c = 0; c < w; ++c)
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x)
+      p.a[(r0 + lr) + c * p.lda] = sp[c * R + lr];
 }
 
 // LU leaf, trailing columns (n > m, m <= 16). In the reference, step j swaps
@@ -417,6 +542,13 @@ void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
     ix0 = k1 + (k1 - k2) * incx; i1 = k2; i2 = k1; inc = -1;
   }
   if (inc > 0 ? i1 > i2 : i1 < i2) return;
+  if (incx == 1 && k2 - k1 + 1 <= kSwapMax) {
+    LaswpPermKernel<T><<<(n + 31) / 32, 256, 0, Ctx().stream>>>(
+        n, a, lda, k1, k2, ipiv, Ctx().guard);
+    CountLaunch();
+    LaunchFailed("laswp");
+    return;
+  }
   LaswpKernel<T><<<(n + 127) / 128, 128, 0, Ctx().stream>>>(
       n, a, lda, i1, i2, inc, ix0, incx, ipiv, Ctx().guard);
   CountLaunch();
@@ -441,6 +573,12 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
   const int lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
   const int P = (m + kLeafMaxRows - 1) / kLeafMaxRows;
   const int R = (m + P - 1) / P;
+  if (P > kLeafMaxP) {
+    fprintf(stderr, "hwyblas_b200: LU panel of %d rows exceeds %d\n", m,
+            kLeafMaxP * kLeafMaxRows);
+    Failed(cudaErrorInvalidValue, "getrf leaf size");
+    return;
+  }
   const size_t smem = static_cast<size_t>(w) * R * sizeof(T);
   static bool configured = false;
   if (!configured) {
@@ -458,12 +596,14 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
   args.ipiv = ipiv;
   args.info = info;
   args.info_base = info_base;
+  const size_t slot_bytes = sizeof(T) * 2 * P * (2 * kLeafW + 2);
   args.xchg = static_cast<T*>(
-      Workspace(kWsLeaf, sizeof(T) * (2 * P * (kLeafW + 2) + 2 * kLeafW)));
-  args.barrier = reinterpret_cast<unsigned int*>(ctx.dev_status + 16);
+      Workspace(kWsLeaf, slot_bytes + sizeof(unsigned int) * 2 * kLeafMaxP));
+  args.tags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(args.xchg) +
+                                              slot_bytes);
   args.timeout_flag = ctx.dev_status;
   if (P > 1) {
-    cudaMemsetAsync(args.barrier, 0, sizeof(unsigned int), ctx.stream);
+    cudaMemsetAsync(args.tags, 0, sizeof(unsigned int) * 2 * P, ctx.stream);
     void* kargs[] = {&args};
     Failed(cudaLaunchCooperativeKernel(
                reinterpret_cast<void*>(GetrfLeafPanelKernel<T>), P,

@@ -15,7 +15,7 @@
 // the accumulator every 256 reproduces the reference bit for bit.
 //
 // Tiling: a CTA computes a 128 x 64 tile of C with 8 consumer warps (32 x 32
-// each: 2 x 4 MMAs per k8 step) and one producer warp that streams 16-deep k
+// each: 2 x 4 MMAs per k8 step); lane 0 of warp 0 also streams 16-deep k
 // slices of op(A) (eight 16 x 16 boxes, M-contiguous) and op(B) (16 x 64,
 // K-contiguous) into a 4-stage shared-memory ring with TMA (128-byte swizzle:
 // the 16-byte chunk c of row r lands at chunk c ^ (r & 7)) and mbarriers.
@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kBM = 128, kBN = 64, kBK = 16, kStages = 4;
 constexpr int kConsumerWarps = 8;
-constexpr int kThreads = (kConsumerWarps + 1) * 32;
+constexpr int kThreads = kConsumerWarps * 32;
 constexpr int kTileABytes = kBM * kBK * 8;  // 8 boxes of 16 (m) x 16 (k)
 constexpr int kABoxBytes = 16 * kBK * 8;
 constexpr int kTileBBytes = kBN * kBK * 8;
@@ -79,6 +79,26 @@ __device__ __forceinline__ bool InPart(const GemmParams& p, int i, int j) {
   return true;
 }
 
+// Tile `tile` in groups of 16 tile rows: consecutive tiles walk down a band
+// of 16 tile rows column by column, so the tiles in flight at once form a
+// compact block of C and share their A and B tiles in L2.
+__device__ __forceinline__ void TileOrigin(int tile, int tiles_m, int tiles_n,
+                                           int* m0, int* n0) {
+  const int per_group = 16 * tiles_n;
+  const int first_m = (tile / per_group) * 16;
+  const int gm = min(tiles_m - first_m, 16);
+  const int in_group = tile % per_group;
+  *m0 = (first_m + in_group % gm) * kBM;
+  *n0 = (in_group / gm) * kBN;
+}
+
+// Tiles entirely outside a triangular C part are skipped.
+__device__ __forceinline__ bool SkipTile(const GemmParams& p, int m0, int n0) {
+  if (p.part == kLower && m0 + kBM - 1 < n0) return true;
+  if (p.part == kUpper && m0 > n0 + kBN - 1) return true;
+  return false;
+}
+
 __device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
                                      double b0, double b1) {
   asm volatile(
@@ -88,22 +108,53 @@ __device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
 }
 
+// Producer cursor: lane 0 of warp 0 issues the TMA loads of the CTA's
+// k-slices in order (across tile boundaries), kStages - 1 slices ahead of
+// the consumers.
+struct Producer {
+  int tile, kt, gs;
+};
+
+__device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
+                                          int tiles_m, int tiles_n, int kt_total,
+                                          uint8_t* smem, uint64_t* full,
+                                          uint64_t* empty, const CUtensorMap* tm_a,
+                                          const CUtensorMap* tm_b) {
+  const int num_tiles = tiles_m * tiles_n;
+  int m0 = 0, n0 = 0;
+  while (pr.tile < num_tiles) {
+    TileOrigin(pr.tile, tiles_m, tiles_n, &m0, &n0);
+    if (!SkipTile(p, m0, n0)) break;
+    pr.tile += gridDim.x;
+  }
+  if (pr.tile >= num_tiles) return true;
+  const int s = pr.gs % kStages, round = pr.gs / kStages;
+  if (round > 0 && !MbarWait(&empty[s], (round - 1) & 1, p.timeout_flag)) return false;
+  uint8_t* st = smem + s * kStageBytes;
+  MbarArriveExpectTx(&full[s], kStageBytes);
+#pragma unroll
+  for (int b = 0; b < kBM / 16; ++b)
+    TmaLoad2d(st + b * kABoxBytes, tm_a, m0 + 16 * b, pr.kt * kBK, &full[s]);
+  TmaLoad2d(st + kTileABytes, tm_b, pr.kt * kBK, n0, &full[s]);
+  ++pr.gs;
+  if (++pr.kt == kt_total) {
+    pr.kt = 0;
+    pr.tile += gridDim.x;
+  }
+  return true;
+}
+
 template <bool kMulti>
 __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
   if (p.guard != nullptr && *p.guard != 0) return;
-  // Tiles in groups of 16 tile rows, so that a wave of CTAs covers a compact
-  // block of C and shares its A and B tiles in L2.
+  // Persistent: CTA b computes tiles b, b + gridDim.x, ... Lane 0 of warp 0
+  // streams the k-slices across tile boundaries (the stage counter gs runs
+  // over all of the CTA's k-slices), so the next tile's loads overlap this
+  // tile's epilogue.
   const int tiles_m = (p.m + kBM - 1) / kBM, tiles_n = (p.n + kBN - 1) / kBN;
-  const int per_group = 16 * tiles_n;
-  const int first_m = (static_cast<int>(blockIdx.x) / per_group) * 16;
-  const int gm = min(tiles_m - first_m, 16);
-  const int in_group = static_cast<int>(blockIdx.x) % per_group;
-  const int m0 = (first_m + in_group % gm) * kBM;
-  const int n0 = (in_group / gm) * kBN;
-  if (p.part == kLower && m0 + kBM - 1 < n0) return;
-  if (p.part == kUpper && m0 > n0 + kBN - 1) return;
+  const int num_tiles = tiles_m * tiles_n;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024 - (SmemAddr(smem_raw) & 1023)) & 1023);
@@ -119,26 +170,15 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
   }
   __syncthreads();
   const int kt_total = (p.k + kBK - 1) / kBK;
-
-  if (warp == kConsumerWarps) {
-    // Producer warp: one lane streams the k-slices through the ring.
-    if (lane == 0) {
-      PrefetchTmap(&tm_a);
-      PrefetchTmap(&tm_b);
-      for (int kt = 0; kt < kt_total; ++kt) {
-        const int s = kt % kStages, round = kt / kStages;
-        if (round > 0 && !MbarWait(&empty[s], (round - 1) & 1, p.timeout_flag))
-          break;
-        uint8_t* st = smem + s * kStageBytes;
-        MbarArriveExpectTx(&full[s], kStageBytes);
-#pragma unroll
-        for (int b = 0; b < kBM / 16; ++b)
-          TmaLoad2d(st + b * kABoxBytes, &tm_a, m0 + 16 * b, kt * kBK, &full[s]);
-        TmaLoad2d(st + kTileABytes, &tm_b, kt * kBK, n0, &full[s]);
-      }
-    }
-    return;
+  const bool producer = (warp == 0 && lane == 0);
+  Producer pr{static_cast<int>(blockIdx.x), 0, 0};
+  if (producer) {
+    PrefetchTmap(&tm_a);
+    PrefetchTmap(&tm_b);
+    for (int i = 0; i < kStages - 1; ++i)
+      IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty, &tm_a, &tm_b);
   }
+  __syncwarp();
 
   const int wm = warp % 4, wn = warp / 4;
   const int g = lane >> 2, t = lane & 3;
@@ -148,6 +188,11 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
   const int ccol0 = 2 * ((2 * t) & 3) + ((2 * t) >> 2);
   const int ccol1 = 2 * ((2 * t + 1) & 3) + ((2 * t + 1) >> 2);
   const int bcol = 2 * (g & 3) + (g >> 2);  // tile column of this lane's B
+  int gs = 0;
+  for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+  int m0, n0;
+  TileOrigin(tile, tiles_m, tiles_n, &m0, &n0);
+  if (SkipTile(p, m0, n0)) continue;
   // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
   // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
   const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
@@ -174,8 +219,8 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
         }
       }
 
-  for (int kt = 0; kt < kt_total; ++kt) {
-    const int s = kt % kStages, round = kt / kStages;
+  for (int kt = 0; kt < kt_total; ++kt, ++gs) {
+    const int s = gs % kStages, round = gs / kStages;
     if (!MbarWait(&full[s], round & 1, p.timeout_flag)) return;
     const double* sa = reinterpret_cast<const double*>(smem + s * kStageBytes);
     const uint8_t* sb = smem + s * kStageBytes + kTileABytes;
@@ -210,6 +255,9 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
     }
     __syncwarp();
     if (lane == 0) MbarArrive(&empty[s]);
+    if (producer)
+      IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty, &tm_a, &tm_b);
+    __syncwarp();
 
     if constexpr (kMulti) {
       // End of a reference KC chunk: merge into the running C value.
@@ -272,6 +320,87 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
         }
         p.c[i + j * p.ldc] = v;
       }
+  }  // tile loop
+}
+
+// Small products: one thread per C element, the same FMA chain over k in
+// chunks of 256 and the same merges as the tensor-core kernel (so the same
+// bits), without its TMA pipeline whose fixed costs dominate tiny shapes.
+__global__ void __launch_bounds__(256)
+    DgemmDirectKernel(GemmParams p, View<double> a, View<double> b) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  const int i = blockIdx.x * 32 + threadIdx.x % 32;
+  const int j = blockIdx.y * 8 + threadIdx.x / 32;
+  if (!InPart(p, i, j)) return;
+  const bool crossing = p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j);
+  double cv = 0.0;
+  for (int pc = 0; pc < p.k; pc += 256) {
+    const int pe = min(p.k, pc + 256);
+    double acc = 0.0;
+    for (int q = pc; q < pe; ++q) acc = fma(a.data[i * a.rs + q * a.cs],
+                                            b.data[q * b.rs + j * b.cs], acc);
+    const double r = p.alpha * acc;
+    if (pc != 0 || p.beta == 1.0) {
+      if (pc == 0) cv = p.c[i + j * p.ldc];
+      cv = r + cv;
+    } else if (p.beta == 0.0) {
+      cv = r;
+    } else {
+      const double cin = p.c[i + j * p.ldc];
+      if (crossing) {
+        const double bc = p.beta * cin;
+        cv = r + bc;
+      } else {
+        cv = fma(cin, p.beta, r);
+      }
+    }
+  }
+  p.c[i + j * p.ldc] = cv;
+}
+
+// As DgemmDirectKernel for k > 256: each 256-wide chunk's FMA chain is
+// independent, so tpe threads (a power of two >= the chunk count) compute
+// one element's chunks in parallel and the first of them merges the chunk
+// sums in order.
+__global__ void __launch_bounds__(256)
+    DgemmDirectChunkKernel(GemmParams p, View<double> a, View<double> b, int tpe) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  __shared__ double part[256];
+  const int epb = 256 / tpe;
+  const int e = threadIdx.x / tpe, ch = threadIdx.x % tpe;
+  const long long elem = static_cast<long long>(blockIdx.x) * epb + e;
+  const int i = static_cast<int>(elem % p.m), j = static_cast<int>(elem / p.m);
+  const int nc = (p.k + 255) / 256;
+  const bool valid = elem < static_cast<long long>(p.m) * p.n;
+  double acc = 0.0;
+  if (valid && ch < nc) {
+    const int pe = min(p.k, ch * 256 + 256);
+    for (int q = ch * 256; q < pe; ++q)
+      acc = fma(a.data[i * a.rs + q * a.cs], b.data[q * b.rs + j * b.cs], acc);
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (!valid || ch != 0 || !InPart(p, i, j)) return;
+  const bool crossing = p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j);
+  double cv = 0.0;
+  for (int c = 0; c < nc; ++c) {
+    const double r = p.alpha * part[threadIdx.x + c];
+    if (c != 0 || p.beta == 1.0) {
+      if (c == 0) cv = p.c[i + j * p.ldc];
+      cv = r + cv;
+    } else if (p.beta == 0.0) {
+      cv = r;
+    } else {
+      const double cin = p.c[i + j * p.ldc];
+      if (crossing) {
+        const double bc = p.beta * cin;
+        cv = r + bc;
+      } else {
+        cv = fma(cin, p.beta, r);
+      }
+    }
+  }
+  p.c[i + j * p.ldc] = cv;
 }
 
 // Copies op(X) (rows x cols, strided view) into a dense column-major buffer
@@ -393,6 +522,38 @@ template const float* Canonical(View<float>, int, int, int, long long*);
 void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
            double beta, double* c, int ldc, Part part) {
   Context& ctx = Ctx();
+  if (static_cast<long long>(m) * n * k <= (1LL << 22) || m < 32 || n < 32) {
+    GemmParams p;
+    p.m = m;
+    p.n = n;
+    p.k = k;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.c = c;
+    p.ldc = ldc;
+    p.part = part;
+    p.timeout_flag = ctx.dev_status;
+    p.guard = ctx.guard;
+    const int nc = (k + 255) / 256;
+    if (nc == 1) {
+      const dim3 grid((m + 31) / 32, (n + 7) / 8);
+      DgemmDirectKernel<<<grid, 256, 0, ctx.stream>>>(p, a, b);
+      CountLaunch();
+      LaunchFailed("dgemm direct");
+      return;
+    }
+    if (nc <= 256) {
+      int tpe = 1;
+      while (tpe < nc) tpe *= 2;
+      const long long elems = static_cast<long long>(m) * n;
+      const long long blocks = (elems + (256 / tpe) - 1) / (256 / tpe);
+      DgemmDirectChunkKernel<<<static_cast<unsigned>(blocks), 256, 0, ctx.stream>>>(
+          p, a, b, tpe);
+      CountLaunch();
+      LaunchFailed("dgemm direct chunks");
+      return;
+    }
+  }
   long long lda, ldb;
   const double* ca = Canonical(a, m, k, kWsPackA, &lda);
   const double* cb = Canonical(b, k, n, kWsPackB, &ldb);
@@ -418,19 +579,35 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const long long tiles =
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
+  static int resident_multi = 1, resident_single = 1;
   if (!configured) {
     cudaFuncSetAttribute(DgemmDmmaKernel<true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     cudaFuncSetAttribute(DgemmDmmaKernel<false>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident_multi, DgemmDmmaKernel<true>,
+                                                  kThreads, kSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident_single, DgemmDmmaKernel<false>,
+                                                  kThreads, kSmemBytes);
+    resident_multi = std::max(resident_multi, 1);
+    resident_single = std::max(resident_single, 1);
     configured = true;
   }
-  if (k > 256) {
-    DgemmDmmaKernel<true><<<static_cast<unsigned>(tiles), kThreads, kSmemBytes,
-                            ctx.stream>>>(ma, mb, p);
+  // Persistent grid: at most one wave of resident CTAs. Short K (the LU and
+  // Cholesky trailing updates, K = 64) runs the variant that prefetches C
+  // into registers at the start of each tile, so the C loads overlap the
+  // tile's MMAs instead of stalling the epilogue; it needs ~200 registers a
+  // thread (one CTA per SM). Long K runs the lean variant at two CTAs per SM
+  // (measured at n = 8192: 31.1 vs 27.4 TFLOP/s; getrf n = 16384: 480 vs
+  // 440 ms the other way round).
+  const bool multi = k <= 512;
+  const long long wave =
+      static_cast<long long>(ctx.num_sms) * (multi ? resident_multi : resident_single);
+  const unsigned grid = static_cast<unsigned>(std::min(tiles, wave));
+  if (multi) {
+    DgemmDmmaKernel<true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   } else {
-    DgemmDmmaKernel<false><<<static_cast<unsigned>(tiles), kThreads, kSmemBytes,
-                             ctx.stream>>>(ma, mb, p);
+    DgemmDmmaKernel<false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   }
   CountLaunch();
   LaunchFailed("dgemm");
