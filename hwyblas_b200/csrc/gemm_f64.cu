@@ -15,7 +15,7 @@
 // the accumulator every 256 reproduces the reference bit for bit.
 //
 // Tiling: a CTA computes a 128 x 64 tile of C with 8 consumer warps (32 x 32
-// each: 2 x 4 MMAs per k8 step); lane 0 of warp 0 also streams 16-deep k
+// each: 2 x 4 MMAs per k8 step) and one producer warp that streams 16-deep k
 // slices of op(A) (eight 16 x 16 boxes, M-contiguous) and op(B) (16 x 64,
 // K-contiguous) into a 4-stage shared-memory ring with TMA (128-byte swizzle:
 // the 16-byte chunk c of row r lands at chunk c ^ (r & 7)) and mbarriers.
@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kBM = 128, kBN = 64, kBK = 16, kStages = 4;
 constexpr int kConsumerWarps = 8;
-constexpr int kThreads = kConsumerWarps * 32;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
 constexpr int kTileABytes = kBM * kBK * 8;  // 8 boxes of 16 (m) x 16 (k)
 constexpr int kABoxBytes = 16 * kBK * 8;
 constexpr int kTileBBytes = kBN * kBK * 8;
@@ -108,9 +108,8 @@ __device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
 }
 
-// Producer cursor: lane 0 of warp 0 issues the TMA loads of the CTA's
-// k-slices in order (across tile boundaries), kStages - 1 slices ahead of
-// the consumers.
+// Producer cursor: the TMA loads of the CTA's k-slices in order, across
+// tile boundaries.
 struct Producer {
   int tile, kt, gs;
 };
@@ -144,12 +143,13 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
   return true;
 }
 
-template <bool kMulti>
-__global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
+// 168 registers: nine warps of a CTA share the 16K registers of each SM
+// sub-partition three at a time.
+__global__ void __maxnreg__(168)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
   if (p.guard != nullptr && *p.guard != 0) return;
-  // Persistent: CTA b computes tiles b, b + gridDim.x, ... Lane 0 of warp 0
+  // Persistent: CTA b computes tiles b, b + gridDim.x, ... The producer
   // streams the k-slices across tile boundaries (the stage counter gs runs
   // over all of the CTA's k-slices), so the next tile's loads overlap this
   // tile's epilogue.
@@ -170,15 +170,20 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
   }
   __syncthreads();
   const int kt_total = (p.k + kBK - 1) / kBK;
-  const bool producer = (warp == 0 && lane == 0);
-  Producer pr{static_cast<int>(blockIdx.x), 0, 0};
-  if (producer) {
-    PrefetchTmap(&tm_a);
-    PrefetchTmap(&tm_b);
-    for (int i = 0; i < kStages - 1; ++i)
-      IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty, &tm_a, &tm_b);
+  if (warp == kConsumerWarps) {
+    // Producer warp: one lane streams the k-slices through the ring.
+    if (lane == 0) {
+      PrefetchTmap(&tm_a);
+      PrefetchTmap(&tm_b);
+      Producer pr{static_cast<int>(blockIdx.x), 0, 0};
+      while (pr.tile < num_tiles) {
+        if (!IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
+                       &tm_a, &tm_b))
+          return;
+      }
+    }
+    return;
   }
-  __syncwarp();
 
   const int wm = warp % 4, wn = warp / 4;
   const int g = lane >> 2, t = lane & 3;
@@ -190,76 +195,71 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
   const int bcol = 2 * (g & 3) + (g >> 2);  // tile column of this lane's B
   int gs = 0;
   for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
-  int m0, n0;
-  TileOrigin(tile, tiles_m, tiles_n, &m0, &n0);
-  if (SkipTile(p, m0, n0)) continue;
-  // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
-  // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
-  const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
-  double acc[2][4][4];
-  double cacc[2][4][4];  // kMulti: C_in, then the running merged value
-  uint32_t in_part = 0, crossing = 0;
+    int m0, n0;
+    TileOrigin(tile, tiles_m, tiles_n, &m0, &n0);
+    if (SkipTile(p, m0, n0)) continue;
+    // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
+    // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
+    const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
+    double acc[2][4][4];
+    // C_in, loaded before the MMAs so that the loads overlap them, then the
+    // running value merged at the end of every 256-deep chunk.
+    double cacc[2][4][4];
+    uint32_t in_part = 0, crossing = 0;
 #pragma unroll
-  for (int mb = 0; mb < 2; ++mb)
+    for (int mb = 0; mb < 2; ++mb)
 #pragma unroll
-    for (int nb = 0; nb < 4; ++nb)
+      for (int nb = 0; nb < 4; ++nb)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int bit = (mb * 4 + nb) * 4 + e;
-        const int i = row0 + mb * 16 + (e >> 1);
-        const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
-        acc[mb][nb][e] = 0.0;
-        const bool inside = InPart(p, i, j);
-        if (inside) in_part |= 1u << bit;
-        if (inside && p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j))
-          crossing |= 1u << bit;
-        if constexpr (kMulti) {
-          cacc[mb][nb][e] =
-              (inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
+        for (int e = 0; e < 4; ++e) {
+          const int bit = (mb * 4 + nb) * 4 + e;
+          const int i = row0 + mb * 16 + (e >> 1);
+          const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
+          acc[mb][nb][e] = 0.0;
+          const bool inside = InPart(p, i, j);
+          if (inside) in_part |= 1u << bit;
+          if (inside && p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j))
+            crossing |= 1u << bit;
+          cacc[mb][nb][e] = (inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
+        }
+
+    for (int kt = 0; kt < kt_total; ++kt, ++gs) {
+      const int s = gs % kStages, round = gs / kStages;
+      if (!MbarWait(&full[s], round & 1, p.timeout_flag)) return;
+      const double* sa = reinterpret_cast<const double*>(smem + s * kStageBytes);
+      const uint8_t* sb = smem + s * kStageBytes + kTileABytes;
+#pragma unroll
+      for (int ks = 0; ks < kBK / 8; ++ks) {
+        double af[2][4];
+        const int klo = ks * 8 + t, khi = klo + 4;
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          const uint8_t* box = reinterpret_cast<const uint8_t*>(sa) +
+                               (wm * 2 + mb) * kABoxBytes;
+          const double2 lo = *reinterpret_cast<const double2*>(
+              box + klo * 128 + ((cg ^ (klo & 7)) << 4));
+          const double2 hi = *reinterpret_cast<const double2*>(
+              box + khi * 128 + ((cg ^ (khi & 7)) << 4));
+          af[mb][0] = lo.x;
+          af[mb][1] = lo.y;
+          af[mb][2] = hi.x;
+          af[mb][3] = hi.y;
+        }
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb) {
+          const int r = wn * 32 + nb * 8 + bcol;
+          const int k0 = ks * 8 + t, k1 = k0 + 4;
+          const double b0 = *reinterpret_cast<const double*>(
+              sb + r * 128 + (((k0 >> 1) ^ (r & 7)) << 4) + ((k0 & 1) << 3));
+          const double b1 = *reinterpret_cast<const double*>(
+              sb + r * 128 + (((k1 >> 1) ^ (r & 7)) << 4) + ((k1 & 1) << 3));
+          Dmma(acc[0][nb], af[0], b0, b1);
+          Dmma(acc[1][nb], af[1], b0, b1);
         }
       }
+      __syncwarp();
+      if (lane == 0) MbarArrive(&empty[s]);
 
-  for (int kt = 0; kt < kt_total; ++kt, ++gs) {
-    const int s = gs % kStages, round = gs / kStages;
-    if (!MbarWait(&full[s], round & 1, p.timeout_flag)) return;
-    const double* sa = reinterpret_cast<const double*>(smem + s * kStageBytes);
-    const uint8_t* sb = smem + s * kStageBytes + kTileABytes;
-#pragma unroll
-    for (int ks = 0; ks < kBK / 8; ++ks) {
-      double af[2][4];
-      const int klo = ks * 8 + t, khi = klo + 4;
-#pragma unroll
-      for (int mb = 0; mb < 2; ++mb) {
-        const uint8_t* box = reinterpret_cast<const uint8_t*>(sa) +
-                             (wm * 2 + mb) * kABoxBytes;
-        const double2 lo = *reinterpret_cast<const double2*>(
-            box + klo * 128 + ((cg ^ (klo & 7)) << 4));
-        const double2 hi = *reinterpret_cast<const double2*>(
-            box + khi * 128 + ((cg ^ (khi & 7)) << 4));
-        af[mb][0] = lo.x;
-        af[mb][1] = lo.y;
-        af[mb][2] = hi.x;
-        af[mb][3] = hi.y;
-      }
-#pragma unroll
-      for (int nb = 0; nb < 4; ++nb) {
-        const int r = wn * 32 + nb * 8 + bcol;
-        const int k0 = ks * 8 + t, k1 = k0 + 4;
-        const double b0 = *reinterpret_cast<const double*>(
-            sb + r * 128 + (((k0 >> 1) ^ (r & 7)) << 4) + ((k0 & 1) << 3));
-        const double b1 = *reinterpret_cast<const double*>(
-            sb + r * 128 + (((k1 >> 1) ^ (r & 7)) << 4) + ((k1 & 1) << 3));
-        Dmma(acc[0][nb], af[0], b0, b1);
-        Dmma(acc[1][nb], af[1], b0, b1);
-      }
-    }
-    __syncwarp();
-    if (lane == 0) MbarArrive(&empty[s]);
-    if (producer)
-      IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty, &tm_a, &tm_b);
-    __syncwarp();
-
-    if constexpr (kMulti) {
       // End of a reference KC chunk: merge into the running C value.
       if ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_total) {
         const bool first = (kt < kKtPerChunk);
@@ -286,41 +286,21 @@ __global__ void __launch_bounds__(kThreads, kMulti ? 1 : 2)
             }
       }
     }
-  }
 
-  // Epilogue: write C.
+    // Epilogue: write C.
 #pragma unroll
-  for (int mb = 0; mb < 2; ++mb)
+    for (int mb = 0; mb < 2; ++mb)
 #pragma unroll
-    for (int nb = 0; nb < 4; ++nb)
+      for (int nb = 0; nb < 4; ++nb)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int bit = (mb * 4 + nb) * 4 + e;
-        if (!((in_part >> bit) & 1u)) continue;
-        const int i = row0 + mb * 16 + (e >> 1);
-        const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
-        double v;
-        if constexpr (kMulti) {
-          v = cacc[mb][nb][e];
-        } else {
-          const double r = p.alpha * acc[mb][nb][e];
-          if (p.beta == 0.0) {
-            v = r;
-          } else {
-            const double cin = p.c[i + j * p.ldc];
-            if ((crossing >> bit) & 1u) {
-              const double bc = p.beta * cin;
-              v = r + bc;
-            } else if (p.beta == 1.0) {
-              v = r + cin;
-            } else {
-              v = fma(cin, p.beta, r);
-            }
-          }
+        for (int e = 0; e < 4; ++e) {
+          const int bit = (mb * 4 + nb) * 4 + e;
+          if (!((in_part >> bit) & 1u)) continue;
+          const int i = row0 + mb * 16 + (e >> 1);
+          const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
+          p.c[i + j * p.ldc] = cacc[mb][nb][e];
         }
-        p.c[i + j * p.ldc] = v;
-      }
-  }  // tile loop
+  }
 }
 
 // Small products: one thread per C element, the same FMA chain over k in
@@ -579,36 +559,18 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const long long tiles =
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
-  static int resident_multi = 1, resident_single = 1;
   if (!configured) {
-    cudaFuncSetAttribute(DgemmDmmaKernel<true>,
+    cudaFuncSetAttribute(DgemmDmmaKernel,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaFuncSetAttribute(DgemmDmmaKernel<false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident_multi, DgemmDmmaKernel<true>,
-                                                  kThreads, kSmemBytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident_single, DgemmDmmaKernel<false>,
-                                                  kThreads, kSmemBytes);
-    resident_multi = std::max(resident_multi, 1);
-    resident_single = std::max(resident_single, 1);
     configured = true;
   }
-  // Persistent grid: at most one wave of resident CTAs. Short K (the LU and
-  // Cholesky trailing updates, K = 64) runs the variant that prefetches C
-  // into registers at the start of each tile, so the C loads overlap the
-  // tile's MMAs instead of stalling the epilogue; it needs ~200 registers a
-  // thread (one CTA per SM). Long K runs the lean variant at two CTAs per SM
-  // (measured at n = 8192: 31.1 vs 27.4 TFLOP/s; getrf n = 16384: 480 vs
-  // 440 ms the other way round).
-  const bool multi = k <= 512;
-  const long long wave =
-      static_cast<long long>(ctx.num_sms) * (multi ? resident_multi : resident_single);
-  const unsigned grid = static_cast<unsigned>(std::min(tiles, wave));
-  if (multi) {
-    DgemmDmmaKernel<true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
-  } else {
-    DgemmDmmaKernel<false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
-  }
+  // Persistent grid: one CTA per SM (the accumulators and the prefetched C
+  // take 128 of each thread's registers). Measured against a variant whose
+  // producer is lane 0 of warp 0 (8 warps): dgemm n = 8192 32.9 vs 27.5
+  // TFLOP/s, getrf n = 16384 418 vs 440 ms.
+  const unsigned grid =
+      static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
+  DgemmDmmaKernel<<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   CountLaunch();
   LaunchFailed("dgemm");
 }
