@@ -18,6 +18,7 @@ __all__ = [
     "dgetrf2", "dgetrs", "dgesv", "dpotrf", "dpotrf2", "dpotrs", "dposv",
     "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
+    "idamax_noalloc",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -41,7 +42,7 @@ from ._api import (  # noqa: E402  (needs lib())
     dgemm, sgemm, dtrsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
     dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
     cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
-    dgemm_emulated, dgemm_ddref,
+    dgemm_emulated, dgemm_ddref, idamax_noalloc,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

@@ -45,6 +45,7 @@ PROTOTYPES = {
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),
     "hwyblas_fp64_peak_tflops": (ctypes.c_double, []),
+    "hwyblas_idamax_noalloc": (I, [I, P, I, P, P]),
 }
 
 EXPORTED = sorted(PROTOTYPES)

@@ -147,6 +147,13 @@ def dgemm_ddref(transa, transb, m, k, a, lda, b, ldb, n, cols, out, ldo):
                               _ptr(out), _i(ldo))
 
 
+def idamax_noalloc(n, x, incx, result, stream=None):
+    """1-based index of max |x| into the device int `result`, with no
+    allocation (x and result in device memory); returns the status code."""
+    return lib().hwyblas_idamax_noalloc(int(n), _ptr(x), int(incx), _ptr(result),
+                                        stream)
+
+
 def cblas_dgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
                 ldc):
     lib().cblas_dgemm(layout, transa, transb, m, n, k, alpha, _ptr(a), lda,

@@ -14,6 +14,9 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <mutex>
+
+#include "../../include/hwyblas_b200.h"
 #include "device.cuh"
 #include "internal.h"
 
@@ -632,4 +635,112 @@ void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base) 
   LaunchFailed("potrf leaf");
 }
 
+// ---------------------------------------------------------------------------
+// IDAMAX that allocates nothing (hwyblas_idamax_noalloc).
+//
+// For callers that must not allocate device memory during a call: a
+// cudaMalloc or cudaFree synchronizes the whole device, which stalls work the
+// caller keeps in flight on other streams, and a caller that has handed all
+// free device memory to its own pool has none left to give. This variant
+// runs IamaxKernel with its per-block partial results and its completion
+// ticket in a fixed scratch array that is part of the loaded module, takes
+// the caller's stream, and leaves the 1-based index in device memory.
+//
+// Scratch: one block per kNoAllocSegment elements, the partial (value,
+// index) of at most kNoAllocMaxBlocks blocks, so n <= 1024 * 16384 =
+// 16,777,216 (larger n is rejected). The ticket word must be zero when a call
+// starts: set-up zeroes the array, and the kernel's last block resets the
+// ticket before it returns. All calls on one device share the array, so two
+// calls that overlap in time (different streams without ordering, or two host
+// threads) race on it and give wrong results.
+namespace {
+constexpr int kNoAllocSegment = 16384;
+constexpr int kNoAllocMaxBlocks = 1024;
+constexpr size_t kNoAllocValueBytes = kNoAllocMaxBlocks * sizeof(double);
+constexpr size_t kNoAllocIndexBytes = kNoAllocMaxBlocks * sizeof(int);
+constexpr size_t kNoAllocScratchBytes = 16384;  // values, indices, ticket
+static_assert(kNoAllocValueBytes + kNoAllocIndexBytes + 256 <= kNoAllocScratchBytes,
+              "no-alloc scratch layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Set-up, once per device with that device current: the scratch address and
+// a zeroed array (ordered on `stream` before the first launch).
+cudaError_t NoAllocScratch(int device, cudaStream_t stream, void** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[device] == nullptr) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(ptr, 0, kNoAllocScratchBytes, stream);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = ptr;
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+// Whether a kernel on `device` may read or write p.
+bool DeviceAccessible(const void* p, int device) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (attr.type == cudaMemoryTypeManaged) return true;
+  if (attr.type == cudaMemoryTypeDevice) return attr.device == device;
+  if (attr.type == cudaMemoryTypeHost) return attr.devicePointer != nullptr;
+  return false;
+}
+}  // namespace
+
 }  // namespace hb
+
+extern "C" HWYBLAS_API int hwyblas_idamax_noalloc(int n, const double* x, int incx,
+                                                  int* result, void* stream) {
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (static_cast<long long>(n) >
+      static_cast<long long>(hb::kNoAllocMaxBlocks) * hb::kNoAllocSegment) {
+    fprintf(stderr,
+            "hwyblas_idamax_noalloc: n = %d exceeds the maximum of %d elements "
+            "that its fixed scratch holds\n",
+            n, hb::kNoAllocMaxBlocks * hb::kNoAllocSegment);
+    hb::ReportError("IDAMAX_NOALLOC", 1);
+    return -1;
+  }
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  if (device < 0 || device >= hb::kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  if (!hb::DeviceAccessible(result, device)) {
+    hb::ReportError("IDAMAX_NOALLOC", 4);
+    return -4;
+  }
+  if (n < 1 || incx <= 0) {  // the reference returns 0 (src/level1.cc:383-402)
+    e = cudaMemsetAsync(result, 0, sizeof(int), s);
+    return static_cast<int>(e);
+  }
+  const long long span = static_cast<long long>(n - 1) * incx + 1;
+  if (!hb::DeviceAccessible(x, device) ||
+      !hb::DeviceAccessible(x + (span - 1), device)) {
+    hb::ReportError("IDAMAX_NOALLOC", 2);
+    return -2;
+  }
+  void* scratch = nullptr;
+  e = hb::NoAllocScratch(device, s, &scratch);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  double* values = reinterpret_cast<double*>(base);
+  int* indices = reinterpret_cast<int*>(base + hb::kNoAllocValueBytes);
+  unsigned int* ticket = reinterpret_cast<unsigned int*>(
+      base + hb::kNoAllocValueBytes + hb::kNoAllocIndexBytes);
+  const int blocks = (n + hb::kNoAllocSegment - 1) / hb::kNoAllocSegment;
+  hb::IamaxKernel<double><<<blocks, 1024, 0, s>>>(n, x, incx, values, indices,
+                                                  ticket, result);
+  hb::CountLaunch();
+  return static_cast<int>(cudaGetLastError());
+}

@@ -160,4 +160,7 @@ void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,
 // the context set the timeout flag since the last check. Synchronises.
 bool CheckDeviceStatus(const char* what);
 
+// Reports an invalid argument through the error handler (default: xerbla_).
+void ReportError(const char* routine, int info);
+
 }  // namespace hb

@@ -233,6 +233,27 @@ HWYBLAS_API uint64_t hwyblas_launch_count(void);
  * the reference. */
 HWYBLAS_API double hwyblas_fp64_peak_tflops(void);
 
+/* IDAMAX that allocates no memory: for callers that must not allocate
+ * device memory during a call (a cudaMalloc/cudaFree synchronizes the whole
+ * device and stalls the caller's other streams; a caller that has given all
+ * free device memory to its own pool has none to spare). No counterpart in
+ * the reference; the index is the one idamax_ returns (src/level1.cc:383-402).
+ *   x       device-accessible vector of n elements with stride incx
+ *   result  device-accessible int that receives the 1-based index (0 when
+ *           n < 1 or incx <= 0), stream-ordered: read it after `stream`
+ *   stream  a cudaStream_t (NULL: the legacy default stream)
+ * Returns 0 once the work is enqueued, -1 if n > 16,777,216 (the partial
+ * results of the fixed 16 KB scratch array), -2 / -4 if x / result is not
+ * accessible from the current device (each also reported through the error
+ * handler as IDAMAX_NOALLOC), or a positive cudaError_t.
+ * The scratch is a static array in the library's device code, one per
+ * device. The first call on a device sets it up (looks up its address and
+ * zeroes it on `stream`); make that call before capturing a stream. All
+ * calls on a device share the array: calls that overlap in time (unordered
+ * streams, or several host threads at once) race on it. */
+HWYBLAS_API int hwyblas_idamax_noalloc(int n, const double* x, int incx,
+                                       int* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
