@@ -18,7 +18,7 @@ __all__ = [
     "dgetrf2", "dgetrs", "dgesv", "dpotrf", "dpotrf2", "dpotrs", "dposv",
     "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
-    "idamax_noalloc",
+    "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -42,7 +42,8 @@ from ._api import (  # noqa: E402  (needs lib())
     dgemm, sgemm, dtrsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
     dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
     cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
-    dgemm_emulated, dgemm_ddref, idamax_noalloc,
+    dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
+    set_mixed_slices,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

@@ -41,6 +41,9 @@ PROTOTYPES = {
     # Extensions
     "hwyblas_dgemm_emulated": (I, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI, PI]),
     "hwyblas_dgemm_ddref": (None, [C, C, PI, PI, PI, P, PI, P, PI, PI, P, P, PI]),
+    "hwyblas_dgesv_mixed": (None, [PI, PI, P, PI, P, P, PI, P, PI, PI, PI]),
+    "hwyblas_dposv_mixed": (None, [C, PI, PI, P, PI, P, PI, P, PI, PI, PI]),
+    "hwyblas_set_mixed_slices": (I, [I]),
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),

@@ -147,6 +147,29 @@ def dgemm_ddref(transa, transb, m, k, a, lda, b, ldb, n, cols, out, ldo):
                               _ptr(out), _i(ldo))
 
 
+def dgesv_mixed(n, nrhs, a, lda, ipiv, b, ldb, x, ldx):
+    """Mixed-precision solve (DSGESV semantics). Returns (info, iter)."""
+    info, it = ctypes.c_int(0), ctypes.c_int(0)
+    lib().hwyblas_dgesv_mixed(_i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(ipiv), _ptr(b),
+                              _i(ldb), _ptr(x), _i(ldx), ctypes.byref(it),
+                              ctypes.byref(info))
+    return info.value, it.value
+
+
+def dposv_mixed(uplo, n, nrhs, a, lda, b, ldb, x, ldx):
+    """Mixed-precision Cholesky solve (DSPOSV semantics). Returns (info, iter)."""
+    info, it = ctypes.c_int(0), ctypes.c_int(0)
+    lib().hwyblas_dposv_mixed(_c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(b),
+                              _i(ldb), _ptr(x), _i(ldx), ctypes.byref(it),
+                              ctypes.byref(info))
+    return info.value, it.value
+
+
+def set_mixed_slices(slices):
+    """Slice count of the mixed solvers' trailing updates; returns the old one."""
+    return lib().hwyblas_set_mixed_slices(int(slices))
+
+
 def idamax_noalloc(n, x, incx, result, stream=None):
     """1-based index of max |x| into the device int `result`, with no
     allocation (x and result in device memory); returns the status code."""

@@ -873,6 +873,95 @@ HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
   return used;
 }
 
+// Slice count of the mixed solvers' trailing updates (calling thread).
+static thread_local int t_mixed_slices = 4;
+
+HWYBLAS_API int hwyblas_set_mixed_slices(int slices) {
+  const int prev = t_mixed_slices;
+  if (slices >= 1 && slices <= 8) t_mixed_slices = slices;
+  return prev;
+}
+
+HWYBLAS_API void hwyblas_dgesv_mixed(const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
+                                     double* a, const hwyblas_int* lda_p,
+                                     hwyblas_int* ipiv, const double* b,
+                                     const hwyblas_int* ldb_p, double* x,
+                                     const hwyblas_int* ldx_p, hwyblas_int* iter,
+                                     hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p, ldx = *ldx_p;
+  *info = 0;
+  *iter = 0;
+  if (n < 0) *info = -1;
+  else if (nrhs < 0) *info = -2;
+  else if (lda < std::max(1, n)) *info = -4;
+  else if (ldb < std::max(1, n)) *info = -7;
+  else if (ldx < std::max(1, n)) *info = -9;
+  if (*info != 0) {
+    hb::ReportError("DGESV_MIXED", -*info);
+    return;
+  }
+  if (n == 0) return;
+  hb::Staged<double> sa, sb, sx;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sx.In(x, ldx, n, nrhs, hb::kWsStageX, false)) return;
+  if (!sp.In(ipiv, n, 0, false)) return;
+  int it = 0;
+  const int finfo = hb::DgesvMixed(n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld,
+                                   sx.dev, sx.ld, t_mixed_slices, &it);
+  if (finfo < 0) {
+    hb::Finish("DGESV_MIXED");
+    return;
+  }
+  if (it < 0) sa.Out();  // the FP64 factors, as DSGESV leaves them
+  sp.Out();
+  if (finfo == 0 && nrhs > 0) sx.Out();
+  *iter = it;
+  *info = finfo;
+  hb::Finish("DGESV_MIXED");
+}
+
+HWYBLAS_API void hwyblas_dposv_mixed(const char* uplo, const hwyblas_int* n_p,
+                                     const hwyblas_int* nrhs_p, double* a,
+                                     const hwyblas_int* lda_p, const double* b,
+                                     const hwyblas_int* ldb_p, double* x,
+                                     const hwyblas_int* ldx_p, hwyblas_int* iter,
+                                     hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p, ldx = *ldx_p;
+  const char u = hb::Up(*uplo);
+  const bool upper = (u == 'U');
+  *info = 0;
+  *iter = 0;
+  if (!upper && u != 'L') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -7;
+  else if (ldx < std::max(1, n)) *info = -9;
+  if (*info != 0) {
+    hb::ReportError("DPOSV_MIXED", -*info);
+    return;
+  }
+  if (n == 0) return;
+  hb::Staged<double> sa, sb, sx;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sx.In(x, ldx, n, nrhs, hb::kWsStageX, false)) return;
+  int it = 0;
+  const int finfo = hb::DposvMixed(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld,
+                                   sx.dev, sx.ld, t_mixed_slices, &it);
+  if (finfo < 0) {
+    hb::Finish("DPOSV_MIXED");
+    return;
+  }
+  if (it < 0) sa.Out();
+  if (finfo == 0 && nrhs > 0) sx.Out();
+  *iter = it;
+  *info = finfo;
+  hb::Finish("DPOSV_MIXED");
+}
+
 HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
                                      const hwyblas_int* m_p,
                                      const hwyblas_int* ncols_p,

@@ -599,7 +599,8 @@ int OzakiMaxK(int S) { return static_cast<int>((2147483647LL / (S * 16384LL)) / 
 // Returns the slice count used (0 if the inputs were not finite and the plain
 // FP64 path ran instead).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
-                  View<double> b, double beta, double* c, int ldc, int slices) {
+                  View<double> b, double beta, double* c, int ldc, int slices,
+                  bool check_finite) {
   Context& ctx = Ctx();
   cudaStream_t st = ctx.stream;
   const int S = std::min(8, std::max(1, slices));
@@ -616,8 +617,10 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
   bt.cs = b.rs;
   Exponents(bt, n, k, col_exp, nonfinite, st);
   int host_nonfinite = 0;
-  cudaMemcpyAsync(&host_nonfinite, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st);
-  if (Failed(cudaStreamSynchronize(st), "ozaki exponents")) return -1;
+  if (check_finite) {
+    cudaMemcpyAsync(&host_nonfinite, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (Failed(cudaStreamSynchronize(st), "ozaki exponents")) return -1;
+  }
   if (host_nonfinite) {
     // Inf/NaN cannot be sliced: the plain FP64 path propagates them.
     Dgemm(m, n, k, alpha, a, b, beta, c, ldc, kAll);

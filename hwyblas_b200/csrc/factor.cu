@@ -545,10 +545,15 @@ void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
     ix0 = k1 + (k1 - k2) * incx; i1 = k2; i2 = k1; inc = -1;
   }
   if (inc > 0 ? i1 > i2 : i1 < i2) return;
-  if (incx == 1 && k2 - k1 + 1 <= kSwapMax) {
-    LaswpPermKernel<T><<<(n + 31) / 32, 256, 0, Ctx().stream>>>(
-        n, a, lda, k1, k2, ipiv, Ctx().guard);
-    CountLaunch();
+  if (incx == 1) {
+    // Consecutive runs of at most kSwapMax interchanges, in order: the same
+    // sequence of interchanges as one pass over k1..k2.
+    for (int c1 = k1; c1 <= k2; c1 += kSwapMax) {
+      const int c2 = std::min(k2, c1 + kSwapMax - 1);
+      LaswpPermKernel<T><<<(n + 31) / 32, 256, 0, Ctx().stream>>>(
+          n, a, lda, c1, c2, ipiv, Ctx().guard);
+      CountLaunch();
+    }
     LaunchFailed("laswp");
     return;
   }

@@ -257,7 +257,12 @@ __global__ void __maxnreg__(168)
           Dmma(acc[1][nb], af[1], b0, b1);
         }
       }
+      // The stage was read through the generic proxy and will be rewritten
+      // by TMA (the async proxy): the proxy fence orders this warp's reads
+      // before the release. Without it B200 showed stale-stage reads (one
+      // warp's 16 x 32 block wrong in about 1 of 4 GEMMs of 8128^2 x 64).
       __syncwarp();
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       if (lane == 0) MbarArrive(&empty[s]);
 
       // End of a reference KC chunk: merge into the running C value.

@@ -74,7 +74,8 @@ enum WorkspaceSlot : int {
   kWsMixed3 = 10,
   kWsBatch = 11,
   kWsEmulW = 12,   // emulated-GEMM FP64 partial sums between passes
-  kNumWorkspaceSlots = 13
+  kWsStageX = 13,  // host-pointer staging of a solver's solution
+  kNumWorkspaceSlots = 14
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -132,6 +133,10 @@ template <typename T>
 void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
            T* b, int ldb);
 void Potrf(bool upper, int n, double* a, int lda, int* info);
+// Getrf2 / Potrf2 of a block whose first column is global column col0 (for
+// INFO); the Cholesky one turns later kernels into no-ops after a failure.
+void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0);
+void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
 void Potrf2(bool upper, int n, double* a, int lda, int* info);
 void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
            int ldb);
@@ -148,9 +153,12 @@ void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
 
 // FP64-accurate GEMM on INT8 tensor cores with `slices` slices (1..8);
 // returns the slice count used, 0 if non-finite inputs sent it to Dgemm, -1
-// on a CUDA error.
+// on a CUDA error. check_finite = false skips that test and its host
+// synchronization (callers whose inputs are known finite, or that detect a
+// non-finite result themselves).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
-                  View<double> b, double beta, double* c, int ldc, int slices);
+                  View<double> b, double beta, double* c, int ldc, int slices,
+                  bool check_finite = true);
 int OzakiMaxK(int S);
 // out(:, jj) = op(A) op(B)(:, cols[jj]) in double-double (error reference).
 void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,
@@ -159,6 +167,15 @@ void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,
 // Host-side wait-timeout check: returns true (and reports) if any kernel on
 // the context set the timeout flag since the last check. Synchronises.
 bool CheckDeviceStatus(const char* what);
+
+// Mixed-precision solvers (LAPACK DSGESV / DSPOSV semantics) on device data;
+// the trailing updates of the factorization use `slices` INT8 slices. Return
+// INFO (0; > 0 from the FP64 fallback's factorization; -1 on a CUDA error)
+// and set *iter to DSGESV's ITER.
+int DgesvMixed(int n, int nrhs, double* a, int lda, int* ipiv, const double* b,
+               int ldb, double* x, int ldx, int slices, int* iter);
+int DposvMixed(bool upper, int n, int nrhs, double* a, int lda, const double* b,
+               int ldb, double* x, int ldx, int slices, int* iter);
 
 // Reports an invalid argument through the error handler (default: xerbla_).
 void ReportError(const char* routine, int info);

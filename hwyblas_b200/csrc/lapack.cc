@@ -51,6 +51,10 @@ void Getrf2(int m, int n, T* a, int lda, int* ipiv, int* info) {
   GetrfRec<T>(m, n, a, lda, ipiv, info, 0);
 }
 
+void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0) {
+  GetrfRec<double>(m, n, a, lda, ipiv, info, col0);
+}
+
 template <typename T>
 void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info) {
   if (m == 0 || n == 0) return;
@@ -125,6 +129,14 @@ void Potrf2(bool upper, int n, double* a, int lda, int* info) {
   const int* saved = ctx.guard;
   ctx.guard = info;
   Potrf2Rec(upper, n, a, lda, info, 0);
+  ctx.guard = saved;
+}
+
+void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0) {
+  Context& ctx = Ctx();
+  const int* saved = ctx.guard;
+  ctx.guard = info;
+  Potrf2Rec(upper, n, a, lda, info, col0);
   ctx.guard = saved;
 }
 

@@ -1,0 +1,709 @@
+// Mixed-precision linear solvers: dgesv / dposv whose factorization spends
+// its flops on the INT8 tensor cores, with FP64 iterative refinement.
+//
+// The reference has no mixed-precision solver (README.md:81: ?sgesv/?sposv
+// are not ported); the driver follows LAPACK's DSGESV / DSPOSV: factor in
+// reduced precision, solve, then iterate r = b - A x (FP64), d = solve(r),
+// x += d until every column satisfies DSGESV's backward criterion
+// ||r||_inf <= ||x||_inf * ||A||_inf * eps * sqrt(n) and its correction has
+// settled (see Refine), at most 30 times; if that fails (or the
+// reduced-precision factorization breaks down), factor and solve in FP64 with
+// the plain path (the reference's own dgetrf/dpotrf order). ITER and IPIV
+// follow DSGESV: ITER >= 0 is the number of refinement steps, ITER < 0 means
+// the FP64 path ran (-2 non-finite A, -3 factorization breakdown, -31 no
+// convergence).
+//
+// Factorization (right-looking, block nb):
+//   LU        panel (pivot search and diagonal block) in FP64 by the
+//             recursive LU, U12 by an FP64 triangular solve, and the
+//             trailing update A22 -= L21 U12 as an Ozaki GEMM with few INT8
+//             slices on tcgen05 (integer-exact products, FP64 recombination).
+//   Cholesky  diagonal block in FP64, L21 by an FP64 triangular solve,
+//             A22 -= L21 L21^T as an Ozaki GEMM.
+// The factors stay in FP64 storage; their accuracy is that of the slices
+// (about 8*S - 1 significant bits), which sets the refinement's contraction.
+//
+// Refinement solves: the diagonal 64 x 64 blocks of the factors are inverted
+// once; each triangular solve is then one cooperative kernel that walks the
+// block rows (x_b = inv(T_bb) r_b, then every CTA updates its share of the
+// remaining rows) with a grid barrier per block.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace hb {
+namespace {
+
+constexpr int kTb = 64;         // diagonal block of the refinement solves
+constexpr int kTrsvRhs = 16;    // right-hand sides per solve launch
+constexpr int kTrsvThreads = 256;
+constexpr int kResRows = 128;   // residual GEMV: rows per CTA
+constexpr int kResK = 256;      // residual GEMV: k per CTA
+constexpr int kResRhs = 16;     // residual GEMV: right-hand sides per launch
+constexpr int kItMax = 30;      // LAPACK's ITERMAX (dsgesv.f)
+
+template <typename T>
+T* At(T* a, long long lda, long long i, long long j) {
+  return a + i + j * lda;
+}
+
+// ||A||_inf partial row sums: CTA (bx, by) sums |a_ij| over columns
+// [by*256, by*256 + 256) for its 256 rows.
+__global__ void RowAbsPartialKernel(int n, const double* a, long long lda,
+                                    double* part) {
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= n) return;
+  const int j0 = blockIdx.y * 256, j1 = min(n, j0 + 256);
+  double s = 0.0;
+  for (int j = j0; j < j1; ++j) s += fabs(a[i + j * lda]);
+  part[static_cast<long long>(blockIdx.y) * n + i] = s;
+}
+
+// Max over rows of the row sums; NaN dominates (its bit pattern is above
+// +Inf's as an unsigned integer).
+__global__ void RowAbsFinishKernel(int n, int parts, const double* part,
+                                   unsigned long long* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (i < n) {
+    for (int c = 0; c < parts; ++c) s += part[static_cast<long long>(c) * n + i];
+  }
+  unsigned long long bits = __double_as_longlong(s);
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_down_sync(0xffffffffu, bits, off);
+    bits = o > bits ? o : bits;
+  }
+  if (threadIdx.x % 32 == 0) atomicMax(out, bits);
+}
+
+// Column-wise max |x_iq| for q < nrhs (bits of a non-negative double).
+__global__ void ColAbsMaxKernel(int n, int nrhs, const double* x, long long ldx,
+                                unsigned long long* out) {
+  const int q = blockIdx.y;
+  unsigned long long bits = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const unsigned long long b = __double_as_longlong(fabs(x[i + q * ldx]));
+    bits = b > bits ? b : bits;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_down_sync(0xffffffffu, bits, off);
+    bits = o > bits ? o : bits;
+  }
+  if (threadIdx.x % 32 == 0) atomicMax(out + q, bits);
+}
+
+// Residual, few right-hand sides: part[c][q][i] = sum over k in chunk c of
+// a(i, k) * x(k, q). One thread per row; the x chunk is staged in shared
+// memory.
+__global__ void __launch_bounds__(kResRows)
+    ResidualPartialKernel(int n, int nrhs, const double* a, long long lda,
+                          const double* x, long long ldx, double* part) {
+  __shared__ double sx[kResRhs][kResK];
+  const int k0 = blockIdx.y * kResK, kc = min(kResK, n - k0);
+  for (int idx = threadIdx.x; idx < kResRhs * kResK; idx += kResRows) {
+    const int q = idx / kResK, k = idx % kResK;
+    sx[q][k] = (q < nrhs && k < kc) ? x[k0 + k + q * ldx] : 0.0;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * kResRows + threadIdx.x;
+  if (i >= n) return;
+  double acc[kResRhs];
+#pragma unroll
+  for (int q = 0; q < kResRhs; ++q) acc[q] = 0.0;
+  const double* ai = a + i + static_cast<long long>(k0) * lda;
+  for (int k = 0; k < kc; ++k) {
+    const double v = ai[static_cast<long long>(k) * lda];
+#pragma unroll
+    for (int q = 0; q < kResRhs; ++q)
+      if (q < nrhs) acc[q] = fma(v, sx[q][k], acc[q]);
+  }
+  double* out = part + static_cast<long long>(blockIdx.y) * nrhs * n;
+#pragma unroll
+  for (int q = 0; q < kResRhs; ++q)
+    if (q < nrhs) out[static_cast<long long>(q) * n + i] = acc[q];
+}
+
+// r(i, q) = b(i, q) - sum over chunks (in chunk order).
+__global__ void ResidualFinishKernel(int n, int nrhs, int chunks,
+                                     const double* part, const double* b,
+                                     long long ldb, double* r, long long ldr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y;
+  if (i >= n || q >= nrhs) return;
+  double s = 0.0;
+  for (int c = 0; c < chunks; ++c)
+    s += part[(static_cast<long long>(c) * nrhs + q) * n + i];
+  r[i + q * ldr] = b[i + q * ldb] - s;
+}
+
+__global__ void AxpyMatrixKernel(int n, int nrhs, const double* d, long long ldd,
+                                 double* x, long long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y;
+  if (i < n && q < nrhs) x[i + q * ldx] += d[i + q * ldd];
+}
+
+// dst(i, q) = src(perm[i], q).
+__global__ void GatherRowsKernel(int n, int nrhs, const int* perm, const double* src,
+                                 long long lds, double* dst, long long ldd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y;
+  if (i < n && q < nrhs) dst[i + q * ldd] = src[perm[i] + q * lds];
+}
+
+// The row permutation of LAPACK pivots: applying the interchanges i <->
+// ipiv[i] - 1 in order to the identity gives perm, and P b = b[perm]. The
+// interchanges are sequential: one thread replays them, on perm and ipiv
+// staged in shared memory when n <= kPermSmem, else in place in global
+// memory.
+constexpr int kPermSmem = 24576;
+__global__ void PermFromPivotsKernel(int n, const int* ipiv, int* perm) {
+  extern __shared__ int sm[];
+  const bool staged = n <= kPermSmem;
+  int* sp = staged ? sm : perm;
+  int* sv = staged ? sm + n : nullptr;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sp[i] = i;
+    if (staged) sv[i] = ipiv[i] - 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < n; ++i) {
+      int p = staged ? sv[i] : ipiv[i] - 1;
+      if (p < 0 || p >= n) p = i;  // never out of bounds
+      const int t = sp[i];
+      sp[i] = sp[p];
+      sp[p] = t;
+    }
+  }
+  __syncthreads();
+  if (staged)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
+}
+
+// Full symmetric matrix from one triangle: dst(i, j) = src(i, j) on the
+// referenced side and src(j, i) on the other. 32 x 32 tiles through shared
+// memory so that both the direct and the mirrored reads are coalesced.
+__global__ void SymmetrizeKernel(int n, int upper, const double* src,
+                                 long long lds, double* dst, long long ldd) {
+  __shared__ double tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  // Mirrored source tile (j0.., i0..) read along its rows.
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int si = j0 + threadIdx.x, sj = i0 + r;
+    if (si < n && sj < n) tile[r][threadIdx.x] = src[si + static_cast<long long>(sj) * lds];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + threadIdx.x, j = j0 + r;
+    if (i >= n || j >= n) continue;
+    const bool referenced = upper ? (i <= j) : (i >= j);
+    dst[i + static_cast<long long>(j) * ldd] =
+        referenced ? src[i + static_cast<long long>(j) * lds] : tile[threadIdx.x][r];
+  }
+}
+
+// Inverses of the diagonal kTb x kTb blocks of a triangular factor stored in
+// w: inv[b] (column-major kTb x kTb, zero outside the triangle). Thread c
+// computes column c by substitution against e_c.
+__global__ void __launch_bounds__(kTb)
+    InvertDiagBlocksKernel(int n, const double* w, long long ldw, int lower,
+                           int unit, double* inv) {
+  extern __shared__ double inv_smem[];  // t, then y: [kTb][kTb + 1] each
+  double(*t)[kTb + 1] = reinterpret_cast<double(*)[kTb + 1]>(inv_smem);
+  double(*y)[kTb + 1] = reinterpret_cast<double(*)[kTb + 1]>(inv_smem + kTb * (kTb + 1));
+  const int b = blockIdx.x, r0 = b * kTb, bs = min(kTb, n - r0);
+  const int c = threadIdx.x;
+  for (int r = 0; r < kTb; ++r)
+    t[r][c] = (r < bs && c < bs) ? w[(r0 + r) + static_cast<long long>(r0 + c) * ldw] : 0.0;
+  __syncthreads();
+  if (c < bs) {
+    if (lower) {
+      for (int r = 0; r < c; ++r) y[r][c] = 0.0;
+      y[c][c] = unit ? 1.0 : 1.0 / t[c][c];
+      for (int r = c + 1; r < bs; ++r) {
+        double s = 0.0;
+        for (int q = c; q < r; ++q) s = fma(t[r][q], y[q][c], s);
+        y[r][c] = unit ? -s : -s / t[r][r];
+      }
+    } else {
+      for (int r = c + 1; r < bs; ++r) y[r][c] = 0.0;
+      y[c][c] = unit ? 1.0 : 1.0 / t[c][c];
+      for (int r = c - 1; r >= 0; --r) {
+        double s = 0.0;
+        for (int q = r + 1; q <= c; ++q) s = fma(t[r][q], y[q][c], s);
+        y[r][c] = unit ? -s : -s / t[r][r];
+      }
+    }
+  }
+  __syncthreads();
+  double* out = inv + static_cast<long long>(b) * kTb * kTb;
+  for (int r = 0; r < kTb; ++r)
+    out[r + c * kTb] = (r < bs && c < bs) ? y[r][c] : 0.0;
+}
+
+// Triangular solve T x = x in place for nrhs <= kTrsvRhs columns of x, with
+// T the lower (forward) or upper (backward) triangle of w and inv the
+// inverses of its diagonal blocks. Cooperative: all CTAs are resident; each
+// step solves one block row redundantly in every CTA (CTA 0 stores it) and
+// then updates the CTA's share of the remaining rows; a grid barrier ends
+// the step. x is read and written through L2 only (.cg), since rows change
+// owner between steps.
+template <bool kLower>
+__global__ void __launch_bounds__(kTrsvThreads)
+    BlockTrsvKernel(int n, int nrhs, const double* w, long long ldw,
+                    const double* inv, double* x, long long ldx,
+                    unsigned int* barrier, int* timeout_flag) {
+  __shared__ double sb[kTb][kTrsvRhs];
+  __shared__ double sx[kTb][kTrsvRhs];
+  const int nblk = (n + kTb - 1) / kTb;
+  unsigned int gen = 0;
+  for (int step = 0; step < nblk; ++step) {
+    const int blk = kLower ? step : nblk - 1 - step;
+    const int r0 = blk * kTb, bs = min(kTb, n - r0);
+    for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+      const int r = idx % kTb, q = idx / kTb;
+      sb[r][q] = (r < bs && q < nrhs) ? __ldcg(x + r0 + r + q * ldx) : 0.0;
+    }
+    __syncthreads();
+    const double* ib = inv + static_cast<long long>(blk) * kTb * kTb;
+    for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+      const int r = idx % kTb, q = idx / kTb;
+      double s = 0.0;
+      if (q < nrhs) {
+        for (int c = 0; c < bs; ++c) s = fma(ib[r + c * kTb], sb[c][q], s);
+      }
+      sx[r][q] = s;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0) {
+      for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+        const int r = idx % kTb, q = idx / kTb;
+        if (r < bs && q < nrhs) __stcg(x + r0 + r + q * ldx, sx[r][q]);
+      }
+    }
+    const int lo = kLower ? r0 + bs : 0, hi = kLower ? n : r0;
+    for (int i = lo + blockIdx.x * kTrsvThreads + threadIdx.x; i < hi;
+         i += gridDim.x * kTrsvThreads) {
+      double acc[kTrsvRhs];
+#pragma unroll
+      for (int q = 0; q < kTrsvRhs; ++q) acc[q] = 0.0;
+      const double* wi = w + i + static_cast<long long>(r0) * ldw;
+      for (int c = 0; c < bs; ++c) {
+        const double l = wi[static_cast<long long>(c) * ldw];
+#pragma unroll
+        for (int q = 0; q < kTrsvRhs; ++q)
+          if (q < nrhs) acc[q] = fma(l, sx[c][q], acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < kTrsvRhs; ++q)
+        if (q < nrhs) {
+          double* xi = x + i + q * ldx;
+          __stcg(xi, __ldcg(xi) - acc[q]);
+        }
+    }
+    if (!GridBarrier(barrier, gridDim.x, ++gen, timeout_flag)) return;
+  }
+}
+
+// Buffers of one mixed solve (device pointers into the thread's workspace).
+struct MixedBuffers {
+  double* w = nullptr;      // n x n factor, leading dimension ldw
+  long long ldw = 0;
+  double* afull = nullptr;  // dposv: the full symmetric A (leading dimension ldw)
+  double* inv_lo = nullptr; // inverses of the diagonal blocks of L and U
+  double* inv_up = nullptr;
+  double* r = nullptr;      // n x nrhs residual
+  double* d = nullptr;      // n x nrhs correction
+  long long ldr = 0;        // of r and d
+  double* part = nullptr;   // residual and norm partial sums
+  int* perm = nullptr;      // LU row permutation
+  unsigned long long* norms = nullptr;  // [0] ||A||, then ||x||, ||r|| columns
+  unsigned int* barrier = nullptr;
+};
+
+long long Round(long long v, long long m) { return (v + m - 1) / m * m; }
+
+bool AllocBuffers(int n, int nrhs, bool sym, MixedBuffers* bf) {
+  bf->ldw = Round(std::max(n, 1), 32);
+  const size_t wbytes = sizeof(double) * static_cast<size_t>(bf->ldw) * n;
+  bf->w = static_cast<double*>(Workspace(kWsMixed, wbytes));
+  if (bf->w == nullptr) return false;
+  if (sym) {
+    bf->afull = static_cast<double*>(Workspace(kWsMixed2, wbytes));
+    if (bf->afull == nullptr) return false;
+  }
+  const size_t nblk = (n + kTb - 1) / kTb;
+  bf->ldr = bf->ldw;
+  const size_t chunks = (n + kResK - 1) / kResK;
+  const size_t rowparts = (n + 255) / 256;
+  const size_t inv_elems = nblk * kTb * kTb;
+  const size_t r_elems = static_cast<size_t>(bf->ldr) * nrhs;
+  const size_t part_elems =
+      std::max(chunks * std::min(nrhs, kResRhs) * n, rowparts * n);
+  const size_t norm_elems = 1 + 3 * static_cast<size_t>(nrhs);
+  const size_t total = sizeof(double) * (2 * inv_elems + 2 * r_elems + part_elems) +
+                       sizeof(int) * Round(n, 64) +
+                       sizeof(unsigned long long) * (norm_elems + 8) + 4096;
+  uint8_t* base = static_cast<uint8_t*>(Workspace(kWsMixed3, total));
+  if (base == nullptr) return false;
+  double* d = reinterpret_cast<double*>(base);
+  bf->inv_lo = d;
+  bf->inv_up = d + inv_elems;
+  bf->r = d + 2 * inv_elems;
+  bf->d = bf->r + r_elems;
+  bf->part = bf->d + r_elems;
+  bf->perm = reinterpret_cast<int*>(bf->part + part_elems);
+  bf->norms = reinterpret_cast<unsigned long long*>(bf->perm + Round(n, 64));
+  bf->barrier = reinterpret_cast<unsigned int*>(bf->norms + norm_elems + 8);
+  return true;
+}
+
+double BitsToDouble(unsigned long long b) {
+  double v;
+  std::memcpy(&v, &b, sizeof v);
+  return v;
+}
+
+void Copy2D(int m, int n, const double* src, long long lds, double* dst,
+            long long ldd) {
+  if (m <= 0 || n <= 0) return;
+  Failed(cudaMemcpy2DAsync(dst, sizeof(double) * ldd, src, sizeof(double) * lds,
+                           sizeof(double) * m, n, cudaMemcpyDeviceToDevice,
+                           Ctx().stream),
+         "mixed copy");
+}
+
+// ||A||_inf of an n x n matrix (host value; waits for the stream).
+double InfNorm(int n, const double* a, long long lda, MixedBuffers& bf) {
+  cudaStream_t st = Ctx().stream;
+  const int rowparts = (n + 255) / 256;
+  cudaMemsetAsync(bf.norms, 0, sizeof(unsigned long long), st);
+  RowAbsPartialKernel<<<dim3(rowparts, rowparts), 256, 0, st>>>(n, a, lda, bf.part);
+  RowAbsFinishKernel<<<rowparts, 256, 0, st>>>(n, rowparts, bf.part, bf.norms);
+  CountLaunch(2);
+  LaunchFailed("mixed norm");
+  unsigned long long bits = 0;
+  cudaMemcpyAsync(&bits, bf.norms, sizeof bits, cudaMemcpyDeviceToHost, st);
+  if (Failed(cudaStreamSynchronize(st), "mixed norm")) return NAN;
+  return BitsToDouble(bits);
+}
+
+// r := b - A x (FP64). Many right-hand sides go through the DMMA GEMM; few
+// through a split-k GEMV whose partial sums are added in a fixed order.
+void Residual(int n, int nrhs, const double* a, long long lda, const double* b,
+              long long ldb, const double* x, long long ldx, MixedBuffers& bf) {
+  cudaStream_t st = Ctx().stream;
+  if (nrhs >= kResRhs) {
+    Copy2D(n, nrhs, b, ldb, bf.r, bf.ldr);
+    Dgemm(n, nrhs, n, -1.0, ColMajor(a, lda), ColMajor(x, ldx), 1.0, bf.r,
+          static_cast<int>(bf.ldr), kAll);
+    return;
+  }
+  const int chunks = (n + kResK - 1) / kResK;
+  ResidualPartialKernel<<<dim3((n + kResRows - 1) / kResRows, chunks), kResRows, 0, st>>>(
+      n, nrhs, a, lda, x, ldx, bf.part);
+  ResidualFinishKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(
+      n, nrhs, chunks, bf.part, b, ldb, bf.r, bf.ldr);
+  CountLaunch(2);
+  LaunchFailed("mixed residual");
+}
+
+// Column max-norms of `count` n x nrhs matrices into host arrays (waits for
+// the stream); norms[c][q] = max_i |m_c(i, q)|.
+bool ColumnNorms(int n, int nrhs, int count, const double* const* mats,
+                 const long long* lds, MixedBuffers& bf,
+                 std::vector<std::vector<double>>* norms) {
+  cudaStream_t st = Ctx().stream;
+  unsigned long long* dn = bf.norms + 1;
+  cudaMemsetAsync(dn, 0, sizeof(unsigned long long) * count * nrhs, st);
+  const int blocks = std::min(64, (n + 255) / 256);
+  for (int c = 0; c < count; ++c) {
+    ColAbsMaxKernel<<<dim3(blocks, nrhs), 256, 0, st>>>(n, nrhs, mats[c], lds[c],
+                                                        dn + c * nrhs);
+  }
+  CountLaunch(count);
+  LaunchFailed("mixed column norms");
+  std::vector<unsigned long long> bits(static_cast<size_t>(count) * nrhs);
+  cudaMemcpyAsync(bits.data(), dn, sizeof(unsigned long long) * bits.size(),
+                  cudaMemcpyDeviceToHost, st);
+  if (Failed(cudaStreamSynchronize(st), "mixed column norms")) return false;
+  norms->assign(count, std::vector<double>(nrhs));
+  for (int c = 0; c < count; ++c)
+    for (int q = 0; q < nrhs; ++q) (*norms)[c][q] = BitsToDouble(bits[c * nrhs + q]);
+  return true;
+}
+
+void InvertDiagBlocks(int n, const double* w, long long ldw, bool lower, bool unit,
+                      double* inv) {
+  const int nblk = (n + kTb - 1) / kTb;
+  const int smem = 2 * kTb * (kTb + 1) * static_cast<int>(sizeof(double));
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(InvertDiagBlocksKernel,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    configured = true;
+  }
+  InvertDiagBlocksKernel<<<nblk, kTb, smem, Ctx().stream>>>(n, w, ldw, lower ? 1 : 0,
+                                                            unit ? 1 : 0, inv);
+  CountLaunch();
+  LaunchFailed("mixed diagonal inverses");
+}
+
+void PermFromPivots(int n, const int* ipiv, int* perm) {
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(PermFromPivotsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * kPermSmem * static_cast<int>(sizeof(int)));
+    configured = true;
+  }
+  const size_t smem = n <= kPermSmem ? 2 * sizeof(int) * n : 0;
+  PermFromPivotsKernel<<<1, 1024, smem, Ctx().stream>>>(n, ipiv, perm);
+  CountLaunch();
+  LaunchFailed("mixed permutation");
+}
+
+// x := T^{-1} x for the lower or upper triangle of w.
+void BlockTrsv(bool lower, int n, int nrhs, const double* w, long long ldw,
+               const double* inv, double* x, long long ldx, unsigned int* barrier) {
+  Context& ctx = Ctx();
+  static int grid = 0;
+  if (grid == 0) {
+    int lo = 0, up = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, BlockTrsvKernel<true>,
+                                                  kTrsvThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, BlockTrsvKernel<false>,
+                                                  kTrsvThreads, 0);
+    grid = ctx.num_sms * std::max(1, std::min({lo, up, 2}));
+  }
+  int nn = n;
+  long long lw = ldw, lx = ldx;
+  int* flag = ctx.dev_status;
+  const void* fn = lower ? reinterpret_cast<const void*>(BlockTrsvKernel<true>)
+                         : reinterpret_cast<const void*>(BlockTrsvKernel<false>);
+  for (int q0 = 0; q0 < nrhs; q0 += kTrsvRhs) {
+    int nr = std::min(kTrsvRhs, nrhs - q0);
+    double* xq = x + static_cast<long long>(q0) * ldx;
+    cudaMemsetAsync(barrier, 0, sizeof(unsigned int), ctx.stream);
+    void* args[] = {&nn, &nr, const_cast<double**>(&w), &lw,
+                    const_cast<double**>(&inv), &xq, &lx, &barrier, &flag};
+    Failed(cudaLaunchCooperativeKernel(fn, grid, kTrsvThreads, args, 0, ctx.stream),
+           "mixed triangular solve");
+    CountLaunch();
+  }
+}
+
+// dst := A^{-1} src with the mixed factors (LU: P, unit L, U; Cholesky: L,
+// and L^T mirrored into the upper triangle of w).
+void MixedSolve(bool lu, int n, int nrhs, MixedBuffers& bf, const double* src,
+                long long lds, double* dst, long long ldd) {
+  if (lu) {
+    GatherRowsKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, Ctx().stream>>>(
+        n, nrhs, bf.perm, src, lds, dst, ldd);
+    CountLaunch();
+    LaunchFailed("mixed gather");
+  } else {
+    Copy2D(n, nrhs, src, lds, dst, ldd);
+  }
+  BlockTrsv(true, n, nrhs, bf.w, bf.ldw, bf.inv_lo, dst, ldd, bf.barrier);
+  BlockTrsv(false, n, nrhs, bf.w, bf.ldw, bf.inv_up, dst, ldd, bf.barrier);
+}
+
+int MixedBlock(int n) { return n >= 4096 ? 512 : 256; }
+
+// Right-looking LU of w with FP64 panels and Ozaki trailing updates.
+void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slices) {
+  const int nb = MixedBlock(n);
+  const int lw = static_cast<int>(ldw);
+  for (int j = 0; j < n; j += nb) {
+    const int jb = std::min(nb, n - j);
+    GetrfPanel(n - j, jb, At(w, ldw, j, j), lw, ipiv + j, info, j);
+    AdjustPivots(ipiv, j, j + jb, j);
+    if (j > 0) Laswp<double>(j, w, lw, j + 1, j + jb, ipiv, 1);
+    if (j + jb < n) {
+      const int rest = n - j - jb;
+      Laswp<double>(rest, At(w, ldw, 0, j + jb), lw, j + 1, j + jb, ipiv, 1);
+      TrsmFull<double>(true, true, false, true, jb, rest, 1.0, At(w, ldw, j, j), lw,
+                       At(w, ldw, j, j + jb), lw);
+      DgemmEmulated(rest, rest, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
+                    ColMajor<double>(At(w, ldw, j, j + jb), ldw), 1.0,
+                    At(w, ldw, j + jb, j + jb), lw, slices, false);
+    }
+  }
+}
+
+// Right-looking lower Cholesky of w (full symmetric storage) with FP64
+// diagonal blocks and Ozaki trailing updates; then L^T is mirrored into the
+// upper triangle for the backward solve.
+void MixedPotrf(int n, double* w, long long ldw, int* info, int slices) {
+  const int nb = MixedBlock(n);
+  const int lw = static_cast<int>(ldw);
+  for (int j = 0; j < n; j += nb) {
+    const int jb = std::min(nb, n - j);
+    PotrfPanel(false, jb, At(w, ldw, j, j), lw, info, j);
+    if (j + jb < n) {
+      const int rest = n - j - jb;
+      Context& ctx = Ctx();
+      const int* saved = ctx.guard;
+      ctx.guard = info;
+      TrsmFull<double>(false, true, true, false, rest, jb, 1.0, At(w, ldw, j, j), lw,
+                       At(w, ldw, j + jb, j), lw);
+      ctx.guard = saved;
+      DgemmEmulated(rest, rest, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
+                    ColMajor<double>(At(w, ldw, j + jb, j), ldw, true), 1.0,
+                    At(w, ldw, j + jb, j + jb), lw, slices, false);
+    }
+  }
+  const dim3 grid((n + 31) / 32, (n + 31) / 32);
+  // Upper triangle := transpose of the lower one (in place is safe: each
+  // tile reads only the lower triangle and writes only the upper one).
+  SymmetrizeKernel<<<grid, dim3(32, 8), 0, Ctx().stream>>>(n, 0, w, ldw, w, ldw);
+  CountLaunch();
+  LaunchFailed("mixed mirror");
+}
+
+// The refinement loop shared by both solvers. Each step computes r = b - A x
+// in FP64, d = A^{-1} r with the reduced-precision factors, and x += d. It
+// stops once every column meets LAPACK's DSGESV backward criterion
+// ||r||_inf <= ||x||_inf ||A||_inf eps sqrt(n) (dsgesv.f) and its correction
+// has settled: ||d||_inf <= 2^-52 ||x||_inf, or no longer halving (the
+// forward-error stopping rule of iterative refinement). Returns the number of
+// corrections applied, or -31 if 30 did not get there.
+int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const double* b,
+           long long ldb, double* x, long long ldx, double anrm, MixedBuffers& bf) {
+  cudaStream_t st = Ctx().stream;
+  const double eps = 0.5 * 2.220446049250313e-16;  // DLAMCH('Epsilon')
+  const double cte = anrm * eps * std::sqrt(static_cast<double>(n));
+  MixedSolve(lu, n, nrhs, bf, b, ldb, x, ldx);  // x = A^{-1} b, reduced precision
+  std::vector<std::vector<double>> nm;
+  std::vector<double> dprev(nrhs, INFINITY);
+  const double* mats[3] = {x, bf.r, bf.d};
+  const long long lds[3] = {ldx, bf.ldr, bf.ldr};
+  for (int it = 0; it < kItMax; ++it) {
+    Residual(n, nrhs, a, lda, b, ldb, x, ldx, bf);
+    MixedSolve(lu, n, nrhs, bf, bf.r, bf.ldr, bf.d, bf.ldr);
+    if (!ColumnNorms(n, nrhs, 3, mats, lds, bf, &nm)) return -kItMax - 1;
+    AxpyMatrixKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(n, nrhs, bf.d, bf.ldr,
+                                                                  x, ldx);
+    CountLaunch();
+    bool done = true;
+    for (int q = 0; q < nrhs; ++q) {
+      const double xn = nm[0][q], rn = nm[1][q], dn = nm[2][q];
+      const bool backward = rn <= xn * cte;  // false on NaN
+      const bool settled = dn <= 0x1p-52 * xn || dn > 0.5 * dprev[q];
+      if (!(backward && settled)) done = false;
+      dprev[q] = dn;
+    }
+    if (done) return it + 1;
+  }
+  return -kItMax - 1;
+}
+
+}  // namespace
+
+int DgesvMixed(int n, int nrhs, double* a, int lda, int* ipiv, const double* b,
+               int ldb, double* x, int ldx, int slices, int* iter) {
+  Context& ctx = Ctx();
+  cudaStream_t st = ctx.stream;
+  MixedBuffers bf;
+  *iter = 0;
+  if (!AllocBuffers(n, nrhs, false, &bf)) return -1;
+  int* dinfo = ctx.dev_status + 1;
+  const double anrm = InfNorm(n, a, lda, bf);
+  int fallback = 0;
+  if (!std::isfinite(anrm)) {
+    fallback = -2;
+  } else {
+    cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+    Copy2D(n, n, a, lda, bf.w, bf.ldw);
+    MixedGetrf(n, bf.w, bf.ldw, ipiv, dinfo, slices);
+    int finfo = 0;
+    cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (Failed(cudaStreamSynchronize(st), "mixed getrf")) return -1;
+    if (finfo != 0) {
+      fallback = -3;
+    } else {
+      InvertDiagBlocks(n, bf.w, bf.ldw, true, true, bf.inv_lo);
+      InvertDiagBlocks(n, bf.w, bf.ldw, false, false, bf.inv_up);
+      PermFromPivots(n, ipiv, bf.perm);
+      const int it = Refine(true, n, nrhs, a, lda, b, ldb, x, ldx, anrm, bf);
+      if (it >= 0) {
+        *iter = it;
+        return 0;
+      }
+      fallback = it;
+    }
+  }
+  // FP64: the plain LU and solve on A itself.
+  *iter = fallback;
+  cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+  Getrf<double>(n, n, a, lda, ipiv, dinfo);
+  int finfo = 0;
+  cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (Failed(cudaStreamSynchronize(st), "mixed fallback getrf")) return -1;
+  if (finfo == 0) {
+    Copy2D(n, nrhs, b, ldb, x, ldx);
+    Getrs<double>(false, n, nrhs, a, lda, ipiv, x, ldx);
+  }
+  return finfo;
+}
+
+int DposvMixed(bool upper, int n, int nrhs, double* a, int lda, const double* b,
+               int ldb, double* x, int ldx, int slices, int* iter) {
+  Context& ctx = Ctx();
+  cudaStream_t st = ctx.stream;
+  MixedBuffers bf;
+  *iter = 0;
+  if (!AllocBuffers(n, nrhs, true, &bf)) return -1;
+  int* dinfo = ctx.dev_status + 1;
+  const dim3 grid((n + 31) / 32, (n + 31) / 32);
+  SymmetrizeKernel<<<grid, dim3(32, 8), 0, st>>>(n, upper ? 1 : 0, a, lda, bf.afull,
+                                                 bf.ldw);
+  CountLaunch();
+  LaunchFailed("mixed symmetrize");
+  const double anrm = InfNorm(n, bf.afull, bf.ldw, bf);
+  int fallback = 0;
+  if (!std::isfinite(anrm)) {
+    fallback = -2;
+  } else {
+    cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+    Copy2D(n, n, bf.afull, bf.ldw, bf.w, bf.ldw);
+    MixedPotrf(n, bf.w, bf.ldw, dinfo, slices);
+    int finfo = 0;
+    cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (Failed(cudaStreamSynchronize(st), "mixed potrf")) return -1;
+    if (finfo != 0) {
+      fallback = -3;
+    } else {
+      InvertDiagBlocks(n, bf.w, bf.ldw, true, false, bf.inv_lo);
+      InvertDiagBlocks(n, bf.w, bf.ldw, false, false, bf.inv_up);
+      const int it = Refine(false, n, nrhs, bf.afull, bf.ldw, b, ldb, x, ldx, anrm, bf);
+      if (it >= 0) {
+        *iter = it;
+        return 0;
+      }
+      fallback = it;
+    }
+  }
+  *iter = fallback;
+  cudaMemsetAsync(dinfo, 0, sizeof(int), st);
+  Potrf(upper, n, a, lda, dinfo);
+  int finfo = 0;
+  cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (Failed(cudaStreamSynchronize(st), "mixed fallback potrf")) return -1;
+  if (finfo == 0) {
+    Copy2D(n, nrhs, b, ldb, x, ldx);
+    Potrs(upper, n, nrhs, a, lda, x, ldx);
+  }
+  return finfo;
+}
+
+}  // namespace hb

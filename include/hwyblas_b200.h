@@ -218,6 +218,36 @@ HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
                                      const hwyblas_int* cols, double* out,
                                      const hwyblas_int* ldo);
 
+/* Mixed-precision solve of A X = B (LAPACK DSGESV semantics; the reference
+ * has no mixed-precision solver, README.md:81). The LU's trailing updates run
+ * as INT8-slice GEMMs on the tensor cores (hwyblas_set_mixed_slices slices,
+ * default 4), the panels (pivot search, diagonal block) in FP64; X is then
+ * refined in FP64 until every column meets ||r||_inf <= ||x||_inf ||A||_inf
+ * eps sqrt(n) and its last correction is below 2^-52 ||x||_inf or stopped
+ * halving. ITER >= 0: refinement steps taken, A unchanged, IPIV from
+ * the mixed factorization. ITER < 0: the FP64 path ran (-2 non-finite A, -3
+ * breakdown, -31 no convergence in 30 steps), A holds its LU factors and
+ * IPIV its pivots (src/lapack/getrf.cc:217-280 order). INFO as dgesv_. */
+HWYBLAS_API void hwyblas_dgesv_mixed(const hwyblas_int* n, const hwyblas_int* nrhs,
+                                     double* a, const hwyblas_int* lda,
+                                     hwyblas_int* ipiv, const double* b,
+                                     const hwyblas_int* ldb, double* x,
+                                     const hwyblas_int* ldx, hwyblas_int* iter,
+                                     hwyblas_int* info);
+/* Mixed-precision Cholesky solve (LAPACK DSPOSV semantics), as
+ * hwyblas_dgesv_mixed with a Cholesky factorization; on ITER < 0, A holds
+ * the FP64 factor of src/lapack/potrf.cc:121-199. */
+HWYBLAS_API void hwyblas_dposv_mixed(const char* uplo, const hwyblas_int* n,
+                                     const hwyblas_int* nrhs, double* a,
+                                     const hwyblas_int* lda, const double* b,
+                                     const hwyblas_int* ldb, double* x,
+                                     const hwyblas_int* ldx, hwyblas_int* iter,
+                                     hwyblas_int* info);
+/* Slice count (1..8) of the mixed solvers' trailing updates for the calling
+ * thread; returns the previous value (other values only query). Like the
+ * reference's hwyblas_set_ilaenv (lapack.h:74-80), a tuning knob. */
+HWYBLAS_API int hwyblas_set_mixed_slices(int slices);
+
 /* Stream for subsequent calls of the calling thread (a cudaStream_t; NULL
  * restores the library's per-thread stream). No counterpart in the
  * reference, which has no device. */

@@ -56,6 +56,25 @@ def test_dgemm_config_1024(hb, orc):
     run_gemm(hb, orc, "N", "N", 1024, 1024, 1024, 1.5, 0.5, seed=1)
 
 
+def test_dgemm_persistent_many_tiles_repeated(hb, orc):
+    """The LU trailing-update shape at n = 8192 (8128^2 x 64, ~55 tiles per
+    persistent CTA, the shared-memory ring reused across tiles), four times:
+    every run bit-identical to the oracle. This shape exposed a stale-stage
+    read (generic reads vs TMA rewrites of the ring without a proxy fence)."""
+    import os
+    rng = np.random.default_rng(77)
+    m = n = 8128
+    k = 64
+    a, b, c = rand(rng, m, k), rand(rng, k, n), rand(rng, m, n)
+    c_orc = c.copy(order="F")
+    orc.set_threads(os.cpu_count() or 8)
+    orc.dgemm("N", "N", m, n, k, -1.0, a, m, b, k, 1.0, c_orc, m)
+    for _ in range(4):
+        c_gpu = c.copy(order="F")
+        hb.dgemm("N", "N", m, n, k, -1.0, a, m, b, k, 1.0, c_gpu, m)
+        assert same_bits(c_gpu, c_orc), first_diff(c_gpu, c_orc)
+
+
 @pytest.mark.parametrize("kind", ["nan_a", "inf_b", "inf_times_zero", "nan_c"])
 def test_dgemm_special_values(hb, orc, kind):
     def special(a, b, c):

@@ -44,6 +44,23 @@ def test_dgetrf_config_4096(hb, orc):
     assert lu_ratio(a, a1, p1, n, n) < 30
 
 
+def test_dgetrf_8192(hb, orc):
+    """dgetrf n=8192: 128 trailing updates with many tiles per persistent CTA
+    and 8-CTA cooperative leaves; factors and ipiv bit-identical."""
+    import os
+    rng = np.random.default_rng(8192)
+    n = 8192
+    a = rand(rng, n, n)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1 = np.zeros(n, np.int32)
+    p2 = np.zeros(n, np.int32)
+    assert hb.dgetrf(n, n, a1, n, p1) == 0
+    orc.set_threads(os.cpu_count() or 8)
+    assert orc.dgetrf(n, n, a2, n, p2) == 0
+    assert np.array_equal(p1, p2)
+    assert same_bits(a1, a2), first_diff(a1, a2)
+
+
 @pytest.mark.parametrize("recursive", [False, True])
 @pytest.mark.parametrize("n", [5, 40])
 def test_tiny_pivots(hb, recursive, n):

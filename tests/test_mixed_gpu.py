@@ -1,0 +1,175 @@
+"""Mixed-precision dgesv / dposv (LAPACK DSGESV / DSPOSV semantics) through
+the C ABI.
+
+The reference has no mixed-precision solver, so the checks are stated
+against its FP64 routines (the oracle): the refined solution's normwise
+forward error is at most that of the oracle's dgesv / dposv solution (within
+a factor of 4: both sit at the cond * eps noise level), its residual meets DSGESV's backward criterion, A is left
+unchanged, and every path that falls back to FP64 (non-finite A, a singular
+or indefinite matrix, no convergence) gives bit for bit the plain path's
+factors and solution. Matrices follow the north-star workload: A = H1 diag(s)
+H2 with H1, H2 products of 4 Householder reflectors and s geometric from 1 to
+1/cond; SPD A = G G^T / n + 1e-3 I.
+"""
+import numpy as np
+import pytest
+
+from tests.oracle_lib import same_bits
+
+pytestmark = pytest.mark.gpu
+
+EPS = 2.0 ** -53
+
+
+def householder_matrix(rng, n, cond):
+    s = np.geomspace(1.0, 1.0 / cond, n)
+    a = np.diag(s)
+    for side in range(2):
+        for _ in range(4):
+            v = rng.standard_normal(n)
+            v /= np.linalg.norm(v)
+            if side == 0:
+                a = a - 2.0 * np.outer(v, v @ a)
+            else:
+                a = a - 2.0 * np.outer(a @ v, v)
+    return np.asfortranarray(a)
+
+
+def spd_matrix(rng, n):
+    g = rng.standard_normal((n, n))
+    return np.asfortranarray(g @ g.T / n + 1e-3 * np.eye(n))
+
+
+def fwd_err(x, xt):
+    return np.linalg.norm(x - xt) / np.linalg.norm(xt)
+
+
+def check_backward(a, x, b, n):
+    r = b - a @ x
+    anrm = np.abs(a).sum(axis=1).max()
+    for q in range(x.shape[1]):
+        assert np.abs(r[:, q]).max() <= 4 * np.abs(x[:, q]).max() * anrm * EPS * np.sqrt(n)
+
+
+@pytest.mark.parametrize("n,nrhs", [(300, 1), (700, 3), (1100, 20)])
+@pytest.mark.parametrize("cond", [1e2, 1e6])
+def test_dgesv_mixed_accuracy(hb, orc, n, nrhs, cond):
+    rng = np.random.default_rng(int(n + nrhs + np.log10(cond)))
+    a = householder_matrix(rng, n, cond)
+    xt = rng.uniform(-1, 1, (n, nrhs))
+    b = np.asfortranarray(a @ xt)
+    a_in = a.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, np.int32)
+    info, it = hb.dgesv_mixed(n, nrhs, a_in, n, ipiv, b, n, x, n)
+    assert info == 0 and it >= 1, (info, it)
+    assert same_bits(a_in, a)  # A untouched when refinement succeeds
+    assert ipiv.min() >= 1 and ipiv.max() <= n
+    check_backward(a, x, b, n)
+    # The FP64 oracle (the reference's dgesv order).
+    a2, x2 = a.copy(order="F"), b.copy(order="F")
+    p2 = np.zeros(n, np.int32)
+    assert orc.dgesv(n, nrhs, a2, n, p2, x2, n) == 0
+    assert fwd_err(x, xt) <= 4.0 * fwd_err(x2, xt) + 1e-15, (fwd_err(x, xt), fwd_err(x2, xt))
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("n,nrhs", [(257, 1), (900, 5)])
+def test_dposv_mixed_accuracy(hb, orc, uplo, n, nrhs):
+    rng = np.random.default_rng(n * 3 + nrhs)
+    a = spd_matrix(rng, n)
+    xt = rng.uniform(-1, 1, (n, nrhs))
+    b = np.asfortranarray(a @ xt)
+    # Only the `uplo` triangle is referenced: poison the other one.
+    a_in = a.copy(order="F")
+    other = np.tril_indices(n, -1) if uplo == "U" else np.triu_indices(n, 1)
+    a_in[other] = np.nan
+    a_keep = a_in.copy(order="F")
+    x = np.zeros((n, nrhs), order="F")
+    info, it = hb.dposv_mixed(uplo, n, nrhs, a_in, n, b, n, x, n)
+    assert info == 0 and it >= 1, (info, it)
+    assert same_bits(a_in, a_keep)
+    check_backward(a, x, b, n)
+    a2, x2 = a.copy(order="F"), b.copy(order="F")
+    assert orc.dposv(uplo, n, nrhs, a2, n, x2, n) == 0
+    assert fwd_err(x, xt) <= 4.0 * fwd_err(x2, xt) + 1e-15
+
+
+@pytest.mark.parametrize("slices", [3, 4, 5])
+def test_dgesv_mixed_slice_counts(hb, slices):
+    n = 500
+    rng = np.random.default_rng(11)
+    a = householder_matrix(rng, n, 1e4)
+    xt = rng.uniform(-1, 1, (n, 2))
+    b = np.asfortranarray(a @ xt)
+    prev = hb.set_mixed_slices(slices)
+    try:
+        x = np.zeros((n, 2), order="F")
+        ipiv = np.zeros(n, np.int32)
+        info, it = hb.dgesv_mixed(n, 2, a.copy(order="F"), n, ipiv, b, n, x, n)
+    finally:
+        hb.set_mixed_slices(prev)
+    assert info == 0 and it >= 1
+    check_backward(a, x, b, n)
+
+
+def test_dgesv_mixed_fallbacks_match_plain(hb):
+    """Non-finite A (ITER -2) and a singular A (ITER -3): the plain FP64 path
+    runs on A itself, so A, IPIV, X and INFO equal dgesv_'s bit for bit."""
+    rng = np.random.default_rng(5)
+    n, nrhs = 150, 2
+    for kind, expect_iter in [("nan", -2), ("singular", -3)]:
+        a = rng.uniform(-1, 1, (n, n))
+        if kind == "nan":
+            a[7, 9] = np.nan
+        else:
+            a[:, 40] = 0.0
+        a = np.asfortranarray(a)
+        b = np.asfortranarray(rng.uniform(-1, 1, (n, nrhs)))
+        a1, x1 = a.copy(order="F"), np.zeros((n, nrhs), order="F")
+        p1 = np.zeros(n, np.int32)
+        info1, it = hb.dgesv_mixed(n, nrhs, a1, n, p1, b, n, x1, n)
+        a2, x2 = a.copy(order="F"), b.copy(order="F")
+        p2 = np.zeros(n, np.int32)
+        info2 = hb.dgesv(n, nrhs, a2, n, p2, x2, n)
+        assert it == expect_iter and info1 == info2
+        assert same_bits(a1, a2) and np.array_equal(p1, p2)
+        if info2 == 0:
+            assert same_bits(x1, x2)
+        else:
+            assert info2 == 41
+
+
+def test_dposv_mixed_indefinite_falls_back(hb):
+    rng = np.random.default_rng(6)
+    n = 200
+    a = spd_matrix(rng, n)
+    a[50, 50] = -5.0
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, 1)))
+    a1, x1 = a.copy(order="F"), np.zeros((n, 1), order="F")
+    info1, it = hb.dposv_mixed("L", n, 1, a1, n, b, n, x1, n)
+    a2, x2 = a.copy(order="F"), b.copy(order="F")
+    info2 = hb.dposv("L", n, 1, a2, n, x2, n)
+    assert it == -3 and info1 == info2 > 0
+    assert same_bits(a1, a2)
+
+
+def test_mixed_quick_returns_and_invalid(hb):
+    a = np.ones(16)
+    x = np.full(16, 7.0)
+    ipiv = np.zeros(4, np.int32)
+    assert hb.dgesv_mixed(0, 1, a, 1, ipiv, a, 1, x, 1) == (0, 0)
+    assert np.all(x == 7.0)
+    with hb.ErrorCapture() as cap:
+        assert hb.dgesv_mixed(-1, 1, a, 1, ipiv, a, 1, x, 1)[0] == -1
+        assert hb.dgesv_mixed(4, -1, a, 4, ipiv, a, 4, x, 4)[0] == -2
+        assert hb.dgesv_mixed(4, 1, a, 3, ipiv, a, 4, x, 4)[0] == -4
+        assert hb.dgesv_mixed(4, 1, a, 4, ipiv, a, 3, x, 4)[0] == -7
+        assert hb.dgesv_mixed(4, 1, a, 4, ipiv, a, 4, x, 3)[0] == -9
+        assert hb.dposv_mixed("X", 4, 1, a, 4, a, 4, x, 4)[0] == -1
+        assert hb.dposv_mixed("L", 4, 1, a, 3, a, 4, x, 4)[0] == -5
+        assert hb.dposv_mixed("L", 4, 1, a, 4, a, 4, x, 3)[0] == -9
+    assert cap.errors == [("DGESV_MIXED", 1), ("DGESV_MIXED", 2), ("DGESV_MIXED", 4),
+                          ("DGESV_MIXED", 7), ("DGESV_MIXED", 9), ("DPOSV_MIXED", 1),
+                          ("DPOSV_MIXED", 5), ("DPOSV_MIXED", 9)]
+    assert np.all(x == 7.0)
