@@ -218,6 +218,7 @@ __global__ void AdjustPivotsKernel(int* ipiv, int begin, int end, int delta) {
 constexpr int kLeafThreads = 512;
 constexpr int kLeafMaxRows = 1024;  // rows per CTA
 constexpr int kLeafMaxP = 64;       // CTAs per panel (m <= 65536)
+constexpr int kLeafMaxCluster = 16; // CTAs of the cluster variant (m <= 16384)
 constexpr int kLeafW = 16;
 
 template <typename T>
@@ -233,13 +234,18 @@ struct LeafArgs {
   int* timeout_flag;
 };
 
-template <typename T>
+// kCluster: the P CTAs form one thread-block cluster and exchange their
+// candidates through distributed shared memory (each publishes into its own
+// shared slot, one cluster barrier, then every CTA reads the P slots), which
+// replaces the global-memory slots and polling of the cooperative variant.
+template <typename T, bool kCluster>
 __global__ void __launch_bounds__(kLeafThreads)
     GetrfLeafPanelKernel(LeafArgs<T> p) {
   extern __shared__ __align__(16) uint8_t leaf_smem[];
   T* sp = reinterpret_cast<T*>(leaf_smem);  // column-major [w][R]
   __shared__ T s_piv[kLeafW], s_rowj[kLeafW];
   __shared__ T s_cand[kLeafMaxP * (2 * kLeafW + 2)];
+  __shared__ T s_slot[2 * (2 * kLeafW + 2)];  // kCluster: own slot per parity
   __shared__ T s_wv[kLeafThreads / 32];
   __shared__ int s_wi[kLeafThreads / 32];
   __shared__ int s_p, s_abort;
@@ -253,9 +259,18 @@ __global__ void __launch_bounds__(kLeafThreads)
   unsigned int* tags = p.tags;
 
   if (threadIdx.x == 0) s_abort = 0;
-  for (int c = 0; c < w; ++c)
-    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x)
-      sp[c * R + lr] = p.a[(r0 + lr) + c * p.lda];
+  for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+    // All of a row's loads in flight before its shared-memory stores.
+    T v[kLeafW];
+#pragma unroll
+    for (int c = 0; c < kLeafW; ++c)
+      if (c < w) v[c] = p.a[(r0 + lr) + c * p.lda];
+#pragma unroll
+    for (int c = 0; c < kLeafW; ++c)
+      if (c < w) sp[c * R + lr] = v[c];
+  }
+  // kCluster: every CTA of the cluster is running before any remote access.
+  if constexpr (kCluster) cooperative_groups::this_cluster().sync();
   __syncthreads();
 
   for (int j = 0; j < w; ++j) {
@@ -276,11 +291,20 @@ __global__ void __launch_bounds__(kLeafThreads)
     }
     if (threadIdx.x % 32 == 0) { s_wv[threadIdx.x / 32] = bv; s_wi[threadIdx.x / 32] = bi; }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int q = 1; q < kLeafThreads / 32; ++q)
-        if (Better(s_wv[q], s_wi[q], bv, bi)) { bv = s_wv[q]; bi = s_wi[q]; }
-      s_p = bi;
-      s_wv[0] = bv;
+    if (threadIdx.x < 32) {
+      // The order of the reduction is immaterial: Better is a total order.
+      bv = threadIdx.x < kLeafThreads / 32 ? s_wv[threadIdx.x] : T(-1);
+      bi = threadIdx.x < kLeafThreads / 32 ? s_wi[threadIdx.x] : 0x7fffffff;
+      for (int off = 16; off > 0; off >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (Better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+      }
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        s_p = bi;
+        s_wv[0] = bv;
+      }
     }
     __syncthreads();
     // (b) exchange the candidates. A CTA holding the whole panel keeps them in
@@ -291,7 +315,32 @@ __global__ void __launch_bounds__(kLeafThreads)
     // round trip. A CTA can only overwrite a parity after every CTA has
     // published the next step, i.e. after all have read this one.
     const int ci = s_p;
-    if (P == 1) {
+    if (kCluster && P > 1) {
+      // Publish into the own slot of this parity; after the cluster barrier
+      // every CTA copies the P slots. A slot parity is rewritten two columns
+      // later, after the next barrier, when every CTA has read it.
+      cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+      T* mine = s_slot + par * slot_len;
+      if (threadIdx.x == 0) {
+        mine[0] = s_wv[0];
+        mine[1] = static_cast<T>(ci == 0x7fffffff ? -1 : ci);
+      }
+      if (threadIdx.x < w) {
+        mine[2 + threadIdx.x] =
+            (ci != 0x7fffffff) ? sp[threadIdx.x * R + (ci - r0)] : T(0);
+        if (j >= r0 && j < r1)
+          mine[2 + kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
+      }
+      cluster.sync();
+      for (int idx = threadIdx.x; idx < P * slot_len; idx += blockDim.x) {
+        const int q = idx / slot_len, e = idx - q * slot_len;
+        const T* peer = cluster.map_shared_rank(s_slot, q);
+        s_cand[idx] = peer[par * slot_len + e];
+      }
+      __syncthreads();
+      if (threadIdx.x < w)
+        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + kLeafW + threadIdx.x];
+    } else if (P == 1) {
       if (threadIdx.x == 0) {
         s_cand[0] = s_wv[0];
         s_cand[1] = static_cast<T>(ci == 0x7fffffff ? -1 : ci);
@@ -346,80 +395,70 @@ __global__ void __launch_bounds__(kLeafThreads)
         s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + kLeafW + threadIdx.x];
     }
     // (c) the global pivot: the reference's IAMAX over rows j..m-1; warp 0
-    // picks the winner among the candidates.
-    __syncthreads();
+    // picks the winner among the candidates and fills the pivot row.
     if (threadIdx.x < 32) {
+      __syncwarp();  // s_rowj was written by lanes of this warp
       T gv = T(-1);
       int gi = 0x7fffffff;
+      int wq = -1;
       for (int q = threadIdx.x; q < P; q += 32) {
         const T fi = s_cand[q * slot_len + 1];
         if (fi < T(0)) continue;
         const T v = s_cand[q * slot_len];
         const int i = static_cast<int>(fi);
-        if (Better(v, i, gv, gi)) { gv = v; gi = i; }
+        if (Better(v, i, gv, gi)) { gv = v; gi = i; wq = q; }
       }
-      int wq = (gi == 0x7fffffff) ? -1 : static_cast<int>(threadIdx.x);
       for (int off = 16; off > 0; off >>= 1) {
         const T ov = __shfl_down_sync(0xffffffffu, gv, off);
         const int oi = __shfl_down_sync(0xffffffffu, gi, off);
         const int oq = __shfl_down_sync(0xffffffffu, wq, off);
         if (Better(ov, oi, gv, gi)) { gv = ov; gi = oi; wq = oq; }
       }
-      if (threadIdx.x == 0) {
-        const T ajj = s_rowj[j];
-        if (isnan(fabs(ajj)) || gi == 0x7fffffff) gi = j;
-        s_p = gi;
-      }
+      gi = __shfl_sync(0xffffffffu, gi, 0);
+      wq = __shfl_sync(0xffffffffu, wq, 0);
+      const T ajj = s_rowj[j];
+      if (isnan(fabs(ajj)) || gi == 0x7fffffff) gi = j;
+      if (threadIdx.x == 0) s_p = gi;
+      // The winner's slot holds row gi (row j's own values if gi == j).
+      if (threadIdx.x < w)
+        s_piv[threadIdx.x] = (gi == j) ? s_rowj[threadIdx.x]
+                                       : s_cand[wq * slot_len + 2 + threadIdx.x];
     }
     __syncthreads();
     const int piv = s_p;
-    if (threadIdx.x < w) {
-      if (piv == j) {
-        s_piv[threadIdx.x] = s_rowj[threadIdx.x];
-      } else {
-        // The winner's slot holds row piv.
-        T val = T(0);
-        for (int q = 0; q < P; ++q) {
-          const T fi = s_cand[q * slot_len + 1];
-          if (fi >= T(0) && static_cast<int>(fi) == piv) val = s_cand[q * slot_len + 2 + threadIdx.x];
-        }
-        s_piv[threadIdx.x] = val;
-      }
-    }
-    __syncthreads();
     const T pivot = s_piv[j];
     if (cta == 0 && threadIdx.x == 0) {
       p.ipiv[j] = piv + 1;
       if (pivot == T(0) && *p.info == 0) *p.info = p.info_base + j + 1;
     }
-    if (pivot != T(0)) {
-      // (d) interchange rows j and piv across the leaf's columns.
-      if (piv != j && threadIdx.x < w) {
-        if (piv >= r0 && piv < r1) sp[threadIdx.x * R + (piv - r0)] = s_rowj[threadIdx.x];
-        if (j >= r0 && j < r1) sp[threadIdx.x * R + (j - r0)] = s_piv[threadIdx.x];
-      }
-      __syncthreads();
-      // (e) column j below the diagonal: * (1/pivot), or / pivot if tiny.
-      const bool tiny = !(fabs(pivot) >= Sfmin<T>());
-      const T rinv = T(1) / pivot;
-      for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
-        if (r0 + lr <= j) continue;
-        T& x = sp[j * R + lr];
-        x = tiny ? x / pivot : x * rinv;
-      }
+    // (d) interchange rows j and piv across the leaf's columns.
+    if (pivot != T(0) && piv != j && threadIdx.x < w) {
+      if (piv >= r0 && piv < r1) sp[threadIdx.x * R + (piv - r0)] = s_rowj[threadIdx.x];
+      if (j >= r0 && j < r1) sp[threadIdx.x * R + (j - r0)] = s_piv[threadIdx.x];
     }
     __syncthreads();
-    // (f) rank-1 update of columns j+1..w-1 (AXPY with alpha = -a(j, k)).
-    // Each thread owns rows; the column loop carries no index arithmetic.
+    // (e) column j below the diagonal: * (1/pivot), or / pivot if tiny (not
+    // for a zero pivot); (f) rank-1 update of columns j+1..w-1 (AXPY with
+    // alpha = -a(j, k)). A thread scales and updates its own rows, so the
+    // next barrier is the next column's first one.
+    const bool scale = pivot != T(0);
+    const bool tiny = !(fabs(pivot) >= Sfmin<T>());
+    const T rinv = T(1) / pivot;
     const int len = p.m - j - 1;
     for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
       if (r0 + lr <= j) continue;
-      const T x = sp[j * R + lr];
+      T x = sp[j * R + lr];
+      if (scale) {
+        x = tiny ? x / pivot : x * rinv;
+        sp[j * R + lr] = x;
+      }
       for (int k = j + 1; k < w; ++k)
         sp[k * R + lr] = Axpy(sp[k * R + lr], -s_piv[k], x, len, p.lanes);
     }
-    __syncthreads();
   }
+  __syncthreads();
+  // kCluster: no CTA exits while a peer may still read its slot.
+  if constexpr (kCluster) cooperative_groups::this_cluster().sync();
   for (int c = 0; c < w; ++c)
     for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x)
       p.a[(r0 + lr) + c * p.lda] = sp[c * R + lr];
@@ -588,11 +627,35 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
     return;
   }
   const size_t smem = static_cast<size_t>(w) * R * sizeof(T);
+  const int smem_max = kLeafW * kLeafMaxRows * static_cast<int>(sizeof(T));
+  static int max_cluster = 0;
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(GetrfLeafPanelKernel<T>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kLeafW * kLeafMaxRows * static_cast<int>(sizeof(T)));
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true>,
+                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    // The largest cluster of full-size leaf CTAs the device can co-schedule.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kLeafMaxCluster);
+    cfg.blockDim = dim3(kLeafThreads);
+    cfg.dynamicSmemBytes = smem_max;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = kLeafMaxCluster;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int size = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&size, GetrfLeafPanelKernel<T, true>,
+                                             &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      size = 0;
+    }
+    max_cluster = std::min(size, kLeafMaxCluster);
     configured = true;
   }
   LeafArgs<T> args;
@@ -610,15 +673,30 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
   args.tags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(args.xchg) +
                                               slot_bytes);
   args.timeout_flag = ctx.dev_status;
-  if (P > 1) {
+  if (P > 1 && P <= max_cluster) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P);
+    cfg.blockDim = dim3(kLeafThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx.stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = P;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    Failed(cudaLaunchKernelEx(&cfg, GetrfLeafPanelKernel<T, true>, args),
+           "getrf leaf (cluster)");
+  } else if (P > 1) {
     cudaMemsetAsync(args.tags, 0, sizeof(unsigned int) * 2 * P, ctx.stream);
     void* kargs[] = {&args};
     Failed(cudaLaunchCooperativeKernel(
-               reinterpret_cast<void*>(GetrfLeafPanelKernel<T>), P,
+               reinterpret_cast<void*>(GetrfLeafPanelKernel<T, false>), P,
                kLeafThreads, kargs, smem, ctx.stream),
            "getrf leaf (cooperative)");
   } else {
-    GetrfLeafPanelKernel<T><<<1, kLeafThreads, smem, ctx.stream>>>(args);
+    GetrfLeafPanelKernel<T, false><<<1, kLeafThreads, smem, ctx.stream>>>(args);
   }
   CountLaunch();
   LaunchFailed("getrf leaf");

@@ -42,7 +42,7 @@ namespace hb {
 namespace {
 
 constexpr int kTb = 64;         // diagonal block of the refinement solves
-constexpr int kTrsvRhs = 16;    // right-hand sides per solve launch
+constexpr int kTrsvRhs = 64;    // right-hand sides per solve launch
 constexpr int kTrsvThreads = 256;
 constexpr int kResRows = 128;   // residual GEMV: rows per CTA
 constexpr int kResK = 256;      // residual GEMV: k per CTA
@@ -253,62 +253,70 @@ __global__ void __launch_bounds__(kTb)
 // Triangular solve T x = x in place for nrhs <= kTrsvRhs columns of x, with
 // T the lower (forward) or upper (backward) triangle of w and inv the
 // inverses of its diagonal blocks. Cooperative: all CTAs are resident; each
-// step solves one block row redundantly in every CTA (CTA 0 stores it) and
-// then updates the CTA's share of the remaining rows; a grid barrier ends
-// the step. x is read and written through L2 only (.cg), since rows change
-// owner between steps.
+// step solves one block row redundantly in every CTA (x_b = inv_b * x_b from
+// shared memory; CTA 0 stores it) and then updates the CTA's share of the
+// remaining rows, one row per thread with the block row's 64 factor entries
+// in registers; a grid barrier ends the step. x is read and written through
+// L2 only (.cg), since rows change owner between steps.
+constexpr int kTrsvSmem = (kTb * kTb + 2 * kTb * kTrsvRhs) * 8;
 template <bool kLower>
 __global__ void __launch_bounds__(kTrsvThreads)
     BlockTrsvKernel(int n, int nrhs, const double* w, long long ldw,
                     const double* inv, double* x, long long ldx,
                     unsigned int* barrier, int* timeout_flag) {
-  __shared__ double sb[kTb][kTrsvRhs];
-  __shared__ double sx[kTb][kTrsvRhs];
+  extern __shared__ double trsv_smem[];
+  double* si = trsv_smem;              // inv block, column-major kTb x kTb
+  double* sb = si + kTb * kTb;         // sb[q * kTb + r]
+  double* sx = sb + kTb * kTrsvRhs;    // sx[q * kTb + r]
   const int nblk = (n + kTb - 1) / kTb;
   unsigned int gen = 0;
   for (int step = 0; step < nblk; ++step) {
     const int blk = kLower ? step : nblk - 1 - step;
     const int r0 = blk * kTb, bs = min(kTb, n - r0);
-    for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+    const double* ib = inv + static_cast<long long>(blk) * kTb * kTb;
+    for (int idx = threadIdx.x; idx < kTb * kTb; idx += kTrsvThreads) si[idx] = ib[idx];
+    for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
       const int r = idx % kTb, q = idx / kTb;
-      sb[r][q] = (r < bs && q < nrhs) ? __ldcg(x + r0 + r + q * ldx) : 0.0;
+      sb[idx] = r < bs ? __ldcg(x + r0 + r + q * ldx) : 0.0;
     }
     __syncthreads();
-    const double* ib = inv + static_cast<long long>(blk) * kTb * kTb;
-    for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+    for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
       const int r = idx % kTb, q = idx / kTb;
-      double s = 0.0;
-      if (q < nrhs) {
-        for (int c = 0; c < bs; ++c) s = fma(ib[r + c * kTb], sb[c][q], s);
+      const double* bq = sb + q * kTb;
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+      for (int c = 0; c < kTb; c += 2) {
+        s0 = fma(si[r + c * kTb], bq[c], s0);
+        s1 = fma(si[r + (c + 1) * kTb], bq[c + 1], s1);
       }
-      sx[r][q] = s;
+      sx[idx] = s0 + s1;
     }
     __syncthreads();
     if (blockIdx.x == 0) {
-      for (int idx = threadIdx.x; idx < kTb * kTrsvRhs; idx += kTrsvThreads) {
+      for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
         const int r = idx % kTb, q = idx / kTb;
-        if (r < bs && q < nrhs) __stcg(x + r0 + r + q * ldx, sx[r][q]);
+        if (r < bs) __stcg(x + r0 + r + q * ldx, sx[idx]);
       }
     }
     const int lo = kLower ? r0 + bs : 0, hi = kLower ? n : r0;
     for (int i = lo + blockIdx.x * kTrsvThreads + threadIdx.x; i < hi;
          i += gridDim.x * kTrsvThreads) {
-      double acc[kTrsvRhs];
-#pragma unroll
-      for (int q = 0; q < kTrsvRhs; ++q) acc[q] = 0.0;
       const double* wi = w + i + static_cast<long long>(r0) * ldw;
-      for (int c = 0; c < bs; ++c) {
-        const double l = wi[static_cast<long long>(c) * ldw];
+      double l[kTb];
 #pragma unroll
-        for (int q = 0; q < kTrsvRhs; ++q)
-          if (q < nrhs) acc[q] = fma(l, sx[c][q], acc[q]);
-      }
+      for (int c = 0; c < kTb; ++c)
+        l[c] = c < bs ? wi[static_cast<long long>(c) * ldw] : 0.0;
+      for (int q = 0; q < nrhs; ++q) {
+        const double* xq = sx + q * kTb;
+        double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-      for (int q = 0; q < kTrsvRhs; ++q)
-        if (q < nrhs) {
-          double* xi = x + i + q * ldx;
-          __stcg(xi, __ldcg(xi) - acc[q]);
+        for (int c = 0; c < kTb; c += 2) {
+          a0 = fma(l[c], xq[c], a0);
+          a1 = fma(l[c + 1], xq[c + 1], a1);
         }
+        double* xi = x + i + q * ldx;
+        __stcg(xi, __ldcg(xi) - (a0 + a1));
+      }
     }
     if (!GridBarrier(barrier, gridDim.x, ++gen, timeout_flag)) return;
   }
@@ -477,11 +485,15 @@ void BlockTrsv(bool lower, int n, int nrhs, const double* w, long long ldw,
   Context& ctx = Ctx();
   static int grid = 0;
   if (grid == 0) {
+    cudaFuncSetAttribute(BlockTrsvKernel<true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem);
+    cudaFuncSetAttribute(BlockTrsvKernel<false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem);
     int lo = 0, up = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, BlockTrsvKernel<true>,
-                                                  kTrsvThreads, 0);
+                                                  kTrsvThreads, kTrsvSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, BlockTrsvKernel<false>,
-                                                  kTrsvThreads, 0);
+                                                  kTrsvThreads, kTrsvSmem);
     grid = ctx.num_sms * std::max(1, std::min({lo, up, 2}));
   }
   int nn = n;
@@ -495,7 +507,8 @@ void BlockTrsv(bool lower, int n, int nrhs, const double* w, long long ldw,
     cudaMemsetAsync(barrier, 0, sizeof(unsigned int), ctx.stream);
     void* args[] = {&nn, &nr, const_cast<double**>(&w), &lw,
                     const_cast<double**>(&inv), &xq, &lx, &barrier, &flag};
-    Failed(cudaLaunchCooperativeKernel(fn, grid, kTrsvThreads, args, 0, ctx.stream),
+    Failed(cudaLaunchCooperativeKernel(fn, grid, kTrsvThreads, args, kTrsvSmem,
+                                       ctx.stream),
            "mixed triangular solve");
     CountLaunch();
   }
@@ -585,6 +598,7 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
   MixedSolve(lu, n, nrhs, bf, b, ldb, x, ldx);  // x = A^{-1} b, reduced precision
   std::vector<std::vector<double>> nm;
   std::vector<double> dprev(nrhs, INFINITY);
+  std::vector<char> settled_col(nrhs, 0);
   const double* mats[3] = {x, bf.r, bf.d};
   const long long lds[3] = {ldx, bf.ldr, bf.ldr};
   for (int it = 0; it < kItMax; ++it) {
@@ -594,12 +608,15 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
     AxpyMatrixKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(n, nrhs, bf.d, bf.ldr,
                                                                   x, ldx);
     CountLaunch();
+    // A column is done once it has met both tests; later corrections only
+    // move it within the noise of the FP64 residual.
     bool done = true;
     for (int q = 0; q < nrhs; ++q) {
       const double xn = nm[0][q], rn = nm[1][q], dn = nm[2][q];
       const bool backward = rn <= xn * cte;  // false on NaN
       const bool settled = dn <= 0x1p-52 * xn || dn > 0.5 * dprev[q];
-      if (!(backward && settled)) done = false;
+      if (backward && settled) settled_col[q] = 1;
+      if (!settled_col[q]) done = false;
       dprev[q] = dn;
     }
     if (done) return it + 1;
