@@ -1,22 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the level-3 hot path on B200 (one JSON line on rank 0).
 
-Headline metric: FP64-accurate TFLOP/s of DGEMM at M = N = K = 8192 (column-
-major NN, A, B, C uniform[-1, 1] from a seed, alpha 1.5, beta 0.5), i.e.
-2*8192^3 useful FP64 flops per step, on the fastest FP64-accurate path of the
-library (the plain FP64 tensor-pipe GEMM; the emulated path reports beside
-it when available). The dgesv n=16384 part of the metric is reported in the
-"dgesv" object when enabled.
+Metric: FP64-accurate TFLOP/s, dgemm n=8192 and dgesv n=16384, emulated /
+mixed against plain.
+
+Headline (`value`): DGEMM M = N = K = 8192, column-major NN, C = A B, with
+A and B entries u * 2^e (u uniform[-1, 1], e uniform in {-8..8}, seeded), on
+the emulated-FP64 path (Ozaki INT8 slices on tcgen05, slice count chosen
+automatically) - 2 * 8192^3 useful FP64 flops per step. "FP64-accurate": its
+normwise error against a double-double product of 64 sampled columns must not
+exceed the plain FP64 path's error on the same inputs (both are reported).
 
 value  : device-timed, inputs resident in HBM, CUDA events on the library's
          stream, max over ranks; whole-job TFLOP/s (sum over ranks).
-e2e    : the same metric through the public C ABI with pinned HOST buffers:
-         every step copies A, B, C in and C out inside the timed region.
-Replicas only: every rank runs its own 8192^3 product (weak scaling).
+e2e    : the same product through the public C ABI with pinned HOST buffers
+         (A, B copied in and C copied out inside the timed region).
+plain  : the plain FP64 tensor-pipe DGEMM (bit-identical to the reference)
+         on the same inputs, and its error.
+dgesv  : n = 16384, A = H1 diag(s) H2 (H1, H2 products of 4 Householder
+         reflectors, s geometric from 1 to 1/cond): the plain FP64 dgesv
+         (bit-identical to the reference's LU) against the mixed-precision
+         solver, forward errors against the known solution, iterations; and
+         dposv on SPD A = G G^T / n + 1e-3 I.
+Replicas only: every rank runs its own problems (weak scaling).
 
 --impl reference times the reference's CPU implementation of the path on this
-host's cores (the oracle port of the reference's hot path, all threads) on a
-bounded sample of the same workload.
+host's cores (the oracle port of the reference's DGEMM with its per-element
+order, all threads) on a bounded column sample of the same workload.
 """
 import argparse
 import datetime
@@ -34,19 +44,24 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_DEFAULT = 8192
-ALPHA, BETA = 1.5, 0.5
+GESV_N_DEFAULT = 16384
+SPREAD = 8
 METRIC = "FP64-accurate TFLOP/s: dgemm n=8192, dgesv n=16384; emulated/mixed vs plain"
+FALLBACK_BF16_TFLOPS = 1590.0
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=N_DEFAULT)
-    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--gesv-n", type=int, default=GESV_N_DEFAULT)
+    p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-dgesv", action="store_true")
+    p.add_argument("--no-sweep", action="store_true")
     return p.parse_args()
 
 
@@ -161,6 +176,11 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def spread_matrix(rng, rows, cols, spread):
+    e = rng.integers(-spread, spread + 1, (rows, cols))
+    return np.asfortranarray(rng.uniform(-1, 1, (rows, cols)) * np.exp2(e))
+
+
 def cpu_dgemm_sample(n, cols, steps, threads):
     """TFLOP/s of the reference's DGEMM order (oracle port) on an n x cols x n
     slice of the workload (a bounded sample: cols of the n output columns)."""
@@ -168,20 +188,24 @@ def cpu_dgemm_sample(n, cols, steps, threads):
     orc = Oracle()
     orc.set_threads(threads)
     rng = np.random.default_rng(7)
-    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
-    b = np.asfortranarray(rng.uniform(-1, 1, (n, cols)))
-    c = np.asfortranarray(rng.uniform(-1, 1, (n, cols)))
-    orc.dgemm("N", "N", n, cols, n, ALPHA, a, n, b, n, BETA, c, n)  # warm-up
+    a = spread_matrix(rng, n, n, SPREAD)
+    b = spread_matrix(rng, n, cols, SPREAD)
+    c = np.zeros((n, cols), order="F")
+    orc.dgemm("N", "N", n, cols, n, 1.0, a, n, b, n, 0.0, c, n)  # warm-up
     best = float("inf")
     for _ in range(steps):
         t0 = time.perf_counter()
-        orc.dgemm("N", "N", n, cols, n, ALPHA, a, n, b, n, BETA, c, n)
+        orc.dgemm("N", "N", n, cols, n, 1.0, a, n, b, n, 0.0, c, n)
         best = min(best, time.perf_counter() - t0)
     flops = 2.0 * n * cols * n
-    return flops / best / 1e12, f"dgemm NN {n}x{cols}x{n} (1/{n // cols} of the output columns), best of {steps}"
+    return flops / best / 1e12, (f"dgemm NN {n}x{cols}x{n} (1/{n // cols} of the output "
+                                 f"columns), best of {steps}")
 
 
-# ---------------------------------------------------------------------------
+def workload_name(n):
+    return (f"dgemm NN M=N=K={n}, C = A B, A and B entries u*2^e (u~U[-1,1], "
+            f"e~U{{-{SPREAD}..{SPREAD}}}), FP64-accurate")
+
 
 def run_reference(args):
     world, rank, local = dist_setup()
@@ -190,15 +214,14 @@ def run_reference(args):
     threads = cpu_threads()
     n = args.n
     cols = max(64, n // 8)
-    steps = max(1, args.steps if args.steps < 5 else 3)
+    steps = max(1, min(args.steps, 3))
     tf, sample = cpu_dgemm_sample(n, cols, steps, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": tf, "unit": "TFLOP/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True,
         "ms_per_step": 2.0 * n ** 3 / (tf * 1e12) * 1e3, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1])",
-        "config": {"workload": f"dgemm NN M=N=K={n} alpha=1.5 beta=0.5 (column-major)",
-                   "parallelism": "host threads"},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": workload_name(n), "parallelism": "host threads"},
         "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
@@ -210,6 +233,253 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# GPU arm.
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"bf16_tflops": FALLBACK_BF16_TFLOPS, "hbm_gbs": 6650.0}, "fallback"
+
+
+def device_spread(torch, n, spread, gen):
+    u = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+    e = torch.randint(-spread, spread + 1, (n * n,), device="cuda", generator=gen)
+    return u * torch.exp2(e.to(torch.float64))
+
+
+def normwise_error(torch, hb, a, b, c, n, cols):
+    """||C[:, cols] - (A B)[:, cols]||_F / (||A||_F ||B[:, cols]||_F) with the
+    exact product from the library's double-double reference kernel."""
+    ref = torch.empty(n * len(cols), dtype=torch.float64, device="cuda")
+    ci = torch.tensor(cols, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    hb.dgemm_ddref("N", "N", n, n, a, n, b, n, n, ci, ref, n)
+    cm = c.view(n, n)[cols]        # rows of the row-major view = columns of C
+    bm = b.view(n, n)[cols]
+    num = torch.linalg.norm(cm.reshape(-1) - ref)
+    den = torch.linalg.norm(a) * torch.linalg.norm(bm.reshape(-1))
+    return float((num / den).item())
+
+
+def timed(torch, stream, fn, steps):
+    """Average milliseconds of fn() over `steps` calls, CUDA events on the
+    library's stream, synchronized on both sides."""
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def int8_products(slices):
+    return slices * (slices + 1) // 2
+
+
+def run_dgemm(args, torch, hb, stream, dist, world, rank, local):
+    """The headline: FP64-accurate DGEMM, emulated and plain, same inputs."""
+    n = args.n
+    flops = 2.0 * n ** 3
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    A = device_spread(torch, n, SPREAD, g)
+    B = device_spread(torch, n, SPREAD, g)
+    C = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    Cp = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()  # inputs come from torch's stream
+    cols = list(range(0, n, max(1, n // 64)))[:64]
+    used = [0]
+
+    def emulated():
+        used[0] = hb.dgemm_emulated("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, 0)
+
+    def plain():
+        hb.dgemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, Cp, n)
+
+    for _ in range(args.warmup):
+        emulated()
+        plain()
+    torch.cuda.synchronize()
+    err_emul = normwise_error(torch, hb, A, B, C, n, cols)
+    err_plain = normwise_error(torch, hb, A, B, Cp, n, cols)
+
+    # Timed region: the emulated path, with the slice-product kernel timed.
+    props = torch.cuda.get_device_properties(local)
+    clocks = Clocks(f"GPU-{props.uuid}" if hasattr(props, "uuid") else local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = hb.launch_count()
+    hb.kernel_timer(hb.KERNEL_OZAKI_GEMM)
+    hb.kernel_timer_read()
+    ms = timed(torch, stream, emulated, args.steps)
+    oz_ms, oz_launches = hb.kernel_timer_read()
+    hb.kernel_timer(0)
+    launches = hb.launch_count() - launches0
+    dist.barrier()
+    clk = clocks.stop()
+    ms_max = dist.max(ms)
+    value = world * flops / (ms_max * 1e-3) / 1e12
+
+    # Plain FP64 path on the same inputs, DMMA kernel timed.
+    hb.kernel_timer(hb.KERNEL_DMMA_GEMM)
+    hb.kernel_timer_read()
+    ms_plain = dist.max(timed(torch, stream, plain, max(3, args.steps // 2)))
+    dm_ms, dm_launches = hb.kernel_timer_read()
+    hb.kernel_timer(0)
+    S = used[0]
+    out = {
+        "value": value, "ms": ms_max, "slices": S, "launches": launches, "clocks": clk,
+        "err_emulated": err_emul, "err_plain": err_plain,
+        "fp64_accurate": bool(err_emul <= err_plain),
+        "plain": {"tflops": world * flops / (ms_plain * 1e-3) / 1e12, "ms": ms_plain,
+                  "err": err_plain},
+        "ozaki_kernel_ms_per_launch": oz_ms / max(1, oz_launches),
+        "ozaki_launches_per_step": oz_launches / args.steps,
+        "dmma_kernel_ms_per_launch": dm_ms / max(1, dm_launches),
+    }
+
+    # Slice sweep S = 3..8 (one warm and one timed call each) and the wider
+    # exponent spread.
+    if not args.no_sweep and rank == 0:
+        sweep = {}
+        for s in range(3, 9):
+            def one(s=s):
+                hb.dgemm_emulated("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, s)
+            one()
+            t = timed(torch, stream, one, 1)
+            sweep[str(s)] = {"tflops": flops / (t * 1e-3) / 1e12,
+                             "err": normwise_error(torch, hb, A, B, C, n, cols)}
+        out["sweep"] = sweep
+        g30 = torch.Generator(device="cuda").manual_seed(99)
+        A30 = device_spread(torch, n, 30, g30)
+        B30 = device_spread(torch, n, 30, g30)
+        torch.cuda.synchronize()
+        s30 = hb.dgemm_emulated("N", "N", n, n, n, 1.0, A30, n, B30, n, 0.0, C, n, 0)
+        e30 = normwise_error(torch, hb, A30, B30, C, n, cols)
+        hb.dgemm("N", "N", n, n, n, 1.0, A30, n, B30, n, 0.0, Cp, n)
+        p30 = normwise_error(torch, hb, A30, B30, Cp, n, cols)
+        out["spread30"] = {"slices": s30, "err_emulated": e30, "err_plain": p30}
+        del A30, B30
+
+    # End to end through the C ABI with pinned host buffers: A, B in, C out
+    # (beta = 0: C is not read).
+    ha = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+    hbuf = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+    hc = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+    ha.copy_(A.cpu())
+    hbuf.copy_(B.cpu())
+    an, bn, cn = ha.numpy(), hbuf.numpy(), hc.numpy()
+
+    def e2e_call():
+        hb.dgemm_emulated("N", "N", n, n, n, 1.0, an, n, bn, n, 0.0, cn, n, 0)
+
+    e2e_call()
+    dist.barrier()
+    e2e_ms = dist.max(timed(torch, stream, e2e_call, args.e2e_steps))
+    out["e2e"] = {"value": world * flops / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                  "h2d_bytes_per_step": 2 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n}
+    del A, B, C, Cp
+    return out
+
+
+def householder_device(torch, n, cond, seed):
+    """A = H1 diag(s) H2 (column-major, flat): H1, H2 products of 4 Householder
+    reflectors from seeded Gaussian vectors, s geometric from 1 to 1/cond."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    s = torch.logspace(0.0, -float(np.log10(cond)), n, dtype=torch.float64, device="cuda")
+    M = torch.diag(s)  # row-major storage of M; reflectors keep it dense
+    for side in range(2):
+        for _ in range(4):
+            v = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+            v /= torch.linalg.norm(v)
+            if side == 0:
+                M -= 2.0 * torch.outer(v, v @ M)
+            else:
+                M -= 2.0 * torch.outer(M @ v, v)
+    return M  # M's row-major storage is A^T column-major: solve with A = M^T
+
+
+def run_solvers(args, torch, hb, stream):
+    """dgesv and dposv at n = args.gesv_n: plain FP64 against mixed."""
+    n = args.gesv_n
+    res = {"n": n}
+    gesv_flops = lambda nrhs: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * nrhs
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cases = [(1e6, 1), (1e6, 64), (1e2, 1), (1e10, 1)]
+    mats = {}
+    for cond, nrhs in cases:
+        if cond not in mats:
+            mats[cond] = householder_device(torch, n, cond, 7)
+        M = mats[cond]                      # the matrix A is M^T (column-major data of M)
+        A = M.reshape(-1)
+        g = torch.Generator(device="cuda").manual_seed(3)
+        xt = torch.rand(nrhs, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        Bm = (M.t() @ xt.t()).t().contiguous()   # rows of Bm = columns of B = A xt
+        torch.cuda.synchronize()
+        out = {}
+        for kind in ("plain", "mixed"):
+            best = None
+            for _ in range(2):  # one warm-up, one timed
+                a = A.clone()
+                x = Bm.clone() if kind == "plain" else torch.zeros_like(Bm)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                if kind == "plain":
+                    info = hb.dgesv(n, nrhs, a, n, ipiv, x, n)
+                    it = None
+                else:
+                    info, it = hb.dgesv_mixed(n, nrhs, a, n, ipiv, Bm, n, x, n)
+                torch.cuda.synchronize()
+                best = time.perf_counter() - t0
+            err = float((torch.linalg.norm(x - xt) / torch.linalg.norm(xt)).item())
+            out[kind] = {"ms": best * 1e3, "tflops": gesv_flops(nrhs) / best / 1e12,
+                         "solves_per_s": 1.0 / best, "fwd_err": err, "info": info}
+            if it is not None:
+                out[kind]["iterations"] = it
+        out["speedup"] = out["plain"]["ms"] / out["mixed"]["ms"]
+        out["mixed_err_le_plain"] = bool(out["mixed"]["fwd_err"] <= out["plain"]["fwd_err"])
+        res[f"dgesv_cond{cond:g}_nrhs{nrhs}"] = out
+    del mats
+    # dposv: SPD A = G G^T / n + 1e-3 I.
+    g = torch.Generator(device="cuda").manual_seed(11)
+    G = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    S = G @ G.t() / n + 1e-3 * torch.eye(n, dtype=torch.float64, device="cuda")
+    del G
+    xt = torch.rand(1, n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    Bm = (S @ xt.t()).t().contiguous()
+    A = S.reshape(-1)
+    out = {}
+    posv_flops = n ** 3 / 3.0 + 2.0 * n * n
+    for kind in ("plain", "mixed"):
+        for _ in range(2):
+            a = A.clone()
+            x = Bm.clone() if kind == "plain" else torch.zeros_like(Bm)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if kind == "plain":
+                info, it = hb.dposv("L", n, 1, a, n, x, n), None
+            else:
+                info, it = hb.dposv_mixed("L", n, 1, a, n, Bm, n, x, n)
+            torch.cuda.synchronize()
+            best = time.perf_counter() - t0
+        err = float((torch.linalg.norm(x - xt) / torch.linalg.norm(xt)).item())
+        out[kind] = {"ms": best * 1e3, "tflops": posv_flops / best / 1e12, "fwd_err": err,
+                     "info": info}
+        if it is not None:
+            out[kind]["iterations"] = it
+    out["speedup"] = out["plain"]["ms"] / out["mixed"]["ms"]
+    res["dposv_spd_nrhs1"] = out
+    return res
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -217,65 +487,24 @@ def run_ours(args):
     dist = Dist(world, rank, local, "nccl")
     import hwyblas_b200 as hb
     lib = hb.lib()
-    n = args.n
-    flops = 2.0 * n ** 3
-    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
-    A = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-    B = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-    C0 = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-    C = C0.clone()
-    torch.cuda.synchronize()  # inputs come from torch's stream
     stream = torch.cuda.Stream()
     hb.set_stream(stream)
-    peak = float(lib.hwyblas_fp64_peak_tflops())
+    n = args.n
+    d = run_dgemm(args, torch, hb, stream, dist, world, rank, local)
 
-    def step():
-        hb.dgemm("N", "N", n, n, n, ALPHA, A, n, B, n, BETA, C, n)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    props = torch.cuda.get_device_properties(local)
-    clocks = Clocks(f"GPU-{props.uuid}" if hasattr(props, "uuid") else local)
-    dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    launches0 = hb.launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    dist.barrier()
-    clk = clocks.stop()
-    launches = hb.launch_count() - launches0
-    ms = e0.elapsed_time(e1) / args.steps
-    ms_max = dist.max(ms)
-    value = world * flops / (ms_max * 1e-3) / 1e12
-
-    # End to end through the C ABI with pinned host buffers.
-    ha = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
-    hbuf = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
-    hc = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
-    ha.copy_(A.cpu())
-    hbuf.copy_(B.cpu())
-    hc.copy_(C0.cpu())
-    an, bn, cn = ha.numpy(), hbuf.numpy(), hc.numpy()
-    hb.dgemm("N", "N", n, n, n, ALPHA, an, n, bn, n, BETA, cn, n)  # warm-up
-    dist.barrier()
-    torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.e2e_steps):
-        hb.dgemm("N", "N", n, n, n, ALPHA, an, n, bn, n, BETA, cn, n)
-    f1.record(stream)
-    f1.synchronize()
-    e2e_ms = dist.max(f0.elapsed_time(f1) / args.e2e_steps)
-    e2e = world * flops / (e2e_ms * 1e-3) / 1e12
+    peaks, peak_kind = measured_peaks()
+    int8_peak = 2.0 * float(peaks.get("bf16_tflops", FALLBACK_BF16_TFLOPS))
+    fp64_peak = float(lib.hwyblas_fp64_peak_tflops())
+    S = d["slices"]
+    # Dominant kernel: the slice-product GEMM. Algorithmic work = INT8
+    # multiply-adds of all S(S+1)/2 slice products, 2 n^3 ops each, spread
+    # over the launches of one step.
+    per_step_ops = int8_products(S) * 2.0 * n ** 3 if S > 0 else 0.0
+    per_launch_ops = per_step_ops / max(1.0, d["ozaki_launches_per_step"])
+    oz_ms = d["ozaki_kernel_ms_per_launch"]
+    achieved = per_launch_ops / (oz_ms * 1e-3) / 1e12 if oz_ms > 0 else None
+    dm_ms = d["dmma_kernel_ms_per_launch"]
+    dm_achieved = 2.0 * n ** 3 / (dm_ms * 1e-3) / 1e12 if dm_ms > 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -284,30 +513,50 @@ def run_ours(args):
         cpu = {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": sample}
 
+    solvers = None
+    if rank == 0 and world == 1 and not args.no_dgesv:
+        solvers = run_solvers(args, torch, hb, stream)
+
     if rank == 0:
-        achieved = flops / (ms * 1e-3) / 1e12
         line = {
-            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+            "metric": METRIC, "value": d["value"], "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded uniform[-1,1])",
-            "config": {"workload": f"dgemm NN M=N=K={n} alpha=1.5 beta=0.5, FP64 DMMA path "
-                                   "(bit-identical to the reference)",
-                       "path": "plain FP64 tensor pipe", "parallelism": f"replicas x{world}",
-                       "l2": "inputs (3 x 512 MiB) larger than L2"},
-            "e2e": {"value": e2e, "unit": "TFLOP/s", "h2d_bytes_per_step": 3 * 8 * n * n,
-                    "d2h_bytes_per_step": 8 * n * n},
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "dtype": "int8 slices -> f64", "data": "synthetic (seeded)",
+            "config": {"workload": workload_name(n), "path": "emulated FP64 (Ozaki INT8 "
+                       "slices on tcgen05), slices chosen automatically",
+                       "slices": S, "parallelism": f"replicas x{world}",
+                       "l2": "inputs (2 x 512 MiB FP64) larger than L2"},
+            "fp64_accurate": d["fp64_accurate"],
+            "error": {"emulated": d["err_emulated"], "plain": d["err_plain"],
+                      "measure": "normwise ||C - AB||_F / (||A||_F ||B||_F) on 64 columns "
+                                 "against a double-double product"},
+            "plain": d["plain"],
+            "speedup_vs_plain": d["plain"]["ms"] / d["ms"],
+            "e2e": d["e2e"],
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak,
+                         "unit": "TOPS (INT8)",
+                         "frac": achieved / int8_peak if achieved else None,
                          "traffic": None,
-                         "peak_source": "measured FP64 DMMA issue rate on this GPU "
-                                        "(hwyblas_fp64_peak_tflops); no FP64 figure in "
-                                        "MEASURED_PEAKS.json",
-                         "kernel": "DgemmDmmaKernel<true>"},
+                         "kernel": "OzakiGemmKernel (slice products, "
+                                   f"{d['ozaki_launches_per_step']:.0f} launches per step)",
+                         "peak_source": f"2 x bf16_tflops of {peak_kind} MEASURED_PEAKS "
+                                        "(INT8 dense rate = 2 x bf16)"},
+            "roofline_plain": {"bound": "tensor", "achieved": dm_achieved,
+                               "peak": fp64_peak, "unit": "TFLOP/s (FP64)",
+                               "frac": dm_achieved / fp64_peak if dm_achieved else None,
+                               "kernel": "DgemmDmmaKernel",
+                               "peak_source": "measured DMMA issue rate "
+                                              "(hwyblas_fp64_peak_tflops)"},
             "cpu_baseline": cpu,
-            "clocks": clk,
-            "gpu_launches": launches,
+            "clocks": d["clocks"],
+            "gpu_launches": d["launches"],
         }
+        if "sweep" in d:
+            line["slice_sweep"] = d["sweep"]
+            line["spread30"] = d["spread30"]
+        if solvers is not None:
+            line["solvers"] = solvers
         print(json.dumps(line), flush=True)
     dist.close()
     return 0

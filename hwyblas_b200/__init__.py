@@ -19,6 +19,8 @@ __all__ = [
     "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
+    "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
+    "KERNEL_LU_LEAF",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -43,7 +45,8 @@ from ._api import (  # noqa: E402  (needs lib())
     dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
     cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
     dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
-    set_mixed_slices,
+    set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
+    KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

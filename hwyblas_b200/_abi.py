@@ -47,6 +47,8 @@ PROTOTYPES = {
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),
+    "hwyblas_kernel_timer": (None, [I]),
+    "hwyblas_kernel_timer_read": (D, [PI]),
     "hwyblas_fp64_peak_tflops": (ctypes.c_double, []),
     "hwyblas_idamax_noalloc": (I, [I, P, I, P, P]),
 }

@@ -223,6 +223,21 @@ class ErrorCapture:
         return False
 
 
+KERNEL_DMMA_GEMM, KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF = 1, 2, 3
+
+
+def kernel_timer(family):
+    """Time every launch of a kernel family with CUDA events (0 = off)."""
+    lib().hwyblas_kernel_timer(int(family))
+
+
+def kernel_timer_read():
+    """(total milliseconds, launches) of the timed kernel since the last read."""
+    n = ctypes.c_int(0)
+    ms = lib().hwyblas_kernel_timer_read(ctypes.byref(n))
+    return float(ms), n.value
+
+
 def launch_count():
     """Kernels launched by the library so far (all threads)."""
     return int(lib().hwyblas_launch_count())

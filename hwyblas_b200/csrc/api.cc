@@ -16,6 +16,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "../../include/hwyblas_b200.h"
 #include "internal.h"
@@ -23,6 +26,30 @@
 namespace hb {
 
 std::atomic<uint64_t> g_launches{0};
+
+namespace {
+std::mutex g_timer_mu;
+int g_timer_family = kFamilyNone;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timer_events;
+}  // namespace
+
+cudaEvent_t KernelTimerStart(int family, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_timer_mu);
+  if (family != g_timer_family || family == kFamilyNone) return nullptr;
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  cudaEventRecord(e, stream);
+  return e;
+}
+
+void KernelTimerStop(cudaEvent_t start, cudaStream_t stream) {
+  if (start == nullptr) return;
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, stream);
+  std::lock_guard<std::mutex> lock(g_timer_mu);
+  g_timer_events.emplace_back(start, e);
+}
 
 namespace {
 
@@ -1000,6 +1027,29 @@ HWYBLAS_API int hwyblas_last_cuda_error(void) {
   const int e = c.last_error;
   c.last_error = 0;
   return e;
+}
+
+HWYBLAS_API void hwyblas_kernel_timer(int family) {
+  std::lock_guard<std::mutex> lock(hb::g_timer_mu);
+  hb::g_timer_family = family;
+}
+
+HWYBLAS_API double hwyblas_kernel_timer_read(int* launches) {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  {
+    std::lock_guard<std::mutex> lock(hb::g_timer_mu);
+    ev.swap(hb::g_timer_events);
+  }
+  double total = 0.0;
+  for (auto& pr : ev) {
+    float ms = 0.0f;
+    cudaEventSynchronize(pr.second);
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) total += ms;
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  if (launches != nullptr) *launches = static_cast<int>(ev.size());
+  return total;
 }
 
 HWYBLAS_API uint64_t hwyblas_launch_count(void) {

@@ -540,7 +540,9 @@ bool LaunchOzaki(const CUtensorMap& ma, const CUtensorMap& mb,
   }
   const long long tiles =
       static_cast<long long>((p.m + kEBM - 1) / kEBM) * ((p.n + kEBN - 1) / kEBN);
+  cudaEvent_t t0 = KernelTimerStart(kFamilyOzakiGemm, st);
   kernel<<<static_cast<unsigned>(tiles), kEThreads, Cfg::kSmem, st>>>(ma, mb, p);
+  KernelTimerStop(t0, st);
   CountLaunch();
   return !LaunchFailed("ozaki gemm");
 }

@@ -673,6 +673,7 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
   args.tags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(args.xchg) +
                                               slot_bytes);
   args.timeout_flag = ctx.dev_status;
+  cudaEvent_t t0 = KernelTimerStart(kFamilyLuLeaf, ctx.stream);
   if (P > 1 && P <= max_cluster) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P);
@@ -698,6 +699,7 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
   } else {
     GetrfLeafPanelKernel<T, false><<<1, kLeafThreads, smem, ctx.stream>>>(args);
   }
+  KernelTimerStop(t0, ctx.stream);
   CountLaunch();
   LaunchFailed("getrf leaf");
   if (n > w) {

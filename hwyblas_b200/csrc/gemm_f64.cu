@@ -575,7 +575,9 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   // TFLOP/s, getrf n = 16384 418 vs 440 ms.
   const unsigned grid =
       static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
+  cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
   DgemmDmmaKernel<<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  KernelTimerStop(t0, ctx.stream);
   CountLaunch();
   LaunchFailed("dgemm");
 }

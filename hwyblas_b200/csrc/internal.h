@@ -89,6 +89,19 @@ inline void CountLaunch(uint64_t n = 1) {
   g_launches.fetch_add(n, std::memory_order_relaxed);
 }
 
+// Kernel timer (instrumentation): when the timed family is enabled, the
+// launch sites of that kernel family bracket each launch with CUDA events on
+// their stream. KernelTimerStart returns the start event (nullptr when
+// disabled); KernelTimerStop records the stop event and keeps the pair.
+enum KernelFamily : int {
+  kFamilyNone = 0,
+  kFamilyDmmaGemm = 1,   // DgemmDmmaKernel
+  kFamilyOzakiGemm = 2,  // OzakiGemmKernel (all passes)
+  kFamilyLuLeaf = 3,     // GetrfLeafPanelKernel
+};
+cudaEvent_t KernelTimerStart(int family, cudaStream_t stream);
+void KernelTimerStop(cudaEvent_t start, cudaStream_t stream);
+
 // ---------------------------------------------------------------------------
 // Device-level routines (device pointers; stream-ordered on Ctx().stream).
 

@@ -258,6 +258,13 @@ HWYBLAS_API int hwyblas_last_cuda_error(void);
 /* Number of kernels the library has launched (all threads). No counterpart
  * in the reference; used to count launches inside timed regions. */
 HWYBLAS_API uint64_t hwyblas_launch_count(void);
+/* Kernel timer (instrumentation, no counterpart in the reference): while
+ * family f is selected (1 FP64 DMMA GEMM kernel, 2 emulated-GEMM slice-product
+ * kernel, 3 LU leaf kernel; 0 none), each launch of that kernel is bracketed
+ * by CUDA events on its stream. hwyblas_kernel_timer_read waits for them and
+ * returns the summed milliseconds (and the launch count), then forgets them. */
+HWYBLAS_API void hwyblas_kernel_timer(int family);
+HWYBLAS_API double hwyblas_kernel_timer_read(int* launches);
 /* Measured FP64 tensor-pipe throughput of the current device (TFLOP/s), from
  * a DMMA issue-rate loop; the FP64 roofline denominator. No counterpart in
  * the reference. */
