@@ -62,6 +62,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-dgesv", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv-mixed"],
+                   help="run one call of a hot-path piece and exit (for profilers): the LU "
+                        "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
+                        "gesv-n, each after one warm-up call")
     return p.parse_args()
 
 
@@ -562,8 +566,40 @@ def run_ours(args):
     return 0
 
 
+def run_case(args):
+    """One warm-up and one profiled call of a single hot-path piece."""
+    import torch
+    import hwyblas_b200 as hb
+    torch.cuda.set_device(0)
+    n = args.gesv_n
+    g = torch.Generator(device="cuda").manual_seed(1)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    if args.case == "leaf":
+        a0 = torch.rand(n * 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        call = lambda a: hb.dgetrf2(n, 16, a, n, ipiv)
+    else:
+        a0 = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        b = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+        x = torch.zeros_like(b)
+        if args.case == "getrf":
+            call = lambda a: hb.dgetrf(n, n, a, n, ipiv)
+        else:
+            call = lambda a: hb.dgesv_mixed(n, 1, a, n, ipiv, b, n, x, n)
+    for _ in range(2):
+        a = a0.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = call(a)
+        torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "n": n, "ms": (time.perf_counter() - t0) * 1e3,
+                      "result": r}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.case is not None:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

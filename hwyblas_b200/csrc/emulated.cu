@@ -430,16 +430,25 @@ __global__ void __launch_bounds__(kEThreads, 1)
             if (col < p.n) p.w[row + static_cast<long long>(col) * p.m] = sum[j] + comp[j];
           }
         } else {
+          // All loads of the chunk (column exponents, C) are issued before
+          // its stores, which the compiler cannot reorder them across.
+          int f[32];
+          double cin[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            sum[j] += comp[j];
+            const int col = n0 + cc * 32 + j;
+            f[j] = (col < p.n) ? p.col_exp[col] : kZeroExp;
+            cin[j] = (col < p.n && p.beta != 0.0) ? p.c[row + col * p.ldc] : 0.0;
+          }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int col = n0 + cc * 32 + j;
             if (col >= p.n) continue;
-            const int f = p.col_exp[col];
             double v = 0.0;
-            if (f != kZeroExp && e_row != kZeroExp) v = ldexp(sum[j] + comp[j], e_row + f + 4);
-            double* cp = p.c + row + col * p.ldc;
+            if (f[j] != kZeroExp && e_row != kZeroExp) v = ldexp(sum[j], e_row + f[j] + 4);
             const double r = p.alpha * v;
-            *cp = (p.beta == 0.0) ? r : fma(p.beta, *cp, r);
+            p.c[row + col * p.ldc] = (p.beta == 0.0) ? r : fma(p.beta, cin[j], r);
           }
         }
       }

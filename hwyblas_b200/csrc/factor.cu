@@ -128,79 +128,130 @@ __global__ void LaswpKernel(int n, T* a, long long lda, int i1, int i2,
   }
 }
 
-// LASWP for incx = 1 and at most 64 interchanges: the interchanges only move
-// data among the rows k1..k2 and their partners, so their net effect is one
-// permutation of at most 128 rows. Warp 0 of every block replays the
-// interchanges on a table of (row, row whose data it holds) in shared memory;
-// then the block's threads gather the permuted rows of their 32 columns in
-// one parallel pass (the values moved, and so the result, are the same).
-constexpr int kSwapMax = 64;
+// LASWP for incx = 1 and at most kSwapMax interchanges: the interchanges
+// only move data among the rows k1..k2 and their partners, so their net
+// effect is one permutation of at most 2 kSwapMax rows. Thread 0 of every
+// block replays the interchanges on a table of (row, row whose data it holds)
+// in shared memory - rows k1..k2 at fixed slots, partners outside found
+// through a small hash - and then each warp permutes whole columns: its lanes
+// read the table's source rows of a column into registers and write them to
+// the destination rows (the values moved, and so the result, are the same).
+constexpr int kSwapMax = 512;
+constexpr int kSwapTable = 2 * kSwapMax;
+constexpr int kSwapHash = 2048;  // power of two, > kSwapMax
+constexpr int kLaswpCols = 64;   // columns per block
 template <typename T>
 __global__ void __launch_bounds__(256)
     LaswpPermKernel(int n, T* a, long long lda, int k1, int k2,
                     const int* ipiv, const int* guard) {
   if (guard != nullptr && *guard != 0) return;
-  __shared__ int pos[2 * kSwapMax], src[2 * kSwapMax], piv[kSwapMax];
+  __shared__ int pos[kSwapTable], src[kSwapTable];
+  __shared__ int hkey[kSwapHash], hfirst[kSwapHash], spiv[kSwapMax], sslot[kSwapMax];
+  __shared__ int wsum[8];
   __shared__ int cnt;
-  __shared__ T tile[2 * kSwapMax][33];
   const int nb = k2 - k1 + 1;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (int t = lane; t < nb; t += 32) {
-      pos[t] = k1 + t;
-      src[t] = k1 + t;
-      piv[t] = ipiv[k1 - 1 + t];
-    }
-    int c = nb;
-    __syncwarp();
-    for (int i = k1; i <= k2; ++i) {
-      const int p = piv[i - k1];
-      if (p == i) continue;
-      int sp;
-      if (p >= k1 && p <= k2) {
-        sp = p - k1;
-      } else {
-        // Partner outside k1..k2: find it among the extra slots, or add it.
-        sp = -1;
-        for (int t0 = nb; t0 < c; t0 += 32) {
-          const int t = t0 + lane;
-          const unsigned hit = __ballot_sync(0xffffffffu, t < c && pos[t] == p);
-          if (hit != 0u) {
-            sp = t0 + __ffs(hit) - 1;
-            break;
-          }
-        }
-        if (sp < 0) {
-          sp = c;
-          if (lane == 0) {
-            pos[c] = p;
-            src[c] = p;
-          }
-          ++c;
-        }
+  for (int t = threadIdx.x; t < kSwapHash; t += blockDim.x) {
+    hkey[t] = -1;
+    hfirst[t] = 0x7fffffff;
+  }
+  __syncthreads();
+  // (1) Partners outside k1..k2 enter a hash (row -> first swap that names
+  // it); rows inside have fixed slots.
+  const int t0 = threadIdx.x;  // nb <= kSwapMax = 2 * blockDim.x: two swaps a thread
+  for (int t = t0; t < nb; t += blockDim.x) {
+    const int p = ipiv[k1 - 1 + t];
+    spiv[t] = p;
+    pos[t] = k1 + t;
+    src[t] = k1 + t;
+    if (p != k1 + t && (p < k1 || p > k2)) {
+      int hh = static_cast<int>((static_cast<unsigned>(p) * 40503u) & (kSwapHash - 1));
+      while (true) {
+        const int prev = atomicCAS(&hkey[hh], -1, p);
+        if (prev == -1 || prev == p) break;
+        hh = (hh + 1) & (kSwapHash - 1);
       }
-      __syncwarp();
-      if (lane == 0) {
-        const int si = i - k1;
-        const int t = src[si];
-        src[si] = src[sp];
-        src[sp] = t;
-      }
-      __syncwarp();
+      atomicMin(&hfirst[hh], t);
     }
-    if (lane == 0) cnt = c;
+  }
+  __syncthreads();
+  // (2) The first swap naming each outside row gets the next extra slot, in
+  // swap order: a block-wide prefix count of the first occurrences.
+  int flag[2] = {0, 0}, hs[2] = {-1, -1};
+  for (int r = 0; r < 2; ++r) {
+    const int t = t0 + r * blockDim.x;
+    if (t >= nb) continue;
+    const int pp = spiv[t];
+    if (pp == k1 + t || (pp >= k1 && pp <= k2)) continue;
+    int hh = static_cast<int>((static_cast<unsigned>(pp) * 40503u) & (kSwapHash - 1));
+    while (hkey[hh] != pp) hh = (hh + 1) & (kSwapHash - 1);
+    hs[r] = hh;
+    flag[r] = hfirst[hh] == t ? 1 : 0;
+  }
+  // Exclusive scan over t = 0..nb-1 of flag (t = t0 + r*blockDim.x).
+  int base = 0;
+  for (int r = 0; r < 2; ++r) {
+    int v = flag[r];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    int incl = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += o;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) {
+      if (w < warp) before += wsum[w];
+      total += wsum[w];
+    }
+    __syncthreads();
+    const int t = t0 + r * blockDim.x;
+    if (flag[r]) {
+      const int slot = nb + base + before + incl - v;
+      pos[slot] = spiv[t];
+      src[slot] = spiv[t];
+      hfirst[hs[r]] = -(slot + 1);  // from now on: the row's slot
+    }
+    base += total;
+  }
+  __syncthreads();
+  for (int r = 0; r < 2; ++r) {
+    const int t = t0 + r * blockDim.x;
+    if (t >= nb) continue;
+    const int pp = spiv[t];
+    sslot[t] = (pp >= k1 && pp <= k2) ? pp - k1 : (hs[r] >= 0 ? -hfirst[hs[r]] - 1 : t);
+  }
+  if (threadIdx.x == 0) cnt = nb + base;
+  __syncthreads();
+  // (3) The interchanges themselves, in order, on the source table.
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < nb; ++t) {
+      const int sp = sslot[t];
+      if (sp == t) continue;
+      const int a0 = src[t];
+      src[t] = src[sp];
+      src[sp] = a0;
+    }
   }
   __syncthreads();
   const int c = cnt;
-  const int col0 = blockIdx.x * 32;
-  for (int idx = threadIdx.x; idx < c * 32; idx += blockDim.x) {
-    const int t = idx / 32, cc = idx % 32;
-    if (col0 + cc < n) tile[t][cc] = a[(src[t] - 1) + (col0 + cc) * lda];
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < c * 32; idx += blockDim.x) {
-    const int t = idx / 32, cc = idx % 32;
-    if (col0 + cc < n) a[(pos[t] - 1) + (col0 + cc) * lda] = tile[t][cc];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int col_end = min(n, (blockIdx.x + 1) * kLaswpCols);
+  for (int col = blockIdx.x * kLaswpCols + warp; col < col_end; col += blockDim.x / 32) {
+    T* ac = a + static_cast<long long>(col) * lda;
+    T v[kSwapTable / 32];
+#pragma unroll
+    for (int r = 0; r < kSwapTable / 32; ++r) {
+      const int e = lane + 32 * r;
+      if (e < c) v[r] = ac[src[e] - 1];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kSwapTable / 32; ++r) {
+      const int e = lane + 32 * r;
+      if (e < c) ac[pos[e] - 1] = v[r];
+    }
+    __syncwarp();
   }
 }
 
@@ -589,7 +640,7 @@ void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
     // sequence of interchanges as one pass over k1..k2.
     for (int c1 = k1; c1 <= k2; c1 += kSwapMax) {
       const int c2 = std::min(k2, c1 + kSwapMax - 1);
-      LaswpPermKernel<T><<<(n + 31) / 32, 256, 0, Ctx().stream>>>(
+      LaswpPermKernel<T><<<(n + kLaswpCols - 1) / kLaswpCols, 256, 0, Ctx().stream>>>(
           n, a, lda, c1, c2, ipiv, Ctx().guard);
       CountLaunch();
     }
