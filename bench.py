@@ -17,6 +17,8 @@ e2e    : the same product through the public C ABI with pinned HOST buffers
          (A, B copied in and C copied out inside the timed region).
 plain  : the plain FP64 tensor-pipe DGEMM (bit-identical to the reference)
          on the same inputs, and its error.
+batched: 10,000 problems, n log-uniform in [8, 512], dgetrf + dgetrs + dgemm
+         each, batched persistent launches against a per-problem loop.
 dgesv  : n = 16384, A = H1 diag(s) H2 (H1, H2 products of 4 Householder
          reflectors, s geometric from 1 to 1/cond): the plain FP64 dgesv
          (bit-identical to the reference's LU) against the mixed-precision
@@ -62,6 +64,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-dgesv", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
     p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv-mixed"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
@@ -484,6 +487,101 @@ def run_solvers(args, torch, hb, stream):
     return res
 
 
+def run_batched(args, torch, hb, count=10000, loop_sample=300):
+    """Config 5: `count` problems, n log-uniform in [8, 512], each dgetrf +
+    dgetrs (nrhs uniform in 1..16) + dgemm (n x n x n), FP64 and FP32: the
+    batched persistent launches against a per-problem loop of the
+    single-problem routines (timed on a sample, scaled to the batch)."""
+    rng = np.random.default_rng(2024)
+    ns = np.exp(rng.uniform(np.log(8), np.log(512), count)).astype(int).clip(8, 512)
+    rhs = rng.integers(1, 17, count)
+    flops = float(np.sum(2.0 / 3.0 * ns ** 3 + 2.0 * ns ** 2 * rhs + 2.0 * ns ** 3))
+    out = {"count": count, "flops": flops}
+    for prec, dtype in (("d", torch.float64), ("s", torch.float32)):
+        sz_a = [int(n) * int(n) for n in ns]
+        sz_b = [int(n) * int(r) for n, r in zip(ns, rhs)]
+        A0 = torch.rand(sum(sz_a), dtype=dtype, device="cuda") * 2 - 1
+        A = torch.empty_like(A0)
+        B = torch.rand(sum(sz_b), dtype=dtype, device="cuda")
+        G1 = torch.rand(sum(sz_a), dtype=dtype, device="cuda") * 2 - 1
+        G2 = torch.rand(sum(sz_a), dtype=dtype, device="cuda") * 2 - 1
+        G3 = torch.zeros(sum(sz_a), dtype=dtype, device="cuda")
+        P = torch.zeros(int(ns.sum()), dtype=torch.int32, device="cuda")
+
+        def views(buf, sizes):
+            v, o = [], 0
+            for s_ in sizes:
+                v.append(buf[o:o + s_])
+                o += s_
+            return v
+
+        va, vb = views(A, sz_a), views(B, sz_b)
+        v1, v2, v3 = views(G1, sz_a), views(G2, sz_a), views(G3, sz_a)
+        vp = views(P, [int(n) for n in ns])
+        nl, rl = [int(n) for n in ns], [int(r) for r in rhs]
+
+        def batched():
+            hb.getrf_batched(nl, va, nl, vp, precision=prec)
+            hb.getrs_batched("N", nl, rl, va, nl, vp, vb, nl, precision=prec)
+            hb.gemm_batched("N", "N", nl, nl, nl, 1.0, v1, nl, v2, nl, 0.0, v3, nl,
+                            precision=prec)
+
+        times = []
+        for _ in range(2):
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batched()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        t_batched = times[-1]
+        entry = {"batched_ms": t_batched * 1e3, "tflops": flops / t_batched / 1e12}
+        if prec == "d":
+            # The per-problem loop on a sample of the same problems.
+            idx = rng.choice(count, loop_sample, replace=False)
+            A.copy_(A0)
+            torch.cuda.synchronize()
+
+            def loop(ids):
+                for i in ids:
+                    n, r = nl[i], rl[i]
+                    hb.dgetrf(n, n, va[i], n, vp[i])
+                    hb.dgetrs("N", n, r, va[i], n, vp[i], vb[i], n)
+                    hb.dgemm("N", "N", n, n, n, 1.0, v1[i], n, v2[i], n, 0.0, v3[i], n)
+
+            loop(idx[:10])  # warm-up
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            loop(idx)
+            torch.cuda.synchronize()
+            t_loop = time.perf_counter() - t0
+            frac = float(np.sum(ns[idx] ** 3)) / float(np.sum(ns ** 3))
+            entry["loop_ms_estimate"] = t_loop / frac * 1e3
+            entry["loop_sample"] = f"{loop_sample} problems ({100 * frac:.1f} % of the n^3 work)"
+            entry["speedup_vs_loop"] = entry["loop_ms_estimate"] / entry["batched_ms"]
+            # getrf alone, batched vs loop on the same sample.
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hb.getrf_batched(nl, va, nl, vp)
+            torch.cuda.synchronize()
+            t_gb = time.perf_counter() - t0
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for i in idx:
+                hb.dgetrf(nl[i], nl[i], va[i], nl[i], vp[i])
+            torch.cuda.synchronize()
+            t_gl = (time.perf_counter() - t0) / frac
+            entry["getrf_batched_ms"] = t_gb * 1e3
+            entry["getrf_loop_ms_estimate"] = t_gl * 1e3
+            entry["getrf_speedup_vs_loop"] = t_gl / t_gb
+        out["fp64" if prec == "d" else "fp32"] = entry
+        del A0, A, B, G1, G2, G3, P
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -520,6 +618,9 @@ def run_ours(args):
     solvers = None
     if rank == 0 and world == 1 and not args.no_dgesv:
         solvers = run_solvers(args, torch, hb, stream)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = run_batched(args, torch, hb)
 
     if rank == 0:
         line = {
@@ -561,6 +662,8 @@ def run_ours(args):
             line["spread30"] = d["spread30"]
         if solvers is not None:
             line["solvers"] = solvers
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     dist.close()
     return 0

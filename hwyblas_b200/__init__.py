@@ -20,7 +20,7 @@ __all__ = [
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
-    "KERNEL_LU_LEAF",
+    "KERNEL_LU_LEAF", "getrf_batched", "getrs_batched", "gemm_batched",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -46,7 +46,7 @@ from ._api import (  # noqa: E402  (needs lib())
     cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
     dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
-    KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF,
+    KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

@@ -44,6 +44,14 @@ PROTOTYPES = {
     "hwyblas_dgesv_mixed": (None, [PI, PI, P, PI, P, P, PI, P, PI, PI, PI]),
     "hwyblas_dposv_mixed": (None, [C, PI, PI, P, PI, P, PI, P, PI, PI, PI]),
     "hwyblas_set_mixed_slices": (I, [I]),
+    "hwyblas_dgetrf_batched": (None, [P, P, P, P, P, I]),
+    "hwyblas_sgetrf_batched": (None, [P, P, P, P, P, I]),
+    "hwyblas_dgetrs_batched": (None, [ctypes.c_char, P, P, P, P, P, P, P, I, PI]),
+    "hwyblas_sgetrs_batched": (None, [ctypes.c_char, P, P, P, P, P, P, P, I, PI]),
+    "hwyblas_dgemm_batched": (None, [ctypes.c_char, ctypes.c_char, P, P, P, D, P, P, P, P,
+                                     D, P, P, I]),
+    "hwyblas_sgemm_batched": (None, [ctypes.c_char, ctypes.c_char, P, P, P, F, P, P, P, P,
+                                     F, P, P, I]),
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
     "hwyblas_launch_count": (ctypes.c_uint64, []),

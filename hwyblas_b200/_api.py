@@ -170,6 +170,41 @@ def set_mixed_slices(slices):
     return lib().hwyblas_set_mixed_slices(int(slices))
 
 
+def _ints(vals):
+    return (ctypes.c_int * max(1, len(vals)))(*[int(v) for v in vals])
+
+
+def _ptrs(objs):
+    return (ctypes.c_void_p * max(1, len(objs)))(*[_ptr(o) for o in objs])
+
+
+def getrf_batched(n, a, lda, ipiv, precision="d"):
+    """Batched LU: n, lda sequences of ints; a, ipiv sequences of device
+    buffers (tensors or addresses). Returns the per-problem INFO list."""
+    count = len(n)
+    info = (ctypes.c_int * max(1, count))()
+    fn = lib().hwyblas_dgetrf_batched if precision == "d" else lib().hwyblas_sgetrf_batched
+    fn(_ints(n), _ptrs(a), _ints(lda), _ptrs(ipiv), info, count)
+    return list(info)[:count]
+
+
+def getrs_batched(trans, n, nrhs, a, lda, ipiv, b, ldb, precision="d"):
+    """Batched LU solve (per-problem sizes as sequences). Returns INFO."""
+    info = ctypes.c_int(0)
+    fn = lib().hwyblas_dgetrs_batched if precision == "d" else lib().hwyblas_sgetrs_batched
+    fn(_c(trans)[0:1], _ints(n), _ints(nrhs),
+       _ptrs(a), _ints(lda), _ptrs(ipiv), _ptrs(b), _ints(ldb), len(n), ctypes.byref(info))
+    return info.value
+
+
+def gemm_batched(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                 precision="d"):
+    """Batched GEMM (per-problem sizes as sequences, shared alpha and beta)."""
+    fn = lib().hwyblas_dgemm_batched if precision == "d" else lib().hwyblas_sgemm_batched
+    fn(_c(transa)[0:1], _c(transb)[0:1], _ints(m), _ints(n), _ints(k), float(alpha), _ptrs(a),
+       _ints(lda), _ptrs(b), _ints(ldb), float(beta), _ptrs(c), _ints(ldc), len(m))
+
+
 def idamax_noalloc(n, x, incx, result, stream=None):
     """1-based index of max |x| into the device int `result`, with no
     allocation (x and result in device memory); returns the status code."""

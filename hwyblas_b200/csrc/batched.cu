@@ -1,0 +1,1028 @@
+// Batched LU, LU solve and GEMM for many small problems of uneven sizes
+// (n up to a few hundred): one persistent launch per routine in which each
+// CTA takes whole problems from a work queue (largest first) and runs the
+// reference's algorithm on it, call for call:
+//   GETRF  src/lapack/getrf.cc:216-280 (nb = 64) and 112-207 (recursion to
+//          the 16-column leaf of src/lapack/factor_kernels.cc:79-183)
+//   GETRS  src/lapack/getrf.cc:287-339
+//   TRSM   src/trsm.cc:87-135 (split max(32, (r/2)/32*32)), base solves of
+//          src/trsm-inl.h:107-174 (reciprocal diagonal, column pairs)
+//   GEMM   src/gemm_kernel-inl.h:161-224 (a sequential FMA chain per element,
+//          restarted every KC = 256 (double) / 384 (float), merged in order)
+// so every problem's result is bit-identical to the single-problem routines.
+// The reference has no batched API; the entry points follow the argument
+// conventions of its single-problem routines with arrays of sizes, leading
+// dimensions and device pointers.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <tuple>
+#include <vector>
+
+#include "../../include/hwyblas_b200.h"
+#include "device.cuh"
+#include "internal.h"
+#include "ref_order.cuh"
+
+namespace hb {
+
+int RefLanesDouble();
+
+namespace {
+
+template <typename T>
+struct Kc;
+template <>
+struct Kc<double> {
+  static constexpr int value = 256;
+};
+template <>
+struct Kc<float> {
+  static constexpr int value = 384;
+};
+
+// A strided matrix operand on the device: element (i, j) at p[i*rs + j*cs].
+template <typename T>
+struct Mat {
+  T* p;
+  long long rs, cs;
+  __device__ T& operator()(long long i, long long j) const { return p[i * rs + j * cs]; }
+  __device__ Mat sub(long long i, long long j) const { return {p + i * rs + j * cs, rs, cs}; }
+};
+
+template <typename T>
+__device__ __forceinline__ Mat<T> Col(T* p, long long ld) {
+  return {p, 1, ld};
+}
+
+// C := alpha*A*B + beta*C (m x n, inner k) with the reference's per-element
+// order; the CTA's threads share the elements.
+template <typename T>
+__device__ void CtaGemm(int m, int n, int k, T alpha, Mat<T> a, Mat<T> b, T beta,
+                        Mat<T> c) {
+  constexpr int KC = Kc<T>::value;
+  const int total = m * n;
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int i = idx % m, j = idx / m;
+    T cv = T(0);
+    for (int pc = 0; pc < k; pc += KC) {
+      const int pe = min(k, pc + KC);
+      T acc = T(0);
+      for (int q = pc; q < pe; ++q) acc = fma(a(i, q), b(q, j), acc);
+      const T r = alpha * acc;
+      if (pc != 0 || beta == T(1)) {
+        if (pc == 0) cv = c(i, j);
+        cv = r + cv;
+      } else if (beta == T(0)) {
+        cv = r;
+      } else {
+        cv = fma(c(i, j), beta, r);
+      }
+    }
+    if (k > 0) c(i, j) = cv;
+  }
+  __syncthreads();
+}
+
+// Row interchanges k1..k2 (1-based, increasing) of ncols columns.
+template <typename T>
+__device__ void CtaLaswp(int ncols, Mat<T> a, int k1, int k2, const int* ipiv) {
+  for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
+    for (int i = k1; i <= k2; ++i) {
+      const int ip = ipiv[i - 1];
+      if (ip != i) {
+        const T t = a(i - 1, col);
+        a(i - 1, col) = a(ip - 1, col);
+        a(ip - 1, col) = t;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Backward interchanges (incx = -1): k2 down to k1.
+template <typename T>
+__device__ void CtaLaswpBack(int ncols, Mat<T> a, int k1, int k2, const int* ipiv) {
+  for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
+    for (int i = k2; i >= k1; --i) {
+      const int ip = ipiv[i - 1];
+      if (ip != i) {
+        const T t = a(i - 1, col);
+        a(i - 1, col) = a(ip - 1, col);
+        a(ip - 1, col) = t;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Base solve of the TRSM recursion (r <= 32): x op(T) = b for each of the
+// `other` rows of x, in solve order with the reciprocal diagonal and column
+// pairs; t is already the right-side triangle (lower: solved from the last
+// column). st and sinv are shared scratch.
+template <typename T>
+__device__ void CtaTrsmBase(Mat<T> t, bool lower, bool unit, int r, int other, T* x,
+                            long long xs_row, long long xs_col, T (*st)[33], T* sinv) {
+  for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+    const int s = idx / 32, u = idx % 32;
+    T v = T(0);
+    if (s < r && u < r) {
+      const int q = lower ? r - 1 - s : s, j = lower ? r - 1 - u : u;
+      if (s < u || (s == u && !unit)) v = t(q, j);
+    }
+    st[s][u] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int s = threadIdx.x;
+    sinv[s] = (s < r && !unit) ? T(1) / st[s][s] : T(1);
+  }
+  __syncthreads();
+  for (int row = threadIdx.x; row < other; row += blockDim.x) {
+    T* xr = x + row * xs_row;
+    T y[32];
+#pragma unroll
+    for (int s = 0; s < 32; ++s)
+      if (s < r) y[s] = xr[(lower ? r - 1 - s : s) * xs_col];
+#pragma unroll
+    for (int step = 0; step + 1 < 32; step += 2) {
+      if (step + 2 <= r) {
+        T acc0 = y[step], acc1 = y[step + 1];
+#pragma unroll
+        for (int s = 0; s < step; ++s) {
+          acc0 = fma(-y[s], st[s][step], acc0);
+          acc1 = fma(-y[s], st[s][step + 1], acc1);
+        }
+        if (!unit) acc0 = acc0 * sinv[step];
+        y[step] = acc0;
+        acc1 = fma(-acc0, st[step][step + 1], acc1);
+        if (!unit) acc1 = acc1 * sinv[step + 1];
+        y[step + 1] = acc1;
+      } else if (step < r) {
+        T acc = y[step];
+#pragma unroll
+        for (int s = 0; s < step; ++s) acc = fma(-y[s], st[s][step], acc);
+        if (!unit) acc = acc * sinv[step];
+        y[step] = acc;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 32; ++s)
+      if (s < r) xr[(lower ? r - 1 - s : s) * xs_col] = y[s];
+  }
+  __syncthreads();
+}
+
+// Left-side triangular solve op(T) X = B (op(T) is `tri`, r x r; X is r x
+// other, column-major ld ldb) by the reference's recursion, emulated with an
+// explicit stack: top half, GEMM update, bottom half (lower; upper mirrored).
+template <typename T>
+__device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other, T* b,
+                            long long ldb, T (*st)[33], T* sinv) {
+  if (r <= 0 || other <= 0) return;
+  int s_off[8], s_r[8], s_ph[8];
+  int sp = 0;
+  s_off[0] = 0;
+  s_r[0] = r;
+  s_ph[0] = 0;
+  while (sp >= 0) {
+    const int off = s_off[sp], rr = s_r[sp];
+    if (rr <= 32) {
+      // TrsmSolve for the left side: X^T op(T)^T = B^T, rows of X^T are the
+      // columns of B.
+      Mat<T> t = tri.sub(off, off);
+      const Mat<T> tt = {t.p, t.cs, t.rs};
+      CtaTrsmBase(tt, !lower, unit, rr, other, b + off, ldb, 1, st, sinv);
+      --sp;
+      continue;
+    }
+    const int r1 = max(32, (rr / 2) / 32 * 32), r2 = rr - r1;
+    const int ph = s_ph[sp]++;
+    if (ph == 2) {
+      --sp;
+      continue;
+    }
+    if (lower) {
+      if (ph == 0) {
+        ++sp;
+        s_off[sp] = off;
+        s_r[sp] = r1;
+        s_ph[sp] = 0;
+      } else {
+        CtaGemm<T>(r2, other, r1, T(-1), tri.sub(off + r1, off), Col(b + off, ldb), T(1),
+                   Col(b + off + r1, ldb));
+        ++sp;
+        s_off[sp] = off + r1;
+        s_r[sp] = r2;
+        s_ph[sp] = 0;
+      }
+    } else {
+      if (ph == 0) {
+        ++sp;
+        s_off[sp] = off + r1;
+        s_r[sp] = r2;
+        s_ph[sp] = 0;
+      } else {
+        CtaGemm<T>(r1, other, r2, T(-1), tri.sub(off, off + r1), Col(b + off + r1, ldb),
+                   T(1), Col(b + off, ldb));
+        ++sp;
+        s_off[sp] = off;
+        s_r[sp] = r1;
+        s_ph[sp] = 0;
+      }
+    }
+  }
+}
+
+// Shared scratch of the per-CTA LU.
+template <typename T>
+struct LuShared {
+  T st[32][33];
+  T sinv[32];
+  T wv[32];
+  int wi[32];
+  int piv;
+};
+
+// LU leaf (min(m, n) <= 16) on an m x n block: partial pivoting with the
+// reference's pivot choice, reciprocal scaling (or division below sfmin) and
+// AXPY rounding; trailing columns (n > m) take all interchanges, then the
+// updates with the final L.
+template <typename T>
+__device__ void CtaLeaf(int m, int n, Mat<T> a, int* ipiv, int* info, int col0, int lanes,
+                        LuShared<T>& sh) {
+  const int w = min(m, n);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int nwarps = blockDim.x / 32;
+  for (int j = 0; j < w; ++j) {
+    T bv = T(-1);
+    int bi = 0x7fffffff;
+    for (int i = j + threadIdx.x; i < m; i += blockDim.x) {
+      const T v = fabs(a(i, j));
+      if (v > bv) { bv = v; bi = i; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const T ov = __shfl_down_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (Better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { sh.wv[warp] = bv; sh.wi[warp] = bi; }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < nwarps ? sh.wv[lane] : T(-1);
+      bi = lane < nwarps ? sh.wi[lane] : 0x7fffffff;
+      for (int off = 16; off > 0; off >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (Better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+      }
+      if (lane == 0) {
+        if (isnan(fabs(a(j, j))) || bi == 0x7fffffff) bi = j;
+        sh.piv = bi;
+        ipiv[j] = bi + 1;
+        if (a(bi, j) == T(0) && *info == 0) *info = col0 + j + 1;
+      }
+    }
+    __syncthreads();
+    const int piv = sh.piv;
+    const T pivot = a(piv, j);
+    if (pivot != T(0) && piv != j) {
+      for (int c = threadIdx.x; c < w; c += blockDim.x) {
+        const T t = a(j, c);
+        a(j, c) = a(piv, c);
+        a(piv, c) = t;
+      }
+    }
+    __syncthreads();
+    const bool scale = pivot != T(0);
+    const bool tiny = !(fabs(pivot) >= Sfmin<T>());
+    const T rinv = T(1) / pivot;
+    const int len = m - j - 1;
+    for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) {
+      T x = a(i, j);
+      if (scale) {
+        x = tiny ? x / pivot : x * rinv;
+        a(i, j) = x;
+      }
+      for (int k = j + 1; k < w; ++k) a(i, k) = Axpy(a(i, k), -a(j, k), x, len, lanes);
+    }
+    __syncthreads();
+  }
+  for (int k = w + threadIdx.x; k < n; k += blockDim.x) {
+    for (int j = 0; j < w; ++j) {
+      const int p = ipiv[j] - 1;
+      if (p != j) {
+        const T t = a(j, k);
+        a(j, k) = a(p, k);
+        a(p, k) = t;
+      }
+    }
+    for (int j = 0; j < w; ++j) {
+      const T alpha = -a(j, k);
+      const int len = m - j - 1;
+      for (int i = j + 1; i < m; ++i) a(i, k) = Axpy(a(i, k), alpha, a(i, j), len, lanes);
+    }
+  }
+  __syncthreads();
+}
+
+// The reference's recursive LU (Getrf2) of an m x n block at a, with the
+// block's pivots in ipiv (block-relative, 1-based) and col0 its first global
+// column (for INFO). Recursion emulated with an explicit stack; frames sit
+// on the block's diagonal at offset off.
+template <typename T>
+__device__ void CtaGetrfRec(int m, int n, Mat<T> a, int* ipiv, int* info, int col0,
+                            int lanes, LuShared<T>& sh) {
+  int s_m[12], s_n[12], s_off[12], s_ph[12];
+  int sp = 0;
+  s_m[0] = m;
+  s_n[0] = n;
+  s_off[0] = 0;
+  s_ph[0] = 0;
+  while (sp >= 0) {
+    const int fm = s_m[sp], fn = s_n[sp], off = s_off[sp];
+    const Mat<T> fa = a.sub(off, off);
+    int* fp = ipiv + off;
+    if (fm == 0 || fn == 0) {
+      --sp;
+      continue;
+    }
+    const int mn = min(fm, fn);
+    if (mn <= 16) {
+      CtaLeaf(fm, fn, fa, fp, info, col0 + off, lanes, sh);
+      --sp;
+      continue;
+    }
+    const int n1 = mn / 2, n2 = fn - n1;
+    const int ph = s_ph[sp]++;
+    if (ph == 0) {
+      ++sp;
+      s_m[sp] = fm;
+      s_n[sp] = n1;
+      s_off[sp] = off;
+      s_ph[sp] = 0;
+    } else if (ph == 1) {
+      CtaLaswp(n2, fa.sub(0, n1), 1, n1, fp);
+      CtaTrsmLeft(fa, true, true, n1, n2, &fa(0, n1), fa.cs, sh.st, sh.sinv);
+      CtaGemm<T>(fm - n1, n2, n1, T(-1), fa.sub(n1, 0), fa.sub(0, n1), T(1),
+                 fa.sub(n1, n1));
+      ++sp;
+      s_m[sp] = fm - n1;
+      s_n[sp] = n2;
+      s_off[sp] = off + n1;
+      s_ph[sp] = 0;
+    } else {
+      for (int i = n1 + threadIdx.x; i < mn; i += blockDim.x) fp[i] += n1;
+      __syncthreads();
+      CtaLaswp(n1, fa, n1 + 1, mn, fp);
+      --sp;
+    }
+  }
+}
+
+// The reference's blocked LU (Getrf, nb = 64) of an n x n matrix.
+template <typename T>
+__device__ void CtaGetrf(int n, Mat<T> a, int* ipiv, int* info, int lanes,
+                         LuShared<T>& sh) {
+  constexpr int nb = 64;
+  if (n == 0) return;
+  if (nb >= n) {
+    CtaGetrfRec(n, n, a, ipiv, info, 0, lanes, sh);
+    return;
+  }
+  for (int j = 0; j < n; j += nb) {
+    const int jb = min(n - j, nb);
+    CtaGetrfRec(n - j, jb, a.sub(j, j), ipiv + j, info, j, lanes, sh);
+    for (int i = j + threadIdx.x; i < j + jb; i += blockDim.x) ipiv[i] += j;
+    __syncthreads();
+    CtaLaswp(j, a, j + 1, j + jb, ipiv);
+    if (j + jb < n) {
+      CtaLaswp(n - j - jb, a.sub(0, j + jb), j + 1, j + jb, ipiv);
+      CtaTrsmLeft(a.sub(j, j), true, true, jb, n - j - jb, &a(j, j + jb), a.cs, sh.st,
+                  sh.sinv);
+      CtaGemm<T>(n - j - jb, n - j - jb, jb, T(-1), a.sub(j + jb, j), a.sub(j, j + jb),
+                 T(1), a.sub(j + jb, j + jb));
+    }
+  }
+}
+
+// The reference's Getrs: solve op(A) X = B with the LU factors.
+template <typename T>
+__device__ void CtaGetrs(bool trans, int n, int nrhs, Mat<T> a, const int* ipiv, T* b,
+                         long long ldb, LuShared<T>& sh) {
+  if (n == 0 || nrhs == 0) return;
+  const Mat<T> bm = Col(b, ldb);
+  if (!trans) {
+    CtaLaswp(nrhs, bm, 1, n, ipiv);
+    CtaTrsmLeft(a, true, true, n, nrhs, b, ldb, sh.st, sh.sinv);
+    CtaTrsmLeft(a, false, false, n, nrhs, b, ldb, sh.st, sh.sinv);
+  } else {
+    // op(T) = T^T: the transposed view, upper <-> lower.
+    const Mat<T> at = {a.p, a.cs, a.rs};
+    CtaTrsmLeft(at, true, false, n, nrhs, b, ldb, sh.st, sh.sinv);
+    CtaTrsmLeft(at, false, true, n, nrhs, b, ldb, sh.st, sh.sinv);
+    CtaLaswpBack(nrhs, bm, 1, n, ipiv);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent batched kernels: CTAs take problems from a queue ordered by
+// decreasing size until it is empty (no waits).
+
+template <typename T>
+struct BatchArgs {
+  int count;
+  const int* order;      // problem indices, largest first
+  unsigned int* next;    // queue head, zero at launch
+  const int* m;          // getrf/getrs: n; gemm: m
+  const int* n;          // getrs: nrhs; gemm: n
+  const int* k;          // gemm: k
+  const int* lda;
+  const int* ldb;
+  const int* ldc;
+  T* const* a;
+  T* const* b;
+  T* const* c;
+  int* const* ipiv;
+  int* info;
+  T alpha, beta;
+  int flags;             // getrs: trans; gemm: transa | transb << 1
+  int lanes;
+};
+
+template <typename T>
+__device__ __forceinline__ int NextProblem(const BatchArgs<T>& p, int* slot) {
+  if (threadIdx.x == 0) *slot = static_cast<int>(atomicAdd(p.next, 1u));
+  __syncthreads();
+  const int q = *slot;
+  __syncthreads();
+  return q < p.count ? p.order[q] : -1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) BatchedGetrfKernel(BatchArgs<T> p) {
+  __shared__ LuShared<T> sh;
+  __shared__ int slot;
+  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+    if (threadIdx.x == 0) p.info[id] = 0;
+    __syncthreads();
+    CtaGetrf(p.m[id], Col(p.a[id], p.lda[id]), p.ipiv[id], &p.info[id], p.lanes, sh);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) BatchedGetrsKernel(BatchArgs<T> p) {
+  __shared__ LuShared<T> sh;
+  __shared__ int slot;
+  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+    CtaGetrs(p.flags != 0, p.m[id], p.n[id], Col(p.a[id], p.lda[id]), p.ipiv[id], p.b[id],
+             p.ldb[id], sh);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) BatchedGemmKernel(BatchArgs<T> p) {
+  __shared__ int slot;
+  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+    const long long la = p.lda[id], lb = p.ldb[id];
+    const Mat<T> a = (p.flags & 1) ? Mat<T>{p.a[id], la, 1} : Col(p.a[id], la);
+    const Mat<T> b = (p.flags & 2) ? Mat<T>{p.b[id], lb, 1} : Col(p.b[id], lb);
+    const int m = p.m[id], n = p.n[id], k = p.k[id];
+    if (m == 0 || n == 0) continue;
+    if (k == 0 || p.alpha == T(0)) {
+      // Only C := beta*C (C not read for beta == 0), as the single GEMM.
+      if (p.beta != T(1)) {
+        const Mat<T> c = Col(p.c[id], p.ldc[id]);
+        for (int idx = threadIdx.x; idx < m * n; idx += blockDim.x) {
+          const int i = idx % m, j = idx / m;
+          c(i, j) = (p.beta == T(0)) ? T(0) : c(i, j) * p.beta;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    CtaGemm<T>(m, n, k, p.alpha, a, b, p.beta, Col(p.c[id], p.ldc[id]));
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+namespace {
+
+// Whether [p, p + bytes) lies inside one device allocation (cuMemGetAddressRange
+// through the runtime's driver entry point), with the last ranges cached: a
+// batch usually carves its problems out of a few allocations.
+using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddressRangeFn RangeFn() {
+  static AddressRangeFn fn = [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &ptr, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<AddressRangeFn>(nullptr);
+    return reinterpret_cast<AddressRangeFn>(ptr);
+  }();
+  return fn;
+}
+
+struct ExtentChecker {
+  std::vector<std::pair<uintptr_t, uintptr_t>> ranges;
+  bool Check(const void* p, size_t bytes) {
+    if (bytes == 0) return true;
+    if (p == nullptr) return false;
+    const uintptr_t lo = reinterpret_cast<uintptr_t>(p), hi = lo + bytes;
+    for (const auto& r : ranges)
+      if (lo >= r.first && hi <= r.second) return true;
+    AddressRangeFn fn = RangeFn();
+    if (fn == nullptr) return false;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (fn(&base, &size, static_cast<CUdeviceptr>(lo)) != CUDA_SUCCESS) return false;
+    const uintptr_t b = static_cast<uintptr_t>(base);
+    ranges.emplace_back(b, b + size);
+    if (ranges.size() > 64) ranges.erase(ranges.begin());
+    return lo >= b && hi <= b + size;
+  }
+};
+
+// Pinned host staging for a batch's descriptor, copied to the device in one
+// transfer.
+struct HostStage {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void* Get(size_t want) {
+    if (bytes < want) {
+      if (ptr != nullptr) {
+        cudaStreamSynchronize(Ctx().stream);
+        cudaFreeHost(ptr);
+      }
+      ptr = nullptr;
+      bytes = 0;
+      if (cudaMallocHost(&ptr, want) != cudaSuccess) return nullptr;
+      bytes = want;
+    }
+    return ptr;
+  }
+};
+thread_local HostStage t_stage;
+
+size_t Align8(size_t v) { return (v + 7) / 8 * 8; }
+
+// Lays out the descriptor of a batch: int arrays then pointer arrays.
+struct Layout {
+  size_t off_order, off_next, off_m, off_n, off_k, off_lda, off_ldb, off_ldc, off_info;
+  size_t off_a, off_b, off_c, off_ipiv, total;
+  explicit Layout(int count) {
+    size_t o = 0;
+    const size_t ints = sizeof(int) * static_cast<size_t>(count);
+    off_order = o; o = Align8(o + ints);
+    off_next = o; o = Align8(o + 64);
+    off_m = o; o = Align8(o + ints);
+    off_n = o; o = Align8(o + ints);
+    off_k = o; o = Align8(o + ints);
+    off_lda = o; o = Align8(o + ints);
+    off_ldb = o; o = Align8(o + ints);
+    off_ldc = o; o = Align8(o + ints);
+    off_info = o; o = Align8(o + ints);
+    const size_t ptrs = sizeof(void*) * static_cast<size_t>(count);
+    off_a = o; o += ptrs;
+    off_b = o; o += ptrs;
+    off_c = o; o += ptrs;
+    off_ipiv = o; o += ptrs;
+    total = o;
+  }
+};
+
+enum BatchKind { kBatchGetrf = 0, kBatchGetrs = 1, kBatchGemm = 2 };
+
+template <typename T>
+void* KernelOf(int kind) {
+  if (kind == kBatchGetrf) return reinterpret_cast<void*>(BatchedGetrfKernel<T>);
+  if (kind == kBatchGetrs) return reinterpret_cast<void*>(BatchedGetrsKernel<T>);
+  return reinterpret_cast<void*>(BatchedGemmKernel<T>);
+}
+
+// Threads per CTA for a batch: the autotuner's choice for the batch's size
+// bucket (the median problem's log2 size), measured once per process on a
+// synthetic sample of that size (see Autotune below).
+struct TuneKey {
+  int kind, bytes, bucket;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(kind, bytes, bucket) < std::tie(o.kind, o.bytes, o.bucket);
+  }
+};
+
+}  // namespace
+}  // namespace hb
+
+namespace hb {
+namespace {
+
+// A batch as the host sees it: per-problem sizes and device pointers.
+template <typename T>
+struct HostBatch {
+  int count = 0;
+  std::vector<int> m, n, k, lda, ldb, ldc;
+  std::vector<T*> a, b, c;
+  std::vector<int*> ipiv;
+  T alpha = T(1), beta = T(0);
+  int flags = 0;
+};
+
+// Work of one problem, for the largest-first order.
+template <typename T>
+double WorkOf(int kind, const HostBatch<T>& bt, int i) {
+  const double m = bt.m[i], n = bt.n.empty() ? 0 : bt.n[i];
+  if (kind == kBatchGetrf) return m * m * m;
+  if (kind == kBatchGetrs) return m * m * (n + 1);
+  return m * n * (bt.k[i] + 1);
+}
+
+// Packs the descriptor, copies it to the device, launches the persistent
+// kernel with `threads` threads a CTA. Problem info lands in dev_info (if
+// non-null) on return of the stream.
+template <typename T>
+bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info) {
+  Context& ctx = Ctx();
+  const int count = bt.count;
+  const Layout L(count);
+  uint8_t* host = static_cast<uint8_t*>(t_stage.Get(L.total));
+  uint8_t* dev = static_cast<uint8_t*>(Workspace(kWsBatch, L.total));
+  if (host == nullptr || dev == nullptr) {
+    Failed(cudaErrorMemoryAllocation, "batched descriptor");
+    return false;
+  }
+  int* order = reinterpret_cast<int*>(host + L.off_order);
+  std::iota(order, order + count, 0);
+  std::vector<double> work(count);
+  for (int i = 0; i < count; ++i) work[i] = WorkOf(kind, bt, i);
+  std::stable_sort(order, order + count, [&](int x, int y) { return work[x] > work[y]; });
+  std::memset(host + L.off_next, 0, 64);
+  auto put_ints = [&](size_t off, const std::vector<int>& v) {
+    if (!v.empty()) std::memcpy(host + off, v.data(), sizeof(int) * count);
+  };
+  put_ints(L.off_m, bt.m);
+  put_ints(L.off_n, bt.n);
+  put_ints(L.off_k, bt.k);
+  put_ints(L.off_lda, bt.lda);
+  put_ints(L.off_ldb, bt.ldb);
+  put_ints(L.off_ldc, bt.ldc);
+  auto put_ptrs = [&](size_t off, const void* src) {
+    if (src != nullptr) std::memcpy(host + off, src, sizeof(void*) * count);
+  };
+  put_ptrs(L.off_a, bt.a.empty() ? nullptr : bt.a.data());
+  put_ptrs(L.off_b, bt.b.empty() ? nullptr : bt.b.data());
+  put_ptrs(L.off_c, bt.c.empty() ? nullptr : bt.c.data());
+  put_ptrs(L.off_ipiv, bt.ipiv.empty() ? nullptr : bt.ipiv.data());
+  if (Failed(cudaMemcpyAsync(dev, host, L.total, cudaMemcpyHostToDevice, ctx.stream),
+             "batched descriptor copy"))
+    return false;
+  BatchArgs<T> args;
+  args.count = count;
+  args.order = reinterpret_cast<const int*>(dev + L.off_order);
+  args.next = reinterpret_cast<unsigned int*>(dev + L.off_next);
+  args.m = reinterpret_cast<const int*>(dev + L.off_m);
+  args.n = reinterpret_cast<const int*>(dev + L.off_n);
+  args.k = reinterpret_cast<const int*>(dev + L.off_k);
+  args.lda = reinterpret_cast<const int*>(dev + L.off_lda);
+  args.ldb = reinterpret_cast<const int*>(dev + L.off_ldb);
+  args.ldc = reinterpret_cast<const int*>(dev + L.off_ldc);
+  args.a = reinterpret_cast<T* const*>(dev + L.off_a);
+  args.b = reinterpret_cast<T* const*>(dev + L.off_b);
+  args.c = reinterpret_cast<T* const*>(dev + L.off_c);
+  args.ipiv = reinterpret_cast<int* const*>(dev + L.off_ipiv);
+  args.info = reinterpret_cast<int*>(dev + L.off_info);
+  args.alpha = bt.alpha;
+  args.beta = bt.beta;
+  args.flags = bt.flags;
+  args.lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  void* fn = KernelOf<T>(kind);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0);
+  const int grid = std::max(1, std::min(count, ctx.num_sms * std::max(per_sm, 1)));
+  void* kargs[] = {&args};
+  if (Failed(cudaLaunchKernel(fn, grid, threads, kargs, 0, ctx.stream), "batched launch"))
+    return false;
+  CountLaunch();
+  if (dev_info != nullptr) *dev_info = args.info;
+  return true;
+}
+
+__global__ void FillRandomKernel(double* x, long long count, unsigned seed, double diag,
+                                 int n) {
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+       i < count; i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    unsigned h = static_cast<unsigned>(i) * 2654435761u ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    double v = (h & 0xffffff) / 8388608.0 - 1.0;
+    const long long e = i % (static_cast<long long>(n) * n);
+    if (e % (n + 1) == 0) v += diag;
+    x[i] = v;
+  }
+}
+
+// The autotuner: threads per CTA in {64, 128, 256} for (routine, type, size
+// bucket), timed on 96 synthetic problems of the bucket's representative
+// size (results do not depend on the choice: every problem's arithmetic is
+// the same whichever threads run it).
+template <typename T>
+int TunedThreads(int kind, int median_m, int median_n) {
+  static std::mutex mu;
+  static std::map<TuneKey, int> cache;
+  int bucket = 0;
+  while ((2 << bucket) <= std::max(1, median_m)) ++bucket;
+  const TuneKey key{kind, static_cast<int>(sizeof(T)), bucket};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  const int nn = std::min(512, std::max(8, 3 << std::max(0, bucket - 1)));
+  const int rhs = kind == kBatchGemm ? nn : std::max(1, std::min(16, median_n));
+  const int S = 96;
+  Context& ctx = Ctx();
+  const size_t mat = static_cast<size_t>(nn) * nn;
+  T *A = nullptr, *B = nullptr, *C = nullptr;
+  int* P = nullptr;
+  int best = 256;
+  if (cudaMalloc(&A, sizeof(T) * mat * S) == cudaSuccess &&
+      cudaMalloc(&B, sizeof(T) * static_cast<size_t>(nn) * rhs * S) == cudaSuccess &&
+      cudaMalloc(&C, sizeof(T) * static_cast<size_t>(nn) * rhs * S) == cudaSuccess &&
+      cudaMalloc(&P, sizeof(int) * nn * S) == cudaSuccess) {
+    HostBatch<T> bt;
+    bt.count = S;
+    for (int i = 0; i < S; ++i) {
+      bt.m.push_back(nn);
+      bt.n.push_back(rhs);
+      bt.k.push_back(nn);
+      bt.lda.push_back(nn);
+      bt.ldb.push_back(nn);
+      bt.ldc.push_back(nn);
+      bt.a.push_back(A + mat * i);
+      bt.b.push_back(B + static_cast<size_t>(nn) * rhs * i);
+      bt.c.push_back(C + static_cast<size_t>(nn) * rhs * i);
+      bt.ipiv.push_back(P + nn * i);
+    }
+    bt.alpha = T(1);
+    bt.beta = T(0);
+    if (sizeof(T) == 8) {
+      FillRandomKernel<<<256, 256, 0, ctx.stream>>>(reinterpret_cast<double*>(A),
+                                                    static_cast<long long>(mat * S), 7u,
+                                                    nn, nn);
+    } else {
+      cudaMemsetAsync(A, 0, sizeof(T) * mat * S, ctx.stream);
+    }
+    cudaMemsetAsync(B, 0, sizeof(T) * static_cast<size_t>(nn) * rhs * S, ctx.stream);
+    cudaMemsetAsync(P, 0, sizeof(int) * nn * S, ctx.stream);
+    if (kind == kBatchGetrs) {
+      // Valid pivots for the solve: the identity.
+      std::vector<int> ident(static_cast<size_t>(nn) * S);
+      for (size_t i = 0; i < ident.size(); ++i) ident[i] = static_cast<int>(i % nn) + 1;
+      cudaMemcpy(P, ident.data(), sizeof(int) * ident.size(), cudaMemcpyHostToDevice);
+    }
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int threads : {64, 128, 256}) {
+      LaunchBatch(kind, bt, threads, nullptr);  // warm-up
+      cudaEventRecord(e0, ctx.stream);
+      LaunchBatch(kind, bt, threads, nullptr);
+      cudaEventRecord(e1, ctx.stream);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = threads;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  cudaStreamSynchronize(ctx.stream);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  cudaFree(P);
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = best;
+  return best;
+}
+
+int Median(std::vector<int> v) {
+  if (v.empty()) return 0;
+  std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+  return v[v.size() / 2];
+}
+
+}  // namespace
+}  // namespace hb
+
+namespace hb {
+namespace {
+
+// Runs a validated batch: autotuned launch, then (getrf) the per-problem
+// INFO back to the host. Synchronous, like the single-problem routines.
+template <typename T>
+void RunBatch(int kind, const HostBatch<T>& bt, int* info_out, const char* name) {
+  if (bt.count == 0) return;
+  const int threads = TunedThreads<T>(kind, Median(bt.m), bt.n.empty() ? 0 : Median(bt.n));
+  int* dev_info = nullptr;
+  if (!LaunchBatch(kind, bt, threads, &dev_info)) return;
+  LaunchFailed(name);
+  if (info_out != nullptr) {
+    Failed(cudaMemcpyAsync(info_out, dev_info, sizeof(int) * bt.count,
+                           cudaMemcpyDeviceToHost, Ctx().stream),
+           "batched info");
+  }
+  Failed(cudaStreamSynchronize(Ctx().stream), name);
+  CheckDeviceStatus(name);
+}
+
+template <typename T>
+void GetrfBatched(const int* n, T* const* a, const int* lda, int* const* ipiv, int* info,
+                  int count, const char* name) {
+  if (count < 0) {
+    ReportError(name, 6);
+    return;
+  }
+  HostBatch<T> bt;
+  bt.count = count;
+  ExtentChecker ext;
+  for (int i = 0; i < count; ++i) {
+    if (n[i] < 0) { ReportError(name, 1); return; }
+    if (lda[i] < std::max(1, n[i])) { ReportError(name, 3); return; }
+    const size_t elems = n[i] == 0 ? 0 : static_cast<size_t>(lda[i]) * (n[i] - 1) + n[i];
+    if (!ext.Check(a[i], sizeof(T) * elems)) { ReportError(name, 2); return; }
+    if (!ext.Check(ipiv[i], sizeof(int) * n[i])) { ReportError(name, 4); return; }
+  }
+  bt.m.assign(n, n + count);
+  bt.lda.assign(lda, lda + count);
+  bt.a.assign(a, a + count);
+  bt.ipiv.assign(ipiv, ipiv + count);
+  RunBatch(kBatchGetrf, bt, info, name);
+}
+
+template <typename T>
+void GetrsBatched(char trans, const int* n, const int* nrhs, T* const* a, const int* lda,
+                  int* const* ipiv, T* const* b, const int* ldb, int count, int* info,
+                  const char* name) {
+  *info = 0;
+  const char t = (trans >= 'a' && trans <= 'z') ? static_cast<char>(trans - 32) : trans;
+  if (t != 'N' && t != 'T' && t != 'C') *info = -1;
+  else if (count < 0) *info = -9;
+  HostBatch<T> bt;
+  ExtentChecker ext;
+  for (int i = 0; *info == 0 && i < count; ++i) {
+    if (n[i] < 0) *info = -2;
+    else if (nrhs[i] < 0) *info = -3;
+    else if (lda[i] < std::max(1, n[i])) *info = -5;
+    else if (ldb[i] < std::max(1, n[i])) *info = -8;
+    else {
+      const size_t ea = n[i] == 0 ? 0 : static_cast<size_t>(lda[i]) * (n[i] - 1) + n[i];
+      const size_t eb = (n[i] == 0 || nrhs[i] == 0)
+                            ? 0 : static_cast<size_t>(ldb[i]) * (nrhs[i] - 1) + n[i];
+      if (!ext.Check(a[i], sizeof(T) * ea)) *info = -4;
+      else if (!ext.Check(ipiv[i], sizeof(int) * n[i])) *info = -6;
+      else if (!ext.Check(b[i], sizeof(T) * eb)) *info = -7;
+    }
+  }
+  if (*info != 0) {
+    ReportError(name, -*info);
+    return;
+  }
+  bt.count = count;
+  bt.m.assign(n, n + count);
+  bt.n.assign(nrhs, nrhs + count);
+  bt.lda.assign(lda, lda + count);
+  bt.ldb.assign(ldb, ldb + count);
+  bt.a.assign(a, a + count);
+  bt.b.assign(b, b + count);
+  bt.ipiv.assign(ipiv, ipiv + count);
+  bt.flags = (t == 'N') ? 0 : 1;
+  RunBatch(kBatchGetrs, bt, nullptr, name);
+}
+
+template <typename T>
+void GemmBatched(char transa, char transb, const int* m, const int* n, const int* k,
+                 T alpha, T* const* a, const int* lda, T* const* b, const int* ldb, T beta,
+                 T* const* c, const int* ldc, int count, const char* name) {
+  auto up = [](char ch) { return (ch >= 'a' && ch <= 'z') ? static_cast<char>(ch - 32) : ch; };
+  const char ta = up(transa), tb = up(transb);
+  int pos = 0;
+  if (ta != 'N' && ta != 'T' && ta != 'C') pos = 1;
+  else if (tb != 'N' && tb != 'T' && tb != 'C') pos = 2;
+  else if (count < 0) pos = 14;
+  ExtentChecker ext;
+  for (int i = 0; pos == 0 && i < count; ++i) {
+    const bool tra = ta != 'N', trb = tb != 'N';
+    const int ra = tra ? k[i] : m[i], ca = tra ? m[i] : k[i];
+    const int rb = trb ? n[i] : k[i], cb = trb ? k[i] : n[i];
+    if (m[i] < 0) pos = 3;
+    else if (n[i] < 0) pos = 4;
+    else if (k[i] < 0) pos = 5;
+    else if (lda[i] < std::max(1, ra)) pos = 8;
+    else if (ldb[i] < std::max(1, rb)) pos = 10;
+    else if (ldc[i] < std::max(1, m[i])) pos = 13;
+    else if (m[i] > 0 && n[i] > 0) {
+      const bool compute = k[i] > 0 && alpha != T(0);
+      const size_t ea = (!compute || ra == 0 || ca == 0) ? 0
+                        : static_cast<size_t>(lda[i]) * (ca - 1) + ra;
+      const size_t eb = (!compute || rb == 0 || cb == 0) ? 0
+                        : static_cast<size_t>(ldb[i]) * (cb - 1) + rb;
+      const size_t ec = static_cast<size_t>(ldc[i]) * (n[i] - 1) + m[i];
+      if (!ext.Check(a[i], sizeof(T) * ea)) pos = 7;
+      else if (!ext.Check(b[i], sizeof(T) * eb)) pos = 9;
+      else if (!ext.Check(c[i], sizeof(T) * ec)) pos = 12;
+    }
+  }
+  if (pos != 0) {
+    ReportError(name, pos);
+    return;
+  }
+  HostBatch<T> bt;
+  bt.count = count;
+  bt.m.assign(m, m + count);
+  bt.n.assign(n, n + count);
+  bt.k.assign(k, k + count);
+  bt.lda.assign(lda, lda + count);
+  bt.ldb.assign(ldb, ldb + count);
+  bt.ldc.assign(ldc, ldc + count);
+  bt.a.assign(a, a + count);
+  bt.b.assign(b, b + count);
+  bt.c.assign(c, c + count);
+  bt.alpha = alpha;
+  bt.beta = beta;
+  bt.flags = (ta != 'N' ? 1 : 0) | (tb != 'N' ? 2 : 0);
+  RunBatch(kBatchGemm, bt, nullptr, name);
+}
+
+}  // namespace
+}  // namespace hb
+
+extern "C" {
+
+HWYBLAS_API void hwyblas_dgetrf_batched(const hwyblas_int* n, double* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        hwyblas_int* info, hwyblas_int count) {
+  hb::GetrfBatched<double>(n, a, lda, ipiv, info, count, "DGETRF_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_sgetrf_batched(const hwyblas_int* n, float* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        hwyblas_int* info, hwyblas_int count) {
+  hb::GetrfBatched<float>(n, a, lda, ipiv, info, count, "SGETRF_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_dgetrs_batched(char trans, const hwyblas_int* n,
+                                        const hwyblas_int* nrhs, double* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        double* const* b, const hwyblas_int* ldb,
+                                        hwyblas_int count, hwyblas_int* info) {
+  hb::GetrsBatched<double>(trans, n, nrhs, a, lda, ipiv, b, ldb, count, info,
+                           "DGETRS_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_sgetrs_batched(char trans, const hwyblas_int* n,
+                                        const hwyblas_int* nrhs, float* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        float* const* b, const hwyblas_int* ldb,
+                                        hwyblas_int count, hwyblas_int* info) {
+  hb::GetrsBatched<float>(trans, n, nrhs, a, lda, ipiv, b, ldb, count, info,
+                          "SGETRS_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_dgemm_batched(char transa, char transb, const hwyblas_int* m,
+                                       const hwyblas_int* n, const hwyblas_int* k,
+                                       double alpha, double* const* a,
+                                       const hwyblas_int* lda, double* const* b,
+                                       const hwyblas_int* ldb, double beta,
+                                       double* const* c, const hwyblas_int* ldc,
+                                       hwyblas_int count) {
+  hb::GemmBatched<double>(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                          count, "DGEMM_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_sgemm_batched(char transa, char transb, const hwyblas_int* m,
+                                       const hwyblas_int* n, const hwyblas_int* k,
+                                       float alpha, float* const* a,
+                                       const hwyblas_int* lda, float* const* b,
+                                       const hwyblas_int* ldb, float beta,
+                                       float* const* c, const hwyblas_int* ldc,
+                                       hwyblas_int count) {
+  hb::GemmBatched<float>(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                         count, "SGEMM_BATCHED");
+}
+
+}  // extern "C"

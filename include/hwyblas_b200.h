@@ -248,6 +248,48 @@ HWYBLAS_API void hwyblas_dposv_mixed(const char* uplo, const hwyblas_int* n,
  * reference's hwyblas_set_ilaenv (lapack.h:74-80), a tuning knob. */
 HWYBLAS_API int hwyblas_set_mixed_slices(int slices);
 
+/* Batched LU, LU solve and GEMM over `count` independent problems of
+ * uneven sizes (no counterpart in the reference, which solves one problem a
+ * call). Arrays of sizes, leading dimensions and INFO are host memory; the
+ * matrices and pivot vectors are device memory (each array entry a device
+ * pointer, checked to lie inside one device allocation). One persistent
+ * launch per call: CTAs take problems largest first; threads per CTA come
+ * from an autotuner (per routine, type and size bucket, measured once per
+ * process). Every problem's result is bit-identical to the single-problem
+ * routine (dgetrf_, dgetrs_, dgemm_ and their single-precision forms). Errors
+ * are reported through the error handler with the position of the offending
+ * argument (any problem). Synchronous on return. */
+HWYBLAS_API void hwyblas_dgetrf_batched(const hwyblas_int* n, double* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        hwyblas_int* info, hwyblas_int count);
+HWYBLAS_API void hwyblas_sgetrf_batched(const hwyblas_int* n, float* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        hwyblas_int* info, hwyblas_int count);
+HWYBLAS_API void hwyblas_dgetrs_batched(char trans, const hwyblas_int* n,
+                                        const hwyblas_int* nrhs, double* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        double* const* b, const hwyblas_int* ldb,
+                                        hwyblas_int count, hwyblas_int* info);
+HWYBLAS_API void hwyblas_sgetrs_batched(char trans, const hwyblas_int* n,
+                                        const hwyblas_int* nrhs, float* const* a,
+                                        const hwyblas_int* lda, hwyblas_int* const* ipiv,
+                                        float* const* b, const hwyblas_int* ldb,
+                                        hwyblas_int count, hwyblas_int* info);
+HWYBLAS_API void hwyblas_dgemm_batched(char transa, char transb, const hwyblas_int* m,
+                                       const hwyblas_int* n, const hwyblas_int* k,
+                                       double alpha, double* const* a,
+                                       const hwyblas_int* lda, double* const* b,
+                                       const hwyblas_int* ldb, double beta,
+                                       double* const* c, const hwyblas_int* ldc,
+                                       hwyblas_int count);
+HWYBLAS_API void hwyblas_sgemm_batched(char transa, char transb, const hwyblas_int* m,
+                                       const hwyblas_int* n, const hwyblas_int* k,
+                                       float alpha, float* const* a,
+                                       const hwyblas_int* lda, float* const* b,
+                                       const hwyblas_int* ldb, float beta,
+                                       float* const* c, const hwyblas_int* ldc,
+                                       hwyblas_int count);
+
 /* Stream for subsequent calls of the calling thread (a cudaStream_t; NULL
  * restores the library's per-thread stream). No counterpart in the
  * reference, which has no device. */

@@ -1,0 +1,154 @@
+"""Batched LU, LU solve and GEMM through the C ABI.
+
+The reference has no batched API; every problem of a batch must come out bit
+for bit as the single-problem routine gives it (dgetrf_, dgetrs_, dgemm_,
+sgemm_ - themselves pinned bit-exact to the oracle - and the oracle's sgetrf
+for single precision), whatever the mix of sizes. Sizes cover the leaf (<=
+16), recursion (<= 64) and blocked (> 64) regimes of the LU and the KC chunk
+boundaries of the GEMM.
+"""
+import numpy as np
+import pytest
+
+from tests.oracle_lib import same_bits, first_diff
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 7, 16, 17, 31, 33, 64, 65, 100, 128, 129, 200, 257, 300, 384]
+
+
+def carve(torch, sizes_elems, dtype):
+    """One device allocation carved into per-problem views (contiguous)."""
+    total = int(sum(sizes_elems))
+    buf = torch.empty(max(total, 1), dtype=dtype, device="cuda")
+    views, off = [], 0
+    for s in sizes_elems:
+        views.append(buf[off:off + s])
+        off += s
+    return buf, views
+
+
+def test_dgetrf_batched_matches_single(hb, cuda):
+    torch = cuda
+    rng = np.random.default_rng(1)
+    ns = SIZES + list(rng.integers(1, 260, 40))
+    ldas = [n + int(rng.integers(0, 3)) for n in ns]
+    _, mats = carve(torch, [l * n for l, n in zip(ldas, ns)], torch.float64)
+    _, pivs = carve(torch, ns, torch.int32)
+    host = []
+    for i, (n, l) in enumerate(zip(ns, ldas)):
+        a = rng.uniform(-1, 1, l * n)
+        if i == 5:
+            a.reshape(n, l)[3, :] = 0.0  # singular: column 3 of problem 5 is zero
+        host.append(a)
+        mats[i].copy_(torch.from_numpy(a))
+    torch.cuda.synchronize()
+    info = hb.getrf_batched(ns, mats, ldas, pivs)
+    for i, (n, l) in enumerate(zip(ns, ldas)):
+        a1 = torch.from_numpy(host[i]).cuda()
+        p1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        info1 = hb.dgetrf(n, n, a1, l, p1)
+        got, want = mats[i].cpu().numpy(), a1.cpu().numpy()
+        assert info[i] == info1, (i, n, info[i], info1)
+        assert np.array_equal(pivs[i].cpu().numpy(), p1.cpu().numpy()), (i, n)
+        assert same_bits(got, want), (i, n, first_diff(got, want))
+    assert info[5] == 4
+
+
+def test_sgetrf_batched_matches_oracle(hb, orc, cuda):
+    torch = cuda
+    rng = np.random.default_rng(2)
+    ns = SIZES
+    _, mats = carve(torch, [n * n for n in ns], torch.float32)
+    _, pivs = carve(torch, ns, torch.int32)
+    host = [rng.uniform(-1, 1, n * n).astype(np.float32) for n in ns]
+    for i in range(len(ns)):
+        mats[i].copy_(torch.from_numpy(host[i]))
+    torch.cuda.synchronize()
+    info = hb.getrf_batched(ns, mats, ns, pivs, precision="s")
+    for i, n in enumerate(ns):
+        a = np.asfortranarray(host[i].reshape(n, n).T)
+        p = np.zeros(n, np.int32)
+        assert orc.sgetrf(n, n, a, n, p) == info[i]
+        got = mats[i].cpu().numpy().reshape(n, n).T
+        assert np.array_equal(pivs[i].cpu().numpy(), p), (i, n)
+        assert same_bits(got, a), (i, n, first_diff(got, a))
+
+
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_dgetrs_batched_matches_single(hb, cuda, trans):
+    torch = cuda
+    rng = np.random.default_rng(3)
+    ns = SIZES
+    nrhs = [int(rng.integers(1, 17)) for _ in ns]
+    _, mats = carve(torch, [n * n for n in ns], torch.float64)
+    _, pivs = carve(torch, ns, torch.int32)
+    _, rhs = carve(torch, [n * r for n, r in zip(ns, nrhs)], torch.float64)
+    for i, n in enumerate(ns):
+        mats[i].copy_(torch.from_numpy(rng.uniform(-1, 1, n * n) + np.eye(n).ravel() * 2))
+        rhs[i].copy_(torch.from_numpy(rng.uniform(-1, 1, n * nrhs[i])))
+    torch.cuda.synchronize()
+    assert all(v == 0 for v in hb.getrf_batched(ns, mats, ns, pivs))
+    b0 = [r.clone() for r in rhs]
+    torch.cuda.synchronize()
+    assert hb.getrs_batched(trans, ns, nrhs, mats, ns, pivs, rhs, ns) == 0
+    for i, n in enumerate(ns):
+        x = b0[i].clone()
+        torch.cuda.synchronize()
+        hb.dgetrs(trans, n, nrhs[i], mats[i], n, pivs[i], x, n)
+        got, want = rhs[i].cpu().numpy(), x.cpu().numpy()
+        assert same_bits(got, want), (i, n, first_diff(got, want))
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("alpha,beta", [(1.5, 0.5), (-1.0, 1.0), (1.0, 0.0), (0.0, 2.0)])
+def test_gemm_batched_matches_single(hb, cuda, ta, tb, alpha, beta):
+    torch = cuda
+    rng = np.random.default_rng(4)
+    dims = [(1, 1, 1), (0, 5, 3), (5, 0, 3), (7, 9, 0), (33, 17, 300), (64, 64, 64),
+            (129, 65, 257), (200, 100, 513)] + [tuple(int(v) for v in rng.integers(1, 150, 3))
+                                                for _ in range(12)]
+    for prec, dtype, single in (("d", torch.float64, hb.dgemm), ("s", torch.float32, hb.sgemm)):
+        m = [d[0] for d in dims]
+        n = [d[1] for d in dims]
+        k = [d[2] for d in dims]
+        lda = [max(1, (kk if ta != "N" else mm)) for mm, kk in zip(m, k)]
+        ldb = [max(1, (nn if tb != "N" else kk)) for nn, kk in zip(n, k)]
+        ldc = [max(1, mm) for mm in m]
+        ea = [la * max(1, (mm if ta != "N" else kk)) for la, mm, kk in zip(lda, m, k)]
+        eb = [lb * max(1, (kk if tb != "N" else nn)) for lb, nn, kk in zip(ldb, n, k)]
+        ec = [lc * max(1, nn) for lc, nn in zip(ldc, n)]
+        _, A = carve(torch, ea, dtype)
+        _, B = carve(torch, eb, dtype)
+        _, C = carve(torch, ec, dtype)
+        for v in A + B + C:
+            v.copy_(torch.from_numpy(rng.uniform(-1, 1, v.numel())))
+        C0 = [v.clone() for v in C]
+        torch.cuda.synchronize()
+        hb.gemm_batched(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, precision=prec)
+        for i in range(len(dims)):
+            c1 = C0[i].clone()
+            torch.cuda.synchronize()
+            single(ta, tb, m[i], n[i], k[i], alpha, A[i], lda[i], B[i], ldb[i], beta, c1, ldc[i])
+            got, want = C[i].cpu().numpy(), c1.cpu().numpy()
+            assert same_bits(got, want), (prec, i, dims[i], first_diff(got, want))
+
+
+def test_batched_invalid_arguments(hb, cuda):
+    torch = cuda
+    a = torch.zeros(16, dtype=torch.float64, device="cuda")
+    p = torch.zeros(4, dtype=torch.int32, device="cuda")
+    host = np.zeros(16)
+    with hb.ErrorCapture() as cap:
+        hb.getrf_batched([4], [a], [4], [p])  # valid
+        hb.getrf_batched([-1], [a], [4], [p])
+        hb.getrf_batched([4], [a], [3], [p])
+        hb.getrf_batched([4], [host], [4], [p])
+        assert hb.getrs_batched("X", [4], [1], [a], [4], [p], [a], [4]) == -1
+        assert hb.getrs_batched("N", [4], [1], [a], [4], [p], [a], [3]) == -8
+        hb.gemm_batched("N", "N", [2], [2], [2], 1.0, [a], [1], [a], [2], 0.0, [a], [2])
+    assert cap.errors == [("DGETRF_BATCHED", 1), ("DGETRF_BATCHED", 3),
+                          ("DGETRF_BATCHED", 2),
+                          ("DGETRS_BATCHED", 1), ("DGETRS_BATCHED", 8),
+                          ("DGEMM_BATCHED", 8)]
