@@ -21,6 +21,7 @@ __all__ = [
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
     "KERNEL_LU_LEAF", "getrf_batched", "getrs_batched", "gemm_batched",
+    "trsm_batched",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -47,6 +48,7 @@ from ._api import (  # noqa: E402  (needs lib())
     dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
     KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,
+    trsm_batched,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

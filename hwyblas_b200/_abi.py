@@ -48,6 +48,8 @@ PROTOTYPES = {
     "hwyblas_sgetrf_batched": (None, [P, P, P, P, P, I]),
     "hwyblas_dgetrs_batched": (None, [ctypes.c_char, P, P, P, P, P, P, P, I, PI]),
     "hwyblas_sgetrs_batched": (None, [ctypes.c_char, P, P, P, P, P, P, P, I, PI]),
+    "hwyblas_dtrsm_batched": (None, [ctypes.c_char] * 4 + [P, P, D, P, P, P, P, I]),
+    "hwyblas_strsm_batched": (None, [ctypes.c_char] * 4 + [P, P, F, P, P, P, P, I]),
     "hwyblas_dgemm_batched": (None, [ctypes.c_char, ctypes.c_char, P, P, P, D, P, P, P, P,
                                      D, P, P, I]),
     "hwyblas_sgemm_batched": (None, [ctypes.c_char, ctypes.c_char, P, P, P, F, P, P, P, P,

@@ -197,6 +197,13 @@ def getrs_batched(trans, n, nrhs, a, lda, ipiv, b, ldb, precision="d"):
     return info.value
 
 
+def trsm_batched(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, precision="d"):
+    """Batched TRSM (per-problem sizes as sequences, shared alpha)."""
+    fn = lib().hwyblas_dtrsm_batched if precision == "d" else lib().hwyblas_strsm_batched
+    fn(_c(side)[0:1], _c(uplo)[0:1], _c(transa)[0:1], _c(diag)[0:1], _ints(m), _ints(n),
+       float(alpha), _ptrs(a), _ints(lda), _ptrs(b), _ints(ldb), len(m))
+
+
 def gemm_batched(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
                  precision="d"):
     """Batched GEMM (per-problem sizes as sequences, shared alpha and beta)."""

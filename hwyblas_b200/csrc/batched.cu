@@ -237,6 +237,54 @@ __device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other,
   }
 }
 
+// Right-side triangular solve X op(T) = B (X is other x r, column-major ld
+// ldb), the reference's recursion for the right side: lower solves the
+// trailing block first, upper the leading one.
+template <typename T>
+__device__ void CtaTrsmRight(Mat<T> tri, bool lower, bool unit, int r, int other, T* b,
+                             long long ldb, T (*st)[33], T* sinv) {
+  if (r <= 0 || other <= 0) return;
+  int s_off[8], s_r[8], s_ph[8];
+  int sp = 0;
+  s_off[0] = 0;
+  s_r[0] = r;
+  s_ph[0] = 0;
+  while (sp >= 0) {
+    const int off = s_off[sp], rr = s_r[sp];
+    if (rr <= 32) {
+      CtaTrsmBase(tri.sub(off, off), lower, unit, rr, other, b + off * ldb, 1, ldb, st,
+                  sinv);
+      --sp;
+      continue;
+    }
+    const int r1 = max(32, (rr / 2) / 32 * 32), r2 = rr - r1;
+    const int ph = s_ph[sp]++;
+    if (ph == 2) {
+      --sp;
+      continue;
+    }
+    const bool first_trailing = lower;
+    if (ph == 0) {
+      ++sp;
+      s_off[sp] = first_trailing ? off + r1 : off;
+      s_r[sp] = first_trailing ? r2 : r1;
+      s_ph[sp] = 0;
+    } else {
+      if (lower) {
+        CtaGemm<T>(other, r1, r2, T(-1), Col(b + (off + r1) * ldb, ldb),
+                   tri.sub(off + r1, off), T(1), Col(b + off * ldb, ldb));
+      } else {
+        CtaGemm<T>(other, r2, r1, T(-1), Col(b + off * ldb, ldb), tri.sub(off, off + r1),
+                   T(1), Col(b + (off + r1) * ldb, ldb));
+      }
+      ++sp;
+      s_off[sp] = first_trailing ? off : off + r1;
+      s_r[sp] = first_trailing ? r1 : r2;
+      s_ph[sp] = 0;
+    }
+  }
+}
+
 // Shared scratch of the per-CTA LU.
 template <typename T>
 struct LuShared {
@@ -483,6 +531,38 @@ __global__ void __launch_bounds__(256) BatchedGetrsKernel(BatchArgs<T> p) {
   }
 }
 
+// TRSM (src/trsm.cc:137-180): B := alpha*B first (alpha != 1; B zeroed for
+// alpha == 0), then the recursion on op(A). flags: bit 0 right side, bit 1
+// lower, bit 2 transposed, bit 3 unit diagonal.
+template <typename T>
+__global__ void __launch_bounds__(256) BatchedTrsmKernel(BatchArgs<T> p) {
+  __shared__ LuShared<T> sh;
+  __shared__ int slot;
+  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+    const int m = p.m[id], n = p.n[id];
+    if (m == 0 || n == 0) continue;
+    const bool right = p.flags & 1, lower = p.flags & 2, trans = p.flags & 4,
+               unit = p.flags & 8;
+    T* b = p.b[id];
+    const long long ldb = p.ldb[id];
+    if (p.alpha != T(1)) {
+      for (int idx = threadIdx.x; idx < m * n; idx += blockDim.x) {
+        T& v = b[idx % m + (idx / m) * ldb];
+        v = (p.alpha == T(0)) ? T(0) : v * p.alpha;
+      }
+      __syncthreads();
+      if (p.alpha == T(0)) continue;
+    }
+    const long long la = p.lda[id];
+    const Mat<T> tri = trans ? Mat<T>{p.a[id], la, 1} : Col(p.a[id], la);
+    const bool op_lower = trans ? !lower : lower;
+    if (right)
+      CtaTrsmRight(tri, op_lower, unit, n, m, b, ldb, sh.st, sh.sinv);
+    else
+      CtaTrsmLeft(tri, op_lower, unit, m, n, b, ldb, sh.st, sh.sinv);
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) BatchedGemmKernel(BatchArgs<T> p) {
   __shared__ int slot;
@@ -600,12 +680,13 @@ struct Layout {
   }
 };
 
-enum BatchKind { kBatchGetrf = 0, kBatchGetrs = 1, kBatchGemm = 2 };
+enum BatchKind { kBatchGetrf = 0, kBatchGetrs = 1, kBatchGemm = 2, kBatchTrsm = 3 };
 
 template <typename T>
 void* KernelOf(int kind) {
   if (kind == kBatchGetrf) return reinterpret_cast<void*>(BatchedGetrfKernel<T>);
   if (kind == kBatchGetrs) return reinterpret_cast<void*>(BatchedGetrsKernel<T>);
+  if (kind == kBatchTrsm) return reinterpret_cast<void*>(BatchedTrsmKernel<T>);
   return reinterpret_cast<void*>(BatchedGemmKernel<T>);
 }
 
@@ -625,6 +706,28 @@ struct TuneKey {
 namespace hb {
 namespace {
 
+// Graphs of recent batch shapes (per host thread).
+struct GraphKey {
+  int kind, bytes, count, threads, grid;
+  void* dev;
+  void* host;
+  size_t total;
+  double alpha, beta;
+  int flags, lanes;
+  cudaStream_t stream;
+  bool operator==(const GraphKey& o) const {
+    return kind == o.kind && bytes == o.bytes && count == o.count && threads == o.threads &&
+           grid == o.grid && dev == o.dev && host == o.host && total == o.total &&
+           alpha == o.alpha && beta == o.beta && flags == o.flags && lanes == o.lanes &&
+           stream == o.stream;
+  }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec;
+};
+thread_local std::vector<GraphEntry> t_graphs;
+
 // A batch as the host sees it: per-problem sizes and device pointers.
 template <typename T>
 struct HostBatch {
@@ -642,6 +745,7 @@ double WorkOf(int kind, const HostBatch<T>& bt, int i) {
   const double m = bt.m[i], n = bt.n.empty() ? 0 : bt.n[i];
   if (kind == kBatchGetrf) return m * m * m;
   if (kind == kBatchGetrs) return m * m * (n + 1);
+  if (kind == kBatchTrsm) return m * n * (std::max(m, n) + 1);
   return m * n * (bt.k[i] + 1);
 }
 
@@ -649,7 +753,8 @@ double WorkOf(int kind, const HostBatch<T>& bt, int i) {
 // kernel with `threads` threads a CTA. Problem info lands in dev_info (if
 // non-null) on return of the stream.
 template <typename T>
-bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info) {
+bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info,
+                 bool use_graph) {
   Context& ctx = Ctx();
   const int count = bt.count;
   const Layout L(count);
@@ -681,9 +786,6 @@ bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info) 
   put_ptrs(L.off_b, bt.b.empty() ? nullptr : bt.b.data());
   put_ptrs(L.off_c, bt.c.empty() ? nullptr : bt.c.data());
   put_ptrs(L.off_ipiv, bt.ipiv.empty() ? nullptr : bt.ipiv.data());
-  if (Failed(cudaMemcpyAsync(dev, host, L.total, cudaMemcpyHostToDevice, ctx.stream),
-             "batched descriptor copy"))
-    return false;
   BatchArgs<T> args;
   args.count = count;
   args.order = reinterpret_cast<const int*>(dev + L.off_order);
@@ -708,10 +810,50 @@ bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info) 
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0);
   const int grid = std::max(1, std::min(count, ctx.num_sms * std::max(per_sm, 1)));
   void* kargs[] = {&args};
+  if (dev_info != nullptr) *dev_info = args.info;
+  // The descriptor copy and the launch replay as one CUDA graph when the
+  // same batch shape comes again (same workspace, staging buffer and kernel
+  // arguments); the legacy default stream cannot be captured.
+  if (use_graph && ctx.stream != nullptr) {
+    GraphKey key{kind, static_cast<int>(sizeof(T)), count, threads, grid, dev, host,
+                 L.total, static_cast<double>(args.alpha), static_cast<double>(args.beta),
+                 args.flags, args.lanes, ctx.stream};
+    for (auto& e : t_graphs) {
+      if (e.key == key) {
+        if (Failed(cudaGraphLaunch(e.exec, ctx.stream), "batched graph launch")) return false;
+        CountLaunch();
+        return true;
+      }
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal) ==
+              cudaSuccess;
+    if (ok) {
+      cudaMemcpyAsync(dev, host, L.total, cudaMemcpyHostToDevice, ctx.stream);
+      cudaLaunchKernel(fn, grid, threads, kargs, 0, ctx.stream);
+      ok = cudaStreamEndCapture(ctx.stream, &graph) == cudaSuccess && graph != nullptr &&
+           cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+      if (graph != nullptr) cudaGraphDestroy(graph);
+    }
+    if (ok) {
+      if (t_graphs.size() >= 8) {
+        cudaGraphExecDestroy(t_graphs.front().exec);
+        t_graphs.erase(t_graphs.begin());
+      }
+      t_graphs.push_back({key, exec});
+      if (Failed(cudaGraphLaunch(exec, ctx.stream), "batched graph launch")) return false;
+      CountLaunch();
+      return true;
+    }
+    cudaGetLastError();  // capture unavailable: launch directly
+  }
+  if (Failed(cudaMemcpyAsync(dev, host, L.total, cudaMemcpyHostToDevice, ctx.stream),
+             "batched descriptor copy"))
+    return false;
   if (Failed(cudaLaunchKernel(fn, grid, threads, kargs, 0, ctx.stream), "batched launch"))
     return false;
   CountLaunch();
-  if (dev_info != nullptr) *dev_info = args.info;
   return true;
 }
 
@@ -794,9 +936,9 @@ int TunedThreads(int kind, int median_m, int median_n) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int threads : {64, 128, 256}) {
-      LaunchBatch(kind, bt, threads, nullptr);  // warm-up
+      LaunchBatch(kind, bt, threads, nullptr, false);  // warm-up
       cudaEventRecord(e0, ctx.stream);
-      LaunchBatch(kind, bt, threads, nullptr);
+      LaunchBatch(kind, bt, threads, nullptr, false);
       cudaEventRecord(e1, ctx.stream);
       cudaEventSynchronize(e1);
       float ms = 0.f;
@@ -839,7 +981,7 @@ void RunBatch(int kind, const HostBatch<T>& bt, int* info_out, const char* name)
   if (bt.count == 0) return;
   const int threads = TunedThreads<T>(kind, Median(bt.m), bt.n.empty() ? 0 : Median(bt.n));
   int* dev_info = nullptr;
-  if (!LaunchBatch(kind, bt, threads, &dev_info)) return;
+  if (!LaunchBatch(kind, bt, threads, &dev_info, true)) return;
   LaunchFailed(name);
   if (info_out != nullptr) {
     Failed(cudaMemcpyAsync(info_out, dev_info, sizeof(int) * bt.count,
@@ -912,6 +1054,50 @@ void GetrsBatched(char trans, const int* n, const int* nrhs, T* const* a, const 
   bt.ipiv.assign(ipiv, ipiv + count);
   bt.flags = (t == 'N') ? 0 : 1;
   RunBatch(kBatchGetrs, bt, nullptr, name);
+}
+
+template <typename T>
+void TrsmBatched(char side, char uplo, char transa, char diag, const int* m, const int* n,
+                 T alpha, T* const* a, const int* lda, T* const* b, const int* ldb,
+                 int count, const char* name) {
+  auto up = [](char ch) { return (ch >= 'a' && ch <= 'z') ? static_cast<char>(ch - 32) : ch; };
+  const char sd = up(side), ul = up(uplo), ta = up(transa), dg = up(diag);
+  int pos = 0;
+  if (sd != 'L' && sd != 'R') pos = 1;
+  else if (ul != 'L' && ul != 'U') pos = 2;
+  else if (ta != 'N' && ta != 'T' && ta != 'C') pos = 3;
+  else if (dg != 'N' && dg != 'U') pos = 4;
+  else if (count < 0) pos = 12;
+  ExtentChecker ext;
+  for (int i = 0; pos == 0 && i < count; ++i) {
+    const int ka = sd == 'L' ? m[i] : n[i];
+    if (m[i] < 0) pos = 5;
+    else if (n[i] < 0) pos = 6;
+    else if (lda[i] < std::max(1, ka)) pos = 9;
+    else if (ldb[i] < std::max(1, m[i])) pos = 11;
+    else if (m[i] > 0 && n[i] > 0) {
+      const size_t ea = alpha == T(0) ? 0 : static_cast<size_t>(lda[i]) * (ka - 1) + ka;
+      const size_t eb = static_cast<size_t>(ldb[i]) * (n[i] - 1) + m[i];
+      if (!ext.Check(a[i], sizeof(T) * ea)) pos = 8;
+      else if (!ext.Check(b[i], sizeof(T) * eb)) pos = 10;
+    }
+  }
+  if (pos != 0) {
+    ReportError(name, pos);
+    return;
+  }
+  HostBatch<T> bt;
+  bt.count = count;
+  bt.m.assign(m, m + count);
+  bt.n.assign(n, n + count);
+  bt.lda.assign(lda, lda + count);
+  bt.ldb.assign(ldb, ldb + count);
+  bt.a.assign(a, a + count);
+  bt.b.assign(b, b + count);
+  bt.alpha = alpha;
+  bt.flags = (sd == 'R' ? 1 : 0) | (ul == 'L' ? 2 : 0) | (ta != 'N' ? 4 : 0) |
+             (dg == 'U' ? 8 : 0);
+  RunBatch(kBatchTrsm, bt, nullptr, name);
 }
 
 template <typename T>
@@ -1001,6 +1187,24 @@ HWYBLAS_API void hwyblas_sgetrs_batched(char trans, const hwyblas_int* n,
                                         hwyblas_int count, hwyblas_int* info) {
   hb::GetrsBatched<float>(trans, n, nrhs, a, lda, ipiv, b, ldb, count, info,
                           "SGETRS_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_dtrsm_batched(char side, char uplo, char transa, char diag,
+                                       const hwyblas_int* m, const hwyblas_int* n,
+                                       double alpha, double* const* a,
+                                       const hwyblas_int* lda, double* const* b,
+                                       const hwyblas_int* ldb, hwyblas_int count) {
+  hb::TrsmBatched<double>(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, count,
+                          "DTRSM_BATCHED");
+}
+
+HWYBLAS_API void hwyblas_strsm_batched(char side, char uplo, char transa, char diag,
+                                       const hwyblas_int* m, const hwyblas_int* n,
+                                       float alpha, float* const* a,
+                                       const hwyblas_int* lda, float* const* b,
+                                       const hwyblas_int* ldb, hwyblas_int count) {
+  hb::TrsmBatched<float>(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb, count,
+                         "STRSM_BATCHED");
 }
 
 HWYBLAS_API void hwyblas_dgemm_batched(char transa, char transb, const hwyblas_int* m,

@@ -256,7 +256,8 @@ HWYBLAS_API int hwyblas_set_mixed_slices(int slices);
  * launch per call: CTAs take problems largest first; threads per CTA come
  * from an autotuner (per routine, type and size bucket, measured once per
  * process). Every problem's result is bit-identical to the single-problem
- * routine (dgetrf_, dgetrs_, dgemm_ and their single-precision forms). Errors
+ * routine (dgetrf_, dgetrs_, dtrsm_, dgemm_ and their single-precision forms).
+ * Errors
  * are reported through the error handler with the position of the offending
  * argument (any problem). Synchronous on return. */
 HWYBLAS_API void hwyblas_dgetrf_batched(const hwyblas_int* n, double* const* a,
@@ -275,6 +276,16 @@ HWYBLAS_API void hwyblas_sgetrs_batched(char trans, const hwyblas_int* n,
                                         const hwyblas_int* lda, hwyblas_int* const* ipiv,
                                         float* const* b, const hwyblas_int* ldb,
                                         hwyblas_int count, hwyblas_int* info);
+HWYBLAS_API void hwyblas_dtrsm_batched(char side, char uplo, char transa, char diag,
+                                       const hwyblas_int* m, const hwyblas_int* n,
+                                       double alpha, double* const* a,
+                                       const hwyblas_int* lda, double* const* b,
+                                       const hwyblas_int* ldb, hwyblas_int count);
+HWYBLAS_API void hwyblas_strsm_batched(char side, char uplo, char transa, char diag,
+                                       const hwyblas_int* m, const hwyblas_int* n,
+                                       float alpha, float* const* a,
+                                       const hwyblas_int* lda, float* const* b,
+                                       const hwyblas_int* ldb, hwyblas_int count);
 HWYBLAS_API void hwyblas_dgemm_batched(char transa, char transb, const hwyblas_int* m,
                                        const hwyblas_int* n, const hwyblas_int* k,
                                        double alpha, double* const* a,

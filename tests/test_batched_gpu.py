@@ -152,3 +152,58 @@ def test_batched_invalid_arguments(hb, cuda):
                           ("DGETRF_BATCHED", 2),
                           ("DGETRS_BATCHED", 1), ("DGETRS_BATCHED", 8),
                           ("DGEMM_BATCHED", 8)]
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "U"), ("U", "N", "N"),
+                                             ("L", "T", "N"), ("U", "T", "U")])
+def test_trsm_batched_matches_single(hb, cuda, side, uplo, trans, diag):
+    torch = cuda
+    rng = np.random.default_rng(5)
+    dims = [(1, 1), (5, 33), (33, 5), (64, 17), (100, 70), (129, 40), (40, 129), (300, 3)]
+    for prec, dtype in (("d", torch.float64),):
+        m = [d[0] for d in dims]
+        n = [d[1] for d in dims]
+        ka = [mm if side == "L" else nn for mm, nn in zip(m, n)]
+        _, A = carve(torch, [k * k for k in ka], dtype)
+        _, B = carve(torch, [mm * nn for mm, nn in zip(m, n)], dtype)
+        for i, k in enumerate(ka):
+            A[i].copy_(torch.from_numpy(rng.uniform(-1, 1, k * k) + np.eye(k).ravel() * k))
+            B[i].copy_(torch.from_numpy(rng.uniform(-1, 1, m[i] * n[i])))
+        B0 = [v.clone() for v in B]
+        torch.cuda.synchronize()
+        for alpha in (1.0, -0.5):
+            for i in range(len(dims)):
+                B[i].copy_(B0[i])
+            torch.cuda.synchronize()
+            hb.trsm_batched(side, uplo, trans, diag, m, n, alpha, A, ka, B, m, precision=prec)
+            for i in range(len(dims)):
+                x = B0[i].clone()
+                torch.cuda.synchronize()
+                hb.dtrsm(side, uplo, trans, diag, m[i], n[i], alpha, A[i], ka[i], x, m[i])
+                got, want = B[i].cpu().numpy(), x.cpu().numpy()
+                assert same_bits(got, want), (side, uplo, trans, diag, alpha, i,
+                                              first_diff(got, want))
+
+
+def test_batched_repeated_shape_replays(hb, cuda):
+    """The same batch shape twice (the second call replays the captured
+    graph) with new data: both results bit-identical to single calls."""
+    torch = cuda
+    rng = np.random.default_rng(6)
+    ns = [3, 40, 70, 130, 20]
+    _, mats = carve(torch, [n * n for n in ns], torch.float64)
+    _, pivs = carve(torch, ns, torch.int32)
+    for rep in range(3):
+        host = [rng.uniform(-1, 1, n * n) for n in ns]
+        for i in range(len(ns)):
+            mats[i].copy_(torch.from_numpy(host[i]))
+        torch.cuda.synchronize()
+        info = hb.getrf_batched(ns, mats, ns, pivs)
+        for i, n in enumerate(ns):
+            a1 = torch.from_numpy(host[i]).cuda()
+            p1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            assert hb.dgetrf(n, n, a1, n, p1) == info[i]
+            assert same_bits(mats[i].cpu().numpy(), a1.cpu().numpy()), (rep, i)
+            assert np.array_equal(pivs[i].cpu().numpy(), p1.cpu().numpy())
