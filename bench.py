@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--no-dgesv", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--nrhs", type=int, default=1, help="right-hand sides of --case gesv-mixed")
     p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv-mixed"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
@@ -682,12 +683,12 @@ def run_case(args):
         call = lambda a: hb.dgetrf2(n, 16, a, n, ipiv)
     else:
         a0 = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-        b = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+        b = torch.rand(n * args.nrhs, dtype=torch.float64, device="cuda", generator=g)
         x = torch.zeros_like(b)
         if args.case == "getrf":
             call = lambda a: hb.dgetrf(n, n, a, n, ipiv)
         else:
-            call = lambda a: hb.dgesv_mixed(n, 1, a, n, ipiv, b, n, x, n)
+            call = lambda a: hb.dgesv_mixed(n, args.nrhs, a, n, ipiv, b, n, x, n)
     for _ in range(2):
         a = a0.clone()
         torch.cuda.synchronize()

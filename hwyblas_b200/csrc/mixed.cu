@@ -258,47 +258,144 @@ __global__ void __launch_bounds__(kTb)
 // remaining rows, one row per thread with the block row's 64 factor entries
 // in registers; a grid barrier ends the step. x is read and written through
 // L2 only (.cg), since rows change owner between steps.
-constexpr int kTrsvSmem = (kTb * kTb + 2 * kTb * kTrsvRhs) * 8;
+constexpr int kLd = kTb + 1;  // padded column stride of the shared blocks
+constexpr int kTrsvSmem = (kTb * kLd + 2 * kLd * kTrsvRhs) * 8;
 template <bool kLower>
 __global__ void __launch_bounds__(kTrsvThreads)
     BlockTrsvKernel(int n, int nrhs, const double* w, long long ldw,
                     const double* inv, double* x, long long ldx,
                     unsigned int* barrier, int* timeout_flag) {
   extern __shared__ double trsv_smem[];
-  double* si = trsv_smem;              // inv block, column-major kTb x kTb
-  double* sb = si + kTb * kTb;         // sb[q * kTb + r]
-  double* sx = sb + kTb * kTrsvRhs;    // sx[q * kTb + r]
+  double* si = trsv_smem;              // inv block: si[r + c * kLd]
+  double* sb = si + kTb * kLd;         // sb[q * kLd + r]
+  double* sx = sb + kLd * kTrsvRhs;    // sx[q * kLd + r]
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int g = lane >> 2, t = lane & 3;
+  const int nbl = (nrhs + 7) / 8;
   const int nblk = (n + kTb - 1) / kTb;
   unsigned int gen = 0;
   for (int step = 0; step < nblk; ++step) {
     const int blk = kLower ? step : nblk - 1 - step;
     const int r0 = blk * kTb, bs = min(kTb, n - r0);
     const double* ib = inv + static_cast<long long>(blk) * kTb * kTb;
-    for (int idx = threadIdx.x; idx < kTb * kTb; idx += kTrsvThreads) si[idx] = ib[idx];
-    for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
+    for (int idx = threadIdx.x; idx < kTb * kTb; idx += kTrsvThreads)
+      si[(idx % kTb) + (idx / kTb) * kLd] = ib[idx];
+    for (int idx = threadIdx.x; idx < kTb * nbl * 8; idx += kTrsvThreads) {
       const int r = idx % kTb, q = idx / kTb;
-      sb[idx] = r < bs ? __ldcg(x + r0 + r + q * ldx) : 0.0;
+      sb[q * kLd + r] = (r < bs && q < nrhs) ? __ldcg(x + r0 + r + q * ldx) : 0.0;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
-      const int r = idx % kTb, q = idx / kTb;
-      const double* bq = sb + q * kTb;
-      double s0 = 0.0, s1 = 0.0;
-#pragma unroll 8
-      for (int c = 0; c < kTb; c += 2) {
-        s0 = fma(si[r + c * kTb], bq[c], s0);
-        s1 = fma(si[r + (c + 1) * kTb], bq[c + 1], s1);
+    if (nrhs >= 8) {
+      // x_b = inv_b * b_b on the FP64 tensor pipe: warp w computes 16-row
+      // block w % 4 for the 8-column blocks w / 4, w / 4 + 2, ...
+      const int mb = warp % 4;
+      for (int nb = warp / 4; nb < nbl; nb += kTrsvThreads / 128) {
+        double d[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int kk = 0; kk < kTb / 8; ++kk) {
+          const int c0 = kk * 8 + t;
+          const double a0 = si[(mb * 16 + g) + c0 * kLd];
+          const double a1 = si[(mb * 16 + g + 8) + c0 * kLd];
+          const double a2 = si[(mb * 16 + g) + (c0 + 4) * kLd];
+          const double a3 = si[(mb * 16 + g + 8) + (c0 + 4) * kLd];
+          const double b0 = sb[(nb * 8 + g) * kLd + c0];
+          const double b1 = sb[(nb * 8 + g) * kLd + c0 + 4];
+          asm volatile(
+              "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+              "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+              : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+              : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+        }
+        const int q0 = nb * 8 + 2 * t, row0 = mb * 16 + g;
+        sx[q0 * kLd + row0] = d[0];
+        sx[(q0 + 1) * kLd + row0] = d[1];
+        sx[q0 * kLd + row0 + 8] = d[2];
+        sx[(q0 + 1) * kLd + row0 + 8] = d[3];
       }
-      sx[idx] = s0 + s1;
+    } else {
+      for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
+        const int r = idx % kTb, q = idx / kTb;
+        const double* bq = sb + q * kLd;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < kTb; c += 2) {
+          s0 = fma(si[r + c * kLd], bq[c], s0);
+          s1 = fma(si[r + (c + 1) * kLd], bq[c + 1], s1);
+        }
+        sx[q * kLd + r] = s0 + s1;
+      }
     }
     __syncthreads();
     if (blockIdx.x == 0) {
       for (int idx = threadIdx.x; idx < kTb * nrhs; idx += kTrsvThreads) {
         const int r = idx % kTb, q = idx / kTb;
-        if (r < bs) __stcg(x + r0 + r + q * ldx, sx[idx]);
+        if (r < bs) __stcg(x + r0 + r + q * ldx, sx[q * kLd + r]);
       }
     }
     const int lo = kLower ? r0 + bs : 0, hi = kLower ? n : r0;
+    if (nrhs >= 8) {
+      // Many right-hand sides: the update is a (rows x 64) x (64 x nrhs)
+      // product; each warp takes 16-row blocks on the FP64 tensor pipe
+      // (m16n8k8: A from the factor, B from the solved block in shared
+      // memory).
+      const int nwarps = kTrsvThreads / 32;
+      for (int rb = lo + 16 * (blockIdx.x * nwarps + warp); rb < hi;
+           rb += 16 * gridDim.x * nwarps) {
+        const int i0 = rb + g, i1 = rb + g + 8;
+        const double* w0 = w + i0 + static_cast<long long>(r0) * ldw;
+        const double* w1 = w + i1 + static_cast<long long>(r0) * ldw;
+        double af[kTb / 8][4];
+#pragma unroll
+        for (int kk = 0; kk < kTb / 8; ++kk) {
+          const int c0 = kk * 8 + t, c1 = c0 + 4;
+          af[kk][0] = (i0 < hi && c0 < bs) ? w0[static_cast<long long>(c0) * ldw] : 0.0;
+          af[kk][1] = (i1 < hi && c0 < bs) ? w1[static_cast<long long>(c0) * ldw] : 0.0;
+          af[kk][2] = (i0 < hi && c1 < bs) ? w0[static_cast<long long>(c1) * ldw] : 0.0;
+          af[kk][3] = (i1 < hi && c1 < bs) ? w1[static_cast<long long>(c1) * ldw] : 0.0;
+        }
+        // All products first, then all loads of x, then all stores: the
+        // read-modify-writes must not wait on one another.
+        double d[kTrsvRhs / 8][4];
+#pragma unroll
+        for (int nb = 0; nb < kTrsvRhs / 8; ++nb) d[nb][0] = d[nb][1] = d[nb][2] = d[nb][3] = 0.0;
+        // k outer, column blocks inner: consecutive MMAs are independent.
+#pragma unroll
+        for (int kk = 0; kk < kTb / 8; ++kk) {
+#pragma unroll
+          for (int nb = 0; nb < kTrsvRhs / 8; ++nb) {
+            if (nb >= nbl) continue;
+            const int qb = nb * 8 + g;  // this lane's B column
+            const double b0 = sx[qb * kLd + kk * 8 + t];
+            const double b1 = sx[qb * kLd + kk * 8 + t + 4];
+            asm volatile(
+                "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+                "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                : "+d"(d[nb][0]), "+d"(d[nb][1]), "+d"(d[nb][2]), "+d"(d[nb][3])
+                : "d"(af[kk][0]), "d"(af[kk][1]), "d"(af[kk][2]), "d"(af[kk][3]),
+                  "d"(b0), "d"(b1));
+          }
+        }
+        double xv[kTrsvRhs / 8][4];
+#pragma unroll
+        for (int nb = 0; nb < kTrsvRhs / 8; ++nb) {
+          const int q0 = nb * 8 + 2 * t, q1 = q0 + 1;
+          xv[nb][0] = (i0 < hi && q0 < nrhs) ? __ldcg(x + i0 + q0 * ldx) : 0.0;
+          xv[nb][1] = (i0 < hi && q1 < nrhs) ? __ldcg(x + i0 + q1 * ldx) : 0.0;
+          xv[nb][2] = (i1 < hi && q0 < nrhs) ? __ldcg(x + i1 + q0 * ldx) : 0.0;
+          xv[nb][3] = (i1 < hi && q1 < nrhs) ? __ldcg(x + i1 + q1 * ldx) : 0.0;
+        }
+#pragma unroll
+        for (int nb = 0; nb < kTrsvRhs / 8; ++nb) {
+          const int q0 = nb * 8 + 2 * t, q1 = q0 + 1;
+          if (i0 < hi && q0 < nrhs) __stcg(x + i0 + q0 * ldx, xv[nb][0] - d[nb][0]);
+          if (i0 < hi && q1 < nrhs) __stcg(x + i0 + q1 * ldx, xv[nb][1] - d[nb][1]);
+          if (i1 < hi && q0 < nrhs) __stcg(x + i1 + q0 * ldx, xv[nb][2] - d[nb][2]);
+          if (i1 < hi && q1 < nrhs) __stcg(x + i1 + q1 * ldx, xv[nb][3] - d[nb][3]);
+        }
+      }
+      if (!GridBarrier(barrier, gridDim.x, ++gen, timeout_flag)) return;
+      continue;
+    }
     for (int i = lo + blockIdx.x * kTrsvThreads + threadIdx.x; i < hi;
          i += gridDim.x * kTrsvThreads) {
       const double* wi = w + i + static_cast<long long>(r0) * ldw;
@@ -307,7 +404,7 @@ __global__ void __launch_bounds__(kTrsvThreads)
       for (int c = 0; c < kTb; ++c)
         l[c] = c < bs ? wi[static_cast<long long>(c) * ldw] : 0.0;
       for (int q = 0; q < nrhs; ++q) {
-        const double* xq = sx + q * kTb;
+        const double* xq = sx + q * kLd;
         double a0 = 0.0, a1 = 0.0;
 #pragma unroll
         for (int c = 0; c < kTb; c += 2) {
