@@ -66,7 +66,10 @@ def parse():
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--nrhs", type=int, default=1, help="right-hand sides of --case gesv-mixed")
-    p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv-mixed"],
+    p.add_argument("--kernels", action="store_true",
+                   help="with --case: per-kernel device time of the call (CUPTI activity "
+                        "records through torch.profiler)")
+    p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv", "gesv-mixed"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
                         "gesv-n, each after one warm-up call")
@@ -606,6 +609,11 @@ def run_ours(args):
     per_launch_ops = per_step_ops / max(1.0, d["ozaki_launches_per_step"])
     oz_ms = d["ozaki_kernel_ms_per_launch"]
     achieved = per_launch_ops / (oz_ms * 1e-3) / 1e12 if oz_ms > 0 else None
+    # DRAM traffic of the slice-product kernel per launch at n = 8192, S = 8
+    # (ncu dram__bytes_read.sum + dram__bytes_write.sum of this workload, a
+    # one-pass capture): high pass 7.886e9 B, low pass 4.341e9 B. Other
+    # shapes have no measured figure.
+    traffic = (7.886e9 + 4.341e9) / 2.0 if (n == 8192 and S == 8) else None
     dm_ms = d["dmma_kernel_ms_per_launch"]
     dm_achieved = 2.0 * n ** 3 / (dm_ms * 1e-3) / 1e12 if dm_ms > 0 else None
 
@@ -643,7 +651,8 @@ def run_ours(args):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": int8_peak,
                          "unit": "TOPS (INT8)",
                          "frac": achieved / int8_peak if achieved else None,
-                         "traffic": None,
+                         "traffic": traffic,
+                         "traffic_unit": "bytes per launch (DRAM, ncu)",
                          "kernel": "OzakiGemmKernel (slice products, "
                                    f"{d['ozaki_launches_per_step']:.0f} launches per step)",
                          "peak_source": f"2 x bf16_tflops of {peak_kind} MEASURED_PEAKS "
@@ -687,16 +696,38 @@ def run_case(args):
         x = torch.zeros_like(b)
         if args.case == "getrf":
             call = lambda a: hb.dgetrf(n, n, a, n, ipiv)
+        elif args.case == "gesv":
+            call = lambda a: hb.dgesv(n, args.nrhs, a, n, ipiv, b.clone(), n)
         else:
             call = lambda a: hb.dgesv_mixed(n, args.nrhs, a, n, ipiv, b, n, x, n)
-    for _ in range(2):
-        a = a0.clone()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = call(a)
-        torch.cuda.synchronize()
-    print(json.dumps({"case": args.case, "n": n, "ms": (time.perf_counter() - t0) * 1e3,
-                      "result": r}))
+    a = a0.clone()
+    call(a)  # warm-up
+    a = a0.clone()
+    torch.cuda.synchronize()
+    prof = None
+    if args.kernels:
+        from torch.profiler import ProfilerActivity, profile
+        prof = profile(activities=[ProfilerActivity.CUDA])
+        prof.__enter__()
+    t0 = time.perf_counter()
+    r = call(a)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    out = {"case": args.case, "n": n, "nrhs": args.nrhs, "ms": ms, "result": r}
+    if prof is not None:
+        prof.__exit__(None, None, None)
+        rows = []
+        for e in prof.key_averages():
+            t = getattr(e, "device_time_total", 0) or 0
+            if t > 0:
+                name = e.key.replace("(anonymous namespace)::", "").replace("void ", "")
+                rows.append((t, e.count, name.split("(")[0][-70:]))
+        rows.sort(reverse=True)
+        total = sum(r_[0] for r_ in rows)
+        out["kernel_sum_ms"] = total / 1e3
+        out["kernels"] = [{"name": k, "launches": c, "ms": t / 1e3,
+                           "share": t / total if total else 0.0} for t, c, k in rows[:12]]
+    print(json.dumps(out))
     return 0
 
 
