@@ -611,11 +611,14 @@ int OzakiMaxK(int S) { return static_cast<int>((2147483647LL / (S * 16384LL)) / 
 // FP64 path ran instead).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite) {
+                  bool check_finite, int ws_set) {
+  const int ws_emul = ws_set ? kWsEmul2 : kWsEmul;
+  const int ws_acc = ws_set ? kWsEmulAcc2 : kWsEmulAcc;
+  const int ws_w = ws_set ? kWsEmulW2 : kWsEmulW;
   Context& ctx = Ctx();
   cudaStream_t st = ctx.stream;
   const int S = std::min(8, std::max(1, slices));
-  int* exps = static_cast<int*>(Workspace(kWsEmulAcc, sizeof(int) * (m + n + 64)));
+  int* exps = static_cast<int*>(Workspace(ws_acc, sizeof(int) * (m + n + 64)));
   int* row_exp = exps;
   int* col_exp = exps + m;
   int* nonfinite = exps + m + n;
@@ -641,7 +644,7 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
   const int kchunk = std::min(k, kmax);
   const long long kp = (static_cast<long long>(kchunk) + 15) / 16 * 16;
   int8_t* slices_a = static_cast<int8_t*>(
-      Workspace(kWsEmul, static_cast<size_t>(S) * (static_cast<size_t>(m) + n) * kp + 256));
+      Workspace(ws_emul, static_cast<size_t>(S) * (static_cast<size_t>(m) + n) * kp + 256));
   int8_t* slices_b = slices_a + static_cast<size_t>(S) * m * kp;
   OzakiParams p;
   p.m = m;
@@ -651,7 +654,7 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
   p.alpha = alpha;
   p.c = c;
   p.ldc = ldc;
-  p.w = (S > 4) ? static_cast<double*>(Workspace(kWsEmulW, sizeof(double) *
+  p.w = (S > 4) ? static_cast<double*>(Workspace(ws_w, sizeof(double) *
                                                             static_cast<size_t>(m) * n))
                 : nullptr;
   p.timeout_flag = ctx.dev_status;

@@ -75,7 +75,10 @@ enum WorkspaceSlot : int {
   kWsBatch = 11,
   kWsEmulW = 12,   // emulated-GEMM FP64 partial sums between passes
   kWsStageX = 13,  // host-pointer staging of a solver's solution
-  kNumWorkspaceSlots = 14
+  kWsEmul2 = 14,   // emulated-GEMM buffers of a second, concurrent stream
+  kWsEmulAcc2 = 15,
+  kWsEmulW2 = 16,
+  kNumWorkspaceSlots = 17
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -168,10 +171,12 @@ void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
 // returns the slice count used, 0 if non-finite inputs sent it to Dgemm, -1
 // on a CUDA error. check_finite = false skips that test and its host
 // synchronization (callers whose inputs are known finite, or that detect a
-// non-finite result themselves).
+// non-finite result themselves). ws_set 1 takes a second set of workspace
+// slots, for a call that runs concurrently with another one on a second
+// stream.
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite = true);
+                  bool check_finite = true, int ws_set = 0);
 int OzakiMaxK(int S);
 // out(:, jj) = op(A) op(B)(:, cols[jj]) in double-double (error reference).
 void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,

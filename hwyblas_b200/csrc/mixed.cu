@@ -631,25 +631,97 @@ void MixedSolve(bool lu, int n, int nrhs, MixedBuffers& bf, const double* src,
 // slicing and epilogue (measured at n = 16384: 1024 beats 512 by ~5 %).
 int MixedBlock(int n) { return n >= 8192 ? 1024 : (n >= 4096 ? 512 : 256); }
 
-// Right-looking LU of w with FP64 panels and Ozaki trailing updates.
+// A high-priority stream of the calling thread for the look-ahead panel
+// work, and two events to order it against the context's stream.
+struct Lookahead {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t to_look = nullptr, to_main = nullptr;
+  bool ok = false;
+};
+Lookahead& GetLookahead() {
+  static thread_local Lookahead la;
+  if (!la.ok) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    la.ok = cudaStreamCreateWithPriority(&la.stream, cudaStreamNonBlocking, greatest) ==
+                cudaSuccess &&
+            cudaEventCreateWithFlags(&la.to_look, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&la.to_main, cudaEventDisableTiming) == cudaSuccess;
+    if (!la.ok) cudaGetLastError();
+  }
+  return la;
+}
+
+// Runs f with the context's stream switched to s.
+template <typename F>
+void OnStream(cudaStream_t s, F f) {
+  Context& ctx = Ctx();
+  const cudaStream_t saved = ctx.stream;
+  ctx.stream = s;
+  f();
+  ctx.stream = saved;
+}
+
+// Right-looking LU of w with FP64 panels and Ozaki trailing updates, with a
+// look-ahead of one panel: on a high-priority stream, the pivots of panel j
+// are applied, the columns of panel j+1 are updated first and panel j+1 is
+// factored, while the context's stream updates the rest of the trailing
+// matrix. The two touch disjoint columns; each waits for the other where one
+// reads what the other writes (the row interchanges need the previous
+// trailing update finished, the trailing update needs the interchanges).
 void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slices) {
+  Context& ctx = Ctx();
   const int nb = MixedBlock(n);
   const int lw = static_cast<int>(ldw);
+  const cudaStream_t main = ctx.stream;
+  Lookahead& la = GetLookahead();
+  const cudaStream_t look = la.ok ? la.stream : main;
+  auto signal = [&](cudaEvent_t ev, cudaStream_t from, cudaStream_t to) {
+    if (from == to) return;
+    cudaEventRecord(ev, from);
+    cudaStreamWaitEvent(to, ev, 0);
+  };
+  const auto update = [&](int j, int jb, int c0, int nc, int ws_set) {
+    // Columns [c0, c0 + nc) of the trailing matrix: U12 by the FP64
+    // triangular solve, then A22 -= L21 U12 on the INT8 tensor cores.
+    const int rest = n - j - jb;
+    TrsmFull<double>(true, true, false, true, jb, nc, 1.0, At(w, ldw, j, j), lw,
+                     At(w, ldw, j, c0), lw);
+    DgemmEmulated(rest, nc, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
+                  ColMajor<double>(At(w, ldw, j, c0), ldw), 1.0, At(w, ldw, j + jb, c0), lw,
+                  slices, false, ws_set);
+  };
+  signal(la.to_look, main, look);
+  OnStream(look, [&] {
+    const int jb0 = std::min(nb, n);
+    GetrfPanel(n, jb0, w, lw, ipiv, info, 0);
+  });
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
-    GetrfPanel(n - j, jb, At(w, ldw, j, j), lw, ipiv + j, info, j);
-    AdjustPivots(ipiv, j, j + jb, j);
-    if (j > 0) Laswp<double>(j, w, lw, j + 1, j + jb, ipiv, 1);
-    if (j + jb < n) {
-      const int rest = n - j - jb;
-      Laswp<double>(rest, At(w, ldw, 0, j + jb), lw, j + 1, j + jb, ipiv, 1);
-      TrsmFull<double>(true, true, false, true, jb, rest, 1.0, At(w, ldw, j, j), lw,
-                       At(w, ldw, j, j + jb), lw);
-      DgemmEmulated(rest, rest, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
-                    ColMajor<double>(At(w, ldw, j, j + jb), ldw), 1.0,
-                    At(w, ldw, j + jb, j + jb), lw, slices, false);
+    const int rest = n - j - jb;
+    const int next = std::min(nb, rest);
+    // Panel j is factored (on look). Its interchanges reach every other
+    // column once main's previous trailing update is done.
+    signal(la.to_look, main, look);
+    OnStream(look, [&] {
+      if (j > 0) AdjustPivots(ipiv, j, j + jb, j);
+      if (j > 0) Laswp<double>(j, w, lw, j + 1, j + jb, ipiv, 1);
+      if (rest > 0) {
+        Laswp<double>(rest, At(w, ldw, 0, j + jb), lw, j + 1, j + jb, ipiv, 1);
+        update(j, jb, j + jb, next, 1);
+      }
+    });
+    if (rest > next) signal(la.to_main, look, main);
+    if (rest > 0) {
+      OnStream(look, [&] {
+        GetrfPanel(rest, next, At(w, ldw, j + jb, j + jb), lw, ipiv + j + jb, info, j + jb);
+      });
+    }
+    if (rest > next) {
+      OnStream(main, [&] { update(j, jb, j + jb + next, rest - next, 0); });
     }
   }
+  signal(la.to_main, look, main);
 }
 
 // Right-looking lower Cholesky of w (full symmetric storage) with FP64
