@@ -266,14 +266,14 @@ struct LeafArgs {
 // candidates through distributed shared memory (each publishes into its own
 // shared slot, one cluster barrier, then every CTA reads the P slots), which
 // replaces the global-memory slots and polling of the cooperative variant.
-template <typename T, bool kCluster>
+template <typename T, bool kCluster, int W>
 __global__ void __launch_bounds__(kLeafThreads)
     GetrfLeafPanelKernel(LeafArgs<T> p) {
   extern __shared__ __align__(16) uint8_t leaf_smem[];
   T* sp = reinterpret_cast<T*>(leaf_smem);  // column-major [w][R]
-  __shared__ T s_piv[kLeafW], s_rowj[kLeafW];
-  __shared__ T s_cand[kLeafMaxP * (2 * kLeafW + 2)];
-  __shared__ T s_slot[2 * (2 * kLeafW + 2)];  // kCluster: own slot per parity
+  __shared__ T s_piv[W], s_rowj[W];
+  __shared__ T s_cand[(kCluster ? kLeafMaxCluster : kLeafMaxP) * (2 * W + 2)];
+  __shared__ T s_slot[2 * (2 * W + 2)];  // kCluster: own slot per parity
   __shared__ T s_wv[kLeafThreads / 32];
   __shared__ int s_wi[kLeafThreads / 32];
   __shared__ int s_p, s_abort;
@@ -282,19 +282,19 @@ __global__ void __launch_bounds__(kLeafThreads)
   const int r0 = cta * rows_per, r1 = min(p.m, r0 + rows_per);
   const int R = rows_per;
   const int w = p.w;
-  const int slot_len = 2 * kLeafW + 2;
+  const int slot_len = 2 * W + 2;
   T* cand = p.xchg;  // [2][P][slot_len]
   unsigned int* tags = p.tags;
 
   if (threadIdx.x == 0) s_abort = 0;
   for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
     // All of a row's loads in flight before its shared-memory stores.
-    T v[kLeafW];
+    T v[W];
 #pragma unroll
-    for (int c = 0; c < kLeafW; ++c)
+    for (int c = 0; c < W; ++c)
       if (c < w) v[c] = p.a[(r0 + lr) + c * p.lda];
 #pragma unroll
-    for (int c = 0; c < kLeafW; ++c)
+    for (int c = 0; c < W; ++c)
       if (c < w) sp[c * R + lr] = v[c];
   }
   // kCluster: every CTA of the cluster is running before any remote access.
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         mine[2 + threadIdx.x] =
             (ci != 0x7fffffff) ? sp[threadIdx.x * R + (ci - r0)] : T(0);
         if (j >= r0 && j < r1)
-          mine[2 + kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
+          mine[2 + W + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
       }
       cluster.sync();
       for (int idx = threadIdx.x; idx < P * slot_len; idx += blockDim.x) {
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kLeafThreads)
       }
       __syncthreads();
       if (threadIdx.x < w)
-        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + kLeafW + threadIdx.x];
+        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + W + threadIdx.x];
     } else if (P == 1) {
       if (threadIdx.x == 0) {
         s_cand[0] = s_wv[0];
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         slot[2 + threadIdx.x] =
             (ci != 0x7fffffff) ? sp[threadIdx.x * R + (ci - r0)] : T(0);
         if (j >= r0 && j < r1)
-          slot[2 + kLeafW + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
+          slot[2 + W + threadIdx.x] = sp[threadIdx.x * R + (j - r0)];
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kLeafThreads)
         s_cand[idx] = *(volatile const T*)&cand[par * P * slot_len + idx];
       __syncthreads();
       if (threadIdx.x < w)
-        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + kLeafW + threadIdx.x];
+        s_rowj[threadIdx.x] = s_cand[(j / rows_per) * slot_len + 2 + W + threadIdx.x];
     }
     // (c) the global pivot: the reference's IAMAX over rows j..m-1; warp 0
     // picks the winner among the candidates and fills the pivot row.
@@ -640,36 +640,35 @@ void AdjustPivots(int* ipiv, int begin, int end, int delta) {
   LaunchFailed("adjust pivots");
 }
 
+// Rows per CTA of the 32-column leaf: its 32 columns and the static slots
+// stay within the 227 KB of shared memory a CTA can have.
+constexpr int kWideLeafRows = 832;
+
 template <typename T>
-void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
-               int info_base) {
+void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
+               int leaf_w) {
   Context& ctx = Ctx();
   const int w = std::min(m, n);
   const int lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
-  const int P = (m + kLeafMaxRows - 1) / kLeafMaxRows;
+  const bool wide = leaf_w == 32 && w > kLeafW;
+  const int max_rows = wide ? kWideLeafRows : kLeafMaxRows;
+  const int P = (m + max_rows - 1) / max_rows;
   const int R = (m + P - 1) / P;
-  if (P > kLeafMaxP) {
-    fprintf(stderr, "hwyblas_b200: LU panel of %d rows exceeds %d\n", m,
-            kLeafMaxP * kLeafMaxRows);
+  if (P > kLeafMaxP || (wide && P > kLeafMaxCluster)) {
+    fprintf(stderr, "hwyblas_b200: LU panel of %d rows exceeds the leaf's limit\n", m);
     Failed(cudaErrorInvalidValue, "getrf leaf size");
     return;
   }
   const size_t smem = static_cast<size_t>(w) * R * sizeof(T);
   const int smem_max = kLeafW * kLeafMaxRows * static_cast<int>(sizeof(T));
-  static int max_cluster = 0;
+  const int smem_wide = 32 * kWideLeafRows * static_cast<int>(sizeof(T));
+  static int max_cluster = 0, max_cluster_wide = 0;
   static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true>,
-                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    // The largest cluster of full-size leaf CTAs the device can co-schedule.
+  auto cluster_limit = [](const void* fn, int smem_bytes) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kLeafMaxCluster);
     cfg.blockDim = dim3(kLeafThreads);
-    cfg.dynamicSmemBytes = smem_max;
+    cfg.dynamicSmemBytes = smem_bytes;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeClusterDimension;
     attr.val.clusterDim.x = kLeafMaxCluster;
@@ -678,13 +677,32 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     int size = 0;
-    if (cudaOccupancyMaxPotentialClusterSize(&size, GetrfLeafPanelKernel<T, true>,
-                                             &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxPotentialClusterSize(&size, fn, &cfg) != cudaSuccess) {
       cudaGetLastError();
       size = 0;
     }
-    max_cluster = std::min(size, kLeafMaxCluster);
+    return std::min(size, kLeafMaxCluster);
+  };
+  if (!configured) {
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, false, kLeafW>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true, kLeafW>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true, kLeafW>,
+                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true, 32>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_wide);
+    cudaFuncSetAttribute(GetrfLeafPanelKernel<T, true, 32>,
+                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    max_cluster = cluster_limit(
+        reinterpret_cast<const void*>(GetrfLeafPanelKernel<T, true, kLeafW>), smem_max);
+    max_cluster_wide = cluster_limit(
+        reinterpret_cast<const void*>(GetrfLeafPanelKernel<T, true, 32>), smem_wide);
     configured = true;
+  }
+  if (wide && P > max_cluster_wide) {
+    Failed(cudaErrorInvalidValue, "getrf wide leaf cluster");
+    return;
   }
   LeafArgs<T> args;
   args.m = m;
@@ -702,7 +720,7 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
                                               slot_bytes);
   args.timeout_flag = ctx.dev_status;
   cudaEvent_t t0 = KernelTimerStart(kFamilyLuLeaf, ctx.stream);
-  if (P > 1 && P <= max_cluster) {
+  if (wide || (P > 1 && P <= max_cluster)) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P);
     cfg.blockDim = dim3(kLeafThreads);
@@ -715,17 +733,22 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
     attr.val.clusterDim.z = 1;
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
-    Failed(cudaLaunchKernelEx(&cfg, GetrfLeafPanelKernel<T, true>, args),
-           "getrf leaf (cluster)");
+    if (wide) {
+      Failed(cudaLaunchKernelEx(&cfg, GetrfLeafPanelKernel<T, true, 32>, args),
+             "getrf wide leaf (cluster)");
+    } else {
+      Failed(cudaLaunchKernelEx(&cfg, GetrfLeafPanelKernel<T, true, kLeafW>, args),
+             "getrf leaf (cluster)");
+    }
   } else if (P > 1) {
     cudaMemsetAsync(args.tags, 0, sizeof(unsigned int) * 2 * P, ctx.stream);
     void* kargs[] = {&args};
     Failed(cudaLaunchCooperativeKernel(
-               reinterpret_cast<void*>(GetrfLeafPanelKernel<T, false>), P,
+               reinterpret_cast<void*>(GetrfLeafPanelKernel<T, false, kLeafW>), P,
                kLeafThreads, kargs, smem, ctx.stream),
            "getrf leaf (cooperative)");
   } else {
-    GetrfLeafPanelKernel<T, false><<<1, kLeafThreads, smem, ctx.stream>>>(args);
+    GetrfLeafPanelKernel<T, false, kLeafW><<<1, kLeafThreads, smem, ctx.stream>>>(args);
   }
   KernelTimerStop(t0, ctx.stream);
   CountLaunch();
@@ -737,8 +760,8 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info,
     LaunchFailed("getrf leaf trailing");
   }
 }
-template void GetrfLeaf<double>(int, int, double*, int, int*, int*, int);
-template void GetrfLeaf<float>(int, int, float*, int, int*, int*, int);
+template void GetrfLeaf<double>(int, int, double*, int, int*, int*, int, int);
+template void GetrfLeaf<float>(int, int, float*, int, int*, int*, int, int);
 
 void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base) {
   PotrfLeafKernel<<<1, 256, 0, Ctx().stream>>>(upper ? 1 : 0, n, a, lda, info,

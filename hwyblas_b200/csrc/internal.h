@@ -135,7 +135,8 @@ void AdjustPivots(int* ipiv, int begin, int end, int delta);
 // 1-based); *info (device) set to info_base + j + 1 at the first zero pivot
 // if it is still 0.
 template <typename T>
-void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base);
+void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
+               int leaf_w = 16);
 // PotrfLeaf on device: n <= 64; sets *info to info_base + j + 1 and stops at
 // the first non-positive (or NaN) diagonal, if *info is still 0.
 void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base);
@@ -151,7 +152,10 @@ void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
 void Potrf(bool upper, int n, double* a, int lda, int* info);
 // Getrf2 / Potrf2 of a block whose first column is global column col0 (for
 // INFO); the Cholesky one turns later kernels into no-ops after a failure.
-void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0);
+// GetrfPanel with leaf_w = 32 stops the recursion at 32 columns (not the
+// reference's structure; for the mixed solver's panels).
+void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0,
+                int leaf_w = 16);
 void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
 void Potrf2(bool upper, int n, double* a, int lda, int* info);
 void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
