@@ -24,9 +24,11 @@
 // (about 8*S - 1 significant bits), which sets the refinement's contraction.
 //
 // Refinement solves: the diagonal 64 x 64 blocks of the factors are inverted
-// once; each triangular solve is then one cooperative kernel that walks the
-// block rows (x_b = inv(T_bb) r_b, then every CTA updates its share of the
-// remaining rows) with a grid barrier per block.
+// once; each triangular solve is then one cooperative kernel per group of
+// 16-column chains of right-hand sides in which each solved 64-row block is
+// published through a flag and consumed by the CTAs owning later blocks
+// (ChainTrsvKernel); above kChainSlots blocks per CTA, a kernel with a grid
+// barrier per block (BlockTrsvKernel).
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -419,6 +421,268 @@ __global__ void __launch_bounds__(kTrsvThreads)
   }
 }
 
+// Triangular solve without grid barriers: x := T^{-1} x in 16-column chains
+// of right-hand sides, one group of CTAs per chain. Block position p (solve
+// order: block p for the lower triangle, nblk-1-p for the upper) is owned by
+// one CTA of the chain, in zigzag order (round r = p / P, CTA p % P for even
+// r and P-1 - p % P for odd r, which evens out the row blocks' unequal
+// work). A CTA keeps the partial right-hand sides of its blocks in shared
+// memory and sweeps the positions in order: once x_p is published (a flag
+// per position), it subtracts T_ip x_p from each of its blocks i after p.
+// The owner of p+1 does that block first and finishes it at once,
+// x_{p+1} = inv_{p+1} * acc, and publishes it before its other blocks: the
+// critical path is one 64 x 64 product, one inverse product and one flag
+// per block. Factor tiles and inverse blocks stream through a 4-stage
+// cp.async ring in the order the sweeps consume them, independent of x (the
+// depth matters: 3 stages left the critical tiles waiting on HBM).
+constexpr int kCw = 16;           // right-hand sides per chain
+constexpr int kChainLd = kTb + 4; // padded stride: conflict-free fragments
+constexpr int kChainSlots = 8;    // row blocks per CTA at most
+constexpr int kChainStages = 4;
+constexpr int kChainThreads = 256;
+constexpr int kChainTile = kTb * kChainLd;  // doubles per staged tile
+constexpr int kChainVec = kCw * kChainLd;   // doubles per 64 x 16 block
+constexpr int kChainSmem =
+    (kChainStages * kChainTile + (kChainSlots + 2) * kChainVec) * 8;
+
+struct ChainOwn {
+  int c, P, owned, nblk;
+  __device__ int Pos(int s) const { return s * P + ((s & 1) ? P - 1 - c : c); }
+  __device__ bool Owns(int p) const {
+    const int r = p / P, j = p % P;
+    return ((r & 1) ? P - 1 - j : j) == c;
+  }
+};
+
+// Walks the items of a CTA in consumption order: sweep -1 holds the inverse
+// of position 0 (its owner only); sweep p >= 0 holds, for each own slot s
+// with Pos(s) > p in order, the tile (s, p) and, when Pos(s) == p + 1, the
+// inverse of slot s right after it.
+struct ChainCursor {
+  int p = -1, s = 0, sf = 0, phase = 0;
+  // kind: 0 tile, 1 inverse; false at the end.
+  __device__ bool Next(const ChainOwn& o, int& kind, int& slot, int& sweep) {
+    while (true) {
+      if (p < 0) {
+        if (phase == 0 && o.owned > 0 && o.Pos(0) == 0) {
+          phase = 1;
+          kind = 1, slot = 0, sweep = -1;
+          return true;
+        }
+        p = 0, phase = 0;
+        while (sf < o.owned && o.Pos(sf) <= p) ++sf;
+        s = sf;
+        continue;
+      }
+      if (p > o.nblk - 2) return false;
+      if (s >= o.owned) {
+        ++p, phase = 0;
+        while (sf < o.owned && o.Pos(sf) <= p) ++sf;
+        s = sf;
+        continue;
+      }
+      sweep = p, slot = s;
+      if (phase == 0) {
+        kind = 0;
+        if (o.Pos(s) == p + 1) phase = 1; else ++s;
+      } else {
+        kind = 1, phase = 0, ++s;
+      }
+      return true;
+    }
+  }
+};
+
+__device__ __forceinline__ void CpAsync16(double* dst, const double* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+               :
+               : "r"(SmemAddr(dst)), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void CpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// One m16n8k8 FP64 product chain over k = 0..63: d += A(16 x 64) B(64 x 8),
+// A column-major with stride kChainLd starting at row `row`, B stored by
+// column (b[col * kChainLd + k]).
+__device__ __forceinline__ void ChainMma(const double* a, int row, const double* b,
+                                         int g, int t, double d[4]) {
+#pragma unroll
+  for (int kk = 0; kk < kTb / 8; ++kk) {
+    const int c0 = kk * 8 + t;
+    const double a0 = a[c0 * kChainLd + row + g];
+    const double a1 = a[c0 * kChainLd + row + g + 8];
+    const double a2 = a[(c0 + 4) * kChainLd + row + g];
+    const double a3 = a[(c0 + 4) * kChainLd + row + g + 8];
+    const double b0 = b[g * kChainLd + c0];
+    const double b1 = b[g * kChainLd + c0 + 4];
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+        "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+  }
+}
+
+template <bool kLower>
+__global__ void __launch_bounds__(kChainThreads, 1)
+    ChainTrsvKernel(int n, int nrhs, const double* w, long long ldw, const double* inv,
+                    double* x, long long ldx, int P, unsigned int* flags,
+                    unsigned int epoch, int* timeout_flag) {
+  extern __shared__ __align__(16) double chain_smem[];
+  double* stage = chain_smem;                        // kChainStages tiles
+  double* acc = stage + kChainStages * kChainTile;   // kChainSlots blocks
+  double* xs = acc + kChainSlots * kChainVec;        // 2 blocks
+  __shared__ int s_ok;
+  const int nblk = (n + kTb - 1) / kTb;
+  const int chain = blockIdx.x / P;
+  const int q0 = chain * kCw;
+  if (q0 >= nrhs) return;
+  const int ncols = min(kCw, nrhs - q0);
+  const int nbl = (ncols + 7) / 8;
+  ChainOwn own;
+  own.c = blockIdx.x % P, own.P = P, own.nblk = nblk;
+  own.owned = 0;
+  while (own.owned < kChainSlots && own.Pos(own.owned) < nblk) ++own.owned;
+  if (own.owned == 0) return;
+  unsigned int* cflags = flags + static_cast<long long>(chain) * nblk;
+  double* xc = x + static_cast<long long>(q0) * ldx;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, t = lane & 3;
+  const int rg = warp & 3, nb = warp >> 2;  // 16-row group, 8-column block
+  auto blk = [&](int p) { return kLower ? p : nblk - 1 - p; };
+
+  // Partial right-hand sides of the own blocks: b restricted to their rows.
+  for (int s = 0; s < own.owned; ++s) {
+    const int r0 = blk(own.Pos(s)) * kTb, bs = min(kTb, n - r0);
+    for (int idx = tid; idx < kTb * kCw; idx += kChainThreads) {
+      const int r = idx % kTb, q = idx / kTb;
+      acc[s * kChainVec + q * kChainLd + r] =
+          (r < bs && q < ncols) ? xc[r0 + r + static_cast<long long>(q) * ldx] : 0.0;
+    }
+  }
+
+  // Stages one item: tile (rows of slot s, columns of position p) or the
+  // inverse block of slot s, zero-filled outside the matrix.
+  auto issue = [&](int kind, int slot, int sweep, double* dst) {
+    const double* src;
+    long long ld;
+    int rows, cols;
+    if (kind == 0) {
+      const int ri = blk(own.Pos(slot)) * kTb, ci = blk(sweep) * kTb;
+      src = w + ri + static_cast<long long>(ci) * ldw;
+      ld = ldw, rows = min(kTb, n - ri), cols = min(kTb, n - ci);
+    } else {
+      src = inv + static_cast<long long>(blk(own.Pos(slot))) * kTb * kTb;
+      ld = kTb, rows = kTb, cols = kTb;
+    }
+#pragma unroll
+    for (int j = 0; j < kTb * kTb / 2 / kChainThreads; ++j) {
+      const int idx = tid + j * kChainThreads;
+      const int col = idx / (kTb / 2), row = (idx % (kTb / 2)) * 2;
+      const int bytes = col < cols ? max(0, min(2, rows - row)) * 8 : 0;
+      CpAsync16(dst + col * kChainLd + row, bytes > 0 ? src + row + col * ld : w, bytes);
+    }
+  };
+
+  ChainCursor fetch, use;
+  int fk, fs, fp;
+#pragma unroll
+  for (int i = 0; i < kChainStages - 1; ++i) {
+    if (fetch.Next(own, fk, fs, fp)) issue(fk, fs, fp, stage + i * kChainTile);
+    CpAsyncCommit();
+  }
+  int item = 0, cur_sweep = -2;
+  int kind, slot, sweep;
+  while (use.Next(own, kind, slot, sweep)) {
+    if (sweep != cur_sweep) {
+      cur_sweep = sweep;
+      if (sweep >= 0 && !own.Owns(sweep)) {
+        // Wait for x at this position, then bring it into shared memory.
+        if (tid == 0) {
+          uint32_t polls = 0;
+          int good = 1;
+          while (true) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                         : "=r"(v)
+                         : "l"(cflags + sweep)
+                         : "memory");
+            if (v == epoch) break;
+            if ((++polls & 255u) == 0 &&
+                (*reinterpret_cast<volatile int*>(timeout_flag) != 0 || polls >= kMaxPolls)) {
+              atomicExch(timeout_flag, 1);
+              good = 0;
+              break;
+            }
+          }
+          s_ok = good;
+        }
+        __syncthreads();
+        if (!s_ok) break;  // timed out: the host reports it
+        const int r0 = blk(sweep) * kTb, bs = min(kTb, n - r0);
+        double* xd = xs + (sweep & 1) * kChainVec;
+        for (int idx = tid; idx < kTb * kCw; idx += kChainThreads) {
+          const int r = idx % kTb, q = idx / kTb;
+          xd[q * kChainLd + r] =
+              (r < bs && q < ncols) ? __ldcg(xc + r0 + r + static_cast<long long>(q) * ldx)
+                                    : 0.0;
+        }
+      }
+    }
+    CpAsyncWait<kChainStages - 2>();
+    __syncthreads();
+    // Refill the stage consumed one item ago.
+    if (fetch.Next(own, fk, fs, fp))
+      issue(fk, fs, fp, stage + ((item + kChainStages - 1) % kChainStages) * kChainTile);
+    CpAsyncCommit();
+    const double* tile = stage + (item % kChainStages) * kChainTile;
+    double* as = acc + slot * kChainVec;
+    if (kind == 0) {
+      // acc_s -= T(rows of s, columns of sweep) * x_sweep
+      if (nb < nbl) {
+        double d[4] = {0.0, 0.0, 0.0, 0.0};
+        ChainMma(tile, rg * 16, xs + (sweep & 1) * kChainVec + nb * 8 * kChainLd, g, t, d);
+        const int row = rg * 16 + g, q = nb * 8 + 2 * t;
+        as[q * kChainLd + row] -= d[0];
+        as[(q + 1) * kChainLd + row] -= d[1];
+        as[q * kChainLd + row + 8] -= d[2];
+        as[(q + 1) * kChainLd + row + 8] -= d[3];
+      }
+    } else {
+      // x at position sweep + 1 (this slot): inv * acc_s, kept and published.
+      const int pos = sweep + 1;
+      const int r0 = blk(pos) * kTb, bs = min(kTb, n - r0);
+      double* xd = xs + (pos & 1) * kChainVec;
+      if (nb < nbl) {
+        double d[4] = {0.0, 0.0, 0.0, 0.0};
+        ChainMma(tile, rg * 16, as + nb * 8 * kChainLd, g, t, d);
+        const int row = rg * 16 + g, q = nb * 8 + 2 * t;
+        const double v[4] = {d[0], d[1], d[2], d[3]};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int rr = row + (e >> 1) * 8, qq = q + (e & 1);
+          xd[qq * kChainLd + rr] = v[e];
+          if (rr < bs && qq < ncols) xc[r0 + rr + static_cast<long long>(qq) * ldx] = v[e];
+        }
+      }
+      // The barrier orders every thread's stores of x before thread 0's
+      // release at GPU scope, which makes them visible to the acquirer.
+      __syncthreads();
+      if (tid == 0)
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(cflags + pos), "r"(epoch)
+                     : "memory");
+    }
+    ++item;
+  }
+  CpAsyncWait<0>();
+}
+
 // Buffers of one mixed solve (device pointers into the thread's workspace).
 struct MixedBuffers {
   double* w = nullptr;      // n x n factor, leading dimension ldw
@@ -433,6 +697,7 @@ struct MixedBuffers {
   int* perm = nullptr;      // LU row permutation
   unsigned long long* norms = nullptr;  // [0] ||A||, then ||x||, ||r|| columns
   unsigned int* barrier = nullptr;
+  unsigned int* flags = nullptr;  // per-position ready flags of the chained solve
 };
 
 long long Round(long long v, long long m) { return (v + m - 1) / m * m; }
@@ -455,9 +720,14 @@ bool AllocBuffers(int n, int nrhs, bool sym, MixedBuffers* bf) {
   const size_t part_elems =
       std::max(chunks * std::min(nrhs, kResRhs) * n, rowparts * n);
   const size_t norm_elems = 1 + 3 * static_cast<size_t>(nrhs);
+  // Chained solves launch at most num_sms / ceil(nblk / kChainSlots) chains
+  // of nblk flags, which is at most max(nblk, kChainSlots * num_sms).
+  const size_t flag_elems = Round(
+      std::max<size_t>(nblk, static_cast<size_t>(kChainSlots) * Ctx().num_sms) + 64, 64);
   const size_t total = sizeof(double) * (2 * inv_elems + 2 * r_elems + part_elems) +
                        sizeof(int) * Round(n, 64) +
-                       sizeof(unsigned long long) * (norm_elems + 8) + 4096;
+                       sizeof(unsigned long long) * (norm_elems + 8) +
+                       sizeof(unsigned int) * flag_elems + 4096;
   uint8_t* base = static_cast<uint8_t*>(Workspace(kWsMixed3, total));
   if (base == nullptr) return false;
   double* d = reinterpret_cast<double*>(base);
@@ -469,6 +739,7 @@ bool AllocBuffers(int n, int nrhs, bool sym, MixedBuffers* bf) {
   bf->perm = reinterpret_cast<int*>(bf->part + part_elems);
   bf->norms = reinterpret_cast<unsigned long long*>(bf->perm + Round(n, 64));
   bf->barrier = reinterpret_cast<unsigned int*>(bf->norms + norm_elems + 8);
+  bf->flags = bf->barrier + 64;
   return true;
 }
 
@@ -576,9 +847,58 @@ void PermFromPivots(int n, const int* ipiv, int* perm) {
   LaunchFailed("mixed permutation");
 }
 
+// Chained solve (ChainTrsvKernel) of x := T^{-1} x; false when the row
+// blocks do not fit the CTAs' slots (n above kChainSlots * 64 * resident
+// CTAs), in which case nothing was launched.
+bool ChainTrsv(bool lower, int n, int nrhs, const double* w, long long ldw,
+               const double* inv, double* x, long long ldx, unsigned int* flags) {
+  Context& ctx = Ctx();
+  static int capacity = -1;
+  if (capacity < 0) {
+    cudaFuncSetAttribute(ChainTrsvKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kChainSmem);
+    cudaFuncSetAttribute(ChainTrsvKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kChainSmem);
+    int lo = 0, up = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lo, ChainTrsvKernel<true>, kChainThreads,
+                                                  kChainSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, ChainTrsvKernel<false>, kChainThreads,
+                                                  kChainSmem);
+    capacity = ctx.num_sms * std::min(lo, up);
+    cudaGetLastError();
+  }
+  const int nblk = (n + kTb - 1) / kTb;
+  const int pmin = (nblk + kChainSlots - 1) / kChainSlots;
+  if (capacity <= 0 || pmin > capacity) return false;
+  const int chains = (nrhs + kCw - 1) / kCw;
+  const int per_launch = std::max(1, std::min(chains, capacity / pmin));
+  int nn = n;
+  long long lw = ldw, lx = ldx;
+  int* tflag = ctx.dev_status;
+  unsigned int epoch = 1;
+  const void* fn = lower ? reinterpret_cast<const void*>(ChainTrsvKernel<true>)
+                         : reinterpret_cast<const void*>(ChainTrsvKernel<false>);
+  for (int c0 = 0; c0 < chains; c0 += per_launch) {
+    const int nc = std::min(per_launch, chains - c0);
+    int P = std::min(nblk, capacity / nc);
+    int nr = std::min(nrhs - c0 * kCw, nc * kCw);
+    double* xq = x + static_cast<long long>(c0) * kCw * ldx;
+    cudaMemsetAsync(flags, 0, sizeof(unsigned int) * nblk * nc, ctx.stream);
+    void* args[] = {&nn, &nr, const_cast<double**>(&w), &lw, const_cast<double**>(&inv),
+                    &xq, &lx, &P, &flags, &epoch, &tflag};
+    Failed(cudaLaunchCooperativeKernel(fn, nc * P, kChainThreads, args, kChainSmem,
+                                       ctx.stream),
+           "mixed triangular solve");
+    CountLaunch();
+  }
+  return true;
+}
+
 // x := T^{-1} x for the lower or upper triangle of w.
 void BlockTrsv(bool lower, int n, int nrhs, const double* w, long long ldw,
-               const double* inv, double* x, long long ldx, unsigned int* barrier) {
+               const double* inv, double* x, long long ldx, unsigned int* barrier,
+               unsigned int* flags) {
+  if (ChainTrsv(lower, n, nrhs, w, ldw, inv, x, ldx, flags)) return;
   Context& ctx = Ctx();
   static int grid = 0;
   if (grid == 0) {
@@ -623,8 +943,8 @@ void MixedSolve(bool lu, int n, int nrhs, MixedBuffers& bf, const double* src,
   } else {
     Copy2D(n, nrhs, src, lds, dst, ldd);
   }
-  BlockTrsv(true, n, nrhs, bf.w, bf.ldw, bf.inv_lo, dst, ldd, bf.barrier);
-  BlockTrsv(false, n, nrhs, bf.w, bf.ldw, bf.inv_up, dst, ldd, bf.barrier);
+  BlockTrsv(true, n, nrhs, bf.w, bf.ldw, bf.inv_lo, dst, ldd, bf.barrier, bf.flags);
+  BlockTrsv(false, n, nrhs, bf.w, bf.ldw, bf.inv_up, dst, ldd, bf.barrier, bf.flags);
 }
 
 // Panel width: wide enough that the trailing updates amortize their

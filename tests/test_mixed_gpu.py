@@ -73,6 +73,25 @@ def test_dgesv_mixed_accuracy(hb, orc, n, nrhs, cond):
     assert fwd_err(x, xt) <= 4.0 * fwd_err(x2, xt) + 1e-15, (fwd_err(x, xt), fwd_err(x2, xt))
 
 
+def test_dgesv_mixed_many_chains(hb):
+    """70 right-hand sides (five 16-column chains of the refinement's
+    triangular solves, the last one partial) at n = 2100 (33 row blocks, the
+    last partial): same forward-error and backward checks, against the known
+    solution."""
+    n, nrhs = 2100, 70
+    rng = np.random.default_rng(21)
+    a = householder_matrix(rng, n, 1e6)
+    xt = rng.uniform(-1, 1, (n, nrhs))
+    b = np.asfortranarray(a @ xt)
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, np.int32)
+    info, it = hb.dgesv_mixed(n, nrhs, a.copy(order="F"), n, ipiv, b, n, x, n)
+    assert info == 0 and 1 <= it <= 10, (info, it)
+    check_backward(a, x, b, n)
+    ref = np.linalg.solve(a, b)
+    assert fwd_err(x, xt) <= 4.0 * fwd_err(ref, xt) + 1e-15, (fwd_err(x, xt), fwd_err(ref, xt))
+
+
 @pytest.mark.parametrize("uplo", ["L", "U"])
 @pytest.mark.parametrize("n,nrhs", [(257, 1), (900, 5)])
 def test_dposv_mixed_accuracy(hb, orc, uplo, n, nrhs):
