@@ -78,7 +78,8 @@ enum WorkspaceSlot : int {
   kWsEmul2 = 14,   // emulated-GEMM buffers of a second, concurrent stream
   kWsEmulAcc2 = 15,
   kWsEmulW2 = 16,
-  kNumWorkspaceSlots = 17
+  kWsTourney = 17, // tournament-pivoting leaf: candidates and results
+  kNumWorkspaceSlots = 18
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -150,13 +151,13 @@ template <typename T>
 void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
            T* b, int ldb);
 void Potrf(bool upper, int n, double* a, int lda, int* info);
-// Getrf2 / Potrf2 of a block whose first column is global column col0 (for
-// INFO); the Cholesky one turns later kernels into no-ops after a failure.
-// GetrfPanel with leaf_w = 32 stops the recursion at 32 columns (not the
-// reference's structure; for the mixed solver's panels).
-void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0,
-                int leaf_w = 16);
+// Potrf2 of a block whose first column is global column col0 (for INFO);
+// later kernels become no-ops after a failure.
 void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
+// Pivoted LU of an m x nc panel (m >= nc) for the mixed solver (mixed_panel.cu):
+// right-looking over leaf-wide sub-panels, not the reference's recursion;
+// pivots relative to the panel's first row; *info set at the first zero pivot.
+void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col0);
 void Potrf2(bool upper, int n, double* a, int lda, int* info);
 void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
            int ldb);

@@ -27,22 +27,21 @@ T* At(T* a, int lda, int i, int j) {
 // (for INFO: columns are factored left to right, so each leaf sets the device
 // INFO only while it is still 0, to col0 + its own first zero pivot).
 template <typename T>
-void GetrfRec(int m, int n, T* a, int lda, int* ipiv, int* info, int col0,
-              int leaf_w = 16) {
+void GetrfRec(int m, int n, T* a, int lda, int* ipiv, int* info, int col0) {
   if (m == 0 || n == 0) return;
-  if (std::min(m, n) <= leaf_w) {
-    GetrfLeaf<T>(m, n, a, lda, ipiv, info, col0, leaf_w);
+  if (std::min(m, n) <= 16) {
+    GetrfLeaf<T>(m, n, a, lda, ipiv, info, col0);
     return;
   }
   const int n1 = std::min(m, n) / 2;
   const int n2 = n - n1;
-  GetrfRec<T>(m, n1, a, lda, ipiv, info, col0, leaf_w);
+  GetrfRec<T>(m, n1, a, lda, ipiv, info, col0);
   Laswp<T>(n2, At(a, lda, 0, n1), lda, 1, n1, ipiv, 1);
   TrsmFull<T>(true, true, false, true, n1, n2, T(1), a, lda, At(a, lda, 0, n1),
               lda);
   GemmFull<T>(false, false, m - n1, n2, n1, T(-1), At(a, lda, n1, 0), lda,
               At(a, lda, 0, n1), lda, T(1), At(a, lda, n1, n1), lda);
-  GetrfRec<T>(m - n1, n2, At(a, lda, n1, n1), lda, ipiv + n1, info, col0 + n1, leaf_w);
+  GetrfRec<T>(m - n1, n2, At(a, lda, n1, n1), lda, ipiv + n1, info, col0 + n1);
   AdjustPivots(ipiv, n1, std::min(m, n), n1);
   Laswp<T>(n1, a, lda, n1 + 1, std::min(m, n), ipiv, 1);
 }
@@ -50,11 +49,6 @@ void GetrfRec(int m, int n, T* a, int lda, int* ipiv, int* info, int col0,
 template <typename T>
 void Getrf2(int m, int n, T* a, int lda, int* ipiv, int* info) {
   GetrfRec<T>(m, n, a, lda, ipiv, info, 0);
-}
-
-void GetrfPanel(int m, int n, double* a, int lda, int* ipiv, int* info, int col0,
-                int leaf_w) {
-  GetrfRec<double>(m, n, a, lda, ipiv, info, col0, leaf_w);
 }
 
 template <typename T>

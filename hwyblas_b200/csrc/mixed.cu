@@ -951,10 +951,6 @@ void MixedSolve(bool lu, int n, int nrhs, MixedBuffers& bf, const double* src,
 // slicing and epilogue (measured at n = 16384: 1024 beats 512 by ~5 %).
 int MixedBlock(int n) { return n >= 8192 ? 1024 : (n >= 4096 ? 512 : 256); }
 
-// Leaf width of the mixed solver's FP64 panels: 32 columns where the panel's
-// rows fit the 32-column leaf (one cluster of 16 CTAs of 832 rows), which
-// halves the panel recursion's small steps; else the reference's 16.
-int PanelLeafWidth(int m) { return m <= 16 * 832 ? 32 : 16; }
 
 // A high-priority stream of the calling thread for the look-ahead panel
 // work, and two events to order it against the context's stream.
@@ -1019,7 +1015,7 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
   signal(la.to_look, main, look);
   OnStream(look, [&] {
     const int jb0 = std::min(nb, n);
-    GetrfPanel(n, jb0, w, lw, ipiv, info, 0, PanelLeafWidth(n));
+    MixedPanel(n, jb0, w, lw, ipiv, info, 0);
   });
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
@@ -1039,8 +1035,7 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
     if (rest > next) signal(la.to_main, look, main);
     if (rest > 0) {
       OnStream(look, [&] {
-        GetrfPanel(rest, next, At(w, ldw, j + jb, j + jb), lw, ipiv + j + jb, info, j + jb,
-                   PanelLeafWidth(rest));
+        MixedPanel(rest, next, At(w, ldw, j + jb, j + jb), lw, ipiv + j + jb, info, j + jb);
       });
     }
     if (rest > next) {
