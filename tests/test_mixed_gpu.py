@@ -92,6 +92,25 @@ def test_dgesv_mixed_many_chains(hb):
     assert fwd_err(x, xt) <= 4.0 * fwd_err(ref, xt) + 1e-15, (fwd_err(x, xt), fwd_err(ref, xt))
 
 
+def test_dgesv_mixed_tall_panels(hb):
+    """n = 9000: the first panels are 9000 rows tall, so their tournament
+    leaves run 18 CTAs with two merge levels (16 + 2 candidate sets, then 2);
+    forward error and backward criterion as above."""
+    n, nrhs = 9000, 2
+    rng = np.random.default_rng(90)
+    a = householder_matrix(rng, n, 1e6)
+    xt = rng.uniform(-1, 1, (n, nrhs))
+    b = np.asfortranarray(a @ xt)
+    x = np.zeros((n, nrhs), order="F")
+    ipiv = np.zeros(n, np.int32)
+    info, it = hb.dgesv_mixed(n, nrhs, a.copy(order="F"), n, ipiv, b, n, x, n)
+    assert info == 0 and 1 <= it <= 10, (info, it)
+    assert ipiv.min() >= 1 and ipiv.max() <= n
+    check_backward(a, x, b, n)
+    ref = np.linalg.solve(a, b)
+    assert fwd_err(x, xt) <= 4.0 * fwd_err(ref, xt) + 1e-15, (fwd_err(x, xt), fwd_err(ref, xt))
+
+
 @pytest.mark.parametrize("uplo", ["L", "U"])
 @pytest.mark.parametrize("n,nrhs", [(257, 1), (900, 5)])
 def test_dposv_mixed_accuracy(hb, orc, uplo, n, nrhs):
