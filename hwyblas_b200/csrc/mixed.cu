@@ -698,6 +698,7 @@ struct MixedBuffers {
   unsigned long long* norms = nullptr;  // [0] ||A||, then ||x||, ||r|| columns
   unsigned int* barrier = nullptr;
   unsigned int* flags = nullptr;  // per-position ready flags of the chained solve
+  size_t flag_stride = 0;         // flags of a second, concurrent chained solve
 };
 
 long long Round(long long v, long long m) { return (v + m - 1) / m * m; }
@@ -721,9 +722,11 @@ bool AllocBuffers(int n, int nrhs, bool sym, MixedBuffers* bf) {
       std::max(chunks * std::min(nrhs, kResRhs) * n, rowparts * n);
   const size_t norm_elems = 1 + 3 * static_cast<size_t>(nrhs);
   // Chained solves launch at most num_sms / ceil(nblk / kChainSlots) chains
-  // of nblk flags, which is at most max(nblk, kChainSlots * num_sms).
-  const size_t flag_elems = Round(
+  // of nblk flags, which is at most max(nblk, kChainSlots * num_sms); the
+  // factorization runs two at once (one a stream).
+  bf->flag_stride = Round(
       std::max<size_t>(nblk, static_cast<size_t>(kChainSlots) * Ctx().num_sms) + 64, 64);
+  const size_t flag_elems = 2 * bf->flag_stride;
   const size_t total = sizeof(double) * (2 * inv_elems + 2 * r_elems + part_elems) +
                        sizeof(int) * Round(n, 64) +
                        sizeof(unsigned long long) * (norm_elems + 8) +
@@ -985,12 +988,14 @@ void OnStream(cudaStream_t s, F f) {
 
 // Right-looking LU of w with FP64 panels and Ozaki trailing updates, with a
 // look-ahead of one panel: on a high-priority stream, the pivots of panel j
-// are applied, the columns of panel j+1 are updated first and panel j+1 is
-// factored, while the context's stream updates the rest of the trailing
-// matrix. The two touch disjoint columns; each waits for the other where one
-// reads what the other writes (the row interchanges need the previous
-// trailing update finished, the trailing update needs the interchanges).
-void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slices) {
+// are applied to the columns of panel j+1, which are updated and factored,
+// while the context's stream applies them to all other columns and updates
+// the rest of the trailing matrix. The two touch disjoint columns; each
+// waits for the other where one reads what the other writes (panel j+1's
+// columns need the previous trailing update finished, the rest needs the
+// adjusted pivots).
+void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slices,
+                MixedBuffers& bf) {
   Context& ctx = Ctx();
   const int nb = MixedBlock(n);
   const int lw = static_cast<int>(ldw);
@@ -1002,12 +1007,26 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
     cudaEventRecord(ev, from);
     cudaStreamWaitEvent(to, ev, 0);
   };
+  // Inverses of the 64 x 64 diagonal blocks of panel j's unit L11, in one
+  // of two buffers by panel parity (look writes panel j+1's while main may
+  // still read panel j's).
+  const auto l11_inv = [&](int j) { return ((j / nb) & 1) ? bf.inv_up : bf.inv_lo; };
+  const auto invert = [&](int j, int jb) {
+    if (j + jb < n) InvertDiagBlocks(jb, At(w, ldw, j, j), ldw, true, true, l11_inv(j));
+  };
   const auto update = [&](int j, int jb, int c0, int nc, int ws_set) {
-    // Columns [c0, c0 + nc) of the trailing matrix: U12 by the FP64
-    // triangular solve, then A22 -= L21 U12 on the INT8 tensor cores.
+    // Columns [c0, c0 + nc) of the trailing matrix: U12 by an FP64
+    // triangular solve, then A22 -= L21 U12 on the INT8 tensor cores. The
+    // next panel's columns (look, ws_set 1) take the chained solve, whose
+    // 64 chains of 16 columns run in one launch with a short critical path;
+    // the wide rest (main) takes the recursive solve, whose large DMMA
+    // GEMMs do the bulk of the flops at a higher rate.
     const int rest = n - j - jb;
-    TrsmFull<double>(true, true, false, true, jb, nc, 1.0, At(w, ldw, j, j), lw,
-                     At(w, ldw, j, c0), lw);
+    if (ws_set == 0 ||
+        !ChainTrsv(true, jb, nc, At(w, ldw, j, j), ldw, l11_inv(j), At(w, ldw, j, c0), ldw,
+                   bf.flags + ws_set * bf.flag_stride))
+      TrsmFull<double>(true, true, false, true, jb, nc, 1.0, At(w, ldw, j, j), lw,
+                       At(w, ldw, j, c0), lw);
     DgemmEmulated(rest, nc, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
                   ColMajor<double>(At(w, ldw, j, c0), ldw), 1.0, At(w, ldw, j + jb, c0), lw,
                   slices, false, ws_set);
@@ -1016,31 +1035,37 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
   OnStream(look, [&] {
     const int jb0 = std::min(nb, n);
     MixedPanel(n, jb0, w, lw, ipiv, info, 0);
+    invert(0, jb0);
   });
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
     const int rest = n - j - jb;
     const int next = std::min(nb, rest);
-    // Panel j is factored (on look). Its interchanges reach every other
-    // column once main's previous trailing update is done.
+    // Panel j is factored (on look). Once main's previous trailing update is
+    // done, look applies the panel's interchanges to the next panel's
+    // columns, updates and factors them; main applies them to the columns
+    // left of the panel and to the rest of the trailing matrix, then updates
+    // the rest. The two streams touch disjoint columns.
     signal(la.to_look, main, look);
     OnStream(look, [&] {
       if (j > 0) AdjustPivots(ipiv, j, j + jb, j);
-      if (j > 0) Laswp<double>(j, w, lw, j + 1, j + jb, ipiv, 1);
-      if (rest > 0) {
-        Laswp<double>(rest, At(w, ldw, 0, j + jb), lw, j + 1, j + jb, ipiv, 1);
-        update(j, jb, j + jb, next, 1);
-      }
     });
-    if (rest > next) signal(la.to_main, look, main);
+    signal(la.to_main, look, main);
     if (rest > 0) {
       OnStream(look, [&] {
+        Laswp<double>(next, At(w, ldw, 0, j + jb), lw, j + 1, j + jb, ipiv, 1);
+        update(j, jb, j + jb, next, 1);
         MixedPanel(rest, next, At(w, ldw, j + jb, j + jb), lw, ipiv + j + jb, info, j + jb);
+        invert(j + jb, next);
       });
     }
-    if (rest > next) {
-      OnStream(main, [&] { update(j, jb, j + jb + next, rest - next, 0); });
-    }
+    OnStream(main, [&] {
+      if (j > 0) Laswp<double>(j, w, lw, j + 1, j + jb, ipiv, 1);
+      if (rest > next) {
+        Laswp<double>(rest - next, At(w, ldw, 0, j + jb + next), lw, j + 1, j + jb, ipiv, 1);
+        update(j, jb, j + jb + next, rest - next, 0);
+      }
+    });
   }
   signal(la.to_main, look, main);
 }
@@ -1133,7 +1158,7 @@ int DgesvMixed(int n, int nrhs, double* a, int lda, int* ipiv, const double* b,
   } else {
     cudaMemsetAsync(dinfo, 0, sizeof(int), st);
     Copy2D(n, n, a, lda, bf.w, bf.ldw);
-    MixedGetrf(n, bf.w, bf.ldw, ipiv, dinfo, slices);
+    MixedGetrf(n, bf.w, bf.ldw, ipiv, dinfo, slices, bf);
     int finfo = 0;
     cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (Failed(cudaStreamSynchronize(st), "mixed getrf")) return -1;
