@@ -199,16 +199,91 @@ __global__ void __launch_bounds__(256)
     sslot[t] = (pp >= k1 && pp <= k2) ? pp - k1 : (hs[r] >= 0 ? -hfirst[hs[r]] - 1 : t);
   }
   if (threadIdx.x == 0) cnt = nb + base;
-  __syncthreads();
-  // (3) The interchanges themselves, in order, on the source table.
-  if (threadIdx.x == 0) {
-    for (int t = 0; t < nb; ++t) {
-      const int sp = sslot[t];
-      if (sp == t) continue;
-      const int a0 = src[t];
-      src[t] = src[sp];
-      src[sp] = a0;
+  // Factorizations' pivots name rows at or below their own (slot >= step);
+  // dlaswp callers may pass any.
+  int ordered = 1;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int t = t0 + r * blockDim.x;
+    if (t < nb && sslot[t] < t) ordered = 0;
+  }
+  if (!__syncthreads_and(ordered)) {
+    // (3) The interchanges in order, on the source table.
+    if (threadIdx.x == 0) {
+      for (int t = 0; t < nb; ++t) {
+        const int sp = sslot[t];
+        if (sp == t) continue;
+        const int a0 = src[t];
+        src[t] = src[sp];
+        src[sp] = a0;
+      }
     }
+  } else {
+  // (3) The interchanges' net effect, without replaying them one by one.
+  // Interchange u swaps slots u and s_u = sslot[u] (s_u >= u). Slot u's
+  // content just before step u is that before step into(u), the last earlier
+  // step whose s_v is u, or its own row if none; after step u, slot u holds
+  // what s_u held, i.e. the content before step prev(u), the last earlier
+  // step with the same s_v, or s_u's own row; an extra slot ends with the
+  // content before the last step naming it. The "content before" chains
+  // point to earlier steps and resolve by pointer jumping.
+  {
+    int into[2] = {-1, -1}, prev[2] = {-1, -1}, later[2] = {0, 0}, su[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) su[r] = t0 + r * blockDim.x < nb ? sslot[t0 + r * blockDim.x] : -1;
+    for (int v = 0; v < nb; ++v) {
+      const int sv = sslot[v];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int u = t0 + r * blockDim.x;
+        if (v < u) {
+          if (sv == u) into[r] = v;
+          if (sv == su[r]) prev[r] = v;
+        } else if (v > u && sv == su[r]) {
+          later[r] = 1;
+        }
+      }
+    }
+    int* ptr = hkey;    // the hash is no longer needed: [2][kSwapMax] each
+    int* val = hfirst;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int u = t0 + r * blockDim.x;
+      if (u < nb) {
+        ptr[u] = into[r];
+        val[u] = pos[u];
+      }
+    }
+    __syncthreads();
+    for (int round = 0, cur = 0; round < 11; ++round, cur ^= 1) {
+      const int* pc = ptr + cur * kSwapMax;
+      const int* vc = val + cur * kSwapMax;
+      int* pn = ptr + (cur ^ 1) * kSwapMax;
+      int* vn = val + (cur ^ 1) * kSwapMax;
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int u = t0 + r * blockDim.x;
+        if (u >= nb) continue;
+        const int q = pc[u];
+        if (q >= 0 && pc[q] < 0) {
+          pn[u] = -1;
+          vn[u] = vc[q];
+        } else {
+          pn[u] = q >= 0 ? pc[q] : -1;
+          vn[u] = vc[u];
+        }
+      }
+      __syncthreads();
+    }
+    const int* vf = val + (11 & 1) * kSwapMax;  // after 11 rounds: buffer 1
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int u = t0 + r * blockDim.x;
+      if (u >= nb) continue;
+      src[u] = prev[r] >= 0 ? vf[prev[r]] : pos[su[r]];
+      if (su[r] >= nb && !later[r]) src[su[r]] = vf[u];
+    }
+  }
   }
   __syncthreads();
   const int c = cnt;

@@ -8,7 +8,7 @@
 //                cooperative launch, no per-column exchange between CTAs);
 //   swap+solve   the sub-panel's interchanges on every other column of the
 //                panel, and U12 = L11^{-1} A12 on the columns to its right;
-//   update       A22 -= L21 U12 (rank 32, the DMMA GEMM).
+//   update       A22 -= L21 U12 (rank 32, one DMMA pass over A22).
 //
 // Pivots are LAPACK-style (row i interchanged with row ipiv[i], 1-based) and
 // end relative to the panel's first row.
@@ -106,6 +106,74 @@ __global__ void __launch_bounds__(256)
     }
     if (lane < ns) col[r0] = n0;
     if (lane + 32 < ns) col[r1] = n1;
+  }
+}
+
+// C -= A B for the mixed panels' rank-w updates (w <= 32): A m x w, B w x n,
+// C m x n, column-major. The reference-order DMMA GEMM streams K in chunks
+// and is built for large K; here K is one MMA k-extent of 32, so the cost is
+// C's read and write. One CTA per 128 x 32 tile of C: -A's 128 x 32 and B's
+// 32 x 32 in padded shared memory, each warp's 16 x 32 block of C loaded
+// straight into its m16n8k8 accumulators, 4 k-steps, stored back.
+constexpr int kRkM = 128, kRkN = 32, kRkK = 32;
+constexpr int kRkLda = kRkM + 4;  // conflict-free A fragments
+constexpr int kRkLdb = kRkK + 4;  // conflict-free B fragments
+__global__ void __launch_bounds__(256)
+    PanelRankUpdateKernel(int m, int n, int kw, const double* a, long long lda,
+                          const double* b, long long ldb, double* c, long long ldc) {
+  __shared__ __align__(16) double sa[kRkK * kRkLda];  // sa[k * kRkLda + row] = -A
+  __shared__ __align__(16) double sb[kRkN * kRkLdb];  // sb[col * kRkLdb + k] = B
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int g = lane >> 2, t = lane & 3;
+  const int r0 = blockIdx.x * kRkM, c0 = blockIdx.y * kRkN;
+  for (int idx = tid; idx < kRkK * kRkM; idx += 256) {
+    const int k = idx / kRkM, r = idx % kRkM;
+    sa[k * kRkLda + r] = (k < kw && r0 + r < m) ? -a[r0 + r + k * lda] : 0.0;
+  }
+  for (int idx = tid; idx < kRkN * kRkK; idx += 256) {
+    const int col = idx / kRkK, k = idx % kRkK;
+    sb[col * kRkLdb + k] = (k < kw && c0 + col < n) ? b[k + (c0 + col) * ldb] : 0.0;
+  }
+  // Warp w: rows w*16 .. +16, all 32 columns of the tile.
+  double d[4][4];
+  const int row = r0 + warp * 16 + g;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int col = c0 + j * 8 + 2 * t;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int rr = row + (e >> 1) * 8, cc = col + (e & 1);
+      d[j][e] = (rr < m && cc < n) ? c[rr + cc * ldc] : 0.0;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int kk = 0; kk < kRkK / 8; ++kk) {
+    const int lr = warp * 16 + g, k0 = kk * 8 + t;
+    const double a0 = sa[k0 * kRkLda + lr];
+    const double a1 = sa[k0 * kRkLda + lr + 8];
+    const double a2 = sa[(k0 + 4) * kRkLda + lr];
+    const double a3 = sa[(k0 + 4) * kRkLda + lr + 8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int col = j * 8 + g;
+      const double b0 = sb[col * kRkLdb + k0];
+      const double b1 = sb[col * kRkLdb + k0 + 4];
+      asm volatile(
+          "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+          "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+          : "+d"(d[j][0]), "+d"(d[j][1]), "+d"(d[j][2]), "+d"(d[j][3])
+          : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int col = c0 + j * 8 + 2 * t;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int rr = row + (e >> 1) * 8, cc = col + (e & 1);
+      if (rr < m && cc < n) c[rr + cc * ldc] = d[j][e];
+    }
   }
 }
 
@@ -652,9 +720,15 @@ void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col
       CountLaunch();
       LaunchFailed("mixed panel interchanges");
     }
-    if (right > 0 && m - c - w > 0)
-      GemmFull<double>(false, false, m - c - w, right, w, -1.0, At(a, lda, c + w, c), lda,
-                       At(a, lda, c, c + w), lda, 1.0, At(a, lda, c + w, c + w), lda);
+    if (right > 0 && m - c - w > 0) {
+      const int mr = m - c - w;
+      PanelRankUpdateKernel<<<dim3((mr + kRkM - 1) / kRkM, (right + kRkN - 1) / kRkN), 256, 0,
+                              ctx.stream>>>(mr, right, w, At(a, lda, c + w, c), lda,
+                                            At(a, lda, c, c + w), lda,
+                                            At(a, lda, c + w, c + w), lda);
+      CountLaunch();
+      LaunchFailed("mixed panel update");
+    }
   }
   PanelPivotOffsetKernel<<<(mn + 255) / 256, 256, 0, ctx.stream>>>(mn, ib, ipiv);
   CountLaunch();
