@@ -699,38 +699,96 @@ int PanelLeafWidth(int m) { return m <= 16 * 832 ? 32 : 16; }
 
 }  // namespace
 
+namespace {
+
+// A stream for the panels' wide rank updates, at a priority between the
+// look-ahead stream's (highest) and the default, and two events to order it
+// against the stream the panel runs on.
+struct PanelSide {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t to_side = nullptr, to_panel = nullptr;
+  bool ok = false;
+};
+PanelSide& GetPanelSide() {
+  static thread_local PanelSide ps;
+  static thread_local bool tried = false;
+  if (!tried) {
+    tried = true;
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int prio = greatest < least ? greatest + 1 : greatest;
+    ps.ok = cudaStreamCreateWithPriority(&ps.stream, cudaStreamNonBlocking, prio) ==
+                cudaSuccess &&
+            cudaEventCreateWithFlags(&ps.to_side, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ps.to_panel, cudaEventDisableTiming) == cudaSuccess;
+    if (!ps.ok) cudaGetLastError();
+  }
+  return ps;
+}
+
+void RankUpdate(int mr, int nr, int w, const double* l21, const double* u12, double* a22,
+                int lda, cudaStream_t st) {
+  if (mr <= 0 || nr <= 0) return;
+  PanelRankUpdateKernel<<<dim3((mr + kRkM - 1) / kRkM, (nr + kRkN - 1) / kRkN), 256, 0, st>>>(
+      mr, nr, w, l21, lda, u12, lda, a22, lda);
+  CountLaunch();
+  LaunchFailed("mixed panel update");
+}
+
+}  // namespace
+
+// Sub-panel c's update is split: the next sub-panel's columns first, on the
+// panel's stream, so that the next leaf can start; the columns beyond them
+// on a side stream, overlapping that leaf. The next interchange+solve kernel
+// touches those columns, so it waits for the side stream.
 void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col0) {
   Context& ctx = Ctx();
+  const cudaStream_t st = ctx.stream;
+  PanelSide& side = GetPanelSide();
   const bool tourney = TournamentFits(m);
   const int ib = tourney ? kTnW : PanelLeafWidth(m);
   const int mn = std::min(m, nc);
   if (mn <= 0) return;
+  bool side_pending = false;
   for (int c = 0; c < mn; c += ib) {
     const int w = std::min(ib, mn - c);
     if (tourney)
       TournamentLeaf(m - c, w, At(a, lda, c, c), lda, ipiv + c, info, col0 + c);
     else
       GetrfLeaf<double>(m - c, w, At(a, lda, c, c), lda, ipiv + c, info, col0 + c, ib);
+    if (side_pending) {
+      cudaStreamWaitEvent(st, side.to_panel, 0);
+      side_pending = false;
+    }
     const int right = nc - c - w;
     const int blocks =
         (c + kSwapCols - 1) / kSwapCols + (right + kSwapCols - 1) / kSwapCols;
     if (blocks > 0) {
-      PanelSwapSolveKernel<<<blocks, 256, 0, ctx.stream>>>(w, c, c, c + w, right, a, lda,
-                                                           ipiv + c);
+      PanelSwapSolveKernel<<<blocks, 256, 0, st>>>(w, c, c, c + w, right, a, lda, ipiv + c);
       CountLaunch();
       LaunchFailed("mixed panel interchanges");
     }
-    if (right > 0 && m - c - w > 0) {
-      const int mr = m - c - w;
-      PanelRankUpdateKernel<<<dim3((mr + kRkM - 1) / kRkM, (right + kRkN - 1) / kRkN), 256, 0,
-                              ctx.stream>>>(mr, right, w, At(a, lda, c + w, c), lda,
-                                            At(a, lda, c, c + w), lda,
-                                            At(a, lda, c + w, c + w), lda);
-      CountLaunch();
-      LaunchFailed("mixed panel update");
+    const int mr = m - c - w;
+    if (right <= 0 || mr <= 0) continue;
+    const int near = std::min(right, ib);
+    const double* l21 = At(a, lda, c + w, c);
+    RankUpdate(mr, near, w, l21, At(a, lda, c, c + w), At(a, lda, c + w, c + w), lda, st);
+    if (right > near) {
+      const int far0 = c + w + near;
+      if (side.ok) {
+        cudaEventRecord(side.to_side, st);
+        cudaStreamWaitEvent(side.stream, side.to_side, 0);
+      }
+      RankUpdate(mr, right - near, w, l21, At(a, lda, c, far0), At(a, lda, c + w, far0), lda,
+                 side.ok ? side.stream : st);
+      if (side.ok) {
+        cudaEventRecord(side.to_panel, side.stream);
+        side_pending = true;
+      }
     }
   }
-  PanelPivotOffsetKernel<<<(mn + 255) / 256, 256, 0, ctx.stream>>>(mn, ib, ipiv);
+  if (side_pending) cudaStreamWaitEvent(st, side.to_panel, 0);
+  PanelPivotOffsetKernel<<<(mn + 255) / 256, 256, 0, st>>>(mn, ib, ipiv);
   CountLaunch();
   LaunchFailed("mixed panel pivots");
 }
