@@ -14,9 +14,10 @@ import os
 from . import _abi
 
 __all__ = [
-    "lib", "dgemm", "sgemm", "dtrsm", "dsyrk", "idamax", "dlaswp", "dgetrf",
-    "dgetrf2", "dgetrs", "dgesv", "dpotrf", "dpotrf2", "dpotrs", "dposv",
-    "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_idamax",
+    "lib", "dgemm", "sgemm", "dtrsm", "strsm", "dsyrk", "idamax", "dlaswp", "dgetrf",
+    "dgetrf2", "dgetrs", "dgesv", "slaswp", "sgetrf", "sgetrf2", "sgetrs", "sgesv",
+    "dpotrf", "dpotrf2", "dpotrs", "dposv",
+    "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_strsm", "cblas_idamax",
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
@@ -42,9 +43,9 @@ def lib():
 
 
 from ._api import (  # noqa: E402  (needs lib())
-    dgemm, sgemm, dtrsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
-    dgesv, dpotrf, dpotrf2, dpotrs, dposv, cblas_dgemm, cblas_sgemm,
-    cblas_dtrsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
+    dgemm, sgemm, dtrsm, strsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
+    dgesv, slaswp, sgetrf, sgetrf2, sgetrs, sgesv, dpotrf, dpotrf2, dpotrs, dposv,
+    cblas_dgemm, cblas_sgemm, cblas_dtrsm, cblas_strsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
     dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
     KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,

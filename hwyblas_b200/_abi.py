@@ -18,6 +18,7 @@ PROTOTYPES = {
     "dgemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]),
     "sgemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]),
     "dtrsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
+    "strsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     "idamax_": (I, [PI, P, PI]),
     "xerbla_": (None, [C, PI, ctypes.c_size_t]),
@@ -28,6 +29,11 @@ PROTOTYPES = {
     "dlaswp_": (None, [PI, P, PI, PI, PI, P, PI]),
     "dgetrs_": (None, [C, PI, PI, P, PI, P, P, PI, PI]),
     "dgesv_": (None, [PI, PI, P, PI, P, P, PI, PI]),
+    "sgetrf_": (None, [PI, PI, P, PI, P, PI]),
+    "sgetrf2_": (None, [PI, PI, P, PI, P, PI]),
+    "slaswp_": (None, [PI, P, PI, PI, PI, P, PI]),
+    "sgetrs_": (None, [C, PI, PI, P, PI, P, P, PI, PI]),
+    "sgesv_": (None, [PI, PI, P, PI, P, P, PI, PI]),
     "dpotrf_": (None, [C, PI, P, PI, PI]),
     "dpotrf2_": (None, [C, PI, P, PI, PI]),
     "dpotrs_": (None, [C, PI, PI, P, PI, P, PI, PI]),
@@ -37,6 +43,7 @@ PROTOTYPES = {
     "cblas_dgemm": (None, [I, I, I, I, I, I, D, P, I, P, I, D, P, I]),
     "cblas_sgemm": (None, [I, I, I, I, I, I, F, P, I, P, I, F, P, I]),
     "cblas_dtrsm": (None, [I, I, I, I, I, I, I, D, P, I, P, I]),
+    "cblas_strsm": (None, [I, I, I, I, I, I, I, F, P, I, P, I]),
     "cblas_idamax": (ctypes.c_size_t, [I, P, I]),
     # Extensions
     "hwyblas_dgemm_emulated": (I, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI, PI]),

@@ -65,6 +65,12 @@ def dtrsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
                  _d(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb))
 
 
+def strsm(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """FP32 triangular solve in place (reference strsm_, src/trsm.cc:190)."""
+    lib().strsm_(_c(side), _c(uplo), _c(transa), _c(diag), _i(m), _i(n),
+                 _f(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb))
+
+
 def dsyrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     """Symmetric rank-k update (reference dsyrk_, src/level3.cc:416)."""
     lib().dsyrk_(_c(uplo), _c(trans), _i(n), _i(k), _d(alpha), _ptr(a), _i(lda),
@@ -106,6 +112,33 @@ def dgetrs(trans, n, nrhs, a, lda, ipiv, b, ldb):
 def dgesv(n, nrhs, a, lda, ipiv, b, ldb):
     """LU solve of A X = B; returns INFO (src/lapack/getrf.cc:348)."""
     return _info_call(lib().dgesv_, _i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(ipiv),
+                      _ptr(b), _i(ldb))
+
+
+def slaswp(n, a, lda, k1, k2, ipiv, incx):
+    """FP32 row interchanges (reference slaswp_, src/lapack/getrf.cc:518)."""
+    lib().slaswp_(_i(n), _ptr(a), _i(lda), _i(k1), _i(k2), _ptr(ipiv), _i(incx))
+
+
+def sgetrf(m, n, a, lda, ipiv):
+    """FP32 blocked LU; returns INFO (reference sgetrf_, src/lapack/getrf.cc:508)."""
+    return _info_call(lib().sgetrf_, _i(m), _i(n), _ptr(a), _i(lda), _ptr(ipiv))
+
+
+def sgetrf2(m, n, a, lda, ipiv):
+    """FP32 recursive LU; returns INFO (reference sgetrf2_, src/lapack/getrf.cc:513)."""
+    return _info_call(lib().sgetrf2_, _i(m), _i(n), _ptr(a), _i(lda), _ptr(ipiv))
+
+
+def sgetrs(trans, n, nrhs, a, lda, ipiv, b, ldb):
+    """FP32 solve with LU factors; returns INFO (src/lapack/getrf.cc:524)."""
+    return _info_call(lib().sgetrs_, _c(trans), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(ipiv), _ptr(b), _i(ldb))
+
+
+def sgesv(n, nrhs, a, lda, ipiv, b, ldb):
+    """FP32 LU solve of A X = B; returns INFO (src/lapack/getrf.cc:531)."""
+    return _info_call(lib().sgesv_, _i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(ipiv),
                       _ptr(b), _i(ldb))
 
 
@@ -233,6 +266,12 @@ def cblas_sgemm(layout, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c,
 
 def cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
     lib().cblas_dtrsm(layout, side, uplo, transa, diag, m, n, alpha, _ptr(a), lda,
+                      _ptr(b), ldb)
+
+
+def cblas_strsm(layout, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """CBLAS FP32 triangular solve (reference cblas_strsm, src/cblas.cc:1950)."""
+    lib().cblas_strsm(layout, side, uplo, transa, diag, m, n, alpha, _ptr(a), lda,
                       _ptr(b), ldb)
 
 

@@ -464,6 +464,15 @@ HWYBLAS_API void dtrsm_(const char* side, const char* uplo, const char* transa,
                         b, ldb);
 }
 
+HWYBLAS_API void strsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m,
+                        const hwyblas_int* n, const float* alpha,
+                        const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb) {
+  hb::TrsmEntry<float>("STRSM", side, uplo, transa, diag, m, n, alpha, a, lda,
+                       b, ldb);
+}
+
 HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
                         const hwyblas_int* n_p, const hwyblas_int* k_p,
                         const double* alpha_p, const double* a,
@@ -549,23 +558,25 @@ static bool CheckGetrf(const char* name, int m, int n, int lda, int* info) {
   return true;
 }
 
-static void GetrfEntry(bool recursive, const hwyblas_int* m_p,
-                       const hwyblas_int* n_p, double* a,
-                       const hwyblas_int* lda_p, hwyblas_int* ipiv,
-                       hwyblas_int* info) {
+extern "C++" {
+// The LU family for T = double and float (the reference instantiates one
+// template for both: getrf.cc:507-546).
+template <typename T>
+static void GetrfEntry(bool recursive, const char* name, const hwyblas_int* m_p,
+                       const hwyblas_int* n_p, T* a, const hwyblas_int* lda_p,
+                       hwyblas_int* ipiv, hwyblas_int* info) {
   const int m = *m_p, n = *n_p, lda = *lda_p;
-  const char* name = recursive ? "DGETRF2" : "DGETRF";
   if (!CheckGetrf(name, m, n, lda, info)) return;
   if (m == 0 || n == 0) return;
-  hb::Staged<double> sa;
+  hb::Staged<T> sa;
   hb::StagedInts sp;
   if (!sa.In(a, lda, m, n, hb::kWsStageA, true)) return;
   if (!sp.In(ipiv, std::min(m, n), 0, false)) return;
   hb::ResetInfo();
   if (recursive) {
-    hb::Getrf2<double>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+    hb::Getrf2<T>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
   } else {
-    hb::Getrf<double>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+    hb::Getrf<T>(m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
   }
   sa.Out();
   sp.Out();
@@ -573,41 +584,30 @@ static void GetrfEntry(bool recursive, const hwyblas_int* m_p,
   hb::Finish(name);
 }
 
-HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
-                         const hwyblas_int* lda, hwyblas_int* ipiv,
-                         hwyblas_int* info) {
-  GetrfEntry(false, m, n, a, lda, ipiv, info);
-}
-
-HWYBLAS_API void dgetrf2_(const hwyblas_int* m, const hwyblas_int* n,
-                          double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
-                          hwyblas_int* info) {
-  GetrfEntry(true, m, n, a, lda, ipiv, info);
-}
-
-HWYBLAS_API void dlaswp_(const hwyblas_int* n_p, double* a,
-                         const hwyblas_int* lda_p, const hwyblas_int* k1_p,
-                         const hwyblas_int* k2_p, const hwyblas_int* ipiv,
-                         const hwyblas_int* incx_p) {
+template <typename T>
+static void LaswpEntry(const char* name, const hwyblas_int* n_p, T* a,
+                       const hwyblas_int* lda_p, const hwyblas_int* k1_p,
+                       const hwyblas_int* k2_p, const hwyblas_int* ipiv,
+                       const hwyblas_int* incx_p) {
   const int n = *n_p, lda = *lda_p, k1 = *k1_p, k2 = *k2_p, incx = *incx_p;
   if (incx == 0 || n <= 0) return;
   const int absinc = incx < 0 ? -incx : incx;
   const int count = k1 + (k2 - k1) * absinc;  // entries ipiv(1..count)
   if (count <= 0 || k2 < k1) return;
-  hb::Staged<double> sa;
+  hb::Staged<T> sa;
   hb::StagedInts sp;
   if (!sa.In(a, lda, lda, n, hb::kWsStageA, true)) return;
   if (!sp.In(ipiv, count, 0, true)) return;
-  hb::Laswp<double>(n, sa.dev, sa.ld, k1, k2, sp.dev, incx);
+  hb::Laswp<T>(n, sa.dev, sa.ld, k1, k2, sp.dev, incx);
   sa.Out();
-  hb::Finish("DLASWP");
+  hb::Finish(name);
 }
 
-HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n_p,
-                         const hwyblas_int* nrhs_p, const double* a,
-                         const hwyblas_int* lda_p, const hwyblas_int* ipiv,
-                         double* b, const hwyblas_int* ldb_p,
-                         hwyblas_int* info) {
+template <typename T>
+static void GetrsEntry(const char* name, const char* trans, const hwyblas_int* n_p,
+                       const hwyblas_int* nrhs_p, const T* a, const hwyblas_int* lda_p,
+                       const hwyblas_int* ipiv, T* b, const hwyblas_int* ldb_p,
+                       hwyblas_int* info) {
   const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
   const char t = hb::Up(*trans);
   const bool notran = (t == 'N');
@@ -618,24 +618,24 @@ HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n_p,
   else if (lda < std::max(1, n)) *info = -5;
   else if (ldb < std::max(1, n)) *info = -8;
   if (*info != 0) {
-    hb::ReportError("DGETRS", -*info);
+    hb::ReportError(name, -*info);
     return;
   }
   if (n == 0 || nrhs == 0) return;
-  hb::Staged<double> sa, sb;
+  hb::Staged<T> sa, sb;
   hb::StagedInts sp;
   if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
   if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
   if (!sp.In(ipiv, n, 0, true)) return;
-  hb::Getrs<double>(!notran, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+  hb::Getrs<T>(!notran, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
   sb.Out();
-  hb::Finish("DGETRS");
+  hb::Finish(name);
 }
 
-HWYBLAS_API void dgesv_(const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
-                        double* a, const hwyblas_int* lda_p, hwyblas_int* ipiv,
-                        double* b, const hwyblas_int* ldb_p,
-                        hwyblas_int* info) {
+template <typename T>
+static void GesvEntry(const char* name, const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
+                      T* a, const hwyblas_int* lda_p, hwyblas_int* ipiv, T* b,
+                      const hwyblas_int* ldb_p, hwyblas_int* info) {
   const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
   *info = 0;
   if (n < 0) *info = -1;
@@ -643,26 +643,89 @@ HWYBLAS_API void dgesv_(const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
   else if (lda < std::max(1, n)) *info = -4;
   else if (ldb < std::max(1, n)) *info = -7;
   if (*info != 0) {
-    hb::ReportError("DGESV", -*info);
+    hb::ReportError(name, -*info);
     return;
   }
   if (n == 0) return;
-  hb::Staged<double> sa, sb;
+  hb::Staged<T> sa, sb;
   hb::StagedInts sp;
   if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
   if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
   if (!sp.In(ipiv, n, 0, false)) return;
   hb::ResetInfo();
-  hb::Getrf<double>(n, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  hb::Getrf<T>(n, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
   const int finfo = hb::ReadInfo();
   if (finfo == 0 && nrhs > 0) {
-    hb::Getrs<double>(false, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+    hb::Getrs<T>(false, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
   }
   sa.Out();
   sp.Out();
   if (finfo == 0) sb.Out();
   *info = finfo;
-  hb::Finish("DGESV");
+  hb::Finish(name);
+}
+}  // extern "C++"
+
+HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv,
+                         hwyblas_int* info) {
+  GetrfEntry<double>(false, "DGETRF", m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void dgetrf2_(const hwyblas_int* m, const hwyblas_int* n,
+                          double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
+                          hwyblas_int* info) {
+  GetrfEntry<double>(true, "DGETRF2", m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void dlaswp_(const hwyblas_int* n, double* a, const hwyblas_int* lda,
+                         const hwyblas_int* k1, const hwyblas_int* k2,
+                         const hwyblas_int* ipiv, const hwyblas_int* incx) {
+  LaswpEntry<double>("DLASWP", n, a, lda, k1, k2, ipiv, incx);
+}
+
+HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const double* a,
+                         const hwyblas_int* lda, const hwyblas_int* ipiv,
+                         double* b, const hwyblas_int* ldb, hwyblas_int* info) {
+  GetrsEntry<double>("DGETRS", trans, n, nrhs, a, lda, ipiv, b, ldb, info);
+}
+
+HWYBLAS_API void dgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, double* a,
+                        const hwyblas_int* lda, hwyblas_int* ipiv, double* b,
+                        const hwyblas_int* ldb, hwyblas_int* info) {
+  GesvEntry<double>("DGESV", n, nrhs, a, lda, ipiv, b, ldb, info);
+}
+
+HWYBLAS_API void sgetrf_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv,
+                         hwyblas_int* info) {
+  GetrfEntry<float>(false, "SGETRF", m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void sgetrf2_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* ipiv,
+                          hwyblas_int* info) {
+  GetrfEntry<float>(true, "SGETRF2", m, n, a, lda, ipiv, info);
+}
+
+HWYBLAS_API void slaswp_(const hwyblas_int* n, float* a, const hwyblas_int* lda,
+                         const hwyblas_int* k1, const hwyblas_int* k2,
+                         const hwyblas_int* ipiv, const hwyblas_int* incx) {
+  LaswpEntry<float>("SLASWP", n, a, lda, k1, k2, ipiv, incx);
+}
+
+HWYBLAS_API void sgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const float* a,
+                         const hwyblas_int* lda, const hwyblas_int* ipiv,
+                         float* b, const hwyblas_int* ldb, hwyblas_int* info) {
+  GetrsEntry<float>("SGETRS", trans, n, nrhs, a, lda, ipiv, b, ldb, info);
+}
+
+HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
+                        const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
+                        const hwyblas_int* ldb, hwyblas_int* info) {
+  GesvEntry<float>("SGESV", n, nrhs, a, lda, ipiv, b, ldb, info);
 }
 
 static bool CheckPotrf(const char* name, const char* uplo, int n, int lda,
@@ -810,14 +873,13 @@ HWYBLAS_API void cblas_sgemm(const CBLAS_LAYOUT layout,
                    lda, b, ldb, beta, c, ldc);
 }
 
-HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
-                             const CBLAS_UPLO uplo,
-                             const CBLAS_TRANSPOSE transa,
-                             const CBLAS_DIAG diag, const hwyblas_int m_in,
-                             const hwyblas_int n_in, const double alpha,
-                             const double* a, const hwyblas_int lda, double* b,
-                             const hwyblas_int ldb) {
-  const char* name = "cblas_dtrsm";
+extern "C++" {
+template <typename T>
+static void CblasTrsm(const char* name, const char* routine, const CBLAS_LAYOUT layout,
+                      const CBLAS_SIDE side, const CBLAS_UPLO uplo,
+                      const CBLAS_TRANSPOSE transa, const CBLAS_DIAG diag,
+                      const hwyblas_int m_in, const hwyblas_int n_in, const T alpha,
+                      const T* a, const hwyblas_int lda, T* b, const hwyblas_int ldb) {
   if (!hb::ValidLayout(name, layout)) return;
   char sc = hb::SideChar(side), uc = hb::UploChar(uplo);
   const char tc = hb::TransChar(transa), dc = hb::DiagChar(diag);
@@ -830,13 +892,34 @@ HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
   }
   if (row) {
     hb::CblasScope scope(name, {2, 3, 4, 5, 7, 6, 8, 9, 10, 11, 12});
-    hb::TrsmEntry<double>("DTRSM", &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda,
-                          b, &ldb);
+    hb::TrsmEntry<T>(routine, &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda, b, &ldb);
   } else {
     hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12});
-    hb::TrsmEntry<double>("DTRSM", &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda,
-                          b, &ldb);
+    hb::TrsmEntry<T>(routine, &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda, b, &ldb);
   }
+}
+}  // extern "C++"
+
+HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m_in,
+                             const hwyblas_int n_in, const double alpha,
+                             const double* a, const hwyblas_int lda, double* b,
+                             const hwyblas_int ldb) {
+  CblasTrsm<double>("cblas_dtrsm", "DTRSM", layout, side, uplo, transa, diag, m_in, n_in,
+                    alpha, a, lda, b, ldb);
+}
+
+HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m_in,
+                             const hwyblas_int n_in, const float alpha,
+                             const float* a, const hwyblas_int lda, float* b,
+                             const hwyblas_int ldb) {
+  CblasTrsm<float>("cblas_strsm", "STRSM", layout, side, uplo, transa, diag, m_in, n_in,
+                   alpha, a, lda, b, ldb);
 }
 
 HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,

@@ -62,6 +62,13 @@ HWYBLAS_API void dtrsm_(const char* side, const char* uplo, const char* transa,
                         const hwyblas_int* n, const double* alpha,
                         const double* a, const hwyblas_int* lda, double* b,
                         const hwyblas_int* ldb);
+/* Single precision (include/hwyblas/hwyblas.h:787, src/trsm.cc:190-195):
+ * the same algorithm at float. */
+HWYBLAS_API void strsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m,
+                        const hwyblas_int* n, const float* alpha,
+                        const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb);
 /* C := alpha*A*A**T + beta*C (trans N) or alpha*A**T*A + beta*C on one
  * triangle. Replaces dsyrk_ (include/hwyblas/hwyblas.h:637,
  * src/level3.cc:416-421). */
@@ -117,6 +124,25 @@ HWYBLAS_API void dgetrs_(const char* trans, const hwyblas_int* n,
 HWYBLAS_API void dgesv_(const hwyblas_int* n, const hwyblas_int* nrhs,
                         double* a, const hwyblas_int* lda, hwyblas_int* ipiv,
                         double* b, const hwyblas_int* ldb, hwyblas_int* info);
+/* Single-precision LU family: the reference instantiates one template for
+ * s and d (src/lapack/getrf.cc:507-546); same algorithms at float, chunks of
+ * 384 in the GEMM chains (include/hwyblas/lapack.h:90, 102, 117, 135, 155). */
+HWYBLAS_API void sgetrf_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv,
+                         hwyblas_int* info);
+HWYBLAS_API void sgetrf2_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* ipiv,
+                          hwyblas_int* info);
+HWYBLAS_API void slaswp_(const hwyblas_int* n, float* a, const hwyblas_int* lda,
+                         const hwyblas_int* k1, const hwyblas_int* k2,
+                         const hwyblas_int* ipiv, const hwyblas_int* incx);
+HWYBLAS_API void sgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const float* a,
+                         const hwyblas_int* lda, const hwyblas_int* ipiv,
+                         float* b, const hwyblas_int* ldb, hwyblas_int* info);
+HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
+                        const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
+                        const hwyblas_int* ldb, hwyblas_int* info);
 /* Cholesky, blocked with nb = 64 (include/hwyblas/lapack.h:663,
  * src/lapack/potrf.cc:128-199, 747-751). */
 HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
@@ -182,6 +208,14 @@ HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
                              const CBLAS_DIAG diag, const hwyblas_int m,
                              const hwyblas_int n, const double alpha,
                              const double* a, const hwyblas_int lda, double* b,
+                             const hwyblas_int ldb);
+/* Single precision (include/hwyblas/cblas.h:858, src/cblas.cc:1950). */
+HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo,
+                             const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m,
+                             const hwyblas_int n, const float alpha,
+                             const float* a, const hwyblas_int lda, float* b,
                              const hwyblas_int ldb);
 /* 0-based (include/hwyblas/cblas.h:128, src/cblas.cc:845). */
 HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,

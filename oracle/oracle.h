@@ -47,6 +47,9 @@ void orc_dlaswp(int n, double* a, int lda, int k1, int k2, const int* ipiv,
 int orc_dgetrf(int m, int n, double* a, int lda, int* ipiv);
 int orc_dgetrf2(int m, int n, double* a, int lda, int* ipiv);
 int orc_sgetrf(int m, int n, float* a, int lda, int* ipiv);
+int orc_sgetrf2(int m, int n, float* a, int lda, int* ipiv);
+void orc_slaswp(int n, float* a, int lda, int k1, int k2, const int* ipiv, int incx);
+int orc_sgesv(int n, int nrhs, float* a, int lda, int* ipiv, float* b, int ldb);
 int orc_dgetrs(char trans, int n, int nrhs, const double* a, int lda,
                const int* ipiv, double* b, int ldb);
 int orc_sgetrs(char trans, int n, int nrhs, const float* a, int lda,

@@ -310,6 +310,23 @@ int orc_dgetrf2(int m, int n, double* a, int lda, int* ipiv) {
 int orc_sgetrf(int m, int n, float* a, int lda, int* ipiv) {
   return orc::Getrf<float>(m, n, a, lda, ipiv);
 }
+/* The reference's s-prefixed LU family is the same template at float
+ * (src/lapack/getrf.cc:507-546). */
+int orc_sgetrf2(int m, int n, float* a, int lda, int* ipiv) {
+  return orc::Getrf2<float>(m, n, a, lda, ipiv);
+}
+void orc_slaswp(int n, float* a, int lda, int k1, int k2, const int* ipiv, int incx) {
+  orc::Laswp<float>(n, a, lda, k1, k2, ipiv, incx);
+}
+int orc_sgesv(int n, int nrhs, float* a, int lda, int* ipiv, float* b, int ldb) {
+  if (n < 0) return -1;
+  if (nrhs < 0) return -2;
+  if (lda < std::max(1, n)) return -4;
+  if (ldb < std::max(1, n)) return -7;
+  int info = orc::Getrf<float>(n, n, a, lda, ipiv);
+  if (info == 0) info = orc::Getrs<float>('N', n, nrhs, a, lda, ipiv, b, ldb);
+  return info;
+}
 int orc_dgetrs(char trans, int n, int nrhs, const double* a, int lda,
                const int* ipiv, double* b, int ldb) {
   return orc::Getrs<double>(trans, n, nrhs, a, lda, ipiv, b, ldb);

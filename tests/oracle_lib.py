@@ -39,6 +39,9 @@ def load_ref():
     lib.dpotrf2_.argtypes = [P] * 5
     lib.dgetrs_.argtypes = [P] * 9
     lib.dgesv_.argtypes = [P] * 8
+    lib.sgetrf_.argtypes = [P] * 6
+    lib.sgetrf2_.argtypes = [P] * 6
+    lib.sgesv_.argtypes = [P] * 8
     return lib
 
 
@@ -65,6 +68,10 @@ class Oracle:
         L.orc_dgetrf.argtypes = [I, I, P, I, P]
         L.orc_dgetrf2.argtypes = [I, I, P, I, P]
         L.orc_sgetrf.argtypes = [I, I, P, I, P]
+        L.orc_sgetrf2.argtypes = [I, I, P, I, P]
+        L.orc_slaswp.argtypes = [I, P, I, I, I, P, I]
+        L.orc_sgesv.argtypes = [I, I, P, I, P, P, I]
+        L.orc_strsm.argtypes = [CH, CH, CH, CH, I, I, F, P, I, P, I]
         L.orc_dgetrs.argtypes = [CH, I, I, P, I, P, P, I]
         L.orc_sgetrs.argtypes = [CH, I, I, P, I, P, P, I]
         L.orc_dgesv.argtypes = [I, I, P, I, P, P, I]
@@ -108,6 +115,22 @@ class Oracle:
     def sgetrf(self, m, n, a, lda, ipiv):
         return self.lib.orc_sgetrf(m, n, ptr(a), lda, ptr(ipiv))
 
+    def sgetrf2(self, m, n, a, lda, ipiv):
+        return self.lib.orc_sgetrf2(m, n, ptr(a), lda, ptr(ipiv))
+
+    def slaswp(self, n, a, lda, k1, k2, ipiv, incx):
+        self.lib.orc_slaswp(n, ptr(a), lda, k1, k2, ptr(ipiv), incx)
+
+    def sgetrs(self, trans, n, nrhs, a, lda, ipiv, b, ldb):
+        return self.lib.orc_sgetrs(_b(trans), n, nrhs, ptr(a), lda, ptr(ipiv), ptr(b), ldb)
+
+    def sgesv(self, n, nrhs, a, lda, ipiv, b, ldb):
+        return self.lib.orc_sgesv(n, nrhs, ptr(a), lda, ptr(ipiv), ptr(b), ldb)
+
+    def strsm(self, side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+        return self.lib.orc_strsm(_b(side), _b(uplo), _b(trans), _b(diag), m, n, alpha,
+                                  ptr(a), lda, ptr(b), ldb)
+
     def dgetrs(self, trans, n, nrhs, a, lda, ipiv, b, ldb):
         return self.lib.orc_dgetrs(_b(trans), n, nrhs, ptr(a), lda, ptr(ipiv), ptr(b), ldb)
 
@@ -131,7 +154,20 @@ def ref_call_getrf(lib, recursive, m, n, a, lda, ipiv):
     info = ctypes.c_int(0)
     args = [ctypes.byref(ctypes.c_int(m)), ctypes.byref(ctypes.c_int(n)), ptr(a),
             ctypes.byref(ctypes.c_int(lda)), ptr(ipiv), ctypes.byref(info)]
-    (lib.dgetrf2_ if recursive else lib.dgetrf_)(*args)
+    if a.dtype == np.float32:
+        (lib.sgetrf2_ if recursive else lib.sgetrf_)(*args)
+    else:
+        (lib.dgetrf2_ if recursive else lib.dgetrf_)(*args)
+    return info.value
+
+
+def ref_call_gesv(lib, n, nrhs, a, lda, ipiv, b, ldb):
+    """The reference driver's ?gesv_ (src/lapack/getrf.cc:531), by dtype."""
+    info = ctypes.c_int(0)
+    fn = lib.sgesv_ if a.dtype == np.float32 else lib.dgesv_
+    fn(ctypes.byref(ctypes.c_int(n)), ctypes.byref(ctypes.c_int(nrhs)), ptr(a),
+       ctypes.byref(ctypes.c_int(lda)), ptr(ipiv), ptr(b), ctypes.byref(ctypes.c_int(ldb)),
+       ctypes.byref(info))
     return info.value
 
 

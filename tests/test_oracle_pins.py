@@ -17,8 +17,8 @@
 import numpy as np
 import pytest
 
-from tests.oracle_lib import (rand, ref_call_getrf, ref_call_potrf, same_bits,
-                              first_diff)
+from tests.oracle_lib import (rand, ref_call_getrf, ref_call_gesv, ref_call_potrf,
+                              same_bits, first_diff)
 
 EPS = np.finfo(np.float64).eps
 
@@ -51,6 +51,41 @@ def test_getrf_matches_reference_driver(orc, ref_drivers, recursive, m, n):
     assert i1 == i2
     assert np.array_equal(p1, p2)
     assert same_bits(a1, a2), first_diff(a1, a2)
+
+
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("m,n", GETRF_SHAPES)
+def test_sgetrf_matches_reference_driver(orc, ref_drivers, recursive, m, n):
+    """The single-precision LU: the reference's getrf.cc at float on the
+    oracle's float BLAS against the oracle's restatement (getrf.cc:507-546)."""
+    rng = np.random.default_rng(m * 1000 + n + 7)
+    lda = m + 2
+    a = rand(rng, lda, n, np.float32)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1 = np.zeros(min(m, n), np.int32)
+    p2 = np.zeros(min(m, n), np.int32)
+    f = orc.sgetrf2 if recursive else orc.sgetrf
+    i1 = f(m, n, a1, lda, p1)
+    i2 = ref_call_getrf(ref_drivers, recursive, m, n, a2, lda, p2)
+    assert i1 == i2
+    assert np.array_equal(p1, p2)
+    assert same_bits(a1, a2), first_diff(a1, a2)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (40, 3), (129, 17), (300, 1)])
+def test_gesv_matches_reference_driver(orc, ref_drivers, dtype, n, nrhs):
+    rng = np.random.default_rng(n + nrhs)
+    a = rand(rng, n, n, dtype)
+    b = rand(rng, n, nrhs, dtype)
+    a1, a2, b1, b2 = (x.copy(order="F") for x in (a, a, b, b))
+    p1 = np.zeros(n, np.int32)
+    p2 = np.zeros(n, np.int32)
+    f = orc.sgesv if dtype == np.float32 else orc.dgesv
+    assert f(n, nrhs, a1, n, p1, b1, n) == ref_call_gesv(ref_drivers, n, nrhs, a2, n, p2,
+                                                         b2, n)
+    assert np.array_equal(p1, p2)
+    assert same_bits(a1, a2) and same_bits(b1, b2), first_diff(b1, b2)
 
 
 @pytest.mark.parametrize("recursive", [False, True])
@@ -271,6 +306,35 @@ def test_trsm_residual_bound(orc, side, uplo, trans, diag, m):
     scale = (np.abs(op) @ np.abs(x)) if side == "L" else (np.abs(x) @ np.abs(op))
     scale = scale + abs(alpha) * np.abs(b) + np.finfo(np.float64).tiny
     assert np.all(res <= 8 * (ka + 2) * EPS / 2 * scale)
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+@pytest.mark.parametrize("m", [1, 31, 33, 100])
+def test_strsm_residual_bound(orc, side, uplo, trans, diag, m):
+    """The single-precision TRSM restatement: the same residual bound with the
+    float epsilon (level3_test.cc:479-520 runs it for float and double)."""
+    rng = np.random.default_rng(m + 3)
+    n = 7
+    ka = m if side == "L" else n
+    a = rand(rng, ka, ka)
+    a = np.asfortranarray((a / ka + np.diag(1.5 + rng.uniform(0, 1, ka))).astype(np.float32))
+    b = rand(rng, m, n, np.float32)
+    alpha = np.float32(0.75)
+    x = b.copy(order="F")
+    assert orc.strsm(side, uplo, trans, diag, m, n, alpha, a, ka, x, m) == 0
+    t = np.tril(a) if uplo == "L" else np.triu(a)
+    if diag == "U":
+        np.fill_diagonal(t, 1.0)
+    op = (t if trans == "N" else t.T).astype(np.float64)
+    X = x.astype(np.float64)
+    lhs = op @ X if side == "L" else X @ op
+    res = np.abs(lhs - float(alpha) * b.astype(np.float64))
+    scale = (np.abs(op) @ np.abs(X)) if side == "L" else (np.abs(X) @ np.abs(op))
+    scale = scale + abs(float(alpha)) * np.abs(b) + np.finfo(np.float32).tiny
+    assert np.all(res <= 8 * (ka + 2) * np.finfo(np.float32).eps / 2 * scale)
 
 
 def test_trsm_alpha_zero_does_not_read_a(orc):
