@@ -38,6 +38,24 @@ PROTOTYPES = {
     "dpotrf2_": (None, [C, PI, P, PI, PI]),
     "dpotrs_": (None, [C, PI, PI, P, PI, P, PI, PI]),
     "dposv_": (None, [C, PI, PI, P, PI, P, PI, PI]),
+    # LAPACKE (by value; char arguments as one byte)
+    "LAPACKE_xerbla": (None, [C, I]),
+    "LAPACKE_set_nancheck": (None, [I]),
+    "LAPACKE_get_nancheck": (I, []),
+    **{f"LAPACKE_{p}getrf{s}": (I, [I, I, I, P, I, P])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}getrf2{s}": (I, [I, I, I, P, I, P])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}getrs{s}": (I, [I, ctypes.c_char, I, I, P, I, P, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}gesv{s}": (I, [I, I, I, P, I, P, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_dpotrf{s}": (I, [I, ctypes.c_char, I, P, I]) for s in ("", "_work")},
+    **{f"LAPACKE_dpotrf2{s}": (I, [I, ctypes.c_char, I, P, I]) for s in ("", "_work")},
+    **{f"LAPACKE_dpotrs{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
+       for s in ("", "_work")},
+    **{f"LAPACKE_dposv{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
+       for s in ("", "_work")},
     # CBLAS (by value)
     "cblas_xerbla": (None, [I, C, C]),
     "cblas_dgemm": (None, [I, I, I, I, I, I, D, P, I, P, I, D, P, I]),

@@ -79,7 +79,9 @@ enum WorkspaceSlot : int {
   kWsEmulAcc2 = 15,
   kWsEmulW2 = 16,
   kWsTourney = 17, // tournament-pivoting leaf: candidates and results
-  kNumWorkspaceSlots = 18
+  kWsLapacke0 = 18, // LAPACKE row-major temporaries (device callers)
+  kWsLapacke1 = 19,
+  kNumWorkspaceSlots = 20
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is

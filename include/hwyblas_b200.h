@@ -164,6 +164,98 @@ HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n,
                         const hwyblas_int* ldb, hwyblas_int* info);
 
 /* ------------------------------------------------------------------------ */
+/* LAPACKE (include/hwyblas/lapacke.h:35-106, 114-149, 206-260, 624-720;
+ * src/lapack/lapacke.cc:37-137, lapacke_linear.cc:22-73,
+ * lapacke_symmetric.cc:22-72, lapacke_util.h:418-480). LAPACKE_xyyzzz checks
+ * the layout (LAPACKE_xerbla(name, -1)), then, unless switched off
+ * (LAPACKE_set_nancheck or LAPACKE_NANCHECK=0), returns -i if input argument
+ * i holds a NaN, then calls LAPACKE_xyyzzz_work. The _work function calls
+ * the LAPACK routine directly for column-major arrays (INFO < 0 shifted by
+ * one for the layout argument); for row-major arrays it checks that each
+ * leading dimension covers the columns (else LAPACKE_xerbla and -i),
+ * transposes into column-major temporaries (host or device, where the
+ * caller's array lives), calls the routine and transposes the outputs
+ * back. Results are bit-identical to the column-major routine on the
+ * transposed data. */
+#define lapack_int hwyblas_int
+#define LAPACK_ROW_MAJOR 101
+#define LAPACK_COL_MAJOR 102
+#define LAPACK_WORK_MEMORY_ERROR -1010
+#define LAPACK_TRANSPOSE_MEMORY_ERROR -1011
+
+/* Prints "Wrong parameter i in NAME" (or the out-of-memory message). */
+HWYBLAS_API void LAPACKE_xerbla(const char* name, lapack_int info);
+HWYBLAS_API void LAPACKE_set_nancheck(int flag);
+HWYBLAS_API int LAPACKE_get_nancheck(void);
+
+HWYBLAS_API lapack_int LAPACKE_dgetrf(int matrix_layout, lapack_int m, lapack_int n,
+                                      double* a, lapack_int lda, lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_dgetrf_work(int matrix_layout, lapack_int m,
+                                           lapack_int n, double* a, lapack_int lda,
+                                           lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_dgetrf2(int matrix_layout, lapack_int m, lapack_int n,
+                                       double* a, lapack_int lda, lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_dgetrf2_work(int matrix_layout, lapack_int m,
+                                            lapack_int n, double* a, lapack_int lda,
+                                            lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_dgetrs(int matrix_layout, char trans, lapack_int n,
+                                      lapack_int nrhs, const double* a, lapack_int lda,
+                                      const lapack_int* ipiv, double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dgetrs_work(int matrix_layout, char trans, lapack_int n,
+                                           lapack_int nrhs, const double* a,
+                                           lapack_int lda, const lapack_int* ipiv,
+                                           double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dgesv(int matrix_layout, lapack_int n, lapack_int nrhs,
+                                     double* a, lapack_int lda, lapack_int* ipiv,
+                                     double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dgesv_work(int matrix_layout, lapack_int n,
+                                          lapack_int nrhs, double* a, lapack_int lda,
+                                          lapack_int* ipiv, double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sgetrf(int matrix_layout, lapack_int m, lapack_int n,
+                                      float* a, lapack_int lda, lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_sgetrf_work(int matrix_layout, lapack_int m,
+                                           lapack_int n, float* a, lapack_int lda,
+                                           lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_sgetrf2(int matrix_layout, lapack_int m, lapack_int n,
+                                       float* a, lapack_int lda, lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_sgetrf2_work(int matrix_layout, lapack_int m,
+                                            lapack_int n, float* a, lapack_int lda,
+                                            lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_sgetrs(int matrix_layout, char trans, lapack_int n,
+                                      lapack_int nrhs, const float* a, lapack_int lda,
+                                      const lapack_int* ipiv, float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sgetrs_work(int matrix_layout, char trans, lapack_int n,
+                                           lapack_int nrhs, const float* a,
+                                           lapack_int lda, const lapack_int* ipiv,
+                                           float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sgesv(int matrix_layout, lapack_int n, lapack_int nrhs,
+                                     float* a, lapack_int lda, lapack_int* ipiv,
+                                     float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sgesv_work(int matrix_layout, lapack_int n,
+                                          lapack_int nrhs, float* a, lapack_int lda,
+                                          lapack_int* ipiv, float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dpotrf(int matrix_layout, char uplo, lapack_int n,
+                                      double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_dpotrf_work(int matrix_layout, char uplo, lapack_int n,
+                                           double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_dpotrf2(int matrix_layout, char uplo, lapack_int n,
+                                       double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_dpotrf2_work(int matrix_layout, char uplo, lapack_int n,
+                                            double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_dpotrs(int matrix_layout, char uplo, lapack_int n,
+                                      lapack_int nrhs, const double* a, lapack_int lda,
+                                      double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dpotrs_work(int matrix_layout, char uplo, lapack_int n,
+                                           lapack_int nrhs, const double* a,
+                                           lapack_int lda, double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dposv(int matrix_layout, char uplo, lapack_int n,
+                                     lapack_int nrhs, double* a, lapack_int lda,
+                                     double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_dposv_work(int matrix_layout, char uplo, lapack_int n,
+                                          lapack_int nrhs, double* a, lapack_int lda,
+                                          double* b, lapack_int ldb);
+
+/* ------------------------------------------------------------------------ */
 /* CBLAS (include/hwyblas/cblas.h:20-45)                                    */
 
 #define CBLAS_INDEX size_t
