@@ -16,8 +16,8 @@ from . import _abi
 __all__ = [
     "lib", "dgemm", "sgemm", "dtrsm", "strsm", "dsyrk", "idamax", "dlaswp", "dgetrf",
     "dgetrf2", "dgetrs", "dgesv", "slaswp", "sgetrf", "sgetrf2", "sgetrs", "sgesv",
-    "dpotrf", "dpotrf2", "dpotrs", "dposv",
-    "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_strsm", "cblas_idamax",
+    "dpotrf", "dpotrf2", "dpotrs", "dposv", "ssyrk", "spotrf", "spotrf2", "spotrs",
+    "sposv", "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_strsm", "cblas_idamax",
     "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
@@ -45,6 +45,7 @@ def lib():
 from ._api import (  # noqa: E402  (needs lib())
     dgemm, sgemm, dtrsm, strsm, dsyrk, idamax, dlaswp, dgetrf, dgetrf2, dgetrs,
     dgesv, slaswp, sgetrf, sgetrf2, sgetrs, sgesv, dpotrf, dpotrf2, dpotrs, dposv,
+    ssyrk, spotrf, spotrf2, spotrs, sposv,
     cblas_dgemm, cblas_sgemm, cblas_dtrsm, cblas_strsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
     dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,

@@ -20,6 +20,7 @@ PROTOTYPES = {
     "dtrsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "strsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
+    "ssyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     "idamax_": (I, [PI, P, PI]),
     "xerbla_": (None, [C, PI, ctypes.c_size_t]),
     "hwyblas_set_error_handler": (P, [P]),
@@ -38,6 +39,10 @@ PROTOTYPES = {
     "dpotrf2_": (None, [C, PI, P, PI, PI]),
     "dpotrs_": (None, [C, PI, PI, P, PI, P, PI, PI]),
     "dposv_": (None, [C, PI, PI, P, PI, P, PI, PI]),
+    "spotrf_": (None, [C, PI, P, PI, PI]),
+    "spotrf2_": (None, [C, PI, P, PI, PI]),
+    "spotrs_": (None, [C, PI, PI, P, PI, P, PI, PI]),
+    "sposv_": (None, [C, PI, PI, P, PI, P, PI, PI]),
     # LAPACKE (by value; char arguments as one byte)
     "LAPACKE_xerbla": (None, [C, I]),
     "LAPACKE_set_nancheck": (None, [I]),
@@ -50,12 +55,14 @@ PROTOTYPES = {
        for p in "ds" for s in ("", "_work")},
     **{f"LAPACKE_{p}gesv{s}": (I, [I, I, I, P, I, P, P, I])
        for p in "ds" for s in ("", "_work")},
-    **{f"LAPACKE_dpotrf{s}": (I, [I, ctypes.c_char, I, P, I]) for s in ("", "_work")},
-    **{f"LAPACKE_dpotrf2{s}": (I, [I, ctypes.c_char, I, P, I]) for s in ("", "_work")},
-    **{f"LAPACKE_dpotrs{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
-       for s in ("", "_work")},
-    **{f"LAPACKE_dposv{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
-       for s in ("", "_work")},
+    **{f"LAPACKE_{p}potrf{s}": (I, [I, ctypes.c_char, I, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}potrf2{s}": (I, [I, ctypes.c_char, I, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}potrs{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}posv{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
+       for p in "ds" for s in ("", "_work")},
     # CBLAS (by value)
     "cblas_xerbla": (None, [I, C, C]),
     "cblas_dgemm": (None, [I, I, I, I, I, I, D, P, I, P, I, D, P, I]),

@@ -77,6 +77,12 @@ def dsyrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
                  _d(beta), _ptr(c), _i(ldc))
 
 
+def ssyrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """FP32 symmetric rank-k update (reference ssyrk_, src/level3.cc:410)."""
+    lib().ssyrk_(_c(uplo), _c(trans), _i(n), _i(k), _f(alpha), _ptr(a), _i(lda),
+                 _f(beta), _ptr(c), _i(ldc))
+
+
 def idamax(n, x, incx):
     """1-based index of the first largest |x| (reference idamax_)."""
     return lib().idamax_(_i(n), _ptr(x), _i(incx))
@@ -161,6 +167,28 @@ def dpotrs(uplo, n, nrhs, a, lda, b, ldb):
 def dposv(uplo, n, nrhs, a, lda, b, ldb):
     """Cholesky solve of A X = B; returns INFO (src/lapack/posv.cc:78)."""
     return _info_call(lib().dposv_, _c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(b), _i(ldb))
+
+
+def spotrf(uplo, n, a, lda):
+    """FP32 blocked Cholesky; returns INFO (reference spotrf_, src/lapack/potrf.cc:748)."""
+    return _info_call(lib().spotrf_, _c(uplo), _i(n), _ptr(a), _i(lda))
+
+
+def spotrf2(uplo, n, a, lda):
+    """FP32 recursive Cholesky; returns INFO (src/lapack/potrf.cc:753)."""
+    return _info_call(lib().spotrf2_, _c(uplo), _i(n), _ptr(a), _i(lda))
+
+
+def spotrs(uplo, n, nrhs, a, lda, b, ldb):
+    """FP32 solve with the Cholesky factor; returns INFO (src/lapack/posv.cc)."""
+    return _info_call(lib().spotrs_, _c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(b), _i(ldb))
+
+
+def sposv(uplo, n, nrhs, a, lda, b, ldb):
+    """FP32 Cholesky solve of A X = B; returns INFO (src/lapack/posv.cc)."""
+    return _info_call(lib().sposv_, _c(uplo), _i(n), _i(nrhs), _ptr(a), _i(lda),
                       _ptr(b), _i(ldb))
 
 

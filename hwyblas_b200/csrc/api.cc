@@ -473,11 +473,13 @@ HWYBLAS_API void strsm_(const char* side, const char* uplo, const char* transa,
                        b, ldb);
 }
 
-HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
-                        const hwyblas_int* n_p, const hwyblas_int* k_p,
-                        const double* alpha_p, const double* a,
-                        const hwyblas_int* lda_p, const double* beta_p,
-                        double* c, const hwyblas_int* ldc_p) {
+extern "C++" {
+// SYRK for T = double and float (src/level3.cc:410-421).
+template <typename T>
+static void SyrkEntry(const char* name, const char* uplo, const char* trans,
+                      const hwyblas_int* n_p, const hwyblas_int* k_p, const T* alpha_p,
+                      const T* a, const hwyblas_int* lda_p, const T* beta_p, T* c,
+                      const hwyblas_int* ldc_p) {
   const int n = *n_p, k = *k_p, lda = *lda_p, ldc = *ldc_p;
   const char u = hb::Up(*uplo);
   bool t;
@@ -492,20 +494,35 @@ HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
   else if (lda < std::max(1, rows_a)) info = 7;
   else if (ldc < std::max(1, n)) info = 10;
   if (info != 0) {
-    hb::ReportError("DSYRK", info);
+    hb::ReportError(name, info);
     return;
   }
-  const double alpha = *alpha_p, beta = *beta_p;
-  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return;
-  const bool compute = !(alpha == 0.0 || k == 0);
-  hb::Staged<double> sa, sc;
+  const T alpha = *alpha_p, beta = *beta_p;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  const bool compute = !(alpha == T(0) || k == 0);
+  hb::Staged<T> sa, sc;
   if (compute && !sa.In(a, lda, rows_a, t ? n : k, hb::kWsStageA, true)) return;
   // The whole square is copied so that the other triangle comes back as is.
   if (!sc.In(c, ldc, n, n, hb::kWsStageC, true)) return;
-  hb::SyrkFull(u == 'L', t, n, k, alpha, sa.dev, std::max(sa.ld, 1), beta,
+  hb::SyrkFull<T>(u == 'L', t, n, k, alpha, sa.dev, std::max(sa.ld, 1), beta,
                sc.dev, sc.ld);
   sc.Out();
-  hb::Finish("DSYRK");
+  hb::Finish(name);
+}
+}  // extern "C++"
+
+HWYBLAS_API void dsyrk_(const char* uplo, const char* trans, const hwyblas_int* n,
+                        const hwyblas_int* k, const double* alpha, const double* a,
+                        const hwyblas_int* lda, const double* beta, double* c,
+                        const hwyblas_int* ldc) {
+  SyrkEntry<double>("DSYRK", uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+
+HWYBLAS_API void ssyrk_(const char* uplo, const char* trans, const hwyblas_int* n,
+                        const hwyblas_int* k, const float* alpha, const float* a,
+                        const hwyblas_int* lda, const float* beta, float* c,
+                        const hwyblas_int* ldc) {
+  SyrkEntry<float>("SSYRK", uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
 }
 
 HWYBLAS_API hwyblas_int idamax_(const hwyblas_int* n_p, const double* x,
@@ -743,92 +760,127 @@ static bool CheckPotrf(const char* name, const char* uplo, int n, int lda,
   return true;
 }
 
-static void PotrfEntry(bool recursive, const char* uplo, const hwyblas_int* n_p,
-                       double* a, const hwyblas_int* lda_p,
+extern "C++" {
+// The Cholesky family for T = double and float (the reference instantiates
+// one template for both: src/lapack/potrf.cc:747-773, posv.cc).
+template <typename T>
+static void PotrfEntry(bool recursive, const char* name, const char* uplo,
+                       const hwyblas_int* n_p, T* a, const hwyblas_int* lda_p,
                        hwyblas_int* info) {
   const int n = *n_p, lda = *lda_p;
-  const char* name = recursive ? "DPOTRF2" : "DPOTRF";
   bool upper;
   if (!CheckPotrf(name, uplo, n, lda, info, &upper)) return;
   if (n == 0) return;
-  hb::Staged<double> sa;
+  hb::Staged<T> sa;
   if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
   hb::ResetInfo();
   if (recursive) {
-    hb::Potrf2(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+    hb::Potrf2<T>(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
   } else {
-    hb::Potrf(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+    hb::Potrf<T>(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
   }
   sa.Out();
   *info = hb::ReadInfo();
   hb::Finish(name);
 }
 
+static bool CheckPos(const char* name, const char* uplo, int n, int nrhs, int lda, int ldb,
+                     int* info, bool* upper) {
+  const char u = hb::Up(*uplo);
+  *upper = (u == 'U');
+  *info = 0;
+  if (!*upper && u != 'L') *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -7;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return false;
+  }
+  return true;
+}
+
+template <typename T>
+static void PotrsEntry(const char* name, const char* uplo, const hwyblas_int* n_p,
+                       const hwyblas_int* nrhs_p, const T* a, const hwyblas_int* lda_p, T* b,
+                       const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  bool upper;
+  if (!CheckPos(name, uplo, n, nrhs, lda, ldb, info, &upper)) return;
+  if (n == 0 || nrhs == 0) return;
+  hb::Staged<T> sa, sb;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  hb::Potrs<T>(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish(name);
+}
+
+template <typename T>
+static void PosvEntry(const char* name, const char* uplo, const hwyblas_int* n_p,
+                      const hwyblas_int* nrhs_p, T* a, const hwyblas_int* lda_p, T* b,
+                      const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  bool upper;
+  if (!CheckPos(name, uplo, n, nrhs, lda, ldb, info, &upper)) return;
+  if (n == 0) return;
+  hb::Staged<T> sa, sb;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  hb::ResetInfo();
+  hb::Potrf<T>(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  const int finfo = hb::ReadInfo();
+  if (finfo == 0 && nrhs > 0) hb::Potrs<T>(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sa.Out();
+  if (finfo == 0) sb.Out();
+  *info = finfo;
+  hb::Finish(name);
+}
+}  // extern "C++"
+
 HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
                          const hwyblas_int* lda, hwyblas_int* info) {
-  PotrfEntry(false, uplo, n, a, lda, info);
+  PotrfEntry<double>(false, "DPOTRF", uplo, n, a, lda, info);
 }
 
 HWYBLAS_API void dpotrf2_(const char* uplo, const hwyblas_int* n, double* a,
                           const hwyblas_int* lda, hwyblas_int* info) {
-  PotrfEntry(true, uplo, n, a, lda, info);
+  PotrfEntry<double>(true, "DPOTRF2", uplo, n, a, lda, info);
 }
 
-HWYBLAS_API void dpotrs_(const char* uplo, const hwyblas_int* n_p,
-                         const hwyblas_int* nrhs_p, const double* a,
-                         const hwyblas_int* lda_p, double* b,
-                         const hwyblas_int* ldb_p, hwyblas_int* info) {
-  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
-  const char u = hb::Up(*uplo);
-  const bool upper = (u == 'U');
-  *info = 0;
-  if (!upper && u != 'L') *info = -1;
-  else if (n < 0) *info = -2;
-  else if (nrhs < 0) *info = -3;
-  else if (lda < std::max(1, n)) *info = -5;
-  else if (ldb < std::max(1, n)) *info = -7;
-  if (*info != 0) {
-    hb::ReportError("DPOTRS", -*info);
-    return;
-  }
-  if (n == 0 || nrhs == 0) return;
-  hb::Staged<double> sa, sb;
-  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
-  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
-  hb::Potrs(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
-  sb.Out();
-  hb::Finish("DPOTRS");
+HWYBLAS_API void dpotrs_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const double* a, const hwyblas_int* lda, double* b,
+                         const hwyblas_int* ldb, hwyblas_int* info) {
+  PotrsEntry<double>("DPOTRS", uplo, n, nrhs, a, lda, b, ldb, info);
 }
 
-HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n_p,
-                        const hwyblas_int* nrhs_p, double* a,
-                        const hwyblas_int* lda_p, double* b,
-                        const hwyblas_int* ldb_p, hwyblas_int* info) {
-  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
-  const char u = hb::Up(*uplo);
-  const bool upper = (u == 'U');
-  *info = 0;
-  if (!upper && u != 'L') *info = -1;
-  else if (n < 0) *info = -2;
-  else if (nrhs < 0) *info = -3;
-  else if (lda < std::max(1, n)) *info = -5;
-  else if (ldb < std::max(1, n)) *info = -7;
-  if (*info != 0) {
-    hb::ReportError("DPOSV", -*info);
-    return;
-  }
-  if (n == 0) return;
-  hb::Staged<double> sa, sb;
-  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
-  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
-  hb::ResetInfo();
-  hb::Potrf(upper, n, sa.dev, sa.ld, hb::DeviceInfo());
-  const int finfo = hb::ReadInfo();
-  if (finfo == 0 && nrhs > 0) hb::Potrs(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
-  sa.Out();
-  if (finfo == 0) sb.Out();
-  *info = finfo;
-  hb::Finish("DPOSV");
+HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                        double* a, const hwyblas_int* lda, double* b, const hwyblas_int* ldb,
+                        hwyblas_int* info) {
+  PosvEntry<double>("DPOSV", uplo, n, nrhs, a, lda, b, ldb, info);
+}
+
+HWYBLAS_API void spotrf_(const char* uplo, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* info) {
+  PotrfEntry<float>(false, "SPOTRF", uplo, n, a, lda, info);
+}
+
+HWYBLAS_API void spotrf2_(const char* uplo, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* info) {
+  PotrfEntry<float>(true, "SPOTRF2", uplo, n, a, lda, info);
+}
+
+HWYBLAS_API void spotrs_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const float* a, const hwyblas_int* lda, float* b,
+                         const hwyblas_int* ldb, hwyblas_int* info) {
+  PotrsEntry<float>("SPOTRS", uplo, n, nrhs, a, lda, b, ldb, info);
+}
+
+HWYBLAS_API void sposv_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                        float* a, const hwyblas_int* lda, float* b, const hwyblas_int* ldb,
+                        hwyblas_int* info) {
+  PosvEntry<float>("SPOSV", uplo, n, nrhs, a, lda, b, ldb, info);
 }
 
 // ---------------------------------------------------------------------------

@@ -598,35 +598,36 @@ __global__ void GetrfLeafTrailingKernel(int m, int w, int n, T* a,
 
 // ---------------------------------------------------------------------------
 // Cholesky leaf (n <= 64) in one CTA, the block in shared memory.
+template <typename T>
 __global__ void __launch_bounds__(256)
-    PotrfLeafKernel(int upper, int n, double* a, long long lda, int* info,
+    PotrfLeafKernel(int upper, int n, T* a, long long lda, int* info,
                     int info_base, int lanes, const int* guard) {
   if (guard != nullptr && *guard != 0) return;
-  __shared__ double s[64][65];  // s[i][j] = A(i, j)
-  __shared__ double row[64];
+  __shared__ T s[64][65];  // s[i][j] = A(i, j)
+  __shared__ T row[64];
   __shared__ int stop;
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     const int i = idx % n, j = idx / n;
     const bool ref = upper ? (i <= j) : (i >= j);
-    s[i][j] = ref ? a[i + j * lda] : 0.0;
+    s[i][j] = ref ? a[i + j * lda] : T(0);
   }
   if (threadIdx.x == 0) stop = 0;
   __syncthreads();
   for (int j = 0; j < n; ++j) {
     if (threadIdx.x == 0) {
-      const double ajj = s[j][j];
-      if (ajj <= 0.0 || isnan(ajj)) {
+      const T ajj = s[j][j];
+      if (ajj <= T(0) || isnan(ajj)) {
         stop = 1;
         if (*info == 0) *info = info_base + j + 1;
       } else {
-        const double r = sqrt(ajj);
+        const T r = sqrt(ajj);
         s[j][j] = r;
-        row[j] = 1.0 / r;  // rinv
+        row[j] = T(1) / r;  // rinv
       }
     }
     __syncthreads();
     if (stop) break;
-    const double rinv = row[j];
+    const T rinv = row[j];
     __syncthreads();
     if (upper) {
       for (int k = j + 1 + threadIdx.x; k < n; k += blockDim.x) {
@@ -838,13 +839,16 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
 template void GetrfLeaf<double>(int, int, double*, int, int*, int*, int, int);
 template void GetrfLeaf<float>(int, int, float*, int, int*, int*, int, int);
 
-void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base) {
-  PotrfLeafKernel<<<1, 256, 0, Ctx().stream>>>(upper ? 1 : 0, n, a, lda, info,
-                                               info_base, RefLanesDouble(),
-                                               Ctx().guard);
+template <typename T>
+void PotrfLeaf(bool upper, int n, T* a, int lda, int* info, int info_base) {
+  const int lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  PotrfLeafKernel<T><<<1, 256, 0, Ctx().stream>>>(upper ? 1 : 0, n, a, lda, info, info_base,
+                                                  lanes, Ctx().guard);
   CountLaunch();
   LaunchFailed("potrf leaf");
 }
+template void PotrfLeaf<double>(bool, int, double*, int, int*, int);
+template void PotrfLeaf<float>(bool, int, float*, int, int*, int);
 
 // ---------------------------------------------------------------------------
 // IDAMAX that allocates nothing (hwyblas_idamax_noalloc).

@@ -117,7 +117,7 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
            double beta, double* c, int ldc, Part part = kAll);
 // FP32 (chunks of 384), FFMA on the CUDA cores.
 void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
-           float beta, float* c, int ldc);
+           float beta, float* c, int ldc, Part part = kAll);
 // C := beta*C on `part` (beta == 0 writes zeros without reading C).
 template <typename T>
 void ScaleMatrix(int m, int n, T beta, T* c, int ldc, Part part = kAll);
@@ -142,7 +142,8 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
                int leaf_w = 16);
 // PotrfLeaf on device: n <= 64; sets *info to info_base + j + 1 and stops at
 // the first non-positive (or NaN) diagonal, if *info is still 0.
-void PotrfLeaf(bool upper, int n, double* a, int lda, int* info, int info_base);
+template <typename T>
+void PotrfLeaf(bool upper, int n, T* a, int lda, int* info, int info_base);
 
 // LAPACK drivers on device data (ipiv, info: device pointers).
 template <typename T>
@@ -152,7 +153,8 @@ void Getrf2(int m, int n, T* a, int lda, int* ipiv, int* info);
 template <typename T>
 void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
            T* b, int ldb);
-void Potrf(bool upper, int n, double* a, int lda, int* info);
+template <typename T>
+void Potrf(bool upper, int n, T* a, int lda, int* info);
 // Potrf2 of a block whose first column is global column col0 (for INFO);
 // later kernels become no-ops after a failure.
 void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
@@ -160,16 +162,18 @@ void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
 // right-looking over leaf-wide sub-panels, not the reference's recursion;
 // pivots relative to the panel's first row; *info set at the first zero pivot.
 void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col0);
-void Potrf2(bool upper, int n, double* a, int lda, int* info);
-void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
-           int ldb);
+template <typename T>
+void Potrf2(bool upper, int n, T* a, int lda, int* info);
+template <typename T>
+void Potrs(bool upper, int n, int nrhs, const T* a, int lda, T* b, int ldb);
 
 // Level-3 with reference semantics (quick returns, alpha scaling).
 template <typename T>
 void TrsmFull(bool left, bool lower, bool trans, bool unit, int m, int n,
               T alpha, const T* a, int lda, T* b, int ldb);
-void SyrkFull(bool lower, bool trans, int n, int k, double alpha,
-              const double* a, int lda, double beta, double* c, int ldc);
+template <typename T>
+void SyrkFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda, T beta,
+              T* c, int ldc);
 template <typename T>
 void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
               int lda, const T* b, int ldb, T beta, T* c, int ldc);

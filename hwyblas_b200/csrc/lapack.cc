@@ -97,34 +97,36 @@ void Getrs(bool trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
 // kernel of the call into a no-op once a leaf has found a non-positive minor
 // (the reference returns at that point, src/lapack/potrf.cc:86-87, 173).
 namespace {
-void Potrf2Rec(bool upper, int n, double* a, int lda, int* info, int col0) {
+template <typename T>
+void Potrf2Rec(bool upper, int n, T* a, int lda, int* info, int col0) {
   if (n == 0) return;
   if (n <= 32) {
-    PotrfLeaf(upper, n, a, lda, info, col0);
+    PotrfLeaf<T>(upper, n, a, lda, info, col0);
     return;
   }
   const int n1 = n / 2, n2 = n - n1;
-  Potrf2Rec(upper, n1, a, lda, info, col0);
+  Potrf2Rec<T>(upper, n1, a, lda, info, col0);
   if (upper) {
-    TrsmFull<double>(true, false, true, false, n1, n2, 1.0, a, lda,
+    TrsmFull<T>(true, false, true, false, n1, n2, T(1), a, lda,
                      At(a, lda, 0, n1), lda);
-    SyrkFull(false, true, n2, n1, -1.0, At(a, lda, 0, n1), lda, 1.0,
+    SyrkFull<T>(false, true, n2, n1, T(-1), At(a, lda, 0, n1), lda, 1.0,
              At(a, lda, n1, n1), lda);
   } else {
-    TrsmFull<double>(false, true, true, false, n2, n1, 1.0, a, lda,
+    TrsmFull<T>(false, true, true, false, n2, n1, T(1), a, lda,
                      At(a, lda, n1, 0), lda);
-    SyrkFull(true, false, n2, n1, -1.0, At(a, lda, n1, 0), lda, 1.0,
+    SyrkFull<T>(true, false, n2, n1, T(-1), At(a, lda, n1, 0), lda, 1.0,
              At(a, lda, n1, n1), lda);
   }
-  Potrf2Rec(upper, n2, At(a, lda, n1, n1), lda, info, col0 + n1);
+  Potrf2Rec<T>(upper, n2, At(a, lda, n1, n1), lda, info, col0 + n1);
 }
 }  // namespace
 
-void Potrf2(bool upper, int n, double* a, int lda, int* info) {
+template <typename T>
+void Potrf2(bool upper, int n, T* a, int lda, int* info) {
   Context& ctx = Ctx();
   const int* saved = ctx.guard;
   ctx.guard = info;
-  Potrf2Rec(upper, n, a, lda, info, 0);
+  Potrf2Rec<T>(upper, n, a, lda, info, 0);
   ctx.guard = saved;
 }
 
@@ -136,11 +138,12 @@ void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0) {
   ctx.guard = saved;
 }
 
-void Potrf(bool upper, int n, double* a, int lda, int* info) {
+template <typename T>
+void Potrf(bool upper, int n, T* a, int lda, int* info) {
   if (n == 0) return;
   const int nb = 64;
   if (nb >= n) {
-    Potrf2(upper, n, a, lda, info);
+    Potrf2<T>(upper, n, a, lda, info);
     return;
   }
   Context& ctx = Ctx();
@@ -149,25 +152,25 @@ void Potrf(bool upper, int n, double* a, int lda, int* info) {
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
     if (upper) {
-      SyrkFull(false, true, jb, j, -1.0, At(a, lda, 0, j), lda, 1.0,
+      SyrkFull<T>(false, true, jb, j, T(-1), At(a, lda, 0, j), lda, 1.0,
                At(a, lda, j, j), lda);
-      Potrf2Rec(true, jb, At(a, lda, j, j), lda, info, j);
+      Potrf2Rec<T>(true, jb, At(a, lda, j, j), lda, info, j);
       if (j + jb < n) {
-        GemmFull<double>(true, false, jb, n - j - jb, j, -1.0, At(a, lda, 0, j),
+        GemmFull<T>(true, false, jb, n - j - jb, j, T(-1), At(a, lda, 0, j),
                          lda, At(a, lda, 0, j + jb), lda, 1.0,
                          At(a, lda, j, j + jb), lda);
-        TrsmFull<double>(true, false, true, false, jb, n - j - jb, 1.0,
+        TrsmFull<T>(true, false, true, false, jb, n - j - jb, 1.0,
                          At(a, lda, j, j), lda, At(a, lda, j, j + jb), lda);
       }
     } else {
-      SyrkFull(true, false, jb, j, -1.0, At(a, lda, j, 0), lda, 1.0,
+      SyrkFull<T>(true, false, jb, j, T(-1), At(a, lda, j, 0), lda, 1.0,
                At(a, lda, j, j), lda);
-      Potrf2Rec(false, jb, At(a, lda, j, j), lda, info, j);
+      Potrf2Rec<T>(false, jb, At(a, lda, j, j), lda, info, j);
       if (j + jb < n) {
-        GemmFull<double>(false, true, n - j - jb, jb, j, -1.0,
+        GemmFull<T>(false, true, n - j - jb, jb, j, -1.0,
                          At(a, lda, j + jb, 0), lda, At(a, lda, j, 0), lda, 1.0,
                          At(a, lda, j + jb, j), lda);
-        TrsmFull<double>(false, true, true, false, n - j - jb, jb, 1.0,
+        TrsmFull<T>(false, true, true, false, n - j - jb, jb, 1.0,
                          At(a, lda, j, j), lda, At(a, lda, j + jb, j), lda);
       }
     }
@@ -175,18 +178,24 @@ void Potrf(bool upper, int n, double* a, int lda, int* info) {
   ctx.guard = saved;
 }
 
-void Potrs(bool upper, int n, int nrhs, const double* a, int lda, double* b,
-           int ldb) {
+template <typename T>
+void Potrs(bool upper, int n, int nrhs, const T* a, int lda, T* b, int ldb) {
   if (n == 0 || nrhs == 0) return;
   if (upper) {
-    TrsmFull<double>(true, false, true, false, n, nrhs, 1.0, a, lda, b, ldb);
-    TrsmFull<double>(true, false, false, false, n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmFull<T>(true, false, true, false, n, nrhs, T(1), a, lda, b, ldb);
+    TrsmFull<T>(true, false, false, false, n, nrhs, T(1), a, lda, b, ldb);
   } else {
-    TrsmFull<double>(true, true, false, false, n, nrhs, 1.0, a, lda, b, ldb);
-    TrsmFull<double>(true, true, true, false, n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmFull<T>(true, true, false, false, n, nrhs, T(1), a, lda, b, ldb);
+    TrsmFull<T>(true, true, true, false, n, nrhs, T(1), a, lda, b, ldb);
   }
 }
 
+template void Potrf2<double>(bool, int, double*, int, int*);
+template void Potrf2<float>(bool, int, float*, int, int*);
+template void Potrf<double>(bool, int, double*, int, int*);
+template void Potrf<float>(bool, int, float*, int, int*);
+template void Potrs<double>(bool, int, int, const double*, int, double*, int);
+template void Potrs<float>(bool, int, int, const float*, int, float*, int);
 template void Getrf2<double>(int, int, double*, int, int*, int*);
 template void Getrf2<float>(int, int, float*, int, int*, int*);
 template void Getrf<double>(int, int, double*, int, int*, int*);

@@ -264,6 +264,26 @@ void Gesv(int* n, int* r, double* a, int* lda, int* ipiv, double* b, int* ldb, i
 void Gesv(int* n, int* r, float* a, int* lda, int* ipiv, float* b, int* ldb, int* info) {
   sgesv_(n, r, a, lda, ipiv, b, ldb, info);
 }
+void Potrf(bool rec, const char* u, int* n, double* a, int* lda, int* info) {
+  (rec ? dpotrf2_ : dpotrf_)(u, n, a, lda, info);
+}
+void Potrf(bool rec, const char* u, int* n, float* a, int* lda, int* info) {
+  (rec ? spotrf2_ : spotrf_)(u, n, a, lda, info);
+}
+void Potrs(const char* u, int* n, int* r, const double* a, int* lda, double* b, int* ldb,
+           int* info) {
+  dpotrs_(u, n, r, a, lda, b, ldb, info);
+}
+void Potrs(const char* u, int* n, int* r, const float* a, int* lda, float* b, int* ldb,
+           int* info) {
+  spotrs_(u, n, r, a, lda, b, ldb, info);
+}
+void Posv(const char* u, int* n, int* r, double* a, int* lda, double* b, int* ldb, int* info) {
+  dposv_(u, n, r, a, lda, b, ldb, info);
+}
+void Posv(const char* u, int* n, int* r, float* a, int* lda, float* b, int* ldb, int* info) {
+  sposv_(u, n, r, a, lda, b, ldb, info);
+}
 
 }  // namespace
 }  // namespace hb
@@ -343,19 +363,21 @@ lapack_int GesvMain(int layout, int n, int nrhs, T* a, int lda, int* ipiv, T* b,
   return GesvWork(layout, n, nrhs, a, lda, ipiv, b, ldb);
 }
 
-lapack_int PotrfWork(int layout, char uplo, int n, double* a, int lda, bool rec) {
-  const Arg<double> args[1] = {{a, n, n, lda, -5, true, true}};
-  return CallWork(layout, Name<double>(rec ? "potrf2_work" : "potrf_work"), args,
-                  [&](double** p, int* ld) {
+template <typename T>
+lapack_int PotrfWork(int layout, char uplo, int n, T* a, int lda, bool rec) {
+  const Arg<T> args[1] = {{a, n, n, lda, -5, true, true}};
+  return CallWork(layout, Name<T>(rec ? "potrf2_work" : "potrf_work"), args,
+                  [&](T** p, int* ld) {
                     int info = 0;
-                    (rec ? dpotrf2_ : dpotrf_)(&uplo, &n, p[0], &ld[0], &info);
+                    Potrf(rec, &uplo, &n, p[0], &ld[0], &info);
                     return info;
                   });
 }
 
-lapack_int PotrfMain(int layout, char uplo, int n, double* a, int lda, bool rec) {
+template <typename T>
+lapack_int PotrfMain(int layout, char uplo, int n, T* a, int lda, bool rec) {
   if (layout != LAPACK_ROW_MAJOR && layout != LAPACK_COL_MAJOR) {
-    LAPACKE_xerbla(Name<double>(rec ? "potrf2" : "potrf").c_str(), -1);
+    LAPACKE_xerbla(Name<T>(rec ? "potrf2" : "potrf").c_str(), -1);
     return -1;
   }
   if (NanCheck() && HasNanPo(layout, uplo, n, a, lda)) return -4;
@@ -363,25 +385,27 @@ lapack_int PotrfMain(int layout, char uplo, int n, double* a, int lda, bool rec)
 }
 
 // xPOTRS reads A (a triangle) and updates B; xPOSV updates both.
-lapack_int PosWork(int layout, char uplo, int n, int nrhs, double* a, int lda, double* b,
-                   int ldb, bool solve_only) {
-  const Arg<double> args[2] = {{a, n, n, lda, -6, true, !solve_only},
-                               {b, n, nrhs, ldb, -8, true, true}};
-  return CallWork(layout, Name<double>(solve_only ? "potrs_work" : "posv_work"), args,
-                  [&](double** p, int* ld) {
+template <typename T>
+lapack_int PosWork(int layout, char uplo, int n, int nrhs, T* a, int lda, T* b, int ldb,
+                   bool solve_only) {
+  const Arg<T> args[2] = {{a, n, n, lda, -6, true, !solve_only},
+                          {b, n, nrhs, ldb, -8, true, true}};
+  return CallWork(layout, Name<T>(solve_only ? "potrs_work" : "posv_work"), args,
+                  [&](T** p, int* ld) {
                     int info = 0;
                     if (solve_only)
-                      dpotrs_(&uplo, &n, &nrhs, p[0], &ld[0], p[1], &ld[1], &info);
+                      Potrs(&uplo, &n, &nrhs, p[0], &ld[0], p[1], &ld[1], &info);
                     else
-                      dposv_(&uplo, &n, &nrhs, p[0], &ld[0], p[1], &ld[1], &info);
+                      Posv(&uplo, &n, &nrhs, p[0], &ld[0], p[1], &ld[1], &info);
                     return info;
                   });
 }
 
-lapack_int PosMain(int layout, char uplo, int n, int nrhs, double* a, int lda, double* b,
-                   int ldb, bool solve_only) {
+template <typename T>
+lapack_int PosMain(int layout, char uplo, int n, int nrhs, T* a, int lda, T* b, int ldb,
+                   bool solve_only) {
   if (layout != LAPACK_ROW_MAJOR && layout != LAPACK_COL_MAJOR) {
-    LAPACKE_xerbla(Name<double>(solve_only ? "potrs" : "posv").c_str(), -1);
+    LAPACKE_xerbla(Name<T>(solve_only ? "potrs" : "posv").c_str(), -1);
     return -1;
   }
   if (NanCheck()) {
@@ -466,40 +490,46 @@ HB_LAPACKE_LU(d, double)
 HB_LAPACKE_LU(s, float)
 #undef HB_LAPACKE_LU
 
-HWYBLAS_API lapack_int LAPACKE_dpotrf(int layout, char uplo, lapack_int n, double* a,
-                                      lapack_int lda) {
-  return hb::PotrfMain(layout, uplo, n, a, lda, false);
-}
-HWYBLAS_API lapack_int LAPACKE_dpotrf_work(int layout, char uplo, lapack_int n, double* a,
-                                           lapack_int lda) {
-  return hb::PotrfWork(layout, uplo, n, a, lda, false);
-}
-HWYBLAS_API lapack_int LAPACKE_dpotrf2(int layout, char uplo, lapack_int n, double* a,
-                                       lapack_int lda) {
-  return hb::PotrfMain(layout, uplo, n, a, lda, true);
-}
-HWYBLAS_API lapack_int LAPACKE_dpotrf2_work(int layout, char uplo, lapack_int n, double* a,
-                                            lapack_int lda) {
-  return hb::PotrfWork(layout, uplo, n, a, lda, true);
-}
-HWYBLAS_API lapack_int LAPACKE_dpotrs(int layout, char uplo, lapack_int n, lapack_int nrhs,
-                                      const double* a, lapack_int lda, double* b,
-                                      lapack_int ldb) {
-  return hb::PosMain(layout, uplo, n, nrhs, const_cast<double*>(a), lda, b, ldb, true);
-}
-HWYBLAS_API lapack_int LAPACKE_dpotrs_work(int layout, char uplo, lapack_int n,
-                                           lapack_int nrhs, const double* a, lapack_int lda,
-                                           double* b, lapack_int ldb) {
-  return hb::PosWork(layout, uplo, n, nrhs, const_cast<double*>(a), lda, b, ldb, true);
-}
-HWYBLAS_API lapack_int LAPACKE_dposv(int layout, char uplo, lapack_int n, lapack_int nrhs,
-                                     double* a, lapack_int lda, double* b, lapack_int ldb) {
-  return hb::PosMain(layout, uplo, n, nrhs, a, lda, b, ldb, false);
-}
-HWYBLAS_API lapack_int LAPACKE_dposv_work(int layout, char uplo, lapack_int n,
-                                          lapack_int nrhs, double* a, lapack_int lda,
-                                          double* b, lapack_int ldb) {
-  return hb::PosWork(layout, uplo, n, nrhs, a, lda, b, ldb, false);
-}
+#define HB_LAPACKE_PO(p, T)                                                           \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrf(int layout, char uplo, lapack_int n, T* a, \
+                                            lapack_int lda) {                         \
+    return hb::PotrfMain<T>(layout, uplo, n, a, lda, false);                          \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrf_work(int layout, char uplo, lapack_int n, \
+                                                 T* a, lapack_int lda) {              \
+    return hb::PotrfWork<T>(layout, uplo, n, a, lda, false);                          \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrf2(int layout, char uplo, lapack_int n,     \
+                                             T* a, lapack_int lda) {                  \
+    return hb::PotrfMain<T>(layout, uplo, n, a, lda, true);                           \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrf2_work(int layout, char uplo, lapack_int n, \
+                                                  T* a, lapack_int lda) {             \
+    return hb::PotrfWork<T>(layout, uplo, n, a, lda, true);                           \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrs(int layout, char uplo, lapack_int n,      \
+                                            lapack_int nrhs, const T* a,              \
+                                            lapack_int lda, T* b, lapack_int ldb) {   \
+    return hb::PosMain<T>(layout, uplo, n, nrhs, const_cast<T*>(a), lda, b, ldb, true); \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##potrs_work(int layout, char uplo, lapack_int n, \
+                                                 lapack_int nrhs, const T* a,         \
+                                                 lapack_int lda, T* b, lapack_int ldb) { \
+    return hb::PosWork<T>(layout, uplo, n, nrhs, const_cast<T*>(a), lda, b, ldb, true); \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##posv(int layout, char uplo, lapack_int n,       \
+                                           lapack_int nrhs, T* a, lapack_int lda,     \
+                                           T* b, lapack_int ldb) {                    \
+    return hb::PosMain<T>(layout, uplo, n, nrhs, a, lda, b, ldb, false);              \
+  }                                                                                   \
+  HWYBLAS_API lapack_int LAPACKE_##p##posv_work(int layout, char uplo, lapack_int n,  \
+                                                lapack_int nrhs, T* a, lapack_int lda, \
+                                                T* b, lapack_int ldb) {               \
+    return hb::PosWork<T>(layout, uplo, n, nrhs, a, lda, b, ldb, false);              \
+  }
+
+HB_LAPACKE_PO(d, double)
+HB_LAPACKE_PO(s, float)
+#undef HB_LAPACKE_PO
 
 }  // extern "C"

@@ -16,13 +16,21 @@ namespace {
 // a sequential FFMA chain over k restarted every 384 (src/gemm_kernel-inl.h:72).
 constexpr int kSB = 64, kSK = 16;
 
+// `part` restricts C to one triangle (SYRK): elements outside it are neither
+// computed nor written; inside, the chain is the one of the full GEMM.
+__device__ __forceinline__ bool InPart(int part, int i, int j) {
+  return part == kAll || (part == kLower ? i >= j : i <= j);
+}
+
 __global__ void __launch_bounds__(256)
     SgemmKernel(int m, int n, int k, float alpha, View<float> a, View<float> b,
-                float beta, float* c, long long ldc, const int* guard) {
+                float beta, float* c, long long ldc, int part, const int* guard) {
   if (guard != nullptr && *guard != 0) return;
   __shared__ float sa[kSK][kSB + 4];
   __shared__ float sb[kSK][kSB + 4];
   const int m0 = blockIdx.x * kSB, n0 = blockIdx.y * kSB;
+  // A tile wholly outside the triangle has nothing to do.
+  if ((part == kLower && m0 + kSB - 1 < n0) || (part == kUpper && m0 > n0 + kSB - 1)) return;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   float acc[4][4] = {}, cacc[4][4] = {};
   const int kchunk = 384;
@@ -56,7 +64,7 @@ __global__ void __launch_bounds__(256)
             const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
             const float rr = alpha * acc[r][q];
             if (first) {
-              if (i < m && j < n) {
+              if (i < m && j < n && InPart(part, i, j)) {
                 if (beta == 0.f) {
                   cacc[r][q] = rr;
                 } else {
@@ -78,7 +86,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
-      if (i < m && j < n) c[i + j * ldc] = cacc[r][q];
+      if (i < m && j < n && InPart(part, i, j)) c[i + j * ldc] = cacc[r][q];
     }
 }
 
@@ -165,7 +173,7 @@ void LaunchGemm<double>(int m, int n, int k, double alpha, View<double> a,
 template <>
 void LaunchGemm<float>(int m, int n, int k, float alpha, View<float> a,
                        View<float> b, float beta, float* c, int ldc) {
-  Sgemm(m, n, k, alpha, a, b, beta, c, ldc);
+  Sgemm(m, n, k, alpha, a, b, beta, c, ldc, kAll);
 }
 
 // TrsmRecursive (src/trsm.cc:87-135): split at max(32, (r/2)/32*32).
@@ -212,10 +220,10 @@ void TrsmRec(bool left, View<T> tri, bool lower, bool unit, int r, int other,
 }  // namespace
 
 void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
-           float beta, float* c, int ldc) {
+           float beta, float* c, int ldc, Part part) {
   const dim3 grid((m + kSB - 1) / kSB, (n + kSB - 1) / kSB);
   SgemmKernel<<<grid, 256, 0, Ctx().stream>>>(m, n, k, alpha, a, b, beta, c,
-                                              ldc, Ctx().guard);
+                                              ldc, static_cast<int>(part), Ctx().guard);
   CountLaunch();
   LaunchFailed("sgemm");
 }
@@ -269,19 +277,30 @@ template void TrsmFull<double>(bool, bool, bool, bool, int, int, double,
 template void TrsmFull<float>(bool, bool, bool, bool, int, int, float,
                               const float*, int, float*, int);
 
-// Syrk (src/level3.cc:84-139), real: C := alpha*op(A)*op(A)^T + beta*C on one
-// triangle, as a GEMM with a triangular C part.
-void SyrkFull(bool lower, bool trans, int n, int k, double alpha,
-              const double* a, int lda, double beta, double* c, int ldc) {
+// Syrk (src/level3.cc:84-139; ssyrk_/dsyrk_ 410-421), real: C :=
+// alpha*op(A)*op(A)^T + beta*C on one triangle, as a GEMM with a triangular C
+// part (DMMA for double, the FP32 kernel for float).
+template <typename T>
+void SyrkFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda, T beta,
+              T* c, int ldc) {
   const Part part = lower ? kLower : kUpper;
-  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return;
-  if (alpha == 0.0 || k == 0) {
-    ScaleMatrix<double>(n, n, beta, c, ldc, part);
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
     return;
   }
-  Dgemm(n, n, k, alpha, ColMajor<double>(a, lda, trans),
-        ColMajor<double>(a, lda, !trans), beta, c, ldc, part);
+  if constexpr (sizeof(T) == 8) {
+    Dgemm(n, n, k, alpha, ColMajor<T>(a, lda, trans), ColMajor<T>(a, lda, !trans), beta, c,
+          ldc, part);
+  } else {
+    Sgemm(n, n, k, alpha, ColMajor<T>(a, lda, trans), ColMajor<T>(a, lda, !trans), beta, c,
+          ldc, part);
+  }
 }
+template void SyrkFull<double>(bool, bool, int, int, double, const double*, int, double,
+                               double*, int);
+template void SyrkFull<float>(bool, bool, int, int, float, const float*, int, float, float*,
+                              int);
 
 // Gemm (src/gemm.cc:114-131) after argument checks.
 template <typename T>

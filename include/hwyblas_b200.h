@@ -77,6 +77,12 @@ HWYBLAS_API void dsyrk_(const char* uplo, const char* trans,
                         const double* alpha, const double* a,
                         const hwyblas_int* lda, const double* beta, double* c,
                         const hwyblas_int* ldc);
+/* Single precision (include/hwyblas/hwyblas.h:632, src/level3.cc:410-415). */
+HWYBLAS_API void ssyrk_(const char* uplo, const char* trans,
+                        const hwyblas_int* n, const hwyblas_int* k,
+                        const float* alpha, const float* a,
+                        const hwyblas_int* lda, const float* beta, float* c,
+                        const hwyblas_int* ldc);
 /* 1-based index of the first element of largest |x| (0 if n < 1 or
  * incx <= 0). Replaces idamax_ (include/hwyblas/hwyblas.h:169,
  * src/level1.cc:895-897). */
@@ -161,6 +167,22 @@ HWYBLAS_API void dpotrs_(const char* uplo, const hwyblas_int* n,
 HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n,
                         const hwyblas_int* nrhs, double* a,
                         const hwyblas_int* lda, double* b,
+                        const hwyblas_int* ldb, hwyblas_int* info);
+
+/* Single-precision Cholesky family: one template for s and d in the
+ * reference (src/lapack/potrf.cc:747-773, posv.cc; include/hwyblas/lapack.h:
+ * 661, 669, 722, 742); same algorithms at float. */
+HWYBLAS_API void spotrf_(const char* uplo, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void spotrf2_(const char* uplo, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void spotrs_(const char* uplo, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const float* a,
+                         const hwyblas_int* lda, float* b,
+                         const hwyblas_int* ldb, hwyblas_int* info);
+HWYBLAS_API void sposv_(const char* uplo, const hwyblas_int* n,
+                        const hwyblas_int* nrhs, float* a,
+                        const hwyblas_int* lda, float* b,
                         const hwyblas_int* ldb, hwyblas_int* info);
 
 /* ------------------------------------------------------------------------ */
@@ -254,6 +276,26 @@ HWYBLAS_API lapack_int LAPACKE_dposv(int matrix_layout, char uplo, lapack_int n,
 HWYBLAS_API lapack_int LAPACKE_dposv_work(int matrix_layout, char uplo, lapack_int n,
                                           lapack_int nrhs, double* a, lapack_int lda,
                                           double* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_spotrf(int matrix_layout, char uplo, lapack_int n,
+                                      float* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_spotrf_work(int matrix_layout, char uplo, lapack_int n,
+                                           float* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_spotrf2(int matrix_layout, char uplo, lapack_int n,
+                                       float* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_spotrf2_work(int matrix_layout, char uplo, lapack_int n,
+                                            float* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_spotrs(int matrix_layout, char uplo, lapack_int n,
+                                      lapack_int nrhs, const float* a, lapack_int lda,
+                                      float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_spotrs_work(int matrix_layout, char uplo, lapack_int n,
+                                           lapack_int nrhs, const float* a,
+                                           lapack_int lda, float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sposv(int matrix_layout, char uplo, lapack_int n,
+                                     lapack_int nrhs, float* a, lapack_int lda,
+                                     float* b, lapack_int ldb);
+HWYBLAS_API lapack_int LAPACKE_sposv_work(int matrix_layout, char uplo, lapack_int n,
+                                          lapack_int nrhs, float* a, lapack_int lda,
+                                          float* b, lapack_int ldb);
 
 /* ------------------------------------------------------------------------ */
 /* CBLAS (include/hwyblas/cblas.h:20-45)                                    */

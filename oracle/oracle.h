@@ -36,6 +36,8 @@ int orc_dtrsm(char side, char uplo, char transa, char diag, int m, int n,
               double alpha, const double* a, int lda, double* b, int ldb);
 int orc_strsm(char side, char uplo, char transa, char diag, int m, int n,
               float alpha, const float* a, int lda, float* b, int ldb);
+int orc_ssyrk(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+              float beta, float* c, int ldc);
 int orc_dsyrk(char uplo, char trans, int n, int k, double alpha,
               const double* a, int lda, double beta, double* c, int ldc);
 int orc_idamax(int n, const double* x, int incx);
@@ -60,6 +62,10 @@ int orc_dpotrf(char uplo, int n, double* a, int lda);
 int orc_dpotrf2(char uplo, int n, double* a, int lda);
 int orc_dpotrs(char uplo, int n, int nrhs, const double* a, int lda, double* b,
                int ldb);
+int orc_spotrf(char uplo, int n, float* a, int lda);
+int orc_spotrf2(char uplo, int n, float* a, int lda);
+int orc_spotrs(char uplo, int n, int nrhs, const float* a, int lda, float* b, int ldb);
+int orc_sposv(char uplo, int n, int nrhs, float* a, int lda, float* b, int ldb);
 int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
               int ldb);
 

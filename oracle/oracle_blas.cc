@@ -398,9 +398,11 @@ int TrsmF(char side, char uplo, char transa, char diag, int m, int n, T alpha,
 }
 
 // ---------------------------------------------------------------------------
-// SYRK (src/level3.cc:84-139), real only.
-int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a,
-          int lda, double beta, double* c, int ldc) {
+// SYRK (src/level3.cc:84-139), real only; the reference's ssyrk_/dsyrk_
+// (level3.cc:410-421) are the same template at float and double.
+template <typename T>
+int Syrk(char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T beta, T* c,
+         int ldc) {
   const char u = Up(uplo);
   bool t;
   const bool vu = (u == 'L' || u == 'U');
@@ -415,14 +417,20 @@ int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a,
   else if (ldc < std::max(1, n)) info = 10;
   if (info) return info;
   const Part part = (u == 'L') ? kLower : kUpper;
-  if (n == 0 || ((alpha == 0.0 || k == 0) && beta == 1.0)) return 0;
-  if (alpha == 0.0 || k == 0) {
-    ScaleMatrix<double>(n, n, beta, c, ldc, part);
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return 0;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
     return 0;
   }
-  Gemm<double>(n, n, k, alpha, General(t, a, lda), General(!t, a, lda), beta,
-               c, ldc, part);
+  Gemm<T>(n, n, k, alpha, General(t, a, lda), General(!t, a, lda), beta, c, ldc, part);
   return 0;
+}
+template int Syrk<double>(char, char, int, int, double, const double*, int, double, double*,
+                          int);
+template int Syrk<float>(char, char, int, int, float, const float*, int, float, float*, int);
+int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+          double beta, double* c, int ldc) {
+  return Syrk<double>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
 }
 
 // ---------------------------------------------------------------------------
@@ -493,6 +501,10 @@ int orc_strsm(char side, char uplo, char transa, char diag, int m, int n,
 int orc_dsyrk(char uplo, char trans, int n, int k, double alpha,
               const double* a, int lda, double beta, double* c, int ldc) {
   return orc::SyrkD(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int orc_ssyrk(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+              float beta, float* c, int ldc) {
+  return orc::Syrk<float>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
 }
 int orc_idamax(int n, const double* x, int incx) {
   return orc::Iamax<double>(n, x, incx);

@@ -38,6 +38,9 @@ int TrsmF(char side, char uplo, char transa, char diag, int m, int n, T alpha,
 int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a,
           int lda, double beta, double* c, int ldc);
 template <typename T>
+int Syrk(char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T beta, T* c,
+         int ldc);
+template <typename T>
 int Iamax(int n, const T* x, int incx);
 
 template <typename T>

@@ -208,31 +208,33 @@ int Getrs(char trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
   return 0;
 }
 
-int Potrf2D(char uplo, int n, double* a, int lda) {
+template <typename T>
+int Potrf2(char uplo, int n, T* a, int lda) {
   const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
   const bool upper = (u == 'U');
   if (!upper && u != 'L') return -1;
   if (n < 0) return -2;
   if (lda < std::max(1, n)) return -4;
   if (n == 0) return 0;
-  if (n <= 32) return PotrfLeaf<double>(upper, n, a, lda);
+  if (n <= 32) return PotrfLeaf<T>(upper, n, a, lda);
   const int n1 = n / 2, n2 = n - n1;
   const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
-  int iinfo = Potrf2D(uplo, n1, a, lda);
+  int iinfo = Potrf2<T>(uplo, n1, a, lda);
   if (iinfo != 0) return iinfo;
   if (upper) {
-    TrsmF<double>('L', 'U', 'C', 'N', n1, n2, 1.0, a, lda, A(0, n1), lda);
-    SyrkD('U', 'C', n2, n1, -1.0, A(0, n1), lda, 1.0, A(n1, n1), lda);
+    TrsmF<T>('L', 'U', 'C', 'N', n1, n2, T(1), a, lda, A(0, n1), lda);
+    Syrk<T>('U', 'C', n2, n1, T(-1), A(0, n1), lda, T(1), A(n1, n1), lda);
   } else {
-    TrsmF<double>('R', 'L', 'C', 'N', n2, n1, 1.0, a, lda, A(n1, 0), lda);
-    SyrkD('L', 'N', n2, n1, -1.0, A(n1, 0), lda, 1.0, A(n1, n1), lda);
+    TrsmF<T>('R', 'L', 'C', 'N', n2, n1, T(1), a, lda, A(n1, 0), lda);
+    Syrk<T>('L', 'N', n2, n1, T(-1), A(n1, 0), lda, T(1), A(n1, n1), lda);
   }
-  iinfo = Potrf2D(uplo, n2, A(n1, n1), lda);
+  iinfo = Potrf2<T>(uplo, n2, A(n1, n1), lda);
   if (iinfo != 0) return iinfo + n1;
   return 0;
 }
 
-int PotrfD(char uplo, int n, double* a, int lda) {
+template <typename T>
+int Potrf(char uplo, int n, T* a, int lda) {
   const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
   const bool upper = (u == 'U');
   if (!upper && u != 'L') return -1;
@@ -240,28 +242,28 @@ int PotrfD(char uplo, int n, double* a, int lda) {
   if (lda < std::max(1, n)) return -4;
   if (n == 0) return 0;
   const int nb = 64;
-  if (nb >= n) return Potrf2D(uplo, n, a, lda);
+  if (nb >= n) return Potrf2<T>(uplo, n, a, lda);
   const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
     if (upper) {
-      SyrkD('U', 'C', jb, j, -1.0, A(0, j), lda, 1.0, A(j, j), lda);
-      const int info = Potrf2D('U', jb, A(j, j), lda);
+      Syrk<T>('U', 'C', jb, j, T(-1), A(0, j), lda, T(1), A(j, j), lda);
+      const int info = Potrf2<T>('U', jb, A(j, j), lda);
       if (info != 0) return info + j;
       if (j + jb < n) {
-        GemmF<double>('C', 'N', jb, n - j - jb, j, -1.0, A(0, j), lda,
-                      A(0, j + jb), lda, 1.0, A(j, j + jb), lda);
-        TrsmF<double>('L', 'U', 'C', 'N', jb, n - j - jb, 1.0, A(j, j), lda,
+        GemmF<T>('C', 'N', jb, n - j - jb, j, T(-1), A(0, j), lda,
+                      A(0, j + jb), lda, T(1), A(j, j + jb), lda);
+        TrsmF<T>('L', 'U', 'C', 'N', jb, n - j - jb, T(1), A(j, j), lda,
                       A(j, j + jb), lda);
       }
     } else {
-      SyrkD('L', 'N', jb, j, -1.0, A(j, 0), lda, 1.0, A(j, j), lda);
-      const int info = Potrf2D('L', jb, A(j, j), lda);
+      Syrk<T>('L', 'N', jb, j, T(-1), A(j, 0), lda, T(1), A(j, j), lda);
+      const int info = Potrf2<T>('L', jb, A(j, j), lda);
       if (info != 0) return info + j;
       if (j + jb < n) {
-        GemmF<double>('N', 'C', n - j - jb, jb, j, -1.0, A(j + jb, 0), lda,
-                      A(j, 0), lda, 1.0, A(j + jb, j), lda);
-        TrsmF<double>('R', 'L', 'C', 'N', n - j - jb, jb, 1.0, A(j, j), lda,
+        GemmF<T>('N', 'C', n - j - jb, jb, j, T(-1), A(j + jb, 0), lda,
+                      A(j, 0), lda, T(1), A(j + jb, j), lda);
+        TrsmF<T>('R', 'L', 'C', 'N', n - j - jb, jb, T(1), A(j, j), lda,
                       A(j + jb, j), lda);
       }
     }
@@ -269,8 +271,8 @@ int PotrfD(char uplo, int n, double* a, int lda) {
   return 0;
 }
 
-int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b,
-           int ldb) {
+template <typename T>
+int Potrs(char uplo, int n, int nrhs, const T* a, int lda, T* b, int ldb) {
   const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
   const bool upper = (u == 'U');
   if (!upper && u != 'L') return -1;
@@ -280,13 +282,19 @@ int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b,
   if (ldb < std::max(1, n)) return -7;
   if (n == 0 || nrhs == 0) return 0;
   if (upper) {
-    TrsmF<double>('L', 'U', 'C', 'N', n, nrhs, 1.0, a, lda, b, ldb);
-    TrsmF<double>('L', 'U', 'N', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmF<T>('L', 'U', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmF<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
   } else {
-    TrsmF<double>('L', 'L', 'N', 'N', n, nrhs, 1.0, a, lda, b, ldb);
-    TrsmF<double>('L', 'L', 'C', 'N', n, nrhs, 1.0, a, lda, b, ldb);
+    TrsmF<T>('L', 'L', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmF<T>('L', 'L', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
   }
   return 0;
+}
+
+int PotrfD(char uplo, int n, double* a, int lda) { return Potrf<double>(uplo, n, a, lda); }
+int Potrf2D(char uplo, int n, double* a, int lda) { return Potrf2<double>(uplo, n, a, lda); }
+int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b, int ldb) {
+  return Potrs<double>(uplo, n, nrhs, a, lda, b, ldb);
 }
 
 template int GetrfLeaf<double>(int, int, double*, int, int*);
@@ -354,6 +362,28 @@ int orc_dpotrf2(char uplo, int n, double* a, int lda) {
 int orc_dpotrs(char uplo, int n, int nrhs, const double* a, int lda, double* b,
                int ldb) {
   return orc::PotrsD(uplo, n, nrhs, a, lda, b, ldb);
+}
+/* The reference's s-prefixed Cholesky family is the same template at float
+ * (src/lapack/potrf.cc:747-773, posv.cc). */
+int orc_spotrf(char uplo, int n, float* a, int lda) {
+  return orc::Potrf<float>(uplo, n, a, lda);
+}
+int orc_spotrf2(char uplo, int n, float* a, int lda) {
+  return orc::Potrf2<float>(uplo, n, a, lda);
+}
+int orc_spotrs(char uplo, int n, int nrhs, const float* a, int lda, float* b, int ldb) {
+  return orc::Potrs<float>(uplo, n, nrhs, a, lda, b, ldb);
+}
+int orc_sposv(char uplo, int n, int nrhs, float* a, int lda, float* b, int ldb) {
+  const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;
+  if (u != 'U' && u != 'L') return -1;
+  if (n < 0) return -2;
+  if (nrhs < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (ldb < std::max(1, n)) return -7;
+  int info = orc::Potrf<float>(uplo, n, a, lda);
+  if (info == 0) info = orc::Potrs<float>(uplo, n, nrhs, a, lda, b, ldb);
+  return info;
 }
 int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
               int ldb) {

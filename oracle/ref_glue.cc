@@ -118,6 +118,12 @@ void dsyrk_(const char* u, const char* t, const blasint* n, const blasint* k,
   const int info = orc::SyrkD(*u, *t, *n, *k, *alpha, a, *lda, *beta, c, *ldc);
   if (info) hwyblas::ReportError("DSYRK", info);
 }
+void ssyrk_(const char* u, const char* t, const blasint* n, const blasint* k,
+            const float* alpha, const float* a, const blasint* lda, const float* beta,
+            float* c, const blasint* ldc) {
+  const int info = orc::Syrk<float>(*u, *t, *n, *k, *alpha, a, *lda, *beta, c, *ldc);
+  if (info) hwyblas::ReportError("SSYRK", info);
+}
 blasint idamax_(const blasint* n, const double* x, const blasint* incx) {
   return orc::Iamax<double>(*n, x, *incx);
 }

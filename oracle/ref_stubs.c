@@ -9,7 +9,7 @@
     abort();                                                            \
   }
 ORC_STUB(dswap_) ORC_STUB(sswap_) ORC_STUB(ddot_) ORC_STUB(sdot_)
-ORC_STUB(dgemv_) ORC_STUB(sgemv_) ORC_STUB(ssyrk_) ORC_STUB(cdotc_)
+ORC_STUB(dgemv_) ORC_STUB(sgemv_) ORC_STUB(cdotc_)
 ORC_STUB(cgemm_) ORC_STUB(cgemv_) ORC_STUB(cherk_) ORC_STUB(cscal_)
 ORC_STUB(csscal_) ORC_STUB(cswap_) ORC_STUB(ctrsm_) ORC_STUB(icamax_)
 ORC_STUB(izamax_) ORC_STUB(zdotc_) ORC_STUB(zdscal_) ORC_STUB(zgemm_)

@@ -42,6 +42,8 @@ def load_ref():
     lib.sgetrf_.argtypes = [P] * 6
     lib.sgetrf2_.argtypes = [P] * 6
     lib.sgesv_.argtypes = [P] * 8
+    lib.spotrf_.argtypes = [P] * 5
+    lib.spotrf2_.argtypes = [P] * 5
     return lib
 
 
@@ -79,6 +81,11 @@ class Oracle:
         L.orc_dpotrf2.argtypes = [CH, I, P, I]
         L.orc_dpotrs.argtypes = [CH, I, I, P, I, P, I]
         L.orc_dposv.argtypes = [CH, I, I, P, I, P, I]
+        L.orc_spotrf.argtypes = [CH, I, P, I]
+        L.orc_spotrf2.argtypes = [CH, I, P, I]
+        L.orc_spotrs.argtypes = [CH, I, I, P, I, P, I]
+        L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
+        L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
         L.orc_set_lanes(8)
 
     def set_threads(self, n):
@@ -146,6 +153,22 @@ class Oracle:
     def dpotrs(self, uplo, n, nrhs, a, lda, b, ldb):
         return self.lib.orc_dpotrs(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
 
+    def spotrf(self, uplo, n, a, lda):
+        return self.lib.orc_spotrf(_b(uplo), n, ptr(a), lda)
+
+    def spotrf2(self, uplo, n, a, lda):
+        return self.lib.orc_spotrf2(_b(uplo), n, ptr(a), lda)
+
+    def spotrs(self, uplo, n, nrhs, a, lda, b, ldb):
+        return self.lib.orc_spotrs(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
+
+    def sposv(self, uplo, n, nrhs, a, lda, b, ldb):
+        return self.lib.orc_sposv(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
+
+    def ssyrk(self, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+        return self.lib.orc_ssyrk(_b(uplo), _b(trans), n, k, alpha, ptr(a), lda, beta,
+                                  ptr(c), ldc)
+
     def dposv(self, uplo, n, nrhs, a, lda, b, ldb):
         return self.lib.orc_dposv(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
 
@@ -175,7 +198,10 @@ def ref_call_potrf(lib, recursive, uplo, n, a, lda):
     info = ctypes.c_int(0)
     args = [ctypes.c_char_p(_b(uplo)), ctypes.byref(ctypes.c_int(n)), ptr(a),
             ctypes.byref(ctypes.c_int(lda)), ctypes.byref(info)]
-    (lib.dpotrf2_ if recursive else lib.dpotrf_)(*args)
+    if a.dtype == np.float32:
+        (lib.spotrf2_ if recursive else lib.spotrf_)(*args)
+    else:
+        (lib.dpotrf2_ if recursive else lib.dpotrf_)(*args)
     return info.value
 
 

@@ -116,36 +116,38 @@ def test_getrs_gesv_layouts(hb, orc, prec, layout, trans):
                      np.ascontiguousarray(x2))
 
 
+@pytest.mark.parametrize("prec", ["d", "s"])
 @pytest.mark.parametrize("layout", [ROW, COL])
 @pytest.mark.parametrize("uplo", ["U", "L"])
 @pytest.mark.parametrize("recursive", [False, True])
-def test_potrf_potrs_posv_layouts(hb, orc, layout, uplo, recursive):
+def test_potrf_potrs_posv_layouts(hb, orc, prec, layout, uplo, recursive):
+    dt = np.float64 if prec == "d" else np.float32
     rng = np.random.default_rng(8)
     n, nrhs = 130, 6
-    a = spd(rng, n)
-    b = rand(rng, n, nrhs)
+    a = (spd(rng, n) + (0.1 * np.eye(n) if prec == "s" else 0)).astype(dt)
+    b = rand(rng, n, nrhs, dt)
     lda, ldb = n + 2, (nrhs if layout == ROW else n) + 1
     abuf = store(a, layout, lda)
-    fn = getattr(hb.lib(), "LAPACKE_dpotrf2" if recursive else "LAPACKE_dpotrf")
+    fn = getattr(hb.lib(), f"LAPACKE_{prec}potrf2" if recursive else f"LAPACKE_{prec}potrf")
     assert fn(layout, uplo.encode(), n, ptr(abuf), lda) == 0
     f = np.asfortranarray(a.copy())
-    assert (orc.dpotrf2 if recursive else orc.dpotrf)(uplo, n, f, n) == 0
+    assert getattr(orc, f"{prec}potrf2" if recursive else f"{prec}potrf")(uplo, n, f, n) == 0
     got = np.ascontiguousarray(load(abuf, layout, n, n, lda))
     assert same_bits(got, np.ascontiguousarray(f)), first_diff(got, f)
     # potrs with those factors
     bbuf = store(b, layout, ldb)
-    assert hb.lib().LAPACKE_dpotrs(layout, uplo.encode(), n, nrhs, ptr(abuf), lda, ptr(bbuf),
-                                   ldb) == 0
+    assert getattr(hb.lib(), f"LAPACKE_{prec}potrs")(layout, uplo.encode(), n, nrhs, ptr(abuf),
+                                                      lda, ptr(bbuf), ldb) == 0
     x = np.asfortranarray(b.copy())
-    assert orc.dpotrs(uplo, n, nrhs, f, n, x, n) == 0
+    assert getattr(orc, f"{prec}potrs")(uplo, n, nrhs, f, n, x, n) == 0
     assert same_bits(np.ascontiguousarray(load(bbuf, layout, n, nrhs, ldb)),
                      np.ascontiguousarray(x))
     # posv
     abuf, bbuf = store(a, layout, lda), store(b, layout, ldb)
-    assert hb.lib().LAPACKE_dposv(layout, uplo.encode(), n, nrhs, ptr(abuf), lda, ptr(bbuf),
-                                  ldb) == 0
+    assert getattr(hb.lib(), f"LAPACKE_{prec}posv")(layout, uplo.encode(), n, nrhs, ptr(abuf),
+                                                     lda, ptr(bbuf), ldb) == 0
     a2, x2 = np.asfortranarray(a.copy()), np.asfortranarray(b.copy())
-    assert orc.dposv(uplo, n, nrhs, a2, n, x2, n) == 0
+    assert getattr(orc, f"{prec}posv")(uplo, n, nrhs, a2, n, x2, n) == 0
     assert same_bits(np.ascontiguousarray(load(abuf, layout, n, n, lda)),
                      np.ascontiguousarray(a2))
     assert same_bits(np.ascontiguousarray(load(bbuf, layout, n, nrhs, ldb)),

@@ -100,6 +100,20 @@ def test_potrf_matches_reference_driver(orc, ref_drivers, recursive, uplo, n):
     assert same_bits(a1, a2), first_diff(a1, a2)
 
 
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 64, 65, 100, 200])
+def test_spotrf_matches_reference_driver(orc, ref_drivers, recursive, uplo, n):
+    """The single-precision Cholesky: the reference's potrf.cc at float (with
+    the oracle's float SYRK, TRSM, GEMM and leaf) against the restatement."""
+    rng = np.random.default_rng(n + 99)
+    a = spd(rng, n).astype(np.float32)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    f = orc.spotrf2 if recursive else orc.spotrf
+    assert f(uplo, n, a1, n) == ref_call_potrf(ref_drivers, recursive, uplo, n, a2, n)
+    assert same_bits(a1, a2), first_diff(a1, a2)
+
+
 def test_getrf_singular_matches_reference_driver(orc, ref_drivers):
     rng = np.random.default_rng(5)
     m, n = 90, 80
@@ -335,6 +349,32 @@ def test_strsm_residual_bound(orc, side, uplo, trans, diag, m):
     scale = (np.abs(op) @ np.abs(X)) if side == "L" else (np.abs(X) @ np.abs(op))
     scale = scale + abs(float(alpha)) * np.abs(b) + np.finfo(np.float32).tiny
     assert np.all(res <= 8 * (ka + 2) * np.finfo(np.float32).eps / 2 * scale)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_syrk_elementwise_bound(orc, dtype, uplo, trans):
+    """C := alpha op(A) op(A)^T + beta C on the uplo triangle within the GEMM
+    element-wise bound 4(k+2)eps (gemm_test.cc:46-113), the other triangle
+    untouched (level3.cc:84-139)."""
+    rng = np.random.default_rng(17)
+    n, k = 70, 130
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = rand(rng, ra, ca, dtype)
+    c = rand(rng, n, n, dtype)
+    c1 = c.copy(order="F")
+    alpha, beta = dtype(-0.75), dtype(0.5)
+    f = orc.ssyrk if dtype == np.float32 else orc.dsyrk
+    assert f(uplo, trans, n, k, alpha, a, ra, beta, c1, n) == 0
+    A = a.astype(np.float64)
+    op = A if trans == "N" else A.T
+    want = float(alpha) * (op @ op.T) + float(beta) * c.astype(np.float64)
+    bound = 4 * (k + 2) * np.finfo(dtype).eps * (abs(float(alpha)) * (np.abs(op) @ np.abs(op.T))
+                                                  + abs(float(beta)) * np.abs(c))
+    tri = np.tril(np.ones((n, n), bool)) if uplo == "L" else np.triu(np.ones((n, n), bool))
+    assert np.all(np.abs(c1.astype(np.float64) - want)[tri] <= bound[tri])
+    assert np.array_equal(c1[~tri], c[~tri])
 
 
 def test_trsm_alpha_zero_does_not_read_a(orc):

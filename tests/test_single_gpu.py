@@ -1,12 +1,13 @@
 """Single-precision entry points through the C ABI: strsm_, cblas_strsm,
-sgetrf_, sgetrf2_, slaswp_, sgetrs_, sgesv_.
+ssyrk_, sgetrf_, sgetrf2_, slaswp_, sgetrs_, sgesv_, spotrf_, spotrf2_,
+spotrs_, sposv_.
 
-The reference instantiates its LU family and TRSM for float from the same
-templates as for double (src/lapack/getrf.cc:507-546, src/trsm.cc:190), so
-the bar is the same: factors, pivots, INFO and solutions bit-identical to the
-oracle's float restatement (itself pinned against the reference's own
-getrf.cc at float in test_oracle_pins.py), the float GEMM chains in chunks
-of 384.
+The reference instantiates its LU and Cholesky families, TRSM and SYRK for
+float from the same templates as for double (src/lapack/getrf.cc:507-546,
+potrf.cc:747-773, src/trsm.cc:190, src/level3.cc:410), so the bar is the
+same: factors, pivots, INFO and solutions bit-identical to the oracle's float
+restatement (itself pinned against the reference's own getrf.cc and potrf.cc
+at float in test_oracle_pins.py), the float GEMM chains in chunks of 384.
 """
 import numpy as np
 import pytest
@@ -158,3 +159,64 @@ def test_single_invalid_arguments(hb):
         assert hb.sgetrs("X", 4, 1, a, 4, p, a, 4) == -1
         assert hb.sgesv(4, 1, a, 4, p, a, 3) == -7
     assert cap.errors == [("SGETRF", 1), ("SGETRF2", 4), ("SGETRS", 1), ("SGESV", 7)]
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("n,k", [(1, 1), (30, 10), (100, 300), (257, 64)])
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.5])
+def test_ssyrk_bitexact(hb, orc, uplo, trans, n, k, beta):
+    rng = np.random.default_rng(n + k + 5)
+    ra, ca = (n, k) if trans == "N" else (k, n)
+    a = rand(rng, ra, ca, np.float32)
+    c = rand(rng, n + 1, n, np.float32)
+    c1, c2 = c.copy(order="F"), c.copy(order="F")
+    hb.ssyrk(uplo, trans, n, k, -0.75, a, ra, beta, c1, n + 1)
+    orc.ssyrk(uplo, trans, n, k, np.float32(-0.75), a, ra, np.float32(beta), c2, n + 1)
+    assert same_bits(c1, c2), first_diff(c1, c2)
+
+
+def _spd32(rng, n):
+    g = rng.standard_normal((n, n))
+    return np.asfortranarray((g @ g.T / n + 1e-1 * np.eye(n)).astype(np.float32))
+
+
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 64, 65, 100, 200, 600])
+def test_spotrf_bitexact(hb, orc, recursive, uplo, n):
+    rng = np.random.default_rng(n + 41)
+    a = _spd32(rng, n)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    f1 = hb.spotrf2 if recursive else hb.spotrf
+    f2 = orc.spotrf2 if recursive else orc.spotrf
+    assert f1(uplo, n, a1, n) == f2(uplo, n, a2, n) == 0
+    assert same_bits(a1, a2), first_diff(a1, a2)
+
+
+@pytest.mark.parametrize("uplo", ["U", "L"])
+def test_spotrf_not_positive_definite(hb, orc, uplo):
+    rng = np.random.default_rng(3)
+    n = 90
+    a = _spd32(rng, n)
+    a[50, 50] = -1.0
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    i1 = hb.spotrf(uplo, n, a1, n)
+    assert i1 == orc.spotrf(uplo, n, a2, n) and i1 > 0
+    assert same_bits(a1, a2)
+
+
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (65, 3), (200, 17)])
+def test_spotrs_sposv_bitexact(hb, orc, uplo, n, nrhs):
+    rng = np.random.default_rng(n * 3 + nrhs)
+    a = _spd32(rng, n)
+    b = rand(rng, n, nrhs, np.float32)
+    f = a.copy(order="F")
+    assert orc.spotrf(uplo, n, f, n) == 0
+    x1, x2 = b.copy(order="F"), b.copy(order="F")
+    assert hb.spotrs(uplo, n, nrhs, f, n, x1, n) == orc.spotrs(uplo, n, nrhs, f, n, x2, n) == 0
+    assert same_bits(x1, x2), first_diff(x1, x2)
+    a1, a2, y1, y2 = (v.copy(order="F") for v in (a, a, b, b))
+    assert hb.sposv(uplo, n, nrhs, a1, n, y1, n) == orc.sposv(uplo, n, nrhs, a2, n, y2, n) == 0
+    assert same_bits(a1, a2) and same_bits(y1, y2)
