@@ -20,6 +20,11 @@ PROTOTYPES = {
     "dtrsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "strsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
+    **{f"{p}symm_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
+    **{f"{p}syr2k_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
+    **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])
+       for p in "ds" for r in ("gemmtr", "gemmt")},
+    **{f"{p}trmm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]) for p in "ds"},
     "ssyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     "idamax_": (I, [PI, P, PI]),
     "xerbla_": (None, [C, PI, ctypes.c_size_t]),
@@ -70,6 +75,14 @@ PROTOTYPES = {
     "cblas_dtrsm": (None, [I, I, I, I, I, I, I, D, P, I, P, I]),
     "cblas_strsm": (None, [I, I, I, I, I, I, I, F, P, I, P, I]),
     "cblas_idamax": (ctypes.c_size_t, [I, P, I]),
+    **{f"cblas_{p}trmm": (None, [I, I, I, I, I, I, I, S, P, I, P, I])
+       for p, S in (("d", D), ("s", F))},
+    **{f"cblas_{p}symm": (None, [I, I, I, I, I, S, P, I, P, I, S, P, I])
+       for p, S in (("d", D), ("s", F))},
+    **{f"cblas_{p}syr2k": (None, [I, I, I, I, I, S, P, I, P, I, S, P, I])
+       for p, S in (("d", D), ("s", F))},
+    **{f"cblas_{p}{r}": (None, [I, I, I, I, I, I, S, P, I, P, I, S, P, I])
+       for p, S in (("d", D), ("s", F)) for r in ("gemmtr", "gemmt")},
     # Extensions
     "hwyblas_dgemm_emulated": (I, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI, PI]),
     "hwyblas_dgemm_ddref": (None, [C, C, PI, PI, PI, P, PI, P, PI, PI, P, P, PI]),

@@ -8,6 +8,7 @@ place), and calls the C ABI. Matrices are column-major: pass
 LAPACK wrappers return INFO.
 """
 import ctypes
+import numbers
 
 from . import lib
 
@@ -81,6 +82,55 @@ def ssyrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
     """FP32 symmetric rank-k update (reference ssyrk_, src/level3.cc:410)."""
     lib().ssyrk_(_c(uplo), _c(trans), _i(n), _i(k), _f(alpha), _ptr(a), _i(lda),
                  _f(beta), _ptr(c), _i(ldc))
+
+
+def _scal(p):
+    return _d if p == "d" else _f
+
+
+def symm(p, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Symmetric matrix product; p is "d" or "s" (reference dsymm_/ssymm_,
+    src/level3.cc:362-375)."""
+    sc = _scal(p)
+    getattr(lib(), f"{p}symm_")(_c(side), _c(uplo), _i(m), _i(n), sc(alpha), _ptr(a),
+                                _i(lda), _ptr(b), _i(ldb), sc(beta), _ptr(c), _i(ldc))
+
+
+def syr2k(p, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Symmetric rank-2k update (reference dsyr2k_/ssyr2k_, src/level3.cc:456-469)."""
+    sc = _scal(p)
+    getattr(lib(), f"{p}syr2k_")(_c(uplo), _c(trans), _i(n), _i(k), sc(alpha), _ptr(a),
+                                 _i(lda), _ptr(b), _i(ldb), sc(beta), _ptr(c), _i(ldc))
+
+
+def gemmtr(p, uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c, ldc, name="gemmtr"):
+    """GEMM on one triangle of C (reference ?gemmtr_ and the alias ?gemmt_,
+    src/level3.cc:508-575)."""
+    sc = _scal(p)
+    getattr(lib(), f"{p}{name}_")(_c(uplo), _c(transa), _c(transb), _i(n), _i(k), sc(alpha),
+                                  _ptr(a), _i(lda), _ptr(b), _i(ldb), sc(beta), _ptr(c),
+                                  _i(ldc))
+
+
+def trmm(p, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """Triangular matrix product in place (reference dtrmm_/strmm_,
+    src/level3.cc:581-592)."""
+    getattr(lib(), f"{p}trmm_")(_c(side), _c(uplo), _c(transa), _c(diag), _i(m), _i(n),
+                                _scal(p)(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb))
+
+
+def cblas_level3(name, *args):
+    """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
+    scalars, array arguments given as numpy arrays or device pointers."""
+    conv = []
+    for x in args:
+        if isinstance(x, numbers.Integral):
+            conv.append(int(x))
+        elif isinstance(x, numbers.Real):
+            conv.append(float(x))
+        else:
+            conv.append(_ptr(x))
+    getattr(lib(), f"cblas_{name}")(*conv)
 
 
 def idamax(n, x, incx):

@@ -509,6 +509,156 @@ static void SyrkEntry(const char* name, const char* uplo, const char* trans,
   sc.Out();
   hb::Finish(name);
 }
+
+// SYMM (src/level3.cc:26-76).
+template <typename T>
+static void SymmEntry(const char* name, const char* side, const char* uplo,
+                      const hwyblas_int* m_p, const hwyblas_int* n_p, const T* alpha_p,
+                      const T* a, const hwyblas_int* lda_p, const T* b,
+                      const hwyblas_int* ldb_p, const T* beta_p, T* c,
+                      const hwyblas_int* ldc_p) {
+  const int m = *m_p, n = *n_p, lda = *lda_p, ldb = *ldb_p, ldc = *ldc_p;
+  const char s = hb::Up(*side), u = hb::Up(*uplo);
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const int ka = (s == 'L') ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (lda < std::max(1, ka)) info = 7;
+  else if (ldb < std::max(1, m)) info = 9;
+  else if (ldc < std::max(1, m)) info = 12;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p, beta = *beta_p;
+  if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return;
+  const bool compute = (alpha != T(0));
+  hb::Staged<T> sa, sb, sc;
+  if (compute && !sa.In(a, lda, ka, ka, hb::kWsStageA, true)) return;
+  if (compute && !sb.In(b, ldb, m, n, hb::kWsStageB, true)) return;
+  if (!sc.In(c, ldc, m, n, hb::kWsStageC, beta != T(0))) return;
+  hb::SymmFull<T>(s == 'L', u == 'L', m, n, alpha, sa.dev, std::max(sa.ld, 1), sb.dev,
+                  std::max(sb.ld, 1), beta, sc.dev, sc.ld);
+  sc.Out();
+  hb::Finish(name);
+}
+
+// SYR2K (src/level3.cc:153-221).
+template <typename T>
+static void Syr2kEntry(const char* name, const char* uplo, const char* trans,
+                       const hwyblas_int* n_p, const hwyblas_int* k_p, const T* alpha_p,
+                       const T* a, const hwyblas_int* lda_p, const T* b,
+                       const hwyblas_int* ldb_p, const T* beta_p, T* c,
+                       const hwyblas_int* ldc_p) {
+  const int n = *n_p, k = *k_p, lda = *lda_p, ldb = *ldb_p, ldc = *ldc_p;
+  const char u = hb::Up(*uplo);
+  bool t;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool vt = hb::DecodeOp(*trans, &t);
+  const int rows = t ? k : n;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!vt) info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, rows)) info = 7;
+  else if (ldb < std::max(1, rows)) info = 9;
+  else if (ldc < std::max(1, n)) info = 12;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p, beta = *beta_p;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  const bool compute = !(alpha == T(0) || k == 0);
+  hb::Staged<T> sa, sb, sc;
+  if (compute && !sa.In(a, lda, rows, t ? n : k, hb::kWsStageA, true)) return;
+  if (compute && !sb.In(b, ldb, rows, t ? n : k, hb::kWsStageB, true)) return;
+  // The whole square is copied so that the other triangle comes back as is.
+  if (!sc.In(c, ldc, n, n, hb::kWsStageC, true)) return;
+  hb::Syr2kFull<T>(u == 'L', t, n, k, alpha, sa.dev, std::max(sa.ld, 1), sb.dev,
+                   std::max(sb.ld, 1), beta, sc.dev, sc.ld);
+  sc.Out();
+  hb::Finish(name);
+}
+
+// GEMMTR and its alias GEMMT (src/level3.cc:226-280).
+template <typename T>
+static void GemmtrEntry(const char* name, const char* uplo, const char* transa,
+                        const char* transb, const hwyblas_int* n_p, const hwyblas_int* k_p,
+                        const T* alpha_p, const T* a, const hwyblas_int* lda_p, const T* b,
+                        const hwyblas_int* ldb_p, const T* beta_p, T* c,
+                        const hwyblas_int* ldc_p) {
+  const int n = *n_p, k = *k_p, lda = *lda_p, ldb = *ldb_p, ldc = *ldc_p;
+  const char u = hb::Up(*uplo);
+  bool ta, tb;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool va = hb::DecodeOp(*transa, &ta), vb = hb::DecodeOp(*transb, &tb);
+  const int rows_a = ta ? k : n, rows_b = tb ? n : k;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!va) info = 2;
+  else if (!vb) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, n)) info = 13;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p, beta = *beta_p;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  const bool compute = !(alpha == T(0) || k == 0);
+  hb::Staged<T> sa, sb, sc;
+  if (compute && !sa.In(a, lda, rows_a, ta ? n : k, hb::kWsStageA, true)) return;
+  if (compute && !sb.In(b, ldb, rows_b, tb ? k : n, hb::kWsStageB, true)) return;
+  if (!sc.In(c, ldc, n, n, hb::kWsStageC, true)) return;
+  hb::GemmtrFull<T>(u == 'L', ta, tb, n, k, alpha, sa.dev, std::max(sa.ld, 1), sb.dev,
+                    std::max(sb.ld, 1), beta, sc.dev, sc.ld);
+  sc.Out();
+  hb::Finish(name);
+}
+
+// TRMM (src/level3.cc:284-342).
+template <typename T>
+static void TrmmEntry(const char* name, const char* side, const char* uplo,
+                      const char* transa, const char* diag, const hwyblas_int* m_p,
+                      const hwyblas_int* n_p, const T* alpha_p, const T* a,
+                      const hwyblas_int* lda_p, T* b, const hwyblas_int* ldb_p) {
+  const int m = *m_p, n = *n_p, lda = *lda_p, ldb = *ldb_p;
+  const char s = hb::Up(*side), u = hb::Up(*uplo), d = hb::Up(*diag);
+  bool trans;
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const bool vt = hb::DecodeOp(*transa, &trans), vd = (d == 'U' || d == 'N');
+  const int ka = (s == 'L') ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (!vt) info = 3;
+  else if (!vd) info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, ka)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  const T alpha = *alpha_p;
+  if (m == 0 || n == 0) return;
+  hb::Staged<T> sa, sb;
+  if (alpha != T(0) && !sa.In(a, lda, ka, ka, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, m, n, hb::kWsStageB, alpha != T(0))) return;
+  hb::TrmmFull<T>(s == 'L', u == 'L', trans, d == 'U', m, n, alpha, sa.dev,
+                  std::max(sa.ld, 1), sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish(name);
+}
 }  // extern "C++"
 
 HWYBLAS_API void dsyrk_(const char* uplo, const char* trans, const hwyblas_int* n,
@@ -523,6 +673,78 @@ HWYBLAS_API void ssyrk_(const char* uplo, const char* trans, const hwyblas_int* 
                         const hwyblas_int* lda, const float* beta, float* c,
                         const hwyblas_int* ldc) {
   SyrkEntry<float>("SSYRK", uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+
+HWYBLAS_API void dsymm_(const char* side, const char* uplo, const hwyblas_int* m,
+                        const hwyblas_int* n, const double* alpha, const double* a,
+                        const hwyblas_int* lda, const double* b, const hwyblas_int* ldb,
+                        const double* beta, double* c, const hwyblas_int* ldc) {
+  SymmEntry<double>("DSYMM", side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+HWYBLAS_API void ssymm_(const char* side, const char* uplo, const hwyblas_int* m,
+                        const hwyblas_int* n, const float* alpha, const float* a,
+                        const hwyblas_int* lda, const float* b, const hwyblas_int* ldb,
+                        const float* beta, float* c, const hwyblas_int* ldc) {
+  SymmEntry<float>("SSYMM", side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+HWYBLAS_API void dsyr2k_(const char* uplo, const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* k, const double* alpha, const double* a,
+                         const hwyblas_int* lda, const double* b, const hwyblas_int* ldb,
+                         const double* beta, double* c, const hwyblas_int* ldc) {
+  Syr2kEntry<double>("DSYR2K", uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+HWYBLAS_API void ssyr2k_(const char* uplo, const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* k, const float* alpha, const float* a,
+                         const hwyblas_int* lda, const float* b, const hwyblas_int* ldb,
+                         const float* beta, float* c, const hwyblas_int* ldc) {
+  Syr2kEntry<float>("SSYR2K", uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+HWYBLAS_API void dgemmtr_(const char* uplo, const char* transa, const char* transb,
+                          const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                          const double* a, const hwyblas_int* lda, const double* b,
+                          const hwyblas_int* ldb, const double* beta, double* c,
+                          const hwyblas_int* ldc) {
+  GemmtrEntry<double>("DGEMMTR", uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c,
+                      ldc);
+}
+HWYBLAS_API void sgemmtr_(const char* uplo, const char* transa, const char* transb,
+                          const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                          const float* a, const hwyblas_int* lda, const float* b,
+                          const hwyblas_int* ldb, const float* beta, float* c,
+                          const hwyblas_int* ldc) {
+  GemmtrEntry<float>("SGEMMTR", uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c,
+                     ldc);
+}
+HWYBLAS_API void dgemmt_(const char* uplo, const char* transa, const char* transb,
+                         const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                         const double* a, const hwyblas_int* lda, const double* b,
+                         const hwyblas_int* ldb, const double* beta, double* c,
+                         const hwyblas_int* ldc) {
+  GemmtrEntry<double>("DGEMMT", uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c,
+                      ldc);
+}
+HWYBLAS_API void sgemmt_(const char* uplo, const char* transa, const char* transb,
+                         const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                         const float* a, const hwyblas_int* lda, const float* b,
+                         const hwyblas_int* ldb, const float* beta, float* c,
+                         const hwyblas_int* ldc) {
+  GemmtrEntry<float>("SGEMMT", uplo, transa, transb, n, k, alpha, a, lda, b, ldb, beta, c,
+                     ldc);
+}
+
+HWYBLAS_API void dtrmm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const double* alpha, const double* a, const hwyblas_int* lda,
+                        double* b, const hwyblas_int* ldb) {
+  TrmmEntry<double>("DTRMM", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb);
+}
+HWYBLAS_API void strmm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const float* alpha, const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb) {
+  TrmmEntry<float>("STRMM", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb);
 }
 
 HWYBLAS_API hwyblas_int idamax_(const hwyblas_int* n_p, const double* x,
@@ -950,6 +1172,98 @@ static void CblasTrsm(const char* name, const char* routine, const CBLAS_LAYOUT 
     hb::TrsmEntry<T>(routine, &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda, b, &ldb);
   }
 }
+
+// CBLAS TRMM (src/cblas.cc:666-700): row-major is B^T := alpha B^T op(A)^T with
+// the other side and triangle; op is unchanged.
+template <typename T>
+static void CblasTrmm(const char* name, const char* routine, const CBLAS_LAYOUT layout,
+                      const CBLAS_SIDE side, const CBLAS_UPLO uplo,
+                      const CBLAS_TRANSPOSE transa, const CBLAS_DIAG diag,
+                      const hwyblas_int m_in, const hwyblas_int n_in, const T alpha,
+                      const T* a, const hwyblas_int lda, T* b, const hwyblas_int ldb) {
+  if (!hb::ValidLayout(name, layout)) return;
+  char sc = hb::SideChar(side), uc = hb::UploChar(uplo);
+  const char tc = hb::TransChar(transa), dc = hb::DiagChar(diag);
+  int m = m_in, n = n_in;
+  const bool row = (layout == CblasRowMajor);
+  if (row) {
+    sc = hb::FlipSide(sc);
+    uc = hb::FlipUplo(uc);
+    std::swap(m, n);
+  }
+  if (row) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 7, 6, 8, 9, 10, 11, 12});
+    TrmmEntry<T>(routine, &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda, b, &ldb);
+  } else {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12});
+    TrmmEntry<T>(routine, &sc, &uc, &tc, &dc, &m, &n, &alpha, a, &lda, b, &ldb);
+  }
+}
+
+// CBLAS SYMM (src/cblas.cc:562-607): row-major is C^T = B^T A^T, A stored as
+// the other triangle, with the other side and m, n swapped.
+template <typename T>
+static void CblasSymm(const char* name, const char* routine, const CBLAS_LAYOUT layout,
+                      const CBLAS_SIDE side, const CBLAS_UPLO uplo, const hwyblas_int m_in,
+                      const hwyblas_int n_in, const T alpha, const T* a,
+                      const hwyblas_int lda, const T* b, const hwyblas_int ldb, const T beta,
+                      T* c, const hwyblas_int ldc) {
+  if (!hb::ValidLayout(name, layout)) return;
+  char sc = hb::SideChar(side), uc = hb::UploChar(uplo);
+  int m = m_in, n = n_in;
+  const bool row = (layout == CblasRowMajor);
+  if (row) {
+    sc = hb::FlipSide(sc);
+    uc = hb::FlipUplo(uc);
+    std::swap(m, n);
+  }
+  if (row) {
+    hb::CblasScope scope(name, {2, 3, 5, 4, 6, 7, 8, 9, 10, 11, 12, 13});
+    SymmEntry<T>(routine, &sc, &uc, &m, &n, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+  } else {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13});
+    SymmEntry<T>(routine, &sc, &uc, &m, &n, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+  }
+}
+
+// CBLAS SYR2K (src/cblas.cc:632-664): row-major flips uplo and N <-> T.
+template <typename T>
+static void CblasSyr2k(const char* name, const char* routine, const CBLAS_LAYOUT layout,
+                       const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE trans,
+                       const hwyblas_int n, const hwyblas_int k, const T alpha, const T* a,
+                       const hwyblas_int lda, const T* b, const hwyblas_int ldb,
+                       const T beta, T* c, const hwyblas_int ldc) {
+  if (!hb::ValidLayout(name, layout)) return;
+  char uc = hb::UploChar(uplo), tc = hb::TransChar(trans);
+  if (layout == CblasRowMajor) {
+    uc = hb::FlipUplo(uc);
+    tc = (tc == 'N') ? 'T' : (tc == 'T' || tc == 'C') ? 'N' : tc;
+  }
+  hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13});
+  Syr2kEntry<T>(routine, &uc, &tc, &n, &k, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+}
+
+// CBLAS GEMMTR / GEMMT (src/cblas.cc:539-566): row-major is the column-major
+// product of the swapped operands on the other triangle.
+template <typename T>
+static void CblasGemmtr(const char* name, const char* routine, const CBLAS_LAYOUT layout,
+                        const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                        const CBLAS_TRANSPOSE transb, const hwyblas_int n,
+                        const hwyblas_int k, const T alpha, const T* a,
+                        const hwyblas_int lda, const T* b, const hwyblas_int ldb, const T beta,
+                        T* c, const hwyblas_int ldc) {
+  if (!hb::ValidLayout(name, layout)) return;
+  const char ta = hb::TransChar(transa), tb = hb::TransChar(transb);
+  const char uc = hb::UploChar(uplo);
+  if (layout == CblasColMajor) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14});
+    GemmtrEntry<T>(routine, &uc, &ta, &tb, &n, &k, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+  } else {
+    const char ur = hb::FlipUplo(uc);
+    hb::CblasScope scope(name, {2, 4, 3, 5, 6, 7, 10, 11, 8, 9, 12, 13, 14});
+    GemmtrEntry<T>(routine, &ur, &tb, &ta, &n, &k, &alpha, b, &ldb, a, &lda, &beta, c, &ldc);
+  }
+}
 }  // extern "C++"
 
 HWYBLAS_API void cblas_dtrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
@@ -973,6 +1287,52 @@ HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
   CblasTrsm<float>("cblas_strsm", "STRSM", layout, side, uplo, transa, diag, m_in, n_in,
                    alpha, a, lda, b, ldb);
 }
+
+#define HB_CBLAS_L3(P, U, T)                                                                \
+  HWYBLAS_API void cblas_##P##trmm(                                                         \
+      const CBLAS_LAYOUT layout, const CBLAS_SIDE side, const CBLAS_UPLO uplo,              \
+      const CBLAS_TRANSPOSE transa, const CBLAS_DIAG diag, const hwyblas_int m,             \
+      const hwyblas_int n, const T alpha, const T* a, const hwyblas_int lda, T* b,          \
+      const hwyblas_int ldb) {                                                              \
+    CblasTrmm<T>("cblas_" #P "trmm", #U "TRMM", layout, side, uplo, transa, diag, m, n,   \
+                 alpha, a, lda, b, ldb);                                                    \
+  }                                                                                         \
+  HWYBLAS_API void cblas_##P##symm(                                                         \
+      const CBLAS_LAYOUT layout, const CBLAS_SIDE side, const CBLAS_UPLO uplo,              \
+      const hwyblas_int m, const hwyblas_int n, const T alpha, const T* a,                  \
+      const hwyblas_int lda, const T* b, const hwyblas_int ldb, const T beta, T* c,         \
+      const hwyblas_int ldc) {                                                              \
+    CblasSymm<T>("cblas_" #P "symm", #U "SYMM", layout, side, uplo, m, n, alpha, a, lda,  \
+                 b, ldb, beta, c, ldc);                                                     \
+  }                                                                                         \
+  HWYBLAS_API void cblas_##P##syr2k(                                                        \
+      const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE trans,        \
+      const hwyblas_int n, const hwyblas_int k, const T alpha, const T* a,                  \
+      const hwyblas_int lda, const T* b, const hwyblas_int ldb, const T beta, T* c,         \
+      const hwyblas_int ldc) {                                                              \
+    CblasSyr2k<T>("cblas_" #P "syr2k", #U "SYR2K", layout, uplo, trans, n, k, alpha, a,   \
+                  lda, b, ldb, beta, c, ldc);                                               \
+  }                                                                                         \
+  HWYBLAS_API void cblas_##P##gemmtr(                                                       \
+      const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,       \
+      const CBLAS_TRANSPOSE transb, const hwyblas_int n, const hwyblas_int k,               \
+      const T alpha, const T* a, const hwyblas_int lda, const T* b, const hwyblas_int ldb,  \
+      const T beta, T* c, const hwyblas_int ldc) {                                          \
+    CblasGemmtr<T>("cblas_" #P "gemmtr", #U "GEMMTR", layout, uplo, transa, transb, n, k, \
+                   alpha, a, lda, b, ldb, beta, c, ldc);                                    \
+  }                                                                                         \
+  HWYBLAS_API void cblas_##P##gemmt(                                                        \
+      const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,       \
+      const CBLAS_TRANSPOSE transb, const hwyblas_int n, const hwyblas_int k,               \
+      const T alpha, const T* a, const hwyblas_int lda, const T* b, const hwyblas_int ldb,  \
+      const T beta, T* c, const hwyblas_int ldc) {                                          \
+    CblasGemmtr<T>("cblas_" #P "gemmt", #U "GEMMT", layout, uplo, transa, transb, n, k,   \
+                   alpha, a, lda, b, ldb, beta, c, ldc);                                    \
+  }
+
+HB_CBLAS_L3(d, D, double)
+HB_CBLAS_L3(s, S, float)
+#undef HB_CBLAS_L3
 
 HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
                                      const hwyblas_int incx) {

@@ -53,9 +53,59 @@ struct GemmParams {
   double* c;
   long long ldc;
   int part;
+  int tri;  // Tri: which operand is triangular (TRMM)
   int* timeout_flag;
   const int* guard;
 };
+
+// k range [*kb, *ke) that the reference multiplies for C(i, j) when an
+// operand is triangular: NonZeroRange of the AVX-512 double micro-tile (MR 16,
+// NR 12, MC 96, NC 4080) holding C(i, j) (src/gemm-inl.h:62-85). Row tiles
+// start at multiples of 16 (MC is a multiple of MR); column tiles at
+// multiples of 12 within NC blocks.
+__device__ __forceinline__ void TriRange(const GemmParams& p, int i, int j, int* kb,
+                                         int* ke) {
+  *kb = 0;
+  *ke = p.k;
+  if (p.tri == kTriALower || p.tri == kTriAUpper) {
+    const int i0 = i & ~15, mr = min(16, p.m - i0);
+    if (p.tri == kTriALower) *ke = min(p.k, i0 + mr);
+    else *kb = i0;
+  } else if (p.tri == kTriBLower || p.tri == kTriBUpper) {
+    constexpr int NR = 12, NC = 4080;
+    const int jc = j / NC * NC, jr = (j - jc) / NR * NR;
+    const int nr = min(NR, min(NC, p.n - jc) - jr);
+    if (p.tri == kTriBLower) *kb = jc + jr;
+    else *ke = min(p.k, jc + jr + nr);
+  }
+}
+
+// The k-slices (of kBK) a tile of C needs: the union of its elements' ranges.
+__device__ __forceinline__ void TileKRange(const GemmParams& p, int m0, int n0, int kt_total,
+                                           int* kt_lo, int* kt_hi) {
+  *kt_lo = 0;
+  *kt_hi = kt_total;
+  int kb, ke;
+  switch (p.tri) {
+    case kTriALower:
+      TriRange(p, min(p.m, m0 + kBM) - 1, 0, &kb, &ke);
+      *kt_hi = (ke + kBK - 1) / kBK;
+      break;
+    case kTriAUpper:
+      *kt_lo = m0 / kBK;
+      break;
+    case kTriBLower:
+      TriRange(p, 0, n0, &kb, &ke);
+      *kt_lo = kb / kBK;
+      break;
+    case kTriBUpper:
+      TriRange(p, 0, min(p.n, n0 + kBN) - 1, &kb, &ke);
+      *kt_hi = (ke + kBK - 1) / kBK;
+      break;
+    default:
+      break;
+  }
+}
 
 // Whether C(i, j) lies in a micro-tile of the reference's AVX-512 double
 // kernel (MR 16, NR 12, MC 96, NC 4080) that crosses the diagonal
@@ -109,11 +159,12 @@ __device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
 }
 
 // Producer cursor: the TMA loads of the CTA's k-slices in order, across
-// tile boundaries.
+// tile boundaries (kt = -1: the current tile's slices are not yet known).
 struct Producer {
-  int tile, kt, gs;
+  int tile, kt, kt_hi, gs;
 };
 
+template <bool kTri>
 __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
                                           int tiles_m, int tiles_n, int kt_total,
                                           uint8_t* smem, uint64_t* full,
@@ -123,8 +174,20 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
   int m0 = 0, n0 = 0;
   while (pr.tile < num_tiles) {
     TileOrigin(pr.tile, tiles_m, tiles_n, &m0, &n0);
-    if (!SkipTile(p, m0, n0)) break;
+    if constexpr (!kTri) {
+      if (!SkipTile(p, m0, n0)) break;
+    } else if (!SkipTile(p, m0, n0)) {
+      if (pr.kt >= 0) break;
+      int lo, hi;
+      TileKRange(p, m0, n0, kt_total, &lo, &hi);
+      if (lo < hi) {
+        pr.kt = lo;
+        pr.kt_hi = hi;
+        break;
+      }
+    }
     pr.tile += gridDim.x;
+    if constexpr (kTri) pr.kt = -1;
   }
   if (pr.tile >= num_tiles) return true;
   const int s = pr.gs % kStages, round = pr.gs / kStages;
@@ -136,8 +199,8 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
     TmaLoad2d(st + b * kABoxBytes, tm_a, m0 + 16 * b, pr.kt * kBK, &full[s]);
   TmaLoad2d(st + kTileABytes, tm_b, pr.kt * kBK, n0, &full[s]);
   ++pr.gs;
-  if (++pr.kt == kt_total) {
-    pr.kt = 0;
+  if (++pr.kt == (kTri ? pr.kt_hi : kt_total)) {
+    pr.kt = kTri ? -1 : 0;
     pr.tile += gridDim.x;
   }
   return true;
@@ -145,6 +208,17 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
 
 // 168 registers: nine warps of a CTA share the 16K registers of each SM
 // sub-partition three at a time.
+//
+// kTri (TRMM): each tile loads only the k-slices its elements need; a 16-row
+// MMA block is exactly one reference row micro-tile, so for a triangular
+// op(A) its MMAs run only inside that tile's k range. Reference column
+// micro-tiles are 12 wide, so an 8-column MMA block of a triangular op(B) can
+// span two ranges: its k8 steps inside both run as MMAs, those outside both
+// are skipped, and the (at most two) steps in between run as per-element FMA
+// chains over the in-range k only, in the MMA's own ascending order. A chunk
+// whose range is empty for an element leaves it unmerged, as the reference
+// skips that micro-tile (src/gemm-inl.h:202-209).
+template <bool kTri>
 __global__ void __maxnreg__(168)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
@@ -175,10 +249,10 @@ __global__ void __maxnreg__(168)
     if (lane == 0) {
       PrefetchTmap(&tm_a);
       PrefetchTmap(&tm_b);
-      Producer pr{static_cast<int>(blockIdx.x), 0, 0};
+      Producer pr{static_cast<int>(blockIdx.x), kTri ? -1 : 0, 0, 0};
       while (pr.tile < num_tiles) {
-        if (!IssueNext(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
-                       &tm_a, &tm_b))
+        if (!IssueNext<kTri>(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
+                             &tm_a, &tm_b))
           return;
       }
     }
@@ -198,6 +272,8 @@ __global__ void __maxnreg__(168)
     int m0, n0;
     TileOrigin(tile, tiles_m, tiles_n, &m0, &n0);
     if (SkipTile(p, m0, n0)) continue;
+    int kt_lo = 0, kt_hi = kt_total;
+    if constexpr (kTri) TileKRange(p, m0, n0, kt_total, &kt_lo, &kt_hi);
     // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
     // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
     const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
@@ -222,8 +298,83 @@ __global__ void __maxnreg__(168)
             crossing |= 1u << bit;
           cacc[mb][nb][e] = (inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
         }
+    // kTri: k ranges of the 16-row blocks [xb, xe) (op(A) triangular), and the
+    // union [ub, ue) and intersection [ib, ie) of the ranges of the 8-column
+    // blocks' columns (op(B) triangular; ranges are monotone in j, so the
+    // first and last columns bound them). Blocks wholly outside C get empty
+    // ranges.
+    int xb[2] = {0, 0}, xe[2] = {p.k, p.k};
+    int ub[4] = {0, 0, 0, 0}, ue[4] = {p.k, p.k, p.k, p.k};
+    int ib[4] = {0, 0, 0, 0}, ie[4] = {p.k, p.k, p.k, p.k};
+    if constexpr (kTri) {
+      const int fr = m0 + wm * 32;
+#pragma unroll
+      for (int mb = 0; mb < 2; ++mb) {
+        if (fr + mb * 16 >= p.m) {
+          xb[mb] = xe[mb] = 0;
+        } else if (p.tri == kTriALower || p.tri == kTriAUpper) {
+          TriRange(p, fr + mb * 16, 0, &xb[mb], &xe[mb]);
+        }
+      }
+#pragma unroll
+      for (int nb = 0; nb < 4; ++nb) {
+        const int j0 = col0 + nb * 8, j1 = min(j0 + 7, p.n - 1);
+        if (j0 >= p.n) {
+          ub[nb] = ue[nb] = ib[nb] = ie[nb] = 0;
+        } else if (p.tri == kTriBLower || p.tri == kTriBUpper) {
+          int b0, e0, b1, e1;
+          TriRange(p, 0, j0, &b0, &e0);
+          TriRange(p, 0, j1, &b1, &e1);
+          ub[nb] = min(b0, b1);
+          ib[nb] = max(b0, b1);
+          ue[nb] = max(e0, e1);
+          ie[nb] = min(e0, e1);
+        }
+      }
+    }
 
-    for (int kt = 0; kt < kt_total; ++kt, ++gs) {
+    // Merge of chunk `chunk` (256 deep) into the running C values.
+    const auto merge = [&](int chunk) {
+      const bool first = (chunk == 0);
+      const int c_lo = chunk * 256, c_hi = min(p.k, c_lo + 256);
+#pragma unroll
+      for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int bit = (mb * 4 + nb) * 4 + e;
+            bool skip = false;
+            if constexpr (kTri) {
+              if (!first) {
+                int kb, ke;
+                TriRange(p, row0 + mb * 16 + (e >> 1),
+                         col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0), &kb, &ke);
+                skip = max(kb, c_lo) >= min(ke, c_hi);
+              }
+            }
+            const double r = p.alpha * acc[mb][nb][e];
+            double& cv = cacc[mb][nb][e];
+            if (skip) {
+              // Outside the element's k range: not merged.
+            } else if (!first || p.beta == 1.0) {
+              cv = r + cv;
+            } else if (p.beta == 0.0) {
+              cv = r;
+            } else if ((crossing >> bit) & 1u) {
+              const double bc = p.beta * cv;
+              cv = r + bc;
+            } else {
+              cv = fma(cv, p.beta, r);
+            }
+            acc[mb][nb][e] = 0.0;
+          }
+    };
+    // Chunk 0 lies before the tile's first k-slice: its k range is empty for
+    // every element, and the reference still applies beta (with alpha * 0).
+    if (kTri && !(kt_lo < kt_hi && kt_lo < kKtPerChunk)) merge(0);
+
+    for (int kt = kt_lo; kt < kt_hi; ++kt, ++gs) {
       const int s = gs % kStages, round = gs / kStages;
       if (!MbarWait(&full[s], round & 1, p.timeout_flag)) return;
       const double* sa = reinterpret_cast<const double*>(smem + s * kStageBytes);
@@ -245,6 +396,7 @@ __global__ void __maxnreg__(168)
           af[mb][2] = hi.x;
           af[mb][3] = hi.y;
         }
+        const int kg = kt * kBK + ks * 8, kend = min(kg + 8, p.k);
 #pragma unroll
         for (int nb = 0; nb < 4; ++nb) {
           const int r = wn * 32 + nb * 8 + bcol;
@@ -253,8 +405,43 @@ __global__ void __maxnreg__(168)
               sb + r * 128 + (((k0 >> 1) ^ (r & 7)) << 4) + ((k0 & 1) << 3));
           const double b1 = *reinterpret_cast<const double*>(
               sb + r * 128 + (((k1 >> 1) ^ (r & 7)) << 4) + ((k1 & 1) << 3));
-          Dmma(acc[0][nb], af[0], b0, b1);
-          Dmma(acc[1][nb], af[1], b0, b1);
+          if constexpr (!kTri) {
+            Dmma(acc[0][nb], af[0], b0, b1);
+            Dmma(acc[1][nb], af[1], b0, b1);
+          } else {
+            if (kg >= p.k || kend <= ub[nb] || kg >= ue[nb]) continue;
+            if (kg >= ib[nb] && kend <= ie[nb]) {
+#pragma unroll
+              for (int mb = 0; mb < 2; ++mb)
+                if (kg >= xb[mb] && kg < xe[mb]) Dmma(acc[mb][nb], af[mb], b0, b1);
+              continue;
+            }
+            // Per-element chains (only for a triangular op(B), whose op(A)
+            // blocks all need every k).
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb) {
+              const uint8_t* box = reinterpret_cast<const uint8_t*>(sa) +
+                                   (wm * 2 + mb) * kABoxBytes;
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const int col = (e & 1) ? ccol1 : ccol0;
+                const int rc = wn * 32 + nb * 8 + col;
+                int kb, ke;
+                TriRange(p, 0, col0 + nb * 8 + col, &kb, &ke);
+                double a_acc = acc[mb][nb][e];
+                for (int q = 0; q < 8; ++q) {
+                  const int kk = ks * 8 + q, kq = kg + q;
+                  if (kq < kb || kq >= ke) continue;
+                  const double av = *reinterpret_cast<const double*>(
+                      box + kk * 128 + ((cg ^ (kk & 7)) << 4) + (e >> 1) * 8);
+                  const double bv = *reinterpret_cast<const double*>(
+                      sb + rc * 128 + (((kk >> 1) ^ (rc & 7)) << 4) + ((kk & 1) << 3));
+                  a_acc = fma(av, bv, a_acc);
+                }
+                acc[mb][nb][e] = a_acc;
+              }
+            }
+          }
         }
       }
       // The stage was read through the generic proxy and will be rewritten
@@ -266,30 +453,7 @@ __global__ void __maxnreg__(168)
       if (lane == 0) MbarArrive(&empty[s]);
 
       // End of a reference KC chunk: merge into the running C value.
-      if ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_total) {
-        const bool first = (kt < kKtPerChunk);
-#pragma unroll
-        for (int mb = 0; mb < 2; ++mb)
-#pragma unroll
-          for (int nb = 0; nb < 4; ++nb)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int bit = (mb * 4 + nb) * 4 + e;
-              const double r = p.alpha * acc[mb][nb][e];
-              double& cv = cacc[mb][nb][e];
-              if (!first || p.beta == 1.0) {
-                cv = r + cv;
-              } else if (p.beta == 0.0) {
-                cv = r;
-              } else if ((crossing >> bit) & 1u) {
-                const double bc = p.beta * cv;
-                cv = r + bc;
-              } else {
-                cv = fma(cv, p.beta, r);
-              }
-              acc[mb][nb][e] = 0.0;
-            }
-      }
+      if ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_hi) merge(kt / kKtPerChunk);
     }
 
     // Epilogue: write C.
@@ -318,11 +482,14 @@ __global__ void __launch_bounds__(256)
   const int j = blockIdx.y * 8 + threadIdx.x / 32;
   if (!InPart(p, i, j)) return;
   const bool crossing = p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j);
+  int kb = 0, ke = p.k;
+  if (p.tri != kTriNone) TriRange(p, i, j, &kb, &ke);
   double cv = 0.0;
   for (int pc = 0; pc < p.k; pc += 256) {
-    const int pe = min(p.k, pc + 256);
+    const int lo = max(pc, kb), hi = min(min(p.k, pc + 256), ke);
+    if (lo >= hi && pc != 0) continue;  // the reference skips the micro-tile
     double acc = 0.0;
-    for (int q = pc; q < pe; ++q) acc = fma(a.data[i * a.rs + q * a.cs],
+    for (int q = lo; q < hi; ++q) acc = fma(a.data[i * a.rs + q * a.cs],
                                             b.data[q * b.rs + j * b.cs], acc);
     const double r = p.alpha * acc;
     if (pc != 0 || p.beta == 1.0) {
@@ -357,10 +524,12 @@ __global__ void __launch_bounds__(256)
   const int i = static_cast<int>(elem % p.m), j = static_cast<int>(elem / p.m);
   const int nc = (p.k + 255) / 256;
   const bool valid = elem < static_cast<long long>(p.m) * p.n;
+  int kb = 0, ke = p.k;
+  if (valid && p.tri != kTriNone) TriRange(p, i, j, &kb, &ke);
   double acc = 0.0;
   if (valid && ch < nc) {
-    const int pe = min(p.k, ch * 256 + 256);
-    for (int q = ch * 256; q < pe; ++q)
+    const int hi = min(min(p.k, ch * 256 + 256), ke);
+    for (int q = max(ch * 256, kb); q < hi; ++q)
       acc = fma(a.data[i * a.rs + q * a.cs], b.data[q * b.rs + j * b.cs], acc);
   }
   part[threadIdx.x] = acc;
@@ -369,6 +538,8 @@ __global__ void __launch_bounds__(256)
   const bool crossing = p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j);
   double cv = 0.0;
   for (int c = 0; c < nc; ++c) {
+    // A chunk outside the element's k range: the reference skips the tile.
+    if (c != 0 && max(c * 256, kb) >= min(min(p.k, c * 256 + 256), ke)) continue;
     const double r = p.alpha * part[threadIdx.x + c];
     if (c != 0 || p.beta == 1.0) {
       if (c == 0) cv = p.c[i + j * p.ldc];
@@ -505,7 +676,7 @@ template const double* Canonical(View<double>, int, int, int, long long*);
 template const float* Canonical(View<float>, int, int, int, long long*);
 
 void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
-           double beta, double* c, int ldc, Part part) {
+           double beta, double* c, int ldc, Part part, Tri tri) {
   Context& ctx = Ctx();
   if (static_cast<long long>(m) * n * k <= (1LL << 22) || m < 32 || n < 32) {
     GemmParams p;
@@ -517,6 +688,7 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
     p.c = c;
     p.ldc = ldc;
     p.part = part;
+    p.tri = tri;
     p.timeout_flag = ctx.dev_status;
     p.guard = ctx.guard;
     const int nc = (k + 255) / 256;
@@ -559,13 +731,16 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   p.c = c;
   p.ldc = ldc;
   p.part = part;
+  p.tri = tri;
   p.timeout_flag = ctx.dev_status;
   p.guard = ctx.guard;
   const long long tiles =
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(DgemmDmmaKernel,
+    cudaFuncSetAttribute(DgemmDmmaKernel<false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    cudaFuncSetAttribute(DgemmDmmaKernel<true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     configured = true;
   }
@@ -576,7 +751,11 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const unsigned grid =
       static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
   cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
-  DgemmDmmaKernel<<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  if (tri == kTriNone) {
+    DgemmDmmaKernel<false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  } else {
+    DgemmDmmaKernel<true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  }
   KernelTimerStop(t0, ctx.stream);
   CountLaunch();
   LaunchFailed("dgemm");

@@ -15,6 +15,10 @@ namespace hb {
 
 // Which part of C a product updates (the reference's Part, src/gemm.h:39).
 enum Part : int { kAll = 0, kLower = 1, kUpper = 2 };
+// A triangular GEMM operand (TRMM): op(A) or op(B) lower or upper. Products
+// are restricted to the k range the reference multiplies for each of its
+// micro-tiles (src/gemm-inl.h:62-85).
+enum Tri : int { kTriNone = 0, kTriALower = 1, kTriAUpper = 2, kTriBLower = 3, kTriBUpper = 4 };
 
 // A strided view of op(X): element (i, p) is data[i * rs + p * cs], with one
 // of rs, cs equal to 1 (column-major storage, possibly transposed). This is
@@ -81,7 +85,9 @@ enum WorkspaceSlot : int {
   kWsTourney = 17, // tournament-pivoting leaf: candidates and results
   kWsLapacke0 = 18, // LAPACKE row-major temporaries (device callers)
   kWsLapacke1 = 19,
-  kNumWorkspaceSlots = 20
+  kWsLevel3 = 20,      // SYMM's symmetrized operand, TRMM's triangle
+  kWsLevel3Copy = 21,  // TRMM's copy of B
+  kNumWorkspaceSlots = 22
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -113,11 +119,14 @@ void KernelTimerStop(cudaEvent_t start, cudaStream_t stream);
 
 // C := alpha*op(A)*op(B) + beta*C on `part` of C; requires m, n, k > 0 and
 // alpha != 0. Bit-identical to the reference's GEMM (double: chunks of 256).
+// `tri` names a triangular operand whose zero triangle (and unit diagonal) is
+// stored explicitly; only the reference's per-micro-tile k ranges are
+// multiplied, so every chain is the reference's.
 void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
-           double beta, double* c, int ldc, Part part = kAll);
+           double beta, double* c, int ldc, Part part = kAll, Tri tri = kTriNone);
 // FP32 (chunks of 384), FFMA on the CUDA cores.
 void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
-           float beta, float* c, int ldc, Part part = kAll);
+           float beta, float* c, int ldc, Part part = kAll, Tri tri = kTriNone);
 // C := beta*C on `part` (beta == 0 writes zeros without reading C).
 template <typename T>
 void ScaleMatrix(int m, int n, T beta, T* c, int ldc, Part part = kAll);
@@ -174,6 +183,20 @@ void TrsmFull(bool left, bool lower, bool trans, bool unit, int m, int n,
 template <typename T>
 void SyrkFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda, T beta,
               T* c, int ldc);
+// SYMM, SYR2K, GEMMTR and TRMM (src/level3.cc:26-76, 153-342) after argument
+// checks.
+template <typename T>
+void SymmFull(bool left, bool lower, int m, int n, T alpha, const T* a, int lda, const T* b,
+              int ldb, T beta, T* c, int ldc);
+template <typename T>
+void Syr2kFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda,
+               const T* b, int ldb, T beta, T* c, int ldc);
+template <typename T>
+void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
+                const T* b, int ldb, T beta, T* c, int ldc);
+template <typename T>
+void TrmmFull(bool left, bool lower, bool trans, bool unit, int m, int n, T alpha,
+              const T* a, int lda, T* b, int ldb);
 template <typename T>
 void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
               int lda, const T* b, int ldb, T beta, T* c, int ldc);

@@ -22,9 +22,50 @@ __device__ __forceinline__ bool InPart(int part, int i, int j) {
   return part == kAll || (part == kLower ? i >= j : i <= j);
 }
 
+// Whether C(i, j) lies in a micro-tile of the reference's AVX-512 float
+// kernel (MR 32, NR 12, MC 128, NC 4080) that crosses the diagonal: those
+// tiles merge as alpha*acc + beta*C with two roundings (src/gemm-inl.h:93-130;
+// src/gemm_kernel-inl.h:64-74).
+__device__ __forceinline__ bool InCrossingTileF(int part, int m, int n, int i, int j) {
+  constexpr int MR = 32, NR = 12, MC = 128, NC = 4080;
+  const int ic = i / MC * MC, mcb = min(MC, m - ic);
+  const int ir = (i - ic) / MR * MR, mr = min(MR, mcb - ir);
+  const int jc = j / NC * NC, ncb = min(NC, n - jc);
+  const int jr = (j - jc) / NR * NR, nr = min(NR, ncb - jr);
+  const int i0 = ic + ir, j0 = jc + jr;
+  if (part == kLower) return !(i0 > j0 + nr - 1);
+  return !(i0 + mr - 1 < j0);
+}
+
+// k range [*kb, *ke) the reference multiplies for C(i, j) when an operand is
+// triangular: NonZeroRange of the AVX-512 float micro-tile (MR 32, NR 12,
+// MC 128, NC 4080) holding C(i, j) (src/gemm-inl.h:62-85). Row tiles start at
+// multiples of 32 (MC is a multiple of MR), column tiles at multiples of 12
+// within NC blocks.
+__device__ __forceinline__ void TriRangeF(int tri, int m, int n, int k, int i, int j, int* kb,
+                                          int* ke) {
+  *kb = 0;
+  *ke = k;
+  if (tri == kTriALower || tri == kTriAUpper) {
+    const int i0 = i & ~31, mr = min(32, m - i0);
+    if (tri == kTriALower) *ke = min(k, i0 + mr);
+    else *kb = i0;
+  } else if (tri == kTriBLower || tri == kTriBUpper) {
+    constexpr int NR = 12, NC = 4080;
+    const int jc = j / NC * NC, jr = (j - jc) / NR * NR;
+    const int nr = min(NR, min(NC, n - jc) - jr);
+    if (tri == kTriBLower) *kb = jc + jr;
+    else *ke = min(k, jc + jr + nr);
+  }
+}
+
+// `tri` (TRMM): each element's chain runs over its micro-tile's k range only,
+// and a chunk outside that range leaves the element unmerged, as the
+// reference skips the micro-tile (src/gemm-inl.h:202-209).
 __global__ void __launch_bounds__(256)
     SgemmKernel(int m, int n, int k, float alpha, View<float> a, View<float> b,
-                float beta, float* c, long long ldc, int part, const int* guard) {
+                float beta, float* c, long long ldc, int part, int tri,
+                const int* guard) {
   if (guard != nullptr && *guard != 0) return;
   __shared__ float sa[kSK][kSB + 4];
   __shared__ float sb[kSK][kSB + 4];
@@ -34,6 +75,15 @@ __global__ void __launch_bounds__(256)
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   float acc[4][4] = {}, cacc[4][4] = {};
   const int kchunk = 384;
+  // Row- and column-dependent bounds of the elements' k ranges (tri).
+  int rkb[4], rke[4], ckb[4], cke[4];
+  const int tri_a = (tri == kTriALower || tri == kTriAUpper) ? tri : kTriNone;
+  const int tri_b = (tri == kTriBLower || tri == kTriBUpper) ? tri : kTriNone;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    TriRangeF(tri_a, m, n, k, m0 + tx + 16 * r, 0, &rkb[r], &rke[r]);
+    TriRangeF(tri_b, m, n, k, 0, n0 + ty + 16 * r, &ckb[r], &cke[r]);
+  }
   for (int k0 = 0; k0 < k; k0 += kSK) {
     for (int idx = threadIdx.x; idx < kSK * kSB; idx += 256) {
       const int kk = idx / kSB, mm = idx % kSB;
@@ -50,26 +100,46 @@ __global__ void __launch_bounds__(256)
       for (int r = 0; r < 4; ++r) av[r] = sa[kk][tx + 16 * r];
 #pragma unroll
       for (int q = 0; q < 4; ++q) bv[q] = sb[kk][ty + 16 * q];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[r][q] = fmaf(av[r], bv[q], acc[r][q]);
       const int kg = k0 + kk;
+      if (tri == kTriNone) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[r][q] = fmaf(av[r], bv[q], acc[r][q]);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (kg >= max(rkb[r], ckb[q]) && kg < min(rke[r], cke[q]))
+              acc[r][q] = fmaf(av[r], bv[q], acc[r][q]);
+      }
       if ((kg + 1) % kchunk == 0 || kg + 1 == k) {
         const bool first = kg < kchunk;
+        const int c_lo = kg / kchunk * kchunk, c_hi = kg + 1;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
             const float rr = alpha * acc[r][q];
-            if (first) {
+            if (!first && tri != kTriNone &&
+                max(max(rkb[r], ckb[q]), c_lo) >= min(min(rke[r], cke[q]), c_hi)) {
+              // Outside the element's k range: not merged.
+            } else if (first) {
               if (i < m && j < n && InPart(part, i, j)) {
                 if (beta == 0.f) {
                   cacc[r][q] = rr;
                 } else {
                   const float cin = c[i + j * ldc];
-                  cacc[r][q] = (beta == 1.f) ? rr + cin : fmaf(cin, beta, rr);
+                  if (beta == 1.f) {
+                    cacc[r][q] = rr + cin;
+                  } else if (part != kAll && InCrossingTileF(part, m, n, i, j)) {
+                    const float bc = beta * cin;
+                    cacc[r][q] = rr + bc;
+                  } else {
+                    cacc[r][q] = fmaf(cin, beta, rr);
+                  }
                 }
               }
             } else {
@@ -220,10 +290,11 @@ void TrsmRec(bool left, View<T> tri, bool lower, bool unit, int r, int other,
 }  // namespace
 
 void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
-           float beta, float* c, int ldc, Part part) {
+           float beta, float* c, int ldc, Part part, Tri tri) {
   const dim3 grid((m + kSB - 1) / kSB, (n + kSB - 1) / kSB);
-  SgemmKernel<<<grid, 256, 0, Ctx().stream>>>(m, n, k, alpha, a, b, beta, c,
-                                              ldc, static_cast<int>(part), Ctx().guard);
+  SgemmKernel<<<grid, 256, 0, Ctx().stream>>>(m, n, k, alpha, a, b, beta, c, ldc,
+                                              static_cast<int>(part),
+                                              static_cast<int>(tri), Ctx().guard);
   CountLaunch();
   LaunchFailed("sgemm");
 }
@@ -301,6 +372,163 @@ template void SyrkFull<double>(bool, bool, int, int, double, const double*, int,
                                double*, int);
 template void SyrkFull<float>(bool, bool, int, int, float, const float*, int, float, float*,
                               int);
+
+namespace {
+
+// A GEMM problem on the triangle `part` of C (DMMA for double, FP32 FFMA for
+// float), with the reference's merge rules for tiles crossing the diagonal.
+template <typename T>
+void GemmPart(int m, int n, int k, T alpha, View<T> a, View<T> b, T beta, T* c, int ldc,
+              Part part, Tri tri = kTriNone) {
+  if constexpr (sizeof(T) == 8) {
+    Dgemm(m, n, k, alpha, a, b, beta, c, ldc, part, tri);
+  } else {
+    Sgemm(m, n, k, alpha, a, b, beta, c, ldc, part, tri);
+  }
+}
+
+// out (n x n, leading dimension ldo) := the symmetric matrix whose `lower`
+// (or upper) triangle is stored in a; the other triangle of a is not read.
+template <typename T>
+__global__ void SymmetrizeFullKernel(int n, const T* a, long long lda, bool lower, T* out,
+                                     long long ldo) {
+  const long long total = static_cast<long long>(n) * n;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    const bool stored = lower ? i >= j : i <= j;
+    out[i + j * ldo] = stored ? a[i + j * lda] : a[j + i * lda];
+  }
+}
+
+// out (n x n) := the triangle `lower` of a with explicit zeros in the other
+// one and ones on the diagonal when `unit` (the values the reference packs for
+// a triangular operand, src/pack-inl.h:99-160); the rest of a is not read.
+template <typename T>
+__global__ void TriangleFullKernel(int n, const T* a, long long lda, bool lower, bool unit,
+                                   T* out, long long ldo) {
+  const long long total = static_cast<long long>(n) * n;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    T v = T(0);
+    if (i == j) v = unit ? T(1) : a[i + j * lda];
+    else if (lower ? i > j : i < j) v = a[i + j * lda];
+    out[i + j * ldo] = v;
+  }
+}
+
+int GridFor(long long total) {
+  return static_cast<int>(std::min<long long>((total + 255) / 256, 8192));
+}
+
+}  // namespace
+
+// SYMM: the reference packs the stored triangle mirrored (Structure::
+// kSymmetric, src/pack-inl.h:99-160), i.e. the values of the full symmetric
+// matrix; here that matrix is formed once and the plain GEMM runs on it, so
+// every element's chain is the GEMM's (src/level3.cc:26-82).
+template <typename T>
+void SymmFull(bool left, bool lower, int m, int n, T alpha, const T* a, int lda, const T* b,
+              int ldb, T beta, T* c, int ldc) {
+  if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return;
+  if (alpha == T(0)) {
+    ScaleMatrix<T>(m, n, beta, c, ldc, kAll);
+    return;
+  }
+  const int ka = left ? m : n;
+  T* full = static_cast<T*>(Workspace(kWsLevel3, sizeof(T) * static_cast<size_t>(ka) * ka));
+  if (full == nullptr) return;
+  SymmetrizeFullKernel<T><<<GridFor(static_cast<long long>(ka) * ka), 256, 0, Ctx().stream>>>(
+      ka, a, lda, lower, full, ka);
+  CountLaunch();
+  if (LaunchFailed("symm symmetrize")) return;
+  const View<T> sym = ColMajor<T>(full, ka), gen = ColMajor<T>(b, ldb);
+  GemmPart<T>(m, n, ka, alpha, left ? sym : gen, left ? gen : sym, beta, c, ldc, kAll);
+}
+template void SymmFull<double>(bool, bool, int, int, double, const double*, int,
+                               const double*, int, double, double*, int);
+template void SymmFull<float>(bool, bool, int, int, float, const float*, int, const float*,
+                              int, float, float*, int);
+
+// SYR2K: alpha op(A) op(B)^T + beta C, then + alpha op(B) op(A)^T (beta 1),
+// each a GEMM problem on the uplo triangle (src/level3.cc:153-221).
+template <typename T>
+void Syr2kFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda,
+               const T* b, int ldb, T beta, T* c, int ldc) {
+  const Part part = lower ? kLower : kUpper;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
+    return;
+  }
+  GemmPart<T>(n, n, k, alpha, ColMajor<T>(a, lda, trans), ColMajor<T>(b, ldb, !trans), beta,
+              c, ldc, part);
+  GemmPart<T>(n, n, k, alpha, ColMajor<T>(b, ldb, trans), ColMajor<T>(a, lda, !trans), T(1),
+              c, ldc, part);
+}
+template void Syr2kFull<double>(bool, bool, int, int, double, const double*, int,
+                                const double*, int, double, double*, int);
+template void Syr2kFull<float>(bool, bool, int, int, float, const float*, int, const float*,
+                               int, float, float*, int);
+
+// GEMMTR: op(A) (n x k) op(B) (k x n) on the uplo triangle of C
+// (src/level3.cc:226-280).
+template <typename T>
+void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
+                const T* b, int ldb, T beta, T* c, int ldc) {
+  const Part part = lower ? kLower : kUpper;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
+    return;
+  }
+  GemmPart<T>(n, n, k, alpha, ColMajor<T>(a, lda, ta), ColMajor<T>(b, ldb, tb), beta, c, ldc,
+              part);
+}
+template void GemmtrFull<double>(bool, bool, bool, int, int, double, const double*, int,
+                                 const double*, int, double, double*, int);
+template void GemmtrFull<float>(bool, bool, bool, int, int, float, const float*, int,
+                                const float*, int, float, float*, int);
+
+// TRMM: B := alpha op(A) B (left) or alpha B op(A), computed from a copy of B
+// with beta 0 (src/level3.cc:284-342). The triangle is stored out with its
+// zeros and unit diagonal, and the GEMM multiplies only the k range of each
+// reference micro-tile, so every element is the reference's chain.
+template <typename T>
+void TrmmFull(bool left, bool lower, bool trans, bool unit, int m, int n, T alpha,
+              const T* a, int lda, T* b, int ldb) {
+  if (m == 0 || n == 0) return;
+  if (alpha == T(0)) {
+    ScaleMatrix<T>(m, n, T(0), b, ldb, kAll);
+    return;
+  }
+  const int ka = left ? m : n;
+  T* tri = static_cast<T*>(Workspace(kWsLevel3, sizeof(T) * static_cast<size_t>(ka) * ka));
+  T* copy = static_cast<T*>(Workspace(kWsLevel3Copy, sizeof(T) * static_cast<size_t>(m) * n));
+  if (tri == nullptr || copy == nullptr) return;
+  TriangleFullKernel<T><<<GridFor(static_cast<long long>(ka) * ka), 256, 0, Ctx().stream>>>(
+      ka, a, lda, lower, unit, tri, ka);
+  CountLaunch();
+  if (LaunchFailed("trmm triangle")) return;
+  if (Failed(cudaMemcpy2DAsync(copy, sizeof(T) * m, b, sizeof(T) * ldb, sizeof(T) * m, n,
+                               cudaMemcpyDeviceToDevice, Ctx().stream),
+             "trmm copy"))
+    return;
+  // op(A) is lower exactly when A is lower and not transposed, or upper and
+  // transposed (src/api.h:133-140).
+  const bool op_lower = (lower != trans);
+  const View<T> t = ColMajor<T>(tri, ka, trans), g = ColMajor<T>(copy, m);
+  if (left) {
+    GemmPart<T>(m, n, ka, alpha, t, g, T(0), b, ldb, kAll, op_lower ? kTriALower : kTriAUpper);
+  } else {
+    GemmPart<T>(m, n, ka, alpha, g, t, T(0), b, ldb, kAll, op_lower ? kTriBLower : kTriBUpper);
+  }
+}
+template void TrmmFull<double>(bool, bool, bool, bool, int, int, double, const double*, int,
+                               double*, int);
+template void TrmmFull<float>(bool, bool, bool, bool, int, int, float, const float*, int,
+                              float*, int);
 
 // Gemm (src/gemm.cc:114-131) after argument checks.
 template <typename T>

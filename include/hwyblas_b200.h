@@ -83,6 +83,62 @@ HWYBLAS_API void ssyrk_(const char* uplo, const char* trans,
                         const float* alpha, const float* a,
                         const hwyblas_int* lda, const float* beta, float* c,
                         const hwyblas_int* ldc);
+/* C := alpha*A*B + beta*C (side L) or alpha*B*A + beta*C (side R), A
+ * symmetric with only the uplo triangle read. Replace dsymm_ / ssymm_
+ * (include/hwyblas/hwyblas.h:597, 591; src/level3.cc:369-375, 362-368). */
+HWYBLAS_API void dsymm_(const char* side, const char* uplo, const hwyblas_int* m,
+                        const hwyblas_int* n, const double* alpha, const double* a,
+                        const hwyblas_int* lda, const double* b, const hwyblas_int* ldb,
+                        const double* beta, double* c, const hwyblas_int* ldc);
+HWYBLAS_API void ssymm_(const char* side, const char* uplo, const hwyblas_int* m,
+                        const hwyblas_int* n, const float* alpha, const float* a,
+                        const hwyblas_int* lda, const float* b, const hwyblas_int* ldb,
+                        const float* beta, float* c, const hwyblas_int* ldc);
+/* C := alpha*A*B**T + alpha*B*A**T + beta*C (trans N) or with A**T*B and
+ * B**T*A, on the uplo triangle. Replace dsyr2k_ / ssyr2k_
+ * (include/hwyblas/hwyblas.h:674, 668; src/level3.cc:463-469, 456-462). */
+HWYBLAS_API void dsyr2k_(const char* uplo, const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* k, const double* alpha, const double* a,
+                         const hwyblas_int* lda, const double* b, const hwyblas_int* ldb,
+                         const double* beta, double* c, const hwyblas_int* ldc);
+HWYBLAS_API void ssyr2k_(const char* uplo, const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* k, const float* alpha, const float* a,
+                         const hwyblas_int* lda, const float* b, const hwyblas_int* ldb,
+                         const float* beta, float* c, const hwyblas_int* ldc);
+/* C := alpha*op(A)*op(B) + beta*C on the uplo triangle of the n x n C.
+ * Replace dgemmtr_ / sgemmtr_ and the alias names dgemmt_ / sgemmt_
+ * (include/hwyblas/hwyblas.h:717, 711, 743, 737; src/level3.cc:508-560). */
+HWYBLAS_API void dgemmtr_(const char* uplo, const char* transa, const char* transb,
+                          const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                          const double* a, const hwyblas_int* lda, const double* b,
+                          const hwyblas_int* ldb, const double* beta, double* c,
+                          const hwyblas_int* ldc);
+HWYBLAS_API void sgemmtr_(const char* uplo, const char* transa, const char* transb,
+                          const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                          const float* a, const hwyblas_int* lda, const float* b,
+                          const hwyblas_int* ldb, const float* beta, float* c,
+                          const hwyblas_int* ldc);
+HWYBLAS_API void dgemmt_(const char* uplo, const char* transa, const char* transb,
+                         const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                         const double* a, const hwyblas_int* lda, const double* b,
+                         const hwyblas_int* ldb, const double* beta, double* c,
+                         const hwyblas_int* ldc);
+HWYBLAS_API void sgemmt_(const char* uplo, const char* transa, const char* transb,
+                         const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                         const float* a, const hwyblas_int* lda, const float* b,
+                         const hwyblas_int* ldb, const float* beta, float* c,
+                         const hwyblas_int* ldc);
+/* B := alpha*op(A)*B (side L) or alpha*B*op(A), A triangular (unit diagonal
+ * not read when diag U). Replace dtrmm_ / strmm_ (include/hwyblas/hwyblas.h:769,
+ * 764; src/level3.cc:587-592, 581-586). */
+HWYBLAS_API void dtrmm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const double* alpha, const double* a, const hwyblas_int* lda,
+                        double* b, const hwyblas_int* ldb);
+HWYBLAS_API void strmm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const float* alpha, const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb);
 /* 1-based index of the first element of largest |x| (0 if n < 1 or
  * incx <= 0). Replaces idamax_ (include/hwyblas/hwyblas.h:169,
  * src/level1.cc:895-897). */
@@ -351,6 +407,64 @@ HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
                              const hwyblas_int n, const float alpha,
                              const float* a, const hwyblas_int lda, float* b,
                              const hwyblas_int ldb);
+/* CBLAS forms of the level-3 routines above, both layouts, CBLAS argument
+ * positions in error reports (include/hwyblas/cblas.h:835, 828 trmm; 714, 708
+ * symm; 791, 784 syr2k; 649, 641 gemmtr; 683, 675 gemmt; src/cblas.cc:
+ * 1631-1700, 1727-1746, 1842-1861, 1908-1927). */
+HWYBLAS_API void cblas_dtrmm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const double alpha, const double* a, const hwyblas_int lda,
+                             double* b, const hwyblas_int ldb);
+HWYBLAS_API void cblas_strmm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const float alpha, const float* a, const hwyblas_int lda,
+                             float* b, const hwyblas_int ldb);
+HWYBLAS_API void cblas_dsymm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const hwyblas_int m, const hwyblas_int n,
+                             const double alpha, const double* a, const hwyblas_int lda,
+                             const double* b, const hwyblas_int ldb, const double beta,
+                             double* c, const hwyblas_int ldc);
+HWYBLAS_API void cblas_ssymm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const hwyblas_int m, const hwyblas_int n,
+                             const float alpha, const float* a, const hwyblas_int lda,
+                             const float* b, const hwyblas_int ldb, const float beta,
+                             float* c, const hwyblas_int ldc);
+HWYBLAS_API void cblas_dsyr2k(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                              const CBLAS_TRANSPOSE trans, const hwyblas_int n,
+                              const hwyblas_int k, const double alpha, const double* a,
+                              const hwyblas_int lda, const double* b, const hwyblas_int ldb,
+                              const double beta, double* c, const hwyblas_int ldc);
+HWYBLAS_API void cblas_ssyr2k(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                              const CBLAS_TRANSPOSE trans, const hwyblas_int n,
+                              const hwyblas_int k, const float alpha, const float* a,
+                              const hwyblas_int lda, const float* b, const hwyblas_int ldb,
+                              const float beta, float* c, const hwyblas_int ldc);
+HWYBLAS_API void cblas_dgemmtr(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                               const CBLAS_TRANSPOSE transa, const CBLAS_TRANSPOSE transb,
+                               const hwyblas_int n, const hwyblas_int k, const double alpha,
+                               const double* a, const hwyblas_int lda, const double* b,
+                               const hwyblas_int ldb, const double beta, double* c,
+                               const hwyblas_int ldc);
+HWYBLAS_API void cblas_sgemmtr(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                               const CBLAS_TRANSPOSE transa, const CBLAS_TRANSPOSE transb,
+                               const hwyblas_int n, const hwyblas_int k, const float alpha,
+                               const float* a, const hwyblas_int lda, const float* b,
+                               const hwyblas_int ldb, const float beta, float* c,
+                               const hwyblas_int ldc);
+HWYBLAS_API void cblas_dgemmt(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                              const CBLAS_TRANSPOSE transa, const CBLAS_TRANSPOSE transb,
+                              const hwyblas_int n, const hwyblas_int k, const double alpha,
+                              const double* a, const hwyblas_int lda, const double* b,
+                              const hwyblas_int ldb, const double beta, double* c,
+                              const hwyblas_int ldc);
+HWYBLAS_API void cblas_sgemmt(const CBLAS_LAYOUT layout, const CBLAS_UPLO uplo,
+                              const CBLAS_TRANSPOSE transa, const CBLAS_TRANSPOSE transb,
+                              const hwyblas_int n, const hwyblas_int k, const float alpha,
+                              const float* a, const hwyblas_int lda, const float* b,
+                              const hwyblas_int ldb, const float beta, float* c,
+                              const hwyblas_int ldc);
 /* 0-based (include/hwyblas/cblas.h:128, src/cblas.cc:845). */
 HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
                                      const hwyblas_int incx);

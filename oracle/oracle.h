@@ -69,6 +69,24 @@ int orc_sposv(char uplo, int n, int nrhs, float* a, int lda, float* b, int ldb);
 int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
               int ldb);
 
+/* Level 3 through the GEMM problem model (src/level3.cc:26-342). */
+int orc_dsymm(char side, char uplo, int m, int n, double alpha, const double* a, int lda,
+              const double* b, int ldb, double beta, double* c, int ldc);
+int orc_ssymm(char side, char uplo, int m, int n, float alpha, const float* a, int lda,
+              const float* b, int ldb, float beta, float* c, int ldc);
+int orc_dsyr2k(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+               const double* b, int ldb, double beta, double* c, int ldc);
+int orc_ssyr2k(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+               const float* b, int ldb, float beta, float* c, int ldc);
+int orc_dgemmtr(char uplo, char ta, char tb, int n, int k, double alpha, const double* a,
+                int lda, const double* b, int ldb, double beta, double* c, int ldc);
+int orc_sgemmtr(char uplo, char ta, char tb, int n, int k, float alpha, const float* a,
+                int lda, const float* b, int ldb, float beta, float* c, int ldc);
+int orc_dtrmm(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+              const double* a, int lda, double* b, int ldb);
+int orc_strmm(char side, char uplo, char transa, char diag, int m, int n, float alpha,
+              const float* a, int lda, float* b, int ldb);
+
 /* Leaves, exposed for the known-answer tests. */
 int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv);
 int orc_dpotrf_leaf(int upper, int n, double* a, int lda);

@@ -434,6 +434,186 @@ int SyrkD(char uplo, char trans, int n, int k, double alpha, const double* a, in
 }
 
 // ---------------------------------------------------------------------------
+// SYMM (src/level3.cc:26-76): the reference packs the stored triangle
+// mirrored (Structure::kSymmetric, src/pack-inl.h:99-160), i.e. the values of
+// the full symmetric matrix; the other triangle is never read.
+template <typename T>
+int Symm(char side, char uplo, int m, int n, T alpha, const T* a, int lda, const T* b,
+         int ldb, T beta, T* c, int ldc) {
+  const char s = Up(side), u = Up(uplo);
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const bool left = (s == 'L'), lower = (u == 'L');
+  const int ka = left ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (lda < std::max(1, ka)) info = 7;
+  else if (ldb < std::max(1, m)) info = 9;
+  else if (ldc < std::max(1, m)) info = 12;
+  if (info) return info;
+  if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return 0;
+  if (alpha == T(0)) {
+    ScaleMatrix<T>(m, n, beta, c, ldc, kAll);
+    return 0;
+  }
+  std::vector<T> full(static_cast<size_t>(ka) * ka);
+  for (int j = 0; j < ka; ++j)
+    for (int i = 0; i < ka; ++i) {
+      const bool stored = lower ? (i >= j) : (i <= j);
+      full[i + static_cast<size_t>(j) * ka] =
+          stored ? a[i + static_cast<ptrdiff_t>(j) * lda] : a[j + static_cast<ptrdiff_t>(i) * lda];
+    }
+  const Opnd<T> sym = General(false, full.data(), ka);
+  const Opnd<T> gen = General(false, b, ldb);
+  Gemm<T>(m, n, ka, alpha, left ? sym : gen, left ? gen : sym, beta, c, ldc, kAll);
+  return 0;
+}
+
+// SYR2K (src/level3.cc:153-221): alpha op(A) op(B)^T + beta C, then
+// + alpha op(B) op(A)^T with beta 1, each a GEMM problem on the uplo triangle.
+template <typename T>
+int Syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, int lda, const T* b,
+          int ldb, T beta, T* c, int ldc) {
+  const char u = Up(uplo);
+  bool t;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool vt = DecodeOp(trans, &t);
+  const int rows = t ? k : n;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!vt) info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, rows)) info = 7;
+  else if (ldb < std::max(1, rows)) info = 9;
+  else if (ldc < std::max(1, n)) info = 12;
+  if (info) return info;
+  const Part part = (u == 'L') ? kLower : kUpper;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return 0;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
+    return 0;
+  }
+  Gemm<T>(n, n, k, alpha, General(t, a, lda), General(!t, b, ldb), beta, c, ldc, part);
+  Gemm<T>(n, n, k, alpha, General(t, b, ldb), General(!t, a, lda), T(1), c, ldc, part);
+  return 0;
+}
+
+// GEMMTR and its alias GEMMT (src/level3.cc:226-280): op(A) n x k times
+// op(B) k x n on the uplo triangle of C.
+template <typename T>
+int Gemmtr(char uplo, char transa, char transb, int n, int k, T alpha, const T* a, int lda,
+           const T* b, int ldb, T beta, T* c, int ldc) {
+  const char u = Up(uplo);
+  bool ta, tb;
+  const bool vu = (u == 'L' || u == 'U');
+  const bool va = DecodeOp(transa, &ta), vb = DecodeOp(transb, &tb);
+  const int rows_a = ta ? k : n, rows_b = tb ? n : k;
+  int info = 0;
+  if (!vu) info = 1;
+  else if (!va) info = 2;
+  else if (!vb) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, n)) info = 13;
+  if (info) return info;
+  const Part part = (u == 'L') ? kLower : kUpper;
+  if (n == 0 || ((alpha == T(0) || k == 0) && beta == T(1))) return 0;
+  if (alpha == T(0) || k == 0) {
+    ScaleMatrix<T>(n, n, beta, c, ldc, part);
+    return 0;
+  }
+  Gemm<T>(n, n, k, alpha, General(ta, a, lda), General(tb, b, ldb), beta, c, ldc, part);
+  return 0;
+}
+
+// TRMM (src/level3.cc:284-342), element by element: B(i, j) is the GEMM
+// problem's chain over the k range that the reference multiplies for the
+// micro-tile holding (i, j) (NonZeroRange, src/gemm-inl.h:62-85), restarted
+// every KC; a chunk outside that range is skipped, except the first, which
+// still applies beta = 0 (src/gemm-inl.h:176-209). The triangular operand has
+// explicit zeros outside its triangle and ones on a unit diagonal
+// (src/pack-inl.h:99-160); op(A) is lower when A is lower xor transposed
+// (src/api.h:133-140). B is read from a copy of its input.
+template <typename T>
+int Trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
+         int lda, T* b, int ldb) {
+  const char s = Up(side), u = Up(uplo), d = Up(diag);
+  bool trans;
+  const bool vs = (s == 'L' || s == 'R'), vu = (u == 'L' || u == 'U');
+  const bool vt = DecodeOp(transa, &trans), vd = (d == 'U' || d == 'N');
+  const bool left = (s == 'L'), lower = (u == 'L'), unit = (d == 'U');
+  const int ka = left ? m : n;
+  int info = 0;
+  if (!vs) info = 1;
+  else if (!vu) info = 2;
+  else if (!vt) info = 3;
+  else if (!vd) info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, ka)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info) return info;
+  if (m == 0 || n == 0) return 0;
+  if (alpha == T(0)) {
+    ScaleMatrix<T>(m, n, T(0), b, ldb, kAll);
+    return 0;
+  }
+  const size_t K = static_cast<size_t>(ka);
+  std::vector<T> tri(K * K);  // op(A), dense
+  for (int j = 0; j < ka; ++j)
+    for (int i = 0; i < ka; ++i) {
+      T v = T(0);
+      if (i == j) v = unit ? T(1) : a[i + static_cast<ptrdiff_t>(i) * lda];
+      else if (lower ? i > j : i < j) v = a[i + static_cast<ptrdiff_t>(j) * lda];
+      if (trans) tri[j + i * K] = v;
+      else tri[i + j * K] = v;
+    }
+  std::vector<T> copy(static_cast<size_t>(m) * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i)
+      copy[i + static_cast<size_t>(j) * m] = b[i + static_cast<ptrdiff_t>(j) * ldb];
+  const bool op_lower = (lower != trans);
+  const RefTiles<T> t;
+  constexpr size_t KC = KcOf<T>();
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      const size_t ic = i / t.mc * t.mc, mcb = std::min(t.mc, m - ic);
+      const size_t ir = (i - ic) / t.mr * t.mr, mr = std::min(t.mr, mcb - ir);
+      const size_t jc = j / t.nc * t.nc, ncb = std::min(t.nc, n - jc);
+      const size_t jr = (j - jc) / t.nr * t.nr, nr = std::min(t.nr, ncb - jr);
+      const size_t i0 = ic + ir, j0 = jc + jr;
+      size_t kb = 0, ke = K;
+      if (left) {
+        if (op_lower) ke = std::min(ke, i0 + mr);
+        else kb = i0;
+      } else {
+        if (op_lower) kb = j0;
+        else ke = std::min(ke, j0 + nr);
+      }
+      T cv = T(0);
+      for (size_t pc = 0; pc < K; pc += KC) {
+        const size_t lo = std::max(kb, pc), hi = std::max(lo, std::min(ke, pc + KC));
+        if (lo == hi && pc != 0) continue;
+        T acc = T(0);
+        for (size_t q = lo; q < hi; ++q) {
+          const T av = left ? tri[i + q * K] : copy[i + q * m];
+          const T bv = left ? copy[q + static_cast<size_t>(j) * m] : tri[q + j * K];
+          acc = std::fma(av, bv, acc);
+        }
+        cv = (pc == 0) ? Merge(acc, alpha, T(0), T(0), false)
+                       : Merge(acc, alpha, T(1), cv, false);
+      }
+      b[i + static_cast<ptrdiff_t>(j) * ldb] = cv;
+    }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // IAMAX (src/level1.cc:383-402; src/level1-inl.h:343-423): 1-based index of
 // the first element of largest |x|; NaNs never compare larger, so one is only
 // returned when it is x[0].
@@ -506,6 +686,27 @@ int orc_ssyrk(char uplo, char trans, int n, int k, float alpha, const float* a, 
               float beta, float* c, int ldc) {
   return orc::Syrk<float>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
 }
+#define ORC_L3(P, T)                                                                       \
+  int orc_##P##symm(char side, char uplo, int m, int n, T alpha, const T* a, int lda,       \
+                    const T* b, int ldb, T beta, T* c, int ldc) {                            \
+    return orc::Symm<T>(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);             \
+  }                                                                                          \
+  int orc_##P##syr2k(char uplo, char trans, int n, int k, T alpha, const T* a, int lda,     \
+                     const T* b, int ldb, T beta, T* c, int ldc) {                           \
+    return orc::Syr2k<T>(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);           \
+  }                                                                                          \
+  int orc_##P##gemmtr(char uplo, char ta, char tb, int n, int k, T alpha, const T* a,       \
+                      int lda, const T* b, int ldb, T beta, T* c, int ldc) {                 \
+    return orc::Gemmtr<T>(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, beta, c, ldc);         \
+  }                                                                                          \
+  int orc_##P##trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha,    \
+                    const T* a, int lda, T* b, int ldb) {                                    \
+    return orc::Trmm<T>(side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb);             \
+  }
+ORC_L3(d, double)
+ORC_L3(s, float)
+#undef ORC_L3
+
 int orc_idamax(int n, const double* x, int incx) {
   return orc::Iamax<double>(n, x, incx);
 }

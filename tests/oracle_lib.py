@@ -86,6 +86,12 @@ class Oracle:
         L.orc_spotrs.argtypes = [CH, I, I, P, I, P, I]
         L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
         L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
+        for pre, S in (("d", D), ("s", F)):
+            getattr(L, f"orc_{pre}symm").argtypes = [CH, CH, I, I, S, P, I, P, I, S, P, I]
+            getattr(L, f"orc_{pre}syr2k").argtypes = [CH, CH, I, I, S, P, I, P, I, S, P, I]
+            getattr(L, f"orc_{pre}gemmtr").argtypes = [CH, CH, CH, I, I, S, P, I, P, I, S, P,
+                                                        I]
+            getattr(L, f"orc_{pre}trmm").argtypes = [CH, CH, CH, CH, I, I, S, P, I, P, I]
         L.orc_set_lanes(8)
 
     def set_threads(self, n):
@@ -168,6 +174,23 @@ class Oracle:
     def ssyrk(self, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
         return self.lib.orc_ssyrk(_b(uplo), _b(trans), n, k, alpha, ptr(a), lda, beta,
                                   ptr(c), ldc)
+
+    # Level 3 through the GEMM problem model; p is "d" or "s".
+    def symm(self, p, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc):
+        return getattr(self.lib, f"orc_{p}symm")(_b(side), _b(uplo), m, n, alpha, ptr(a), lda,
+                                                 ptr(b), ldb, beta, ptr(c), ldc)
+
+    def syr2k(self, p, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+        return getattr(self.lib, f"orc_{p}syr2k")(_b(uplo), _b(trans), n, k, alpha, ptr(a),
+                                                  lda, ptr(b), ldb, beta, ptr(c), ldc)
+
+    def gemmtr(self, p, uplo, ta, tb, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+        return getattr(self.lib, f"orc_{p}gemmtr")(_b(uplo), _b(ta), _b(tb), n, k, alpha,
+                                                   ptr(a), lda, ptr(b), ldb, beta, ptr(c), ldc)
+
+    def trmm(self, p, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+        return getattr(self.lib, f"orc_{p}trmm")(_b(side), _b(uplo), _b(transa), _b(diag), m,
+                                                 n, alpha, ptr(a), lda, ptr(b), ldb)
 
     def dposv(self, uplo, n, nrhs, a, lda, b, ldb):
         return self.lib.orc_dposv(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)

@@ -246,7 +246,9 @@ def test_cblas_dtrsm_row_major(hb, orc):
 @pytest.mark.parametrize("uplo", ["L", "U"])
 @pytest.mark.parametrize("trans", ["N", "T"])
 @pytest.mark.parametrize("n,k", [(1, 1), (30, 10), (100, 300), (257, 64)])
-@pytest.mark.parametrize("beta", [0.0, 1.0, 0.5])
+# beta 0.3: beta*C is inexact, so the crossing-tile merge alpha*acc + beta*C
+# (two roundings) differs from fma(C, beta, alpha*acc).
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.5, 0.3])
 def test_dsyrk_bitexact(hb, orc, uplo, trans, n, k, beta):
     rng = np.random.default_rng(n + k)
     ra, ca = (n, k) if trans == "N" else (k, n)

@@ -377,6 +377,224 @@ def test_syrk_elementwise_bound(orc, dtype, uplo, trans):
     assert np.array_equal(c1[~tri], c[~tri])
 
 
+def _structured(rng, n, ld, uplo, dtype, diag="G"):
+    """n x n matrix (leading dimension ld) with NaN wherever the routine must
+    not read: the other triangle, the padding and, for a unit diagonal, the
+    diagonal (tests/test_util.h:274-304)."""
+    a = np.full((ld, n), np.nan, dtype=dtype, order="F")
+    for j in range(n):
+        for i in range(n):
+            if (i > j) if uplo == "L" else (i < j):
+                a[i, j] = rng.uniform(-1, 1)
+        if diag == "N":
+            a[j, j] = (1.5 if rng.uniform() >= 0.5 else -1.5) + 0.5 * rng.uniform(-1, 1)
+        elif diag == "G":
+            a[j, j] = rng.uniform(-1, 1)
+    return a
+
+
+def _dense(a, n, uplo, kind):
+    """The dense matrix a structured argument stands for: symmetric ("S"),
+    triangular ("N") or unit triangular ("U")."""
+    t = np.array(a[:n, :n], dtype=np.float64)
+    low = np.tril(np.ones((n, n), bool), -1)
+    keep = low if uplo == "L" else low.T
+    d = np.where(keep, t, 0.0)
+    if kind == "S":
+        return d + d.T + np.diag(np.diag(t))
+    return d + (np.eye(n) if kind == "U" else np.diag(np.diag(t)))
+
+
+def _within(got, want, bound, tol):
+    return np.all(np.abs(got.astype(np.float64) - want) <= tol * bound + 1e-300)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("m,n", [(1, 7), (13, 40), (100, 7), (300, 40)])
+def test_symm_bound(orc, dtype, side, uplo, m, n):
+    """SYMM within 4(ka+2)eps of the exact product, reading only the stored
+    triangle; beta = 0 does not read C (tests/level3_test.cc:33-89)."""
+    p = "s" if dtype == np.float32 else "d"
+    rng = np.random.default_rng(m * 7 + n)
+    ka = m if side == "L" else n
+    lda, ldb, ldc = ka + 2, m + 1, m + 3
+    a = _structured(rng, ka, lda, uplo, dtype)
+    b = rand(rng, ldb, n, dtype)
+    A, B = _dense(a, ka, uplo, "S"), b[:m].astype(np.float64)
+    for alpha, beta in [(1.5, 0.5), (-1.0, 0.0)]:
+        c = rand(rng, ldc, n, dtype)
+        if beta == 0.0:
+            c[:] = np.nan
+        c0 = c[:m].astype(np.float64)
+        prod = A @ B if side == "L" else B @ A
+        aprod = np.abs(A) @ np.abs(B) if side == "L" else np.abs(B) @ np.abs(A)
+        want = alpha * prod + (beta * c0 if beta != 0 else 0.0)
+        bound = abs(alpha) * aprod + (abs(beta) * np.abs(c0) if beta != 0 else 0.0)
+        assert orc.symm(p, side, uplo, m, n, dtype(alpha), a, lda, b, ldb, dtype(beta), c,
+                        ldc) == 0
+        assert _within(c[:m], want, bound, 4 * (ka + 2) * np.finfo(dtype).eps)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("n,k", [(1, 3), (37, 13), (100, 300)])
+def test_syr2k_gemmtr_bound(orc, dtype, uplo, trans, n, k):
+    """SYR2K within 4(2k+2)eps and GEMMTR within 4(k+2)eps on the uplo
+    triangle, the other triangle untouched, beta = 0 not reading C
+    (tests/level3_test.cc:150-200, 300-360)."""
+    p = "s" if dtype == np.float32 else "d"
+    rng = np.random.default_rng(n * 31 + k)
+    rows, cols = (n, k) if trans == "N" else (k, n)
+    lda = ldb = rows + 1
+    ldc = n + 2
+    a, b = rand(rng, lda, cols, dtype), rand(rng, ldb, cols, dtype)
+    A, B = a[:rows].astype(np.float64), b[:rows].astype(np.float64)
+    opA, opB = (A, B) if trans == "N" else (A.T, B.T)
+    tri = np.tril(np.ones((n, n), bool)) if uplo == "L" else np.triu(np.ones((n, n), bool))
+    eps = np.finfo(dtype).eps
+    for alpha, beta in [(0.75, -0.5), (-1.25, 0.0)]:
+        c = rand(rng, ldc, n, dtype)
+        if beta == 0.0:
+            c[:n][tri] = np.nan
+        c0 = c.copy(order="F")
+        cc = c0[:n].astype(np.float64)
+        bc = beta * cc if beta != 0 else 0.0
+        abc = abs(beta) * np.abs(cc) if beta != 0 else 0.0
+        want = alpha * (opA @ opB.T + opB @ opA.T) + bc
+        bound = abs(alpha) * (np.abs(opA) @ np.abs(opB.T) + np.abs(opB) @ np.abs(opA.T)) + abc
+        assert orc.syr2k(p, uplo, trans, n, k, dtype(alpha), a, lda, b, ldb, dtype(beta), c,
+                         ldc) == 0
+        assert _within(c[:n][tri], want[tri], bound[tri], 4 * (2 * k + 2) * eps)
+        assert same_bits(c[:n][~tri], c0[:n][~tri])
+        # GEMMTR with op(B) = B^T for trans N (and the mirror for T).
+        ta, tb = trans, ("T" if trans == "N" else "N")
+        c = c0.copy(order="F")
+        want = alpha * (opA @ opB.T) + bc
+        bound = abs(alpha) * (np.abs(opA) @ np.abs(opB.T)) + abc
+        assert orc.gemmtr(p, uplo, ta, tb, n, k, dtype(alpha), a, lda, b, ldb, dtype(beta), c,
+                          ldc) == 0
+        assert _within(c[:n][tri], want[tri], bound[tri], 4 * (k + 2) * eps)
+        assert same_bits(c[:n][~tri], c0[:n][~tri])
+
+
+TRI_CASES = [(s, u, t, d) for s in "LR" for u in "LU" for t in "NT" for d in "NU"]
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("side,uplo,trans,diag", TRI_CASES)
+def test_trmm_bound(orc, dtype, side, uplo, trans, diag):
+    """TRMM within 4(ka+2)eps of the exact product for every side, uplo,
+    trans and diag, never reading the other triangle or a unit diagonal
+    (tests/level3_test.cc:417-475)."""
+    p = "s" if dtype == np.float32 else "d"
+    eps = np.finfo(dtype).eps
+    for m, n in [(1, 19), (37, 19), (300, 19), (11, 5), (11, 300)]:
+        rng = np.random.default_rng(m * 100 + n)
+        ka = m if side == "L" else n
+        lda, ldb = ka + 1, m + 2
+        a = _structured(rng, ka, lda, uplo, dtype, diag)
+        b = rand(rng, ldb, n, dtype)
+        T = _dense(a, ka, uplo, diag)
+        op = T if trans == "N" else T.T
+        B = b[:m].astype(np.float64)
+        alpha = 1.5
+        want = alpha * (op @ B if side == "L" else B @ op)
+        bound = alpha * (np.abs(op) @ np.abs(B) if side == "L" else np.abs(B) @ np.abs(op))
+        pad = b[m:].copy()
+        assert orc.trmm(p, side, uplo, trans, diag, m, n, dtype(alpha), a, lda, b, ldb) == 0
+        assert _within(b[:m], want, bound, 4 * (ka + 2) * eps), (m, n)
+        assert same_bits(b[m:], pad)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("side,uplo,trans,diag", TRI_CASES)
+def test_trmm_is_the_gemm_chain(orc, dtype, side, uplo, trans, diag):
+    """For finite data the per-micro-tile k range only drops products with a
+    structural zero, so TRMM equals the GEMM problem on the explicit triangle
+    bit for bit (src/gemm-inl.h:62-85, 202-209), chunk boundaries included."""
+    p = "s" if dtype == np.float32 else "d"
+    m, n = (700, 45) if side == "L" else (45, 700)
+    rng = np.random.default_rng(5)
+    ka = m if side == "L" else n
+    a = _structured(rng, ka, ka, uplo, dtype, diag)
+    b = rand(rng, m, n, dtype)
+    T = np.asfortranarray(_dense(a, ka, uplo, diag).astype(dtype))
+    b1, c = b.copy(order="F"), np.zeros((m, n), dtype, order="F")
+    assert orc.trmm(p, side, uplo, trans, diag, m, n, dtype(-0.5), a, ka, b1, m) == 0
+    gemm = orc.sgemm if dtype == np.float32 else orc.dgemm
+    if side == "L":
+        gemm(trans, "N", m, n, ka, dtype(-0.5), T, ka, b, m, dtype(0), c, m)
+    else:
+        gemm("N", trans, m, n, ka, dtype(-0.5), b, m, T, ka, dtype(0), c, m)
+    assert same_bits(b1, c), first_diff(b1, c)
+
+
+def test_trmm_micro_tile_ranges_known_answer(orc):
+    """The reference multiplies the whole k range of a micro-tile, structural
+    zeros included (src/gemm-inl.h:62-85, 202-215): with B(20, :) infinite, a
+    lower op(A) (micro-tiles of 16 rows) gives finite rows 0-15, NaN rows
+    16-19 (0 * inf inside tile [16, 32)) and infinite or NaN rows 20 on."""
+    m, n = 40, 3
+    a = np.asfortranarray(np.tril(np.full((m, m), 0.5)))
+    b = np.ones((m, n), order="F")
+    b[20, :] = np.inf
+    assert orc.trmm("d", "L", "L", "N", "N", m, n, 1.0, a, m, b, m) == 0
+    assert np.all(np.isfinite(b[:16]))
+    assert np.all(np.isnan(b[16:20]))
+    assert not np.any(np.isfinite(b[20:]))
+    # Right side, lower op(A): column tiles of 12 take k from their first
+    # column on, so a non-finite B(:, 5) reaches columns 0-11 only.
+    b = np.ones((n, m), order="F")
+    b[:, 5] = np.inf
+    assert orc.trmm("d", "R", "L", "N", "N", n, m, 1.0, a, m, b, n) == 0
+    assert not np.any(np.isfinite(b[:, :6]))
+    assert np.all(np.isnan(b[:, 6:12]))
+    assert np.all(np.isfinite(b[:, 12:]))
+
+
+def test_level3_quick_returns_and_errors(orc):
+    """Argument checks (INFO positions) and quick returns of SYMM, SYR2K,
+    GEMMTR and TRMM (src/level3.cc:26-342): alpha = 0 and beta = 1 leave C,
+    alpha = 0 scales without reading A or B, TRMM with alpha = 0 zeroes B."""
+    nan = np.full(16, np.nan)
+    c = np.arange(16.0)
+    c1 = c.copy()
+    assert orc.symm("d", "L", "U", 4, 4, 0.0, nan, 4, nan, 4, 1.0, c1, 4) == 0
+    assert same_bits(c1, c)
+    assert orc.symm("d", "L", "U", 4, 4, 0.0, nan, 4, nan, 4, 2.0, c1, 4) == 0
+    assert np.array_equal(c1, 2 * c)
+    c1 = c.copy()
+    assert orc.syr2k("d", "L", "N", 4, 0, 1.0, nan, 4, nan, 4, 0.0, c1, 4) == 0
+    tri = np.tril(np.ones((4, 4), bool)).ravel(order="F")
+    assert np.all(c1[tri] == 0) and np.array_equal(c1[~tri], c[~tri])
+    c1 = c.copy()
+    assert orc.gemmtr("d", "U", "N", "N", 4, 3, 0.0, nan, 4, nan, 4, 3.0, c1, 4) == 0
+    assert np.array_equal(c1[~tri | np.eye(4, dtype=bool).ravel()],
+                          3 * c[~tri | np.eye(4, dtype=bool).ravel()])
+    b = np.arange(16.0)
+    assert orc.trmm("d", "L", "L", "N", "N", 4, 4, 0.0, nan, 4, b, 4) == 0
+    assert np.all(b == 0)
+    z = np.zeros(16)
+    assert orc.symm("d", "X", "U", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 1
+    assert orc.symm("d", "L", "X", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 2
+    assert orc.symm("d", "R", "U", 4, 5, 1.0, z, 4, z, 4, 0.0, z, 4) == 7
+    assert orc.symm("d", "L", "U", 4, 4, 1.0, z, 4, z, 3, 0.0, z, 4) == 9
+    assert orc.symm("d", "L", "U", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 3) == 12
+    assert orc.syr2k("d", "U", "X", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 2
+    assert orc.syr2k("d", "U", "T", 4, 5, 1.0, z, 4, z, 5, 0.0, z, 4) == 7
+    assert orc.syr2k("d", "U", "N", 4, 4, 1.0, z, 4, z, 3, 0.0, z, 4) == 9
+    assert orc.gemmtr("d", "U", "N", "X", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 3
+    assert orc.gemmtr("d", "U", "N", "N", 4, -1, 1.0, z, 4, z, 4, 0.0, z, 4) == 5
+    assert orc.gemmtr("d", "U", "N", "T", 4, 4, 1.0, z, 4, z, 3, 0.0, z, 4) == 10
+    assert orc.gemmtr("d", "U", "N", "N", 4, 4, 1.0, z, 4, z, 4, 0.0, z, 3) == 13
+    assert orc.trmm("d", "L", "U", "N", "X", 4, 4, 1.0, z, 4, z, 4) == 4
+    assert orc.trmm("d", "R", "U", "N", "N", 4, 5, 1.0, z, 4, z, 4) == 9
+    assert orc.trmm("d", "L", "U", "N", "N", 4, 4, 1.0, z, 4, z, 3) == 11
+
+
 def test_trsm_alpha_zero_does_not_read_a(orc):
     a = np.full(9, np.nan)
     b = np.ones(6)
