@@ -87,6 +87,15 @@ int orc_dtrmm(char side, char uplo, char transa, char diag, int m, int n, double
 int orc_strmm(char side, char uplo, char transa, char diag, int m, int n, float alpha,
               const float* a, int lda, float* b, int ldb);
 
+/* Triangular inverse and GETRI (src/lapack/triangular.cc:18-166,
+ * src/lapack/getrf.cc:369-483). */
+int orc_dtrti2(char uplo, char diag, int n, double* a, int lda);
+int orc_strti2(char uplo, char diag, int n, float* a, int lda);
+int orc_dtrtri(char uplo, char diag, int n, double* a, int lda);
+int orc_strtri(char uplo, char diag, int n, float* a, int lda);
+int orc_dgetri(int n, double* a, int lda, const int* ipiv, double* work, int lwork);
+int orc_sgetri(int n, float* a, int lda, const int* ipiv, float* work, int lwork);
+
 /* Leaves, exposed for the known-answer tests. */
 int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv);
 int orc_dpotrf_leaf(int upper, int n, double* a, int lda);

@@ -614,6 +614,62 @@ int Trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha, co
 }
 
 // ---------------------------------------------------------------------------
+// TRMV, op N, contiguous x (src/trmv-inl.h:44-80): x := A x. The product
+// collects in a zeroed y, in strips of 4 columns: the strip's diagonal block
+// element by element as y += v * x (product and sum rounded separately, the
+// reference being built without contraction), then the rectangle below
+// (lower) or above (upper) it by the axpy GEMV kernel, which chains an fma
+// per column in column order for each row (src/gemv-inl.h:54-84, 280-292).
+template <typename T>
+void TrmvN(bool lower, bool unit, int n, const T* a, int lda, T* x) {
+  if (n <= 0) return;
+  std::vector<T> y(n, T(0));
+  const auto A = [&](int i, int j) { return a[i + static_cast<ptrdiff_t>(j) * lda]; };
+  for (int j = 0; j < n; j += 4) {
+    const int cols = std::min(4, n - j);
+    for (int jj = j; jj < j + cols; ++jj)
+      for (int ii = j; ii < j + cols; ++ii) {
+        if (lower ? ii < jj : ii > jj) continue;
+        const T v = (ii == jj && unit) ? T(1) : A(ii, jj);
+        const T prod = v * x[jj];
+        y[ii] = y[ii] + prod;
+      }
+    const int row0 = lower ? j + cols : 0;
+    const int rows = lower ? n - row0 : j;
+    for (int c = j; c < j + cols; ++c)
+      for (int i = row0; i < row0 + rows; ++i) y[i] = std::fma(A(i, c), x[c], y[i]);
+  }
+  std::copy(y.begin(), y.end(), x);
+}
+
+// GEMV, op N, contiguous x and y (src/gemv.cc:48-77; src/gemv-inl.h:40-52,
+// 280-292, 318-333): y := beta y (beta 0 writes zeros), then with
+// t = alpha * x, y(i) = fma(A(i, j), t(j), y(i)) for j in order.
+template <typename T>
+void GemvN(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y) {
+  if (m <= 0 || n <= 0 || (alpha == T(0) && beta == T(1))) return;
+  if (beta != T(1)) {
+    for (int i = 0; i < m; ++i) y[i] = (beta == T(0)) ? T(0) : y[i] * beta;
+  }
+  if (alpha == T(0)) return;
+  for (int j = 0; j < n; ++j) {
+    const T t = alpha * x[j];
+    const T* col = a + static_cast<ptrdiff_t>(j) * lda;
+    for (int i = 0; i < m; ++i) y[i] = std::fma(col[i], t, y[i]);
+  }
+}
+
+template void TrmvN<double>(bool, bool, int, const double*, int, double*);
+template void TrmvN<float>(bool, bool, int, const float*, int, float*);
+template void GemvN<double>(int, int, double, const double*, int, const double*, double,
+                            double*);
+template void GemvN<float>(int, int, float, const float*, int, const float*, float, float*);
+template int Trmm<double>(char, char, char, char, int, int, double, const double*, int,
+                          double*, int);
+template int Trmm<float>(char, char, char, char, int, int, float, const float*, int, float*,
+                         int);
+
+// ---------------------------------------------------------------------------
 // IAMAX (src/level1.cc:383-402; src/level1-inl.h:343-423): 1-based index of
 // the first element of largest |x|; NaNs never compare larger, so one is only
 // returned when it is x[0].

@@ -42,6 +42,15 @@ int Syrk(char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T be
          int ldc);
 template <typename T>
 int Iamax(int n, const T* x, int incx);
+template <typename T>
+int Trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
+         int lda, T* b, int ldb);
+// TRMV with op N and GEMV with op N on contiguous vectors, in the
+// reference's kernel order (src/trmv-inl.h, src/gemv-inl.h).
+template <typename T>
+void TrmvN(bool lower, bool unit, int n, const T* a, int lda, T* x);
+template <typename T>
+void GemvN(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y);
 
 template <typename T>
 int GetrfLeaf(int m, int n, T* a, int lda, int* ipiv);

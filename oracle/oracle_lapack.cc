@@ -291,6 +291,153 @@ int Potrs(char uplo, int n, int nrhs, const T* a, int lda, T* b, int ldb) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Triangular inverse and GETRI (src/lapack/triangular.cc:18-166;
+// src/lapack/getrf.cc:369-483), in the reference's call order: TRTI2 column
+// by column (an exact reciprocal of the diagonal, then TRMV of the finished
+// part and a scaling by -A(j, j)), TRTRI in blocks of 64 with TRMM, TRSM and
+// TRTI2, and GETRI solving inv(A) L = inv(U) block column by block column
+// from the right (GEMM and TRSM; GEMV unblocked) before undoing the column
+// interchanges.
+
+static char UpC(char c) { return (c >= 'a' && c <= 'z') ? c - 32 : c; }
+
+template <typename T>
+int Trti2(char uplo, char diag, int n, T* a, int lda) {
+  const bool upper = UpC(uplo) == 'U', nounit = UpC(diag) == 'N';
+  if (!upper && UpC(uplo) != 'L') return -1;
+  if (!nounit && UpC(diag) != 'U') return -2;
+  if (n < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  const auto A = [&](int i, int j) -> T& { return a[i + static_cast<ptrdiff_t>(j) * lda]; };
+  const auto scal = [](int len, T alpha, T* x) {
+    if (len <= 0 || alpha == T(1)) return;
+    for (int i = 0; i < len; ++i) x[i] *= alpha;
+  };
+  if (upper) {
+    for (int j = 0; j < n; ++j) {
+      T ajj = T(-1);
+      if (nounit) {
+        A(j, j) = T(1) / A(j, j);
+        ajj = -A(j, j);
+      }
+      TrmvN<T>(false, !nounit, j, a, lda, &A(0, j));
+      scal(j, ajj, &A(0, j));
+    }
+  } else {
+    for (int j = n - 1; j >= 0; --j) {
+      T ajj = T(-1);
+      if (nounit) {
+        A(j, j) = T(1) / A(j, j);
+        ajj = -A(j, j);
+      }
+      if (j < n - 1) {
+        TrmvN<T>(true, !nounit, n - j - 1, &A(j + 1, j + 1), lda, &A(j + 1, j));
+        scal(n - j - 1, ajj, &A(j + 1, j));
+      }
+    }
+  }
+  return 0;
+}
+
+template <typename T>
+int Trtri(char uplo, char diag, int n, T* a, int lda) {
+  const bool upper = UpC(uplo) == 'U', nounit = UpC(diag) == 'N';
+  if (!upper && UpC(uplo) != 'L') return -1;
+  if (!nounit && UpC(diag) != 'U') return -2;
+  if (n < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (n == 0) return 0;
+  const auto A = [&](int i, int j) { return a + i + static_cast<ptrdiff_t>(j) * lda; };
+  if (nounit) {
+    for (int i = 0; i < n; ++i)
+      if (*A(i, i) == T(0)) return i + 1;
+  }
+  const char d = nounit ? 'N' : 'U';
+  constexpr int nb = 64;  // ILAENV(1, xTRTRI) (src/lapack/environment.cc:134-137)
+  if (nb >= n) return Trti2<T>(uplo, d, n, a, lda);
+  if (upper) {
+    for (int j = 0; j < n; j += nb) {
+      const int jb = std::min(nb, n - j);
+      Trmm<T>('L', 'U', 'N', d, j, jb, T(1), a, lda, A(0, j), lda);
+      TrsmF<T>('R', 'U', 'N', d, j, jb, T(-1), A(j, j), lda, A(0, j), lda);
+      Trti2<T>('U', d, jb, A(j, j), lda);
+    }
+  } else {
+    const int nn = ((n - 1) / nb) * nb;
+    for (int j = nn; j >= 0; j -= nb) {
+      const int jb = std::min(nb, n - j);
+      if (j + jb < n) {
+        Trmm<T>('L', 'L', 'N', d, n - j - jb, jb, T(1), A(j + jb, j + jb), lda, A(j + jb, j),
+                lda);
+        TrsmF<T>('R', 'L', 'N', d, n - j - jb, jb, T(-1), A(j, j), lda, A(j + jb, j), lda);
+      }
+      Trti2<T>('L', d, jb, A(j, j), lda);
+    }
+  }
+  return 0;
+}
+
+// work/lwork as LAPACK's: lwork = -1 queries; the block width falls to
+// lwork / n (unblocked below 2) when lwork < 64 n. work[0] returns the size
+// used.
+template <typename T>
+int Getri(int n, T* a, int lda, const int* ipiv, T* work, int lwork) {
+  int nb = 64;  // ILAENV(1, xGETRI) (src/lapack/environment.cc:105-106)
+  const int lwkopt = std::max(1, n * nb);
+  work[0] = static_cast<T>(lwkopt);
+  const bool lquery = (lwork == -1);
+  if (n < 0) return -1;
+  if (lda < std::max(1, n)) return -3;
+  if (lwork < std::max(1, n) && !lquery) return -6;
+  if (lquery || n == 0) return 0;
+  const int info = Trtri<T>('U', 'N', n, a, lda);
+  if (info > 0) return info;
+  const auto A = [&](int i, int j) -> T& { return a[i + static_cast<ptrdiff_t>(j) * lda]; };
+  int nbmin = 2;
+  const int ldwork = n;
+  int iws;
+  if (nb > 1 && nb < n) {
+    iws = std::max(ldwork * nb, 1);
+    if (lwork < iws) {
+      nb = lwork / ldwork;
+      nbmin = 2;  // ILAENV(2, xGETRI)
+    }
+  } else {
+    iws = n;
+  }
+  if (nb < nbmin || nb >= n) {
+    for (int j = n - 1; j >= 0; --j) {
+      for (int i = j + 1; i < n; ++i) {
+        work[i] = A(i, j);
+        A(i, j) = T(0);
+      }
+      if (j < n - 1) GemvN<T>(n, n - j - 1, T(-1), &A(0, j + 1), lda, work + j + 1, T(1), &A(0, j));
+    }
+  } else {
+    const int nn = ((n - 1) / nb) * nb;
+    for (int j = nn; j >= 0; j -= nb) {
+      const int jb = std::min(nb, n - j);
+      for (int jj = j; jj < j + jb; ++jj)
+        for (int i = jj + 1; i < n; ++i) {
+          work[i + static_cast<ptrdiff_t>(jj - j) * ldwork] = A(i, jj);
+          A(i, jj) = T(0);
+        }
+      if (j + jb < n)
+        GemmF<T>('N', 'N', n, jb, n - j - jb, T(-1), &A(0, j + jb), lda, work + j + jb, ldwork,
+                 T(1), &A(0, j), lda);
+      TrsmF<T>('R', 'L', 'N', 'U', n, jb, T(1), work + j, ldwork, &A(0, j), lda);
+    }
+  }
+  for (int j = n - 2; j >= 0; --j) {
+    const int jp = ipiv[j] - 1;
+    if (jp != j)
+      for (int i = 0; i < n; ++i) std::swap(A(i, j), A(i, jp));
+  }
+  work[0] = static_cast<T>(iws);
+  return 0;
+}
+
 int PotrfD(char uplo, int n, double* a, int lda) { return Potrf<double>(uplo, n, a, lda); }
 int Potrf2D(char uplo, int n, double* a, int lda) { return Potrf2<double>(uplo, n, a, lda); }
 int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b, int ldb) {
@@ -308,6 +455,24 @@ extern "C" {
 void orc_dlaswp(int n, double* a, int lda, int k1, int k2, const int* ipiv,
                 int incx) {
   orc::Laswp<double>(n, a, lda, k1, k2, ipiv, incx);
+}
+int orc_dtrti2(char uplo, char diag, int n, double* a, int lda) {
+  return orc::Trti2<double>(uplo, diag, n, a, lda);
+}
+int orc_strti2(char uplo, char diag, int n, float* a, int lda) {
+  return orc::Trti2<float>(uplo, diag, n, a, lda);
+}
+int orc_dtrtri(char uplo, char diag, int n, double* a, int lda) {
+  return orc::Trtri<double>(uplo, diag, n, a, lda);
+}
+int orc_strtri(char uplo, char diag, int n, float* a, int lda) {
+  return orc::Trtri<float>(uplo, diag, n, a, lda);
+}
+int orc_dgetri(int n, double* a, int lda, const int* ipiv, double* work, int lwork) {
+  return orc::Getri<double>(n, a, lda, ipiv, work, lwork);
+}
+int orc_sgetri(int n, float* a, int lda, const int* ipiv, float* work, int lwork) {
+  return orc::Getri<float>(n, a, lda, ipiv, work, lwork);
 }
 int orc_dgetrf(int m, int n, double* a, int lda, int* ipiv) {
   return orc::Getrf<double>(m, n, a, lda, ipiv);

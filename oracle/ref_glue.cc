@@ -1,6 +1,6 @@
 // Glue for building the reference's own LU/Cholesky drivers (TEST
-// INFRASTRUCTURE ONLY). The reference's src/lapack/getrf.cc, potrf.cc and
-// environment.cc compile without Highway; they reach BLAS through the exported
+// INFRASTRUCTURE ONLY). The reference's src/lapack/getrf.cc, potrf.cc,
+// triangular.cc and environment.cc compile without Highway; they reach BLAS through the exported
 // Fortran symbols (src/lapack/blas.h:48-79, 338-352) and their leaves through
 // hwyblas::lapack::GetrfLeaf/PotrfLeaf (src/lapack/factor_kernels.h:34-40).
 // The Highway-based BLAS itself cannot be built here (Highway is absent), so
@@ -8,11 +8,13 @@
 // reference drivers to them lets the tests check the oracle's own LAPACK
 // restatement against the reference's driver code, bit for bit.
 //
-// Routines the hot path never reaches (complex types, xGETRI's helpers) abort;
-// the Fortran ones are in ref_stubs.c.
+// Routines the checked path never reaches (complex types, norms and condition
+// estimates) abort; the Fortran ones are in ref_stubs.c. triangular.cc is
+// built too, for xTRTRI and xTRTI2 under xGETRI.
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
+#include <utility>
 
 #include "src/common.h"
 #include "src/lapack/factor_kernels.h"
@@ -51,18 +53,53 @@ blasint PotrfLeaf(bool upper, blasint n, T* a, blasint lda) {
   }
 }
 template <typename T>
-blasint Trtri(char, char, blasint, T*, blasint) {
-  Unreached("Trtri");
-}
-template <typename T>
 void Lacgv(blasint, T*, blasint) {
   Unreached("Lacgv");
 }
+// Norms, condition estimation and safe scaling: only xTRCON, xTRRFS and
+// xLATRS of triangular.cc use them, and the checked path (xTRTRI, xTRTI2)
+// does not.
+template <typename T>
+void Rscl(blasint, RealT<T>, T*, blasint) {
+  Unreached("Rscl");
+}
+template <typename T>
+RealT<T> Lange(char, blasint, blasint, const T*, blasint, RealT<T>*) {
+  Unreached("Lange");
+}
+template <typename T>
+RealT<T> Lantr(char, char, char, blasint, blasint, const T*, blasint, RealT<T>*) {
+  Unreached("Lantr");
+}
+template <typename R>
+void Lacn2(blasint, R*, R*, blasint*, R*, blasint*, blasint*) {
+  Unreached("Lacn2");
+}
+template <typename T>
+void Lacn2(blasint, T*, T*, RealT<T>*, blasint*, blasint*) {
+  Unreached("Lacn2");
+}
+template <typename T>
+T Ladiv(T, T) {
+  Unreached("Ladiv");
+}
+template void Lacn2<float>(blasint, float*, float*, blasint*, float*, blasint*, blasint*);
+template void Lacn2<double>(blasint, double*, double*, blasint*, double*, blasint*, blasint*);
+template void Lacn2<std::complex<float>>(blasint, std::complex<float>*, std::complex<float>*,
+                                         float*, blasint*, blasint*);
+template void Lacn2<std::complex<double>>(blasint, std::complex<double>*,
+                                          std::complex<double>*, double*, blasint*, blasint*);
+template std::complex<float> Ladiv<std::complex<float>>(std::complex<float>,
+                                                        std::complex<float>);
+template std::complex<double> Ladiv<std::complex<double>>(std::complex<double>,
+                                                          std::complex<double>);
 #define ORC_INST(T)                                                   \
   template blasint GetrfLeaf<T>(blasint, blasint, T*, blasint, blasint*); \
   template blasint PotrfLeaf<T>(bool, blasint, T*, blasint);          \
-  template blasint Trtri<T>(char, char, blasint, T*, blasint);        \
-  template void Lacgv<T>(blasint, T*, blasint);
+  template void Lacgv<T>(blasint, T*, blasint);                       \
+  template void Rscl<T>(blasint, RealT<T>, T*, blasint);              \
+  template RealT<T> Lange<T>(char, blasint, blasint, const T*, blasint, RealT<T>*); \
+  template RealT<T> Lantr<T>(char, char, char, blasint, blasint, const T*, blasint, RealT<T>*);
 ORC_INST(float)
 ORC_INST(double)
 ORC_INST(std::complex<float>)
@@ -130,6 +167,34 @@ blasint idamax_(const blasint* n, const double* x, const blasint* incx) {
 blasint isamax_(const blasint* n, const float* x, const blasint* incx) {
   return orc::Iamax<float>(*n, x, *incx);
 }
+// TRMV, GEMV and SWAP for xTRTI2 and xGETRI: op N with unit strides, the only
+// forms those drivers call (src/lapack/triangular.cc:46-75;
+// src/lapack/getrf.cc:436-476).
+#define ORC_L2(P, T)                                                                      \
+  void P##trmv_(const char* u, const char* t, const char* d, const blasint* n, const T* a, \
+                const blasint* lda, T* x, const blasint* incx) {                          \
+    if ((*t != 'N' && *t != 'n') || *incx != 1) Unreached(#P "trmv_ form");                \
+    orc::TrmvN<T>(*u == 'L' || *u == 'l', *d == 'U' || *d == 'u', *n, a, *lda, x);       \
+  }                                                                                        \
+  void P##gemv_(const char* t, const blasint* m, const blasint* n, const T* alpha,         \
+                const T* a, const blasint* lda, const T* x, const blasint* incx,           \
+                const T* beta, T* y, const blasint* incy) {                                \
+    if ((*t != 'N' && *t != 'n') || *incx != 1 || *incy != 1) Unreached(#P "gemv_ form");  \
+    orc::GemvN<T>(*m, *n, *alpha, a, *lda, x, *beta, y);                                   \
+  }                                                                                        \
+  void P##swap_(const blasint* n, T* x, const blasint* incx, T* y, const blasint* incy) {  \
+    for (blasint i = 0; i < *n; ++i) std::swap(x[i * *incx], y[i * *incy]);               \
+  }                                                                                        \
+  void P##trmm_(const char* s, const char* u, const char* t, const char* d,                \
+                const blasint* m, const blasint* n, const T* alpha, const T* a,            \
+                const blasint* lda, T* b, const blasint* ldb) {                            \
+    const int info = orc::Trmm<T>(*s, *u, *t, *d, *m, *n, *alpha, a, *lda, b, *ldb);      \
+    if (info) hwyblas::ReportError(#P "TRMM", info);                                       \
+  }
+ORC_L2(d, double)
+ORC_L2(s, float)
+#undef ORC_L2
+
 void dscal_(const blasint* n, const double* a, double* x, const blasint* incx) {
   if (*n <= 0 || *incx <= 0) return;
   for (blasint i = 0; i < *n; ++i) x[i * *incx] *= *a;

@@ -1,5 +1,6 @@
-/* Fortran BLAS symbols that the reference's LU/Cholesky sources reference but
- * that the checked path never calls (complex types, xGETRI). TEST
+/* Fortran BLAS symbols that the reference's LU, Cholesky and triangular
+ * sources reference but that the checked path never calls (complex types,
+ * condition numbers and refinement of triangular systems). TEST
  * INFRASTRUCTURE ONLY: they abort if reached. */
 #include <stdio.h>
 #include <stdlib.h>
@@ -8,8 +9,13 @@
     fprintf(stderr, "oracle/_ref: " #name " is not part of the checked path\n"); \
     abort();                                                            \
   }
-ORC_STUB(dswap_) ORC_STUB(sswap_) ORC_STUB(ddot_) ORC_STUB(sdot_)
-ORC_STUB(dgemv_) ORC_STUB(sgemv_) ORC_STUB(cdotc_)
+ORC_STUB(ddot_) ORC_STUB(sdot_) ORC_STUB(cdotc_)
+ORC_STUB(dasum_) ORC_STUB(sasum_) ORC_STUB(daxpy_) ORC_STUB(saxpy_)
+ORC_STUB(dcopy_) ORC_STUB(scopy_) ORC_STUB(dtrsv_) ORC_STUB(strsv_)
+ORC_STUB(caxpy_) ORC_STUB(ccopy_) ORC_STUB(cdotu_) ORC_STUB(ctrmm_)
+ORC_STUB(ctrmv_) ORC_STUB(ctrsv_) ORC_STUB(dzasum_) ORC_STUB(scasum_)
+ORC_STUB(zaxpy_) ORC_STUB(zcopy_) ORC_STUB(zdotu_) ORC_STUB(ztrmm_)
+ORC_STUB(ztrmv_) ORC_STUB(ztrsv_)
 ORC_STUB(cgemm_) ORC_STUB(cgemv_) ORC_STUB(cherk_) ORC_STUB(cscal_)
 ORC_STUB(csscal_) ORC_STUB(cswap_) ORC_STUB(ctrsm_) ORC_STUB(icamax_)
 ORC_STUB(izamax_) ORC_STUB(zdotc_) ORC_STUB(zdscal_) ORC_STUB(zgemm_)

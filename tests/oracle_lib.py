@@ -44,6 +44,10 @@ def load_ref():
     lib.sgesv_.argtypes = [P] * 8
     lib.spotrf_.argtypes = [P] * 5
     lib.spotrf2_.argtypes = [P] * 5
+    for pre in "ds":
+        getattr(lib, f"{pre}getri_").argtypes = [P] * 7
+        getattr(lib, f"{pre}trtri_").argtypes = [P] * 6
+        getattr(lib, f"{pre}trti2_").argtypes = [P] * 6
     return lib
 
 
@@ -86,6 +90,10 @@ class Oracle:
         L.orc_spotrs.argtypes = [CH, I, I, P, I, P, I]
         L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
         L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
+        for pre in "ds":
+            getattr(L, f"orc_{pre}getri").argtypes = [I, P, I, P, P, I]
+            getattr(L, f"orc_{pre}trtri").argtypes = [CH, CH, I, P, I]
+            getattr(L, f"orc_{pre}trti2").argtypes = [CH, CH, I, P, I]
         for pre, S in (("d", D), ("s", F)):
             getattr(L, f"orc_{pre}symm").argtypes = [CH, CH, I, I, S, P, I, P, I, S, P, I]
             getattr(L, f"orc_{pre}syr2k").argtypes = [CH, CH, I, I, S, P, I, P, I, S, P, I]
@@ -192,6 +200,15 @@ class Oracle:
         return getattr(self.lib, f"orc_{p}trmm")(_b(side), _b(uplo), _b(transa), _b(diag), m,
                                                  n, alpha, ptr(a), lda, ptr(b), ldb)
 
+    def getri(self, n, a, lda, ipiv, work, lwork):
+        p = "s" if a.dtype == np.float32 else "d"
+        return getattr(self.lib, f"orc_{p}getri")(n, ptr(a), lda, ptr(ipiv), ptr(work), lwork)
+
+    def trtri(self, uplo, diag, n, a, lda, unblocked=False):
+        p = "s" if a.dtype == np.float32 else "d"
+        fn = getattr(self.lib, f"orc_{p}{'trti2' if unblocked else 'trtri'}")
+        return fn(_b(uplo), _b(diag), n, ptr(a), lda)
+
     def dposv(self, uplo, n, nrhs, a, lda, b, ldb):
         return self.lib.orc_dposv(_b(uplo), n, nrhs, ptr(a), lda, ptr(b), ldb)
 
@@ -225,6 +242,25 @@ def ref_call_potrf(lib, recursive, uplo, n, a, lda):
         (lib.spotrf2_ if recursive else lib.spotrf_)(*args)
     else:
         (lib.dpotrf2_ if recursive else lib.dpotrf_)(*args)
+    return info.value
+
+
+def ref_call_getri(lib, n, a, lda, ipiv, work, lwork):
+    """The reference driver's ?getri_ (src/lapack/getrf.cc:538-544), by dtype."""
+    info = ctypes.c_int(0)
+    fn = lib.sgetri_ if a.dtype == np.float32 else lib.dgetri_
+    fn(ctypes.byref(ctypes.c_int(n)), ptr(a), ctypes.byref(ctypes.c_int(lda)), ptr(ipiv),
+       ptr(work), ctypes.byref(ctypes.c_int(lwork)), ctypes.byref(info))
+    return info.value
+
+
+def ref_call_trtri(lib, unblocked, uplo, diag, n, a, lda):
+    """The reference's ?trtri_ / ?trti2_ (src/lapack/triangular.cc:1645-1659)."""
+    info = ctypes.c_int(0)
+    pre = "s" if a.dtype == np.float32 else "d"
+    fn = getattr(lib, f"{pre}{'trti2' if unblocked else 'trtri'}_")
+    fn(ctypes.c_char_p(_b(uplo)), ctypes.c_char_p(_b(diag)), ctypes.byref(ctypes.c_int(n)),
+       ptr(a), ctypes.byref(ctypes.c_int(lda)), ctypes.byref(info))
     return info.value
 
 

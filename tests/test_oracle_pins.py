@@ -595,6 +595,91 @@ def test_level3_quick_returns_and_errors(orc):
     assert orc.trmm("d", "L", "U", "N", "N", 4, 4, 1.0, z, 4, z, 3) == 11
 
 
+@pytest.mark.parametrize("unblocked", [False, True])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 17, 64, 65, 130, 300])
+def test_trtri_matches_reference_driver(orc, ref_drivers, unblocked, uplo, diag, n):
+    """The oracle's triangular inverse against the reference's own xTRTRI and
+    xTRTI2 (src/lapack/triangular.cc:18-166) on the oracle's TRMM, TRSM, TRMV
+    and SCAL, bit for bit; the unread triangle and a unit diagonal hold NaN."""
+    from tests.oracle_lib import ref_call_trtri
+    for dtype in (np.float64, np.float32):
+        rng = np.random.default_rng(n * 3 + (diag == "U"))
+        lda = n + 2
+        a = np.full((lda, n), np.nan, dtype=dtype, order="F")
+        t = rng.uniform(-1, 1, (n, n)) / np.sqrt(n)
+        keep = np.tril(np.ones((n, n), bool), -1)
+        if uplo == "U":
+            keep = keep.T
+        a[:n][keep] = t[keep]
+        if diag == "N":
+            a[np.arange(n), np.arange(n)] = 1.0 + rng.uniform(0, 1, n)
+        a1, a2 = a.copy(order="F"), a.copy(order="F")
+        i1 = orc.trtri(uplo, diag, n, a1, lda, unblocked=unblocked)
+        i2 = ref_call_trtri(ref_drivers, unblocked, uplo, diag, n, a2, lda)
+        assert i1 == i2 == 0
+        assert same_bits(a1, a2), first_diff(a1, a2)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 33, 64, 65, 100, 200, 300])
+@pytest.mark.parametrize("lwork_kind", ["opt", "min", "mid"])
+def test_getri_matches_reference_driver(orc, ref_drivers, n, lwork_kind):
+    """The oracle's GETRI against the reference's own xGETRI
+    (src/lapack/getrf.cc:369-483) after the same LU: blocked (lwork = 64 n),
+    unblocked (lwork = n) and a reduced block width (lwork = 20 n)."""
+    from tests.oracle_lib import ref_call_getri
+    for dtype in (np.float64, np.float32):
+        rng = np.random.default_rng(n + 11)
+        lda = n + 1
+        a = rand(rng, lda, n, dtype)
+        ipiv = np.zeros(n, np.int32)
+        assert orc.dgetrf(n, n, a, lda, ipiv) == 0 if dtype == np.float64 else \
+            orc.sgetrf(n, n, a, lda, ipiv) == 0
+        lwork = {"opt": 64 * n, "min": n, "mid": 20 * n}[lwork_kind]
+        a1, a2 = a.copy(order="F"), a.copy(order="F")
+        w1, w2 = np.zeros(max(lwork, 1), dtype), np.zeros(max(lwork, 1), dtype)
+        i1 = orc.getri(n, a1, lda, ipiv, w1, lwork)
+        i2 = ref_call_getri(ref_drivers, n, a2, lda, ipiv, w2, lwork)
+        assert i1 == i2 == 0
+        assert same_bits(a1, a2), first_diff(a1, a2)
+        assert w1[0] == w2[0]
+
+
+def test_getri_singular_and_arguments(orc, ref_drivers):
+    """INFO = i for U(i, i) exactly zero (A left as TRTRI's check found it),
+    argument errors and the workspace query, as the reference's xGETRI."""
+    from tests.oracle_lib import ref_call_getri
+    n = 6
+    a = np.asfortranarray(np.triu(np.ones((n, n))) + np.eye(n))
+    a[3, 3] = 0.0
+    ipiv = np.arange(1, n + 1, dtype=np.int32)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    w1, w2 = np.zeros(64 * n), np.zeros(64 * n)
+    assert orc.getri(n, a1, n, ipiv, w1, 64 * n) == 4
+    assert ref_call_getri(ref_drivers, n, a2, n, ipiv, w2, 64 * n) == 4
+    assert same_bits(a1, a2)
+    w = np.zeros(1)
+    assert orc.getri(100, a1, 100, ipiv, w, -1) == 0 and w[0] == 6400
+    assert orc.getri(-1, a1, 1, ipiv, w, 1) == -1
+    assert orc.getri(n, a1, n - 1, ipiv, w, 64 * n) == -3
+    assert orc.getri(n, a1, n, ipiv, w, n - 1) == -6
+
+
+def test_getri_inverse_residual(orc):
+    """inv(A) from GETRF + GETRI satisfies |A inv(A) - I| <= c n eps |A| |inv(A)|."""
+    rng = np.random.default_rng(2)
+    n = 150
+    a = rand(rng, n, n)
+    inv = a.copy(order="F")
+    ipiv = np.zeros(n, np.int32)
+    assert orc.dgetrf(n, n, inv, n, ipiv) == 0
+    w = np.zeros(64 * n)
+    assert orc.getri(n, inv, n, ipiv, w, 64 * n) == 0
+    r = np.abs(a @ inv - np.eye(n))
+    assert np.all(r <= 10 * n * EPS * (np.abs(a) @ np.abs(inv)))
+
+
 def test_trsm_alpha_zero_does_not_read_a(orc):
     a = np.full(9, np.nan)
     b = np.ones(6)
