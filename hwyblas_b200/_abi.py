@@ -25,6 +25,8 @@ PROTOTYPES = {
     **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])
        for p in "ds" for r in ("gemmtr", "gemmt")},
     **{f"{p}trmm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]) for p in "ds"},
+    **{f"{p}getri_": (None, [PI, P, PI, P, P, PI, PI]) for p in "ds"},
+    **{f"{p}{r}_": (None, [C, C, PI, P, PI, PI]) for p in "ds" for r in ("trtri", "trti2")},
     "ssyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     "idamax_": (I, [PI, P, PI]),
     "xerbla_": (None, [C, PI, ctypes.c_size_t]),
@@ -67,6 +69,10 @@ PROTOTYPES = {
     **{f"LAPACKE_{p}potrs{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
        for p in "ds" for s in ("", "_work")},
     **{f"LAPACKE_{p}posv{s}": (I, [I, ctypes.c_char, I, I, P, I, P, I])
+       for p in "ds" for s in ("", "_work")},
+    **{f"LAPACKE_{p}getri": (I, [I, I, P, I, P]) for p in "ds"},
+    **{f"LAPACKE_{p}getri_work": (I, [I, I, P, I, P, P, I]) for p in "ds"},
+    **{f"LAPACKE_{p}trtri{s}": (I, [I, ctypes.c_char, ctypes.c_char, I, P, I])
        for p in "ds" for s in ("", "_work")},
     # CBLAS (by value)
     "cblas_xerbla": (None, [I, C, C]),

@@ -119,6 +119,26 @@ def trmm(p, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
                                 _scal(p)(alpha), _ptr(a), _i(lda), _ptr(b), _i(ldb))
 
 
+def getri(p, n, a, lda, ipiv, work, lwork):
+    """Inverse from the LU factors; returns INFO (reference ?getri_,
+    src/lapack/getrf.cc:538-544). work may be a 1-element array for a
+    query (lwork = -1)."""
+    info = ctypes.c_int(0)
+    getattr(lib(), f"{p}getri_")(_i(n), _ptr(a), _i(lda), _ptr(ipiv), _ptr(work), _i(lwork),
+                                 ctypes.byref(info))
+    return info.value
+
+
+def trtri(p, uplo, diag, n, a, lda, unblocked=False):
+    """Triangular inverse in place; returns INFO (reference ?trtri_ / ?trti2_,
+    src/lapack/triangular.cc:1645-1659)."""
+    info = ctypes.c_int(0)
+    name = "trti2" if unblocked else "trtri"
+    getattr(lib(), f"{p}{name}_")(_c(uplo), _c(diag), _i(n), _ptr(a), _i(lda),
+                                  ctypes.byref(info))
+    return info.value
+
+
 def cblas_level3(name, *args):
     """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
     scalars, array arguments given as numpy arrays or device pointers."""

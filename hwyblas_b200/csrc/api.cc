@@ -903,6 +903,77 @@ static void GesvEntry(const char* name, const hwyblas_int* n_p, const hwyblas_in
   *info = finfo;
   hb::Finish(name);
 }
+
+// WORK(1) := v in the caller's array (host or device).
+template <typename T>
+static void StoreWork0(T* work, T v) {
+  if (work == nullptr) return;
+  if (hb::IsDevicePointer(work)) {
+    hb::Failed(cudaMemcpyAsync(work, &v, sizeof(T), cudaMemcpyHostToDevice, Ctx().stream),
+               "work(1)");
+    hb::Failed(cudaStreamSynchronize(Ctx().stream), "sync");
+  } else {
+    *work = v;
+  }
+}
+
+// xGETRI (src/lapack/getrf.cc:369-483): WORK(1) = max(1, 64 n) before the
+// argument checks, lwork = -1 queries, lwork < 64 n narrows the blocks. The
+// library's own workspace holds the block columns; the caller's WORK only
+// reports sizes.
+template <typename T>
+static void GetriEntry(const char* name, const hwyblas_int* n_p, T* a,
+                       const hwyblas_int* lda_p, const hwyblas_int* ipiv, T* work,
+                       const hwyblas_int* lwork_p, hwyblas_int* info) {
+  const int n = *n_p, lda = *lda_p, lwork = *lwork_p;
+  StoreWork0<T>(work, static_cast<T>(std::max(1, n * 64)));
+  const bool lquery = (lwork == -1);
+  *info = 0;
+  if (n < 0) *info = -1;
+  else if (lda < std::max(1, n)) *info = -3;
+  else if (lwork < std::max(1, n) && !lquery) *info = -6;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return;
+  }
+  if (lquery || n == 0) return;
+  hb::Staged<T> sa;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sp.In(ipiv, n, 0, true)) return;
+  int iws = 0;
+  const int r = hb::GetriFull<T>(n, sa.dev, sa.ld, sp.dev, lwork, &iws);
+  sa.Out();
+  hb::Finish(name);
+  *info = r;
+  if (r == 0) StoreWork0<T>(work, static_cast<T>(iws));
+}
+
+// xTRTRI / xTRTI2 (src/lapack/triangular.cc:18-166).
+template <typename T>
+static void TrtriEntry(bool unblocked, const char* name, const char* uplo, const char* diag,
+                       const hwyblas_int* n_p, T* a, const hwyblas_int* lda_p,
+                       hwyblas_int* info) {
+  const int n = *n_p, lda = *lda_p;
+  const char u = hb::Up(*uplo), d = hb::Up(*diag);
+  *info = 0;
+  if (u != 'U' && u != 'L') *info = -1;
+  else if (d != 'N' && d != 'U') *info = -2;
+  else if (n < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return;
+  }
+  if (n == 0) return;
+  hb::Staged<T> sa;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  const int r = unblocked ? hb::Trti2Full<T>(u == 'U', d == 'U', n, sa.dev, sa.ld)
+                          : hb::TrtriFull<T>(u == 'U', d == 'U', n, sa.dev, sa.ld);
+  sa.Out();
+  hb::Finish(name);
+  *info = r;
+}
 }  // extern "C++"
 
 HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
@@ -966,6 +1037,24 @@ HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* ldb, hwyblas_int* info) {
   GesvEntry<float>("SGESV", n, nrhs, a, lda, ipiv, b, ldb, info);
 }
+
+#define HB_GETRI(P, U, T)                                                                 \
+  HWYBLAS_API void P##getri_(const hwyblas_int* n, T* a, const hwyblas_int* lda,          \
+                             const hwyblas_int* ipiv, T* work, const hwyblas_int* lwork,  \
+                             hwyblas_int* info) {                                         \
+    GetriEntry<T>(#U "GETRI", n, a, lda, ipiv, work, lwork, info);                        \
+  }                                                                                       \
+  HWYBLAS_API void P##trtri_(const char* uplo, const char* diag, const hwyblas_int* n,    \
+                             T* a, const hwyblas_int* lda, hwyblas_int* info) {           \
+    TrtriEntry<T>(false, #U "TRTRI", uplo, diag, n, a, lda, info);                        \
+  }                                                                                       \
+  HWYBLAS_API void P##trti2_(const char* uplo, const char* diag, const hwyblas_int* n,    \
+                             T* a, const hwyblas_int* lda, hwyblas_int* info) {           \
+    TrtriEntry<T>(true, #U "TRTI2", uplo, diag, n, a, lda, info);                         \
+  }
+HB_GETRI(d, D, double)
+HB_GETRI(s, S, float)
+#undef HB_GETRI
 
 static bool CheckPotrf(const char* name, const char* uplo, int n, int lda,
                        int* info, bool* upper) {

@@ -87,7 +87,9 @@ enum WorkspaceSlot : int {
   kWsLapacke1 = 19,
   kWsLevel3 = 20,      // SYMM's symmetrized operand, TRMM's triangle
   kWsLevel3Copy = 21,  // TRMM's copy of B
-  kNumWorkspaceSlots = 22
+  kWsGetri = 22,       // GETRI's block column of L
+  kWsTrti2 = 23,       // TRTI2's column between read and write
+  kNumWorkspaceSlots = 24
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -191,6 +193,16 @@ void SymmFull(bool left, bool lower, int m, int n, T alpha, const T* a, int lda,
 template <typename T>
 void Syr2kFull(bool lower, bool trans, int n, int k, T alpha, const T* a, int lda,
                const T* b, int ldb, T beta, T* c, int ldc);
+// TRTI2, TRTRI and GETRI (src/lapack/triangular.cc:18-166,
+// src/lapack/getrf.cc:369-483) after argument checks. TRTRI returns i > 0 for
+// A(i, i) == 0 (non-unit; A untouched); GETRI returns its INFO and the WORK(1)
+// value of a successful call in *iws.
+template <typename T>
+int Trti2Full(bool upper, bool unit, int n, T* a, int lda);
+template <typename T>
+int TrtriFull(bool upper, bool unit, int n, T* a, int lda);
+template <typename T>
+int GetriFull(int n, T* a, int lda, const int* ipiv, int lwork, int* iws);
 template <typename T>
 void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
                 const T* b, int ldb, T beta, T* c, int ldc);

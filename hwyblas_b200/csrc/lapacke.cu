@@ -84,7 +84,7 @@ void Transpose(int rows, int cols, const T* in, long long ld_in, T* out, long lo
 }
 
 // Whether the logical rows x cols matrix (row-major: a[i*ld + j]) has a NaN
-// in part 'G' (all), 'U' (i <= j) or 'L' (i >= j).
+// in part 'G' (all), 'U' (i <= j), 'L' (i >= j), 'u' (i < j) or 'l' (i > j).
 template <typename T>
 __global__ void NanKernel(int rows, int cols, const T* a, long long ld, int rowmajor, char part,
                           int* flag) {
@@ -94,6 +94,7 @@ __global__ void NanKernel(int rows, int cols, const T* a, long long ld, int rowm
     const int i = rowmajor ? static_cast<int>(e / cols) : static_cast<int>(e % rows);
     const int j = rowmajor ? static_cast<int>(e % cols) : static_cast<int>(e / rows);
     if ((part == 'U' && i > j) || (part == 'L' && i < j)) continue;
+    if ((part == 'u' && i >= j) || (part == 'l' && i <= j)) continue;
     const T x = rowmajor ? a[static_cast<long long>(i) * ld + j] : a[i + j * ld];
     if (x != x) atomicExch(flag, 1);
   }
@@ -112,6 +113,7 @@ bool HasNan(int layout, char part, int m, int n, const T* a, int lda) {
     for (int j = 0; j < n; ++j) {
       for (int i = 0; i < m; ++i) {
         if ((part == 'U' && i > j) || (part == 'L' && i < j)) continue;
+        if ((part == 'u' && i >= j) || (part == 'l' && i <= j)) continue;
         const T x = rowmajor ? a[static_cast<size_t>(i) * lda + j]
                              : a[i + static_cast<size_t>(j) * lda];
         if (std::isnan(x)) return true;
@@ -137,6 +139,16 @@ bool HasNan(int layout, char part, int m, int n, const T* a, int lda) {
 char TrPart(char uplo) {
   const char u = (uplo >= 'a' && uplo <= 'z') ? static_cast<char>(uplo - 32) : uplo;
   return (u == 'U' || u == 'L') ? u : 0;
+}
+
+// LAPACKE_xtr_nancheck (lapacke_util.h:89-119): the triangle, without the
+// diagonal when unit; invalid uplo or diag checks nothing.
+template <typename T>
+bool HasNanTr(int layout, char uplo, char diag, int n, const T* a, int lda) {
+  const char part = TrPart(uplo);
+  const char d = (diag >= 'a' && diag <= 'z') ? static_cast<char>(diag - 32) : diag;
+  if (part == 0 || (d != 'U' && d != 'N')) return false;
+  return HasNan(layout, d == 'U' ? static_cast<char>(part + 32) : part, n, n, a, lda);
 }
 
 template <typename T>
@@ -278,6 +290,18 @@ void Potrs(const char* u, int* n, int* r, const float* a, int* lda, float* b, in
            int* info) {
   spotrs_(u, n, r, a, lda, b, ldb, info);
 }
+void Getri(int* n, double* a, int* lda, const int* ipiv, double* w, int* lw, int* info) {
+  dgetri_(n, a, lda, ipiv, w, lw, info);
+}
+void Getri(int* n, float* a, int* lda, const int* ipiv, float* w, int* lw, int* info) {
+  sgetri_(n, a, lda, ipiv, w, lw, info);
+}
+void Trtri(const char* u, const char* d, int* n, double* a, int* lda, int* info) {
+  dtrtri_(u, d, n, a, lda, info);
+}
+void Trtri(const char* u, const char* d, int* n, float* a, int* lda, int* info) {
+  strtri_(u, d, n, a, lda, info);
+}
 void Posv(const char* u, int* n, int* r, double* a, int* lda, double* b, int* ldb, int* info) {
   dposv_(u, n, r, a, lda, b, ldb, info);
 }
@@ -415,6 +439,75 @@ lapack_int PosMain(int layout, char uplo, int n, int nrhs, T* a, int lda, T* b, 
   return PosWork(layout, uplo, n, nrhs, a, lda, b, ldb, solve_only);
 }
 
+// xGETRI (lapacke_linear.cc:75-96): a workspace query (lwork = -1) runs on
+// the caller's array after the leading-dimension check, as CallWork's query
+// branch (lapacke_util.h:437-452).
+template <typename T>
+lapack_int GetriWork(int layout, int n, T* a, int lda, const int* ipiv, T* work, int lwork) {
+  const std::string name = Name<T>("getri_work");
+  const auto call = [&](T** p, int* ld) {
+    int info = 0;
+    Getri(&n, p[0], &ld[0], ipiv, work, &lwork, &info);
+    return info;
+  };
+  if (lwork == -1 && layout == LAPACK_ROW_MAJOR) {
+    if (lda < n) {
+      LAPACKE_xerbla(name.c_str(), -4);
+      return -4;
+    }
+    T* p[1] = {a};
+    int ld[1] = {std::max(1, n)};
+    const int info = call(p, ld);
+    return info < 0 ? info - 1 : info;
+  }
+  const Arg<T> args[1] = {{a, n, n, lda, -4, true, true}};
+  return CallWork(layout, name, args, call);
+}
+
+// WithWorkspace (lapacke_util.h:494-512): query, allocate, call.
+template <typename T>
+lapack_int GetriMain(int layout, int n, T* a, int lda, const int* ipiv) {
+  const std::string name = Name<T>("getri");
+  if (layout != LAPACK_ROW_MAJOR && layout != LAPACK_COL_MAJOR) {
+    LAPACKE_xerbla(name.c_str(), -1);
+    return -1;
+  }
+  if (NanCheck() && HasNan(layout, 'G', n, n, a, lda)) return -3;
+  T query = T(0);
+  lapack_int info = GetriWork(layout, n, a, lda, ipiv, &query, -1);
+  if (info != 0) return info;
+  const int lwork = static_cast<int>(query);
+  std::vector<T> buffer;
+  try {
+    buffer.resize(static_cast<size_t>(std::max(lwork, 1)));
+  } catch (const std::bad_alloc&) {
+    LAPACKE_xerbla(name.c_str(), LAPACK_WORK_MEMORY_ERROR);
+    return LAPACK_WORK_MEMORY_ERROR;
+  }
+  return GetriWork(layout, n, a, lda, ipiv, buffer.data(), lwork);
+}
+
+// xTRTRI (lapacke_linear.cc:276-298).
+template <typename T>
+lapack_int TrtriWork(int layout, char uplo, char diag, int n, T* a, int lda) {
+  const Arg<T> args[1] = {{a, n, n, lda, -6, true, true}};
+  return CallWork(layout, Name<T>("trtri_work"), args, [&](T** p, int* ld) {
+    int info = 0;
+    Trtri(&uplo, &diag, &n, p[0], &ld[0], &info);
+    return info;
+  });
+}
+
+template <typename T>
+lapack_int TrtriMain(int layout, char uplo, char diag, int n, T* a, int lda) {
+  if (layout != LAPACK_ROW_MAJOR && layout != LAPACK_COL_MAJOR) {
+    LAPACKE_xerbla(Name<T>("trtri").c_str(), -1);
+    return -1;
+  }
+  if (NanCheck() && HasNanTr(layout, uplo, diag, n, a, lda)) return -5;
+  return TrtriWork(layout, uplo, diag, n, a, lda);
+}
+
 }  // namespace
 }  // namespace hb
 
@@ -485,6 +578,28 @@ HWYBLAS_API int LAPACKE_get_nancheck(void) {
                                                 lapack_int ldb) {                     \
     return hb::GesvWork<T>(layout, n, nrhs, a, lda, ipiv, b, ldb);                    \
   }
+
+#define HB_LAPACKE_INV(p, T)                                                              \
+  HWYBLAS_API lapack_int LAPACKE_##p##getri(int layout, lapack_int n, T* a, lapack_int lda,  \
+                                            const lapack_int* ipiv) {                       \
+    return hb::GetriMain<T>(layout, n, a, lda, ipiv);                                       \
+  }                                                                                         \
+  HWYBLAS_API lapack_int LAPACKE_##p##getri_work(int layout, lapack_int n, T* a,            \
+                                                 lapack_int lda, const lapack_int* ipiv,    \
+                                                 T* work, lapack_int lwork) {               \
+    return hb::GetriWork<T>(layout, n, a, lda, ipiv, work, lwork);                          \
+  }                                                                                         \
+  HWYBLAS_API lapack_int LAPACKE_##p##trtri(int layout, char uplo, char diag, lapack_int n, \
+                                            T* a, lapack_int lda) {                         \
+    return hb::TrtriMain<T>(layout, uplo, diag, n, a, lda);                                 \
+  }                                                                                         \
+  HWYBLAS_API lapack_int LAPACKE_##p##trtri_work(int layout, char uplo, char diag,          \
+                                                 lapack_int n, T* a, lapack_int lda) {      \
+    return hb::TrtriWork<T>(layout, uplo, diag, n, a, lda);                                 \
+  }
+HB_LAPACKE_INV(d, double)
+HB_LAPACKE_INV(s, float)
+#undef HB_LAPACKE_INV
 
 HB_LAPACKE_LU(d, double)
 HB_LAPACKE_LU(s, float)

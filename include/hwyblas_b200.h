@@ -205,6 +205,31 @@ HWYBLAS_API void sgetrs_(const char* trans, const hwyblas_int* n,
 HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
                         const hwyblas_int* ldb, hwyblas_int* info);
+/* Inverse from the LU factorization: inv(U) by ?trtri, then inv(A) L =
+ * inv(U) in block columns of 64 (lwork >= 64 n; narrower blocks for a
+ * smaller lwork, column by column below 2 n), then the column interchanges.
+ * WORK(1) returns 64 n (query, lwork = -1) or the size used. info > 0:
+ * U(info, info) is exactly zero. Replace dgetri_ / sgetri_
+ * (include/hwyblas/lapack.h:174, 171; src/lapack/getrf.cc:369-483, 538-544). */
+HWYBLAS_API void dgetri_(const hwyblas_int* n, double* a, const hwyblas_int* lda,
+                         const hwyblas_int* ipiv, double* work, const hwyblas_int* lwork,
+                         hwyblas_int* info);
+HWYBLAS_API void sgetri_(const hwyblas_int* n, float* a, const hwyblas_int* lda,
+                         const hwyblas_int* ipiv, float* work, const hwyblas_int* lwork,
+                         hwyblas_int* info);
+/* Inverse of a triangular matrix in place (unit diagonal not read when
+ * diag = 'U'): ?trtri blocked (64), ?trti2 unblocked. ?trtri: info > 0 when
+ * A(info, info) is exactly zero (A unchanged). Replace dtrtri_ / strtri_ /
+ * dtrti2_ / strti2_ (include/hwyblas/lapack.h:288, 285, 276, 273;
+ * src/lapack/triangular.cc:18-166, 1645-1659). */
+HWYBLAS_API void dtrtri_(const char* uplo, const char* diag, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void strtri_(const char* uplo, const char* diag, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void dtrti2_(const char* uplo, const char* diag, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void strti2_(const char* uplo, const char* diag, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
 /* Cholesky, blocked with nb = 64 (include/hwyblas/lapack.h:663,
  * src/lapack/potrf.cc:128-199, 747-751). */
 HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
@@ -312,6 +337,28 @@ HWYBLAS_API lapack_int LAPACKE_sgesv(int matrix_layout, lapack_int n, lapack_int
 HWYBLAS_API lapack_int LAPACKE_sgesv_work(int matrix_layout, lapack_int n,
                                           lapack_int nrhs, float* a, lapack_int lda,
                                           lapack_int* ipiv, float* b, lapack_int ldb);
+/* LAPACKE forms of ?getri and ?trtri (include/hwyblas/lapacke.h:269-287,
+ * 478-500; src/lapack/lapacke_linear.cc:75-96, 276-298, 500-548): row-major
+ * through a transposed temporary; LAPACKE_?getri allocates the workspace
+ * after a query. */
+HWYBLAS_API lapack_int LAPACKE_dgetri(int matrix_layout, lapack_int n, double* a,
+                                      lapack_int lda, const lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_sgetri(int matrix_layout, lapack_int n, float* a,
+                                      lapack_int lda, const lapack_int* ipiv);
+HWYBLAS_API lapack_int LAPACKE_dgetri_work(int matrix_layout, lapack_int n, double* a,
+                                           lapack_int lda, const lapack_int* ipiv,
+                                           double* work, lapack_int lwork);
+HWYBLAS_API lapack_int LAPACKE_sgetri_work(int matrix_layout, lapack_int n, float* a,
+                                           lapack_int lda, const lapack_int* ipiv,
+                                           float* work, lapack_int lwork);
+HWYBLAS_API lapack_int LAPACKE_dtrtri(int matrix_layout, char uplo, char diag, lapack_int n,
+                                      double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_strtri(int matrix_layout, char uplo, char diag, lapack_int n,
+                                      float* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_dtrtri_work(int matrix_layout, char uplo, char diag,
+                                           lapack_int n, double* a, lapack_int lda);
+HWYBLAS_API lapack_int LAPACKE_strtri_work(int matrix_layout, char uplo, char diag,
+                                           lapack_int n, float* a, lapack_int lda);
 HWYBLAS_API lapack_int LAPACKE_dpotrf(int matrix_layout, char uplo, lapack_int n,
                                       double* a, lapack_int lda);
 HWYBLAS_API lapack_int LAPACKE_dpotrf_work(int matrix_layout, char uplo, lapack_int n,
