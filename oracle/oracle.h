@@ -96,6 +96,15 @@ int orc_strtri(char uplo, char diag, int n, float* a, int lda);
 int orc_dgetri(int n, double* a, int lda, const int* ipiv, double* work, int lwork);
 int orc_sgetri(int n, float* a, int lda, const int* ipiv, float* work, int lwork);
 
+/* Iterative refinement with error bounds (src/lapack/gesvx.cc:319-456);
+ * work holds 3 n, iwork n. */
+int orc_dgerfs(char trans, int n, int nrhs, const double* a, int lda, const double* af,
+               int ldaf, const int* ipiv, const double* b, int ldb, double* x, int ldx,
+               double* ferr, double* berr, double* work, int* iwork);
+int orc_sgerfs(char trans, int n, int nrhs, const float* a, int lda, const float* af,
+               int ldaf, const int* ipiv, const float* b, int ldb, float* x, int ldx,
+               float* ferr, float* berr, float* work, int* iwork);
+
 /* Leaves, exposed for the known-answer tests. */
 int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv);
 int orc_dpotrf_leaf(int upper, int n, double* a, int lda);

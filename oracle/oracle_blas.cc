@@ -659,6 +659,99 @@ void GemvN(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y)
   }
 }
 
+// Vector lanes of the reference's SIMD target: 8 doubles / 16 floats
+// (AVX-512) or 4 / 8 (AVX2).
+template <typename T>
+static size_t RefLanes() {
+  return sizeof(T) == 8 ? g_lanes : 2 * g_lanes;
+}
+
+// The lane sum of a vector (ReduceSum): halves added lane-wise until one
+// lane is left, i.e. ((v0+v4)+(v2+v6)) + ((v1+v5)+(v3+v7)) for 8 lanes.
+template <typename T>
+static T ReduceSumLanes(std::vector<T> v) {
+  for (size_t h = v.size() / 2; h >= 1; h /= 2)
+    for (size_t i = 0; i < h; ++i) v[i] = v[i] + v[i + h];
+  return v[0];
+}
+
+// GEMV, op T, contiguous x and y (src/gemv-inl.h:163-196, 294-307, 318-333):
+// y := beta y, then y(c) += alpha * (lane sum of the dot product of column c
+// with x), lane l holding the fma chain over the rows i = l mod N in order
+// (zero products past the end of the last vector).
+template <typename T>
+void GemvT(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y) {
+  if (m <= 0 || n <= 0 || (alpha == T(0) && beta == T(1))) return;
+  if (beta != T(1)) {
+    for (int j = 0; j < n; ++j) y[j] = (beta == T(0)) ? T(0) : y[j] * beta;
+  }
+  if (alpha == T(0)) return;
+  const size_t N = RefLanes<T>();
+  const size_t full = static_cast<size_t>(m) / N * N;
+  for (int c = 0; c < n; ++c) {
+    const T* col = a + static_cast<ptrdiff_t>(c) * lda;
+    std::vector<T> s(N, T(0));
+    for (size_t i = 0; i < full; ++i) s[i % N] = std::fma(col[i], x[i], s[i % N]);
+    if (full < static_cast<size_t>(m)) {
+      for (size_t l = 0; l < N; ++l) {
+        const size_t i = full + l;
+        s[l] = (i < static_cast<size_t>(m)) ? std::fma(col[i], x[i], s[l])
+                                            : std::fma(T(0), T(0), s[l]);
+      }
+    }
+    const T prod = alpha * ReduceSumLanes(s);
+    y[c] = y[c] + prod;
+  }
+}
+
+// ASUM, contiguous (src/level1.cc:357-368; src/level1-inl.h:186-217): four
+// accumulator vectors over blocks of 4 vectors, remaining whole vectors into
+// the first, the zero-padded tail into the second, then (s0+s1)+(s2+s3) and
+// the lane sum.
+template <typename T>
+T AbsSum(int n, const T* x) {
+  if (n < 1) return T(0);
+  const size_t N = RefLanes<T>(), len = static_cast<size_t>(n);
+  std::vector<T> s0(N, T(0)), s1(N, T(0)), s2(N, T(0)), s3(N, T(0));
+  size_t i = 0;
+  for (; i + 4 * N <= len; i += 4 * N)
+    for (size_t l = 0; l < N; ++l) {
+      s0[l] = std::fabs(x[i + l]) + s0[l];
+      s1[l] = std::fabs(x[i + N + l]) + s1[l];
+      s2[l] = std::fabs(x[i + 2 * N + l]) + s2[l];
+      s3[l] = std::fabs(x[i + 3 * N + l]) + s3[l];
+    }
+  for (; i + N <= len; i += N)
+    for (size_t l = 0; l < N; ++l) s0[l] = std::fabs(x[i + l]) + s0[l];
+  if (i < len)
+    for (size_t l = 0; l < N; ++l) s1[l] = (i + l < len ? std::fabs(x[i + l]) : T(0)) + s1[l];
+  std::vector<T> sum(N);
+  for (size_t l = 0; l < N; ++l) sum[l] = (s0[l] + s1[l]) + (s2[l] + s3[l]);
+  return ReduceSumLanes(sum);
+}
+
+// AXPY, contiguous (src/level1.cc:120-128; src/level1-inl.h:37-76): blocks
+// of two vectors as fma(alpha, x, y), the rest as y + alpha * x.
+template <typename T>
+void AxpyRef(int n, T alpha, const T* x, T* y) {
+  if (n <= 0 || alpha == T(0)) return;
+  const size_t N = RefLanes<T>(), len = static_cast<size_t>(n);
+  size_t i = 0;
+  for (; i + 2 * N <= len; i += 2 * N)
+    for (size_t l = 0; l < 2 * N; ++l) y[i + l] = std::fma(alpha, x[i + l], y[i + l]);
+  for (; i < len; ++i) {
+    const T prod = x[i] * alpha;
+    y[i] = y[i] + prod;
+  }
+}
+
+template void GemvT<double>(int, int, double, const double*, int, const double*, double,
+                            double*);
+template void GemvT<float>(int, int, float, const float*, int, const float*, float, float*);
+template double AbsSum<double>(int, const double*);
+template float AbsSum<float>(int, const float*);
+template void AxpyRef<double>(int, double, const double*, double*);
+template void AxpyRef<float>(int, float, const float*, float*);
 template void TrmvN<double>(bool, bool, int, const double*, int, double*);
 template void TrmvN<float>(bool, bool, int, const float*, int, float*);
 template void GemvN<double>(int, int, double, const double*, int, const double*, double,

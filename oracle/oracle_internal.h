@@ -51,6 +51,14 @@ template <typename T>
 void TrmvN(bool lower, bool unit, int n, const T* a, int lda, T* x);
 template <typename T>
 void GemvN(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y);
+template <typename T>
+void GemvT(int m, int n, T alpha, const T* a, int lda, const T* x, T beta, T* y);
+// ASUM and AXPY on contiguous vectors in the reference's lane order
+// (src/level1-inl.h:37-76, 186-217).
+template <typename T>
+T AbsSum(int n, const T* x);
+template <typename T>
+void AxpyRef(int n, T alpha, const T* x, T* y);
 
 template <typename T>
 int GetrfLeaf(int m, int n, T* a, int lda, int* ipiv);

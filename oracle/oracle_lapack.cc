@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <limits>
 #include <utility>
 
 #include "oracle.h"
@@ -438,6 +439,208 @@ int Getri(int n, T* a, int lda, const int* ipiv, T* work, int lwork) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// GERFS (src/lapack/gesvx.cc:319-456) with its condition estimator xLACN2
+// (src/lapack/trsen.cc:2243-2366), real types. Reverse communication as in
+// LAPACK: kase 1 asks for x := op(A) x, kase 2 for x := op(A)^T x.
+
+template <typename T>
+static T MaxRef(T a, T b) {
+  return a > b ? a : b;  // src/lapack/lapack_common.h:145-152
+}
+
+template <typename T>
+void Lacn2(int n, T* v, T* x, int* isgn, T* est, int* kase, int* isave) {
+  constexpr int itmax = 5;
+  const auto sign_vector = [&]() {
+    for (int i = 0; i < n; ++i) {
+      x[i] = (x[i] >= T(0)) ? T(1) : T(-1);
+      isgn[i] = static_cast<int>(std::lround(x[i]));
+    }
+  };
+  const auto unit_vector = [&]() {
+    for (int i = 0; i < n; ++i) x[i] = T(0);
+    x[isave[1] - 1] = T(1);
+    *kase = 1;
+    isave[0] = 3;
+  };
+  const auto final_stage = [&]() {
+    T altsgn = T(1);
+    for (int i = 0; i < n; ++i) {
+      x[i] = altsgn * (T(1) + T(i) / T(n - 1));
+      altsgn = -altsgn;
+    }
+    *kase = 1;
+    isave[0] = 5;
+  };
+  if (*kase == 0) {
+    for (int i = 0; i < n; ++i) x[i] = T(1) / T(n);
+    *kase = 1;
+    isave[0] = 1;
+    return;
+  }
+  switch (isave[0]) {
+    default:  // an out-of-range state runs the first iteration's step
+    case 1:  // x = A x, first iteration
+      if (n == 1) {
+        v[0] = x[0];
+        *est = std::fabs(v[0]);
+        *kase = 0;
+        return;
+      }
+      *est = AbsSum<T>(n, x);
+      sign_vector();
+      *kase = 2;
+      isave[0] = 2;
+      return;
+    case 2:  // x = A^T x, first iteration
+      isave[1] = Iamax<T>(n, x, 1);
+      isave[2] = 2;
+      unit_vector();
+      return;
+    case 3: {  // x = A x
+      for (int i = 0; i < n; ++i) v[i] = x[i];
+      const T estold = *est;
+      *est = AbsSum<T>(n, v);
+      bool same = true;
+      for (int i = 0; i < n && same; ++i) {
+        const T xs = (x[i] >= T(0)) ? T(1) : T(-1);
+        if (static_cast<int>(std::lround(xs)) != isgn[i]) same = false;
+      }
+      if (same || *est <= estold) {
+        final_stage();
+        return;
+      }
+      sign_vector();
+      *kase = 2;
+      isave[0] = 4;
+      return;
+    }
+    case 4: {  // x = A^T x
+      const int jlast = isave[1];
+      isave[1] = Iamax<T>(n, x, 1);
+      if (x[jlast - 1] != std::fabs(x[isave[1] - 1]) && isave[2] < itmax) {
+        isave[2] = isave[2] + 1;
+        unit_vector();
+        return;
+      }
+      final_stage();
+      return;
+    }
+    case 5: {  // x = A x, final stage
+      const T temp = T(2) * (AbsSum<T>(n, x) / T(3 * n));
+      if (temp > *est) {
+        for (int i = 0; i < n; ++i) v[i] = x[i];
+        *est = temp;
+      }
+      *kase = 0;
+      return;
+    }
+  }
+}
+
+template <typename T>
+int Gerfs(char trans, int n, int nrhs, const T* a, int lda, const T* af, int ldaf,
+          const int* ipiv, const T* b, int ldb, T* x, int ldx, T* ferr, T* berr, T* work,
+          int* iwork) {
+  constexpr int itmax = 5;
+  const char t = UpC(trans);
+  const bool notran = (t == 'N');
+  if (!notran && t != 'T' && t != 'C') return -1;
+  if (n < 0) return -2;
+  if (nrhs < 0) return -3;
+  if (lda < std::max(1, n)) return -5;
+  if (ldaf < std::max(1, n)) return -7;
+  if (ldb < std::max(1, n)) return -10;
+  if (ldx < std::max(1, n)) return -12;
+  if (n == 0 || nrhs == 0) {
+    for (int j = 0; j < nrhs; ++j) ferr[j] = berr[j] = T(0);
+    return 0;
+  }
+  const char transn = notran ? 'N' : 'C', transt = notran ? 'C' : 'N';
+  const int nz = n + 1;
+  const T eps = std::numeric_limits<T>::epsilon() * T(0.5);
+  const T safmin = std::numeric_limits<T>::min();
+  const T safe1 = T(nz) * safmin;
+  const T safe2 = safe1 / eps;
+  T* rw = work;       // abs(op(A))*abs(X) + abs(B)
+  T* wk = work + n;   // residual, then the estimator's x
+  T* vv = work + 2 * n;
+  const auto A = [&](int i, int k) { return a[i + static_cast<ptrdiff_t>(k) * lda]; };
+  for (int j = 0; j < nrhs; ++j) {
+    T* xj = x + static_cast<ptrdiff_t>(j) * ldx;
+    const T* bj = b + static_cast<ptrdiff_t>(j) * ldb;
+    int count = 1;
+    T lstres = T(3);
+    for (;;) {
+      for (int i = 0; i < n; ++i) wk[i] = bj[i];
+      if (notran) GemvN<T>(n, n, T(-1), a, lda, xj, T(1), wk);
+      else GemvT<T>(n, n, T(-1), a, lda, xj, T(1), wk);
+      for (int i = 0; i < n; ++i) rw[i] = std::fabs(bj[i]);
+      if (notran) {
+        for (int k = 0; k < n; ++k) {
+          const T xk = std::fabs(xj[k]);
+          for (int i = 0; i < n; ++i) {
+            const T prod = std::fabs(A(i, k)) * xk;
+            rw[i] = rw[i] + prod;
+          }
+        }
+      } else {
+        for (int k = 0; k < n; ++k) {
+          T sum = T(0);
+          for (int i = 0; i < n; ++i) {
+            const T prod = std::fabs(A(i, k)) * std::fabs(xj[i]);
+            sum = sum + prod;
+          }
+          rw[k] = rw[k] + sum;
+        }
+      }
+      T sm = T(0);
+      for (int i = 0; i < n; ++i) {
+        if (rw[i] > safe2) {
+          sm = MaxRef(sm, std::fabs(wk[i]) / rw[i]);
+        } else {
+          sm = MaxRef(sm, (std::fabs(wk[i]) + safe1) / (rw[i] + safe1));
+        }
+      }
+      berr[j] = sm;
+      if (berr[j] > eps && T(2) * berr[j] <= lstres && count <= itmax) {
+        Getrs<T>(t, n, 1, af, ldaf, ipiv, wk, n);
+        AxpyRef<T>(n, T(1), wk, xj);
+        lstres = berr[j];
+        count = count + 1;
+        continue;
+      }
+      break;
+    }
+    for (int i = 0; i < n; ++i) {
+      const T scaled = T(nz) * eps * rw[i];
+      if (rw[i] > safe2) {
+        rw[i] = std::fabs(wk[i]) + scaled;
+      } else {
+        rw[i] = std::fabs(wk[i]) + scaled + safe1;
+      }
+    }
+    int kase = 0;
+    int isave[3] = {0, 0, 0};
+    for (;;) {
+      Lacn2<T>(n, vv, wk, iwork, &ferr[j], &kase, isave);
+      if (kase == 0) break;
+      if (kase == 1) {
+        Getrs<T>(transt, n, 1, af, ldaf, ipiv, wk, n);
+        for (int i = 0; i < n; ++i) wk[i] = rw[i] * wk[i];
+      } else {
+        for (int i = 0; i < n; ++i) wk[i] = rw[i] * wk[i];
+        Getrs<T>(transn, n, 1, af, ldaf, ipiv, wk, n);
+      }
+    }
+    T lx = T(0);
+    for (int i = 0; i < n; ++i) lx = MaxRef(lx, std::fabs(xj[i]));
+    if (lx != T(0)) ferr[j] = ferr[j] / lx;
+  }
+  return 0;
+}
+
 int PotrfD(char uplo, int n, double* a, int lda) { return Potrf<double>(uplo, n, a, lda); }
 int Potrf2D(char uplo, int n, double* a, int lda) { return Potrf2<double>(uplo, n, a, lda); }
 int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b, int ldb) {
@@ -473,6 +676,18 @@ int orc_dgetri(int n, double* a, int lda, const int* ipiv, double* work, int lwo
 }
 int orc_sgetri(int n, float* a, int lda, const int* ipiv, float* work, int lwork) {
   return orc::Getri<float>(n, a, lda, ipiv, work, lwork);
+}
+int orc_dgerfs(char trans, int n, int nrhs, const double* a, int lda, const double* af,
+               int ldaf, const int* ipiv, const double* b, int ldb, double* x, int ldx,
+               double* ferr, double* berr, double* work, int* iwork) {
+  return orc::Gerfs<double>(trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, berr,
+                            work, iwork);
+}
+int orc_sgerfs(char trans, int n, int nrhs, const float* a, int lda, const float* af,
+               int ldaf, const int* ipiv, const float* b, int ldb, float* x, int ldx,
+               float* ferr, float* berr, float* work, int* iwork) {
+  return orc::Gerfs<float>(trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, berr,
+                           work, iwork);
 }
 int orc_dgetrf(int m, int n, double* a, int lda, int* ipiv) {
   return orc::Getrf<double>(m, n, a, lda, ipiv);

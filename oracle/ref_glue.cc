@@ -10,7 +10,8 @@
 //
 // Routines the checked path never reaches (complex types, norms and condition
 // estimates) abort; the Fortran ones are in ref_stubs.c. triangular.cc is
-// built too, for xTRTRI and xTRTI2 under xGETRI.
+// built too, for xTRTRI and xTRTI2 under xGETRI, and gesvx.cc and trsen.cc
+// for xGERFS and its xLACN2.
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -56,9 +57,8 @@ template <typename T>
 void Lacgv(blasint, T*, blasint) {
   Unreached("Lacgv");
 }
-// Norms, condition estimation and safe scaling: only xTRCON, xTRRFS and
-// xLATRS of triangular.cc use them, and the checked path (xTRTRI, xTRTI2)
-// does not.
+// Norms and safe scaling: only xTRCON, xTRRFS, xLATRS, xGECON and xGESVX use
+// them, and the checked paths (xTRTRI, xTRTI2, xGERFS) do not.
 template <typename T>
 void Rscl(blasint, RealT<T>, T*, blasint) {
   Unreached("Rscl");
@@ -71,33 +71,80 @@ template <typename T>
 RealT<T> Lantr(char, char, char, blasint, blasint, const T*, blasint, RealT<T>*) {
   Unreached("Lantr");
 }
-template <typename R>
-void Lacn2(blasint, R*, R*, blasint*, R*, blasint*, blasint*) {
-  Unreached("Lacn2");
-}
-template <typename T>
-void Lacn2(blasint, T*, T*, RealT<T>*, blasint*, blasint*) {
-  Unreached("Lacn2");
-}
 template <typename T>
 T Ladiv(T, T) {
   Unreached("Ladiv");
 }
-template void Lacn2<float>(blasint, float*, float*, blasint*, float*, blasint*, blasint*);
-template void Lacn2<double>(blasint, double*, double*, blasint*, double*, blasint*, blasint*);
-template void Lacn2<std::complex<float>>(blasint, std::complex<float>*, std::complex<float>*,
-                                         float*, blasint*, blasint*);
-template void Lacn2<std::complex<double>>(blasint, std::complex<double>*,
-                                          std::complex<double>*, double*, blasint*, blasint*);
 template std::complex<float> Ladiv<std::complex<float>>(std::complex<float>,
                                                         std::complex<float>);
 template std::complex<double> Ladiv<std::complex<double>>(std::complex<double>,
                                                           std::complex<double>);
+// Householder, rotation and eigenvalue helpers of trsen.cc (built only for
+// its xLACN2) and the complex helpers of gesvx.cc: never reached.
+template <typename R>
+void Ladiv(R, R, R, R, R*, R*) {
+  Unreached("Ladiv");
+}
+template <typename T>
+void Lacpy(char, blasint, blasint, const T*, blasint, T*, blasint) {
+  Unreached("Lacpy");
+}
+template <typename T>
+void Larfg(blasint, T*, T*, blasint, T*) {
+  Unreached("Larfg");
+}
+template <typename T>
+void Larf(char, blasint, blasint, const T*, blasint, T, T*, blasint, T*) {
+  Unreached("Larf");
+}
+template <typename R>
+void Lartg(R, R, R*, R*, R*) {
+  Unreached("Lartg");
+}
+template <typename R>
+void Lanv2(R*, R*, R*, R*, R*, R*, R*, R*, R*, R*) {
+  Unreached("Lanv2");
+}
+template <typename T>
+std::enable_if_t<IsComplex<T>::value> Lartg(T, T, RealT<T>*, T*, T*) {
+  Unreached("Lartg");
+}
+template <typename T>
+std::enable_if_t<IsComplex<T>::value> Rot(blasint, T*, blasint, T*, blasint, RealT<T>, T) {
+  Unreached("Rot");
+}
+template <typename T>
+blasint Imax1(blasint, const T*, blasint) {
+  Unreached("Imax1");
+}
+template <typename T>
+RealT<T> Sum1(blasint, const T*, blasint) {
+  Unreached("Sum1");
+}
+#define ORC_REAL_INST(R)                                                   \
+  template void Ladiv<R>(R, R, R, R, R*, R*);                              \
+  template void Lartg<R>(R, R, R*, R*, R*);                                \
+  template void Lanv2<R>(R*, R*, R*, R*, R*, R*, R*, R*, R*, R*);
+ORC_REAL_INST(float)
+ORC_REAL_INST(double)
+#undef ORC_REAL_INST
+#define ORC_CPLX_INST(T)                                                   \
+  template std::enable_if_t<IsComplex<T>::value> Lartg<T>(T, T, RealT<T>*, T*, T*); \
+  template std::enable_if_t<IsComplex<T>::value> Rot<T>(blasint, T*, blasint, T*, blasint, \
+                                                        RealT<T>, T);     \
+  template blasint Imax1<T>(blasint, const T*, blasint);                   \
+  template RealT<T> Sum1<T>(blasint, const T*, blasint);
+ORC_CPLX_INST(std::complex<float>)
+ORC_CPLX_INST(std::complex<double>)
+#undef ORC_CPLX_INST
 #define ORC_INST(T)                                                   \
   template blasint GetrfLeaf<T>(blasint, blasint, T*, blasint, blasint*); \
   template blasint PotrfLeaf<T>(bool, blasint, T*, blasint);          \
   template void Lacgv<T>(blasint, T*, blasint);                       \
   template void Rscl<T>(blasint, RealT<T>, T*, blasint);              \
+  template void Lacpy<T>(char, blasint, blasint, const T*, blasint, T*, blasint); \
+  template void Larfg<T>(blasint, T*, T*, blasint, T*);               \
+  template void Larf<T>(char, blasint, blasint, const T*, blasint, T, T*, blasint, T*); \
   template RealT<T> Lange<T>(char, blasint, blasint, const T*, blasint, RealT<T>*); \
   template RealT<T> Lantr<T>(char, char, char, blasint, blasint, const T*, blasint, RealT<T>*);
 ORC_INST(float)
@@ -167,9 +214,10 @@ blasint idamax_(const blasint* n, const double* x, const blasint* incx) {
 blasint isamax_(const blasint* n, const float* x, const blasint* incx) {
   return orc::Iamax<float>(*n, x, *incx);
 }
-// TRMV, GEMV and SWAP for xTRTI2 and xGETRI: op N with unit strides, the only
-// forms those drivers call (src/lapack/triangular.cc:46-75;
-// src/lapack/getrf.cc:436-476).
+// TRMV, GEMV, SWAP, ASUM, COPY and AXPY for xTRTI2, xGETRI, xGERFS and xLACN2:
+// unit strides, the only form those drivers use (src/lapack/triangular.cc:
+// 46-75; src/lapack/getrf.cc:436-476; src/lapack/gesvx.cc:407-440;
+// src/lapack/trsen.cc:2284-2360).
 #define ORC_L2(P, T)                                                                      \
   void P##trmv_(const char* u, const char* t, const char* d, const blasint* n, const T* a, \
                 const blasint* lda, T* x, const blasint* incx) {                          \
@@ -179,8 +227,22 @@ blasint isamax_(const blasint* n, const float* x, const blasint* incx) {
   void P##gemv_(const char* t, const blasint* m, const blasint* n, const T* alpha,         \
                 const T* a, const blasint* lda, const T* x, const blasint* incx,           \
                 const T* beta, T* y, const blasint* incy) {                                \
-    if ((*t != 'N' && *t != 'n') || *incx != 1 || *incy != 1) Unreached(#P "gemv_ form");  \
-    orc::GemvN<T>(*m, *n, *alpha, a, *lda, x, *beta, y);                                   \
+    if (*incx != 1 || *incy != 1) Unreached(#P "gemv_ form");                             \
+    if (*t == 'N' || *t == 'n') orc::GemvN<T>(*m, *n, *alpha, a, *lda, x, *beta, y);       \
+    else orc::GemvT<T>(*m, *n, *alpha, a, *lda, x, *beta, y);                              \
+  }                                                                                        \
+  T P##asum_(const blasint* n, const T* x, const blasint* incx) {                          \
+    if (*incx != 1) Unreached(#P "asum_ form");                                            \
+    return orc::AbsSum<T>(*n, x);                                                          \
+  }                                                                                        \
+  void P##copy_(const blasint* n, const T* x, const blasint* incx, T* y,                   \
+                const blasint* incy) {                                                     \
+    for (blasint i = 0; i < *n; ++i) y[i * *incy] = x[i * *incx];                         \
+  }                                                                                        \
+  void P##axpy_(const blasint* n, const T* alpha, const T* x, const blasint* incx, T* y,   \
+                const blasint* incy) {                                                     \
+    if (*incx != 1 || *incy != 1) Unreached(#P "axpy_ form");                             \
+    orc::AxpyRef<T>(*n, *alpha, x, y);                                                     \
   }                                                                                        \
   void P##swap_(const blasint* n, T* x, const blasint* incx, T* y, const blasint* incy) {  \
     for (blasint i = 0; i < *n; ++i) std::swap(x[i * *incx], y[i * *incy]);               \

@@ -10,8 +10,7 @@
     abort();                                                            \
   }
 ORC_STUB(ddot_) ORC_STUB(sdot_) ORC_STUB(cdotc_)
-ORC_STUB(dasum_) ORC_STUB(sasum_) ORC_STUB(daxpy_) ORC_STUB(saxpy_)
-ORC_STUB(dcopy_) ORC_STUB(scopy_) ORC_STUB(dtrsv_) ORC_STUB(strsv_)
+ORC_STUB(dtrsv_) ORC_STUB(strsv_) ORC_STUB(drot_) ORC_STUB(srot_)
 ORC_STUB(caxpy_) ORC_STUB(ccopy_) ORC_STUB(cdotu_) ORC_STUB(ctrmm_)
 ORC_STUB(ctrmv_) ORC_STUB(ctrsv_) ORC_STUB(dzasum_) ORC_STUB(scasum_)
 ORC_STUB(zaxpy_) ORC_STUB(zcopy_) ORC_STUB(zdotu_) ORC_STUB(ztrmm_)

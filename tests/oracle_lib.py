@@ -45,6 +45,7 @@ def load_ref():
     lib.spotrf_.argtypes = [P] * 5
     lib.spotrf2_.argtypes = [P] * 5
     for pre in "ds":
+        getattr(lib, f"{pre}gerfs_").argtypes = [P] * 17
         getattr(lib, f"{pre}getri_").argtypes = [P] * 7
         getattr(lib, f"{pre}trtri_").argtypes = [P] * 6
         getattr(lib, f"{pre}trti2_").argtypes = [P] * 6
@@ -91,6 +92,8 @@ class Oracle:
         L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
         L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
         for pre in "ds":
+            getattr(L, f"orc_{pre}gerfs").argtypes = [CH, I, I, P, I, P, I, P, P, I, P, I, P,
+                                                       P, P, P]
             getattr(L, f"orc_{pre}getri").argtypes = [I, P, I, P, P, I]
             getattr(L, f"orc_{pre}trtri").argtypes = [CH, CH, I, P, I]
             getattr(L, f"orc_{pre}trti2").argtypes = [CH, CH, I, P, I]
@@ -200,6 +203,13 @@ class Oracle:
         return getattr(self.lib, f"orc_{p}trmm")(_b(side), _b(uplo), _b(transa), _b(diag), m,
                                                  n, alpha, ptr(a), lda, ptr(b), ldb)
 
+    def gerfs(self, trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, berr,
+              work, iwork):
+        p = "s" if a.dtype == np.float32 else "d"
+        return getattr(self.lib, f"orc_{p}gerfs")(_b(trans), n, nrhs, ptr(a), lda, ptr(af),
+                                                  ldaf, ptr(ipiv), ptr(b), ldb, ptr(x), ldx,
+                                                  ptr(ferr), ptr(berr), ptr(work), ptr(iwork))
+
     def getri(self, n, a, lda, ipiv, work, lwork):
         p = "s" if a.dtype == np.float32 else "d"
         return getattr(self.lib, f"orc_{p}getri")(n, ptr(a), lda, ptr(ipiv), ptr(work), lwork)
@@ -251,6 +261,18 @@ def ref_call_getri(lib, n, a, lda, ipiv, work, lwork):
     fn = lib.sgetri_ if a.dtype == np.float32 else lib.dgetri_
     fn(ctypes.byref(ctypes.c_int(n)), ptr(a), ctypes.byref(ctypes.c_int(lda)), ptr(ipiv),
        ptr(work), ctypes.byref(ctypes.c_int(lwork)), ctypes.byref(info))
+    return info.value
+
+
+def ref_call_gerfs(lib, trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, berr,
+                   work, iwork):
+    """The reference's ?gerfs_ (src/lapack/gesvx.cc:796-806), by dtype."""
+    info = ctypes.c_int(0)
+    fn = lib.sgerfs_ if a.dtype == np.float32 else lib.dgerfs_
+    I = lambda v: ctypes.byref(ctypes.c_int(v))  # noqa: E731
+    fn(ctypes.c_char_p(_b(trans)), I(n), I(nrhs), ptr(a), I(lda), ptr(af), I(ldaf), ptr(ipiv),
+       ptr(b), I(ldb), ptr(x), I(ldx), ptr(ferr), ptr(berr), ptr(work), ptr(iwork),
+       ctypes.byref(info))
     return info.value
 
 

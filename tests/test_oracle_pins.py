@@ -680,6 +680,84 @@ def test_getri_inverse_residual(orc):
     assert np.all(r <= 10 * n * EPS * (np.abs(a) @ np.abs(inv)))
 
 
+def gerfs_case(rng, n, dtype, cond_spread=1.0):
+    """A with column scales spread over cond_spread, a copy for its LU and
+    the pivot array."""
+    scale = np.exp(np.linspace(0, np.log(cond_spread), n))[None, :]
+    a = np.asfortranarray((rand(rng, n, n) * scale).astype(dtype))
+    return a, a.copy(order="F"), np.zeros(max(n, 1), np.int32)
+
+
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (2, 3), (5, 2), (17, 1), (64, 2), (150, 3)])
+@pytest.mark.parametrize("spread", [1.0, 1e6])
+def test_gerfs_matches_reference_driver(orc, ref_drivers, trans, n, nrhs, spread):
+    """The oracle's GERFS and LACN2 against the reference's own gesvx.cc and
+    trsen.cc on the oracle's BLAS: X, FERR, BERR and the work arrays bit for
+    bit (src/lapack/gesvx.cc:319-456; src/lapack/trsen.cc:2243-2366)."""
+    from tests.oracle_lib import ref_call_gerfs
+    for dtype in (np.float64, np.float32):
+        rng = np.random.default_rng(n * 13 + nrhs + int(spread))
+        a, af, ipiv = gerfs_case(rng, n, dtype, spread)
+        assert ref_call_getrf(ref_drivers, False, n, n, af, n, ipiv) == 0
+        b = rand(rng, n, nrhs, dtype)
+        x = b.copy(order="F")
+        assert orc.dgetrs(trans, n, nrhs, af, n, ipiv, x, n) == 0 if dtype == np.float64 \
+            else orc.sgetrs(trans, n, nrhs, af, n, ipiv, x, n) == 0
+        x = np.asfortranarray((x * (1 + 1e-4 * rng.standard_normal(x.shape))).astype(dtype))
+        outs = []
+        for call in ("orc", "ref"):
+            xx = x.copy(order="F")
+            ferr, berr = np.zeros(nrhs, dtype), np.zeros(nrhs, dtype)
+            work, iwork = np.zeros(3 * n, dtype), np.zeros(n, np.int32)
+            if call == "orc":
+                info = orc.gerfs(trans, n, nrhs, a, n, af, n, ipiv, b, n, xx, n, ferr, berr,
+                                 work, iwork)
+            else:
+                info = ref_call_gerfs(ref_drivers, trans, n, nrhs, a, n, af, n, ipiv, b, n, xx,
+                                      n, ferr, berr, work, iwork)
+            assert info == 0
+            outs.append((xx, ferr, berr, work, iwork))
+        for u, v in zip(outs[0], outs[1]):
+            assert same_bits(u, v) if u.dtype != np.int32 else np.array_equal(u, v)
+
+
+def test_gerfs_bounds_and_arguments(orc):
+    """BERR near eps after refinement, FERR bounding the true error, and the
+    argument checks and quick return of xGERFS."""
+    rng = np.random.default_rng(6)
+    n, nrhs = 120, 2
+    a = rand(rng, n, n)
+    af = a.copy(order="F")
+    ipiv = np.zeros(n, np.int32)
+    assert orc.dgetrf(n, n, af, n, ipiv) == 0
+    xt = rand(rng, n, nrhs)
+    b = np.asfortranarray(a @ xt)
+    x = b.copy(order="F")
+    assert orc.dgetrs("N", n, nrhs, af, n, ipiv, x, n) == 0
+    x += 1e-6
+    ferr, berr = np.zeros(nrhs), np.zeros(nrhs)
+    work, iwork = np.zeros(3 * n), np.zeros(n, np.int32)
+    assert orc.gerfs("N", n, nrhs, a, n, af, n, ipiv, b, n, x, n, ferr, berr, work, iwork) == 0
+    assert np.all(berr < 4 * EPS)
+    err = np.max(np.abs(x - xt), axis=0) / np.max(np.abs(x), axis=0)
+    assert np.all(err <= ferr)
+    f0, b0 = np.full(2, 7.0), np.full(2, 7.0)
+    assert orc.gerfs("N", 0, 2, a, 1, af, 1, ipiv, b, 1, x, 1, f0, b0, work, iwork) == 0
+    assert np.all(f0 == 0) and np.all(b0 == 0)
+    assert orc.gerfs("X", n, 1, a, n, af, n, ipiv, b, n, x, n, ferr, berr, work, iwork) == -1
+    assert orc.gerfs("N", -1, 1, a, n, af, n, ipiv, b, n, x, n, ferr, berr, work, iwork) == -2
+    assert orc.gerfs("N", n, -1, a, n, af, n, ipiv, b, n, x, n, ferr, berr, work, iwork) == -3
+    assert orc.gerfs("N", n, 1, a, n - 1, af, n, ipiv, b, n, x, n, ferr, berr, work,
+                     iwork) == -5
+    assert orc.gerfs("N", n, 1, a, n, af, n - 1, ipiv, b, n, x, n, ferr, berr, work,
+                     iwork) == -7
+    assert orc.gerfs("N", n, 1, a, n, af, n, ipiv, b, n - 1, x, n, ferr, berr, work,
+                     iwork) == -10
+    assert orc.gerfs("N", n, 1, a, n, af, n, ipiv, b, n, x, n - 1, ferr, berr, work,
+                     iwork) == -12
+
+
 def test_trsm_alpha_zero_does_not_read_a(orc):
     a = np.full(9, np.nan)
     b = np.ones(6)
