@@ -26,6 +26,8 @@ PROTOTYPES = {
        for p in "ds" for r in ("gemmtr", "gemmt")},
     **{f"{p}trmm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]) for p in "ds"},
     **{f"{p}getri_": (None, [PI, P, PI, P, P, PI, PI]) for p in "ds"},
+    **{f"{p}gerfs_": (None, [C, PI, PI, P, PI, P, PI, P, P, PI, P, PI, P, P, P, P, PI])
+       for p in "ds"},
     **{f"{p}{r}_": (None, [C, C, PI, P, PI, PI]) for p in "ds" for r in ("trtri", "trti2")},
     "ssyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     "idamax_": (I, [PI, P, PI]),

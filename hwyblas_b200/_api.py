@@ -129,6 +129,18 @@ def getri(p, n, a, lda, ipiv, work, lwork):
     return info.value
 
 
+def gerfs(p, trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, berr, work,
+          iwork):
+    """Iterative refinement with error bounds; returns INFO (reference
+    ?gerfs_, src/lapack/gesvx.cc:796-806)."""
+    info = ctypes.c_int(0)
+    getattr(lib(), f"{p}gerfs_")(_c(trans), _i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(af),
+                                 _i(ldaf), _ptr(ipiv), _ptr(b), _i(ldb), _ptr(x), _i(ldx),
+                                 _ptr(ferr), _ptr(berr), _ptr(work), _ptr(iwork),
+                                 ctypes.byref(info))
+    return info.value
+
+
 def trtri(p, uplo, diag, n, a, lda, unblocked=False):
     """Triangular inverse in place; returns INFO (reference ?trtri_ / ?trti2_,
     src/lapack/triangular.cc:1645-1659)."""

@@ -974,6 +974,98 @@ static void TrtriEntry(bool unblocked, const char* name, const char* uplo, const
   hb::Finish(name);
   *info = r;
 }
+
+// An array of `count` elements made available on the device (copied in and,
+// by Out, back when it is host memory).
+template <typename E>
+struct StagedVec {
+  E* dev = nullptr;
+  E* host = nullptr;
+  size_t count = 0;
+  bool In(E* p, size_t n, int slot) {
+    count = n;
+    if (p == nullptr || n == 0) return true;
+    if (hb::IsDevicePointer(p)) {
+      dev = p;
+      return true;
+    }
+    host = p;
+    dev = static_cast<E*>(hb::Workspace(slot, sizeof(E) * n));
+    if (dev == nullptr) return false;
+    return !hb::Failed(cudaMemcpyAsync(dev, p, sizeof(E) * n, cudaMemcpyHostToDevice,
+                                       Ctx().stream),
+                       "copy in");
+  }
+  void Out() {
+    if (host == nullptr || count == 0) return;
+    hb::Failed(cudaMemcpyAsync(host, dev, sizeof(E) * count, cudaMemcpyDeviceToHost,
+                               Ctx().stream),
+               "copy out");
+  }
+};
+
+// Stores v[0..n) into the caller's array p (host or device).
+template <typename T>
+static void StoreVector(T* p, const T* v, int n) {
+  if (p == nullptr || n <= 0) return;
+  if (hb::IsDevicePointer(p)) {
+    hb::Failed(cudaMemcpyAsync(p, v, sizeof(T) * n, cudaMemcpyHostToDevice, Ctx().stream),
+               "store");
+    hb::Failed(cudaStreamSynchronize(Ctx().stream), "sync");
+  } else {
+    for (int i = 0; i < n; ++i) p[i] = v[i];
+  }
+}
+
+// xGERFS (src/lapack/gesvx.cc:319-456, 796-806).
+template <typename T>
+static void GerfsEntry(const char* name, const char* trans, const hwyblas_int* n_p,
+                       const hwyblas_int* nrhs_p, const T* a, const hwyblas_int* lda_p,
+                       const T* af, const hwyblas_int* ldaf_p, const hwyblas_int* ipiv,
+                       const T* b, const hwyblas_int* ldb_p, T* x, const hwyblas_int* ldx_p,
+                       T* ferr, T* berr, T* work, hwyblas_int* iwork, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldaf = *ldaf_p, ldb = *ldb_p,
+            ldx = *ldx_p;
+  bool t = false;
+  const bool vt = hb::DecodeOp(*trans, &t);
+  *info = 0;
+  if (!vt) *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldaf < std::max(1, n)) *info = -7;
+  else if (ldb < std::max(1, n)) *info = -10;
+  else if (ldx < std::max(1, n)) *info = -12;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return;
+  }
+  std::vector<T> fe(std::max(nrhs, 0), T(0)), be(std::max(nrhs, 0), T(0));
+  if (n == 0 || nrhs == 0) {
+    StoreVector<T>(ferr, fe.data(), nrhs);
+    StoreVector<T>(berr, be.data(), nrhs);
+    return;
+  }
+  hb::Staged<T> sa, saf, sb, sx;
+  hb::StagedInts sp;
+  StagedVec<T> sw;
+  StagedVec<int> si;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!saf.In(af, ldaf, n, n, hb::kWsStageAF, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sx.In(x, ldx, n, nrhs, hb::kWsStageX, true)) return;
+  if (!sp.In(ipiv, n, 0, true)) return;
+  if (!sw.In(work, 3 * static_cast<size_t>(n), hb::kWsGerfsWork)) return;
+  if (!si.In(iwork, static_cast<size_t>(n), hb::kWsGerfsIwork)) return;
+  hb::GerfsFull<T>(t, n, nrhs, sa.dev, sa.ld, saf.dev, saf.ld, sp.dev, sb.dev, sb.ld, sx.dev,
+                   sx.ld, fe.data(), be.data(), sw.dev, si.dev);
+  sx.Out();
+  sw.Out();
+  si.Out();
+  hb::Finish(name);
+  StoreVector<T>(ferr, fe.data(), nrhs);
+  StoreVector<T>(berr, be.data(), nrhs);
+}
 }  // extern "C++"
 
 HWYBLAS_API void dgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
@@ -1037,6 +1129,20 @@ HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* ldb, hwyblas_int* info) {
   GesvEntry<float>("SGESV", n, nrhs, a, lda, ipiv, b, ldb, info);
 }
+
+#define HB_GERFS(P, U, T)                                                                 \
+  HWYBLAS_API void P##gerfs_(const char* trans, const hwyblas_int* n,                     \
+                             const hwyblas_int* nrhs, const T* a, const hwyblas_int* lda, \
+                             const T* af, const hwyblas_int* ldaf, const hwyblas_int* ipiv, \
+                             const T* b, const hwyblas_int* ldb, T* x,                     \
+                             const hwyblas_int* ldx, T* ferr, T* berr, T* work,            \
+                             hwyblas_int* iwork, hwyblas_int* info) {                      \
+    GerfsEntry<T>(#U "GERFS", trans, n, nrhs, a, lda, af, ldaf, ipiv, b, ldb, x, ldx, ferr, \
+                  berr, work, iwork, info);                                               \
+  }
+HB_GERFS(d, D, double)
+HB_GERFS(s, S, float)
+#undef HB_GERFS
 
 #define HB_GETRI(P, U, T)                                                                 \
   HWYBLAS_API void P##getri_(const hwyblas_int* n, T* a, const hwyblas_int* lda,          \

@@ -89,7 +89,12 @@ enum WorkspaceSlot : int {
   kWsLevel3Copy = 21,  // TRMM's copy of B
   kWsGetri = 22,       // GETRI's block column of L
   kWsTrti2 = 23,       // TRTI2's column between read and write
-  kNumWorkspaceSlots = 24
+  kWsStageAF = 24,     // host-pointer staging of GERFS's factors
+  kWsRefine = 25,      // GERFS vectors
+  kWsRefineInt = 26,
+  kWsGerfsWork = 27,   // host-pointer staging of GERFS's WORK and IWORK
+  kWsGerfsIwork = 28,
+  kNumWorkspaceSlots = 29
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -203,6 +208,13 @@ template <typename T>
 int TrtriFull(bool upper, bool unit, int n, T* a, int lda);
 template <typename T>
 int GetriFull(int n, T* a, int lda, const int* ipiv, int lwork, int* iws);
+// GERFS (src/lapack/gesvx.cc:319-456) after argument checks, n, nrhs > 0:
+// device a, af, ipiv, b, x (refined in place), work (3n) and iwork (n) or
+// null; host ferr and berr.
+template <typename T>
+void GerfsFull(bool trans, int n, int nrhs, const T* a, int lda, const T* af, int ldaf,
+               const int* ipiv, const T* b, int ldb, T* x, int ldx, T* ferr, T* berr,
+               T* work, int* iwork);
 template <typename T>
 void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
                 const T* b, int ldb, T beta, T* c, int ldc);

@@ -217,6 +217,23 @@ HWYBLAS_API void dgetri_(const hwyblas_int* n, double* a, const hwyblas_int* lda
 HWYBLAS_API void sgetri_(const hwyblas_int* n, float* a, const hwyblas_int* lda,
                          const hwyblas_int* ipiv, float* work, const hwyblas_int* lwork,
                          hwyblas_int* info);
+/* Iterative refinement of X for op(A) X = B with the LU factors AF, IPIV
+ * (at most 5 steps while the componentwise backward error BERR halves and
+ * exceeds eps), then forward error bounds FERR by the LACN2 estimate;
+ * WORK holds 3 n, IWORK n. Replace dgerfs_ / sgerfs_
+ * (include/hwyblas/lapack.h:465, 458; src/lapack/gesvx.cc:319-456, 796-806). */
+HWYBLAS_API void dgerfs_(const char* trans, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const double* a, const hwyblas_int* lda, const double* af,
+                         const hwyblas_int* ldaf, const hwyblas_int* ipiv, const double* b,
+                         const hwyblas_int* ldb, double* x, const hwyblas_int* ldx,
+                         double* ferr, double* berr, double* work, hwyblas_int* iwork,
+                         hwyblas_int* info);
+HWYBLAS_API void sgerfs_(const char* trans, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const float* a, const hwyblas_int* lda, const float* af,
+                         const hwyblas_int* ldaf, const hwyblas_int* ipiv, const float* b,
+                         const hwyblas_int* ldb, float* x, const hwyblas_int* ldx,
+                         float* ferr, float* berr, float* work, hwyblas_int* iwork,
+                         hwyblas_int* info);
 /* Inverse of a triangular matrix in place (unit diagonal not read when
  * diag = 'U'): ?trtri blocked (64), ?trti2 unblocked. ?trtri: info > 0 when
  * A(info, info) is exactly zero (A unchanged). Replace dtrtri_ / strtri_ /
