@@ -151,6 +151,18 @@ def trtri(p, uplo, diag, n, a, lda, unblocked=False):
     return info.value
 
 
+def zgemm(p, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """Complex GEMM; p is "z" or "c", arrays complex128 / complex64, alpha and
+    beta Python complex (reference zgemm_/cgemm_, src/gemm.cc:160-177)."""
+    import numpy as np
+    rt = np.float64 if p == "z" else np.float32
+    al = np.array([complex(alpha).real, complex(alpha).imag], rt)
+    be = np.array([complex(beta).real, complex(beta).imag], rt)
+    getattr(lib(), f"{p}gemm_")(_c(transa), _c(transb), _i(m), _i(n), _i(k), al.ctypes.data,
+                                _ptr(a), _i(lda), _ptr(b), _i(ldb), be.ctypes.data, _ptr(c),
+                                _i(ldc))
+
+
 def cblas_level3(name, *args):
     """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
     scalars, array arguments given as numpy arrays or device pointers."""

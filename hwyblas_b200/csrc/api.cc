@@ -511,6 +511,74 @@ static void SyrkEntry(const char* name, const char* uplo, const char* trans,
 }
 
 // SYMM (src/level3.cc:26-76).
+// Complex GEMM (src/gemm.cc:67-123): R is the real type, arrays interleaved.
+static int DecodeOp3(char c) {
+  const char u = hb::Up(c);
+  return u == 'N' ? 0 : u == 'T' ? 1 : u == 'C' ? 2 : -1;
+}
+template <typename R>
+static void ZgemmEntry(const char* name, const char* transa, const char* transb,
+                       const hwyblas_int* m_p, const hwyblas_int* n_p, const hwyblas_int* k_p,
+                       const R* alpha, const R* a, const hwyblas_int* lda_p, const R* b,
+                       const hwyblas_int* ldb_p, const R* beta, R* c, const hwyblas_int* ldc_p) {
+  const int m = *m_p, n = *n_p, k = *k_p, lda = *lda_p, ldb = *ldb_p, ldc = *ldc_p;
+  const int ta = DecodeOp3(*transa), tb = DecodeOp3(*transb);
+  const int rows_a = ta == 0 ? m : k, rows_b = tb == 0 ? k : n;
+  int info = 0;
+  if (ta < 0) info = 1;
+  else if (tb < 0) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, m)) info = 13;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  if (m == 0 || n == 0) return;
+  const bool alpha_zero = alpha[0] == R(0) && alpha[1] == R(0);
+  const bool beta_one = beta[0] == R(1) && beta[1] == R(0);
+  const bool beta_zero = beta[0] == R(0) && beta[1] == R(0);
+  if ((k == 0 || alpha_zero) && beta_one) return;
+  const bool compute = !(k == 0 || alpha_zero);
+  // Complex arrays staged as real ones with twice the rows.
+  hb::Staged<R> sa, sb, sc;
+  if (compute) {
+    if (!sa.In(a, 2 * lda, 2 * rows_a, ta == 0 ? k : m, hb::kWsStageA, true)) return;
+    if (!sb.In(b, 2 * ldb, 2 * rows_b, tb == 0 ? n : k, hb::kWsStageB, true)) return;
+  }
+  if (!sc.In(c, 2 * ldc, 2 * m, n, hb::kWsStageC, !beta_zero)) return;
+  hb::ZgemmFull<R>(ta, tb, m, n, k, alpha, sa.dev, std::max(sa.ld / 2, 1), sb.dev,
+                   std::max(sb.ld / 2, 1), beta, sc.dev, sc.ld / 2);
+  sc.Out();
+  hb::Finish(name);
+}
+
+// CBLAS complex GEMM (src/cblas.cc:520-537): row-major as the column-major
+// product of the swapped operands; alpha and beta by address.
+template <typename R>
+static void CblasZgemm(const char* name, const char* routine, CBLAS_LAYOUT layout,
+                       CBLAS_TRANSPOSE transa, CBLAS_TRANSPOSE transb, hwyblas_int m,
+                       hwyblas_int n, hwyblas_int k, const void* alpha, const void* a,
+                       hwyblas_int lda, const void* b, hwyblas_int ldb, const void* beta,
+                       void* c, hwyblas_int ldc) {
+  if (!hb::ValidLayout(name, layout)) return;
+  const char ta = hb::TransChar(transa), tb = hb::TransChar(transb);
+  const R* al = static_cast<const R*>(alpha);
+  const R* be = static_cast<const R*>(beta);
+  if (layout == CblasColMajor) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14});
+    ZgemmEntry<R>(routine, &ta, &tb, &m, &n, &k, al, static_cast<const R*>(a), &lda,
+                  static_cast<const R*>(b), &ldb, be, static_cast<R*>(c), &ldc);
+  } else {
+    hb::CblasScope scope(name, {3, 2, 5, 4, 6, 7, 10, 11, 8, 9, 12, 13, 14});
+    ZgemmEntry<R>(routine, &tb, &ta, &n, &m, &k, al, static_cast<const R*>(b), &ldb,
+                  static_cast<const R*>(a), &lda, be, static_cast<R*>(c), &ldc);
+  }
+}
+
 template <typename T>
 static void SymmEntry(const char* name, const char* side, const char* uplo,
                       const hwyblas_int* m_p, const hwyblas_int* n_p, const T* alpha_p,
@@ -673,6 +741,39 @@ HWYBLAS_API void ssyrk_(const char* uplo, const char* trans, const hwyblas_int* 
                         const hwyblas_int* lda, const float* beta, float* c,
                         const hwyblas_int* ldc) {
   SyrkEntry<float>("SSYRK", uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+
+HWYBLAS_API void zgemm_(const char* transa, const char* transb, const hwyblas_int* m,
+                        const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                        const double* a, const hwyblas_int* lda, const double* b,
+                        const hwyblas_int* ldb, const double* beta, double* c,
+                        const hwyblas_int* ldc) {
+  ZgemmEntry<double>("ZGEMM", transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+HWYBLAS_API void cgemm_(const char* transa, const char* transb, const hwyblas_int* m,
+                        const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                        const float* a, const hwyblas_int* lda, const float* b,
+                        const hwyblas_int* ldb, const float* beta, float* c,
+                        const hwyblas_int* ldc) {
+  ZgemmEntry<float>("CGEMM", transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+HWYBLAS_API void cblas_zgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k, const void* alpha,
+                             const void* a, const hwyblas_int lda, const void* b,
+                             const hwyblas_int ldb, const void* beta, void* c,
+                             const hwyblas_int ldc) {
+  CblasZgemm<double>("cblas_zgemm", "ZGEMM", layout, transa, transb, m, n, k, alpha, a, lda, b,
+                     ldb, beta, c, ldc);
+}
+HWYBLAS_API void cblas_cgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k, const void* alpha,
+                             const void* a, const hwyblas_int lda, const void* b,
+                             const hwyblas_int ldb, const void* beta, void* c,
+                             const hwyblas_int ldc) {
+  CblasZgemm<float>("cblas_cgemm", "CGEMM", layout, transa, transb, m, n, k, alpha, a, lda, b,
+                    ldb, beta, c, ldc);
 }
 
 HWYBLAS_API void dsymm_(const char* side, const char* uplo, const hwyblas_int* m,

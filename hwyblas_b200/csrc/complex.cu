@@ -1,0 +1,251 @@
+// Complex GEMM (zgemm_, cgemm_), bit-identical to the reference's complex
+// micro-kernel (src/gemm_kernel-inl.h:226-428) in its blocked driver
+// (src/gemm-inl.h:152-232).
+//
+// Complex numbers are interleaved (re, im). For every element of C the
+// reference accumulates four real FMA chains over each KC = 256 chunk of k:
+//
+//   rr = sum ar*br, ir = sum ai*br   (acc_re += a * re(b))
+//   ri = sum ar*bi, ii = sum ai*bi   (acc_im += a * im(b))
+//
+// then forms ab = (rr - ii, ir + ri), r = alpha * ab as
+// (ab.re*al.re - ab.im*al.im, ab.im*al.re + ab.re*al.im) with every product
+// and sum rounded, and merges r into C: r (beta 0), r + C (beta 1, and every
+// chunk after the first), or r + beta*C with beta*C formed the same way.
+// op(A) and op(B) with 'C' are conjugated while loaded (the reference's
+// packing), which negates imaginary parts exactly.
+//
+// The chains are independent per element, so a SIMT kernel computes them
+// directly: 64 x 32 complex tiles per 256-thread CTA, 4 x 2 elements per
+// thread, k in shared-memory slices of 16 (real and imaginary planes apart,
+// so every load is conflict free).
+#include <algorithm>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace hb {
+namespace {
+
+template <typename R>
+__device__ __forceinline__ R Mul(R x, R y) {
+  if constexpr (sizeof(R) == 8) return __dmul_rn(x, y);
+  else return __fmul_rn(x, y);
+}
+template <typename R>
+__device__ __forceinline__ R Add(R x, R y) {
+  if constexpr (sizeof(R) == 8) return __dadd_rn(x, y);
+  else return __fadd_rn(x, y);
+}
+template <typename R>
+__device__ __forceinline__ R Sub(R x, R y) {
+  if constexpr (sizeof(R) == 8) return __dsub_rn(x, y);
+  else return __fsub_rn(x, y);
+}
+template <typename R>
+__device__ __forceinline__ R Fma(R x, R y, R z) {
+  if constexpr (sizeof(R) == 8) return fma(x, y, z);
+  else return fmaf(x, y, z);
+}
+
+constexpr int kZM = 64, kZN = 32, kZK = 16, kZChunk = 256;
+
+// A complex operand: element (i, p) has its real part at
+// data[2 * (i * rs + p * cs)]; conj negates the imaginary part.
+template <typename R>
+struct ZView {
+  const R* data;
+  long long rs, cs;
+  int conj;
+};
+
+template <typename R>
+struct ZParams {
+  int m, n, k;
+  R alpha_re, alpha_im, beta_re, beta_im;
+  ZView<R> a, b;
+  R* c;
+  long long ldc;  // complex elements
+  const int* guard;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  __shared__ R sa_re[kZK][kZM + 1], sa_im[kZK][kZM + 1];
+  __shared__ R sb_re[kZK][kZN + 1], sb_im[kZK][kZN + 1];
+  const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  R rr[4][2] = {}, ir[4][2] = {}, ri[4][2] = {}, ii[4][2] = {};
+  R cre[4][2] = {}, cim[4][2] = {};
+  const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
+  const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
+  for (int k0 = 0; k0 < p.k; k0 += kZK) {
+    for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
+      const int kk = idx / kZM, mm = idx % kZM;
+      const int gi = m0 + mm, gk = k0 + kk;
+      R vr = R(0), vi = R(0);
+      if (gi < p.m && gk < p.k) {
+        const R* e = p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs);
+        vr = e[0];
+        vi = p.a.conj ? -e[1] : e[1];
+      }
+      sa_re[kk][mm] = vr;
+      sa_im[kk][mm] = vi;
+    }
+    for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
+      const int kk = idx / kZN, nn = idx % kZN;
+      const int gj = n0 + nn, gk = k0 + kk;
+      R vr = R(0), vi = R(0);
+      if (gj < p.n && gk < p.k) {
+        const R* e = p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs);
+        vr = e[0];
+        vi = p.b.conj ? -e[1] : e[1];
+      }
+      sb_re[kk][nn] = vr;
+      sb_im[kk][nn] = vi;
+    }
+    __syncthreads();
+    const int kend = min(kZK, p.k - k0);
+    for (int kk = 0; kk < kend; ++kk) {
+      R ar[4], ai[4], br[2], bi[2];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        ar[r] = sa_re[kk][tx + 16 * r];
+        ai[r] = sa_im[kk][tx + 16 * r];
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        br[q] = sb_re[kk][ty + 16 * q];
+        bi[q] = sb_im[kk][ty + 16 * q];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          rr[r][q] = Fma(ar[r], br[q], rr[r][q]);
+          ir[r][q] = Fma(ai[r], br[q], ir[r][q]);
+          ri[r][q] = Fma(ar[r], bi[q], ri[r][q]);
+          ii[r][q] = Fma(ai[r], bi[q], ii[r][q]);
+        }
+      const int kg = k0 + kk;
+      if ((kg + 1) % kZChunk == 0 || kg + 1 == p.k) {
+        const bool first = kg < kZChunk;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
+            const R ab_re = Sub(rr[r][q], ii[r][q]);
+            const R ab_im = Add(ir[r][q], ri[r][q]);
+            const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
+            const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
+            if (!first) {
+              cre[r][q] = Add(t_re, cre[r][q]);
+              cim[r][q] = Add(t_im, cim[r][q]);
+            } else if (i < p.m && j < p.n) {
+              if (beta_zero) {
+                cre[r][q] = t_re;
+                cim[r][q] = t_im;
+              } else {
+                const R* ce = p.c + 2 * (i + j * p.ldc);
+                const R c0 = ce[0], c1 = ce[1];
+                if (beta_one) {
+                  cre[r][q] = Add(t_re, c0);
+                  cim[r][q] = Add(t_im, c1);
+                } else {
+                  const R b_re = Sub(Mul(c0, p.beta_re), Mul(c1, p.beta_im));
+                  const R b_im = Add(Mul(c1, p.beta_re), Mul(c0, p.beta_im));
+                  cre[r][q] = Add(t_re, b_re);
+                  cim[r][q] = Add(t_im, b_im);
+                }
+              }
+            }
+            rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
+          }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
+      if (i < p.m && j < p.n) {
+        R* ce = p.c + 2 * (i + j * p.ldc);
+        ce[0] = cre[r][q];
+        ce[1] = cim[r][q];
+      }
+    }
+}
+
+// C := beta * C (beta 0: zeros, C not read), each element as the complex
+// product (c.re*b.re - c.im*b.im, c.re*b.im + c.im*b.re) (gemm.cc:48-64).
+template <typename R>
+__global__ void ZScaleKernel(int m, int n, R beta_re, R beta_im, R* c, long long ldc,
+                             const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  const long long total = static_cast<long long>(m) * n;
+  const bool zero = (beta_re == R(0) && beta_im == R(0));
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
+    R* ce = c + 2 * (i + j * ldc);
+    if (zero) {
+      ce[0] = R(0);
+      ce[1] = R(0);
+    } else {
+      const R c0 = ce[0], c1 = ce[1];
+      ce[0] = Sub(Mul(c0, beta_re), Mul(c1, beta_im));
+      ce[1] = Add(Mul(c0, beta_im), Mul(c1, beta_re));
+    }
+  }
+}
+
+}  // namespace
+
+// GEMM (src/gemm.cc:67-123) for complex data after argument checks: a, b, c
+// interleaved, leading dimensions in complex elements; alpha, beta as
+// (re, im).
+template <typename R>
+void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, int lda,
+               const R* b, int ldb, const R* beta, R* c, int ldc) {
+  if (m == 0 || n == 0) return;
+  const bool alpha_zero = (alpha[0] == R(0) && alpha[1] == R(0));
+  const bool beta_one = (beta[0] == R(1) && beta[1] == R(0));
+  if ((k == 0 || alpha_zero) && beta_one) return;
+  if (k == 0 || alpha_zero) {
+    const long long total = static_cast<long long>(m) * n;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 8));
+    ZScaleKernel<R><<<blocks, 256, 0, Ctx().stream>>>(m, n, beta[0], beta[1], c, ldc,
+                                                        Ctx().guard);
+    CountLaunch();
+    LaunchFailed("complex scale");
+    return;
+  }
+  ZParams<R> p;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.alpha_re = alpha[0];
+  p.alpha_im = alpha[1];
+  p.beta_re = beta[0];
+  p.beta_im = beta[1];
+  // op: 0 N, 1 T, 2 C. Element (i, p) of op(A): A(i, p) or A(p, i).
+  p.a = ta == 0 ? ZView<R>{a, 1, lda, 0} : ZView<R>{a, lda, 1, ta == 2 ? 1 : 0};
+  p.b = tb == 0 ? ZView<R>{b, 1, ldb, 0} : ZView<R>{b, ldb, 1, tb == 2 ? 1 : 0};
+  p.c = c;
+  p.ldc = ldc;
+  p.guard = Ctx().guard;
+  const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
+  ZgemmKernel<R><<<grid, 256, 0, Ctx().stream>>>(p);
+  CountLaunch();
+  LaunchFailed("complex gemm");
+}
+template void ZgemmFull<double>(int, int, int, int, int, const double*, const double*, int,
+                                const double*, int, const double*, double*, int);
+template void ZgemmFull<float>(int, int, int, int, int, const float*, const float*, int,
+                               const float*, int, const float*, float*, int);
+
+}  // namespace hb

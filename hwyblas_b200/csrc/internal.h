@@ -215,6 +215,11 @@ template <typename T>
 void GerfsFull(bool trans, int n, int nrhs, const T* a, int lda, const T* af, int ldaf,
                const int* ipiv, const T* b, int ldb, T* x, int ldx, T* ferr, T* berr,
                T* work, int* iwork);
+// Complex GEMM (src/gemm.cc:67-123) after argument checks: interleaved
+// (re, im) arrays, leading dimensions in complex elements, op 0 N / 1 T / 2 C.
+template <typename R>
+void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, int lda,
+               const R* b, int ldb, const R* beta, R* c, int ldc);
 template <typename T>
 void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
                 const T* b, int ldb, T beta, T* c, int ldc);

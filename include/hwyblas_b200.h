@@ -83,6 +83,20 @@ HWYBLAS_API void ssyrk_(const char* uplo, const char* trans,
                         const float* alpha, const float* a,
                         const hwyblas_int* lda, const float* beta, float* c,
                         const hwyblas_int* ldc);
+/* Complex GEMM, interleaved (re, im) arrays, leading dimensions in complex
+ * elements, transa/transb N, T or C (conjugate transpose); bit-identical to
+ * the reference's complex micro-kernel. Replace zgemm_ / cgemm_
+ * (include/hwyblas/hwyblas.h:582, 576; src/gemm.cc:67-123). */
+HWYBLAS_API void zgemm_(const char* transa, const char* transb, const hwyblas_int* m,
+                        const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
+                        const double* a, const hwyblas_int* lda, const double* b,
+                        const hwyblas_int* ldb, const double* beta, double* c,
+                        const hwyblas_int* ldc);
+HWYBLAS_API void cgemm_(const char* transa, const char* transb, const hwyblas_int* m,
+                        const hwyblas_int* n, const hwyblas_int* k, const float* alpha,
+                        const float* a, const hwyblas_int* lda, const float* b,
+                        const hwyblas_int* ldb, const float* beta, float* c,
+                        const hwyblas_int* ldc);
 /* C := alpha*A*B + beta*C (side L) or alpha*B*A + beta*C (side R), A
  * symmetric with only the uplo triangle read. Replace dsymm_ / ssymm_
  * (include/hwyblas/hwyblas.h:597, 591; src/level3.cc:369-375, 362-368). */
@@ -475,6 +489,20 @@ HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
  * positions in error reports (include/hwyblas/cblas.h:835, 828 trmm; 714, 708
  * symm; 791, 784 syr2k; 649, 641 gemmtr; 683, 675 gemmt; src/cblas.cc:
  * 1631-1700, 1727-1746, 1842-1861, 1908-1927). */
+/* CBLAS complex GEMM, alpha and beta by address (include/hwyblas/cblas.h:631,
+ * 623; src/cblas.cc:520-537). */
+HWYBLAS_API void cblas_zgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k, const void* alpha,
+                             const void* a, const hwyblas_int lda, const void* b,
+                             const hwyblas_int ldb, const void* beta, void* c,
+                             const hwyblas_int ldc);
+HWYBLAS_API void cblas_cgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_TRANSPOSE transb, const hwyblas_int m,
+                             const hwyblas_int n, const hwyblas_int k, const void* alpha,
+                             const void* a, const hwyblas_int lda, const void* b,
+                             const hwyblas_int ldb, const void* beta, void* c,
+                             const hwyblas_int ldc);
 HWYBLAS_API void cblas_dtrmm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
                              const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
                              const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,

@@ -69,6 +69,12 @@ int orc_sposv(char uplo, int n, int nrhs, float* a, int lda, float* b, int ldb);
 int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
               int ldb);
 
+/* Complex GEMM, interleaved (re, im) (src/gemm.cc:67-123,
+ * src/gemm_kernel-inl.h:226-428). */
+int orc_zgemm(char ta, char tb, int m, int n, int k, const double* alpha, const double* a,
+              int lda, const double* b, int ldb, const double* beta, double* c, int ldc);
+int orc_cgemm(char ta, char tb, int m, int n, int k, const float* alpha, const float* a,
+              int lda, const float* b, int ldb, const float* beta, float* c, int ldc);
 /* Level 3 through the GEMM problem model (src/level3.cc:26-342). */
 int orc_dsymm(char side, char uplo, int m, int n, double alpha, const double* a, int lda,
               const double* b, int ldb, double beta, double* c, int ldc);

@@ -763,6 +763,116 @@ template int Trmm<float>(char, char, char, char, int, int, float, const float*, 
                          int);
 
 // ---------------------------------------------------------------------------
+// Complex GEMM (src/gemm.cc:67-123; src/gemm_kernel-inl.h:226-428;
+// src/gemm-inl.h:152-232), element by element. Arrays interleave (re, im);
+// op 'C' conjugates while packing. Per KC = 256 chunk of k, four fma chains
+// rr = sum ar*br, ir = sum ai*br, ri = sum ar*bi, ii = sum ai*bi give
+// ab = (rr - ii, ir + ri) and r = alpha * ab as (ab.re*al.re - ab.im*al.im,
+// ab.im*al.re + ab.re*al.im), every product and sum rounded; the first chunk
+// merges r, r + C or r + beta*C (beta 0, 1, other), the later ones r + C.
+template <typename R>
+int ZgemmF(char transa, char transb, int m, int n, int k, const R* alpha, const R* a, int lda,
+           const R* b, int ldb, const R* beta, R* c, int ldc) {
+  const auto op = [](char ch) {
+    ch = Up(ch);
+    return ch == 'N' ? 0 : ch == 'T' ? 1 : ch == 'C' ? 2 : -1;
+  };
+  const int ta = op(transa), tb = op(transb);
+  const int rows_a = ta == 0 ? m : k, rows_b = tb == 0 ? k : n;
+  int info = 0;
+  if (ta < 0) info = 1;
+  else if (tb < 0) info = 2;
+  else if (m < 0) info = 3;
+  else if (n < 0) info = 4;
+  else if (k < 0) info = 5;
+  else if (lda < std::max(1, rows_a)) info = 8;
+  else if (ldb < std::max(1, rows_b)) info = 10;
+  else if (ldc < std::max(1, m)) info = 13;
+  if (info) return info;
+  if (m == 0 || n == 0) return 0;
+  const bool alpha_zero = alpha[0] == R(0) && alpha[1] == R(0);
+  const bool beta_zero = beta[0] == R(0) && beta[1] == R(0);
+  const bool beta_one = beta[0] == R(1) && beta[1] == R(0);
+  if ((k == 0 || alpha_zero) && beta_one) return 0;
+  const auto C = [&](int i, int j) { return c + 2 * (i + static_cast<ptrdiff_t>(j) * ldc); };
+  if (k == 0 || alpha_zero) {
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < m; ++i) {
+        R* e = C(i, j);
+        if (beta_zero) {
+          e[0] = e[1] = R(0);
+        } else {
+          const R c0 = e[0], c1 = e[1];
+          const R p0 = c0 * beta[0], p1 = c1 * beta[1], p2 = c0 * beta[1], p3 = c1 * beta[0];
+          e[0] = p0 - p1;
+          e[1] = p2 + p3;
+        }
+      }
+    return 0;
+  }
+  // Element (i, p) of op(A) and (p, j) of op(B) as (re, im).
+  const auto opa = [&](int i, int p, R* re, R* im) {
+    const R* e = ta == 0 ? a + 2 * (i + static_cast<ptrdiff_t>(p) * lda)
+                         : a + 2 * (p + static_cast<ptrdiff_t>(i) * lda);
+    *re = e[0];
+    *im = ta == 2 ? -e[1] : e[1];
+  };
+  const auto opb = [&](int p, int j, R* re, R* im) {
+    const R* e = tb == 0 ? b + 2 * (p + static_cast<ptrdiff_t>(j) * ldb)
+                         : b + 2 * (j + static_cast<ptrdiff_t>(p) * ldb);
+    *re = e[0];
+    *im = tb == 2 ? -e[1] : e[1];
+  };
+  constexpr int KC = 256;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      R cre = R(0), cim = R(0);
+      for (int pc = 0; pc < k; pc += KC) {
+        const int pe = std::min(k, pc + KC);
+        R rr = R(0), ir = R(0), ri = R(0), ii = R(0);
+        for (int p = pc; p < pe; ++p) {
+          R ar, ai, br, bi;
+          opa(i, p, &ar, &ai);
+          opb(p, j, &br, &bi);
+          rr = std::fma(ar, br, rr);
+          ir = std::fma(ai, br, ir);
+          ri = std::fma(ar, bi, ri);
+          ii = std::fma(ai, bi, ii);
+        }
+        const R ab_re = rr - ii, ab_im = ir + ri;
+        const R q0 = ab_re * alpha[0], q1 = ab_im * alpha[1];
+        const R q2 = ab_im * alpha[0], q3 = ab_re * alpha[1];
+        const R t_re = q0 - q1, t_im = q2 + q3;
+        if (pc != 0) {
+          cre = t_re + cre;
+          cim = t_im + cim;
+        } else if (beta_zero) {
+          cre = t_re;
+          cim = t_im;
+        } else {
+          const R c0 = C(i, j)[0], c1 = C(i, j)[1];
+          if (beta_one) {
+            cre = t_re + c0;
+            cim = t_im + c1;
+          } else {
+            const R s0 = c0 * beta[0], s1 = c1 * beta[1], s2 = c1 * beta[0], s3 = c0 * beta[1];
+            const R b_re = s0 - s1, b_im = s2 + s3;
+            cre = t_re + b_re;
+            cim = t_im + b_im;
+          }
+        }
+      }
+      C(i, j)[0] = cre;
+      C(i, j)[1] = cim;
+    }
+  return 0;
+}
+template int ZgemmF<double>(char, char, int, int, int, const double*, const double*, int,
+                            const double*, int, const double*, double*, int);
+template int ZgemmF<float>(char, char, int, int, int, const float*, const float*, int,
+                           const float*, int, const float*, float*, int);
+
+// ---------------------------------------------------------------------------
 // IAMAX (src/level1.cc:383-402; src/level1-inl.h:343-423): 1-based index of
 // the first element of largest |x|; NaNs never compare larger, so one is only
 // returned when it is x[0].
@@ -835,6 +945,15 @@ int orc_ssyrk(char uplo, char trans, int n, int k, float alpha, const float* a, 
               float beta, float* c, int ldc) {
   return orc::Syrk<float>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
 }
+int orc_zgemm(char ta, char tb, int m, int n, int k, const double* alpha, const double* a,
+              int lda, const double* b, int ldb, const double* beta, double* c, int ldc) {
+  return orc::ZgemmF<double>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int orc_cgemm(char ta, char tb, int m, int n, int k, const float* alpha, const float* a,
+              int lda, const float* b, int ldb, const float* beta, float* c, int ldc) {
+  return orc::ZgemmF<float>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
 #define ORC_L3(P, T)                                                                       \
   int orc_##P##symm(char side, char uplo, int m, int n, T alpha, const T* a, int lda,       \
                     const T* b, int ldb, T beta, T* c, int ldc) {                            \

@@ -91,6 +91,8 @@ class Oracle:
         L.orc_spotrs.argtypes = [CH, I, I, P, I, P, I]
         L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
         L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
+        L.orc_zgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
+        L.orc_cgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
         for pre in "ds":
             getattr(L, f"orc_{pre}gerfs").argtypes = [CH, I, I, P, I, P, I, P, P, I, P, I, P,
                                                        P, P, P]
@@ -210,6 +212,16 @@ class Oracle:
                                                   ldaf, ptr(ipiv), ptr(b), ldb, ptr(x), ldx,
                                                   ptr(ferr), ptr(berr), ptr(work), ptr(iwork))
 
+    def zgemm(self, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+        """Complex GEMM on complex128 / complex64 arrays (by c's dtype)."""
+        z = c.dtype == np.complex128
+        rt = np.float64 if z else np.float32
+        al = np.array([complex(alpha).real, complex(alpha).imag], rt)
+        be = np.array([complex(beta).real, complex(beta).imag], rt)
+        fn = self.lib.orc_zgemm if z else self.lib.orc_cgemm
+        return fn(_b(ta), _b(tb), m, n, k, al.ctypes.data, ptr(a), lda, ptr(b), ldb,
+                  be.ctypes.data, ptr(c), ldc)
+
     def getri(self, n, a, lda, ipiv, work, lwork):
         p = "s" if a.dtype == np.float32 else "d"
         return getattr(self.lib, f"orc_{p}getri")(n, ptr(a), lda, ptr(ipiv), ptr(work), lwork)
@@ -289,6 +301,12 @@ def ref_call_trtri(lib, unblocked, uplo, diag, n, a, lda):
 def rand(rng, rows, cols, dtype=np.float64):
     """Column-major uniform[-1, 1] matrix (the reference tests' Random<T>)."""
     return np.asfortranarray(rng.uniform(-1.0, 1.0, (rows, cols)).astype(dtype))
+
+
+def creal(x):
+    """The interleaved real view of a complex array (any order)."""
+    x = np.ascontiguousarray(np.asarray(x).T)
+    return x.view(np.float64 if x.dtype == np.complex128 else np.float32)
 
 
 def same_bits(x, y):

@@ -17,7 +17,7 @@
 import numpy as np
 import pytest
 
-from tests.oracle_lib import (rand, ref_call_getrf, ref_call_gesv, ref_call_potrf,
+from tests.oracle_lib import (creal, rand, ref_call_getrf, ref_call_gesv, ref_call_potrf,
                               same_bits, first_diff)
 
 EPS = np.finfo(np.float64).eps
@@ -756,6 +756,57 @@ def test_gerfs_bounds_and_arguments(orc):
                      iwork) == -10
     assert orc.gerfs("N", n, 1, a, n, af, n, ipiv, b, n, x, n - 1, ferr, berr, work,
                      iwork) == -12
+
+
+def crand(rng, rows, cols, dtype=np.complex128):
+    return np.asfortranarray((rng.uniform(-1, 1, (rows, cols))
+                              + 1j * rng.uniform(-1, 1, (rows, cols))).astype(dtype))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("ta", ["N", "T", "C"])
+@pytest.mark.parametrize("tb", ["N", "T", "C"])
+def test_zgemm_elementwise_bound(orc, dtype, ta, tb):
+    """Complex GEMM within the element-wise bound 4(k+2)eps of the exact
+    product (tests/gemm_test.cc:46-113 with complex types), op C conjugating,
+    across KC chunks."""
+    rng = np.random.default_rng(3)
+    m, n, k = 37, 23, 300
+    a = crand(rng, m if ta == "N" else k, k if ta == "N" else m, dtype)
+    b = crand(rng, k if tb == "N" else n, n if tb == "N" else k, dtype)
+    c = crand(rng, m, n, dtype)
+    op = lambda x, t: x if t == "N" else (x.T if t == "T" else x.conj().T)  # noqa: E731
+    A, B = op(a.astype(np.complex128), ta), op(b.astype(np.complex128), tb)
+    alpha, beta = 1.5 - 0.5j, 0.25 + 0.75j
+    want = alpha * (A @ B) + beta * c.astype(np.complex128)
+    bound = abs(alpha) * (np.abs(A) @ np.abs(B)) + abs(beta) * np.abs(c)
+    c1 = c.copy(order="F")
+    assert orc.zgemm(ta, tb, m, n, k, alpha, a, a.shape[0], b, b.shape[0], beta, c1, m) == 0
+    eps = np.finfo(dtype).eps
+    assert np.all(np.abs(c1.astype(np.complex128) - want) <= 4 * (k + 2) * eps * bound * 2)
+
+
+def test_zgemm_special_cases(orc):
+    """alpha = 0 scales C (beta 0 writes zeros without reading C), beta = 1
+    with alpha = 0 leaves C, argument checks (src/gemm.cc:67-123)."""
+    rng = np.random.default_rng(4)
+    nan = np.full((4, 4), np.nan + 1j * np.nan, order="F")
+    c = crand(rng, 4, 4)
+    c1 = c.copy(order="F")
+    assert orc.zgemm("N", "N", 4, 4, 4, 0.0, nan, 4, nan, 4, 1.0, c1, 4) == 0
+    assert same_bits(creal(c1), creal(c))
+    assert orc.zgemm("N", "N", 4, 4, 4, 0.0, nan, 4, nan, 4, 2.0 - 1.0j, c1, 4) == 0
+    assert np.allclose(c1, (2 - 1j) * c, rtol=1e-15)
+    c2 = nan.copy(order="F")
+    assert orc.zgemm("C", "T", 4, 4, 0, 1.0, nan, 4, nan, 4, 0.0, c2, 4) == 0
+    assert np.all(c2 == 0)
+    z = np.zeros((4, 4), np.complex128, order="F")
+    assert orc.zgemm("X", "N", 4, 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 1
+    assert orc.zgemm("N", "X", 4, 4, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 2
+    assert orc.zgemm("N", "N", 4, 4, -1, 1.0, z, 4, z, 4, 0.0, z, 4) == 5
+    assert orc.zgemm("T", "N", 4, 4, 5, 1.0, z, 4, z, 5, 0.0, z, 4) == 8
+    assert orc.zgemm("N", "C", 4, 5, 4, 1.0, z, 4, z, 4, 0.0, z, 4) == 10
+    assert orc.zgemm("N", "N", 5, 4, 4, 1.0, z, 5, z, 4, 0.0, z, 4) == 13
 
 
 def test_trsm_alpha_zero_does_not_read_a(orc):
