@@ -16,7 +16,7 @@
 // packing), which negates imaginary parts exactly.
 //
 // The chains are independent per element, so a SIMT kernel computes them
-// directly: 64 x 32 complex tiles per 256-thread CTA, 4 x 2 elements per
+// directly: 64 x 64 complex tiles per 256-thread CTA, 4 x 4 elements per
 // thread, k in shared-memory slices of 16 (real and imaginary planes apart,
 // so every load is conflict free).
 #include <algorithm>
@@ -48,7 +48,7 @@ __device__ __forceinline__ R Fma(R x, R y, R z) {
   else return fmaf(x, y, z);
 }
 
-constexpr int kZM = 64, kZN = 32, kZK = 16, kZChunk = 256;
+constexpr int kZM = 64, kZN = 64, kZK = 16, kZChunk = 256;
 
 // A complex operand: element (i, p) has its real part at
 // data[2 * (i * rs + p * cs)]; conj negates the imaginary part.
@@ -69,6 +69,10 @@ struct ZParams {
   const int* guard;
 };
 
+// One CTA: a 64 x 64 complex tile, 4 x 4 elements per thread (rows
+// tx + 16 r, columns ty + 16 q). A chunk ends on a slice boundary (256 is a
+// multiple of 16), where the thread merges its chunk into C in memory: the
+// running value stays in C itself, so no registers hold it.
 template <typename R>
 __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
   if (p.guard != nullptr && *p.guard != 0) return;
@@ -76,8 +80,11 @@ __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
   __shared__ R sb_re[kZK][kZN + 1], sb_im[kZK][kZN + 1];
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  R rr[4][2] = {}, ir[4][2] = {}, ri[4][2] = {}, ii[4][2] = {};
-  R cre[4][2] = {}, cim[4][2] = {};
+  R rr[4][4], ir[4][4], ri[4][4], ii[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
   const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
   const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
   for (int k0 = 0; k0 < p.k; k0 += kZK) {
@@ -106,78 +113,59 @@ __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
       sb_im[kk][nn] = vi;
     }
     __syncthreads();
-    const int kend = min(kZK, p.k - k0);
-    for (int kk = 0; kk < kend; ++kk) {
-      R ar[4], ai[4], br[2], bi[2];
+    const auto step = [&](int kk) {
+      R ar[4], ai[4], br[4], bi[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         ar[r] = sa_re[kk][tx + 16 * r];
         ai[r] = sa_im[kk][tx + 16 * r];
-      }
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        br[q] = sb_re[kk][ty + 16 * q];
-        bi[q] = sb_im[kk][ty + 16 * q];
+        br[r] = sb_re[kk][ty + 16 * r];
+        bi[r] = sb_im[kk][ty + 16 * r];
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < 4; ++q) {
           rr[r][q] = Fma(ar[r], br[q], rr[r][q]);
           ir[r][q] = Fma(ai[r], br[q], ir[r][q]);
           ri[r][q] = Fma(ar[r], bi[q], ri[r][q]);
           ii[r][q] = Fma(ai[r], bi[q], ii[r][q]);
         }
-      const int kg = k0 + kk;
-      if ((kg + 1) % kZChunk == 0 || kg + 1 == p.k) {
-        const bool first = kg < kZChunk;
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
-            const R ab_re = Sub(rr[r][q], ii[r][q]);
-            const R ab_im = Add(ir[r][q], ri[r][q]);
-            const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
-            const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
-            if (!first) {
-              cre[r][q] = Add(t_re, cre[r][q]);
-              cim[r][q] = Add(t_im, cim[r][q]);
-            } else if (i < p.m && j < p.n) {
-              if (beta_zero) {
-                cre[r][q] = t_re;
-                cim[r][q] = t_im;
-              } else {
-                const R* ce = p.c + 2 * (i + j * p.ldc);
-                const R c0 = ce[0], c1 = ce[1];
-                if (beta_one) {
-                  cre[r][q] = Add(t_re, c0);
-                  cim[r][q] = Add(t_im, c1);
-                } else {
-                  const R b_re = Sub(Mul(c0, p.beta_re), Mul(c1, p.beta_im));
-                  const R b_im = Add(Mul(c1, p.beta_re), Mul(c0, p.beta_im));
-                  cre[r][q] = Add(t_re, b_re);
-                  cim[r][q] = Add(t_im, b_im);
-                }
-              }
-            }
-            rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
-          }
-      }
-    }
+    };
+    const int kend = min(kZK, p.k - k0);
+#pragma unroll 2
+    for (int kk = 0; kk < kend; ++kk) step(kk);
     __syncthreads();
-  }
+    if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= p.k) {
+      const bool first = k0 < kZChunk;
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 4; ++r)
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
-      if (i < p.m && j < p.n) {
-        R* ce = p.c + 2 * (i + j * p.ldc);
-        ce[0] = cre[r][q];
-        ce[1] = cim[r][q];
-      }
+        for (int q = 0; q < 4; ++q) {
+          const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
+          const R ab_re = Sub(rr[r][q], ii[r][q]);
+          const R ab_im = Add(ir[r][q], ri[r][q]);
+          rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
+          if (i >= p.m || j >= p.n) continue;
+          const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
+          const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
+          R* ce = p.c + 2 * (i + j * p.ldc);
+          if (first && beta_zero) {
+            ce[0] = t_re;
+            ce[1] = t_im;
+          } else if (!first || beta_one) {
+            ce[0] = Add(t_re, ce[0]);
+            ce[1] = Add(t_im, ce[1]);
+          } else {
+            const R c0 = ce[0], c1 = ce[1];
+            const R b_re = Sub(Mul(c0, p.beta_re), Mul(c1, p.beta_im));
+            const R b_im = Add(Mul(c1, p.beta_re), Mul(c0, p.beta_im));
+            ce[0] = Add(t_re, b_re);
+            ce[1] = Add(t_im, b_im);
+          }
+        }
     }
+  }
 }
 
 // C := beta * C (beta 0: zeros, C not read), each element as the complex

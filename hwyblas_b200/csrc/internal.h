@@ -226,6 +226,11 @@ void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a,
 template <typename T>
 void TrmmFull(bool left, bool lower, bool trans, bool unit, int m, int n, T alpha,
               const T* a, int lda, T* b, int ldb);
+// TRMM with the triangle already dense in tri (zeros outside it, ones on a
+// unit diagonal), leading dimension ldt.
+template <typename T>
+void TrmmDense(bool left, bool lower, bool trans, int m, int n, T alpha, const T* tri, int ldt,
+               T* b, int ldb);
 template <typename T>
 void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
               int lda, const T* b, int ldb, T beta, T* c, int ldc);

@@ -95,6 +95,85 @@ __global__ void __launch_bounds__(kTrti2Threads)
   }
 }
 
+// TRTI2 of the diagonal blocks of order nb (the last one n - (nblk-1) nb) of
+// an n x n triangle, one CTA per block, the block in shared memory; each
+// block's arithmetic is Trti2Kernel's. orig receives the blocks as they were
+// (leading dimension nb), for the TRSMs that divide by them.
+template <typename T>
+__global__ void __launch_bounds__(64)
+    Trti2BlocksKernel(int n, int nb, T* a, long long lda, int upper, int unit, T* orig,
+                      const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ T s[64][65];
+  const int j0 = blockIdx.x * nb, jb = min(nb, n - j0), t = threadIdx.x;
+  T* blk = a + j0 + static_cast<long long>(j0) * lda;
+  T* saved = orig + static_cast<long long>(blockIdx.x) * nb * nb;
+  for (int j = 0; j < jb; ++j) {
+    if (t < jb) {
+      const T v = blk[t + j * lda];
+      s[t][j] = v;
+      saved[t + j * nb] = v;
+    }
+  }
+  __syncthreads();
+  for (int step = 0; step < jb; ++step) {
+    const int j = upper ? step : jb - 1 - step;
+    T ajj = T(-1), dinv = T(0);
+    if (!unit) {
+      dinv = T(1) / s[j][j];
+      ajj = -dinv;
+    }
+    T y = T(0);
+    bool mine = false;
+    if (upper && t < j) {
+      mine = true;
+      const int send = min((t & ~3) + 4, j);
+      for (int jj = t; jj < send; ++jj) {
+        const T v = (jj == t && unit) ? T(1) : s[t][jj];
+        y = AddRn(y, MulRn(v, s[jj][j]));
+      }
+      for (int c = send; c < j; ++c) y = Fma(s[t][c], s[c][j], y);
+      y = MulRn(y, ajj);
+    } else if (!upper && t > j && t < jb) {
+      mine = true;
+      const int r0 = j + 1, li = t - r0, s0 = li & ~3;
+      for (int lc = 0; lc < s0; ++lc) y = Fma(s[t][r0 + lc], s[r0 + lc][j], y);
+      for (int lc = s0; lc <= li; ++lc) {
+        const T v = (lc == li && unit) ? T(1) : s[t][r0 + lc];
+        y = AddRn(y, MulRn(v, s[r0 + lc][j]));
+      }
+      y = MulRn(y, ajj);
+    }
+    __syncthreads();
+    if (mine) s[t][j] = y;
+    if (t == j && !unit) s[j][j] = dinv;
+    __syncthreads();
+  }
+  if (t < jb) {
+    for (int j = 0; j < jb; ++j) {
+      const bool tri = upper ? t <= j : t >= j;
+      if (tri) blk[t + j * lda] = s[t][j];
+    }
+  }
+}
+
+// dense(i, j) := the triangle value of A(i, j) (zero outside it, one on a
+// unit diagonal) for i in [r0, r1), j in [c0, c1).
+template <typename T>
+__global__ void DenseTriangleKernel(int r0, int r1, int c0, int c1, const T* a, long long lda,
+                                    int upper, int unit, T* dense, long long ldd) {
+  const int rows = r1 - r0;
+  const long long total = static_cast<long long>(rows) * (c1 - c0);
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = r0 + static_cast<int>(e % rows), j = c0 + static_cast<int>(e / rows);
+    T v = T(0);
+    if (i == j) v = unit ? T(1) : a[i + j * lda];
+    else if (upper ? i < j : i > j) v = a[i + j * lda];
+    dense[i + j * ldd] = v;
+  }
+}
+
 // *out = 1 + the first i with A(i, i) == 0, or 0.
 template <typename T>
 __global__ void FirstZeroDiagKernel(int n, const T* a, long long lda, int* out) {
@@ -213,27 +292,60 @@ int TrtriFull(bool upper, bool unit, int n, T* a, int lda) {
     Trti2<T>(upper, unit, n, a, lda);
     return 0;
   }
+  // Every diagonal block's TRTI2 reads only that block, and the reference
+  // inverts block j right after the TRMM and TRSM of its block column, which
+  // write other entries and divide by the block as it was. So all blocks are
+  // inverted at once up front (one CTA each), their original values kept for
+  // those TRSMs; every value is the same as in the reference's order.
+  const int nblk = (n + nb - 1) / nb;
+  T* orig = static_cast<T*>(
+      Workspace(kWsTrti2, sizeof(T) * static_cast<size_t>(nblk) * nb * nb));
+  if (orig == nullptr) return 0;
+  Trti2BlocksKernel<T><<<nblk, 64, 0, Ctx().stream>>>(n, nb, a, lda, upper ? 1 : 0,
+                                                       unit ? 1 : 0, orig, Ctx().guard);
+  CountLaunch();
+  if (LaunchFailed("trti2 blocks")) return 0;
   const auto A = [&](int i, int j) { return a + i + static_cast<long long>(j) * lda; };
+  const auto D = [&](int j) { return orig + static_cast<long long>(j / nb) * nb * nb; };
+  // The finished part of the inverse, kept dense for the TRMMs (each TRMM
+  // multiplies by it with the zeros and ones written out): one block column
+  // is added per step instead of rewriting the whole triangle. Workspaces
+  // are sized once, so that no step reallocates.
+  const long long ldd = (n + 1) / 2 * 2;
+  T* dense = static_cast<T*>(Workspace(kWsLevel3, sizeof(T) * static_cast<size_t>(ldd) * n));
+  if (dense == nullptr ||
+      Workspace(kWsLevel3Copy, sizeof(T) * static_cast<size_t>(n) * nb) == nullptr)
+    return 0;
+  Failed(cudaMemsetAsync(dense, 0, sizeof(T) * static_cast<size_t>(ldd) * n, Ctx().stream),
+         "trtri dense");
+  const auto add_columns = [&](int r0, int r1, int c0, int c1) {
+    const long long total = static_cast<long long>(r1 - r0) * (c1 - c0);
+    if (total <= 0) return;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 4096));
+    DenseTriangleKernel<T><<<blocks, 256, 0, Ctx().stream>>>(r0, r1, c0, c1, a, lda,
+                                                              upper ? 1 : 0, unit ? 1 : 0,
+                                                              dense, ldd);
+    CountLaunch();
+  };
   if (upper) {
-    for (int j = 0; j < n; j += nb) {
+    add_columns(0, std::min(nb, n), 0, std::min(nb, n));
+    for (int j = nb; j < n; j += nb) {
       const int jb = std::min(nb, n - j);
-      if (j > 0) {
-        TrmmFull<T>(true, false, false, unit, j, jb, T(1), a, lda, A(0, j), lda);
-        TrsmFull<T>(false, false, false, unit, j, jb, T(-1), A(j, j), lda, A(0, j), lda);
-      }
-      Trti2<T>(true, unit, jb, A(j, j), lda);
+      TrmmDense<T>(true, false, false, j, jb, T(1), dense, static_cast<int>(ldd), A(0, j), lda);
+      TrsmFull<T>(false, false, false, unit, j, jb, T(-1), D(j), nb, A(0, j), lda);
+      add_columns(0, j + jb, j, j + jb);
     }
   } else {
     const int nn = ((n - 1) / nb) * nb;
-    for (int j = nn; j >= 0; j -= nb) {
+    add_columns(nn, n, nn, n);
+    for (int j = nn - nb; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
-      if (j + jb < n) {
-        const int m = n - j - jb;
-        TrmmFull<T>(true, true, false, unit, m, jb, T(1), A(j + jb, j + jb), lda, A(j + jb, j),
-                    lda);
-        TrsmFull<T>(false, true, false, unit, m, jb, T(-1), A(j, j), lda, A(j + jb, j), lda);
-      }
-      Trti2<T>(false, unit, jb, A(j, j), lda);
+      const int m = n - j - jb;
+      const T* tri = dense + (j + jb) + (j + jb) * ldd;
+      TrmmDense<T>(true, true, false, m, jb, T(1), tri, static_cast<int>(ldd), A(j + jb, j),
+                   lda);
+      TrsmFull<T>(false, true, false, unit, m, jb, T(-1), D(j), nb, A(j + jb, j), lda);
+      add_columns(j, n, j, j + jb);
     }
   }
   return 0;
@@ -247,6 +359,7 @@ template <typename T>
 int GetriFull(int n, T* a, int lda, const int* ipiv, int lwork, int* iws_out) {
   const int info = TrtriFull<T>(true, false, n, a, lda);
   if (info > 0) return info;
+
   int nb = 64;  // ILAENV(1, xGETRI) (src/lapack/environment.cc:105-106)
   int nbmin = 2;
   const int ldwork = n;
@@ -282,7 +395,10 @@ int GetriFull(int n, T* a, int lda, const int* ipiv, int lwork, int* iws_out) {
       }
     }
   } else {
-    const size_t welems = static_cast<size_t>(ldwork) * nb;
+    // The block columns of L, leading dimension rounded up to even so that
+    // the GEMM reads them in place.
+    const int ldw = (ldwork + 1) / 2 * 2;
+    const size_t welems = static_cast<size_t>(ldw) * nb;
     T* w = static_cast<T*>(Workspace(kWsGetri, sizeof(T) * welems));
     if (w == nullptr) return 0;
     // Entries on and above the diagonal of a block are never read; zeroed
@@ -291,14 +407,14 @@ int GetriFull(int n, T* a, int lda, const int* ipiv, int lwork, int* iws_out) {
     const int nn = ((n - 1) / nb) * nb;
     for (int j = nn; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
-      GetriCopyKernel<T><<<dim3((n + 255) / 256, jb), 256, 0, st>>>(n, j, a, lda, w, ldwork);
+      GetriCopyKernel<T><<<dim3((n + 255) / 256, jb), 256, 0, st>>>(n, j, a, lda, w, ldw);
       CountLaunch();
       if (LaunchFailed("getri copy")) return 0;
       if (j + jb < n) {
-        GemmFull<T>(false, false, n, jb, n - j - jb, T(-1), A(0, j + jb), lda, w + j + jb,
-                    ldwork, T(1), A(0, j), lda);
+        GemmFull<T>(false, false, n, jb, n - j - jb, T(-1), A(0, j + jb), lda, w + j + jb, ldw,
+                    T(1), A(0, j), lda);
       }
-      TrsmFull<T>(false, true, false, true, n, jb, T(1), w + j, ldwork, A(0, j), lda);
+      TrsmFull<T>(false, true, false, true, n, jb, T(1), w + j, ldw, A(0, j), lda);
     }
   }
   if (n > 1) {

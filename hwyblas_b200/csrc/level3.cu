@@ -505,12 +505,23 @@ void TrmmFull(bool left, bool lower, bool trans, bool unit, int m, int n, T alph
   }
   const int ka = left ? m : n;
   T* tri = static_cast<T*>(Workspace(kWsLevel3, sizeof(T) * static_cast<size_t>(ka) * ka));
-  T* copy = static_cast<T*>(Workspace(kWsLevel3Copy, sizeof(T) * static_cast<size_t>(m) * n));
-  if (tri == nullptr || copy == nullptr) return;
+  if (tri == nullptr) return;
   TriangleFullKernel<T><<<GridFor(static_cast<long long>(ka) * ka), 256, 0, Ctx().stream>>>(
       ka, a, lda, lower, unit, tri, ka);
   CountLaunch();
   if (LaunchFailed("trmm triangle")) return;
+  TrmmDense<T>(left, lower, trans, m, n, alpha, tri, ka, b, ldb);
+}
+
+// TRMM on a triangle already stored dense (zeros and unit diagonal written
+// out), from a copy of B.
+template <typename T>
+void TrmmDense(bool left, bool lower, bool trans, int m, int n, T alpha, const T* tri, int ldt,
+               T* b, int ldb) {
+  if (m == 0 || n == 0) return;
+  const int ka = left ? m : n;
+  T* copy = static_cast<T*>(Workspace(kWsLevel3Copy, sizeof(T) * static_cast<size_t>(m) * n));
+  if (copy == nullptr) return;
   if (Failed(cudaMemcpy2DAsync(copy, sizeof(T) * m, b, sizeof(T) * ldb, sizeof(T) * m, n,
                                cudaMemcpyDeviceToDevice, Ctx().stream),
              "trmm copy"))
@@ -518,13 +529,17 @@ void TrmmFull(bool left, bool lower, bool trans, bool unit, int m, int n, T alph
   // op(A) is lower exactly when A is lower and not transposed, or upper and
   // transposed (src/api.h:133-140).
   const bool op_lower = (lower != trans);
-  const View<T> t = ColMajor<T>(tri, ka, trans), g = ColMajor<T>(copy, m);
+  const View<T> t = ColMajor<T>(tri, ldt, trans), g = ColMajor<T>(copy, m);
   if (left) {
     GemmPart<T>(m, n, ka, alpha, t, g, T(0), b, ldb, kAll, op_lower ? kTriALower : kTriAUpper);
   } else {
     GemmPart<T>(m, n, ka, alpha, g, t, T(0), b, ldb, kAll, op_lower ? kTriBLower : kTriBUpper);
   }
 }
+template void TrmmDense<double>(bool, bool, bool, int, int, double, const double*, int,
+                                double*, int);
+template void TrmmDense<float>(bool, bool, bool, int, int, float, const float*, int, float*,
+                               int);
 template void TrmmFull<double>(bool, bool, bool, bool, int, int, double, const double*, int,
                                double*, int);
 template void TrmmFull<float>(bool, bool, bool, bool, int, int, float, const float*, int,
