@@ -54,6 +54,10 @@ struct GemmParams {
   long long ldc;
   int part;
   int tri;  // Tri: which operand is triangular (TRMM)
+  // Split over the KC chunks of k: work item (tile, chunk) writes the
+  // chunk's raw accumulators to partial[(chunk * n + j) * m + i].
+  double* partial;
+  int nchunks;
   int* timeout_flag;
   const int* guard;
 };
@@ -164,32 +168,54 @@ struct Producer {
   int tile, kt, kt_hi, gs;
 };
 
-template <bool kTri>
+// The k-slices [*lo, *hi) of work item w (a tile, or a tile's chunk when
+// split); false when the tile lies outside C's part.
+template <bool kTri, bool kSplit>
+__device__ __forceinline__ bool WorkRange(const GemmParams& p, int w, int tiles_m, int tiles_n,
+                                          int kt_total, int* m0, int* n0, int* lo, int* hi) {
+  const int tile = kSplit ? w / p.nchunks : w;
+  TileOrigin(tile, tiles_m, tiles_n, m0, n0);
+  if (SkipTile(p, *m0, *n0)) return false;
+  *lo = 0;
+  *hi = kt_total;
+  if constexpr (kTri) TileKRange(p, *m0, *n0, kt_total, lo, hi);
+  if constexpr (kSplit) {
+    const int c = w % p.nchunks;
+    *lo = max(*lo, c * kKtPerChunk);
+    *hi = min(*hi, (c + 1) * kKtPerChunk);
+  }
+  return true;
+}
+
+template <bool kTri, bool kSplit>
 __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
                                           int tiles_m, int tiles_n, int kt_total,
                                           uint8_t* smem, uint64_t* full,
                                           uint64_t* empty, const CUtensorMap* tm_a,
                                           const CUtensorMap* tm_b) {
   const int num_tiles = tiles_m * tiles_n;
+  const int num_work = kSplit ? num_tiles * p.nchunks : num_tiles;
   int m0 = 0, n0 = 0;
-  while (pr.tile < num_tiles) {
-    TileOrigin(pr.tile, tiles_m, tiles_n, &m0, &n0);
-    if constexpr (!kTri) {
+  while (pr.tile < num_work) {
+    if constexpr (!kTri && !kSplit) {
+      TileOrigin(pr.tile, tiles_m, tiles_n, &m0, &n0);
       if (!SkipTile(p, m0, n0)) break;
-    } else if (!SkipTile(p, m0, n0)) {
-      if (pr.kt >= 0) break;
+    } else {
       int lo, hi;
-      TileKRange(p, m0, n0, kt_total, &lo, &hi);
-      if (lo < hi) {
-        pr.kt = lo;
-        pr.kt_hi = hi;
-        break;
+      if (WorkRange<kTri, kSplit>(p, pr.tile, tiles_m, tiles_n, kt_total, &m0, &n0, &lo,
+                                  &hi)) {
+        if (pr.kt >= 0) break;
+        if (lo < hi) {
+          pr.kt = lo;
+          pr.kt_hi = hi;
+          break;
+        }
       }
     }
     pr.tile += gridDim.x;
-    if constexpr (kTri) pr.kt = -1;
+    if constexpr (kTri || kSplit) pr.kt = -1;
   }
-  if (pr.tile >= num_tiles) return true;
+  if (pr.tile >= num_work) return true;
   const int s = pr.gs % kStages, round = pr.gs / kStages;
   if (round > 0 && !MbarWait(&empty[s], (round - 1) & 1, p.timeout_flag)) return false;
   uint8_t* st = smem + s * kStageBytes;
@@ -199,8 +225,8 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
     TmaLoad2d(st + b * kABoxBytes, tm_a, m0 + 16 * b, pr.kt * kBK, &full[s]);
   TmaLoad2d(st + kTileABytes, tm_b, pr.kt * kBK, n0, &full[s]);
   ++pr.gs;
-  if (++pr.kt == (kTri ? pr.kt_hi : kt_total)) {
-    pr.kt = kTri ? -1 : 0;
+  if (++pr.kt == ((kTri || kSplit) ? pr.kt_hi : kt_total)) {
+    pr.kt = (kTri || kSplit) ? -1 : 0;
     pr.tile += gridDim.x;
   }
   return true;
@@ -218,7 +244,7 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
 // chains over the in-range k only, in the MMA's own ascending order. A chunk
 // whose range is empty for an element leaves it unmerged, as the reference
 // skips that micro-tile (src/gemm-inl.h:202-209).
-template <bool kTri>
+template <bool kTri, bool kSplit>
 __global__ void __maxnreg__(168)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
@@ -229,6 +255,7 @@ __global__ void __maxnreg__(168)
   // tile's epilogue.
   const int tiles_m = (p.m + kBM - 1) / kBM, tiles_n = (p.n + kBN - 1) / kBN;
   const int num_tiles = tiles_m * tiles_n;
+  const int num_work = kSplit ? num_tiles * p.nchunks : num_tiles;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024 - (SmemAddr(smem_raw) & 1023)) & 1023);
@@ -249,10 +276,10 @@ __global__ void __maxnreg__(168)
     if (lane == 0) {
       PrefetchTmap(&tm_a);
       PrefetchTmap(&tm_b);
-      Producer pr{static_cast<int>(blockIdx.x), kTri ? -1 : 0, 0, 0};
-      while (pr.tile < num_tiles) {
-        if (!IssueNext<kTri>(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
-                             &tm_a, &tm_b))
+      Producer pr{static_cast<int>(blockIdx.x), (kTri || kSplit) ? -1 : 0, 0, 0};
+      while (pr.tile < num_work) {
+        if (!IssueNext<kTri, kSplit>(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
+                                     &tm_a, &tm_b))
           return;
       }
     }
@@ -268,12 +295,17 @@ __global__ void __maxnreg__(168)
   const int ccol1 = 2 * ((2 * t + 1) & 3) + ((2 * t + 1) >> 2);
   const int bcol = 2 * (g & 3) + (g >> 2);  // tile column of this lane's B
   int gs = 0;
-  for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
-    int m0, n0;
-    TileOrigin(tile, tiles_m, tiles_n, &m0, &n0);
-    if (SkipTile(p, m0, n0)) continue;
-    int kt_lo = 0, kt_hi = kt_total;
-    if constexpr (kTri) TileKRange(p, m0, n0, kt_total, &kt_lo, &kt_hi);
+  for (int w = blockIdx.x; w < num_work; w += gridDim.x) {
+    int m0, n0, kt_lo = 0, kt_hi = kt_total;
+    if constexpr (!kTri && !kSplit) {
+      TileOrigin(w, tiles_m, tiles_n, &m0, &n0);
+      if (SkipTile(p, m0, n0)) continue;
+    } else {
+      if (!WorkRange<kTri, kSplit>(p, w, tiles_m, tiles_n, kt_total, &m0, &n0, &kt_lo,
+                                   &kt_hi))
+        continue;
+      if (kSplit && kt_lo >= kt_hi) continue;
+    }
     // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
     // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
     const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
@@ -296,7 +328,8 @@ __global__ void __maxnreg__(168)
           if (inside) in_part |= 1u << bit;
           if (inside && p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j))
             crossing |= 1u << bit;
-          cacc[mb][nb][e] = (inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
+          cacc[mb][nb][e] =
+              (!kSplit && inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
         }
     // kTri: k ranges of the 16-row blocks [xb, xe) (op(A) triangular), and the
     // union [ub, ue) and intersection [ib, ie) of the ranges of the 8-column
@@ -372,7 +405,7 @@ __global__ void __maxnreg__(168)
     };
     // Chunk 0 lies before the tile's first k-slice: its k range is empty for
     // every element, and the reference still applies beta (with alpha * 0).
-    if (kTri && !(kt_lo < kt_hi && kt_lo < kKtPerChunk)) merge(0);
+    if (kTri && !kSplit && !(kt_lo < kt_hi && kt_lo < kKtPerChunk)) merge(0);
 
     for (int kt = kt_lo; kt < kt_hi; ++kt, ++gs) {
       const int s = gs % kStages, round = gs / kStages;
@@ -453,10 +486,13 @@ __global__ void __maxnreg__(168)
       if (lane == 0) MbarArrive(&empty[s]);
 
       // End of a reference KC chunk: merge into the running C value.
-      if ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_hi) merge(kt / kKtPerChunk);
+      if (!kSplit && ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_hi))
+        merge(kt / kKtPerChunk);
     }
 
-    // Epilogue: write C.
+    // Epilogue: write C, or the chunk's raw accumulators.
+    const long long pbase =
+        kSplit ? static_cast<long long>(w % p.nchunks) * p.n * static_cast<long long>(p.m) : 0;
 #pragma unroll
     for (int mb = 0; mb < 2; ++mb)
 #pragma unroll
@@ -467,8 +503,52 @@ __global__ void __maxnreg__(168)
           if (!((in_part >> bit) & 1u)) continue;
           const int i = row0 + mb * 16 + (e >> 1);
           const int j = col0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
-          p.c[i + j * p.ldc] = cacc[mb][nb][e];
+          if constexpr (kSplit) {
+            p.partial[pbase + static_cast<long long>(j) * p.m + i] = acc[mb][nb][e];
+          } else {
+            p.c[i + j * p.ldc] = cacc[mb][nb][e];
+          }
         }
+  }
+}
+
+// The merge after a split launch: for each element of C's part, the chunks
+// in order, exactly as the tile kernel merges them (a chunk outside a
+// triangular operand's range for the element is skipped; chunk 0 still
+// applies beta, with a zero accumulator when its range is empty).
+__global__ void __launch_bounds__(256) DgemmSplitMergeKernel(GemmParams p) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  const long long total = static_cast<long long>(p.m) * p.n;
+  const long long plane = total;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % p.m), j = static_cast<int>(e / p.m);
+    if (!InPart(p, i, j)) continue;
+    const bool crossing = p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j);
+    int kb = 0, ke = p.k;
+    if (p.tri != kTriNone) TriRange(p, i, j, &kb, &ke);
+    double cv = 0.0;
+    for (int c = 0; c < p.nchunks; ++c) {
+      const bool nonempty = max(c * 256, kb) < min(min(p.k, c * 256 + 256), ke);
+      if (!nonempty && c != 0) continue;
+      const double acc = nonempty ? p.partial[c * plane + e] : 0.0;
+      const double r = p.alpha * acc;
+      if (c != 0 || p.beta == 1.0) {
+        if (c == 0) cv = p.c[i + j * p.ldc];
+        cv = r + cv;
+      } else if (p.beta == 0.0) {
+        cv = r;
+      } else {
+        const double cin = p.c[i + j * p.ldc];
+        if (crossing) {
+          const double bc = p.beta * cin;
+          cv = r + bc;
+        } else {
+          cv = fma(cin, p.beta, r);
+        }
+      }
+    }
+    p.c[i + j * p.ldc] = cv;
   }
 }
 
@@ -732,17 +812,51 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   p.ldc = ldc;
   p.part = part;
   p.tri = tri;
+  p.partial = nullptr;
+  p.nchunks = 1;
   p.timeout_flag = ctx.dev_status;
   p.guard = ctx.guard;
   const long long tiles =
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(DgemmDmmaKernel<false>,
+    cudaFuncSetAttribute(DgemmDmmaKernel<false, false>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaFuncSetAttribute(DgemmDmmaKernel<true>,
+    cudaFuncSetAttribute(DgemmDmmaKernel<true, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    cudaFuncSetAttribute(DgemmDmmaKernel<false, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    cudaFuncSetAttribute(DgemmDmmaKernel<true, true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     configured = true;
+  }
+  // Few tiles and a long k (a narrow product: TRTRI's and GETRI's block
+  // columns): each tile's KC chunks become separate work items, so that the
+  // chunks of one tile run on different SMs, and a second kernel merges them
+  // in order. Every chain and merge is the unsplit kernel's.
+  const int nchunks = (k + 255) / 256;
+  const size_t pbytes = sizeof(double) * static_cast<size_t>(nchunks) * m * n;
+  if (nchunks >= 2 && tiles * 2 <= ctx.num_sms && pbytes <= (size_t(1) << 31)) {
+    double* partial = static_cast<double*>(Workspace(kWsSplitK, pbytes));
+    if (partial != nullptr) {
+      p.partial = partial;
+      p.nchunks = nchunks;
+      const unsigned grid =
+          static_cast<unsigned>(std::min<long long>(tiles * nchunks, ctx.num_sms));
+      cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
+      if (tri == kTriNone) {
+        DgemmDmmaKernel<false, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+      } else {
+        DgemmDmmaKernel<true, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+      }
+      KernelTimerStop(t0, ctx.stream);
+      const long long total = static_cast<long long>(m) * n;
+      const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 16));
+      DgemmSplitMergeKernel<<<blocks, 256, 0, ctx.stream>>>(p);
+      CountLaunch(2);
+      LaunchFailed("dgemm split");
+      return;
+    }
   }
   // Persistent grid: one CTA per SM (the accumulators and the prefetched C
   // take 128 of each thread's registers). Measured against a variant whose
@@ -752,9 +866,9 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
   cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
   if (tri == kTriNone) {
-    DgemmDmmaKernel<false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+    DgemmDmmaKernel<false, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   } else {
-    DgemmDmmaKernel<true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+    DgemmDmmaKernel<true, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   }
   KernelTimerStop(t0, ctx.stream);
   CountLaunch();

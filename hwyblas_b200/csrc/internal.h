@@ -94,7 +94,8 @@ enum WorkspaceSlot : int {
   kWsRefineInt = 26,
   kWsGerfsWork = 27,   // host-pointer staging of GERFS's WORK and IWORK
   kWsGerfsIwork = 28,
-  kNumWorkspaceSlots = 29
+  kWsSplitK = 29,      // per-chunk accumulators of a split DMMA GEMM
+  kNumWorkspaceSlots = 30
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
