@@ -19,6 +19,8 @@ plain  : the plain FP64 tensor-pipe DGEMM (bit-identical to the reference)
          on the same inputs, and its error.
 batched: 10,000 problems, n log-uniform in [8, 512], dgetrf + dgetrs + dgemm
          each, batched persistent launches against a per-problem loop.
+widened: throughput of the routines beyond the hot path (dtrmm, dsymm,
+         dsyr2k, dgemmtr, dtrtri, dgetri at n = 8192; zgemm, cgemm at 4096).
 dgesv  : n = 16384, A = H1 diag(s) H2 (H1, H2 products of 4 Householder
          reflectors, s geometric from 1 to 1/cond): the plain FP64 dgesv
          (bit-identical to the reference's LU) against the mixed-precision
@@ -65,14 +67,19 @@ def parse():
     p.add_argument("--no-dgesv", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-widened", action="store_true",
+                   help="skip the throughput of the routines beyond the hot path")
     p.add_argument("--nrhs", type=int, default=1, help="right-hand sides of --case gesv-mixed")
     p.add_argument("--kernels", action="store_true",
                    help="with --case: per-kernel device time of the call (CUPTI activity "
                         "records through torch.profiler)")
-    p.add_argument("--case", default=None, choices=["leaf", "getrf", "gesv", "gesv-mixed"],
+    p.add_argument("--case", default=None,
+                   choices=["leaf", "getrf", "gesv", "gesv-mixed", "trtri", "getri", "trmm",
+                            "zgemm"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
-                        "gesv-n, each after one warm-up call")
+                        "gesv-n; dtrtri, dgetri, dtrmm or zgemm at n; each after one "
+                        "warm-up call")
     return p.parse_args()
 
 
@@ -586,6 +593,65 @@ def run_batched(args, torch, hb, count=10000, loop_sample=300):
     return out
 
 
+def run_widened(torch, hb, stream):
+    """Throughput of the routines beyond the hot path (bit-identical to the
+    oracle in the tests), device-resident inputs, CUDA events on the
+    library's stream, best of 3 calls after one warm-up."""
+    g = torch.Generator(device="cuda").manual_seed(3)
+
+    def colmajor(rows, cols, dtype=torch.float64):
+        return (torch.rand(cols, rows, dtype=dtype, device="cuda", generator=g) * 2 - 1).T
+
+    def best(fn, reps=3):
+        fn()
+        return min(timed(torch, stream, fn, 1) for _ in range(reps))
+
+    out = {}
+    n = 8192
+    a, b, c = colmajor(n, n), colmajor(n, n), colmajor(n, n)
+    rows = [("dtrmm LLNN", lambda: hb.trmm("d", "L", "L", "N", "N", n, n, 1.0, a, n, c, n),
+             n ** 3),
+            ("dtrmm RUNN", lambda: hb.trmm("d", "R", "U", "N", "N", n, n, 1.0, a, n, c, n),
+             n ** 3),
+            ("dsymm LU", lambda: hb.symm("d", "L", "U", n, n, 1.0, a, n, b, n, 0.5, c, n),
+             2 * n ** 3),
+            ("dsyr2k LN", lambda: hb.syr2k("d", "L", "N", n, n, 1.0, a, n, b, n, 0.5, c, n),
+             2 * n ** 3),
+            ("dgemmtr LNN", lambda: hb.gemmtr("d", "L", "N", "N", n, n, 1.0, a, n, b, n, 0.5,
+                                              c, n), n ** 3)]
+    for name, fn, flops in rows:
+        ms = best(fn)
+        out[name] = {"n": n, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+    # Inverse: LU of a diagonally dominant matrix, then TRTRI of its U and
+    # GETRI (each call on a fresh copy; the copy is outside the timed call).
+    m = colmajor(n, n)
+    m.diagonal().add_(2.0 * n ** 0.5)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    lu = m.clone().T.contiguous().T
+    hb.dgetrf(n, n, lu, n, ipiv)
+    work = torch.zeros(64 * n, dtype=torch.float64, device="cuda")
+    for name, call, flops in (("dtrtri UN", lambda x: hb.trtri("d", "U", "N", n, x, n),
+                               n ** 3 / 3),
+                              ("dgetri", lambda x: hb.getri("d", n, x, n, ipiv, work, 64 * n),
+                               4 * n ** 3 / 3)):
+        times = []
+        for _ in range(3):
+            x = lu.clone().T.contiguous().T
+            torch.cuda.synchronize()
+            times.append(timed(torch, stream, lambda: call(x), 1))
+        ms = min(times[1:])
+        out[name] = {"n": n, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+    del a, b, c, m, lu, work
+    nz = 4096
+    for p, dt in (("z", torch.complex128), ("c", torch.complex64)):
+        za, zb, zc = colmajor(nz, nz, dt), colmajor(nz, nz, dt), colmajor(nz, nz, dt)
+        ms = best(lambda: hb.zgemm(p, "N", "N", nz, nz, nz, 1.0, za, nz, zb, nz, 0.0, zc, nz))
+        out[p + "gemm NN"] = {"n": nz, "ms": ms, "tflops": 8 * nz ** 3 / (ms * 1e-3) / 1e12}
+    out["note"] = ("useful flops: trmm n^3, symm/syr2k 2n^3, gemmtr n^3, trtri n^3/3, "
+                   "getri 4n^3/3, complex gemm 8n^3")
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -630,6 +696,12 @@ def run_ours(args):
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = run_batched(args, torch, hb)
+    widened = None
+    if rank == 0 and world == 1 and not args.no_widened:
+        try:
+            widened = run_widened(torch, hb, stream)
+        except Exception as exc:  # a side measurement never costs the bench line
+            widened = {"error": repr(exc)[:200]}
 
     if rank == 0:
         line = {
@@ -674,6 +746,8 @@ def run_ours(args):
             line["solvers"] = solvers
         if batched is not None:
             line["batched"] = batched
+        if widened is not None:
+            line["widened"] = widened
         print(json.dumps(line), flush=True)
     dist.close()
     return 0
@@ -687,7 +761,26 @@ def run_case(args):
     n = args.gesv_n
     g = torch.Generator(device="cuda").manual_seed(1)
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
-    if args.case == "leaf":
+    if args.case in ("trtri", "getri", "trmm", "zgemm"):
+        n = args.n
+        ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+        dt = torch.complex128 if args.case == "zgemm" else torch.float64
+        a0 = torch.rand(n * n, dtype=dt, device="cuda", generator=g) * 2 - 1
+        if args.case in ("trtri", "getri"):
+            a0.view(n, n).diagonal().add_(2.0 * n ** 0.5)
+            hb.dgetrf(n, n, a0, n, ipiv)
+        other = torch.rand(n * n, dtype=dt, device="cuda", generator=g) * 2 - 1
+        work = torch.zeros(64 * n, dtype=torch.float64, device="cuda")
+        if args.case == "trtri":
+            call = lambda a: hb.trtri("d", "U", "N", n, a, n)
+        elif args.case == "getri":
+            call = lambda a: hb.getri("d", n, a, n, ipiv, work, 64 * n)
+        elif args.case == "trmm":
+            call = lambda a: hb.trmm("d", "L", "L", "N", "N", n, n, 1.0, other, n, a, n)
+        else:
+            c = torch.zeros_like(a0)
+            call = lambda a: hb.zgemm("z", "N", "N", n, n, n, 1.0, a, n, other, n, 0.0, c, n)
+    elif args.case == "leaf":
         a0 = torch.rand(n * 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         call = lambda a: hb.dgetrf2(n, 16, a, n, ipiv)
     else:
