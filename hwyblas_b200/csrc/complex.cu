@@ -17,9 +17,9 @@
 //
 // The chains are independent per element, so a SIMT kernel computes them
 // directly: 64 x 64 complex tiles per 256-thread CTA, 4 x 4 elements per
-// thread, k in shared-memory slices of 16 (real and imaginary planes apart,
-// so every load is conflict free).
+// thread, k in double-buffered shared-memory slices of 16.
 #include <algorithm>
+#include <cstdint>
 
 #include "device.cuh"
 #include "internal.h"
@@ -69,15 +69,46 @@ struct ZParams {
   const int* guard;
 };
 
-// One CTA: a 64 x 64 complex tile, 4 x 4 elements per thread (rows
-// tx + 16 r, columns ty + 16 q). A chunk ends on a slice boundary (256 is a
-// multiple of 16), where the thread merges its chunk into C in memory: the
-// running value stays in C itself, so no registers hold it.
 template <typename R>
-__global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+// Asynchronous copy of one complex element (src_bytes 0: zero fill).
+template <typename R>
+__device__ __forceinline__ void CpAsyncElem(void* smem_dst, const R* src, bool valid) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  if constexpr (sizeof(R) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+  }
+}
+
+// One CTA: a 64 x 64 complex tile, 4 x 4 elements per thread (rows
+// tx + 16 r, columns ty + 16 q). The k-slices of 16 stream through two
+// shared-memory buffers with cp.async (complex elements stay interleaved, so
+// one shared load gives both parts; conjugation is applied after the load),
+// the next slice in flight while this one is multiplied. A chunk ends on a
+// slice boundary (256 is a multiple of 16), where the thread merges its
+// chunk into C in memory: the running value stays in C itself.
+template <typename R>
+__global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
   if (p.guard != nullptr && *p.guard != 0) return;
-  __shared__ R sa_re[kZK][kZM + 1], sa_im[kZK][kZM + 1];
-  __shared__ R sb_re[kZK][kZN + 1], sb_im[kZK][kZN + 1];
+  using V = typename Vec2<R>::type;
+  extern __shared__ __align__(16) unsigned char zsmem[];
+  V* sa = reinterpret_cast<V*>(zsmem);                 // [2][kZK][kZM]
+  V* sb = sa + 2 * kZK * kZM;                          // [2][kZK][kZN]
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   R rr[4][4], ir[4][4], ri[4][4], ii[4][4];
@@ -87,40 +118,54 @@ __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
     for (int q = 0; q < 4; ++q) rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
   const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
   const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
-  for (int k0 = 0; k0 < p.k; k0 += kZK) {
+  // Consecutive threads copy consecutive addresses: along rows of op(A) when
+  // A is not transposed, else along k; along k of op(B) when B is not
+  // transposed, else along its columns.
+  const bool a_rows = p.a.rs == 1, b_k = p.b.rs == 1;
+  const auto issue = [&](int k0, int buf) {
+    V* da = sa + buf * kZK * kZM;
+    V* db = sb + buf * kZK * kZN;
     for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
-      const int kk = idx / kZM, mm = idx % kZM;
+      const int kk = a_rows ? idx / kZM : idx % kZK, mm = a_rows ? idx % kZM : idx / kZK;
       const int gi = m0 + mm, gk = k0 + kk;
-      R vr = R(0), vi = R(0);
-      if (gi < p.m && gk < p.k) {
-        const R* e = p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs);
-        vr = e[0];
-        vi = p.a.conj ? -e[1] : e[1];
-      }
-      sa_re[kk][mm] = vr;
-      sa_im[kk][mm] = vi;
+      const bool ok = gi < p.m && gk < p.k;
+      const R* src = ok ? p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs) : p.a.data;
+      CpAsyncElem<R>(da + kk * kZM + mm, src, ok);
     }
     for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
-      const int kk = idx / kZN, nn = idx % kZN;
+      const int kk = b_k ? idx % kZK : idx / kZN, nn = b_k ? idx / kZK : idx % kZN;
       const int gj = n0 + nn, gk = k0 + kk;
-      R vr = R(0), vi = R(0);
-      if (gj < p.n && gk < p.k) {
-        const R* e = p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs);
-        vr = e[0];
-        vi = p.b.conj ? -e[1] : e[1];
-      }
-      sb_re[kk][nn] = vr;
-      sb_im[kk][nn] = vi;
+      const bool ok = gj < p.n && gk < p.k;
+      const R* src = ok ? p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs) : p.b.data;
+      CpAsyncElem<R>(db + kk * kZN + nn, src, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const R sa_sign = p.a.conj ? R(-1) : R(1), sb_sign = p.b.conj ? R(-1) : R(1);
+  issue(0, 0);
+  int buf = 0;
+  for (int k0 = 0; k0 < p.k; k0 += kZK, buf ^= 1) {
+    if (k0 + kZK < p.k) {
+      issue(k0 + kZK, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
-    const auto step = [&](int kk) {
+    const V* ca = sa + buf * kZK * kZM;
+    const V* cb = sb + buf * kZK * kZN;
+    const int kend = min(kZK, p.k - k0);
+#pragma unroll 2
+    for (int kk = 0; kk < kend; ++kk) {
       R ar[4], ai[4], br[4], bi[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        ar[r] = sa_re[kk][tx + 16 * r];
-        ai[r] = sa_im[kk][tx + 16 * r];
-        br[r] = sb_re[kk][ty + 16 * r];
-        bi[r] = sb_im[kk][ty + 16 * r];
+        const V va = ca[kk * kZM + tx + 16 * r];
+        const V vb = cb[kk * kZN + ty + 16 * r];
+        ar[r] = va.x;
+        ai[r] = Mul(va.y, sa_sign);
+        br[r] = vb.x;
+        bi[r] = Mul(vb.y, sb_sign);
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r)
@@ -131,10 +176,7 @@ __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
           ri[r][q] = Fma(ar[r], bi[q], ri[r][q]);
           ii[r][q] = Fma(ai[r], bi[q], ii[r][q]);
         }
-    };
-    const int kend = min(kZK, p.k - k0);
-#pragma unroll 2
-    for (int kk = 0; kk < kend; ++kk) step(kk);
+    }
     __syncthreads();
     if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= p.k) {
       const bool first = k0 < kZChunk;
@@ -166,6 +208,11 @@ __global__ void __launch_bounds__(256) ZgemmKernel(ZParams<R> p) {
         }
     }
   }
+}
+
+template <typename R>
+constexpr int ZSmemBytes() {
+  return 2 * (kZK * kZM + kZK * kZN) * 2 * static_cast<int>(sizeof(R));
 }
 
 // C := beta * C (beta 0: zeros, C not read), each element as the complex
@@ -212,6 +259,27 @@ void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, 
     LaunchFailed("complex scale");
     return;
   }
+  // cp.async copies whole complex elements, which must be aligned to their
+  // size; an operand that is not is copied to an aligned buffer first.
+  const auto aligned = [](const R* x, int rows, int cols, int ld, int slot, int* ld_out) {
+    *ld_out = ld;
+    if (reinterpret_cast<uintptr_t>(x) % (2 * sizeof(R)) == 0) return x;
+    R* dst = static_cast<R*>(Workspace(slot, 2 * sizeof(R) * static_cast<size_t>(rows) * cols));
+    if (dst == nullptr) return static_cast<const R*>(nullptr);
+    if (Failed(cudaMemcpy2DAsync(dst, 2 * sizeof(R) * rows, x, 2 * sizeof(R) * ld,
+                                 2 * sizeof(R) * rows, cols, cudaMemcpyDeviceToDevice,
+                                 Ctx().stream),
+               "complex operand copy"))
+      return static_cast<const R*>(nullptr);
+    *ld_out = rows;
+    return static_cast<const R*>(dst);
+  };
+  int lda2, ldb2;
+  a = aligned(a, ta == 0 ? m : k, ta == 0 ? k : m, lda, kWsPackA, &lda2);
+  b = aligned(b, tb == 0 ? k : n, tb == 0 ? n : k, ldb, kWsPackB, &ldb2);
+  if (a == nullptr || b == nullptr) return;
+  lda = lda2;
+  ldb = ldb2;
   ZParams<R> p;
   p.m = m;
   p.n = n;
@@ -227,7 +295,13 @@ void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, 
   p.ldc = ldc;
   p.guard = Ctx().guard;
   const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
-  ZgemmKernel<R><<<grid, 256, 0, Ctx().stream>>>(p);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(ZgemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         ZSmemBytes<R>());
+    configured = true;
+  }
+  ZgemmKernel<R><<<grid, 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
   CountLaunch();
   LaunchFailed("complex gemm");
 }

@@ -100,3 +100,22 @@ def test_cblas_zgemm_row_major_and_errors(hb, orc):
                  z.astype(np.complex64), 2, 0.0, z.astype(np.complex64), 2)
     assert cap.errors == [("cblas_zgemm", 4), ("cblas_cgemm", 1), ("ZGEMM", 1),
                           ("CGEMM", 8)]
+
+
+def test_zgemm_misaligned_device_operand(hb, orc):
+    """A device operand whose complex elements start 8 bytes off a 16-byte
+    boundary is copied to an aligned buffer before the asynchronous copies."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(9)
+    m, n, k = 70, 50, 300
+    a, b, c = (crand(rng, m, k, np.complex128), crand(rng, k, n, np.complex128),
+               crand(rng, m, n, np.complex128))
+    flat = np.zeros(2 * m * k + 1)
+    flat[1:] = a.ravel(order="F").view(np.float64)
+    ta = torch.from_numpy(flat).cuda()
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).T.cuda()  # noqa: E731
+    tc = dev(c)
+    hb.zgemm("z", "N", "N", m, n, k, 1.25 - 0.5j, ta.data_ptr() + 8, m, dev(b), k, 0.5, tc, m)
+    c2 = c.copy(order="F")
+    assert orc.zgemm("N", "N", m, n, k, 1.25 - 0.5j, a, m, b, k, 0.5, c2, m) == 0
+    assert same_bits(creal(tc.cpu().numpy()), creal(c2))
