@@ -244,10 +244,12 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
 // chains over the in-range k only, in the MMA's own ascending order. A chunk
 // whose range is empty for an element leaves it unmerged, as the reference
 // skips that micro-tile (src/gemm-inl.h:202-209).
-template <bool kTri, bool kSplit>
+template <int kTriKind, bool kSplit>
 __global__ void __maxnreg__(168)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
                     const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
+  // kTriKind: 0 no triangular operand, 1 op(A) triangular, 2 op(B).
+  constexpr bool kTri = kTriKind != 0, kTriA = kTriKind == 1, kTriB = kTriKind == 2;
   if (p.guard != nullptr && *p.guard != 0) return;
   // Persistent: CTA b computes tiles b, b + gridDim.x, ... The producer
   // streams the k-slices across tile boundaries (the stage counter gs runs
@@ -345,16 +347,17 @@ __global__ void __maxnreg__(168)
       for (int mb = 0; mb < 2; ++mb) {
         if (fr + mb * 16 >= p.m) {
           xb[mb] = xe[mb] = 0;
-        } else if (p.tri == kTriALower || p.tri == kTriAUpper) {
+        } else if (kTriA) {
           TriRange(p, fr + mb * 16, 0, &xb[mb], &xe[mb]);
         }
       }
 #pragma unroll
       for (int nb = 0; nb < 4; ++nb) {
+        if constexpr (!kTriB) break;
         const int j0 = col0 + nb * 8, j1 = min(j0 + 7, p.n - 1);
         if (j0 >= p.n) {
           ub[nb] = ue[nb] = ib[nb] = ie[nb] = 0;
-        } else if (p.tri == kTriBLower || p.tri == kTriBUpper) {
+        } else {
           int b0, e0, b1, e1;
           TriRange(p, 0, j0, &b0, &e0);
           TriRange(p, 0, j1, &b1, &e1);
@@ -378,7 +381,10 @@ __global__ void __maxnreg__(168)
           for (int e = 0; e < 4; ++e) {
             const int bit = (mb * 4 + nb) * 4 + e;
             bool skip = false;
-            if constexpr (kTri) {
+            if constexpr (kTriA) {
+              // The range is the 16-row block's.
+              if (!first) skip = max(xb[mb], c_lo) >= min(xe[mb], c_hi);
+            } else if constexpr (kTriB) {
               if (!first) {
                 int kb, ke;
                 TriRange(p, row0 + mb * 16 + (e >> 1),
@@ -441,6 +447,11 @@ __global__ void __maxnreg__(168)
           if constexpr (!kTri) {
             Dmma(acc[0][nb], af[0], b0, b1);
             Dmma(acc[1][nb], af[1], b0, b1);
+          } else if constexpr (kTriA) {
+            if (kg >= p.k) continue;
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb)
+              if (kg >= xb[mb] && kg < xe[mb]) Dmma(acc[mb][nb], af[mb], b0, b1);
           } else {
             if (kg >= p.k || kend <= ub[nb] || kg >= ue[nb]) continue;
             if (kg >= ib[nb] && kend <= ie[nb]) {
@@ -820,16 +831,19 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(DgemmDmmaKernel<false, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaFuncSetAttribute(DgemmDmmaKernel<true, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaFuncSetAttribute(DgemmDmmaKernel<false, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    cudaFuncSetAttribute(DgemmDmmaKernel<true, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    const auto set = [](const void* f) {
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    };
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<0, false>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<1, false>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<2, false>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<0, true>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<1, true>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<2, true>));
     configured = true;
   }
+  const int tri_kind =
+      tri == kTriNone ? 0 : (tri == kTriALower || tri == kTriAUpper) ? 1 : 2;
   // Few tiles and a long k (a narrow product: TRTRI's and GETRI's block
   // columns): each tile's KC chunks become separate work items, so that the
   // chunks of one tile run on different SMs, and a second kernel merges them
@@ -844,10 +858,12 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       const unsigned grid =
           static_cast<unsigned>(std::min<long long>(tiles * nchunks, ctx.num_sms));
       cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
-      if (tri == kTriNone) {
-        DgemmDmmaKernel<false, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+      if (tri_kind == 0) {
+        DgemmDmmaKernel<0, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+      } else if (tri_kind == 1) {
+        DgemmDmmaKernel<1, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
       } else {
-        DgemmDmmaKernel<true, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+        DgemmDmmaKernel<2, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
       }
       KernelTimerStop(t0, ctx.stream);
       const long long total = static_cast<long long>(m) * n;
@@ -865,10 +881,12 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const unsigned grid =
       static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
   cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
-  if (tri == kTriNone) {
-    DgemmDmmaKernel<false, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  if (tri_kind == 0) {
+    DgemmDmmaKernel<0, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+  } else if (tri_kind == 1) {
+    DgemmDmmaKernel<1, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   } else {
-    DgemmDmmaKernel<true, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
+    DgemmDmmaKernel<2, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   }
   KernelTimerStop(t0, ctx.stream);
   CountLaunch();
