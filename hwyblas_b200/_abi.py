@@ -21,6 +21,7 @@ PROTOTYPES = {
     "strsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]),
     "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     **{f"{p}gemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "zc"},
+    **{f"{p}trsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]) for p in "zc"},
     **{f"{p}symm_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}syr2k_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])
@@ -85,6 +86,7 @@ PROTOTYPES = {
     "cblas_strsm": (None, [I, I, I, I, I, I, I, F, P, I, P, I]),
     "cblas_idamax": (ctypes.c_size_t, [I, P, I]),
     **{f"cblas_{p}gemm": (None, [I, I, I, I, I, I, P, P, I, P, I, P, P, I]) for p in "zc"},
+    **{f"cblas_{p}trsm": (None, [I, I, I, I, I, I, I, P, P, I, P, I]) for p in "zc"},
     **{f"cblas_{p}trmm": (None, [I, I, I, I, I, I, I, S, P, I, P, I])
        for p, S in (("d", D), ("s", F))},
     **{f"cblas_{p}symm": (None, [I, I, I, I, I, S, P, I, P, I, S, P, I])

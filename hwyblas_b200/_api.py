@@ -163,6 +163,16 @@ def zgemm(p, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
                                 _i(ldc))
 
 
+def ztrsm(p, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
+    """Complex triangular solve in place; p is "z" or "c" (reference
+    ztrsm_/ctrsm_, src/trsm.cc:202-215)."""
+    import numpy as np
+    rt = np.float64 if p == "z" else np.float32
+    al = np.array([complex(alpha).real, complex(alpha).imag], rt)
+    getattr(lib(), f"{p}trsm_")(_c(side), _c(uplo), _c(transa), _c(diag), _i(m), _i(n),
+                                al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb))
+
+
 def cblas_level3(name, *args):
     """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
     scalars, array arguments given as numpy arrays or device pointers."""

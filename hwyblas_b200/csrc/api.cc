@@ -556,6 +556,70 @@ static void ZgemmEntry(const char* name, const char* transa, const char* transb,
   hb::Finish(name);
 }
 
+// Complex TRSM (src/trsm.cc:137-180): R is the real type, arrays interleaved.
+template <typename R>
+static void ZtrsmEntry(const char* name, const char* side, const char* uplo,
+                       const char* transa, const char* diag, const hwyblas_int* m_p,
+                       const hwyblas_int* n_p, const R* alpha, const R* a,
+                       const hwyblas_int* lda_p, R* b, const hwyblas_int* ldb_p) {
+  const int m = *m_p, n = *n_p, lda = *lda_p, ldb = *ldb_p;
+  const char s = hb::Up(*side), u = hb::Up(*uplo), d = hb::Up(*diag);
+  const int op = DecodeOp3(*transa);
+  const bool left = (s == 'L');
+  const int ka = left ? m : n;
+  int info = 0;
+  if (s != 'L' && s != 'R') info = 1;
+  else if (u != 'L' && u != 'U') info = 2;
+  else if (op < 0) info = 3;
+  else if (d != 'U' && d != 'N') info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, ka)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  if (m == 0 || n == 0) return;
+  const bool alpha_zero = alpha[0] == R(0) && alpha[1] == R(0);
+  hb::Staged<R> sa, sb;
+  if (!alpha_zero && !sa.In(a, 2 * lda, 2 * ka, ka, hb::kWsStageA, true)) return;
+  if (!sb.In(b, 2 * ldb, 2 * m, n, hb::kWsStageB, !alpha_zero)) return;
+  hb::ZtrsmFull<R>(left, u == 'L', op, d == 'U', m, n, alpha, sa.dev, std::max(sa.ld / 2, 1),
+                   sb.dev, sb.ld / 2);
+  sb.Out();
+  hb::Finish(name);
+}
+
+// CBLAS complex TRSM (src/cblas.cc:666-700): row-major as the other side and
+// triangle, m and n swapped; alpha by address.
+template <typename R>
+static void CblasZtrsm(const char* name, const char* routine, CBLAS_LAYOUT layout,
+                       CBLAS_SIDE side, CBLAS_UPLO uplo, CBLAS_TRANSPOSE transa,
+                       CBLAS_DIAG diag, hwyblas_int m_in, hwyblas_int n_in, const void* alpha,
+                       const void* a, hwyblas_int lda, void* b, hwyblas_int ldb) {
+  if (!hb::ValidLayout(name, layout)) return;
+  char sc = hb::SideChar(side), uc = hb::UploChar(uplo);
+  const char tc = hb::TransChar(transa), dc = hb::DiagChar(diag);
+  int m = m_in, n = n_in;
+  const bool row = (layout == CblasRowMajor);
+  if (row) {
+    sc = hb::FlipSide(sc);
+    uc = hb::FlipUplo(uc);
+    std::swap(m, n);
+  }
+  const R* al = static_cast<const R*>(alpha);
+  if (row) {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 7, 6, 8, 9, 10, 11, 12});
+    ZtrsmEntry<R>(routine, &sc, &uc, &tc, &dc, &m, &n, al, static_cast<const R*>(a), &lda,
+                  static_cast<R*>(b), &ldb);
+  } else {
+    hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12});
+    ZtrsmEntry<R>(routine, &sc, &uc, &tc, &dc, &m, &n, al, static_cast<const R*>(a), &lda,
+                  static_cast<R*>(b), &ldb);
+  }
+}
+
 // CBLAS complex GEMM (src/cblas.cc:520-537): row-major as the column-major
 // product of the swapped operands; alpha and beta by address.
 template <typename R>
@@ -756,6 +820,34 @@ HWYBLAS_API void cgemm_(const char* transa, const char* transb, const hwyblas_in
                         const hwyblas_int* ldb, const float* beta, float* c,
                         const hwyblas_int* ldc) {
   ZgemmEntry<float>("CGEMM", transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+HWYBLAS_API void ztrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const double* alpha, const double* a, const hwyblas_int* lda,
+                        double* b, const hwyblas_int* ldb) {
+  ZtrsmEntry<double>("ZTRSM", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb);
+}
+HWYBLAS_API void ctrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const float* alpha, const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb) {
+  ZtrsmEntry<float>("CTRSM", side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb);
+}
+HWYBLAS_API void cblas_ztrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const void* alpha, const void* a, const hwyblas_int lda, void* b,
+                             const hwyblas_int ldb) {
+  CblasZtrsm<double>("cblas_ztrsm", "ZTRSM", layout, side, uplo, transa, diag, m, n, alpha, a,
+                     lda, b, ldb);
+}
+HWYBLAS_API void cblas_ctrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const void* alpha, const void* a, const hwyblas_int lda, void* b,
+                             const hwyblas_int ldb) {
+  CblasZtrsm<float>("cblas_ctrsm", "CTRSM", layout, side, uplo, transa, diag, m, n, alpha, a,
+                    lda, b, ldb);
 }
 HWYBLAS_API void cblas_zgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
                              const CBLAS_TRANSPOSE transb, const hwyblas_int m,

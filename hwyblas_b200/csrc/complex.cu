@@ -19,6 +19,7 @@
 // directly: 64 x 64 complex tiles per 256-thread CTA, 4 x 4 elements per
 // thread, k in double-buffered shared-memory slices of 16.
 #include <algorithm>
+#include <cfloat>
 #include <cstdint>
 
 #include "device.cuh"
@@ -238,7 +239,316 @@ __global__ void ZScaleKernel(int m, int n, R beta_re, R beta_im, R* c, long long
   }
 }
 
+// 1 / (c + i d) as the C++ runtime's complex quotient: for double, Smith's
+// method with its scalings for very large and very small magnitudes and its
+// alternative when the ratio is subnormal; for float, the textbook quotient
+// (a c + b d, b c - a d) / (c^2 + d^2) in double precision, rounded. (Checked
+// against the host compiler's complex division on random quotients spanning
+// 2^-60..2^60, zero parts included; non-finite inputs are not reproduced.)
+template <typename R>
+__device__ __forceinline__ void ZRecip(R cr, R ci, R* xr, R* xi) {
+  if constexpr (sizeof(R) == 8) {
+    double a = 1.0, b = 0.0, c = cr, d = ci;
+    const double kBig = DBL_MAX / 2, kMin = DBL_MIN, kEps = DBL_EPSILON;
+    const double kScale = 1.0 / kEps, kMax2 = kBig * kEps;
+    double x, y;
+    if (fabs(c) < fabs(d)) {
+      if (fabs(d) >= kBig) {
+        a = a / 2; b = b / 2; c = c / 2; d = d / 2;
+      }
+      if (fabs(d) < kEps) {
+        a = a * kScale; b = b * kScale; c = c * kScale; d = d * kScale;
+      } else if ((fabs(a) < kMin && fabs(b) < kMax2 && fabs(d) < kMax2) ||
+                 (fabs(b) < kMin && fabs(a) < kMax2 && fabs(d) < kMax2)) {
+        a = a * kScale; b = b * kScale; c = c * kScale; d = d * kScale;
+      }
+      const double ratio = c / d;
+      const double denom = __dadd_rn(__dmul_rn(c, ratio), d);
+      if (fabs(ratio) > kMin) {
+        x = __dadd_rn(__dmul_rn(a, ratio), b) / denom;
+        y = __dsub_rn(__dmul_rn(b, ratio), a) / denom;
+      } else {
+        x = __dadd_rn(__dmul_rn(c, a / d), b) / denom;
+        y = __dsub_rn(__dmul_rn(c, b / d), a) / denom;
+      }
+    } else {
+      if (fabs(c) >= kBig) {
+        a = a / 2; b = b / 2; c = c / 2; d = d / 2;
+      }
+      if (fabs(c) < kEps) {
+        a = a * kScale; b = b * kScale; c = c * kScale; d = d * kScale;
+      } else if ((fabs(a) < kMin && fabs(b) < kMax2 && fabs(c) < kMax2) ||
+                 (fabs(b) < kMin && fabs(a) < kMax2 && fabs(c) < kMax2)) {
+        a = a * kScale; b = b * kScale; c = c * kScale; d = d * kScale;
+      }
+      const double ratio = d / c;
+      const double denom = __dadd_rn(__dmul_rn(d, ratio), c);
+      if (fabs(ratio) > kMin) {
+        x = __dadd_rn(__dmul_rn(b, ratio), a) / denom;
+        y = __dsub_rn(b, __dmul_rn(a, ratio)) / denom;
+      } else {
+        x = __dadd_rn(a, __dmul_rn(d, b / c)) / denom;
+        y = __dsub_rn(b, __dmul_rn(d, a / c)) / denom;
+      }
+    }
+    *xr = x;
+    *xi = y;
+  } else {
+    const double c = cr, d = ci;
+    const double den = __dadd_rn(__dmul_rn(c, c), __dmul_rn(d, d));
+    // a = 1, b = 0: (a c + b d) and (b c - a d) keep their signed zeros.
+    const double re = __dadd_rn(__dmul_rn(1.0, c), __dmul_rn(0.0, d));
+    const double im = __dsub_rn(__dmul_rn(0.0, c), __dmul_rn(1.0, d));
+    *xr = static_cast<float>(re / den);
+    *xi = static_cast<float>(im / den);
+  }
+}
+
+// Complex TRSM base: X T = B for independent rows of X (src/trsm-inl.h:
+// 175-214), T r x r (r <= 32) read through a view. Column j (solve order) is
+// b_j - sum of x_q t(q, j) over the solved q in increasing q, kept as four
+// fma chains (xr tr, xi tr, xr ti, xi ti) combined as (rr - ii, ir + ri),
+// then times inv_j = 1 / t(j, j). One thread owns one row; the row sits in
+// registers indexed in solve order (static indices), T in shared memory.
+// Element (row, j) of X is at x + 2 * (row * xs_row + j * xs_col).
+template <typename R>
+__global__ void __launch_bounds__(128)
+    ZTrsmBaseKernel(ZView<R> tri, int lower, int unit, int r, int rows, R* x,
+                    long long xs_row, long long xs_col, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  // st[s][u] = T(q(s), j(u)) in solve order (conjugated for 'C').
+  __shared__ R st_re[32][33], st_im[32][33];
+  __shared__ R inv_re[32], inv_im[32];
+  for (int idx = threadIdx.x; idx < 32 * 32; idx += blockDim.x) {
+    const int s = idx / 32, u = idx % 32;
+    R vr = R(0), vi = R(0);
+    if (s < r && u < r && (s < u || (s == u && !unit))) {
+      const int q = lower ? r - 1 - s : s, j = lower ? r - 1 - u : u;
+      const R* e = tri.data + 2 * (q * tri.rs + j * tri.cs);
+      vr = e[0];
+      vi = tri.conj ? -e[1] : e[1];
+    }
+    st_re[s][u] = vr;
+    st_im[s][u] = vi;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int s = threadIdx.x;
+    R a = R(1), b = R(0);
+    if (s < r && !unit) ZRecip<R>(st_re[s][s], st_im[s][s], &a, &b);
+    inv_re[s] = a;
+    inv_im[s] = b;
+  }
+  __syncthreads();
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  R* xr = x + 2 * (row * xs_row);
+  R yr[32], yi[32];
+#pragma unroll
+  for (int s = 0; s < 32; ++s) {
+    if (s < r) {
+      const long long off = 2 * ((lower ? r - 1 - s : s) * xs_col);
+      yr[s] = xr[off];
+      yi[s] = xr[off + 1];
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < 32; ++s) {
+    if (s >= r) break;
+    R s_rr = R(0), s_ir = R(0), s_ri = R(0), s_ii = R(0);
+    // Solved columns in increasing original index: solve order 0..s-1 for
+    // upper, s-1 down to 0 for lower.
+    if (lower) {
+#pragma unroll
+      for (int w = 31; w >= 0; --w) {
+        if (w >= s) continue;
+        const R tr = st_re[w][s], ti = st_im[w][s];
+        s_rr = Fma(yr[w], tr, s_rr);
+        s_ir = Fma(yi[w], tr, s_ir);
+        s_ri = Fma(yr[w], ti, s_ri);
+        s_ii = Fma(yi[w], ti, s_ii);
+      }
+    } else {
+#pragma unroll
+      for (int w = 0; w < 32; ++w) {
+        if (w >= s) break;
+        const R tr = st_re[w][s], ti = st_im[w][s];
+        s_rr = Fma(yr[w], tr, s_rr);
+        s_ir = Fma(yi[w], tr, s_ir);
+        s_ri = Fma(yr[w], ti, s_ri);
+        s_ii = Fma(yi[w], ti, s_ii);
+      }
+    }
+    R vr = Sub(yr[s], Sub(s_rr, s_ii));
+    R vi = Sub(yi[s], Add(s_ir, s_ri));
+    if (!unit) {
+      const R a0 = Mul(vr, inv_re[s]), a1 = Mul(vi, inv_im[s]);
+      const R a2 = Mul(vi, inv_re[s]), a3 = Mul(vr, inv_im[s]);
+      vr = Sub(a0, a1);
+      vi = Add(a2, a3);
+    }
+    yr[s] = vr;
+    yi[s] = vi;
+  }
+#pragma unroll
+  for (int s = 0; s < 32; ++s) {
+    if (s < r) {
+      const long long off = 2 * ((lower ? r - 1 - s : s) * xs_col);
+      xr[off] = yr[s];
+      xr[off + 1] = yi[s];
+    }
+  }
+}
+
 }  // namespace
+
+// The complex GEMM kernel on operand views (elements aligned to their size;
+// m, n, k > 0): C := alpha op(A) op(B) + beta C with the reference's merges.
+template <typename R>
+void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, const R* beta,
+                R* c, int ldc) {
+  ZParams<R> p;
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.alpha_re = alpha[0];
+  p.alpha_im = alpha[1];
+  p.beta_re = beta[0];
+  p.beta_im = beta[1];
+  p.a = a;
+  p.b = b;
+  p.c = c;
+  p.ldc = ldc;
+  p.guard = Ctx().guard;
+  const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(ZgemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         ZSmemBytes<R>());
+    configured = true;
+  }
+  ZgemmKernel<R><<<grid, 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
+  CountLaunch();
+  LaunchFailed("complex gemm");
+}
+
+// The complex TRSM recursion (src/trsm.cc:87-135) on an op(A) view.
+template <typename R>
+static void ZTrsmRec(bool left, ZView<R> tri, bool lower, bool unit, int r, int other, R* b,
+                     int ldb) {
+  constexpr int kBase = 32;
+  if (r <= 0 || other <= 0) return;
+  if (r <= kBase) {
+    ZView<R> t = tri;
+    bool lo = lower;
+    long long xs_row, xs_col;
+    if (left) {  // T X = B  <=>  X^T T^T = B^T (src/trsm-inl.h:306-324)
+      t.rs = tri.cs;
+      t.cs = tri.rs;
+      lo = !lower;
+      xs_row = ldb;
+      xs_col = 1;
+    } else {
+      xs_row = 1;
+      xs_col = ldb;
+    }
+    ZTrsmBaseKernel<R><<<(other + 127) / 128, 128, 0, Ctx().stream>>>(
+        t, lo ? 1 : 0, unit ? 1 : 0, r, other, b, xs_row, xs_col, Ctx().guard);
+    CountLaunch();
+    LaunchFailed("complex trsm base");
+    return;
+  }
+  const int r1 = std::max(kBase, (r / 2) / kBase * kBase), r2 = r - r1;
+  const auto sub = [&](int i0, int j0) {
+    ZView<R> v = tri;
+    v.data += 2 * (i0 * tri.rs + j0 * tri.cs);
+    return v;
+  };
+  const ZView<R> t11 = tri, t22 = sub(r1, r1), toff = lower ? sub(r1, 0) : sub(0, r1);
+  const R m1[2] = {R(-1), R(0)}, one[2] = {R(1), R(0)};
+  const auto col = [&](R* p) { return ZView<R>{p, 1, ldb, 0}; };
+  if (left) {
+    R* b1 = b;
+    R* b2 = b + 2 * r1;
+    if (lower) {
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+      ZgemmViews<R>(r2, other, r1, m1, toff, col(b1), one, b2, ldb);
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+    } else {
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+      ZgemmViews<R>(r1, other, r2, m1, toff, col(b2), one, b1, ldb);
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+    }
+  } else {
+    R* b1 = b;
+    R* b2 = b + 2 * static_cast<long long>(r1) * ldb;
+    if (lower) {
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+      ZgemmViews<R>(other, r1, r2, m1, col(b2), toff, one, b1, ldb);
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+    } else {
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+      ZgemmViews<R>(other, r2, r1, m1, col(b1), toff, one, b2, ldb);
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+    }
+  }
+}
+
+// Complex TRSM (src/trsm.cc:137-180) after argument checks: B := alpha B
+// (alpha != 1), zero B for alpha 0, then the recursion on op(A) (op 0 N,
+// 1 T, 2 C). A and B are used where they are when their elements are aligned
+// to their size (cp.async in the GEMM updates), else through aligned copies.
+template <typename R>
+void ZtrsmFull(bool left, bool lower, int op, bool unit, int m, int n, const R* alpha,
+               const R* a, int lda, R* b, int ldb) {
+  if (m == 0 || n == 0) return;
+  const bool alpha_one = alpha[0] == R(1) && alpha[1] == R(0);
+  const bool alpha_zero = alpha[0] == R(0) && alpha[1] == R(0);
+  if (!alpha_one) {
+    const long long total = static_cast<long long>(m) * n;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 8));
+    ZScaleKernel<R><<<blocks, 256, 0, Ctx().stream>>>(m, n, alpha[0], alpha[1], b, ldb,
+                                                        Ctx().guard);
+    CountLaunch();
+    if (LaunchFailed("complex trsm scale")) return;
+  }
+  if (alpha_zero) return;
+  const int ka = left ? m : n;
+  const size_t esz = 2 * sizeof(R);
+  if (reinterpret_cast<uintptr_t>(a) % esz != 0) {
+    R* dst = static_cast<R*>(Workspace(kWsLevel3, esz * static_cast<size_t>(ka) * ka));
+    if (dst == nullptr ||
+        Failed(cudaMemcpy2DAsync(dst, esz * ka, a, esz * lda, esz * ka, ka,
+                                 cudaMemcpyDeviceToDevice, Ctx().stream),
+               "complex trsm copy"))
+      return;
+    a = dst;
+    lda = ka;
+  }
+  R* bw = b;
+  int ldbw = ldb;
+  if (reinterpret_cast<uintptr_t>(b) % esz != 0) {
+    bw = static_cast<R*>(Workspace(kWsLevel3Copy, esz * static_cast<size_t>(m) * n));
+    if (bw == nullptr ||
+        Failed(cudaMemcpy2DAsync(bw, esz * m, b, esz * ldb, esz * m, n,
+                                 cudaMemcpyDeviceToDevice, Ctx().stream),
+               "complex trsm copy"))
+      return;
+    ldbw = m;
+  }
+  const ZView<R> tri = op == 0 ? ZView<R>{a, 1, lda, 0} : ZView<R>{a, lda, 1, op == 2 ? 1 : 0};
+  const bool op_lower = lower != (op != 0);
+  ZTrsmRec<R>(left, tri, op_lower, unit, ka, left ? n : m, bw, ldbw);
+  if (bw != b) {
+    Failed(cudaMemcpy2DAsync(b, esz * ldb, bw, esz * m, esz * m, n, cudaMemcpyDeviceToDevice,
+                             Ctx().stream),
+           "complex trsm copy back");
+  }
+}
+template void ZtrsmFull<double>(bool, bool, int, bool, int, int, const double*, const double*,
+                                int, double*, int);
+template void ZtrsmFull<float>(bool, bool, int, bool, int, int, const float*, const float*,
+                               int, float*, int);
 
 // GEMM (src/gemm.cc:67-123) for complex data after argument checks: a, b, c
 // interleaved, leading dimensions in complex elements; alpha, beta as
@@ -280,30 +590,10 @@ void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, 
   if (a == nullptr || b == nullptr) return;
   lda = lda2;
   ldb = ldb2;
-  ZParams<R> p;
-  p.m = m;
-  p.n = n;
-  p.k = k;
-  p.alpha_re = alpha[0];
-  p.alpha_im = alpha[1];
-  p.beta_re = beta[0];
-  p.beta_im = beta[1];
-  // op: 0 N, 1 T, 2 C. Element (i, p) of op(A): A(i, p) or A(p, i).
-  p.a = ta == 0 ? ZView<R>{a, 1, lda, 0} : ZView<R>{a, lda, 1, ta == 2 ? 1 : 0};
-  p.b = tb == 0 ? ZView<R>{b, 1, ldb, 0} : ZView<R>{b, ldb, 1, tb == 2 ? 1 : 0};
-  p.c = c;
-  p.ldc = ldc;
-  p.guard = Ctx().guard;
-  const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(ZgemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         ZSmemBytes<R>());
-    configured = true;
-  }
-  ZgemmKernel<R><<<grid, 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
-  CountLaunch();
-  LaunchFailed("complex gemm");
+  ZgemmViews<R>(m, n, k, alpha,
+                ta == 0 ? ZView<R>{a, 1, lda, 0} : ZView<R>{a, lda, 1, ta == 2 ? 1 : 0},
+                tb == 0 ? ZView<R>{b, 1, ldb, 0} : ZView<R>{b, ldb, 1, tb == 2 ? 1 : 0}, beta,
+                c, ldc);
 }
 template void ZgemmFull<double>(int, int, int, int, int, const double*, const double*, int,
                                 const double*, int, const double*, double*, int);

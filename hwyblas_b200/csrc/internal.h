@@ -221,6 +221,10 @@ void GerfsFull(bool trans, int n, int nrhs, const T* a, int lda, const T* af, in
 template <typename R>
 void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, int lda,
                const R* b, int ldb, const R* beta, R* c, int ldc);
+// Complex TRSM (src/trsm.cc:137-180) after argument checks, op 0 N / 1 T / 2 C.
+template <typename R>
+void ZtrsmFull(bool left, bool lower, int op, bool unit, int m, int n, const R* alpha,
+               const R* a, int lda, R* b, int ldb);
 template <typename T>
 void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
                 const T* b, int ldb, T beta, T* c, int ldc);

@@ -97,6 +97,17 @@ HWYBLAS_API void cgemm_(const char* transa, const char* transb, const hwyblas_in
                         const float* a, const hwyblas_int* lda, const float* b,
                         const hwyblas_int* ldb, const float* beta, float* c,
                         const hwyblas_int* ldc);
+/* Complex TRSM in place, transa N, T or C; interleaved arrays. Replace
+ * ztrsm_ / ctrsm_ (include/hwyblas/hwyblas.h:802, 797; src/trsm.cc:137-180,
+ * 202-215). */
+HWYBLAS_API void ztrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const double* alpha, const double* a, const hwyblas_int* lda,
+                        double* b, const hwyblas_int* ldb);
+HWYBLAS_API void ctrsm_(const char* side, const char* uplo, const char* transa,
+                        const char* diag, const hwyblas_int* m, const hwyblas_int* n,
+                        const float* alpha, const float* a, const hwyblas_int* lda, float* b,
+                        const hwyblas_int* ldb);
 /* C := alpha*A*B + beta*C (side L) or alpha*B*A + beta*C (side R), A
  * symmetric with only the uplo triangle read. Replace dsymm_ / ssymm_
  * (include/hwyblas/hwyblas.h:597, 591; src/level3.cc:369-375, 362-368). */
@@ -491,6 +502,18 @@ HWYBLAS_API void cblas_strsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
  * 1631-1700, 1727-1746, 1842-1861, 1908-1927). */
 /* CBLAS complex GEMM, alpha and beta by address (include/hwyblas/cblas.h:631,
  * 623; src/cblas.cc:520-537). */
+/* CBLAS complex TRSM, alpha by address (include/hwyblas/cblas.h:879, 872;
+ * src/cblas.cc:666-700, 1970-1990). */
+HWYBLAS_API void cblas_ztrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const void* alpha, const void* a, const hwyblas_int lda, void* b,
+                             const hwyblas_int ldb);
+HWYBLAS_API void cblas_ctrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
+                             const CBLAS_UPLO uplo, const CBLAS_TRANSPOSE transa,
+                             const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
+                             const void* alpha, const void* a, const hwyblas_int lda, void* b,
+                             const hwyblas_int ldb);
 HWYBLAS_API void cblas_zgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
                              const CBLAS_TRANSPOSE transb, const hwyblas_int m,
                              const hwyblas_int n, const hwyblas_int k, const void* alpha,

@@ -75,6 +75,14 @@ int orc_zgemm(char ta, char tb, int m, int n, int k, const double* alpha, const 
               int lda, const double* b, int ldb, const double* beta, double* c, int ldc);
 int orc_cgemm(char ta, char tb, int m, int n, int k, const float* alpha, const float* a,
               int lda, const float* b, int ldb, const float* beta, float* c, int ldc);
+/* Complex TRSM (src/trsm.cc:87-180, src/trsm-inl.h:175-214) and the complex
+ * reciprocal of the C++ runtime (pins the device's restatement). */
+int orc_ztrsm(char side, char uplo, char ta, char diag, int m, int n, const double* alpha,
+              const double* a, int lda, double* b, int ldb);
+int orc_ctrsm(char side, char uplo, char ta, char diag, int m, int n, const float* alpha,
+              const float* a, int lda, float* b, int ldb);
+void orc_zrecip(int n, const double* c, double* out);
+void orc_crecip(int n, const float* c, float* out);
 /* Level 3 through the GEMM problem model (src/level3.cc:26-342). */
 int orc_dsymm(char side, char uplo, int m, int n, double alpha, const double* a, int lda,
               const double* b, int ldb, double beta, double* c, int ldc);

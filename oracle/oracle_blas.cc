@@ -22,6 +22,7 @@
 #include <atomic>
 #include <thread>
 #include <cmath>
+#include <complex>
 #include <cstddef>
 #include <cstring>
 #include <vector>
@@ -770,6 +771,76 @@ template int Trmm<float>(char, char, char, char, int, int, float, const float*, 
 // ab = (rr - ii, ir + ri) and r = alpha * ab as (ab.re*al.re - ab.im*al.im,
 // ab.im*al.re + ab.re*al.im), every product and sum rounded; the first chunk
 // merges r, r + C or r + beta*C (beta 0, 1, other), the later ones r + C.
+// A complex operand: element (i, p) has its real part at
+// data[2 * (i * rs + p * cs)]; conj negates the imaginary part.
+template <typename R>
+struct ZOp {
+  const R* data;
+  ptrdiff_t rs, cs;
+  bool conj;
+  void at(ptrdiff_t i, ptrdiff_t p, R* re, R* im) const {
+    const R* e = data + 2 * (i * rs + p * cs);
+    *re = e[0];
+    *im = conj ? -e[1] : e[1];
+  }
+  ZOp sub(ptrdiff_t i0, ptrdiff_t p0) const {
+    ZOp o = *this;
+    o.data += 2 * (i0 * rs + p0 * cs);
+    return o;
+  }
+};
+
+// The complex GEMM problem (m, n, k > 0, alpha != 0) on operand views.
+template <typename R>
+void ZGemmCore(int m, int n, int k, const R* alpha, ZOp<R> a, ZOp<R> b, const R* beta, R* c,
+               int ldc) {
+  const bool beta_zero = beta[0] == R(0) && beta[1] == R(0);
+  const bool beta_one = beta[0] == R(1) && beta[1] == R(0);
+  const auto C = [&](int i, int j) { return c + 2 * (i + static_cast<ptrdiff_t>(j) * ldc); };
+  constexpr int KC = 256;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) {
+      R cre = R(0), cim = R(0);
+      for (int pc = 0; pc < k; pc += KC) {
+        const int pe = std::min(k, pc + KC);
+        R rr = R(0), ir = R(0), ri = R(0), ii = R(0);
+        for (int p = pc; p < pe; ++p) {
+          R ar, ai, br, bi;
+          a.at(i, p, &ar, &ai);
+          b.at(p, j, &br, &bi);
+          rr = std::fma(ar, br, rr);
+          ir = std::fma(ai, br, ir);
+          ri = std::fma(ar, bi, ri);
+          ii = std::fma(ai, bi, ii);
+        }
+        const R ab_re = rr - ii, ab_im = ir + ri;
+        const R q0 = ab_re * alpha[0], q1 = ab_im * alpha[1];
+        const R q2 = ab_im * alpha[0], q3 = ab_re * alpha[1];
+        const R t_re = q0 - q1, t_im = q2 + q3;
+        if (pc != 0) {
+          cre = t_re + cre;
+          cim = t_im + cim;
+        } else if (beta_zero) {
+          cre = t_re;
+          cim = t_im;
+        } else {
+          const R c0 = C(i, j)[0], c1 = C(i, j)[1];
+          if (beta_one) {
+            cre = t_re + c0;
+            cim = t_im + c1;
+          } else {
+            const R s0 = c0 * beta[0], s1 = c1 * beta[1], s2 = c1 * beta[0], s3 = c0 * beta[1];
+            const R b_re = s0 - s1, b_im = s2 + s3;
+            cre = t_re + b_re;
+            cim = t_im + b_im;
+          }
+        }
+      }
+      C(i, j)[0] = cre;
+      C(i, j)[1] = cim;
+    }
+}
+
 template <typename R>
 int ZgemmF(char transa, char transb, int m, int n, int k, const R* alpha, const R* a, int lda,
            const R* b, int ldb, const R* beta, R* c, int ldc) {
@@ -810,63 +881,150 @@ int ZgemmF(char transa, char transb, int m, int n, int k, const R* alpha, const 
       }
     return 0;
   }
-  // Element (i, p) of op(A) and (p, j) of op(B) as (re, im).
-  const auto opa = [&](int i, int p, R* re, R* im) {
-    const R* e = ta == 0 ? a + 2 * (i + static_cast<ptrdiff_t>(p) * lda)
-                         : a + 2 * (p + static_cast<ptrdiff_t>(i) * lda);
-    *re = e[0];
-    *im = ta == 2 ? -e[1] : e[1];
-  };
-  const auto opb = [&](int p, int j, R* re, R* im) {
-    const R* e = tb == 0 ? b + 2 * (p + static_cast<ptrdiff_t>(j) * ldb)
-                         : b + 2 * (j + static_cast<ptrdiff_t>(p) * ldb);
-    *re = e[0];
-    *im = tb == 2 ? -e[1] : e[1];
-  };
-  constexpr int KC = 256;
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i < m; ++i) {
-      R cre = R(0), cim = R(0);
-      for (int pc = 0; pc < k; pc += KC) {
-        const int pe = std::min(k, pc + KC);
-        R rr = R(0), ir = R(0), ri = R(0), ii = R(0);
-        for (int p = pc; p < pe; ++p) {
-          R ar, ai, br, bi;
-          opa(i, p, &ar, &ai);
-          opb(p, j, &br, &bi);
-          rr = std::fma(ar, br, rr);
-          ir = std::fma(ai, br, ir);
-          ri = std::fma(ar, bi, ri);
-          ii = std::fma(ai, bi, ii);
-        }
-        const R ab_re = rr - ii, ab_im = ir + ri;
-        const R q0 = ab_re * alpha[0], q1 = ab_im * alpha[1];
-        const R q2 = ab_im * alpha[0], q3 = ab_re * alpha[1];
-        const R t_re = q0 - q1, t_im = q2 + q3;
-        if (pc != 0) {
-          cre = t_re + cre;
-          cim = t_im + cim;
-        } else if (beta_zero) {
-          cre = t_re;
-          cim = t_im;
-        } else {
-          const R c0 = C(i, j)[0], c1 = C(i, j)[1];
-          if (beta_one) {
-            cre = t_re + c0;
-            cim = t_im + c1;
-          } else {
-            const R s0 = c0 * beta[0], s1 = c1 * beta[1], s2 = c1 * beta[0], s3 = c0 * beta[1];
-            const R b_re = s0 - s1, b_im = s2 + s3;
-            cre = t_re + b_re;
-            cim = t_im + b_im;
-          }
-        }
-      }
-      C(i, j)[0] = cre;
-      C(i, j)[1] = cim;
-    }
+  const ZOp<R> va = ta == 0 ? ZOp<R>{a, 1, lda, false} : ZOp<R>{a, lda, 1, ta == 2};
+  const ZOp<R> vb = tb == 0 ? ZOp<R>{b, 1, ldb, false} : ZOp<R>{b, ldb, 1, tb == 2};
+  ZGemmCore<R>(m, n, k, alpha, va, vb, beta, c, ldc);
   return 0;
 }
+// ---------------------------------------------------------------------------
+// Complex TRSM (src/trsm.cc:87-180; src/trsm-inl.h:40-70, 175-214, 277-325).
+// The recursion and its GEMM updates (alpha -1, beta 1) are the real ones.
+// The base solves X T = B row by row (T X = B through the transposed
+// triangle): column j in solve order is b_j - sum_q x_q t(q, j) over the
+// solved q in increasing q, the sum kept as the four fma chains
+// (xr*tr, xi*tr, xr*ti, xi*ti) combined as (rr - ii, ir + ri), then
+// multiplied by inv_j = 1 / t(j, j) as (xr*vr - xi*vi, xi*vr + xr*vi). inv_j
+// is the C++ complex quotient, which is what the reference computes.
+template <typename R>
+static void ZTrsmBase(bool left, ZOp<R> tri, bool lower, bool unit, int r, int other, R* b,
+                      int ldb) {
+  if (left) {  // T X = B  <=>  X^T T^T = B^T
+    std::swap(tri.rs, tri.cs);
+    lower = !lower;
+  }
+  std::vector<R> inv_re(r), inv_im(r);
+  for (int j = 0; j < r; ++j) {
+    R dr, di;
+    tri.at(j, j, &dr, &di);
+    const std::complex<R> v = unit ? std::complex<R>(1) : std::complex<R>(1) / std::complex<R>(dr, di);
+    inv_re[j] = v.real();
+    inv_im[j] = v.imag();
+  }
+  // Row `row` of X: element (row, j) at b + 2 * (row * xr + j * xc).
+  const ptrdiff_t xr = left ? ldb : 1, xc = left ? 1 : ldb;
+  for (int row = 0; row < other; ++row) {
+    R* x = b + 2 * (static_cast<ptrdiff_t>(row) * xr);
+    for (int step = 0; step < r; ++step) {
+      const int j = lower ? r - 1 - step : step;
+      const int qb = lower ? j + 1 : 0, qe = lower ? r : j;
+      R s_rr = R(0), s_ir = R(0), s_ri = R(0), s_ii = R(0);
+      for (int q = qb; q < qe; ++q) {
+        R tr, ti;
+        tri.at(q, j, &tr, &ti);
+        const R yr = x[2 * q * xc], yi = x[2 * q * xc + 1];
+        s_rr = std::fma(yr, tr, s_rr);
+        s_ir = std::fma(yi, tr, s_ir);
+        s_ri = std::fma(yr, ti, s_ri);
+        s_ii = std::fma(yi, ti, s_ii);
+      }
+      const R p_re = s_rr - s_ii, p_im = s_ir + s_ri;
+      R vr = x[2 * j * xc] - p_re, vi = x[2 * j * xc + 1] - p_im;
+      if (!unit) {
+        const R a0 = vr * inv_re[j], a1 = vi * inv_im[j], a2 = vi * inv_re[j], a3 = vr * inv_im[j];
+        vr = a0 - a1;
+        vi = a2 + a3;
+      }
+      x[2 * j * xc] = vr;
+      x[2 * j * xc + 1] = vi;
+    }
+  }
+}
+
+template <typename R>
+static void ZTrsmRec(bool left, ZOp<R> tri, bool lower, bool unit, int r, int other, R* b,
+                     int ldb) {
+  constexpr int kBase = 32;
+  if (r <= kBase) {
+    ZTrsmBase<R>(left, tri, lower, unit, r, other, b, ldb);
+    return;
+  }
+  const int r1 = std::max(kBase, (r / 2) / kBase * kBase), r2 = r - r1;
+  const ZOp<R> t11 = tri, t22 = tri.sub(r1, r1);
+  const ZOp<R> toff = lower ? tri.sub(r1, 0) : tri.sub(0, r1);
+  const R m1[2] = {R(-1), R(0)}, one[2] = {R(1), R(0)};
+  const auto col = [&](R* p) { return ZOp<R>{p, 1, ldb, false}; };
+  if (left) {
+    R* b1 = b;
+    R* b2 = b + 2 * r1;
+    if (lower) {
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+      ZGemmCore<R>(r2, other, r1, m1, toff, col(b1), one, b2, ldb);
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+    } else {
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+      ZGemmCore<R>(r1, other, r2, m1, toff, col(b2), one, b1, ldb);
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+    }
+  } else {
+    R* b1 = b;
+    R* b2 = b + 2 * static_cast<ptrdiff_t>(r1) * ldb;
+    if (lower) {
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+      ZGemmCore<R>(other, r1, r2, m1, col(b2), toff, one, b1, ldb);
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+    } else {
+      ZTrsmRec<R>(left, t11, lower, unit, r1, other, b1, ldb);
+      ZGemmCore<R>(other, r2, r1, m1, col(b1), toff, one, b2, ldb);
+      ZTrsmRec<R>(left, t22, lower, unit, r2, other, b2, ldb);
+    }
+  }
+}
+
+template <typename R>
+int ZtrsmF(char side, char uplo, char transa, char diag, int m, int n, const R* alpha,
+           const R* a, int lda, R* b, int ldb) {
+  const char s = Up(side), u = Up(uplo), d = Up(diag), t = Up(transa);
+  const int op = t == 'N' ? 0 : t == 'T' ? 1 : t == 'C' ? 2 : -1;
+  const bool left = (s == 'L');
+  const int ka = left ? m : n;
+  int info = 0;
+  if (s != 'L' && s != 'R') info = 1;
+  else if (u != 'L' && u != 'U') info = 2;
+  else if (op < 0) info = 3;
+  else if (d != 'U' && d != 'N') info = 4;
+  else if (m < 0) info = 5;
+  else if (n < 0) info = 6;
+  else if (lda < std::max(1, ka)) info = 9;
+  else if (ldb < std::max(1, m)) info = 11;
+  if (info) return info;
+  if (m == 0 || n == 0) return 0;
+  const bool alpha_one = alpha[0] == R(1) && alpha[1] == R(0);
+  const bool alpha_zero = alpha[0] == R(0) && alpha[1] == R(0);
+  if (!alpha_one) {
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < m; ++i) {
+        R* e = b + 2 * (i + static_cast<ptrdiff_t>(j) * ldb);
+        if (alpha_zero) {
+          e[0] = e[1] = R(0);
+        } else {
+          const R c0 = e[0], c1 = e[1];
+          const R p0 = c0 * alpha[0], p1 = c1 * alpha[1], p2 = c0 * alpha[1], p3 = c1 * alpha[0];
+          e[0] = p0 - p1;
+          e[1] = p2 + p3;
+        }
+      }
+  }
+  if (alpha_zero) return 0;
+  const ZOp<R> tri = op == 0 ? ZOp<R>{a, 1, lda, false} : ZOp<R>{a, lda, 1, op == 2};
+  const bool op_lower = (u == 'L') != (op != 0);
+  ZTrsmRec<R>(left, tri, op_lower, d == 'U', ka, left ? n : m, b, ldb);
+  return 0;
+}
+template int ZtrsmF<double>(char, char, char, char, int, int, const double*, const double*,
+                            int, double*, int);
+template int ZtrsmF<float>(char, char, char, char, int, int, const float*, const float*, int,
+                           float*, int);
+
 template int ZgemmF<double>(char, char, int, int, int, const double*, const double*, int,
                             const double*, int, const double*, double*, int);
 template int ZgemmF<float>(char, char, int, int, int, const float*, const float*, int,
@@ -952,6 +1110,31 @@ int orc_zgemm(char ta, char tb, int m, int n, int k, const double* alpha, const 
 int orc_cgemm(char ta, char tb, int m, int n, int k, const float* alpha, const float* a,
               int lda, const float* b, int ldb, const float* beta, float* c, int ldc) {
   return orc::ZgemmF<float>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int orc_ztrsm(char side, char uplo, char ta, char diag, int m, int n, const double* alpha,
+              const double* a, int lda, double* b, int ldb) {
+  return orc::ZtrsmF<double>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int orc_ctrsm(char side, char uplo, char ta, char diag, int m, int n, const float* alpha,
+              const float* a, int lda, float* b, int ldb) {
+  return orc::ZtrsmF<float>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+// The complex reciprocal as the C++ runtime computes it, for pinning the
+// device's restatement (Smith's method for double; float in double).
+void orc_zrecip(int n, const double* c, double* out) {
+  for (int i = 0; i < n; ++i) {
+    const std::complex<double> v = std::complex<double>(1) / std::complex<double>(c[2 * i], c[2 * i + 1]);
+    out[2 * i] = v.real();
+    out[2 * i + 1] = v.imag();
+  }
+}
+void orc_crecip(int n, const float* c, float* out) {
+  for (int i = 0; i < n; ++i) {
+    const std::complex<float> v = std::complex<float>(1) / std::complex<float>(c[2 * i], c[2 * i + 1]);
+    out[2 * i] = v.real();
+    out[2 * i + 1] = v.imag();
+  }
 }
 
 #define ORC_L3(P, T)                                                                       \

@@ -92,6 +92,10 @@ class Oracle:
         L.orc_sposv.argtypes = [CH, I, I, P, I, P, I]
         L.orc_ssyrk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
         L.orc_zgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
+        L.orc_ztrsm.argtypes = [CH, CH, CH, CH, I, I, P, P, I, P, I]
+        L.orc_ctrsm.argtypes = [CH, CH, CH, CH, I, I, P, P, I, P, I]
+        L.orc_zrecip.argtypes = [I, P, P]
+        L.orc_crecip.argtypes = [I, P, P]
         L.orc_cgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
         for pre in "ds":
             getattr(L, f"orc_{pre}gerfs").argtypes = [CH, I, I, P, I, P, I, P, P, I, P, I, P,
@@ -221,6 +225,15 @@ class Oracle:
         fn = self.lib.orc_zgemm if z else self.lib.orc_cgemm
         return fn(_b(ta), _b(tb), m, n, k, al.ctypes.data, ptr(a), lda, ptr(b), ldb,
                   be.ctypes.data, ptr(c), ldc)
+
+    def ztrsm(self, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb):
+        """Complex TRSM on complex128 / complex64 arrays (by b's dtype)."""
+        z = b.dtype == np.complex128
+        rt = np.float64 if z else np.float32
+        al = np.array([complex(alpha).real, complex(alpha).imag], rt)
+        fn = self.lib.orc_ztrsm if z else self.lib.orc_ctrsm
+        return fn(_b(side), _b(uplo), _b(ta), _b(diag), m, n, al.ctypes.data, ptr(a), lda,
+                  ptr(b), ldb)
 
     def getri(self, n, a, lda, ipiv, work, lwork):
         p = "s" if a.dtype == np.float32 else "d"

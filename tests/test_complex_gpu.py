@@ -119,3 +119,96 @@ def test_zgemm_misaligned_device_operand(hb, orc):
     c2 = c.copy(order="F")
     assert orc.zgemm("N", "N", m, n, k, 1.25 - 0.5j, a, m, b, k, 0.5, c2, m) == 0
     assert same_bits(creal(tc.cpu().numpy()), creal(c2))
+
+
+CTRI = [(s, u, t, d) for s in "LR" for u in "LU" for t in "NTC" for d in "NU"]
+
+
+def ctriangle(rng, ka, uplo, diag, dtype):
+    """Triangular complex matrix with NaN wherever TRSM must not read."""
+    a = np.full((ka, ka), np.nan + 1j * np.nan, dtype=dtype, order="F")
+    t = (rng.uniform(-1, 1, (ka, ka)) + 1j * rng.uniform(-1, 1, (ka, ka))) / max(ka, 1)
+    keep = np.tril(np.ones((ka, ka), bool), -1)
+    if uplo == "U":
+        keep = keep.T
+    a[keep] = t[keep]
+    if diag == "N":
+        idx = np.arange(ka)
+        a[idx, idx] = (1.5 + rng.uniform(0, 0.5, ka)) * np.exp(1j * rng.uniform(0, 6.28, ka))
+    return a
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("side,uplo,trans,diag", CTRI)
+def test_ztrsm_bitexact(hb, orc, p, side, uplo, trans, diag):
+    dtype = np.complex128 if p == "z" else np.complex64
+    for m, n in [(1, 3), (5, 7), (33, 17), (100, 40), (300, 70)]:
+        if side == "R":
+            m, n = n, m
+        rng = np.random.default_rng(m * 31 + n)
+        ka = m if side == "L" else n
+        a = ctriangle(rng, ka, uplo, diag, dtype)
+        b = crand(rng, m + 1, n, dtype)
+        for alpha in (1.0, 0.5 - 0.75j):
+            b1, b2 = b.copy(order="F"), b.copy(order="F")
+            hb.ztrsm(p, side, uplo, trans, diag, m, n, alpha, a, ka, b1, m + 1)
+            assert orc.ztrsm(side, uplo, trans, diag, m, n, alpha, a, ka, b2, m + 1) == 0
+            assert same_bits(creal(b1), creal(b2)), (m, n, alpha)
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+def test_ztrsm_diagonal_reciprocals(hb, orc, p):
+    """The device's 1/t(j, j) against the C++ runtime's complex quotient (the
+    reference's), through diagonal triangles: magnitudes 2^-40..2^40 and
+    purely real or imaginary diagonals."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(11)
+    for trial in range(8):
+        r = 32
+        d = (rng.uniform(-1, 1, r) * 2.0 ** rng.integers(-40, 40, r)
+             + 1j * rng.uniform(-1, 1, r) * 2.0 ** rng.integers(-40, 40, r))
+        d[trial % r] = d[trial % r].real
+        d[(trial + 5) % r] = 1j * d[(trial + 5) % r].imag
+        a = np.asfortranarray(np.diag(d).astype(dtype))
+        b = np.asfortranarray(np.ones((50, r), dtype))
+        b1, b2 = b.copy(order="F"), b.copy(order="F")
+        hb.ztrsm(p, "R", "U", "N", "N", 50, r, 1.0, a, r, b1, 50)
+        assert orc.ztrsm("R", "U", "N", "N", 50, r, 1.0, a, r, b2, 50) == 0
+        assert same_bits(creal(b1), creal(b2)), trial
+
+
+def test_ztrsm_device_misaligned_and_cblas(hb, orc):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(13)
+    m, n = 90, 40
+    a = ctriangle(rng, m, "L", "N", np.complex128)
+    b = crand(rng, m, n, np.complex128)
+    flat = np.zeros(2 * m * n + 1)
+    flat[1:] = b.ravel(order="F").view(np.float64)
+    tb = torch.from_numpy(flat).cuda()
+    ta = torch.from_numpy(np.ascontiguousarray(a.T)).T.cuda()
+    hb.ztrsm("z", "L", "L", "C", "N", m, n, 1.0 - 1.0j, ta, m, tb.data_ptr() + 8, m)
+    want = b.copy(order="F")
+    assert orc.ztrsm("L", "L", "C", "N", m, n, 1.0 - 1.0j, a, m, want, m) == 0
+    got = tb.cpu().numpy()[1:].view(np.complex128).reshape(n, m).T
+    assert same_bits(creal(got), creal(want))
+    # Row-major CBLAS: B^T := alpha B^T op(A)^T with the other side and triangle.
+    L = hb.lib()
+    al = np.array([0.5, 0.25])
+    brow = np.ascontiguousarray(b)
+    arow = np.ascontiguousarray(a)
+    L.cblas_ztrsm(hb.CblasRowMajor, hb.CblasLeft, hb.CblasLower, hb.CblasNoTrans,
+                  hb.CblasNonUnit, m, n, al.ctypes.data, arow.ctypes.data, m,
+                  brow.ctypes.data, n)
+    want = np.asfortranarray(b.T)
+    assert orc.ztrsm("R", "U", "N", "N", n, m, 0.5 + 0.25j, np.asfortranarray(a.T), m, want,
+                     n) == 0
+    assert same_bits(creal(brow.T), creal(want))
+    with hb.ErrorCapture() as cap:
+        hb.ztrsm("z", "X", "L", "N", "N", 2, 2, 1.0, a, 2, b, 2)
+        hb.ztrsm("c", "L", "L", "N", "N", 2, 2, 1.0, a.astype(np.complex64), 1,
+                 b.astype(np.complex64), 2)
+        L.cblas_ztrsm(hb.CblasRowMajor, hb.CblasLeft, hb.CblasLower, hb.CblasNoTrans,
+                      hb.CblasNonUnit, -1, n, al.ctypes.data, arow.ctypes.data, m,
+                      brow.ctypes.data, n)
+    assert cap.errors == [("ZTRSM", 1), ("CTRSM", 9), ("cblas_ztrsm", 6)]

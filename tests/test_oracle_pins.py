@@ -809,6 +809,53 @@ def test_zgemm_special_cases(orc):
     assert orc.zgemm("N", "N", 5, 4, 4, 1.0, z, 5, z, 4, 0.0, z, 4) == 13
 
 
+CTRI_CASES = [(s, u, t, d) for s in "LR" for u in "LU" for t in "NTC" for d in "NU"]
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("side,uplo,trans,diag", CTRI_CASES)
+def test_ztrsm_residual_bound(orc, dtype, side, uplo, trans, diag):
+    """Complex TRSM: |op(A) X - alpha B| within 8(ka+2)eps |op(A)||X| + ...
+    (tests/level3_test.cc:479-520 with complex types), the unread triangle and
+    a unit diagonal holding NaN."""
+    rng = np.random.default_rng(21)
+    m, n = (70, 13) if side == "L" else (13, 70)
+    ka = m if side == "L" else n
+    a = np.full((ka, ka), np.nan + 1j * np.nan, dtype=dtype, order="F")
+    t = (rng.uniform(-1, 1, (ka, ka)) + 1j * rng.uniform(-1, 1, (ka, ka))) / ka
+    keep = np.tril(np.ones((ka, ka), bool), -1)
+    if uplo == "U":
+        keep = keep.T
+    a[keep] = t[keep]
+    if diag == "N":
+        a[np.arange(ka), np.arange(ka)] = 1.5 + rng.uniform(0, 0.5, ka) + 0.5j
+    T = np.where(keep, a, 0).astype(np.complex128)
+    T[np.arange(ka), np.arange(ka)] = 1.0 if diag == "U" else a[np.arange(ka), np.arange(ka)]
+    op = T if trans == "N" else (T.T if trans == "T" else T.conj().T)
+    b = crand(rng, m, n, dtype)
+    alpha = 0.75 - 0.25j
+    x = b.copy(order="F")
+    assert orc.ztrsm(side, uplo, trans, diag, m, n, alpha, a, ka, x, m) == 0
+    X = x.astype(np.complex128)
+    lhs = op @ X if side == "L" else X @ op
+    bound = (np.abs(op) @ np.abs(X) if side == "L" else np.abs(X) @ np.abs(op))
+    eps = np.finfo(dtype).eps
+    assert np.all(np.abs(lhs - alpha * b.astype(np.complex128)) <= 8 * (ka + 2) * eps * 2 * bound
+                  + 1e-300)
+
+
+def test_complex_reciprocal_is_the_runtime_quotient(orc):
+    """The oracle's 1/d is the C++ runtime's complex quotient (what the
+    reference computes for the TRSM diagonal); sanity against numpy within
+    a few ulps on ordinary values."""
+    rng = np.random.default_rng(2)
+    d = (rng.uniform(-1, 1, 1000) * 2.0 ** rng.integers(-40, 40, 1000)
+         + 1j * rng.uniform(-1, 1, 1000) * 2.0 ** rng.integers(-40, 40, 1000))
+    out = np.zeros(1000, np.complex128)
+    orc.lib.orc_zrecip(1000, d.ctypes.data, out.ctypes.data)
+    assert np.allclose(out, 1 / d, rtol=1e-14, atol=0)
+
+
 def test_trsm_alpha_zero_does_not_read_a(orc):
     a = np.full(9, np.nan)
     b = np.ones(6)
