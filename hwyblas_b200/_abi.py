@@ -22,6 +22,11 @@ PROTOTYPES = {
     "dsyrk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]),
     **{f"{p}gemm_": (None, [C, C, PI, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "zc"},
     **{f"{p}trsm_": (None, [C, C, C, C, PI, PI, P, P, PI, P, PI]) for p in "zc"},
+    **{f"{p}getrf_": (None, [PI, PI, P, PI, P, PI]) for p in "zc"},
+    **{f"{p}getrf2_": (None, [PI, PI, P, PI, P, PI]) for p in "zc"},
+    **{f"{p}laswp_": (None, [PI, P, PI, PI, PI, P, PI]) for p in "zc"},
+    **{f"{p}getrs_": (None, [C, PI, PI, P, PI, P, P, PI, PI]) for p in "zc"},
+    **{f"{p}gesv_": (None, [PI, PI, P, PI, P, P, PI, PI]) for p in "zc"},
     **{f"{p}symm_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}syr2k_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])

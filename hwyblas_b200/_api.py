@@ -173,6 +173,30 @@ def ztrsm(p, side, uplo, transa, diag, m, n, alpha, a, lda, b, ldb):
                                 al.ctypes.data, _ptr(a), _i(lda), _ptr(b), _i(ldb))
 
 
+def zgetrf(p, m, n, a, lda, ipiv, recursive=False):
+    """Complex LU with partial pivoting; p is "z" or "c"; returns INFO
+    (reference zgetrf_/cgetrf_ and ...2_, src/lapack/getrf.cc:508-517)."""
+    fn = getattr(lib(), f"{p}{'getrf2' if recursive else 'getrf'}_")
+    return _info_call(fn, _i(m), _i(n), _ptr(a), _i(lda), _ptr(ipiv))
+
+
+def zlaswp(p, n, a, lda, k1, k2, ipiv, incx):
+    """Complex row interchanges (reference zlaswp_/claswp_, src/lapack/getrf.cc:518)."""
+    getattr(lib(), f"{p}laswp_")(_i(n), _ptr(a), _i(lda), _i(k1), _i(k2), _ptr(ipiv), _i(incx))
+
+
+def zgetrs(p, trans, n, nrhs, a, lda, ipiv, b, ldb):
+    """Complex solve with LU factors, trans N/T/C; returns INFO (src/lapack/getrf.cc:524)."""
+    return _info_call(getattr(lib(), f"{p}getrs_"), _c(trans), _i(n), _i(nrhs), _ptr(a),
+                      _i(lda), _ptr(ipiv), _ptr(b), _i(ldb))
+
+
+def zgesv(p, n, nrhs, a, lda, ipiv, b, ldb):
+    """Complex LU solve of A X = B; returns INFO (src/lapack/getrf.cc:531)."""
+    return _info_call(getattr(lib(), f"{p}gesv_"), _i(n), _i(nrhs), _ptr(a), _i(lda),
+                      _ptr(ipiv), _ptr(b), _i(ldb))
+
+
 def cblas_level3(name, *args):
     """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
     scalars, array arguments given as numpy arrays or device pointers."""

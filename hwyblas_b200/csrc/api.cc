@@ -1097,6 +1097,146 @@ static void GesvEntry(const char* name, const hwyblas_int* n_p, const hwyblas_in
   hb::Finish(name);
 }
 
+// The complex LU family (zgetrf_, cgetrf_, ... : src/lapack/getrf.cc:505-553
+// for T = c64 and c32): interleaved (re, im) arrays, leading dimensions in
+// complex elements. A device array whose address is not aligned to a whole
+// complex element is worked on in an aligned copy (the GEMM and TRSM updates
+// move whole elements).
+template <typename R>
+struct ZWorkMatrix {
+  hb::Staged<R> staged;
+  R* dev = nullptr;
+  int ld = 0;  // complex elements
+  int rows = 0, cols = 0;
+  bool copied = false;
+  bool In(R* p, int ld_in, int rows_in, int cols_in, int slot, bool copy_in,
+          int align_slot = hb::kWsZFactor) {
+    rows = rows_in;
+    cols = cols_in;
+    if (!staged.In(p, 2 * ld_in, 2 * rows_in, cols_in, slot, copy_in)) return false;
+    dev = staged.dev;
+    ld = std::max(staged.ld / 2, 1);
+    if (reinterpret_cast<uintptr_t>(dev) % (2 * sizeof(R)) == 0) return true;
+    const size_t esz = 2 * sizeof(R);
+    R* w = static_cast<R*>(hb::Workspace(align_slot, esz * rows * std::max(cols, 1)));
+    if (w == nullptr) return false;
+    if (copy_in && hb::Failed(cudaMemcpy2DAsync(w, esz * rows, dev, esz * ld, esz * rows, cols,
+                                                cudaMemcpyDeviceToDevice, Ctx().stream),
+                              "complex matrix copy"))
+      return false;
+    dev = w;
+    ld = std::max(rows, 1);
+    copied = true;
+    return true;
+  }
+  void Out() {
+    if (copied) {
+      const size_t esz = 2 * sizeof(R);
+      hb::Failed(cudaMemcpy2DAsync(staged.dev, esz * (staged.ld / 2), dev, esz * ld, esz * rows,
+                                   cols, cudaMemcpyDeviceToDevice, Ctx().stream),
+                 "complex matrix copy back");
+    }
+    staged.Out();
+  }
+};
+
+template <typename R>
+static void ZGetrfEntry(bool recursive, const char* name, const hwyblas_int* m_p,
+                        const hwyblas_int* n_p, R* a, const hwyblas_int* lda_p,
+                        hwyblas_int* ipiv, hwyblas_int* info) {
+  const int m = *m_p, n = *n_p, lda = *lda_p;
+  if (!CheckGetrf(name, m, n, lda, info)) return;
+  if (m == 0 || n == 0) return;
+  ZWorkMatrix<R> sa;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, m, n, hb::kWsStageA, true)) return;
+  if (!sp.In(ipiv, std::min(m, n), 0, false)) return;
+  hb::ResetInfo();
+  hb::ZGetrf<R>(recursive, m, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  sa.Out();
+  sp.Out();
+  *info = hb::ReadInfo();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZLaswpEntry(const char* name, const hwyblas_int* n_p, R* a,
+                        const hwyblas_int* lda_p, const hwyblas_int* k1_p,
+                        const hwyblas_int* k2_p, const hwyblas_int* ipiv,
+                        const hwyblas_int* incx_p) {
+  const int n = *n_p, lda = *lda_p, k1 = *k1_p, k2 = *k2_p, incx = *incx_p;
+  if (incx == 0 || n <= 0) return;
+  const int absinc = incx < 0 ? -incx : incx;
+  const int count = k1 + (k2 - k1) * absinc;
+  if (count <= 0 || k2 < k1) return;
+  hb::Staged<R> sa;
+  hb::StagedInts sp;
+  if (!sa.In(a, 2 * lda, 2 * lda, n, hb::kWsStageA, true)) return;
+  if (!sp.In(ipiv, count, 0, true)) return;
+  hb::ZLaswp<R>(n, sa.dev, sa.ld / 2, k1, k2, sp.dev, incx);
+  sa.Out();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZGetrsEntry(const char* name, const char* trans, const hwyblas_int* n_p,
+                        const hwyblas_int* nrhs_p, const R* a, const hwyblas_int* lda_p,
+                        const hwyblas_int* ipiv, R* b, const hwyblas_int* ldb_p,
+                        hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  const int op = DecodeOp3(*trans);
+  *info = 0;
+  if (op < 0) *info = -1;
+  else if (n < 0) *info = -2;
+  else if (nrhs < 0) *info = -3;
+  else if (lda < std::max(1, n)) *info = -5;
+  else if (ldb < std::max(1, n)) *info = -8;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return;
+  }
+  if (n == 0 || nrhs == 0) return;
+  ZWorkMatrix<R> sa, sb;
+  hb::StagedInts sp;
+  if (!sa.In(const_cast<R*>(a), lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true, hb::kWsZFactorB)) return;
+  if (!sp.In(ipiv, n, 0, true)) return;
+  hb::ZGetrs<R>(op, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZGesvEntry(const char* name, const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
+                       R* a, const hwyblas_int* lda_p, hwyblas_int* ipiv, R* b,
+                       const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  *info = 0;
+  if (n < 0) *info = -1;
+  else if (nrhs < 0) *info = -2;
+  else if (lda < std::max(1, n)) *info = -4;
+  else if (ldb < std::max(1, n)) *info = -7;
+  if (*info != 0) {
+    hb::ReportError(name, -*info);
+    return;
+  }
+  if (n == 0) return;
+  ZWorkMatrix<R> sa, sb;
+  hb::StagedInts sp;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true, hb::kWsZFactorB)) return;
+  if (!sp.In(ipiv, n, 0, false)) return;
+  hb::ResetInfo();
+  hb::ZGetrf<R>(false, n, n, sa.dev, sa.ld, sp.dev, hb::DeviceInfo());
+  const int finfo = hb::ReadInfo();
+  if (finfo == 0 && nrhs > 0) hb::ZGetrs<R>(0, n, nrhs, sa.dev, sa.ld, sp.dev, sb.dev, sb.ld);
+  sa.Out();
+  sp.Out();
+  if (finfo == 0) sb.Out();
+  *info = finfo;
+  hb::Finish(name);
+}
+
 // WORK(1) := v in the caller's array (host or device).
 template <typename T>
 static void StoreWork0(T* work, T v) {
@@ -1322,6 +1462,36 @@ HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* ldb, hwyblas_int* info) {
   GesvEntry<float>("SGESV", n, nrhs, a, lda, ipiv, b, ldb, info);
 }
+
+// Complex LU (src/lapack/getrf.cc:548-549).
+#define HB_ZLU(P, U, R)                                                                   \
+  HWYBLAS_API void P##getrf_(const hwyblas_int* m, const hwyblas_int* n, R* a,            \
+                             const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info) { \
+    ZGetrfEntry<R>(false, U "GETRF", m, n, a, lda, ipiv, info);                          \
+  }                                                                                       \
+  HWYBLAS_API void P##getrf2_(const hwyblas_int* m, const hwyblas_int* n, R* a,           \
+                              const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info) { \
+    ZGetrfEntry<R>(true, U "GETRF2", m, n, a, lda, ipiv, info);                          \
+  }                                                                                       \
+  HWYBLAS_API void P##laswp_(const hwyblas_int* n, R* a, const hwyblas_int* lda,          \
+                             const hwyblas_int* k1, const hwyblas_int* k2,                \
+                             const hwyblas_int* ipiv, const hwyblas_int* incx) {          \
+    ZLaswpEntry<R>(U "LASWP", n, a, lda, k1, k2, ipiv, incx);                            \
+  }                                                                                       \
+  HWYBLAS_API void P##getrs_(const char* trans, const hwyblas_int* n,                     \
+                             const hwyblas_int* nrhs, const R* a, const hwyblas_int* lda, \
+                             const hwyblas_int* ipiv, R* b, const hwyblas_int* ldb,       \
+                             hwyblas_int* info) {                                         \
+    ZGetrsEntry<R>(U "GETRS", trans, n, nrhs, a, lda, ipiv, b, ldb, info);               \
+  }                                                                                       \
+  HWYBLAS_API void P##gesv_(const hwyblas_int* n, const hwyblas_int* nrhs, R* a,          \
+                            const hwyblas_int* lda, hwyblas_int* ipiv, R* b,              \
+                            const hwyblas_int* ldb, hwyblas_int* info) {                  \
+    ZGesvEntry<R>(U "GESV", n, nrhs, a, lda, ipiv, b, ldb, info);                        \
+  }
+HB_ZLU(z, "Z", double)
+HB_ZLU(c, "C", float)
+#undef HB_ZLU
 
 #define HB_GERFS(P, U, T)                                                                 \
   HWYBLAS_API void P##gerfs_(const char* trans, const hwyblas_int* n,                     \

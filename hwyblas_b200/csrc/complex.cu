@@ -21,9 +21,11 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
+#include <cstdio>
 
 #include "device.cuh"
 #include "internal.h"
+#include "ref_order.cuh"
 
 namespace hb {
 namespace {
@@ -239,16 +241,17 @@ __global__ void ZScaleKernel(int m, int n, R beta_re, R beta_im, R* c, long long
   }
 }
 
-// 1 / (c + i d) as the C++ runtime's complex quotient: for double, Smith's
-// method with its scalings for very large and very small magnitudes and its
-// alternative when the ratio is subnormal; for float, the textbook quotient
-// (a c + b d, b c - a d) / (c^2 + d^2) in double precision, rounded. (Checked
-// against the host compiler's complex division on random quotients spanning
-// 2^-60..2^60, zero parts included; non-finite inputs are not reproduced.)
+// (a + i b) / (c + i d) as the C++ runtime's complex quotient: for double,
+// Smith's method with its scalings for very large and very small magnitudes
+// and its alternative when the ratio is subnormal; for float, the textbook
+// quotient (a c + b d, b c - a d) / (c^2 + d^2) in double precision, rounded.
+// (Checked against the host compiler's complex division on random quotients
+// spanning 2^-60..2^60, zero parts included; non-finite inputs are not
+// reproduced.)
 template <typename R>
-__device__ __forceinline__ void ZRecip(R cr, R ci, R* xr, R* xi) {
+__device__ __forceinline__ void ZDiv(R ar, R ai, R cr, R ci, R* xr, R* xi) {
   if constexpr (sizeof(R) == 8) {
-    double a = 1.0, b = 0.0, c = cr, d = ci;
+    double a = ar, b = ai, c = cr, d = ci;
     const double kBig = DBL_MAX / 2, kMin = DBL_MIN, kEps = DBL_EPSILON;
     const double kScale = 1.0 / kEps, kMax2 = kBig * kEps;
     double x, y;
@@ -294,14 +297,19 @@ __device__ __forceinline__ void ZRecip(R cr, R ci, R* xr, R* xi) {
     *xr = x;
     *xi = y;
   } else {
-    const double c = cr, d = ci;
+    const double a = ar, b = ai, c = cr, d = ci;
     const double den = __dadd_rn(__dmul_rn(c, c), __dmul_rn(d, d));
-    // a = 1, b = 0: (a c + b d) and (b c - a d) keep their signed zeros.
-    const double re = __dadd_rn(__dmul_rn(1.0, c), __dmul_rn(0.0, d));
-    const double im = __dsub_rn(__dmul_rn(0.0, c), __dmul_rn(1.0, d));
+    const double re = __dadd_rn(__dmul_rn(a, c), __dmul_rn(b, d));
+    const double im = __dsub_rn(__dmul_rn(b, c), __dmul_rn(a, d));
     *xr = static_cast<float>(re / den);
     *xi = static_cast<float>(im / den);
   }
+}
+
+// 1 / (c + i d): the quotient above with numerator (1, 0).
+template <typename R>
+__device__ __forceinline__ void ZRecip(R cr, R ci, R* xr, R* xi) {
+  ZDiv<R>(R(1), R(0), cr, ci, xr, xi);
 }
 
 // Complex TRSM base: X T = B for independent rows of X (src/trsm-inl.h:
@@ -396,6 +404,311 @@ __global__ void __launch_bounds__(128)
       const long long off = 2 * ((lower ? r - 1 - s : s) * xs_col);
       xr[off] = yr[s];
       xr[off + 1] = yi[s];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Complex LU leaf (src/lapack/factor_kernels.cc:107-139 for complex T).
+//
+// Per column j: the pivot is the first row of largest |re| + |im| (NaN
+// magnitudes never win; a NaN at row j keeps row j: src/level1-inl.h:
+// 343-411); the rows are interchanged across the leaf; the column below the
+// diagonal is multiplied by 1/pivot as (x.re r.re - x.im r.im, x.im r.re +
+// x.re r.im), or divided by the pivot when |pivot| (std::abs) is below the
+// safe minimum; then every later column k gets y += (-a(j, k)) x in the
+// reference's AXPY rounding (src/lapack/factor_kernels.cc:33-72):
+//   columns of fewer reals than one vector: p = alpha x as a complex product
+//   (ar xr - ai xi, ar xi + ai xr), then y + p;
+//   otherwise re: fma(xi, -ai, fma(xr, ar, yr)), im: fma(xr, ai, fma(xi, ar, yi)).
+//
+// The m x w panel (w <= 16) is split by rows over P CTAs holding their rows
+// in shared memory (a cooperative launch when P > 1); per column each CTA
+// publishes its best candidate and one global exchange picks the pivot, as
+// in the real leaf.
+constexpr int kZLeafThreads = 512;
+constexpr int kZLeafW = 16;
+constexpr int kZLeafMaxRows = 512;  // rows per CTA
+constexpr int kZLeafMaxP = 64;      // CTAs per panel (m <= 32768)
+constexpr int kZSlot = 2 + 4 * kZLeafW;  // reals: |a|, row, candidate row, row j
+
+template <typename R>
+struct ZLeafArgs {
+  int m, w, lanes;
+  R* a;            // interleaved (re, im)
+  long long lda;   // complex elements
+  int* ipiv;
+  int* info;
+  int info_base;
+  R* xchg;               // [2][P][kZSlot]
+  unsigned int* tags;    // [2][P], zeroed before a cooperative launch
+  int* timeout_flag;
+};
+
+template <typename R>
+__device__ __forceinline__ R ZMag(R re, R im) {
+  return Add(fabs(re), fabs(im));
+}
+
+template <typename R>
+__device__ __forceinline__ bool ZBetter(R v, int i, R bv, int bi) {
+  return v > bv || (v == bv && v >= R(0) && i < bi);
+}
+
+// std::abs(z) >= s for the safe minimum s. |z| is at least the larger part,
+// so only two parts below s need the magnitude itself: they are scaled by an
+// exact power of two (double) or widened (float) and the square root of the
+// sum of squares is compared in double precision. (std::abs is hypot: an
+// infinite part gives infinity, otherwise a NaN part gives NaN.)
+template <typename R>
+__device__ __forceinline__ bool ZAbsAtLeast(R re, R im, R s) {
+  const R ar = fabs(re), ai = fabs(im);
+  if (isinf(ar) || isinf(ai)) return true;
+  if (isnan(ar) || isnan(ai)) return false;
+  if ((ar > ai ? ar : ai) >= s) return true;
+  const double k = sizeof(R) == 8 ? 0x1p600 : 1.0;
+  const double sr = __dmul_rn(static_cast<double>(ar), k);
+  const double si = __dmul_rn(static_cast<double>(ai), k);
+  const double mag = sqrt(__dadd_rn(__dmul_rn(sr, sr), __dmul_rn(si, si)));
+  return mag >= __dmul_rn(static_cast<double>(s), k);
+}
+
+// y += alpha x for one element of a column of len complex elements.
+template <typename R>
+__device__ __forceinline__ void ZAxpyRef(R& yr, R& yi, R ar, R ai, R xr, R xi, int len,
+                                         int lanes) {
+  if (2 * len < lanes) {
+    const R pr = Sub(Mul(ar, xr), Mul(ai, xi));
+    const R pi = Add(Mul(ar, xi), Mul(ai, xr));
+    yr = Add(yr, pr);
+    yi = Add(yi, pi);
+  } else {
+    const R tr = Fma(xr, ar, yr), ti = Fma(xi, ar, yi);
+    yr = Fma(xi, -ai, tr);
+    yi = Fma(xr, ai, ti);
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p) {
+  constexpr int W = kZLeafW;
+  extern __shared__ __align__(16) unsigned char zleaf_smem[];
+  R* sp = reinterpret_cast<R*>(zleaf_smem);  // [w][rows][2]
+  __shared__ R s_piv[2 * W], s_rowj[2 * W];
+  __shared__ R s_cand[kZLeafMaxP * kZSlot];
+  __shared__ R s_wv[kZLeafThreads / 32];
+  __shared__ int s_wi[kZLeafThreads / 32];
+  __shared__ int s_p, s_abort;
+  const int P = gridDim.x, cta = blockIdx.x;
+  const int rows_per = (p.m + P - 1) / P;
+  const int r0 = cta * rows_per, r1 = min(p.m, r0 + rows_per);
+  const int RW = rows_per;
+  const int w = p.w;
+  const auto el = [&](int c, int lr) -> R* { return sp + 2 * (c * RW + lr); };
+
+  if (threadIdx.x == 0) s_abort = 0;
+  for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+    const R* src = p.a + 2 * (r0 + lr);
+    R v[2 * W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      if (c < w) {
+        v[2 * c] = src[2 * c * p.lda];
+        v[2 * c + 1] = src[2 * c * p.lda + 1];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+      if (c < w) {
+        el(c, lr)[0] = v[2 * c];
+        el(c, lr)[1] = v[2 * c + 1];
+      }
+    }
+  }
+  __syncthreads();
+
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    // (a) local candidate over rows >= j.
+    R bv = R(-1);
+    int bi = 0x7fffffff;
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+      const int gi = r0 + lr;
+      if (gi < j) continue;
+      const R v = ZMag(el(j, lr)[0], el(j, lr)[1]);
+      if (v > bv) { bv = v; bi = gi; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const R ov = __shfl_down_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ZBetter(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    }
+    if (threadIdx.x % 32 == 0) { s_wv[threadIdx.x / 32] = bv; s_wi[threadIdx.x / 32] = bi; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      bv = threadIdx.x < kZLeafThreads / 32 ? s_wv[threadIdx.x] : R(-1);
+      bi = threadIdx.x < kZLeafThreads / 32 ? s_wi[threadIdx.x] : 0x7fffffff;
+      for (int off = 16; off > 0; off >>= 1) {
+        const R ov = __shfl_down_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (ZBetter(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+      }
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        s_p = bi;
+        s_wv[0] = bv;
+      }
+    }
+    __syncthreads();
+    // (b) exchange: slot = (|a|, row, candidate row, row j if owned).
+    const int ci = s_p;
+    R* slot = P == 1 ? s_cand : p.xchg + (par * P + cta) * kZSlot;
+    if (threadIdx.x == 0) {
+      slot[0] = s_wv[0];
+      slot[1] = static_cast<R>(ci == 0x7fffffff ? -1 : ci);
+    }
+    if (threadIdx.x < 2 * w) {
+      const int c = threadIdx.x >> 1, part = threadIdx.x & 1;
+      slot[2 + threadIdx.x] = (ci != 0x7fffffff) ? el(c, ci - r0)[part] : R(0);
+      if (j >= r0 && j < r1) slot[2 + 2 * W + threadIdx.x] = el(c, j - r0)[part];
+    }
+    if (P > 1) {
+      // Release the slot under the step's tag; poll the P tags (bounded) and
+      // copy every slot. A parity is rewritten two steps later, after every
+      // CTA has published the next step and so has read this one.
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p.tags + par * P + cta),
+                     "r"(static_cast<unsigned>(j + 1))
+                     : "memory");
+      }
+      if (threadIdx.x < P) {
+        uint32_t polls = 0;
+        while (true) {
+          unsigned v;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];"
+                       : "=r"(v)
+                       : "l"(p.tags + par * P + threadIdx.x)
+                       : "memory");
+          if (v >= static_cast<unsigned>(j + 1)) break;
+          if (++polls >= kMaxPolls) {
+            atomicExch(p.timeout_flag, 1);
+            s_abort = 1;
+            break;
+          }
+        }
+      }
+      __syncthreads();
+      if (s_abort) return;
+      for (int idx = threadIdx.x; idx < P * kZSlot; idx += blockDim.x)
+        s_cand[idx] = *(volatile const R*)&p.xchg[par * P * kZSlot + idx];
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * w)
+      s_rowj[threadIdx.x] = s_cand[(j / rows_per) * kZSlot + 2 + 2 * W + threadIdx.x];
+    __syncthreads();
+    // (c) the pivot among the candidates; warp 0 fills the pivot row.
+    if (threadIdx.x < 32) {
+      R gv = R(-1);
+      int gi = 0x7fffffff, wq = -1;
+      for (int q = threadIdx.x; q < P; q += 32) {
+        const R fi = s_cand[q * kZSlot + 1];
+        if (fi < R(0)) continue;
+        const R v = s_cand[q * kZSlot];
+        const int i = static_cast<int>(fi);
+        if (ZBetter(v, i, gv, gi)) { gv = v; gi = i; wq = q; }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const R ov = __shfl_down_sync(0xffffffffu, gv, off);
+        const int oi = __shfl_down_sync(0xffffffffu, gi, off);
+        const int oq = __shfl_down_sync(0xffffffffu, wq, off);
+        if (ZBetter(ov, oi, gv, gi)) { gv = ov; gi = oi; wq = oq; }
+      }
+      gi = __shfl_sync(0xffffffffu, gi, 0);
+      wq = __shfl_sync(0xffffffffu, wq, 0);
+      if (isnan(ZMag(s_rowj[2 * j], s_rowj[2 * j + 1])) || gi == 0x7fffffff) gi = j;
+      if (threadIdx.x == 0) s_p = gi;
+      if (threadIdx.x < 2 * w)
+        s_piv[threadIdx.x] = (gi == j) ? s_rowj[threadIdx.x]
+                                       : s_cand[wq * kZSlot + 2 + threadIdx.x];
+    }
+    __syncthreads();
+    const int piv = s_p;
+    const R pr = s_piv[2 * j], pi = s_piv[2 * j + 1];
+    const bool nonzero = pr != R(0) || pi != R(0);
+    if (cta == 0 && threadIdx.x == 0) {
+      p.ipiv[j] = piv + 1;
+      if (!nonzero && *p.info == 0) *p.info = p.info_base + j + 1;
+    }
+    // (d) interchange rows j and piv across the leaf's columns.
+    if (nonzero && piv != j && threadIdx.x < 2 * w) {
+      const int c = threadIdx.x >> 1, part = threadIdx.x & 1;
+      if (piv >= r0 && piv < r1) el(c, piv - r0)[part] = s_rowj[threadIdx.x];
+      if (j >= r0 && j < r1) el(c, j - r0)[part] = s_piv[threadIdx.x];
+    }
+    __syncthreads();
+    // (e) scale column j below the diagonal; (f) update columns j+1..w-1.
+    const bool tiny = !ZAbsAtLeast(pr, pi, Sfmin<R>());
+    R vr = R(0), vi = R(0);
+    if (nonzero && !tiny) ZRecip<R>(pr, pi, &vr, &vi);
+    const int len = p.m - j - 1;
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+      if (r0 + lr <= j) continue;
+      R xr = el(j, lr)[0], xi = el(j, lr)[1];
+      if (nonzero) {
+        if (tiny) {
+          ZDiv<R>(xr, xi, pr, pi, &xr, &xi);
+        } else {
+          const R nr = Sub(Mul(xr, vr), Mul(xi, vi));
+          const R ni = Add(Mul(xi, vr), Mul(xr, vi));
+          xr = nr;
+          xi = ni;
+        }
+        el(j, lr)[0] = xr;
+        el(j, lr)[1] = xi;
+      }
+      for (int k = j + 1; k < w; ++k) {
+        R* y = el(k, lr);
+        ZAxpyRef<R>(y[0], y[1], -s_piv[2 * k], -s_piv[2 * k + 1], xr, xi, len, p.lanes);
+      }
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < w; ++c) {
+    for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
+      R* dst = p.a + 2 * ((r0 + lr) + c * p.lda);
+      dst[0] = el(c, lr)[0];
+      dst[1] = el(c, lr)[1];
+    }
+  }
+}
+
+// Complex LU leaf, trailing columns (n > m, m <= 16): all interchanges, then
+// the updates with the final multipliers (the same arithmetic as the
+// reference's interleaved order, as in the real leaf). One thread per column.
+template <typename R>
+__global__ void ZGetrfLeafTrailingKernel(int m, int w, int n, R* a, long long lda,
+                                         const int* ipiv, int lanes) {
+  const int k = w + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  R* col = a + 2 * k * lda;
+  for (int j = 0; j < w; ++j) {
+    const int q = ipiv[j] - 1;
+    if (q != j) {
+      const R tr = col[2 * j], ti = col[2 * j + 1];
+      col[2 * j] = col[2 * q];
+      col[2 * j + 1] = col[2 * q + 1];
+      col[2 * q] = tr;
+      col[2 * q + 1] = ti;
+    }
+  }
+  for (int j = 0; j < w; ++j) {
+    const R ar = -col[2 * j], ai = -col[2 * j + 1];
+    const int len = m - j - 1;
+    for (int i = j + 1; i < m; ++i) {
+      const R* x = a + 2 * (i + j * lda);
+      ZAxpyRef<R>(col[2 * i], col[2 * i + 1], ar, ai, x[0], x[1], len, lanes);
     }
   }
 }
@@ -599,5 +912,142 @@ template void ZgemmFull<double>(int, int, int, int, int, const double*, const do
                                 const double*, int, const double*, double*, int);
 template void ZgemmFull<float>(int, int, int, int, int, const float*, const float*, int,
                                const float*, int, const float*, float*, int);
+
+// ---------------------------------------------------------------------------
+// Complex LU drivers: the reference's Getrf2 recursion and blocked Getrf
+// (src/lapack/getrf.cc:112-280, nb = 64 from src/lapack/environment.cc:86-88)
+// and Getrs (287-339), call for call, on the complex TRSM and GEMM above.
+
+template <typename R>
+void ZLaswp(int n, R* a, int lda, int k1, int k2, const int* ipiv, int incx) {
+  Laswp<ZPair<R>>(n, reinterpret_cast<ZPair<R>*>(a), lda, k1, k2, ipiv, incx);
+}
+template void ZLaswp<double>(int, double*, int, int, int, const int*, int);
+template void ZLaswp<float>(int, float*, int, int, int, const int*, int);
+
+namespace {
+template <typename R>
+R* ZAt(R* a, int lda, int i, int j) {
+  return a + 2 * (i + static_cast<long long>(j) * lda);
+}
+
+template <typename R>
+void ZGetrfLeaf(int m, int n, R* a, int lda, int* ipiv, int* info, int info_base) {
+  Context& ctx = Ctx();
+  const int w = std::min(m, n);
+  const int lanes = sizeof(R) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  const int P = (m + kZLeafMaxRows - 1) / kZLeafMaxRows;
+  if (P > kZLeafMaxP) {
+    fprintf(stderr, "hwyblas_b200: complex LU panel of %d rows exceeds the leaf's limit\n", m);
+    Failed(cudaErrorInvalidValue, "complex getrf leaf size");
+    return;
+  }
+  const int rows = (m + P - 1) / P;
+  const size_t smem = 2 * sizeof(R) * static_cast<size_t>(w) * rows;
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(ZGetrfLeafKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(2 * sizeof(R) * kZLeafW * kZLeafMaxRows));
+    configured = true;
+  }
+  ZLeafArgs<R> args;
+  args.m = m;
+  args.w = w;
+  args.lanes = lanes;
+  args.a = a;
+  args.lda = lda;
+  args.ipiv = ipiv;
+  args.info = info;
+  args.info_base = info_base;
+  const size_t slot_bytes = sizeof(R) * 2 * kZLeafMaxP * kZSlot;
+  args.xchg = static_cast<R*>(
+      Workspace(kWsLeaf, slot_bytes + sizeof(unsigned int) * 2 * kZLeafMaxP));
+  if (args.xchg == nullptr) return;
+  args.tags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(args.xchg) + slot_bytes);
+  args.timeout_flag = ctx.dev_status;
+  if (P > 1) {
+    cudaMemsetAsync(args.tags, 0, sizeof(unsigned int) * 2 * P, ctx.stream);
+    void* kargs[] = {&args};
+    Failed(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(ZGetrfLeafKernel<R>), P,
+                                       kZLeafThreads, kargs, smem, ctx.stream),
+           "complex getrf leaf (cooperative)");
+  } else {
+    ZGetrfLeafKernel<R><<<1, kZLeafThreads, smem, ctx.stream>>>(args);
+  }
+  CountLaunch();
+  LaunchFailed("complex getrf leaf");
+  if (n > w) {
+    ZGetrfLeafTrailingKernel<R><<<(n - w + 127) / 128, 128, 0, ctx.stream>>>(
+        m, w, n, a, lda, ipiv, lanes);
+    CountLaunch();
+    LaunchFailed("complex getrf leaf trailing");
+  }
+}
+
+template <typename R>
+void ZGetrfRec(int m, int n, R* a, int lda, int* ipiv, int* info, int col0) {
+  if (m == 0 || n == 0) return;
+  if (std::min(m, n) <= 16) {
+    ZGetrfLeaf<R>(m, n, a, lda, ipiv, info, col0);
+    return;
+  }
+  const R one[2] = {R(1), R(0)}, m1[2] = {R(-1), R(0)};
+  const int n1 = std::min(m, n) / 2, n2 = n - n1;
+  ZGetrfRec<R>(m, n1, a, lda, ipiv, info, col0);
+  ZLaswp<R>(n2, ZAt(a, lda, 0, n1), lda, 1, n1, ipiv, 1);
+  ZtrsmFull<R>(true, true, 0, true, n1, n2, one, a, lda, ZAt(a, lda, 0, n1), lda);
+  ZgemmFull<R>(0, 0, m - n1, n2, n1, m1, ZAt(a, lda, n1, 0), lda, ZAt(a, lda, 0, n1), lda,
+               one, ZAt(a, lda, n1, n1), lda);
+  ZGetrfRec<R>(m - n1, n2, ZAt(a, lda, n1, n1), lda, ipiv + n1, info, col0 + n1);
+  AdjustPivots(ipiv, n1, std::min(m, n), n1);
+  ZLaswp<R>(n1, a, lda, n1 + 1, std::min(m, n), ipiv, 1);
+}
+}  // namespace
+
+template <typename R>
+void ZGetrf(bool recursive, int m, int n, R* a, int lda, int* ipiv, int* info) {
+  if (m == 0 || n == 0) return;
+  const int nb = 64, mn = std::min(m, n);
+  if (recursive || nb >= mn) {
+    ZGetrfRec<R>(m, n, a, lda, ipiv, info, 0);
+    return;
+  }
+  const R one[2] = {R(1), R(0)}, m1[2] = {R(-1), R(0)};
+  for (int j = 0; j < mn; j += nb) {
+    const int jb = std::min(mn - j, nb);
+    ZGetrfRec<R>(m - j, jb, ZAt(a, lda, j, j), lda, ipiv + j, info, j);
+    AdjustPivots(ipiv, j, std::min(m, j + jb), j);
+    ZLaswp<R>(j, a, lda, j + 1, j + jb, ipiv, 1);
+    if (j + jb < n) {
+      ZLaswp<R>(n - j - jb, ZAt(a, lda, 0, j + jb), lda, j + 1, j + jb, ipiv, 1);
+      ZtrsmFull<R>(true, true, 0, true, jb, n - j - jb, one, ZAt(a, lda, j, j), lda,
+                   ZAt(a, lda, j, j + jb), lda);
+      if (j + jb < m) {
+        ZgemmFull<R>(0, 0, m - j - jb, n - j - jb, jb, m1, ZAt(a, lda, j + jb, j), lda,
+                     ZAt(a, lda, j, j + jb), lda, one, ZAt(a, lda, j + jb, j + jb), lda);
+      }
+    }
+  }
+}
+template void ZGetrf<double>(bool, int, int, double*, int, int*, int*);
+template void ZGetrf<float>(bool, int, int, float*, int, int*, int*);
+
+template <typename R>
+void ZGetrs(int op, int n, int nrhs, const R* a, int lda, const int* ipiv, R* b, int ldb) {
+  if (n == 0 || nrhs == 0) return;
+  const R one[2] = {R(1), R(0)};
+  if (op == 0) {
+    ZLaswp<R>(nrhs, b, ldb, 1, n, ipiv, 1);
+    ZtrsmFull<R>(true, true, 0, true, n, nrhs, one, a, lda, b, ldb);
+    ZtrsmFull<R>(true, false, 0, false, n, nrhs, one, a, lda, b, ldb);
+  } else {
+    ZtrsmFull<R>(true, false, op, false, n, nrhs, one, a, lda, b, ldb);
+    ZtrsmFull<R>(true, true, op, true, n, nrhs, one, a, lda, b, ldb);
+    ZLaswp<R>(nrhs, b, ldb, 1, n, ipiv, -1);
+  }
+}
+template void ZGetrs<double>(int, int, int, const double*, int, const int*, double*, int);
+template void ZGetrs<float>(int, int, int, const float*, int, const int*, float*, int);
+
 
 }  // namespace hb

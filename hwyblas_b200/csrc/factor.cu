@@ -707,6 +707,8 @@ void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx) {
 }
 template void Laswp<double>(int, double*, int, int, int, const int*, int);
 template void Laswp<float>(int, float*, int, int, int, const int*, int);
+template void Laswp<ZPair<double>>(int, ZPair<double>*, int, int, int, const int*, int);
+template void Laswp<ZPair<float>>(int, ZPair<float>*, int, int, int, const int*, int);
 
 void AdjustPivots(int* ipiv, int begin, int end, int delta) {
   if (end <= begin || delta == 0) return;

@@ -95,7 +95,9 @@ enum WorkspaceSlot : int {
   kWsGerfsWork = 27,   // host-pointer staging of GERFS's WORK and IWORK
   kWsGerfsIwork = 28,
   kWsSplitK = 29,      // per-chunk accumulators of a split DMMA GEMM
-  kNumWorkspaceSlots = 30
+  kWsZFactor = 30,     // aligned copy of a complex matrix being factored
+  kWsZFactorB = 31,    // aligned copy of the right-hand sides of its solve
+  kNumWorkspaceSlots = 32
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -146,6 +148,14 @@ void TrsmSolve(bool left, View<T> tri, bool lower, bool unit, int r,
 // Device IAMAX: writes the 1-based index to *out (device int).
 template <typename T>
 void Iamax(int n, const T* x, int incx, int* out);
+// A complex element as its two parts, aligned as one part: row interchanges
+// move it whole (Laswp<ZPair<R>>).
+template <typename R>
+struct ZPair {
+  R re, im;
+};
+// Lanes of the reference's SIMD vectors of doubles (8 for AVX-512).
+int RefLanesDouble();
 // LASWP on device data; ipiv is a device array (1-based, Fortran k1/k2/incx).
 template <typename T>
 void Laswp(int n, T* a, int lda, int k1, int k2, const int* ipiv, int incx);
@@ -225,6 +235,17 @@ void ZgemmFull(int ta, int tb, int m, int n, int k, const R* alpha, const R* a, 
 template <typename R>
 void ZtrsmFull(bool left, bool lower, int op, bool unit, int m, int n, const R* alpha,
                const R* a, int lda, R* b, int ldb);
+// Complex LU (src/lapack/getrf.cc:112-280) on device data with leading
+// dimension lda in complex elements; ipiv and *info on the device (INFO as
+// for Getrf). recursive: xGETRF2 instead of the blocked xGETRF.
+template <typename R>
+void ZGetrf(bool recursive, int m, int n, R* a, int lda, int* ipiv, int* info);
+// Complex LU solve (src/lapack/getrf.cc:287-339), op 0 N / 1 T / 2 C.
+template <typename R>
+void ZGetrs(int op, int n, int nrhs, const R* a, int lda, const int* ipiv, R* b, int ldb);
+// Complex LASWP on device data (src/lapack/getrf.cc:28-81).
+template <typename R>
+void ZLaswp(int n, R* a, int lda, int k1, int k2, const int* ipiv, int incx);
 template <typename T>
 void GemmtrFull(bool lower, bool ta, bool tb, int n, int k, T alpha, const T* a, int lda,
                 const T* b, int ldb, T beta, T* c, int ldc);

@@ -230,6 +230,38 @@ HWYBLAS_API void sgetrs_(const char* trans, const hwyblas_int* n,
 HWYBLAS_API void sgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
                         const hwyblas_int* ldb, hwyblas_int* info);
+/* Complex LU family (src/lapack/getrf.cc:548-549, the same templates at
+ * c64 and c32): interleaved (re, im) arrays, leading dimensions in complex
+ * elements. Pivots are the first largest |re| + |im|; 1/pivot and the tiny-
+ * pivot quotient are the C++ runtime's complex division. */
+HWYBLAS_API void zgetrf_(const hwyblas_int* m, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info);
+HWYBLAS_API void zgetrf2_(const hwyblas_int* m, const hwyblas_int* n, double* a,
+                          const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info);
+HWYBLAS_API void zlaswp_(const hwyblas_int* n, double* a, const hwyblas_int* lda,
+                         const hwyblas_int* k1, const hwyblas_int* k2,
+                         const hwyblas_int* ipiv, const hwyblas_int* incx);
+HWYBLAS_API void zgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const double* a, const hwyblas_int* lda,
+                         const hwyblas_int* ipiv, double* b, const hwyblas_int* ldb,
+                         hwyblas_int* info);
+HWYBLAS_API void zgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, double* a,
+                        const hwyblas_int* lda, hwyblas_int* ipiv, double* b,
+                        const hwyblas_int* ldb, hwyblas_int* info);
+HWYBLAS_API void cgetrf_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info);
+HWYBLAS_API void cgetrf2_(const hwyblas_int* m, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* ipiv, hwyblas_int* info);
+HWYBLAS_API void claswp_(const hwyblas_int* n, float* a, const hwyblas_int* lda,
+                         const hwyblas_int* k1, const hwyblas_int* k2,
+                         const hwyblas_int* ipiv, const hwyblas_int* incx);
+HWYBLAS_API void cgetrs_(const char* trans, const hwyblas_int* n,
+                         const hwyblas_int* nrhs, const float* a, const hwyblas_int* lda,
+                         const hwyblas_int* ipiv, float* b, const hwyblas_int* ldb,
+                         hwyblas_int* info);
+HWYBLAS_API void cgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
+                        const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
+                        const hwyblas_int* ldb, hwyblas_int* info);
 /* Inverse from the LU factorization: inv(U) by ?trtri, then inv(A) L =
  * inv(U) in block columns of 64 (lwork >= 64 n; narrower blocks for a
  * smaller lwork, column by column below 2 n), then the column interchanges.

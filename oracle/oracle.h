@@ -83,6 +83,19 @@ int orc_ctrsm(char side, char uplo, char ta, char diag, int m, int n, const floa
               const float* a, int lda, float* b, int ldb);
 void orc_zrecip(int n, const double* c, double* out);
 void orc_crecip(int n, const float* c, float* out);
+/* Complex LU family (src/lapack/getrf.cc:28-374 at std::complex). */
+int orc_zgetrf(int m, int n, double* a, int lda, int* ipiv);
+int orc_zgetrf2(int m, int n, double* a, int lda, int* ipiv);
+void orc_zlaswp(int n, double* a, int lda, int k1, int k2, const int* ipiv, int incx);
+int orc_zgetrs(char trans, int n, int nrhs, const double* a, int lda, const int* ipiv,
+               double* b, int ldb);
+int orc_zgesv(int n, int nrhs, double* a, int lda, int* ipiv, double* b, int ldb);
+int orc_cgetrf(int m, int n, float* a, int lda, int* ipiv);
+int orc_cgetrf2(int m, int n, float* a, int lda, int* ipiv);
+void orc_claswp(int n, float* a, int lda, int k1, int k2, const int* ipiv, int incx);
+int orc_cgetrs(char trans, int n, int nrhs, const float* a, int lda, const int* ipiv,
+               float* b, int ldb);
+int orc_cgesv(int n, int nrhs, float* a, int lda, int* ipiv, float* b, int ldb);
 /* Level 3 through the GEMM problem model (src/level3.cc:26-342). */
 int orc_dsymm(char side, char uplo, int m, int n, double alpha, const double* a, int lda,
               const double* b, int ldb, double beta, double* c, int ldc);

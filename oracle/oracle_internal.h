@@ -42,6 +42,14 @@ int Syrk(char uplo, char trans, int n, int k, T alpha, const T* a, int lda, T be
          int ldc);
 template <typename T>
 int Iamax(int n, const T* x, int incx);
+// Complex GEMM and TRSM on interleaved (re, im) arrays, alpha and beta as
+// (re, im) pairs (oracle_blas.cc).
+template <typename R>
+int ZgemmF(char transa, char transb, int m, int n, int k, const R* alpha, const R* a, int lda,
+           const R* b, int ldb, const R* beta, R* c, int ldc);
+template <typename R>
+int ZtrsmF(char side, char uplo, char transa, char diag, int m, int n, const R* alpha,
+           const R* a, int lda, R* b, int ldb);
 template <typename T>
 int Trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
          int lda, T* b, int ldb);

@@ -9,6 +9,9 @@
 //   PotrfLeaf  src/lapack/factor_kernels.cc:187-221
 //   Laswp      src/lapack/getrf.cc:28-81
 //   Getrf2     src/lapack/getrf.cc:112-207 (leaf at min(m, n) <= 16)
+//              (the same templates at std::complex: the leaf's pivot is the
+//              first largest |re| + |im|, src/level1-inl.h:343-411, and its
+//              complex AXPY src/lapack/factor_kernels.cc:33-72)
 //   Getrf      src/lapack/getrf.cc:216-280 (nb = 64, src/lapack/environment.cc:86-88)
 //   Getrs/Gesv src/lapack/getrf.cc:287-374
 //   Potrf2     src/lapack/potrf.cc:48-119 (leaf at n <= 32)
@@ -17,7 +20,9 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <complex>
 #include <limits>
+#include <type_traits>
 #include <utility>
 
 #include "oracle.h"
@@ -50,20 +55,76 @@ static void AxpyColumn(size_t n, T alpha, const T* x, T* y) {
 }
 
 template <typename T>
+struct IsCplx : std::false_type {};
+template <typename R>
+struct IsCplx<std::complex<R>> : std::true_type {};
+template <typename T>
+struct RealOf {
+  using type = T;
+};
+template <typename R>
+struct RealOf<std::complex<R>> {
+  using type = R;
+};
+
+// y[0:n] += alpha * x[0:n] for complex elements (src/lapack/factor_kernels.cc:
+// 33-72): fewer reals than one vector, the complex product and sum of the
+// C++ runtime; otherwise per element re: fma(xi, -ai, fma(xr, ar, yr)),
+// im: fma(xr, ai, fma(xi, ar, yi)).
+template <typename R>
+static void AxpyColumn(size_t n, std::complex<R> alpha, const std::complex<R>* x,
+                       std::complex<R>* y) {
+  if (2 * n < LanesOf<R>()) {
+    for (size_t i = 0; i < n; ++i) y[i] += alpha * x[i];
+    return;
+  }
+  const R ar = alpha.real(), ai = alpha.imag();
+  for (size_t i = 0; i < n; ++i) {
+    const R xr = x[i].real(), xi = x[i].imag();
+    const R tr = std::fma(xr, ar, y[i].real()), ti = std::fma(xi, ar, y[i].imag());
+    y[i] = std::complex<R>(std::fma(xi, -ai, tr), std::fma(xr, ai, ti));
+  }
+}
+
+// 0-based index of the first element of largest |re| + |im| (NaNs never
+// win; a NaN first element is returned: src/level1-inl.h:343-411).
+template <typename R>
+static size_t ArgMaxMagnitude(size_t n, const std::complex<R>* x) {
+  const R first = std::fabs(x[0].real()) + std::fabs(x[0].imag());
+  if (std::isnan(first)) return 0;
+  R best = first;
+  size_t bi = 0;
+  for (size_t i = 1; i < n; ++i) {
+    const R v = std::fabs(x[i].real()) + std::fabs(x[i].imag());
+    if (v > best) {
+      best = v;
+      bi = i;
+    }
+  }
+  return bi;
+}
+
+template <typename T>
 int GetrfLeaf(int m_, int n_, T* a, int lda, int* ipiv) {
+  using R = typename RealOf<T>::type;
   const size_t m = m_, n = n_;
   const auto at = [&](size_t i, size_t j) -> T& { return a[i + j * lda]; };
-  const T sfmin = Sfmin<T>();
+  const R sfmin = Sfmin<R>();
   int info = 0;
   for (size_t j = 0; j < std::min(m, n); ++j) {
-    const size_t p = j + static_cast<size_t>(Iamax<T>(m - j, &at(j, j), 1) - 1);
+    size_t p;
+    if constexpr (IsCplx<T>::value) {
+      p = j + ArgMaxMagnitude<R>(m - j, &at(j, j));
+    } else {
+      p = j + static_cast<size_t>(Iamax<T>(m - j, &at(j, j), 1) - 1);
+    }
     ipiv[j] = static_cast<int>(p + 1);
     const T pivot = at(p, j);
     if (pivot != T(0)) {
       if (p != j) {
         for (size_t k = 0; k < n; ++k) std::swap(at(j, k), at(p, k));
       }
-      if (std::fabs(pivot) >= sfmin) {
+      if (std::abs(pivot) >= sfmin) {
         const T r = T(1) / pivot;
         for (size_t i = j + 1; i < m; ++i) at(i, j) = at(i, j) * r;
       } else {
@@ -108,6 +169,32 @@ int PotrfLeaf(bool upper, int n_, T* a, int lda) {
   return 0;
 }
 
+// TRSM and GEMM of the drivers: the restated real routines, or the complex
+// ones on interleaved (re, im) arrays.
+template <typename T>
+static int TrsmAny(char side, char uplo, char ta, char diag, int m, int n, T alpha, const T* a,
+                   int lda, T* b, int ldb) {
+  if constexpr (IsCplx<T>::value) {
+    using R = typename RealOf<T>::type;
+    return ZtrsmF<R>(side, uplo, ta, diag, m, n, reinterpret_cast<const R*>(&alpha),
+                     reinterpret_cast<const R*>(a), lda, reinterpret_cast<R*>(b), ldb);
+  } else {
+    return TrsmF<T>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+  }
+}
+template <typename T>
+static int GemmAny(char ta, char tb, int m, int n, int k, T alpha, const T* a, int lda,
+                   const T* b, int ldb, T beta, T* c, int ldc) {
+  if constexpr (IsCplx<T>::value) {
+    using R = typename RealOf<T>::type;
+    return ZgemmF<R>(ta, tb, m, n, k, reinterpret_cast<const R*>(&alpha),
+                     reinterpret_cast<const R*>(a), lda, reinterpret_cast<const R*>(b), ldb,
+                     reinterpret_cast<const R*>(&beta), reinterpret_cast<R*>(c), ldc);
+  } else {
+    return GemmF<T>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+  }
+}
+
 // Row interchanges, 1-based k1..k2 and ipiv (src/lapack/getrf.cc:28-81).
 // Blocking by columns does not change any column's result, so this applies
 // the interchanges column by column.
@@ -146,8 +233,8 @@ int Getrf2(int m, int n, T* a, int lda, int* ipiv) {
   int iinfo = Getrf2<T>(m, n1, a, lda, ipiv);
   if (info == 0 && iinfo > 0) info = iinfo;
   Laswp<T>(n2, A(0, n1), lda, 1, n1, ipiv, 1);
-  TrsmF<T>('L', 'L', 'N', 'U', n1, n2, T(1), a, lda, A(0, n1), lda);
-  GemmF<T>('N', 'N', m - n1, n2, n1, T(-1), A(n1, 0), lda, A(0, n1), lda, T(1),
+  TrsmAny<T>('L', 'L', 'N', 'U', n1, n2, T(1), a, lda, A(0, n1), lda);
+  GemmAny<T>('N', 'N', m - n1, n2, n1, T(-1), A(n1, 0), lda, A(0, n1), lda, T(1),
            A(n1, n1), lda);
   iinfo = Getrf2<T>(m - n1, n2, A(n1, n1), lda, ipiv + n1);
   if (info == 0 && iinfo > 0) info = iinfo + n1;
@@ -175,10 +262,10 @@ int Getrf(int m, int n, T* a, int lda, int* ipiv) {
     Laswp<T>(j, a, lda, j + 1, j + jb, ipiv, 1);
     if (j + jb < n) {
       Laswp<T>(n - j - jb, A(0, j + jb), lda, j + 1, j + jb, ipiv, 1);
-      TrsmF<T>('L', 'L', 'N', 'U', jb, n - j - jb, T(1), A(j, j), lda,
+      TrsmAny<T>('L', 'L', 'N', 'U', jb, n - j - jb, T(1), A(j, j), lda,
                A(j, j + jb), lda);
       if (j + jb < m) {
-        GemmF<T>('N', 'N', m - j - jb, n - j - jb, jb, T(-1), A(j + jb, j),
+        GemmAny<T>('N', 'N', m - j - jb, n - j - jb, jb, T(-1), A(j + jb, j),
                  lda, A(j, j + jb), lda, T(1), A(j + jb, j + jb), lda);
       }
     }
@@ -199,11 +286,11 @@ int Getrs(char trans, int n, int nrhs, const T* a, int lda, const int* ipiv,
   if (n == 0 || nrhs == 0) return 0;
   if (notran) {
     Laswp<T>(nrhs, b, ldb, 1, n, ipiv, 1);
-    TrsmF<T>('L', 'L', 'N', 'U', n, nrhs, T(1), a, lda, b, ldb);
-    TrsmF<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'L', 'N', 'U', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
   } else {
-    TrsmF<T>('L', 'U', t, 'N', n, nrhs, T(1), a, lda, b, ldb);
-    TrsmF<T>('L', 'L', t, 'U', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'U', t, 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'L', t, 'U', n, nrhs, T(1), a, lda, b, ldb);
     Laswp<T>(nrhs, b, ldb, 1, n, ipiv, -1);
   }
   return 0;
@@ -649,6 +736,8 @@ int PotrsD(char uplo, int n, int nrhs, const double* a, int lda, double* b, int 
 
 template int GetrfLeaf<double>(int, int, double*, int, int*);
 template int GetrfLeaf<float>(int, int, float*, int, int*);
+template int GetrfLeaf<std::complex<double>>(int, int, std::complex<double>*, int, int*);
+template int GetrfLeaf<std::complex<float>>(int, int, std::complex<float>*, int, int*);
 template int PotrfLeaf<double>(bool, int, double*, int);
 template int PotrfLeaf<float>(bool, int, float*, int);
 
@@ -777,6 +866,37 @@ int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
   if (info == 0) info = orc::PotrsD(uplo, n, nrhs, a, lda, b, ldb);
   return info;
 }
+/* The complex LU family: the same templates at std::complex (src/lapack/
+ * getrf.cc:548-549), interleaved (re, im) arrays. */
+#define ORC_ZLU(P, R)                                                                      \
+  int orc_##P##getrf(int m, int n, R* a, int lda, int* ipiv) {                            \
+    return orc::Getrf<std::complex<R>>(m, n, reinterpret_cast<std::complex<R>*>(a), lda, ipiv); \
+  }                                                                                        \
+  int orc_##P##getrf2(int m, int n, R* a, int lda, int* ipiv) {                           \
+    return orc::Getrf2<std::complex<R>>(m, n, reinterpret_cast<std::complex<R>*>(a), lda, ipiv); \
+  }                                                                                        \
+  void orc_##P##laswp(int n, R* a, int lda, int k1, int k2, const int* ipiv, int incx) {  \
+    orc::Laswp<std::complex<R>>(n, reinterpret_cast<std::complex<R>*>(a), lda, k1, k2, ipiv, \
+                                incx);                                                     \
+  }                                                                                        \
+  int orc_##P##getrs(char trans, int n, int nrhs, const R* a, int lda, const int* ipiv,   \
+                     R* b, int ldb) {                                                      \
+    return orc::Getrs<std::complex<R>>(trans, n, nrhs,                                     \
+                                       reinterpret_cast<const std::complex<R>*>(a), lda,   \
+                                       ipiv, reinterpret_cast<std::complex<R>*>(b), ldb);  \
+  }                                                                                        \
+  int orc_##P##gesv(int n, int nrhs, R* a, int lda, int* ipiv, R* b, int ldb) {           \
+    if (n < 0) return -1;                                                                  \
+    if (nrhs < 0) return -2;                                                               \
+    if (lda < std::max(1, n)) return -4;                                                   \
+    if (ldb < std::max(1, n)) return -7;                                                   \
+    int info = orc_##P##getrf(n, n, a, lda, ipiv);                                         \
+    if (info == 0) info = orc_##P##getrs('N', n, nrhs, a, lda, ipiv, b, ldb);              \
+    return info;                                                                           \
+  }
+ORC_ZLU(z, double)
+ORC_ZLU(c, float)
+#undef ORC_ZLU
 int orc_dgetrf_leaf(int m, int n, double* a, int lda, int* ipiv) {
   return orc::GetrfLeaf<double>(m, n, a, lda, ipiv);
 }

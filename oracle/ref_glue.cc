@@ -8,8 +8,9 @@
 // reference drivers to them lets the tests check the oracle's own LAPACK
 // restatement against the reference's driver code, bit for bit.
 //
-// Routines the checked path never reaches (complex types, norms and condition
-// estimates) abort; the Fortran ones are in ref_stubs.c. triangular.cc is
+// The complex LU leaf and the complex GEMM and TRSM come from the oracle as
+// well (zgetrf_ and cgetrf_ are checked). Routines the checked path never
+// reaches (complex Cholesky, norms and condition estimates) abort; the Fortran ones are in ref_stubs.c. triangular.cc is
 // built too, for xTRTRI and xTRTI2 under xGETRI, and gesvx.cc and trsen.cc
 // for xGERFS and its xLACN2.
 #include <complex>
@@ -39,11 +40,7 @@ void ReportError(const char* routine, blasint info) {
 namespace lapack {
 template <typename T>
 blasint GetrfLeaf(blasint m, blasint n, T* a, blasint lda, blasint* ipiv) {
-  if constexpr (std::is_floating_point_v<T>) {
-    return orc::GetrfLeaf<T>(m, n, a, lda, ipiv);
-  } else {
-    Unreached("complex GetrfLeaf");
-  }
+  return orc::GetrfLeaf<T>(m, n, a, lda, ipiv);
 }
 template <typename T>
 blasint PotrfLeaf(bool upper, blasint n, T* a, blasint lda) {
@@ -208,6 +205,23 @@ void ssyrk_(const char* u, const char* t, const blasint* n, const blasint* k,
   const int info = orc::Syrk<float>(*u, *t, *n, *k, *alpha, a, *lda, *beta, c, *ldc);
   if (info) hwyblas::ReportError("SSYRK", info);
 }
+#define ORC_ZL3(P, U, R)                                                                  \
+  void P##gemm_(const char* ta, const char* tb, const blasint* m, const blasint* n,        \
+                const blasint* k, const R* alpha, const R* a, const blasint* lda,          \
+                const R* b, const blasint* ldb, const R* beta, R* c, const blasint* ldc) { \
+    const int info =                                                                       \
+        orc::ZgemmF<R>(*ta, *tb, *m, *n, *k, alpha, a, *lda, b, *ldb, beta, c, *ldc);      \
+    if (info) hwyblas::ReportError(U "GEMM", info);                                        \
+  }                                                                                        \
+  void P##trsm_(const char* s, const char* u, const char* t, const char* d,                \
+                const blasint* m, const blasint* n, const R* alpha, const R* a,            \
+                const blasint* lda, R* b, const blasint* ldb) {                            \
+    const int info = orc::ZtrsmF<R>(*s, *u, *t, *d, *m, *n, alpha, a, *lda, b, *ldb);     \
+    if (info) hwyblas::ReportError(U "TRSM", info);                                        \
+  }
+ORC_ZL3(z, "Z", double)
+ORC_ZL3(c, "C", float)
+#undef ORC_ZL3
 blasint idamax_(const blasint* n, const double* x, const blasint* incx) {
   return orc::Iamax<double>(*n, x, *incx);
 }

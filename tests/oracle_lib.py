@@ -44,6 +44,11 @@ def load_ref():
     lib.sgesv_.argtypes = [P] * 8
     lib.spotrf_.argtypes = [P] * 5
     lib.spotrf2_.argtypes = [P] * 5
+    for pre in "zc":
+        getattr(lib, f"{pre}getrf_").argtypes = [P] * 6
+        getattr(lib, f"{pre}getrf2_").argtypes = [P] * 6
+        getattr(lib, f"{pre}getrs_").argtypes = [P] * 9
+        getattr(lib, f"{pre}gesv_").argtypes = [P] * 8
     for pre in "ds":
         getattr(lib, f"{pre}gerfs_").argtypes = [P] * 17
         getattr(lib, f"{pre}getri_").argtypes = [P] * 7
@@ -97,6 +102,12 @@ class Oracle:
         L.orc_zrecip.argtypes = [I, P, P]
         L.orc_crecip.argtypes = [I, P, P]
         L.orc_cgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
+        for pre in "zc":
+            getattr(L, f"orc_{pre}getrf").argtypes = [I, I, P, I, P]
+            getattr(L, f"orc_{pre}getrf2").argtypes = [I, I, P, I, P]
+            getattr(L, f"orc_{pre}laswp").argtypes = [I, P, I, I, I, P, I]
+            getattr(L, f"orc_{pre}getrs").argtypes = [CH, I, I, P, I, P, P, I]
+            getattr(L, f"orc_{pre}gesv").argtypes = [I, I, P, I, P, P, I]
         for pre in "ds":
             getattr(L, f"orc_{pre}gerfs").argtypes = [CH, I, I, P, I, P, I, P, P, I, P, I, P,
                                                        P, P, P]
@@ -235,6 +246,26 @@ class Oracle:
         return fn(_b(side), _b(uplo), _b(ta), _b(diag), m, n, al.ctypes.data, ptr(a), lda,
                   ptr(b), ldb)
 
+    # Complex LU family on complex128 / complex64 Fortran-order arrays (by dtype).
+    @staticmethod
+    def _zp(x):
+        return "z" if x.dtype == np.complex128 else "c"
+
+    def zgetrf(self, m, n, a, lda, ipiv, recursive=False):
+        fn = getattr(self.lib, f"orc_{self._zp(a)}{'getrf2' if recursive else 'getrf'}")
+        return fn(m, n, ptr(a), lda, ptr(ipiv))
+
+    def zlaswp(self, n, a, lda, k1, k2, ipiv, incx):
+        getattr(self.lib, f"orc_{self._zp(a)}laswp")(n, ptr(a), lda, k1, k2, ptr(ipiv), incx)
+
+    def zgetrs(self, trans, n, nrhs, a, lda, ipiv, b, ldb):
+        return getattr(self.lib, f"orc_{self._zp(a)}getrs")(_b(trans), n, nrhs, ptr(a), lda,
+                                                          ptr(ipiv), ptr(b), ldb)
+
+    def zgesv(self, n, nrhs, a, lda, ipiv, b, ldb):
+        return getattr(self.lib, f"orc_{self._zp(a)}gesv")(n, nrhs, ptr(a), lda, ptr(ipiv),
+                                                         ptr(b), ldb)
+
     def getri(self, n, a, lda, ipiv, work, lwork):
         p = "s" if a.dtype == np.float32 else "d"
         return getattr(self.lib, f"orc_{p}getri")(n, ptr(a), lda, ptr(ipiv), ptr(work), lwork)
@@ -256,6 +287,25 @@ def ref_call_getrf(lib, recursive, m, n, a, lda, ipiv):
         (lib.sgetrf2_ if recursive else lib.sgetrf_)(*args)
     else:
         (lib.dgetrf2_ if recursive else lib.dgetrf_)(*args)
+    return info.value
+
+
+def ref_call_zgetrf(lib, recursive, m, n, a, lda, ipiv):
+    """The reference driver's zgetrf_/cgetrf_ (and ...2_), by dtype."""
+    info = ctypes.c_int(0)
+    pre = "z" if a.dtype == np.complex128 else "c"
+    fn = getattr(lib, f"{pre}{'getrf2' if recursive else 'getrf'}_")
+    fn(ctypes.byref(ctypes.c_int(m)), ctypes.byref(ctypes.c_int(n)), ptr(a),
+       ctypes.byref(ctypes.c_int(lda)), ptr(ipiv), ctypes.byref(info))
+    return info.value
+
+
+def ref_call_zgetrs(lib, trans, n, nrhs, a, lda, ipiv, b, ldb):
+    info = ctypes.c_int(0)
+    pre = "z" if a.dtype == np.complex128 else "c"
+    I = lambda v: ctypes.byref(ctypes.c_int(v))  # noqa: E731
+    getattr(lib, f"{pre}getrs_")(ctypes.c_char_p(_b(trans)), I(n), I(nrhs), ptr(a), I(lda),
+                                 ptr(ipiv), ptr(b), I(ldb), ctypes.byref(info))
     return info.value
 
 
@@ -309,6 +359,12 @@ def ref_call_trtri(lib, unblocked, uplo, diag, n, a, lda):
     fn(ctypes.c_char_p(_b(uplo)), ctypes.c_char_p(_b(diag)), ctypes.byref(ctypes.c_int(n)),
        ptr(a), ctypes.byref(ctypes.c_int(lda)), ctypes.byref(info))
     return info.value
+
+
+def crand(rng, rows, cols, dtype=np.complex128):
+    """Column-major complex matrix with parts uniform in [-1, 1]."""
+    x = rng.uniform(-1.0, 1.0, (rows, cols)) + 1j * rng.uniform(-1.0, 1.0, (rows, cols))
+    return np.asfortranarray(x.astype(dtype))
 
 
 def rand(rng, rows, cols, dtype=np.float64):

@@ -212,3 +212,178 @@ def test_ztrsm_device_misaligned_and_cblas(hb, orc):
                       hb.CblasNonUnit, -1, n, al.ctypes.data, arow.ctypes.data, m,
                       brow.ctypes.data, n)
     assert cap.errors == [("ZTRSM", 1), ("CTRSM", 9), ("cblas_ztrsm", 6)]
+
+
+# --------------------------------------------------------------------------
+# Complex LU family (zgetrf_, cgetrf_, ...2_, ?laswp_, ?getrs_, ?gesv_)
+# against the oracle's restatement of the reference's drivers and leaf, bit
+# for bit: shapes around the leaf (16) and the block (64), panels split over
+# several CTAs (m > 512), padding, both recursions.
+
+ZLU_SHAPES = [(1, 1), (1, 6), (6, 1), (3, 7), (16, 40), (40, 16), (17, 17), (33, 17),
+              (17, 33), (64, 64), (65, 70), (90, 150), (150, 90), (200, 200), (513, 300),
+              (1100, 260)]
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("m,n", ZLU_SHAPES)
+def test_zgetrf_bitexact(hb, orc, p, recursive, m, n):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(m * 31 + n)
+    lda = m + 3
+    a = crand(rng, lda, n, dtype)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1 = np.zeros(min(m, n), np.int32)
+    p2 = np.zeros(min(m, n), np.int32)
+    i1 = hb.zgetrf(p, m, n, a1, lda, p1, recursive=recursive)
+    i2 = orc.zgetrf(m, n, a2, lda, p2, recursive=recursive)
+    assert i1 == i2 == 0
+    assert np.array_equal(p1, p2)
+    assert same_bits(creal(a1), creal(a2))
+    assert np.array_equal(a1[m:, :], a[m:, :])
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("k", [1, 9, 17, 30])
+def test_zgetrf_singular_info(hb, orc, p, recursive, k):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(100 + k)
+    m, n = 40, 30
+    a = crand(rng, m, n, dtype)
+    a[:, k - 1] = 0
+    if k < n:
+        a[:, n - 1] = 0
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1, p2 = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    assert hb.zgetrf(p, m, n, a1, m, p1, recursive=recursive) == k
+    assert orc.zgetrf(m, n, a2, m, p2, recursive=recursive) == k
+    assert np.array_equal(p1, p2)
+    assert same_bits(creal(a1), creal(a2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("n", [5, 40])
+def test_zgetrf_tiny_pivots(hb, p, recursive, n):
+    """Golden from the reference's TinyPivots test: pivots below the safe
+    minimum divide the column (the runtime's complex quotient), L(i, 0) =
+    2^-min(i, 20) exactly, no interchanges."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    rt = np.float64 if p == "z" else np.float32
+    tiny = np.finfo(rt).tiny / 4
+    a = np.zeros((n, n), dtype, order="F")
+    for i in range(n):
+        a[i, 0] = np.ldexp(tiny, -min(i, 20))
+    for k in range(1, n):
+        a[0, k] = 1
+        a[k, k] = 4
+    ipiv = np.zeros(n, np.int32)
+    assert hb.zgetrf(p, n, n, a, n, ipiv, recursive=recursive) == 0
+    assert np.array_equal(ipiv, np.arange(1, n + 1))
+    for i in range(1, n):
+        assert a[i, 0] == np.ldexp(rt(1), -min(i, 20)), i
+
+
+def test_zgetrf_mixed_magnitudes_and_ties(hb, orc):
+    """Pivots decided by |re| + |im| with ties (first index wins), parts of
+    very different sizes and tiny complex pivots with both parts nonzero."""
+    rng = np.random.default_rng(3)
+    n = 48
+    a = crand(rng, n, n, np.complex128)
+    a[5:12, 0] = 0.5 + 0.5j       # equal magnitudes, several rows
+    a[20, 0] = 1.0 + 0j
+    a[21, 0] = 0 - 1.0j           # the same |re| + |im|
+    a[:, 3] *= 1e-310             # subnormal column: tiny pivots, both parts
+    a[:, 7] = a[:, 7].real * 1e200 + 1j * a[:, 7].imag * 1e-200
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1, p2 = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    i1 = hb.zgetrf("z", n, n, a1, n, p1)
+    i2 = orc.zgetrf(n, n, a2, n, p2)
+    assert i1 == i2
+    assert np.array_equal(p1, p2)
+    assert same_bits(creal(a1), creal(a2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+def test_zgetrs_zgesv_bitexact(hb, orc, p, trans):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(7)
+    n, nrhs = 300, 5
+    a = crand(rng, n, n, dtype)
+    lu = a.copy(order="F")
+    ipiv = np.zeros(n, np.int32)
+    assert orc.zgetrf(n, n, lu, n, ipiv) == 0
+    b = crand(rng, n, nrhs, dtype)
+    b1, b2 = b.copy(order="F"), b.copy(order="F")
+    assert hb.zgetrs(p, trans, n, nrhs, lu, n, ipiv, b1, n) == 0
+    assert orc.zgetrs(trans, n, nrhs, lu, n, ipiv, b2, n) == 0
+    assert same_bits(creal(b1), creal(b2))
+    if trans == "N":
+        a1, a2 = a.copy(order="F"), a.copy(order="F")
+        b1, b2 = b.copy(order="F"), b.copy(order="F")
+        q1, q2 = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        assert hb.zgesv(p, n, nrhs, a1, n, q1, b1, n) == 0
+        assert orc.zgesv(n, nrhs, a2, n, q2, b2, n) == 0
+        assert np.array_equal(q1, q2)
+        assert same_bits(creal(a1), creal(a2)) and same_bits(creal(b1), creal(b2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("incx", [1, -1, 2, -2])
+def test_zlaswp(hb, orc, p, incx):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(9)
+    lda, n = 50, 37
+    a = crand(rng, lda, n, dtype)
+    k1, k2 = 3, 20
+    ipiv = rng.integers(1, lda + 1, k1 + (k2 - k1) * abs(incx)).astype(np.int32)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    hb.zlaswp(p, n, a1, lda, k1, k2, ipiv, incx)
+    orc.zlaswp(n, a2, lda, k1, k2, ipiv, incx)
+    assert np.array_equal(a1, a2)
+
+
+def test_zgetrf_device_arrays_misaligned_and_errors(hb, orc):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(21)
+    m, n = 600, 250
+    a = crand(rng, m, n, np.complex128)
+    want = a.copy(order="F")
+    pw = np.zeros(n, np.int32)
+    assert orc.zgetrf(m, n, want, m, pw) == 0
+    # A device array whose address is 8 bytes past a complex element.
+    flat = np.zeros(2 * m * n + 1)
+    flat[1:] = a.ravel(order="F").view(np.float64)
+    ta = torch.from_numpy(flat).cuda()
+    tp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert hb.zgetrf("z", m, n, ta.data_ptr() + 8, m, tp) == 0
+    got = ta.cpu().numpy()[1:].view(np.complex128).reshape(n, m).T
+    assert np.array_equal(tp.cpu().numpy(), pw)
+    assert same_bits(creal(got), creal(want))
+    # Aligned device arrays (complex64) and the solve on them.
+    a32 = crand(rng, 200, 200, np.complex64)
+    b32 = crand(rng, 200, 2, np.complex64)
+    wa, wb, wp = a32.copy(order="F"), b32.copy(order="F"), np.zeros(200, np.int32)
+    assert orc.zgesv(200, 2, wa, 200, wp, wb, 200) == 0
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x.T)).T.cuda()  # noqa: E731
+    da, db = dev(a32), dev(b32)
+    dp = torch.zeros(200, dtype=torch.int32, device="cuda")
+    assert hb.zgesv("c", 200, 2, da, 200, dp, db, 200) == 0
+    assert same_bits(creal(np.asfortranarray(da.cpu().numpy())), creal(wa))
+    assert same_bits(creal(np.asfortranarray(db.cpu().numpy())), creal(wb))
+    z = np.zeros((4, 4), np.complex128, order="F")
+    ip = np.zeros(4, np.int32)
+    assert hb.zgetrf("z", 0, 4, z, 1, ip) == 0
+    with hb.ErrorCapture() as cap:
+        assert hb.zgetrf("z", -1, 4, z, 4, ip) == -1
+        assert hb.zgetrf("c", 4, -2, z.astype(np.complex64), 4, ip) == -2
+        assert hb.zgetrf("z", 4, 4, z, 3, ip, recursive=True) == -4
+        assert hb.zgetrs("z", "X", 4, 1, z, 4, ip, z, 4) == -1
+        assert hb.zgetrs("c", "N", 4, 1, z.astype(np.complex64), 4, ip,
+                         z.astype(np.complex64), 3) == -8
+        assert hb.zgesv("z", 4, -1, z, 4, ip, z, 4) == -2
+    assert cap.errors == [("ZGETRF", 1), ("CGETRF", 2), ("ZGETRF2", 4), ("ZGETRS", 1),
+                          ("CGETRS", 8), ("ZGESV", 2)]

@@ -920,3 +920,111 @@ def test_gesv_posv_solve(orc):
         f, x = s.copy(order="F"), b.copy(order="F")
         assert orc.dposv(uplo, n, nrhs, f, n, x, n) == 0
         assert np.abs(x - x0).max() < 1e-8
+
+
+# --------------------------------------------------------------------------
+# Complex LU (zgetrf_, cgetrf_): the reference's own getrf.cc at std::complex,
+# built on the oracle's complex leaf, GEMM and TRSM, against the oracle's
+# restatement of the drivers; then the reference tests' checks of the leaf
+# itself (tests/lapack/getrf_test.cc:78-200).
+
+ZGETRF_SHAPES = [(1, 1), (1, 6), (6, 1), (3, 7), (16, 16), (17, 17), (33, 17), (17, 33),
+                 (64, 64), (65, 70), (90, 150), (150, 90), (200, 200)]
+
+
+def _zlu_residual(a0, lu, ipiv, m, n):
+    """||P L U - A||_1 / (n ||A||_1 eps) for the m x n leading block."""
+    k = min(m, n)
+    L = np.tril(lu[:m, :k], -1) + np.eye(m, k)
+    U = np.triu(lu[:k, :n])
+    prod = (L @ U).astype(np.complex128)
+    for i in range(k - 1, -1, -1):
+        p = ipiv[i] - 1
+        prod[[i, p], :] = prod[[p, i], :]
+    orig = a0[:m, :n].astype(np.complex128)
+    eps = np.finfo(np.float64 if a0.dtype == np.complex128 else np.float32).eps / 2
+    an = np.abs(orig).sum(axis=0).max()
+    return np.abs(prod - orig).sum(axis=0).max() / max(n, 1) / an / eps
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("m,n", ZGETRF_SHAPES)
+def test_zgetrf_matches_reference_driver(orc, ref_drivers, dtype, recursive, m, n):
+    from tests.oracle_lib import crand, ref_call_zgetrf
+    rng = np.random.default_rng(m * 977 + n)
+    lda = m + 3
+    a = crand(rng, lda, n, dtype)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1 = np.zeros(min(m, n), np.int32)
+    p2 = np.zeros(min(m, n), np.int32)
+    i1 = orc.zgetrf(m, n, a1, lda, p1, recursive=recursive)
+    i2 = ref_call_zgetrf(ref_drivers, recursive, m, n, a2, lda, p2)
+    assert i1 == i2 == 0
+    assert np.array_equal(p1, p2)
+    assert same_bits(creal(a1), creal(a2)), first_diff(creal(a1), creal(a2))
+    # The reference test's checks: pivots in range, |L| <= sqrt(2) (pivots by
+    # |re| + |im|), a small residual; rows below m untouched.
+    assert np.all(p1 >= np.arange(1, min(m, n) + 1)) and np.all(p1 <= m)
+    eps = np.finfo(np.float64 if dtype == np.complex128 else np.float32).eps
+    Lpart = np.tril(a1[:m, :min(m, n)], -1)
+    assert np.all(np.abs(Lpart) <= np.sqrt(2) * (1 + 4 * eps))
+    assert _zlu_residual(a, a1, p1, m, n) < 30
+    assert np.array_equal(a1[m:, :], a[m:, :])
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("trans", ["N", "T", "C"])
+def test_zgetrs_matches_reference_driver(orc, ref_drivers, dtype, trans):
+    from tests.oracle_lib import crand, ref_call_zgetrs
+    rng = np.random.default_rng(5)
+    n, nrhs = 130, 3
+    a = crand(rng, n, n, dtype)
+    ipiv = np.zeros(n, np.int32)
+    assert orc.zgetrf(n, n, a, n, ipiv) == 0
+    b = crand(rng, n, nrhs, dtype)
+    b1, b2 = b.copy(order="F"), b.copy(order="F")
+    assert orc.zgetrs(trans, n, nrhs, a, n, ipiv, b1, n) == 0
+    assert ref_call_zgetrs(ref_drivers, trans, n, nrhs, a, n, ipiv, b2, n) == 0
+    assert same_bits(creal(b1), creal(b2)), first_diff(creal(b1), creal(b2))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("k", [1, 2, 8, 9, 17, 30])
+def test_zgetrf_exactly_singular(orc, dtype, recursive, k):
+    """A zero column k: INFO = k, U(k, k) = 0, the factorization completed
+    (tests/lapack/getrf_test.cc:142-165)."""
+    from tests.oracle_lib import crand
+    rng = np.random.default_rng(11 + k)
+    m, n = 40, 30
+    a = crand(rng, m, n, dtype)
+    a[:, k - 1] = 0
+    if k < n:
+        a[:, n - 1] = 0
+    lu = a.copy(order="F")
+    ipiv = np.zeros(n, np.int32)
+    assert orc.zgetrf(m, n, lu, m, ipiv, recursive=recursive) == k
+    assert lu[k - 1, k - 1] == 0
+    assert _zlu_residual(a, lu, ipiv, m, n) < 30
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("n", [5, 40])
+def test_zgetrf_tiny_pivots_golden(orc, dtype, recursive, n):
+    """Pivots below the safe minimum divide the column: L(i, 0) = 2^-min(i, 20)
+    exactly and ipiv(i) = i (tests/lapack/getrf_test.cc:172-200)."""
+    rt = np.float64 if dtype == np.complex128 else np.float32
+    tiny = np.finfo(rt).tiny / 4
+    a = np.zeros((n, n), dtype, order="F")
+    for i in range(n):
+        a[i, 0] = np.ldexp(tiny, -min(i, 20))
+    for k in range(1, n):
+        a[0, k] = 1
+        a[k, k] = 4
+    ipiv = np.zeros(n, np.int32)
+    assert orc.zgetrf(n, n, a, n, ipiv, recursive=recursive) == 0
+    assert np.array_equal(ipiv, np.arange(1, n + 1))
+    for i in range(1, n):
+        assert a[i, 0] == np.ldexp(rt(1), -min(i, 20)), i
