@@ -23,6 +23,7 @@ __all__ = [
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
     "KERNEL_LU_LEAF", "getrf_batched", "getrs_batched", "gemm_batched",
     "trsm_batched", "symm", "syr2k", "gemmtr", "trmm", "cblas_level3", "getri", "trtri", "gerfs", "zgemm", "ztrsm", "zgetrf", "zlaswp", "zgetrs", "zgesv",
+    "zpotrf", "zpotrs", "zposv", "zherk",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -51,6 +52,7 @@ from ._api import (  # noqa: E402  (needs lib())
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
     KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,
     trsm_batched, symm, syr2k, gemmtr, trmm, cblas_level3, getri, trtri, gerfs, zgemm, ztrsm, zgetrf, zlaswp, zgetrs, zgesv,
+    zpotrf, zpotrs, zposv, zherk,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,
 )

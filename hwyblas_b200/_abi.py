@@ -27,6 +27,11 @@ PROTOTYPES = {
     **{f"{p}laswp_": (None, [PI, P, PI, PI, PI, P, PI]) for p in "zc"},
     **{f"{p}getrs_": (None, [C, PI, PI, P, PI, P, P, PI, PI]) for p in "zc"},
     **{f"{p}gesv_": (None, [PI, PI, P, PI, P, P, PI, PI]) for p in "zc"},
+    **{f"{p}potrf_": (None, [C, PI, P, PI, PI]) for p in "zc"},
+    **{f"{p}potrf2_": (None, [C, PI, P, PI, PI]) for p in "zc"},
+    **{f"{p}potrs_": (None, [C, PI, PI, P, PI, P, PI, PI]) for p in "zc"},
+    **{f"{p}posv_": (None, [C, PI, PI, P, PI, P, PI, PI]) for p in "zc"},
+    **{f"{p}herk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]) for p in "zc"},
     **{f"{p}symm_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}syr2k_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])

@@ -197,6 +197,32 @@ def zgesv(p, n, nrhs, a, lda, ipiv, b, ldb):
                       _ptr(ipiv), _ptr(b), _i(ldb))
 
 
+def zpotrf(p, uplo, n, a, lda, recursive=False):
+    """Complex Cholesky; returns INFO (reference zpotrf_/cpotrf_ and ...2_)."""
+    fn = getattr(lib(), f"{p}{'potrf2' if recursive else 'potrf'}_")
+    return _info_call(fn, _c(uplo), _i(n), _ptr(a), _i(lda))
+
+
+def zpotrs(p, uplo, n, nrhs, a, lda, b, ldb):
+    """Complex solve with Cholesky factors; returns INFO (src/lapack/posv.cc:31)."""
+    return _info_call(getattr(lib(), f"{p}potrs_"), _c(uplo), _i(n), _i(nrhs), _ptr(a),
+                      _i(lda), _ptr(b), _i(ldb))
+
+
+def zposv(p, uplo, n, nrhs, a, lda, b, ldb):
+    """Complex Cholesky solve of A X = B; returns INFO (src/lapack/posv.cc:85)."""
+    return _info_call(getattr(lib(), f"{p}posv_"), _c(uplo), _i(n), _i(nrhs), _ptr(a),
+                      _i(lda), _ptr(b), _i(ldb))
+
+
+def zherk(p, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+    """Complex Hermitian rank-k update, alpha and beta real (reference
+    zherk_/cherk_, src/level3.cc:439-452)."""
+    sc = _d if p == "z" else _f
+    getattr(lib(), f"{p}herk_")(_c(uplo), _c(trans), _i(n), _i(k), sc(alpha), _ptr(a),
+                                _i(lda), sc(beta), _ptr(c), _i(ldc))
+
+
 def cblas_level3(name, *args):
     """Calls cblas_<name> (d/s symm, syr2k, gemmtr, gemmt, trmm) with by-value
     scalars, array arguments given as numpy arrays or device pointers."""

@@ -1617,6 +1617,93 @@ static void PosvEntry(const char* name, const char* uplo, const hwyblas_int* n_p
   *info = finfo;
   hb::Finish(name);
 }
+// Complex HERK (src/level3.cc:85-140, 439-452): alpha and beta real.
+template <typename R>
+static void ZherkEntry(const char* name, const char* uplo, const char* trans,
+                       const hwyblas_int* n_p, const hwyblas_int* k_p, const R* alpha,
+                       const R* a, const hwyblas_int* lda_p, const R* beta, R* c,
+                       const hwyblas_int* ldc_p) {
+  const int n = *n_p, k = *k_p, lda = *lda_p, ldc = *ldc_p;
+  const char u = hb::Up(*uplo);
+  const int op = DecodeOp3(*trans);
+  const bool no_trans = op == 0;
+  const int rows_a = no_trans ? n : k;
+  int info = 0;
+  if (u != 'L' && u != 'U') info = 1;
+  else if (op != 0 && op != 2) info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, rows_a)) info = 7;
+  else if (ldc < std::max(1, n)) info = 10;
+  if (info != 0) {
+    hb::ReportError(name, info);
+    return;
+  }
+  const R al = *alpha, be = *beta;
+  if (n == 0 || ((al == R(0) || k == 0) && be == R(1))) return;
+  const bool reads_a = !(al == R(0) || k == 0);
+  ZWorkMatrix<R> sa, sc;
+  if (reads_a && !sa.In(const_cast<R*>(a), lda, rows_a, no_trans ? k : n, hb::kWsStageA, true))
+    return;
+  if (!sc.In(c, ldc, n, n, hb::kWsStageC, true, hb::kWsZFactorB)) return;
+  hb::ZherkFull<R>(u == 'L', op, n, k, al, sa.dev, sa.ld, be, sc.dev, sc.ld);
+  sc.Out();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZPotrfEntry(bool recursive, const char* name, const char* uplo,
+                        const hwyblas_int* n_p, R* a, const hwyblas_int* lda_p,
+                        hwyblas_int* info) {
+  const int n = *n_p, lda = *lda_p;
+  bool upper;
+  if (!CheckPotrf(name, uplo, n, lda, info, &upper)) return;
+  if (n == 0) return;
+  ZWorkMatrix<R> sa;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  hb::ResetInfo();
+  hb::ZPotrf<R>(recursive, upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  sa.Out();
+  *info = hb::ReadInfo();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZPotrsEntry(const char* name, const char* uplo, const hwyblas_int* n_p,
+                        const hwyblas_int* nrhs_p, const R* a, const hwyblas_int* lda_p, R* b,
+                        const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  bool upper;
+  if (!CheckPos(name, uplo, n, nrhs, lda, ldb, info, &upper)) return;
+  if (n == 0 || nrhs == 0) return;
+  ZWorkMatrix<R> sa, sb;
+  if (!sa.In(const_cast<R*>(a), lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true, hb::kWsZFactorB)) return;
+  hb::ZPotrs<R>(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sb.Out();
+  hb::Finish(name);
+}
+
+template <typename R>
+static void ZPosvEntry(const char* name, const char* uplo, const hwyblas_int* n_p,
+                       const hwyblas_int* nrhs_p, R* a, const hwyblas_int* lda_p, R* b,
+                       const hwyblas_int* ldb_p, hwyblas_int* info) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldb = *ldb_p;
+  bool upper;
+  if (!CheckPos(name, uplo, n, nrhs, lda, ldb, info, &upper)) return;
+  if (n == 0) return;
+  ZWorkMatrix<R> sa, sb;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true, hb::kWsZFactorB)) return;
+  hb::ResetInfo();
+  hb::ZPotrf<R>(false, upper, n, sa.dev, sa.ld, hb::DeviceInfo());
+  const int finfo = hb::ReadInfo();
+  if (finfo == 0 && nrhs > 0) hb::ZPotrs<R>(upper, n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld);
+  sa.Out();
+  if (finfo == 0) sb.Out();
+  *info = finfo;
+  hb::Finish(name);
+}
 }  // extern "C++"
 
 HWYBLAS_API void dpotrf_(const char* uplo, const hwyblas_int* n, double* a,
@@ -1640,6 +1727,37 @@ HWYBLAS_API void dposv_(const char* uplo, const hwyblas_int* n, const hwyblas_in
                         hwyblas_int* info) {
   PosvEntry<double>("DPOSV", uplo, n, nrhs, a, lda, b, ldb, info);
 }
+
+// Complex Cholesky and HERK (src/lapack/potrf.cc, posv.cc at c64/c32;
+// src/level3.cc:439-452).
+#define HB_ZCHOL(P, U, R)                                                                 \
+  HWYBLAS_API void P##potrf_(const char* uplo, const hwyblas_int* n, R* a,                \
+                             const hwyblas_int* lda, hwyblas_int* info) {                 \
+    ZPotrfEntry<R>(false, U "POTRF", uplo, n, a, lda, info);                             \
+  }                                                                                       \
+  HWYBLAS_API void P##potrf2_(const char* uplo, const hwyblas_int* n, R* a,               \
+                              const hwyblas_int* lda, hwyblas_int* info) {                \
+    ZPotrfEntry<R>(true, U "POTRF2", uplo, n, a, lda, info);                             \
+  }                                                                                       \
+  HWYBLAS_API void P##potrs_(const char* uplo, const hwyblas_int* n,                      \
+                             const hwyblas_int* nrhs, const R* a, const hwyblas_int* lda, \
+                             R* b, const hwyblas_int* ldb, hwyblas_int* info) {           \
+    ZPotrsEntry<R>(U "POTRS", uplo, n, nrhs, a, lda, b, ldb, info);                      \
+  }                                                                                       \
+  HWYBLAS_API void P##posv_(const char* uplo, const hwyblas_int* n,                       \
+                            const hwyblas_int* nrhs, R* a, const hwyblas_int* lda, R* b,  \
+                            const hwyblas_int* ldb, hwyblas_int* info) {                  \
+    ZPosvEntry<R>(U "POSV", uplo, n, nrhs, a, lda, b, ldb, info);                        \
+  }                                                                                       \
+  HWYBLAS_API void P##herk_(const char* uplo, const char* trans, const hwyblas_int* n,    \
+                            const hwyblas_int* k, const R* alpha, const R* a,             \
+                            const hwyblas_int* lda, const R* beta, R* c,                  \
+                            const hwyblas_int* ldc) {                                     \
+    ZherkEntry<R>(U "HERK", uplo, trans, n, k, alpha, a, lda, beta, c, ldc);             \
+  }
+HB_ZCHOL(z, "Z", double)
+HB_ZCHOL(c, "C", float)
+#undef HB_ZCHOL
 
 HWYBLAS_API void spotrf_(const char* uplo, const hwyblas_int* n, float* a,
                          const hwyblas_int* lda, hwyblas_int* info) {

@@ -70,6 +70,11 @@ struct ZParams {
   R* c;
   long long ldc;  // complex elements
   const int* guard;
+  // HERK: only the triangle `part` of C (1 lower, 2 upper; 0 all) is
+  // updated. Elements in micro-tiles of the reference (tmr x tnr, on its
+  // grid) that cross the diagonal merge as its MergeTile does, with the
+  // diagonal's imaginary part dropped when real_diag is set.
+  int part, real_diag, tmr, tnr;
 };
 
 template <typename R>
@@ -113,6 +118,9 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
   V* sa = reinterpret_cast<V*>(zsmem);                 // [2][kZK][kZM]
   V* sb = sa + 2 * kZK * kZM;                          // [2][kZK][kZN]
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
+  // A block wholly outside the triangle of C has nothing to do.
+  if (p.part == 1 && min(m0 + kZM, p.m) - 1 < n0) return;
+  if (p.part == 2 && m0 > min(n0 + kZN, p.n) - 1) return;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   R rr[4][4], ir[4][4], ri[4][4], ii[4][4];
 #pragma unroll
@@ -195,6 +203,35 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
           const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
           const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
           R* ce = p.c + 2 * (i + j * p.ldc);
+          if (p.part != 0) {
+            if (p.part == 1 ? i < j : i > j) continue;
+            const int i0 = i / p.tmr * p.tmr, j0 = j / p.tnr * p.tnr;
+            const int il = min(i0 + p.tmr, p.m) - 1, jl = min(j0 + p.tnr, p.n) - 1;
+            if (!(p.part == 1 ? i0 > jl : il < j0)) {
+              // Crossing tile (src/gemm-inl.h:110-130): v = alpha ab, then
+              // v += beta * c as the C++ runtime's complex product and sum
+              // (beta 1 after the first chunk); on the diagonal with
+              // real_diag, v and c lose their imaginary parts first.
+              const R br = first ? p.beta_re : R(1), bi = first ? p.beta_im : R(0);
+              const bool bz = br == R(0) && bi == R(0);
+              R vr = t_re, vi = t_im;
+              if (p.real_diag && i == j) {
+                vi = R(0);
+                if (!bz) {
+                  const R c0 = ce[0];
+                  vr = Add(vr, Sub(Mul(br, c0), Mul(bi, R(0))));
+                  vi = Add(vi, Add(Mul(br, R(0)), Mul(bi, c0)));
+                }
+              } else if (!bz) {
+                const R c0 = ce[0], c1 = ce[1];
+                vr = Add(vr, Sub(Mul(br, c0), Mul(bi, c1)));
+                vi = Add(vi, Add(Mul(br, c1), Mul(bi, c0)));
+              }
+              ce[0] = vr;
+              ce[1] = vi;
+              continue;
+            }
+          }
           if (first && beta_zero) {
             ce[0] = t_re;
             ce[1] = t_im;
@@ -713,13 +750,122 @@ __global__ void ZGetrfLeafTrailingKernel(int m, int w, int n, R* a, long long ld
   }
 }
 
+// ---------------------------------------------------------------------------
+// Complex Cholesky leaf (src/lapack/factor_kernels.cc:141-175 for complex T,
+// n <= 32) in one CTA, the referenced triangle in shared memory. Per column
+// j: the real part of the diagonal must be positive (else INFO = j + 1 and
+// stop); it becomes (sqrt, 0) and rinv = 1 / sqrt scales the row (upper) or
+// column (lower) part by part; then
+//   upper: column k > j, rows j+1..k: y += (-U(j, k)) conj(U(j, i)), length k - j;
+//   lower: column k > j, rows k..n-1: y += (-conj(L(k, j))) L(i, j), length n - k;
+// in the reference's complex AXPY rounding.
+template <typename R>
+__global__ void __launch_bounds__(256)
+    ZPotrfLeafKernel(int upper, int n, R* a, long long lda, int* info, int info_base,
+                     int lanes, const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  __shared__ R sr[32][33], si[32][33];  // A(i, j)
+  __shared__ R row_r[32], row_i[32];
+  __shared__ R s_rinv;
+  __shared__ int stop;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    const bool ref = upper ? (i <= j) : (i >= j);
+    const R* e = a + 2 * (i + j * lda);
+    sr[i][j] = ref ? e[0] : R(0);
+    si[i][j] = ref ? e[1] : R(0);
+  }
+  if (threadIdx.x == 0) stop = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      const R ajj = sr[j][j];
+      if (ajj <= R(0) || isnan(ajj)) {
+        stop = 1;
+        if (*info == 0) *info = info_base + j + 1;
+      } else {
+        const R r = sqrt(ajj);
+        sr[j][j] = r;
+        si[j][j] = R(0);
+        s_rinv = R(1) / r;
+      }
+    }
+    __syncthreads();
+    if (stop) break;
+    const R rinv = s_rinv;
+    if (upper) {
+      for (int k = j + 1 + threadIdx.x; k < n; k += blockDim.x) {
+        sr[j][k] = Mul(sr[j][k], rinv);
+        si[j][k] = Mul(si[j][k], rinv);
+        row_r[k] = sr[j][k];
+        row_i[k] = -si[j][k];
+      }
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, k = idx / n;
+        if (k <= j || i <= j || i > k) continue;
+        ZAxpyRef<R>(sr[i][k], si[i][k], -sr[j][k], -si[j][k], row_r[i], row_i[i], k - j,
+                    lanes);
+      }
+    } else {
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+        sr[i][j] = Mul(sr[i][j], rinv);
+        si[i][j] = Mul(si[i][j], rinv);
+      }
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, k = idx / n;
+        if (k <= j || i < k) continue;
+        ZAxpyRef<R>(sr[i][k], si[i][k], -sr[k][j], si[k][j], sr[i][j], si[i][j], n - k,
+                    lanes);
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    const bool ref = upper ? (i <= j) : (i >= j);
+    if (ref) {
+      R* e = a + 2 * (i + j * lda);
+      e[0] = sr[i][j];
+      e[1] = si[i][j];
+    }
+  }
+}
+
+// HERK's quick path with beta != 1 (src/gemm.cc:48-64 with real_diagonal):
+// the triangle `part` of C times beta (zeros for beta 0) as the runtime's
+// complex product, the diagonal first reduced to its real part.
+template <typename R>
+__global__ void ZScaleTriangleKernel(int n, int lower, R beta, R* c, long long ldc,
+                                     const int* guard) {
+  if (guard != nullptr && *guard != 0) return;
+  const long long total = static_cast<long long>(n) * n;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % n), j = static_cast<int>(e / n);
+    if (lower ? i < j : i > j) continue;
+    R* ce = c + 2 * (i + j * ldc);
+    R c0 = ce[0], c1 = ce[1];
+    if (i == j) c1 = R(0);
+    if (beta == R(0)) {
+      ce[0] = R(0);
+      ce[1] = R(0);
+    } else {
+      ce[0] = Sub(Mul(c0, beta), Mul(c1, R(0)));
+      ce[1] = Add(Mul(c0, R(0)), Mul(c1, beta));
+    }
+  }
+}
+
 }  // namespace
 
 // The complex GEMM kernel on operand views (elements aligned to their size;
 // m, n, k > 0): C := alpha op(A) op(B) + beta C with the reference's merges.
 template <typename R>
 void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, const R* beta,
-                R* c, int ldc) {
+                R* c, int ldc, int part = 0) {
   ZParams<R> p;
   p.m = m;
   p.n = n;
@@ -733,6 +879,14 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   p.c = c;
   p.ldc = ldc;
   p.guard = Ctx().guard;
+  p.part = part;
+  p.real_diag = part != 0 ? 1 : 0;
+  // The reference's complex micro-tile: 2 vectors of lanes reals per column
+  // (lanes / 2 complex rows each), 6 columns with 32 vector registers, 3
+  // with 16 (src/gemm_kernel-inl.h:243-257).
+  const int lanes = sizeof(R) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  p.tmr = lanes;
+  p.tnr = RefLanesDouble() == 8 ? 6 : 3;
   const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
   static bool configured = false;
   if (!configured) {
@@ -1048,6 +1202,128 @@ void ZGetrs(int op, int n, int nrhs, const R* a, int lda, const int* ipiv, R* b,
 }
 template void ZGetrs<double>(int, int, int, const double*, int, const int*, double*, int);
 template void ZGetrs<float>(int, int, int, const float*, int, const int*, float*, int);
+
+
+// ---------------------------------------------------------------------------
+// Complex HERK (src/level3.cc:85-140): C := alpha op(A) op(A)^H + beta C on
+// the triangle of C, alpha and beta real, op 0 N (A n x k) / 2 C (A k x n).
+// The elements are the complex GEMM's; tiles of the reference crossing the
+// diagonal merge as its MergeTile with the diagonal kept real.
+template <typename R>
+void ZherkFull(bool lower, int op, int n, int k, R alpha, const R* a, int lda, R beta, R* c,
+               int ldc) {
+  if (n == 0 || ((alpha == R(0) || k == 0) && beta == R(1))) return;
+  if (alpha == R(0) || k == 0) {
+    const long long total = static_cast<long long>(n) * n;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 8));
+    ZScaleTriangleKernel<R><<<blocks, 256, 0, Ctx().stream>>>(n, lower ? 1 : 0, beta, c, ldc,
+                                                                Ctx().guard);
+    CountLaunch();
+    LaunchFailed("complex herk scale");
+    return;
+  }
+  const R al[2] = {alpha, R(0)}, be[2] = {beta, R(0)};
+  const ZView<R> plain{a, 1, lda, 0}, herm{a, lda, 1, 1};
+  ZgemmViews<R>(n, n, k, al, op == 0 ? plain : herm, op == 0 ? herm : plain, be, c, ldc,
+                lower ? 1 : 2);
+}
+template void ZherkFull<double>(bool, int, int, int, double, const double*, int, double,
+                                double*, int);
+template void ZherkFull<float>(bool, int, int, int, float, const float*, int, float, float*,
+                               int);
+
+// Complex Cholesky drivers: the reference's Potrf2 recursion (leaf n <= 32)
+// and blocked Potrf (nb = 64, src/lapack/environment.cc:110-111), call for
+// call (src/lapack/potrf.cc:48-199), and Potrs (src/lapack/posv.cc:31-76).
+// The device INFO doubles as the guard that turns the call's later kernels
+// into no-ops once a leaf finds a non-positive minor.
+namespace {
+template <typename R>
+void ZPotrfLeaf(bool upper, int n, R* a, int lda, int* info, int info_base) {
+  const int lanes = sizeof(R) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
+  ZPotrfLeafKernel<R><<<1, 256, 0, Ctx().stream>>>(upper ? 1 : 0, n, a, lda, info, info_base,
+                                                    lanes, Ctx().guard);
+  CountLaunch();
+  LaunchFailed("complex potrf leaf");
+}
+
+template <typename R>
+void ZPotrf2Rec(bool upper, int n, R* a, int lda, int* info, int col0) {
+  if (n == 0) return;
+  if (n <= 32) {
+    ZPotrfLeaf<R>(upper, n, a, lda, info, col0);
+    return;
+  }
+  const R one[2] = {R(1), R(0)};
+  const int n1 = n / 2, n2 = n - n1;
+  ZPotrf2Rec<R>(upper, n1, a, lda, info, col0);
+  if (upper) {
+    ZtrsmFull<R>(true, false, 2, false, n1, n2, one, a, lda, ZAt(a, lda, 0, n1), lda);
+    ZherkFull<R>(false, 2, n2, n1, R(-1), ZAt(a, lda, 0, n1), lda, R(1), ZAt(a, lda, n1, n1),
+                 lda);
+  } else {
+    ZtrsmFull<R>(false, true, 2, false, n2, n1, one, a, lda, ZAt(a, lda, n1, 0), lda);
+    ZherkFull<R>(true, 0, n2, n1, R(-1), ZAt(a, lda, n1, 0), lda, R(1), ZAt(a, lda, n1, n1),
+                 lda);
+  }
+  ZPotrf2Rec<R>(upper, n2, ZAt(a, lda, n1, n1), lda, info, col0 + n1);
+}
+}  // namespace
+
+template <typename R>
+void ZPotrf(bool recursive, bool upper, int n, R* a, int lda, int* info) {
+  if (n == 0) return;
+  Context& ctx = Ctx();
+  const int* saved = ctx.guard;
+  ctx.guard = info;
+  const int nb = 64;
+  if (recursive || nb >= n) {
+    ZPotrf2Rec<R>(upper, n, a, lda, info, 0);
+    ctx.guard = saved;
+    return;
+  }
+  const R one[2] = {R(1), R(0)}, m1[2] = {R(-1), R(0)};
+  for (int j = 0; j < n; j += nb) {
+    const int jb = std::min(nb, n - j);
+    if (upper) {
+      ZherkFull<R>(false, 2, jb, j, R(-1), ZAt(a, lda, 0, j), lda, R(1), ZAt(a, lda, j, j), lda);
+      ZPotrf2Rec<R>(true, jb, ZAt(a, lda, j, j), lda, info, j);
+      if (j + jb < n) {
+        ZgemmFull<R>(2, 0, jb, n - j - jb, j, m1, ZAt(a, lda, 0, j), lda,
+                     ZAt(a, lda, 0, j + jb), lda, one, ZAt(a, lda, j, j + jb), lda);
+        ZtrsmFull<R>(true, false, 2, false, jb, n - j - jb, one, ZAt(a, lda, j, j), lda,
+                     ZAt(a, lda, j, j + jb), lda);
+      }
+    } else {
+      ZherkFull<R>(true, 0, jb, j, R(-1), ZAt(a, lda, j, 0), lda, R(1), ZAt(a, lda, j, j), lda);
+      ZPotrf2Rec<R>(false, jb, ZAt(a, lda, j, j), lda, info, j);
+      if (j + jb < n) {
+        ZgemmFull<R>(0, 2, n - j - jb, jb, j, m1, ZAt(a, lda, j + jb, 0), lda,
+                     ZAt(a, lda, j, 0), lda, one, ZAt(a, lda, j + jb, j), lda);
+        ZtrsmFull<R>(false, true, 2, false, n - j - jb, jb, one, ZAt(a, lda, j, j), lda,
+                     ZAt(a, lda, j + jb, j), lda);
+      }
+    }
+  }
+  ctx.guard = saved;
+}
+template void ZPotrf<double>(bool, bool, int, double*, int, int*);
+template void ZPotrf<float>(bool, bool, int, float*, int, int*);
+
+template <typename R>
+void ZPotrs(bool upper, int n, int nrhs, const R* a, int lda, R* b, int ldb) {
+  if (n == 0 || nrhs == 0) return;
+  const R one[2] = {R(1), R(0)};
+  if (upper) {
+    ZtrsmFull<R>(true, false, 2, false, n, nrhs, one, a, lda, b, ldb);
+    ZtrsmFull<R>(true, false, 0, false, n, nrhs, one, a, lda, b, ldb);
+  } else {
+    ZtrsmFull<R>(true, true, 0, false, n, nrhs, one, a, lda, b, ldb);
+    ZtrsmFull<R>(true, true, 2, false, n, nrhs, one, a, lda, b, ldb);
+  }
+}
+template void ZPotrs<double>(bool, int, int, const double*, int, double*, int);
+template void ZPotrs<float>(bool, int, int, const float*, int, float*, int);
 
 
 }  // namespace hb

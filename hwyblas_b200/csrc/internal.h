@@ -243,6 +243,18 @@ void ZGetrf(bool recursive, int m, int n, R* a, int lda, int* ipiv, int* info);
 // Complex LU solve (src/lapack/getrf.cc:287-339), op 0 N / 1 T / 2 C.
 template <typename R>
 void ZGetrs(int op, int n, int nrhs, const R* a, int lda, const int* ipiv, R* b, int ldb);
+// Complex HERK (src/level3.cc:85-140) on the triangle of C, op 0 N / 2 C,
+// alpha and beta real.
+template <typename R>
+void ZherkFull(bool lower, int op, int n, int k, R alpha, const R* a, int lda, R beta, R* c,
+               int ldc);
+// Complex Cholesky (src/lapack/potrf.cc:48-199) on device data; *info on the
+// device. recursive: xPOTRF2 instead of the blocked xPOTRF.
+template <typename R>
+void ZPotrf(bool recursive, bool upper, int n, R* a, int lda, int* info);
+// Complex Cholesky solve (src/lapack/posv.cc:31-76).
+template <typename R>
+void ZPotrs(bool upper, int n, int nrhs, const R* a, int lda, R* b, int ldb);
 // Complex LASWP on device data (src/lapack/getrf.cc:28-81).
 template <typename R>
 void ZLaswp(int n, R* a, int lda, int k1, int k2, const int* ipiv, int incx);

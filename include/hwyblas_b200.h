@@ -262,6 +262,37 @@ HWYBLAS_API void cgetrs_(const char* trans, const hwyblas_int* n,
 HWYBLAS_API void cgesv_(const hwyblas_int* n, const hwyblas_int* nrhs, float* a,
                         const hwyblas_int* lda, hwyblas_int* ipiv, float* b,
                         const hwyblas_int* ldb, hwyblas_int* info);
+/* Complex Cholesky family (src/lapack/potrf.cc:48-199, posv.cc:31-114 at
+ * c64 and c32) and the complex HERK it updates with (src/level3.cc:85-140,
+ * 439-452; alpha and beta real, the diagonal of C kept real). */
+HWYBLAS_API void zpotrf_(const char* uplo, const hwyblas_int* n, double* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void zpotrf2_(const char* uplo, const hwyblas_int* n, double* a,
+                          const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void zpotrs_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const double* a, const hwyblas_int* lda, double* b,
+                         const hwyblas_int* ldb, hwyblas_int* info);
+HWYBLAS_API void zposv_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                        double* a, const hwyblas_int* lda, double* b, const hwyblas_int* ldb,
+                        hwyblas_int* info);
+HWYBLAS_API void zherk_(const char* uplo, const char* trans, const hwyblas_int* n,
+                        const hwyblas_int* k, const double* alpha, const double* a,
+                        const hwyblas_int* lda, const double* beta, double* c,
+                        const hwyblas_int* ldc);
+HWYBLAS_API void cpotrf_(const char* uplo, const hwyblas_int* n, float* a,
+                         const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void cpotrf2_(const char* uplo, const hwyblas_int* n, float* a,
+                          const hwyblas_int* lda, hwyblas_int* info);
+HWYBLAS_API void cpotrs_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                         const float* a, const hwyblas_int* lda, float* b,
+                         const hwyblas_int* ldb, hwyblas_int* info);
+HWYBLAS_API void cposv_(const char* uplo, const hwyblas_int* n, const hwyblas_int* nrhs,
+                        float* a, const hwyblas_int* lda, float* b, const hwyblas_int* ldb,
+                        hwyblas_int* info);
+HWYBLAS_API void cherk_(const char* uplo, const char* trans, const hwyblas_int* n,
+                        const hwyblas_int* k, const float* alpha, const float* a,
+                        const hwyblas_int* lda, const float* beta, float* c,
+                        const hwyblas_int* ldc);
 /* Inverse from the LU factorization: inv(U) by ?trtri, then inv(A) L =
  * inv(U) in block columns of 64 (lwork >= 64 n; narrower blocks for a
  * smaller lwork, column by column below 2 n), then the column interchanges.

@@ -83,6 +83,20 @@ int orc_ctrsm(char side, char uplo, char ta, char diag, int m, int n, const floa
               const float* a, int lda, float* b, int ldb);
 void orc_zrecip(int n, const double* c, double* out);
 void orc_crecip(int n, const float* c, float* out);
+/* Complex HERK (src/level3.cc:85-140, 439-452), alpha and beta real. */
+int orc_zherk(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+              double beta, double* c, int ldc);
+int orc_cherk(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+              float beta, float* c, int ldc);
+/* Complex Cholesky family (src/lapack/potrf.cc, posv.cc at std::complex). */
+int orc_zpotrf(char uplo, int n, double* a, int lda);
+int orc_zpotrf2(char uplo, int n, double* a, int lda);
+int orc_zpotrs(char uplo, int n, int nrhs, const double* a, int lda, double* b, int ldb);
+int orc_zposv(char uplo, int n, int nrhs, double* a, int lda, double* b, int ldb);
+int orc_cpotrf(char uplo, int n, float* a, int lda);
+int orc_cpotrf2(char uplo, int n, float* a, int lda);
+int orc_cpotrs(char uplo, int n, int nrhs, const float* a, int lda, float* b, int ldb);
+int orc_cposv(char uplo, int n, int nrhs, float* a, int lda, float* b, int ldb);
 /* Complex LU family (src/lapack/getrf.cc:28-374 at std::complex). */
 int orc_zgetrf(int m, int n, double* a, int lda, int* ipiv);
 int orc_zgetrf2(int m, int n, double* a, int lda, int* ipiv);

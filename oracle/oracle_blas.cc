@@ -1020,6 +1020,101 @@ int ZtrsmF(char side, char uplo, char transa, char diag, int m, int n, const R* 
   ZTrsmRec<R>(left, tri, op_lower, d == 'U', ka, left ? n : m, b, ldb);
   return 0;
 }
+// Complex HERK (src/level3.cc:85-140) through the GEMM problem model: every
+// element of the triangle is the complex GEMM's (four FMA chains per KC
+// chunk, ab = (rr - ii, ir + ri), t = alpha ab), merged as the micro-kernel
+// merges in tiles wholly inside the triangle and as MergeTile does in tiles
+// that cross the diagonal (src/gemm-inl.h:86-130): there the diagonal keeps
+// only its real part and v += beta * c is the C++ runtime's complex product
+// and sum (beta 1 after the first chunk). The complex micro-tile is
+// lanes / 2 complex rows per vector, two vectors per column, and 6 columns
+// (3 with 16 vector registers): src/gemm_kernel-inl.h:243-257. The quick
+// path (alpha 0 or k 0) is ScaleMatrix with real_diagonal (src/gemm.cc:48-64).
+template <typename R>
+int ZherkF(char uplo, char trans, int n, int k, R alpha, const R* a, int lda, R beta, R* c,
+           int ldc) {
+  using T = std::complex<R>;
+  const char u = Up(uplo), t = Up(trans);
+  const bool lower = (u == 'L');
+  int info = 0;
+  if (u != 'L' && u != 'U') info = 1;
+  else if (t != 'N' && t != 'C') info = 2;
+  else if (n < 0) info = 3;
+  else if (k < 0) info = 4;
+  else if (lda < std::max(1, t == 'N' ? n : k)) info = 7;
+  else if (ldc < std::max(1, n)) info = 10;
+  if (info != 0) return info;
+  T* C = reinterpret_cast<T*>(c);
+  const auto at = [&](int i, int j) -> T& { return C[i + static_cast<ptrdiff_t>(j) * ldc]; };
+  const auto is_zero = [](T v) { return v.real() == R(0) && v.imag() == R(0); };
+  const T be = T(beta);
+  if (n == 0 || ((alpha == R(0) || k == 0) && beta == R(1))) return 0;
+  if (alpha == R(0) || k == 0) {
+    for (int j = 0; j < n; ++j) {
+      const int begin = lower ? j : 0, end = lower ? n : j + 1;
+      at(j, j) = T(std::real(at(j, j)));
+      for (int i = begin; i < end; ++i) {
+        if (is_zero(be)) at(i, j) = T(0);
+        else at(i, j) *= be;
+      }
+    }
+    return 0;
+  }
+  const ZOp<R> plain{a, 1, lda, false}, herm{a, lda, 1, true};
+  const ZOp<R> va = t == 'N' ? plain : herm, vb = t == 'N' ? herm : plain;
+  const int mr = sizeof(R) == 8 ? g_lanes : 2 * g_lanes, nr = g_lanes >= 8 ? 6 : 3;
+  constexpr int KC = 256;
+  for (int j = 0; j < n; ++j) {
+    for (int i = lower ? j : 0; i < (lower ? n : j + 1); ++i) {
+      const int i0 = i / mr * mr, j0 = j / nr * nr;
+      const int il = std::min(i0 + mr, n) - 1, jl = std::min(j0 + nr, n) - 1;
+      const bool inside = lower ? i0 > jl : il < j0;
+      for (int pc = 0; pc < k; pc += KC) {
+        const int pe = std::min(k, pc + KC);
+        R rr = R(0), ir = R(0), ri = R(0), ii = R(0);
+        for (int p = pc; p < pe; ++p) {
+          R ar, ai, br, bi;
+          va.at(i, p, &ar, &ai);
+          vb.at(p, j, &br, &bi);
+          rr = std::fma(ar, br, rr);
+          ir = std::fma(ai, br, ir);
+          ri = std::fma(ar, bi, ri);
+          ii = std::fma(ai, bi, ii);
+        }
+        const R ab_re = rr - ii, ab_im = ir + ri;
+        const R q0 = ab_re * alpha, q1 = ab_im * R(0), q2 = ab_im * alpha, q3 = ab_re * R(0);
+        const R t_re = q0 - q1, t_im = q2 + q3;
+        const T cij = at(i, j);
+        if (inside) {
+          if (pc == 0 && beta == R(0)) {
+            at(i, j) = T(t_re, t_im);
+          } else if (pc != 0 || beta == R(1)) {
+            at(i, j) = T(t_re + cij.real(), t_im + cij.imag());
+          } else {
+            const R s0 = cij.real() * beta, s1 = cij.imag() * R(0);
+            const R s2 = cij.imag() * beta, s3 = cij.real() * R(0);
+            at(i, j) = T(t_re + (s0 - s1), t_im + (s2 + s3));
+          }
+        } else {
+          const T bc = pc == 0 ? be : T(1);
+          T v(t_re, t_im);
+          if (i == j) {
+            v = T(std::real(v));
+            if (!is_zero(bc)) v += bc * T(std::real(cij));
+          } else if (!is_zero(bc)) {
+            v += bc * cij;
+          }
+          at(i, j) = v;
+        }
+      }
+    }
+  }
+  return 0;
+}
+template int ZherkF<double>(char, char, int, int, double, const double*, int, double, double*,
+                            int);
+template int ZherkF<float>(char, char, int, int, float, const float*, int, float, float*, int);
+
 template int ZtrsmF<double>(char, char, char, char, int, int, const double*, const double*,
                             int, double*, int);
 template int ZtrsmF<float>(char, char, char, char, int, int, const float*, const float*, int,
@@ -1112,6 +1207,14 @@ int orc_cgemm(char ta, char tb, int m, int n, int k, const float* alpha, const f
   return orc::ZgemmF<float>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
+int orc_zherk(char uplo, char trans, int n, int k, double alpha, const double* a, int lda,
+              double beta, double* c, int ldc) {
+  return orc::ZherkF<double>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int orc_cherk(char uplo, char trans, int n, int k, float alpha, const float* a, int lda,
+              float beta, float* c, int ldc) {
+  return orc::ZherkF<float>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
 int orc_ztrsm(char side, char uplo, char ta, char diag, int m, int n, const double* alpha,
               const double* a, int lda, double* b, int ldb) {
   return orc::ZtrsmF<double>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);

@@ -50,6 +50,9 @@ int ZgemmF(char transa, char transb, int m, int n, int k, const R* alpha, const 
 template <typename R>
 int ZtrsmF(char side, char uplo, char transa, char diag, int m, int n, const R* alpha,
            const R* a, int lda, R* b, int ldb);
+template <typename R>
+int ZherkF(char uplo, char trans, int n, int k, R alpha, const R* a, int lda, R beta, R* c,
+           int ldc);
 template <typename T>
 int Trmm(char side, char uplo, char transa, char diag, int m, int n, T alpha, const T* a,
          int lda, T* b, int ldb);

@@ -141,20 +141,33 @@ int GetrfLeaf(int m_, int n_, T* a, int lda, int* ipiv) {
 }
 
 template <typename T>
+static T ConjOf(T v) {
+  if constexpr (IsCplx<T>::value) {
+    return std::conj(v);
+  } else {
+    return v;
+  }
+}
+
+// For complex T (src/lapack/factor_kernels.cc:141-175): only the real part
+// of the diagonal is tested; it becomes (sqrt, 0), and rows (upper) or
+// columns (lower) are scaled part by part by the real 1 / sqrt.
+template <typename T>
 int PotrfLeaf(bool upper, int n_, T* a, int lda) {
+  using R = typename RealOf<T>::type;
   const size_t n = n_;
   const auto at = [&](size_t i, size_t j) -> T& { return a[i + j * lda]; };
   T row[64];
   for (size_t j = 0; j < n; ++j) {
-    T ajj = at(j, j);
-    if (ajj <= T(0) || std::isnan(ajj)) return static_cast<int>(j + 1);
+    R ajj = std::real(at(j, j));
+    if (ajj <= R(0) || std::isnan(ajj)) return static_cast<int>(j + 1);
     ajj = std::sqrt(ajj);
-    at(j, j) = ajj;
-    const T rinv = T(1) / ajj;
+    at(j, j) = T(ajj);
+    const R rinv = R(1) / ajj;
     if (upper) {
       for (size_t k = j + 1; k < n; ++k) {
         at(j, k) = at(j, k) * rinv;
-        row[k] = at(j, k);
+        row[k] = ConjOf(at(j, k));
       }
       for (size_t k = j + 1; k < n; ++k) {
         AxpyColumn(k - j, -at(j, k), &row[j + 1], &at(j + 1, k));
@@ -162,7 +175,7 @@ int PotrfLeaf(bool upper, int n_, T* a, int lda) {
     } else {
       for (size_t i = j + 1; i < n; ++i) at(i, j) = at(i, j) * rinv;
       for (size_t k = j + 1; k < n; ++k) {
-        AxpyColumn(n - k, -at(k, j), &at(k, j), &at(k, k));
+        AxpyColumn(n - k, -ConjOf(at(k, j)), &at(k, j), &at(k, k));
       }
     }
   }
@@ -180,6 +193,17 @@ static int TrsmAny(char side, char uplo, char ta, char diag, int m, int n, T alp
                      reinterpret_cast<const R*>(a), lda, reinterpret_cast<R*>(b), ldb);
   } else {
     return TrsmF<T>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+  }
+}
+template <typename T>
+static int SyrkAny(char uplo, char trans, int n, int k, typename RealOf<T>::type alpha,
+                   const T* a, int lda, typename RealOf<T>::type beta, T* c, int ldc) {
+  if constexpr (IsCplx<T>::value) {
+    using R = typename RealOf<T>::type;
+    return ZherkF<R>(uplo, trans, n, k, alpha, reinterpret_cast<const R*>(a), lda, beta,
+                     reinterpret_cast<R*>(c), ldc);
+  } else {
+    return Syrk<T>(uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
   }
 }
 template <typename T>
@@ -310,11 +334,11 @@ int Potrf2(char uplo, int n, T* a, int lda) {
   int iinfo = Potrf2<T>(uplo, n1, a, lda);
   if (iinfo != 0) return iinfo;
   if (upper) {
-    TrsmF<T>('L', 'U', 'C', 'N', n1, n2, T(1), a, lda, A(0, n1), lda);
-    Syrk<T>('U', 'C', n2, n1, T(-1), A(0, n1), lda, T(1), A(n1, n1), lda);
+    TrsmAny<T>('L', 'U', 'C', 'N', n1, n2, T(1), a, lda, A(0, n1), lda);
+    SyrkAny<T>('U', 'C', n2, n1, -1, A(0, n1), lda, 1, A(n1, n1), lda);
   } else {
-    TrsmF<T>('R', 'L', 'C', 'N', n2, n1, T(1), a, lda, A(n1, 0), lda);
-    Syrk<T>('L', 'N', n2, n1, T(-1), A(n1, 0), lda, T(1), A(n1, n1), lda);
+    TrsmAny<T>('R', 'L', 'C', 'N', n2, n1, T(1), a, lda, A(n1, 0), lda);
+    SyrkAny<T>('L', 'N', n2, n1, -1, A(n1, 0), lda, 1, A(n1, n1), lda);
   }
   iinfo = Potrf2<T>(uplo, n2, A(n1, n1), lda);
   if (iinfo != 0) return iinfo + n1;
@@ -335,23 +359,23 @@ int Potrf(char uplo, int n, T* a, int lda) {
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
     if (upper) {
-      Syrk<T>('U', 'C', jb, j, T(-1), A(0, j), lda, T(1), A(j, j), lda);
+      SyrkAny<T>('U', 'C', jb, j, -1, A(0, j), lda, 1, A(j, j), lda);
       const int info = Potrf2<T>('U', jb, A(j, j), lda);
       if (info != 0) return info + j;
       if (j + jb < n) {
-        GemmF<T>('C', 'N', jb, n - j - jb, j, T(-1), A(0, j), lda,
+        GemmAny<T>('C', 'N', jb, n - j - jb, j, T(-1), A(0, j), lda,
                       A(0, j + jb), lda, T(1), A(j, j + jb), lda);
-        TrsmF<T>('L', 'U', 'C', 'N', jb, n - j - jb, T(1), A(j, j), lda,
+        TrsmAny<T>('L', 'U', 'C', 'N', jb, n - j - jb, T(1), A(j, j), lda,
                       A(j, j + jb), lda);
       }
     } else {
-      Syrk<T>('L', 'N', jb, j, T(-1), A(j, 0), lda, T(1), A(j, j), lda);
+      SyrkAny<T>('L', 'N', jb, j, -1, A(j, 0), lda, 1, A(j, j), lda);
       const int info = Potrf2<T>('L', jb, A(j, j), lda);
       if (info != 0) return info + j;
       if (j + jb < n) {
-        GemmF<T>('N', 'C', n - j - jb, jb, j, T(-1), A(j + jb, 0), lda,
+        GemmAny<T>('N', 'C', n - j - jb, jb, j, T(-1), A(j + jb, 0), lda,
                       A(j, 0), lda, T(1), A(j + jb, j), lda);
-        TrsmF<T>('R', 'L', 'C', 'N', n - j - jb, jb, T(1), A(j, j), lda,
+        TrsmAny<T>('R', 'L', 'C', 'N', n - j - jb, jb, T(1), A(j, j), lda,
                       A(j + jb, j), lda);
       }
     }
@@ -370,11 +394,11 @@ int Potrs(char uplo, int n, int nrhs, const T* a, int lda, T* b, int ldb) {
   if (ldb < std::max(1, n)) return -7;
   if (n == 0 || nrhs == 0) return 0;
   if (upper) {
-    TrsmF<T>('L', 'U', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
-    TrsmF<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'U', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'U', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
   } else {
-    TrsmF<T>('L', 'L', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
-    TrsmF<T>('L', 'L', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'L', 'N', 'N', n, nrhs, T(1), a, lda, b, ldb);
+    TrsmAny<T>('L', 'L', 'C', 'N', n, nrhs, T(1), a, lda, b, ldb);
   }
   return 0;
 }
@@ -448,7 +472,7 @@ int Trtri(char uplo, char diag, int n, T* a, int lda) {
     for (int j = 0; j < n; j += nb) {
       const int jb = std::min(nb, n - j);
       Trmm<T>('L', 'U', 'N', d, j, jb, T(1), a, lda, A(0, j), lda);
-      TrsmF<T>('R', 'U', 'N', d, j, jb, T(-1), A(j, j), lda, A(0, j), lda);
+      TrsmAny<T>('R', 'U', 'N', d, j, jb, T(-1), A(j, j), lda, A(0, j), lda);
       Trti2<T>('U', d, jb, A(j, j), lda);
     }
   } else {
@@ -458,7 +482,7 @@ int Trtri(char uplo, char diag, int n, T* a, int lda) {
       if (j + jb < n) {
         Trmm<T>('L', 'L', 'N', d, n - j - jb, jb, T(1), A(j + jb, j + jb), lda, A(j + jb, j),
                 lda);
-        TrsmF<T>('R', 'L', 'N', d, n - j - jb, jb, T(-1), A(j, j), lda, A(j + jb, j), lda);
+        TrsmAny<T>('R', 'L', 'N', d, n - j - jb, jb, T(-1), A(j, j), lda, A(j + jb, j), lda);
       }
       Trti2<T>('L', d, jb, A(j, j), lda);
     }
@@ -512,9 +536,9 @@ int Getri(int n, T* a, int lda, const int* ipiv, T* work, int lwork) {
           A(i, jj) = T(0);
         }
       if (j + jb < n)
-        GemmF<T>('N', 'N', n, jb, n - j - jb, T(-1), &A(0, j + jb), lda, work + j + jb, ldwork,
+        GemmAny<T>('N', 'N', n, jb, n - j - jb, T(-1), &A(0, j + jb), lda, work + j + jb, ldwork,
                  T(1), &A(0, j), lda);
-      TrsmF<T>('R', 'L', 'N', 'U', n, jb, T(1), work + j, ldwork, &A(0, j), lda);
+      TrsmAny<T>('R', 'L', 'N', 'U', n, jb, T(1), work + j, ldwork, &A(0, j), lda);
     }
   }
   for (int j = n - 2; j >= 0; --j) {
@@ -740,6 +764,8 @@ template int GetrfLeaf<std::complex<double>>(int, int, std::complex<double>*, in
 template int GetrfLeaf<std::complex<float>>(int, int, std::complex<float>*, int, int*);
 template int PotrfLeaf<double>(bool, int, double*, int);
 template int PotrfLeaf<float>(bool, int, float*, int);
+template int PotrfLeaf<std::complex<double>>(bool, int, std::complex<double>*, int);
+template int PotrfLeaf<std::complex<float>>(bool, int, std::complex<float>*, int);
 
 }  // namespace orc
 
@@ -894,6 +920,32 @@ int orc_dposv(char uplo, int n, int nrhs, double* a, int lda, double* b,
     if (info == 0) info = orc_##P##getrs('N', n, nrhs, a, lda, ipiv, b, ldb);              \
     return info;                                                                           \
   }
+#define ORC_ZCHOL(P, R)                                                                    \
+  int orc_##P##potrf(char uplo, int n, R* a, int lda) {                                    \
+    return orc::Potrf<std::complex<R>>(uplo, n, reinterpret_cast<std::complex<R>*>(a), lda); \
+  }                                                                                        \
+  int orc_##P##potrf2(char uplo, int n, R* a, int lda) {                                   \
+    return orc::Potrf2<std::complex<R>>(uplo, n, reinterpret_cast<std::complex<R>*>(a), lda); \
+  }                                                                                        \
+  int orc_##P##potrs(char uplo, int n, int nrhs, const R* a, int lda, R* b, int ldb) {     \
+    return orc::Potrs<std::complex<R>>(uplo, n, nrhs,                                      \
+                                       reinterpret_cast<const std::complex<R>*>(a), lda,   \
+                                       reinterpret_cast<std::complex<R>*>(b), ldb);        \
+  }                                                                                        \
+  int orc_##P##posv(char uplo, int n, int nrhs, R* a, int lda, R* b, int ldb) {            \
+    const char u = (uplo >= 'a' && uplo <= 'z') ? uplo - 32 : uplo;                        \
+    if (u != 'U' && u != 'L') return -1;                                                   \
+    if (n < 0) return -2;                                                                  \
+    if (nrhs < 0) return -3;                                                               \
+    if (lda < std::max(1, n)) return -5;                                                   \
+    if (ldb < std::max(1, n)) return -7;                                                   \
+    int info = orc_##P##potrf(uplo, n, a, lda);                                            \
+    if (info == 0) info = orc_##P##potrs(uplo, n, nrhs, a, lda, b, ldb);                   \
+    return info;                                                                           \
+  }
+ORC_ZCHOL(z, double)
+ORC_ZCHOL(c, float)
+#undef ORC_ZCHOL
 ORC_ZLU(z, double)
 ORC_ZLU(c, float)
 #undef ORC_ZLU

@@ -8,9 +8,10 @@
 // reference drivers to them lets the tests check the oracle's own LAPACK
 // restatement against the reference's driver code, bit for bit.
 //
-// The complex LU leaf and the complex GEMM and TRSM come from the oracle as
-// well (zgetrf_ and cgetrf_ are checked). Routines the checked path never
-// reaches (complex Cholesky, norms and condition estimates) abort; the Fortran ones are in ref_stubs.c. triangular.cc is
+// The complex LU and Cholesky leaves and the complex GEMM, TRSM and HERK come
+// from the oracle as well (zgetrf_, zpotrf_ and their c forms are checked).
+// Routines the checked path never reaches (norms and condition estimates)
+// abort; the Fortran ones are in ref_stubs.c. triangular.cc is
 // built too, for xTRTRI and xTRTI2 under xGETRI, and gesvx.cc and trsen.cc
 // for xGERFS and its xLACN2.
 #include <complex>
@@ -44,11 +45,7 @@ blasint GetrfLeaf(blasint m, blasint n, T* a, blasint lda, blasint* ipiv) {
 }
 template <typename T>
 blasint PotrfLeaf(bool upper, blasint n, T* a, blasint lda) {
-  if constexpr (std::is_floating_point_v<T>) {
-    return orc::PotrfLeaf<T>(upper, n, a, lda);
-  } else {
-    Unreached("complex PotrfLeaf");
-  }
+  return orc::PotrfLeaf<T>(upper, n, a, lda);
 }
 template <typename T>
 void Lacgv(blasint, T*, blasint) {
@@ -219,6 +216,16 @@ void ssyrk_(const char* u, const char* t, const blasint* n, const blasint* k,
     const int info = orc::ZtrsmF<R>(*s, *u, *t, *d, *m, *n, alpha, a, *lda, b, *ldb);     \
     if (info) hwyblas::ReportError(U "TRSM", info);                                        \
   }
+#define ORC_ZHERK(P, U, R)                                                                \
+  void P##herk_(const char* u, const char* t, const blasint* n, const blasint* k,           \
+                const R* alpha, const R* a, const blasint* lda, const R* beta, R* c,        \
+                const blasint* ldc) {                                                      \
+    const int info = orc::ZherkF<R>(*u, *t, *n, *k, *alpha, a, *lda, *beta, c, *ldc);      \
+    if (info) hwyblas::ReportError(U "HERK", info);                                        \
+  }
+ORC_ZHERK(z, "Z", double)
+ORC_ZHERK(c, "C", float)
+#undef ORC_ZHERK
 ORC_ZL3(z, "Z", double)
 ORC_ZL3(c, "C", float)
 #undef ORC_ZL3

@@ -15,7 +15,7 @@ ORC_STUB(caxpy_) ORC_STUB(ccopy_) ORC_STUB(cdotu_) ORC_STUB(ctrmm_)
 ORC_STUB(ctrmv_) ORC_STUB(ctrsv_) ORC_STUB(dzasum_) ORC_STUB(scasum_)
 ORC_STUB(zaxpy_) ORC_STUB(zcopy_) ORC_STUB(zdotu_) ORC_STUB(ztrmm_)
 ORC_STUB(ztrmv_) ORC_STUB(ztrsv_)
-ORC_STUB(cgemv_) ORC_STUB(cherk_) ORC_STUB(cscal_)
+ORC_STUB(cgemv_) ORC_STUB(cscal_)
 ORC_STUB(csscal_) ORC_STUB(cswap_) ORC_STUB(icamax_)
 ORC_STUB(izamax_) ORC_STUB(zdotc_) ORC_STUB(zdscal_)
-ORC_STUB(zgemv_) ORC_STUB(zherk_) ORC_STUB(zscal_) ORC_STUB(zswap_)
+ORC_STUB(zgemv_) ORC_STUB(zscal_) ORC_STUB(zswap_)

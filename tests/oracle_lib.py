@@ -45,6 +45,9 @@ def load_ref():
     lib.spotrf_.argtypes = [P] * 5
     lib.spotrf2_.argtypes = [P] * 5
     for pre in "zc":
+        getattr(lib, f"{pre}potrf_").argtypes = [P] * 5
+        getattr(lib, f"{pre}potrf2_").argtypes = [P] * 5
+        getattr(lib, f"{pre}herk_").argtypes = [P] * 10
         getattr(lib, f"{pre}getrf_").argtypes = [P] * 6
         getattr(lib, f"{pre}getrf2_").argtypes = [P] * 6
         getattr(lib, f"{pre}getrs_").argtypes = [P] * 9
@@ -102,7 +105,13 @@ class Oracle:
         L.orc_zrecip.argtypes = [I, P, P]
         L.orc_crecip.argtypes = [I, P, P]
         L.orc_cgemm.argtypes = [CH, CH, I, I, I, P, P, I, P, I, P, P, I]
+        L.orc_zherk.argtypes = [CH, CH, I, I, D, P, I, D, P, I]
+        L.orc_cherk.argtypes = [CH, CH, I, I, F, P, I, F, P, I]
         for pre in "zc":
+            getattr(L, f"orc_{pre}potrf").argtypes = [CH, I, P, I]
+            getattr(L, f"orc_{pre}potrf2").argtypes = [CH, I, P, I]
+            getattr(L, f"orc_{pre}potrs").argtypes = [CH, I, I, P, I, P, I]
+            getattr(L, f"orc_{pre}posv").argtypes = [CH, I, I, P, I, P, I]
             getattr(L, f"orc_{pre}getrf").argtypes = [I, I, P, I, P]
             getattr(L, f"orc_{pre}getrf2").argtypes = [I, I, P, I, P]
             getattr(L, f"orc_{pre}laswp").argtypes = [I, P, I, I, I, P, I]
@@ -266,6 +275,22 @@ class Oracle:
         return getattr(self.lib, f"orc_{self._zp(a)}gesv")(n, nrhs, ptr(a), lda, ptr(ipiv),
                                                          ptr(b), ldb)
 
+    def zpotrf(self, uplo, n, a, lda, recursive=False):
+        fn = getattr(self.lib, f"orc_{self._zp(a)}{'potrf2' if recursive else 'potrf'}")
+        return fn(_b(uplo), n, ptr(a), lda)
+
+    def zpotrs(self, uplo, n, nrhs, a, lda, b, ldb):
+        return getattr(self.lib, f"orc_{self._zp(a)}potrs")(_b(uplo), n, nrhs, ptr(a), lda,
+                                                          ptr(b), ldb)
+
+    def zposv(self, uplo, n, nrhs, a, lda, b, ldb):
+        return getattr(self.lib, f"orc_{self._zp(a)}posv")(_b(uplo), n, nrhs, ptr(a), lda,
+                                                         ptr(b), ldb)
+
+    def zherk(self, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+        return getattr(self.lib, f"orc_{self._zp(c)}herk")(_b(uplo), _b(trans), n, k, alpha,
+                                                         ptr(a), lda, beta, ptr(c), ldc)
+
     def getri(self, n, a, lda, ipiv, work, lwork):
         p = "s" if a.dtype == np.float32 else "d"
         return getattr(self.lib, f"orc_{p}getri")(n, ptr(a), lda, ptr(ipiv), ptr(work), lwork)
@@ -297,6 +322,16 @@ def ref_call_zgetrf(lib, recursive, m, n, a, lda, ipiv):
     fn = getattr(lib, f"{pre}{'getrf2' if recursive else 'getrf'}_")
     fn(ctypes.byref(ctypes.c_int(m)), ctypes.byref(ctypes.c_int(n)), ptr(a),
        ctypes.byref(ctypes.c_int(lda)), ptr(ipiv), ctypes.byref(info))
+    return info.value
+
+
+def ref_call_zpotrf(lib, recursive, uplo, n, a, lda):
+    """The reference driver's zpotrf_/cpotrf_ (and ...2_), by dtype."""
+    info = ctypes.c_int(0)
+    pre = "z" if a.dtype == np.complex128 else "c"
+    fn = getattr(lib, f"{pre}{'potrf2' if recursive else 'potrf'}_")
+    fn(ctypes.c_char_p(_b(uplo)), ctypes.byref(ctypes.c_int(n)), ptr(a),
+       ctypes.byref(ctypes.c_int(lda)), ctypes.byref(info))
     return info.value
 
 
@@ -365,6 +400,12 @@ def crand(rng, rows, cols, dtype=np.complex128):
     """Column-major complex matrix with parts uniform in [-1, 1]."""
     x = rng.uniform(-1.0, 1.0, (rows, cols)) + 1j * rng.uniform(-1.0, 1.0, (rows, cols))
     return np.asfortranarray(x.astype(dtype))
+
+
+def hpd(rng, n, dtype=np.complex128):
+    """A Hermitian positive definite matrix G G^H / n + 1e-3 I (Fortran order)."""
+    g = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return np.asfortranarray((g @ g.conj().T / n + 1e-3 * np.eye(n)).astype(dtype))
 
 
 def rand(rng, rows, cols, dtype=np.float64):

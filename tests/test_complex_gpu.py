@@ -387,3 +387,115 @@ def test_zgetrf_device_arrays_misaligned_and_errors(hb, orc):
         assert hb.zgesv("z", 4, -1, z, 4, ip, z, 4) == -2
     assert cap.errors == [("ZGETRF", 1), ("CGETRF", 2), ("ZGETRF2", 4), ("ZGETRS", 1),
                           ("CGETRS", 8), ("ZGESV", 2)]
+
+
+# --------------------------------------------------------------------------
+# Complex Cholesky family (zpotrf_, cpotrf_, ...2_, ?potrs_, ?posv_) and the
+# complex HERK it updates with, against the oracle bit for bit.
+
+def _hpd(rng, n, dtype):
+    g = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = g @ g.conj().T / n + 1e-3 * np.eye(n)
+    h += 1j * np.diag(rng.uniform(-1, 1, n))  # an imaginary diagonal is ignored
+    return np.asfortranarray(h.astype(dtype))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("n", [1, 7, 32, 33, 64, 65, 130, 257, 600])
+def test_zpotrf_bitexact(hb, orc, p, uplo, recursive, n):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(n * 3 + (uplo == "U"))
+    lda = n + 2
+    a = crand(rng, lda, n, dtype)  # the other triangle and the padding are garbage
+    a[:n, :] = np.where(np.tril(np.ones((n, n), bool)) if uplo == "L"
+                        else np.triu(np.ones((n, n), bool)), _hpd(rng, n, dtype), a[:n, :])
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    i1 = hb.zpotrf(p, uplo, n, a1, lda, recursive=recursive)
+    i2 = orc.zpotrf(uplo, n, a2, lda, recursive=recursive)
+    assert i1 == i2 == 0
+    assert same_bits(creal(a1), creal(a2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+def test_zpotrf_not_positive_definite(hb, orc, p, uplo):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(17)
+    n = 200
+    for bad in (1, 33, 70, 200):
+        a = _hpd(rng, n, dtype)
+        a[bad - 1, bad - 1] = -1.0
+        a1, a2 = a.copy(order="F"), a.copy(order="F")
+        i1 = hb.zpotrf(p, uplo, n, a1, n)
+        i2 = orc.zpotrf(uplo, n, a2, n)
+        assert i1 == i2 and 0 < i1 <= bad
+        assert same_bits(creal(a1), creal(a2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "C"])
+@pytest.mark.parametrize("n,k,alpha,beta", [(45, 300, -0.75, 0.5), (70, 600, 1.0, 1.0),
+                                            (33, 20, -1.0, 0.0), (64, 0, 2.0, 0.25),
+                                            (40, 10, 0.0, -2.0)])
+def test_zherk_bitexact(hb, orc, p, uplo, trans, n, k, alpha, beta):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(n + k)
+    rows = n if trans == "N" else k
+    a = crand(rng, max(rows, 1), max(k if trans == "N" else n, 1), dtype)
+    c = crand(rng, n, n, dtype)
+    c1, c2 = c.copy(order="F"), c.copy(order="F")
+    hb.zherk(p, uplo, trans, n, k, alpha, a, max(rows, 1), beta, c1, n)
+    assert orc.zherk(uplo, trans, n, k, alpha, a, max(rows, 1), beta, c2, n) == 0
+    assert same_bits(creal(c1), creal(c2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+def test_zpotrs_zposv_bitexact(hb, orc, p, uplo):
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(23)
+    n, nrhs = 300, 4
+    a = _hpd(rng, n, dtype)
+    b = crand(rng, n, nrhs, dtype)
+    f = a.copy(order="F")
+    assert orc.zpotrf(uplo, n, f, n) == 0
+    b1, b2 = b.copy(order="F"), b.copy(order="F")
+    assert hb.zpotrs(p, uplo, n, nrhs, f, n, b1, n) == 0
+    assert orc.zpotrs(uplo, n, nrhs, f, n, b2, n) == 0
+    assert same_bits(creal(b1), creal(b2))
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    b1, b2 = b.copy(order="F"), b.copy(order="F")
+    assert hb.zposv(p, uplo, n, nrhs, a1, n, b1, n) == 0
+    assert orc.zposv(uplo, n, nrhs, a2, n, b2, n) == 0
+    assert same_bits(creal(a1), creal(a2)) and same_bits(creal(b1), creal(b2))
+
+
+def test_zpotrf_device_misaligned_and_errors(hb, orc):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(29)
+    n = 400
+    a = _hpd(rng, n, np.complex128)
+    want = a.copy(order="F")
+    assert orc.zpotrf("L", n, want, n) == 0
+    flat = np.zeros(2 * n * n + 1)
+    flat[1:] = a.ravel(order="F").view(np.float64)
+    ta = torch.from_numpy(flat).cuda()
+    assert hb.zpotrf("z", "L", n, ta.data_ptr() + 8, n) == 0
+    got = ta.cpu().numpy()[1:].view(np.complex128).reshape(n, n).T
+    assert same_bits(creal(got), creal(want))
+    z = np.zeros((4, 4), np.complex128, order="F")
+    assert hb.zpotrf("z", "L", 0, z, 1) == 0
+    with hb.ErrorCapture() as cap:
+        assert hb.zpotrf("z", "X", 4, z, 4) == -1
+        assert hb.zpotrf("c", "U", 4, z.astype(np.complex64), 3, recursive=True) == -4
+        assert hb.zposv("z", "L", 4, -1, z, 4, z, 4) == -3
+        assert hb.zpotrs("c", "U", 4, 1, z.astype(np.complex64), 4,
+                         z.astype(np.complex64), 2) == -7
+        hb.zherk("z", "L", "T", 4, 4, 1.0, z, 4, 1.0, z, 4)
+        hb.zherk("c", "U", "N", 4, 4, 1.0, z.astype(np.complex64), 3, 1.0,
+                 z.astype(np.complex64), 4)
+    assert cap.errors == [("ZPOTRF", 1), ("CPOTRF2", 4), ("ZPOSV", 3), ("CPOTRS", 7),
+                          ("ZHERK", 2), ("CHERK", 7)]

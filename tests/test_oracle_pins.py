@@ -1028,3 +1028,77 @@ def test_zgetrf_tiny_pivots_golden(orc, dtype, recursive, n):
     assert np.array_equal(ipiv, np.arange(1, n + 1))
     for i in range(1, n):
         assert a[i, 0] == np.ldexp(rt(1), -min(i, 20)), i
+
+
+# --------------------------------------------------------------------------
+# Complex Cholesky (zpotrf_, cpotrf_): the reference's own potrf.cc at
+# std::complex on the oracle's complex leaf, HERK, TRSM and GEMM, against the
+# oracle's restatement of the drivers; then the reference tests' checks
+# (tests/lapack/potrf_test.cc:55-120): residual and the non-positive minor.
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("n", [1, 5, 32, 33, 64, 65, 100, 150, 257])
+def test_zpotrf_matches_reference_driver(orc, ref_drivers, dtype, uplo, recursive, n):
+    from tests.oracle_lib import hpd, ref_call_zpotrf
+    rng = np.random.default_rng(n * 7 + (uplo == "U"))
+    lda = n + 2
+    a = np.zeros((lda, n), dtype, order="F")
+    a[:n, :] = hpd(rng, n, dtype)
+    a[:n, :] += 1j * np.diag(rng.uniform(-1, 1, n)).astype(dtype)  # ignored imaginary diagonal
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    i1 = orc.zpotrf(uplo, n, a1, lda, recursive=recursive)
+    i2 = ref_call_zpotrf(ref_drivers, recursive, uplo, n, a2, lda)
+    assert i1 == i2 == 0
+    assert same_bits(creal(a1), creal(a2)), first_diff(creal(a1), creal(a2))
+    f = np.triu(a1[:n]) if uplo == "U" else np.tril(a1[:n])
+    prod = f.conj().T @ f if uplo == "U" else f @ f.conj().T
+    h = a[:n].astype(np.complex128)
+    h[np.diag_indices(n)] = h.diagonal().real
+    eps = np.finfo(np.float64 if dtype == np.complex128 else np.float32).eps
+    assert np.abs(prod - h).max() <= 50 * n * eps * np.abs(h).max()
+    assert np.all(f.diagonal().imag == 0)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("recursive", [False, True])
+def test_zpotrf_not_positive_definite(orc, ref_drivers, dtype, uplo, recursive):
+    from tests.oracle_lib import hpd, ref_call_zpotrf
+    rng = np.random.default_rng(4)
+    n = 120
+    for bad in (1, 40, 77, 120):
+        a = hpd(rng, n, dtype)
+        a[bad - 1, bad - 1] = -1.0
+        a1, a2 = a.copy(order="F"), a.copy(order="F")
+        i1 = orc.zpotrf(uplo, n, a1, n, recursive=recursive)
+        i2 = ref_call_zpotrf(ref_drivers, recursive, uplo, n, a2, n)
+        assert i1 == i2 and 0 < i1 <= bad
+        assert same_bits(creal(a1), creal(a2))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "C"])
+def test_zherk_against_numpy(orc, dtype, uplo, trans):
+    """The oracle's HERK is alpha op(A) op(A)^H + beta C on the triangle with a
+    real diagonal, the other triangle untouched (numerically, in complex128)."""
+    from tests.oracle_lib import crand
+    rng = np.random.default_rng(8)
+    n, k = 45, 300
+    a = crand(rng, n if trans == "N" else k, k if trans == "N" else n, dtype)
+    c = crand(rng, n, n, dtype)
+    c1 = c.copy(order="F")
+    assert orc.zherk(uplo, trans, n, k, -0.75, a, a.shape[0], 0.5, c1, n) == 0
+    opa = a.astype(np.complex128) if trans == "N" else a.astype(np.complex128).conj().T
+    h = c.astype(np.complex128)
+    h[np.diag_indices(n)] = h.diagonal().real
+    want = -0.75 * opa @ opa.conj().T + 0.5 * h
+    tri = np.tril(np.ones((n, n), bool)) if uplo == "L" else np.triu(np.ones((n, n), bool))
+    eps = np.finfo(np.float64 if dtype == np.complex128 else np.float32).eps
+    assert np.abs(c1[tri] - want[tri]).max() <= 20 * k * eps
+    assert np.array_equal(c1[~tri], c[~tri])
+    assert np.all(c1.diagonal().imag == 0)
+    with pytest.raises(AssertionError):
+        assert orc.zherk(uplo, "T", n, k, 1.0, a, a.shape[0], 1.0, c1, n) == 0
