@@ -75,7 +75,7 @@ def parse():
                         "records through torch.profiler)")
     p.add_argument("--case", default=None,
                    choices=["leaf", "getrf", "gesv", "gesv-mixed", "trtri", "getri", "trmm",
-                            "zgemm"],
+                            "zgemm", "zgetrf", "zpotrf"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
                         "gesv-n; dtrtri, dgetri, dtrmm or zgemm at n; each after one "
@@ -647,8 +647,27 @@ def run_widened(torch, hb, stream):
         za, zb, zc = colmajor(nz, nz, dt), colmajor(nz, nz, dt), colmajor(nz, nz, dt)
         ms = best(lambda: hb.zgemm(p, "N", "N", nz, nz, nz, 1.0, za, nz, zb, nz, 0.0, zc, nz))
         out[p + "gemm NN"] = {"n": nz, "ms": ms, "tflops": 8 * nz ** 3 / (ms * 1e-3) / 1e12}
+        # Complex LU of a diagonally dominant matrix and Cholesky of a
+        # Hermitian one with a dominant diagonal (fresh copies, copy untimed).
+        za.diagonal().add_(2.0 * nz ** 0.5)
+        herm = (zb + zb.conj().T) / 2
+        herm.diagonal().add_(2.0 * nz ** 0.5)
+        herm = herm.T.contiguous().T
+        zp = torch.zeros(nz, dtype=torch.int32, device="cuda")
+        for name, src, call, flops in (
+                (p + "getrf", za, lambda x: hb.zgetrf(p, nz, nz, x, nz, zp), 8 * nz ** 3 / 3),
+                (p + "potrf L", herm, lambda x: hb.zpotrf(p, "L", nz, x, nz), 4 * nz ** 3 / 3)):
+            times = []
+            for _ in range(3):
+                x = src.clone().T.contiguous().T
+                torch.cuda.synchronize()
+                times.append(timed(torch, stream, lambda: call(x), 1))
+            ms = min(times[1:])
+            out[name] = {"n": nz, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+        del za, zb, zc, herm
     out["note"] = ("useful flops: trmm n^3, symm/syr2k 2n^3, gemmtr n^3, trtri n^3/3, "
-                   "getri 4n^3/3, complex gemm 8n^3")
+                   "getri 4n^3/3, complex gemm 8n^3, complex getrf 8n^3/3, complex potrf "
+                   "4n^3/3")
     return out
 
 
@@ -761,13 +780,16 @@ def run_case(args):
     n = args.gesv_n
     g = torch.Generator(device="cuda").manual_seed(1)
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
-    if args.case in ("trtri", "getri", "trmm", "zgemm"):
+    if args.case in ("trtri", "getri", "trmm", "zgemm", "zgetrf", "zpotrf"):
         n = args.n
         ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
-        dt = torch.complex128 if args.case == "zgemm" else torch.float64
+        dt = torch.complex128 if args.case[0] == "z" else torch.float64
         a0 = torch.rand(n * n, dtype=dt, device="cuda", generator=g) * 2 - 1
-        if args.case in ("trtri", "getri"):
+        if args.case in ("trtri", "getri", "zgetrf", "zpotrf"):
             a0.view(n, n).diagonal().add_(2.0 * n ** 0.5)
+        if args.case == "zpotrf":
+            a0 = ((a0.view(n, n) + a0.view(n, n).conj().T) / 2).contiguous().view(-1)
+        if args.case in ("trtri", "getri"):
             hb.dgetrf(n, n, a0, n, ipiv)
         other = torch.rand(n * n, dtype=dt, device="cuda", generator=g) * 2 - 1
         work = torch.zeros(64 * n, dtype=torch.float64, device="cuda")
@@ -777,6 +799,10 @@ def run_case(args):
             call = lambda a: hb.getri("d", n, a, n, ipiv, work, 64 * n)
         elif args.case == "trmm":
             call = lambda a: hb.trmm("d", "L", "L", "N", "N", n, n, 1.0, other, n, a, n)
+        elif args.case == "zgetrf":
+            call = lambda a: hb.zgetrf("z", n, n, a, n, ipiv)
+        elif args.case == "zpotrf":
+            call = lambda a: hb.zpotrf("z", "L", n, a, n)
         else:
             c = torch.zeros_like(a0)
             call = lambda a: hb.zgemm("z", "N", "N", n, n, n, 1.0, a, n, other, n, 0.0, c, n)
