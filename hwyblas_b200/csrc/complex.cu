@@ -75,7 +75,66 @@ struct ZParams {
   // grid) that cross the diagonal merge as its MergeTile does, with the
   // diagonal's imaginary part dropped when real_diag is set.
   int part, real_diag, tmr, tnr;
+  // Split over KC chunks: CTA z computes chunk z alone and stores its
+  // alpha * ab to partial[(z n + j) m + i] (interleaved); ZSplitMergeKernel
+  // then merges the chunks in order.
+  R* partial;
 };
+
+// Merges one chunk's t = alpha * ab into element (i, j) of C as the
+// reference does (first: the first KC chunk, which applies beta; later chunks
+// add with beta 1): r, r + C or r + beta C in the micro-kernel's rounding,
+// or the MergeTile rule for HERK tiles crossing the diagonal. Elements
+// outside the triangle of a HERK are left alone.
+template <typename R>
+__device__ __forceinline__ void ZMergeElement(const ZParams<R>& p, int i, int j, bool first,
+                                              R t_re, R t_im) {
+  R* ce = p.c + 2 * (i + j * p.ldc);
+  if (p.part != 0) {
+    if (p.part == 1 ? i < j : i > j) return;
+    const int i0 = i / p.tmr * p.tmr, j0 = j / p.tnr * p.tnr;
+    const int il = min(i0 + p.tmr, p.m) - 1, jl = min(j0 + p.tnr, p.n) - 1;
+    if (!(p.part == 1 ? i0 > jl : il < j0)) {
+      // Crossing tile (src/gemm-inl.h:110-130): v = alpha ab, then v += beta
+      // * c as the C++ runtime's complex product and sum (beta 1 after the
+      // first chunk); on the diagonal with real_diag, v and c lose their
+      // imaginary parts first.
+      const R br = first ? p.beta_re : R(1), bi = first ? p.beta_im : R(0);
+      const bool bz = br == R(0) && bi == R(0);
+      R vr = t_re, vi = t_im;
+      if (p.real_diag && i == j) {
+        vi = R(0);
+        if (!bz) {
+          const R c0 = ce[0];
+          vr = Add(vr, Sub(Mul(br, c0), Mul(bi, R(0))));
+          vi = Add(vi, Add(Mul(br, R(0)), Mul(bi, c0)));
+        }
+      } else if (!bz) {
+        const R c0 = ce[0], c1 = ce[1];
+        vr = Add(vr, Sub(Mul(br, c0), Mul(bi, c1)));
+        vi = Add(vi, Add(Mul(br, c1), Mul(bi, c0)));
+      }
+      ce[0] = vr;
+      ce[1] = vi;
+      return;
+    }
+  }
+  const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
+  const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
+  if (first && beta_zero) {
+    ce[0] = t_re;
+    ce[1] = t_im;
+  } else if (!first || beta_one) {
+    ce[0] = Add(t_re, ce[0]);
+    ce[1] = Add(t_im, ce[1]);
+  } else {
+    const R c0 = ce[0], c1 = ce[1];
+    const R b_re = Sub(Mul(c0, p.beta_re), Mul(c1, p.beta_im));
+    const R b_im = Add(Mul(c1, p.beta_re), Mul(c0, p.beta_im));
+    ce[0] = Add(t_re, b_re);
+    ce[1] = Add(t_im, b_im);
+  }
+}
 
 template <typename R>
 struct Vec2;
@@ -127,8 +186,9 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int q = 0; q < 4; ++q) rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
-  const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
-  const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
+  const bool split = p.partial != nullptr;
+  const int kbeg = split ? blockIdx.z * kZChunk : 0;
+  const int kend = split ? min(p.k, kbeg + kZChunk) : p.k;
   // Consecutive threads copy consecutive addresses: along rows of op(A) when
   // A is not transposed, else along k; along k of op(B) when B is not
   // transposed, else along its columns.
@@ -153,10 +213,10 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   const R sa_sign = p.a.conj ? R(-1) : R(1), sb_sign = p.b.conj ? R(-1) : R(1);
-  issue(0, 0);
+  issue(kbeg, 0);
   int buf = 0;
-  for (int k0 = 0; k0 < p.k; k0 += kZK, buf ^= 1) {
-    if (k0 + kZK < p.k) {
+  for (int k0 = kbeg; k0 < kend; k0 += kZK, buf ^= 1) {
+    if (k0 + kZK < kend) {
       issue(k0 + kZK, buf ^ 1);
       asm volatile("cp.async.wait_group 1;" ::: "memory");
     } else {
@@ -165,9 +225,9 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
     __syncthreads();
     const V* ca = sa + buf * kZK * kZM;
     const V* cb = sb + buf * kZK * kZN;
-    const int kend = min(kZK, p.k - k0);
+    const int kslice = min(kZK, kend - k0);
 #pragma unroll 2
-    for (int kk = 0; kk < kend; ++kk) {
+    for (int kk = 0; kk < kslice; ++kk) {
       R ar[4], ai[4], br[4], bi[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -189,7 +249,7 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
         }
     }
     __syncthreads();
-    if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= p.k) {
+    if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= kend) {
       const bool first = k0 < kZChunk;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
@@ -202,50 +262,30 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
           if (i >= p.m || j >= p.n) continue;
           const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
           const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
-          R* ce = p.c + 2 * (i + j * p.ldc);
-          if (p.part != 0) {
-            if (p.part == 1 ? i < j : i > j) continue;
-            const int i0 = i / p.tmr * p.tmr, j0 = j / p.tnr * p.tnr;
-            const int il = min(i0 + p.tmr, p.m) - 1, jl = min(j0 + p.tnr, p.n) - 1;
-            if (!(p.part == 1 ? i0 > jl : il < j0)) {
-              // Crossing tile (src/gemm-inl.h:110-130): v = alpha ab, then
-              // v += beta * c as the C++ runtime's complex product and sum
-              // (beta 1 after the first chunk); on the diagonal with
-              // real_diag, v and c lose their imaginary parts first.
-              const R br = first ? p.beta_re : R(1), bi = first ? p.beta_im : R(0);
-              const bool bz = br == R(0) && bi == R(0);
-              R vr = t_re, vi = t_im;
-              if (p.real_diag && i == j) {
-                vi = R(0);
-                if (!bz) {
-                  const R c0 = ce[0];
-                  vr = Add(vr, Sub(Mul(br, c0), Mul(bi, R(0))));
-                  vi = Add(vi, Add(Mul(br, R(0)), Mul(bi, c0)));
-                }
-              } else if (!bz) {
-                const R c0 = ce[0], c1 = ce[1];
-                vr = Add(vr, Sub(Mul(br, c0), Mul(bi, c1)));
-                vi = Add(vi, Add(Mul(br, c1), Mul(bi, c0)));
-              }
-              ce[0] = vr;
-              ce[1] = vi;
-              continue;
-            }
-          }
-          if (first && beta_zero) {
-            ce[0] = t_re;
-            ce[1] = t_im;
-          } else if (!first || beta_one) {
-            ce[0] = Add(t_re, ce[0]);
-            ce[1] = Add(t_im, ce[1]);
+          if (split) {
+            R* pe = p.partial + 2 * ((static_cast<long long>(blockIdx.z) * p.n + j) * p.m + i);
+            pe[0] = t_re;
+            pe[1] = t_im;
           } else {
-            const R c0 = ce[0], c1 = ce[1];
-            const R b_re = Sub(Mul(c0, p.beta_re), Mul(c1, p.beta_im));
-            const R b_im = Add(Mul(c1, p.beta_re), Mul(c0, p.beta_im));
-            ce[0] = Add(t_re, b_re);
-            ce[1] = Add(t_im, b_im);
+            ZMergeElement(p, i, j, first, t_re, t_im);
           }
         }
+    }
+  }
+}
+
+// The in-order merge of a split complex GEMM: per element, chunk 0 with the
+// first-chunk rule, then every later chunk (ZMergeElement).
+template <typename R>
+__global__ void ZSplitMergeKernel(ZParams<R> p, int nchunks) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  const long long total = static_cast<long long>(p.m) * p.n;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % p.m), j = static_cast<int>(e / p.m);
+    for (int c = 0; c < nchunks; ++c) {
+      const R* pe = p.partial + 2 * ((static_cast<long long>(c) * p.n + j) * p.m + i);
+      ZMergeElement(p, i, j, c == 0, pe[0], pe[1]);
     }
   }
 }
@@ -894,6 +934,26 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
                          ZSmemBytes<R>());
     configured = true;
   }
+  // Few tiles and several KC chunks: the chunks run in parallel (each one's
+  // alpha * ab does not depend on C) and are merged in order afterwards,
+  // which gives the same C as merging them one after another.
+  const long long tiles = static_cast<long long>(grid.x) * grid.y;
+  const int nchunks = (k + kZChunk - 1) / kZChunk;
+  const size_t pbytes = 2 * sizeof(R) * static_cast<size_t>(nchunks) * m * n;
+  p.partial = nullptr;
+  if (nchunks >= 2 && tiles * 2 <= Ctx().num_sms && pbytes <= (size_t(1) << 30)) {
+    p.partial = static_cast<R*>(Workspace(kWsSplitK, pbytes));
+    if (p.partial == nullptr) return;
+    ZgemmKernel<R><<<dim3(grid.x, grid.y, nchunks), 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
+    CountLaunch();
+    if (LaunchFailed("complex gemm (split)")) return;
+    const long long total = static_cast<long long>(m) * n;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 8));
+    ZSplitMergeKernel<R><<<blocks, 256, 0, Ctx().stream>>>(p, nchunks);
+    CountLaunch();
+    LaunchFailed("complex gemm split merge");
+    return;
+  }
   ZgemmKernel<R><<<grid, 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
   CountLaunch();
   LaunchFailed("complex gemm");
@@ -1279,6 +1339,19 @@ void ZPotrf(bool recursive, bool upper, int n, R* a, int lda, int* info) {
   const int nb = 64;
   if (recursive || nb >= n) {
     ZPotrf2Rec<R>(upper, n, a, lda, info, 0);
+    ctx.guard = saved;
+    return;
+  }
+  // The block updates have few tiles and long k, so the GEMMs split over
+  // their KC chunks; their largest partial buffer is reserved up front
+  // (growing it inside the loop would synchronize at every step).
+  size_t split_bytes = 0;
+  for (int j = 0; j < n; j += nb) {
+    const int jb = std::min(nb, n - j);
+    const size_t chunks = static_cast<size_t>((j + kZChunk - 1) / kZChunk);
+    split_bytes = std::max(split_bytes, 2 * sizeof(R) * chunks * std::max(n - j, jb) * jb);
+  }
+  if (split_bytes > 0 && Workspace(kWsSplitK, split_bytes) == nullptr) {
     ctx.guard = saved;
     return;
   }

@@ -499,3 +499,25 @@ def test_zpotrf_device_misaligned_and_errors(hb, orc):
                  z.astype(np.complex64), 4)
     assert cap.errors == [("ZPOTRF", 1), ("CPOTRF2", 4), ("ZPOSV", 3), ("CPOTRS", 7),
                           ("ZHERK", 2), ("CHERK", 7)]
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+def test_complex_split_chunks_bitexact(hb, orc, p):
+    """Few output tiles and many KC chunks: the chunks run in parallel and
+    merge in order, which must give the sequential result (GEMM with a
+    general beta, and HERK on a triangle)."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(41)
+    m, n, k = 100, 70, 3000
+    a, b, c = crand(rng, m, k, dtype), crand(rng, k, n, dtype), crand(rng, m, n, dtype)
+    c1, c2 = c.copy(order="F"), c.copy(order="F")
+    hb.zgemm(p, "N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, 0.3 - 0.2j, c1, m)
+    assert orc.zgemm("N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, 0.3 - 0.2j, c2, m) == 0
+    assert same_bits(creal(c1), creal(c2))
+    for uplo in ("L", "U"):
+        h = crand(rng, 64, 4096, dtype)
+        d = crand(rng, 64, 64, dtype)
+        d1, d2 = d.copy(order="F"), d.copy(order="F")
+        hb.zherk(p, uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d1, 64)
+        assert orc.zherk(uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d2, 64) == 0
+        assert same_bits(creal(d1), creal(d2))
