@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cstdio>
 
+#include <cooperative_groups.h>
+
 #include "device.cuh"
 #include "internal.h"
 #include "ref_order.cuh"
@@ -566,9 +568,14 @@ __device__ __forceinline__ void ZAxpyRef(R& yr, R& yi, R ar, R ai, R xr, R xi, i
   }
 }
 
-template <typename R>
+// kCluster: the P CTAs form one thread-block cluster and exchange their
+// candidates through distributed shared memory (each publishes into its own
+// shared slot, one cluster barrier, then every CTA reads the P slots)
+// instead of global slots and polling.
+template <typename R, bool kCluster>
 __global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p) {
   constexpr int W = kZLeafW;
+  __shared__ R s_slot[2 * kZSlot];  // kCluster: own slot per parity
   extern __shared__ __align__(16) unsigned char zleaf_smem[];
   R* sp = reinterpret_cast<R*>(zleaf_smem);  // [w][rows][2]
   __shared__ R s_piv[2 * W], s_rowj[2 * W];
@@ -602,6 +609,8 @@ __global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p
       }
     }
   }
+  // kCluster: every CTA of the cluster is running before any remote access.
+  if constexpr (kCluster) cooperative_groups::this_cluster().sync();
   __syncthreads();
 
   for (int j = 0; j < w; ++j) {
@@ -639,7 +648,8 @@ __global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p
     __syncthreads();
     // (b) exchange: slot = (|a|, row, candidate row, row j if owned).
     const int ci = s_p;
-    R* slot = P == 1 ? s_cand : p.xchg + (par * P + cta) * kZSlot;
+    R* slot = P == 1 ? s_cand
+                     : (kCluster ? s_slot + par * kZSlot : p.xchg + (par * P + cta) * kZSlot);
     if (threadIdx.x == 0) {
       slot[0] = s_wv[0];
       slot[1] = static_cast<R>(ci == 0x7fffffff ? -1 : ci);
@@ -649,7 +659,17 @@ __global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p
       slot[2 + threadIdx.x] = (ci != 0x7fffffff) ? el(c, ci - r0)[part] : R(0);
       if (j >= r0 && j < r1) slot[2 + 2 * W + threadIdx.x] = el(c, j - r0)[part];
     }
-    if (P > 1) {
+    if (kCluster && P > 1) {
+      // A parity's slot is rewritten two steps later, after the next
+      // cluster barrier, which every CTA reaches only after reading it.
+      cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+      cluster.sync();
+      for (int idx = threadIdx.x; idx < P * kZSlot; idx += blockDim.x) {
+        const int q = idx / kZSlot, e = idx - q * kZSlot;
+        const R* peer = cluster.map_shared_rank(s_slot, q);
+        s_cand[idx] = peer[par * kZSlot + e];
+      }
+    } else if (P > 1) {
       // Release the slot under the step's tag; poll the P tags (bounded) and
       // copy every slot. A parity is rewritten two steps later, after every
       // CTA has published the next step and so has read this one.
@@ -752,6 +772,8 @@ __global__ void __launch_bounds__(kZLeafThreads) ZGetrfLeafKernel(ZLeafArgs<R> p
     }
   }
   __syncthreads();
+  // kCluster: no CTA exits while a peer may still read its slot.
+  if constexpr (kCluster) cooperative_groups::this_cluster().sync();
   for (int c = 0; c < w; ++c) {
     for (int lr = threadIdx.x; lr < r1 - r0; lr += blockDim.x) {
       R* dst = p.a + 2 * ((r0 + lr) + c * p.lda);
@@ -1159,9 +1181,34 @@ void ZGetrfLeaf(int m, int n, R* a, int lda, int* ipiv, int* info, int info_base
   const int rows = (m + P - 1) / P;
   const size_t smem = 2 * sizeof(R) * static_cast<size_t>(w) * rows;
   static bool configured = false;
+  static int max_cluster = 0;
   if (!configured) {
-    cudaFuncSetAttribute(ZGetrfLeafKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(2 * sizeof(R) * kZLeafW * kZLeafMaxRows));
+    const int smem_max = static_cast<int>(2 * sizeof(R) * kZLeafW * kZLeafMaxRows);
+    cudaFuncSetAttribute(ZGetrfLeafKernel<R, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ZGetrfLeafKernel<R, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+    cudaFuncSetAttribute(ZGetrfLeafKernel<R, true>,
+                         cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kZLeafThreads);
+    cfg.dynamicSmemBytes = smem_max;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 16;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int size = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(
+            &size, reinterpret_cast<const void*>(ZGetrfLeafKernel<R, true>), &cfg) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      size = 0;
+    }
+    max_cluster = std::min(size, 16);
     configured = true;
   }
   ZLeafArgs<R> args;
@@ -1179,14 +1226,29 @@ void ZGetrfLeaf(int m, int n, R* a, int lda, int* ipiv, int* info, int info_base
   if (args.xchg == nullptr) return;
   args.tags = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(args.xchg) + slot_bytes);
   args.timeout_flag = ctx.dev_status;
-  if (P > 1) {
+  if (P > 1 && P <= max_cluster) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P);
+    cfg.blockDim = dim3(kZLeafThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx.stream;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = P;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    Failed(cudaLaunchKernelEx(&cfg, ZGetrfLeafKernel<R, true>, args),
+           "complex getrf leaf (cluster)");
+  } else if (P > 1) {
     cudaMemsetAsync(args.tags, 0, sizeof(unsigned int) * 2 * P, ctx.stream);
     void* kargs[] = {&args};
-    Failed(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(ZGetrfLeafKernel<R>), P,
+    Failed(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(ZGetrfLeafKernel<R, false>), P,
                                        kZLeafThreads, kargs, smem, ctx.stream),
            "complex getrf leaf (cooperative)");
   } else {
-    ZGetrfLeafKernel<R><<<1, kZLeafThreads, smem, ctx.stream>>>(args);
+    ZGetrfLeafKernel<R, false><<<1, kZLeafThreads, smem, ctx.stream>>>(args);
   }
   CountLaunch();
   LaunchFailed("complex getrf leaf");
