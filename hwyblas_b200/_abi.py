@@ -32,6 +32,8 @@ PROTOTYPES = {
     **{f"{p}potrs_": (None, [C, PI, PI, P, PI, P, PI, PI]) for p in "zc"},
     **{f"{p}posv_": (None, [C, PI, PI, P, PI, P, PI, PI]) for p in "zc"},
     **{f"{p}herk_": (None, [C, C, PI, PI, P, P, PI, P, P, PI]) for p in "zc"},
+    "cblas_zherk": (None, [I, I, I, I, I, ctypes.c_double, P, I, ctypes.c_double, P, I]),
+    "cblas_cherk": (None, [I, I, I, I, I, ctypes.c_float, P, I, ctypes.c_float, P, I]),
     **{f"{p}symm_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}syr2k_": (None, [C, C, PI, PI, P, P, PI, P, PI, P, P, PI]) for p in "ds"},
     **{f"{p}{r}_": (None, [C, C, C, PI, PI, P, P, PI, P, PI, P, P, PI])

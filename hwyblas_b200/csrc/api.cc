@@ -1759,6 +1759,40 @@ HB_ZCHOL(z, "Z", double)
 HB_ZCHOL(c, "C", float)
 #undef HB_ZCHOL
 
+// CBLAS complex HERK (src/cblas.cc:610-630, 1825-1841): row-major flips the
+// triangle and swaps N and C (an invalid T stays invalid); error positions
+// are the CBLAS argument numbers.
+extern "C++" {
+template <typename R>
+static void CblasZherk(const char* name, const char* routine, CBLAS_LAYOUT layout,
+                       CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans, hwyblas_int n, hwyblas_int k,
+                       R alpha, const void* a, hwyblas_int lda, R beta, void* c,
+                       hwyblas_int ldc) {
+  if (!hb::ValidLayout(name, layout)) return;
+  char uc = hb::UploChar(uplo), tc = hb::TransChar(trans);
+  if (layout == CblasRowMajor) {
+    uc = hb::FlipUplo(uc);
+    if (tc == 'N') tc = 'C';
+    else if (tc == 'C') tc = 'N';
+  }
+  hb::CblasScope scope(name, {2, 3, 4, 5, 6, 7, 8, 9, 10, 11});
+  ZherkEntry<R>(routine, &uc, &tc, &n, &k, &alpha, static_cast<const R*>(a), &lda, &beta,
+                static_cast<R*>(c), &ldc);
+}
+}  // extern "C++"
+HWYBLAS_API void cblas_zherk(CBLAS_LAYOUT layout, CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans,
+                             hwyblas_int n, hwyblas_int k, double alpha, const void* a,
+                             hwyblas_int lda, double beta, void* c, hwyblas_int ldc) {
+  CblasZherk<double>("cblas_zherk", "ZHERK", layout, uplo, trans, n, k, alpha, a, lda, beta,
+                     c, ldc);
+}
+HWYBLAS_API void cblas_cherk(CBLAS_LAYOUT layout, CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans,
+                             hwyblas_int n, hwyblas_int k, float alpha, const void* a,
+                             hwyblas_int lda, float beta, void* c, hwyblas_int ldc) {
+  CblasZherk<float>("cblas_cherk", "CHERK", layout, uplo, trans, n, k, alpha, a, lda, beta,
+                    c, ldc);
+}
+
 HWYBLAS_API void spotrf_(const char* uplo, const hwyblas_int* n, float* a,
                          const hwyblas_int* lda, hwyblas_int* info) {
   PotrfEntry<float>(false, "SPOTRF", uplo, n, a, lda, info);

@@ -577,6 +577,14 @@ HWYBLAS_API void cblas_ctrsm(const CBLAS_LAYOUT layout, const CBLAS_SIDE side,
                              const CBLAS_DIAG diag, const hwyblas_int m, const hwyblas_int n,
                              const void* alpha, const void* a, const hwyblas_int lda, void* b,
                              const hwyblas_int ldb);
+/* CBLAS complex HERK (src/cblas.cc:1825-1841): row-major flips the triangle
+ * and swaps N and C. */
+HWYBLAS_API void cblas_zherk(CBLAS_LAYOUT layout, CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans,
+                             hwyblas_int n, hwyblas_int k, double alpha, const void* a,
+                             hwyblas_int lda, double beta, void* c, hwyblas_int ldc);
+HWYBLAS_API void cblas_cherk(CBLAS_LAYOUT layout, CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans,
+                             hwyblas_int n, hwyblas_int k, float alpha, const void* a,
+                             hwyblas_int lda, float beta, void* c, hwyblas_int ldc);
 HWYBLAS_API void cblas_zgemm(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE transa,
                              const CBLAS_TRANSPOSE transb, const hwyblas_int m,
                              const hwyblas_int n, const hwyblas_int k, const void* alpha,

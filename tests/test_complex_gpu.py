@@ -521,3 +521,42 @@ def test_complex_split_chunks_bitexact(hb, orc, p):
         hb.zherk(p, uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d1, 64)
         assert orc.zherk(uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d2, 64) == 0
         assert same_bits(creal(d1), creal(d2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["U", "L"])
+@pytest.mark.parametrize("trans", ["N", "C"])
+def test_cblas_zherk_layouts(hb, orc, p, uplo, trans):
+    """Row-major CBLAS HERK is the column-major HERK of the transposed
+    storage with the other triangle and N <-> C (src/cblas.cc:610-630)."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(51)
+    n, k = 70, 300
+    L = hb.lib()
+    fn = L.cblas_zherk if p == "z" else L.cblas_cherk
+    cu = hb.CblasUpper if uplo == "U" else hb.CblasLower
+    ct = hb.CblasNoTrans if trans == "N" else hb.CblasConjTrans
+    rows, cols = (n, k) if trans == "N" else (k, n)
+    a = crand(rng, rows, cols, dtype)
+    c = crand(rng, n, n, dtype)
+    # Column-major.
+    c1, c2 = c.copy(order="F"), c.copy(order="F")
+    fn(hb.CblasColMajor, cu, ct, n, k, -0.5, a.ctypes.data, rows, 0.25, c1.ctypes.data, n)
+    assert orc.zherk(uplo, trans, n, k, -0.5, a, rows, 0.25, c2, n) == 0
+    assert same_bits(creal(c1), creal(c2))
+    # Row-major: the same storage read as the transpose.
+    arow = np.ascontiguousarray(a)
+    crow = np.ascontiguousarray(c)
+    fn(hb.CblasRowMajor, cu, ct, n, k, -0.5, arow.ctypes.data, cols, 0.25, crow.ctypes.data, n)
+    want = np.asfortranarray(c.T)
+    other = "L" if uplo == "U" else "U"
+    flip = "C" if trans == "N" else "N"
+    assert orc.zherk(other, flip, n, k, -0.5, np.asfortranarray(a.T), cols, 0.25, want, n) == 0
+    assert same_bits(creal(crow.T), creal(want))
+    with hb.ErrorCapture() as cap:
+        fn(hb.CblasColMajor, cu, hb.CblasTrans, n, k, 1.0, a.ctypes.data, rows, 1.0,
+           c1.ctypes.data, n)
+        fn(hb.CblasRowMajor, cu, ct, n, k, 1.0, arow.ctypes.data, cols, 1.0,
+           crow.ctypes.data, n - 1)
+    name = "cblas_zherk" if p == "z" else "cblas_cherk"
+    assert cap.errors == [(name, 3), (name, 11)]
