@@ -125,6 +125,7 @@ PROTOTYPES = {
                                      F, P, P, I]),
     "hwyblas_set_stream": (None, [P]),
     "hwyblas_last_cuda_error": (I, []),
+    "hwyblas_set_leaf_wait_limit": (ctypes.c_uint, [ctypes.c_uint]),
     "hwyblas_launch_count": (ctypes.c_uint64, []),
     "hwyblas_kernel_timer": (None, [I]),
     "hwyblas_kernel_timer_read": (D, [PI]),

@@ -2053,9 +2053,6 @@ HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
 // ---------------------------------------------------------------------------
 // Extensions.
 
-// Slice count for the emulated GEMM when the caller passes 0 (auto).
-static int AutoSlices(int k) { return k <= 2048 ? 7 : 8; }
-
 HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
     const char* transa, const char* transb, const hwyblas_int* m_p,
     const hwyblas_int* n_p, const hwyblas_int* k_p, const double* alpha_p,
@@ -2095,10 +2092,10 @@ HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
   if (!compute) {
     hb::ScaleMatrix<double>(m, n, beta, sc.dev, sc.ld, hb::kAll);
   } else {
-    const int S = slices == 0 ? AutoSlices(k) : slices;
+    // slices == 0: chosen from the inputs' exponent spread (emulated.cu).
     used = hb::DgemmEmulated(m, n, k, alpha, hb::ColMajor<double>(sa.dev, sa.ld, ta),
                              hb::ColMajor<double>(sb.dev, sb.ld, tb), beta, sc.dev,
-                             sc.ld, S);
+                             sc.ld, slices);
   }
   sc.Out();
   hb::Finish("DGEMM_EMULATED");
@@ -2225,6 +2222,11 @@ HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
 HWYBLAS_API void hwyblas_set_stream(void* stream) {
   hb::Context& c = Ctx();
   c.stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : c.own_stream;
+}
+
+HWYBLAS_API unsigned int hwyblas_set_leaf_wait_limit(unsigned int polls) {
+  Ctx();
+  return hb::SetLeafWaitLimit(polls);
 }
 
 HWYBLAS_API int hwyblas_last_cuda_error(void) {

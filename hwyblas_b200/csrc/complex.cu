@@ -981,6 +981,48 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   LaunchFailed("complex gemm");
 }
 
+// Partial-buffer bytes of a complex GEMM that splits over its KC chunks (0
+// when it does not split); the same rule as ZgemmViews.
+template <typename R>
+size_t ZSplitBytes(int m, int n, int k) {
+  const long long tiles =
+      static_cast<long long>((m + kZM - 1) / kZM) * ((n + kZN - 1) / kZN);
+  const int nchunks = (k + kZChunk - 1) / kZChunk;
+  const size_t pbytes = 2 * sizeof(R) * static_cast<size_t>(nchunks) * m * n;
+  if (m <= 0 || n <= 0 || nchunks < 2 || tiles * 2 > Ctx().num_sms ||
+      pbytes > (size_t(1) << 30))
+    return 0;
+  return pbytes;
+}
+
+// The largest split buffer any GEMM update of a TRSM recursion on an r x r
+// triangle takes (both split orders, so either uplo).
+template <typename R>
+size_t ZTrsmSplitMax(int r, int other) {
+  constexpr int kBase = 32;
+  if (r <= kBase || other <= 0) return 0;
+  const int r1 = std::max(kBase, (r / 2) / kBase * kBase), r2 = r - r1;
+  return std::max({ZTrsmSplitMax<R>(r1, other), ZTrsmSplitMax<R>(r2, other),
+                   ZSplitBytes<R>(r2, other, r1), ZSplitBytes<R>(r1, other, r2)});
+}
+
+// The same for the recursive LU of an m x n panel.
+template <typename R>
+size_t ZGetrfSplitMax(int m, int n) {
+  if (m <= 0 || n <= 0 || std::min(m, n) <= 16) return 0;
+  const int n1 = std::min(m, n) / 2, n2 = n - n1;
+  return std::max({ZGetrfSplitMax<R>(m, n1), ZTrsmSplitMax<R>(n1, n2),
+                   ZSplitBytes<R>(m - n1, n2, n1), ZGetrfSplitMax<R>(m - n1, n2)});
+}
+
+// Reserves the split buffer a whole driver call needs before its first
+// launch: growing it between launches would synchronize and reallocate in
+// the middle of the call.
+template <typename R>
+bool ZReserveSplit(size_t bytes) {
+  return bytes == 0 || Workspace(kWsSplitK, bytes) != nullptr;
+}
+
 // The complex TRSM recursion (src/trsm.cc:87-135) on an op(A) view.
 template <typename R>
 static void ZTrsmRec(bool left, ZView<R> tri, bool lower, bool unit, int r, int other, R* b,
@@ -1087,6 +1129,7 @@ void ZtrsmFull(bool left, bool lower, int op, bool unit, int m, int n, const R* 
   }
   const ZView<R> tri = op == 0 ? ZView<R>{a, 1, lda, 0} : ZView<R>{a, lda, 1, op == 2 ? 1 : 0};
   const bool op_lower = lower != (op != 0);
+  if (!ZReserveSplit<R>(ZTrsmSplitMax<R>(ka, left ? n : m))) return;
   ZTrsmRec<R>(left, tri, op_lower, unit, ka, left ? n : m, bw, ldbw);
   if (bw != b) {
     Failed(cudaMemcpy2DAsync(b, esz * ldb, bw, esz * m, esz * m, n, cudaMemcpyDeviceToDevice,
@@ -1285,9 +1328,18 @@ void ZGetrf(bool recursive, int m, int n, R* a, int lda, int* ipiv, int* info) {
   if (m == 0 || n == 0) return;
   const int nb = 64, mn = std::min(m, n);
   if (recursive || nb >= mn) {
+    if (!ZReserveSplit<R>(ZGetrfSplitMax<R>(m, n))) return;
     ZGetrfRec<R>(m, n, a, lda, ipiv, info, 0);
     return;
   }
+  size_t split_bytes = 0;
+  for (int j = 0; j < mn; j += nb) {
+    const int jb = std::min(mn - j, nb);
+    split_bytes = std::max({split_bytes, ZGetrfSplitMax<R>(m - j, jb),
+                            ZTrsmSplitMax<R>(jb, n - j - jb),
+                            ZSplitBytes<R>(m - j - jb, n - j - jb, jb)});
+  }
+  if (!ZReserveSplit<R>(split_bytes)) return;
   const R one[2] = {R(1), R(0)}, m1[2] = {R(-1), R(0)};
   for (int j = 0; j < mn; j += nb) {
     const int jb = std::min(mn - j, nb);
@@ -1312,6 +1364,7 @@ template <typename R>
 void ZGetrs(int op, int n, int nrhs, const R* a, int lda, const int* ipiv, R* b, int ldb) {
   if (n == 0 || nrhs == 0) return;
   const R one[2] = {R(1), R(0)};
+  if (!ZReserveSplit<R>(ZTrsmSplitMax<R>(n, nrhs))) return;
   if (op == 0) {
     ZLaswp<R>(nrhs, b, ldb, 1, n, ipiv, 1);
     ZtrsmFull<R>(true, true, 0, true, n, nrhs, one, a, lda, b, ldb);

@@ -488,6 +488,159 @@ __global__ void DoubleDoubleGemmKernel(int m, int ncols, int k, View<double> a,
   out[i + jj * ldo] = hi + lo;
 }
 
+// ---------------------------------------------------------------------------
+// Automatic slice count.
+//
+// The emulated product's error grows with how far the products a(i,p) b(p,j)
+// sit below the scales 2^e_i 2^f_j that the slicing is relative to. With
+// E = max e_i and F = max f_j, the statistic
+//
+//   rho = K (sum_i 4^(e_i - E)) (sum_j 4^(f_j - F))
+//         / sum_p (sum_i (a(i,p) 2^-E)^2) (sum_j (b(p,j) 2^-F)^2)   (>= 1)
+//
+// compares the squared scales with the squared products, and
+// beta = log2(rho) / 2 is the number of bits the data loses to its exponent
+// spread. Measured on B200 (normwise error against a double-double product,
+// spreads 0..30 and graded columns, K = 64..8192) the error of S slices
+// relative to the plain FP64 path's is at most
+//
+//   r(S) = 2^(beta + 52.57 - 8 S + max(0, (8 - log2 K) / 2)) + 0.04,
+//
+// (the last term: both paths round the same result; the K term: FP64 chains
+// shorter than the reference's 256-long chunks are more accurate). The call
+// takes the smallest S with r(S) <= 1/2 and runs the plain FP64 path when no
+// S <= 8 qualifies. Every reduction below runs in a fixed order, so the same
+// inputs always get the same S.
+
+constexpr int kSumSqRowsP = 64;     // rows of a p-contiguous chunk
+constexpr int kSumSqRowsO = 1024;   // rows of an o-contiguous chunk
+
+__global__ void MaxExpKernel(const int* exps, int n, int* out) {
+  __shared__ int s[1024];
+  int mx = kZeroExp;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = max(mx, exps[i]);
+  s[threadIdx.x] = mx;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) s[threadIdx.x] = max(s[threadIdx.x], s[threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+// part[c * inner + p] = sum over the rows o of chunk c of (x(o, p) 2^-E)^2.
+// x.cs == 1: a thread per p, looping over the chunk's rows.
+__global__ void SumSqPContigKernel(View<double> x, int outer, int inner,
+                                   const int* emax, double* part) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= inner) return;
+  const int E = *emax;
+  const int o0 = blockIdx.y * kSumSqRowsP, o1 = min(outer, o0 + kSumSqRowsP);
+  double s = 0.0;
+  if (E != kZeroExp) {
+    for (int o = o0; o < o1; ++o) {
+      const double v = ldexp(x.data[o * x.rs + p * x.cs], -E);
+      s = fma(v, v, s);
+    }
+  }
+  part[static_cast<long long>(blockIdx.y) * inner + p] = s;
+}
+
+// x.rs == 1: a warp per p, lanes along the chunk's rows, fixed shuffle tree.
+__global__ void SumSqOContigKernel(View<double> x, int outer, int inner,
+                                   const int* emax, double* part) {
+  const int p = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (p >= inner) return;
+  const int E = *emax;
+  const int o0 = blockIdx.y * kSumSqRowsO, o1 = min(outer, o0 + kSumSqRowsO);
+  double s = 0.0;
+  if (E != kZeroExp) {
+    for (int o = o0 + lane; o < o1; o += 32) {
+      const double v = ldexp(x.data[o * x.rs + p * x.cs], -E);
+      s = fma(v, v, s);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) part[static_cast<long long>(blockIdx.y) * inner + p] = s;
+}
+
+__device__ double BlockSum(double v, double* s) {
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+    __syncthreads();
+  }
+  const double r = s[0];
+  __syncthreads();
+  return r;
+}
+
+struct AutoArgs {
+  const int* row_exp;
+  const int* col_exp;
+  int m, n, k;
+  const int* emax;      // [0] E of op(A), [1] F of op(B)
+  const double* part_a;  // [chunks_a][k]
+  const double* part_b;  // [chunks_b][k]
+  int chunks_a, chunks_b;
+  int* slices_out;      // the chosen S (0: the plain path)
+};
+
+// One block of 1024 threads: the statistic and the slice count.
+__global__ void AutoSlicesKernel(AutoArgs g) {
+  __shared__ double s[1024];
+  const int E = g.emax[0], F = g.emax[1];
+  double sa = 0.0, sb = 0.0, q = 0.0;
+  if (E != kZeroExp && F != kZeroExp) {
+    for (int i = threadIdx.x; i < g.m; i += blockDim.x)
+      if (g.row_exp[i] != kZeroExp) sa += ldexp(1.0, 2 * (g.row_exp[i] - E));
+    for (int j = threadIdx.x; j < g.n; j += blockDim.x)
+      if (g.col_exp[j] != kZeroExp) sb += ldexp(1.0, 2 * (g.col_exp[j] - F));
+    for (int p = threadIdx.x; p < g.k; p += blockDim.x) {
+      double ca = 0.0, rb = 0.0;
+      for (int c = 0; c < g.chunks_a; ++c) ca += g.part_a[static_cast<long long>(c) * g.k + p];
+      for (int c = 0; c < g.chunks_b; ++c) rb += g.part_b[static_cast<long long>(c) * g.k + p];
+      q = fma(ca, rb, q);
+    }
+  }
+  sa = BlockSum(sa, s);
+  sb = BlockSum(sb, s);
+  q = BlockSum(q, s);
+  if (threadIdx.x == 0) {
+    int S = 1;
+    if (q > 0.0) {
+      const double rho = fmax(1.0, static_cast<double>(g.k) * sa * sb / q);
+      const double beta = 0.5 * log2(rho);
+      const double kterm = fmax(0.0, 0.5 * (8.0 - log2(static_cast<double>(g.k))));
+      S = 0;
+      for (int c = 1; c <= 8; ++c) {
+        if (exp2(beta + 52.57 - 8.0 * c + kterm) + 0.04 <= 0.5) {
+          S = c;
+          break;
+        }
+      }
+    }
+    *g.slices_out = S;
+  }
+}
+
+void SumSquares(View<double> x, int outer, int inner, const int* emax, double* part,
+                int* chunks, cudaStream_t st) {
+  if (x.rs == 1) {
+    *chunks = (outer + kSumSqRowsO - 1) / kSumSqRowsO;
+    const dim3 grid((inner + 7) / 8, *chunks);
+    SumSqOContigKernel<<<grid, 256, 0, st>>>(x, outer, inner, emax, part);
+  } else {
+    *chunks = (outer + kSumSqRowsP - 1) / kSumSqRowsP;
+    const dim3 grid((inner + 255) / 256, *chunks);
+    SumSqPContigKernel<<<grid, 256, 0, st>>>(x, outer, inner, emax, part);
+  }
+  CountLaunch();
+  LaunchFailed("ozaki auto statistics");
+}
+
 template <int S>
 void LaunchSplit(View<double> x, int outer, int inner, const int* exps,
                  int8_t* out, long long kp, cudaStream_t st) {
@@ -607,8 +760,8 @@ bool MakePassMaps(PassMaps* pm, const int8_t* sa, const int8_t* sb, int kc, int 
 // Largest K for which every level sum fits INT32: S K 2^14 < 2^31.
 int OzakiMaxK(int S) { return static_cast<int>((2147483647LL / (S * 16384LL)) / 128 * 128); }
 
-// Returns the slice count used (0 if the inputs were not finite and the plain
-// FP64 path ran instead).
+// Returns the slice count used (0 if the plain FP64 path ran instead: the
+// inputs were not finite, or slices == 0 found no S <= 8 as accurate as it).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
                   bool check_finite, int ws_set) {
@@ -617,29 +770,67 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
   const int ws_w = ws_set ? kWsEmulW2 : kWsEmulW;
   Context& ctx = Ctx();
   cudaStream_t st = ctx.stream;
-  const int S = std::min(8, std::max(1, slices));
-  int* exps = static_cast<int*>(Workspace(ws_acc, sizeof(int) * (m + n + 64)));
-  int* row_exp = exps;
-  int* col_exp = exps + m;
-  int* nonfinite = exps + m + n;
-  cudaMemsetAsync(nonfinite, 0, sizeof(int), st);
-  Exponents(a, m, k, row_exp, nonfinite, st);
+  const bool automatic = (slices == 0);
   // op(B)(p, j): outer j, inner p -> element (j, p) at rs_b * p + cs_b * j.
   View<double> bt;
   bt.data = b.data;
   bt.rs = b.cs;
   bt.cs = b.rs;
-  Exponents(bt, n, k, col_exp, nonfinite, st);
-  int host_nonfinite = 0;
-  if (check_finite) {
-    cudaMemcpyAsync(&host_nonfinite, nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st);
+  // Workspace: ints [row exponents m | column exponents n | nonfinite, S,
+  // E, F, ...] then, for the automatic slice count, the per-p partial sums
+  // of squares of op(A) and op(B).
+  const int chunks_a = a.rs == 1 ? (m + kSumSqRowsO - 1) / kSumSqRowsO
+                                 : (m + kSumSqRowsP - 1) / kSumSqRowsP;
+  const int chunks_b = bt.rs == 1 ? (n + kSumSqRowsO - 1) / kSumSqRowsO
+                                  : (n + kSumSqRowsP - 1) / kSumSqRowsP;
+  const size_t int_bytes = (sizeof(int) * (m + n + 64) + 255) / 256 * 256;
+  const size_t part_bytes =
+      automatic ? sizeof(double) * static_cast<size_t>(chunks_a + chunks_b) * k : 0;
+  char* acc = static_cast<char*>(Workspace(ws_acc, int_bytes + part_bytes));
+  int* exps = reinterpret_cast<int*>(acc);
+  int* row_exp = exps;
+  int* col_exp = exps + m;
+  int* flags = exps + m + n;  // [0] nonfinite, [1] automatic S, [2..3] E, F
+  cudaMemsetAsync(flags, 0, sizeof(int) * 2, st);
+  Exponents(a, m, k, row_exp, flags, st);
+  Exponents(bt, n, k, col_exp, flags, st);
+  if (automatic) {
+    double* part_a = reinterpret_cast<double*>(acc + int_bytes);
+    double* part_b = part_a + static_cast<size_t>(chunks_a) * k;
+    MaxExpKernel<<<1, 1024, 0, st>>>(row_exp, m, flags + 2);
+    MaxExpKernel<<<1, 1024, 0, st>>>(col_exp, n, flags + 3);
+    CountLaunch(2);
+    int ca = 0, cb = 0;
+    SumSquares(a, m, k, flags + 2, part_a, &ca, st);
+    SumSquares(bt, n, k, flags + 3, part_b, &cb, st);
+    AutoArgs g;
+    g.row_exp = row_exp;
+    g.col_exp = col_exp;
+    g.m = m;
+    g.n = n;
+    g.k = k;
+    g.emax = flags + 2;
+    g.part_a = part_a;
+    g.part_b = part_b;
+    g.chunks_a = ca;
+    g.chunks_b = cb;
+    g.slices_out = flags + 1;
+    AutoSlicesKernel<<<1, 1024, 0, st>>>(g);
+    CountLaunch();
+    if (LaunchFailed("ozaki auto slices")) return -1;
+  }
+  int host_flags[2] = {0, 0};
+  if (check_finite || automatic) {
+    cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, st);
     if (Failed(cudaStreamSynchronize(st), "ozaki exponents")) return -1;
   }
-  if (host_nonfinite) {
-    // Inf/NaN cannot be sliced: the plain FP64 path propagates them.
+  if (host_flags[0] || (automatic && host_flags[1] == 0)) {
+    // Inf/NaN cannot be sliced, and a spread too wide for 8 slices would
+    // lose accuracy: the plain FP64 path runs (and propagates Inf/NaN).
     Dgemm(m, n, k, alpha, a, b, beta, c, ldc, kAll);
     return 0;
   }
+  const int S = automatic ? host_flags[1] : std::min(8, std::max(1, slices));
   const int kmax = OzakiMaxK(S);
   const int kchunk = std::min(k, kmax);
   const long long kp = (static_cast<long long>(kchunk) + 15) / 16 * 16;

@@ -324,6 +324,11 @@ constexpr int kLeafMaxP = 64;       // CTAs per panel (m <= 65536)
 constexpr int kLeafMaxCluster = 16; // CTAs of the cluster variant (m <= 16384)
 constexpr int kLeafW = 16;
 
+// Polls of the cooperative leaf's candidate exchange before a CTA gives up
+// (sets the timeout flag and returns). hwyblas_set_leaf_wait_limit lowers it
+// so that a test can make the wait run out; 0 there restores this default.
+__device__ uint32_t g_leaf_poll_limit = kMaxPolls;
+
 template <typename T>
 struct LeafArgs {
   int m, w, lanes;
@@ -482,7 +487,7 @@ __global__ void __launch_bounds__(kLeafThreads)
                        : "l"(tags + par * P + threadIdx.x)
                        : "memory");
           if (v >= static_cast<unsigned>(j + 1)) break;
-          if (++polls >= kMaxPolls) {
+          if (++polls >= g_leaf_poll_limit) {
             atomicExch(p.timeout_flag, 1);
             s_abort = 1;
             break;
@@ -841,6 +846,14 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
 template void GetrfLeaf<double>(int, int, double*, int, int*, int*, int, int);
 template void GetrfLeaf<float>(int, int, float*, int, int*, int*, int, int);
 
+unsigned int SetLeafWaitLimit(unsigned int polls) {
+  unsigned int prev = kMaxPolls;
+  cudaMemcpyFromSymbol(&prev, g_leaf_poll_limit, sizeof(prev));
+  const unsigned int v = polls == 0 ? kMaxPolls : polls;
+  Failed(cudaMemcpyToSymbol(g_leaf_poll_limit, &v, sizeof(v)), "leaf wait limit");
+  return prev;
+}
+
 template <typename T>
 void PotrfLeaf(bool upper, int n, T* a, int lda, int* info, int info_base) {
   const int lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
@@ -885,19 +898,23 @@ constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
-// Set-up, once per device with that device current: the scratch address and
-// a zeroed array (ordered on `stream` before the first launch).
+// The scratch address on the current device, looked up on every call (the
+// lookup allocates nothing). Set-up zeroes the array, ordered on `stream`
+// before the launch, the first time a device's address is seen and again
+// whenever it changes: a context torn down and created again (for instance
+// after cudaDeviceReset) loads the module afresh, possibly elsewhere, with a
+// ticket that is not known to be zero.
 cudaError_t NoAllocScratch(int device, cudaStream_t stream, void** out) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[device] == nullptr) {
-    void* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
+  if (g_noalloc_ptr[device] != ptr) {
     e = cudaMemsetAsync(ptr, 0, kNoAllocScratchBytes, stream);
     if (e != cudaSuccess) return e;
     g_noalloc_ptr[device] = ptr;
   }
-  *out = g_noalloc_ptr[device];
+  *out = ptr;
   return cudaSuccess;
 }
 

@@ -167,6 +167,9 @@ void AdjustPivots(int* ipiv, int begin, int end, int delta);
 template <typename T>
 void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
                int leaf_w = 16);
+// Sets the poll limit of the cooperative leaf's exchange on the current
+// device (0: the default); returns the previous one.
+unsigned int SetLeafWaitLimit(unsigned int polls);
 // PotrfLeaf on device: n <= 64; sets *info to info_base + j + 1 and stops at
 // the first non-positive (or NaN) diagonal, if *info is still 0.
 template <typename T>

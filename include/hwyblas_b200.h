@@ -660,12 +660,16 @@ HWYBLAS_API CBLAS_INDEX cblas_idamax(const hwyblas_int n, const double* x,
 
 /* FP64-accurate GEMM on the INT8 tensor cores (Ozaki scheme): each row of
  * op(A) and column of op(B) is scaled by a power of two and cut into `slices`
- * 7-bit integer slices (1..8; 0 = chosen from K), the slice products with
- * index sum below `slices` run as exact INT32 tensor-core GEMMs, and the
- * levels are recombined in FP64 with compensated summation. Arguments and
- * errors as dgemm_ (position 14: slices). Returns the slice count used (0:
- * non-finite inputs, computed by the plain FP64 path instead; -1: error).
- * No counterpart in the reference (a north-star extension). */
+ * 8-bit integer slices (1..8), the slice products with index sum below
+ * `slices` run as exact INT32 tensor-core GEMMs, and the levels are
+ * recombined in FP64 with compensated summation. slices = 0 chooses the
+ * count from the inputs: the smallest whose estimated normwise error, given
+ * the exponent spread of the rows of op(A) and columns of op(B) and K, is at
+ * most half the plain FP64 path's (7 for uniform data, 8 for spreads of
+ * several binades), or the plain path when no count up to 8 is. Arguments
+ * and errors as dgemm_ (position 14: slices). Returns the slice count used
+ * (0: the plain FP64 path ran: non-finite inputs, or slices = 0 and a spread
+ * too wide for 8 slices; -1: error). No counterpart in the reference. */
 HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
     const char* transa, const char* transb, const hwyblas_int* m,
     const hwyblas_int* n, const hwyblas_int* k, const double* alpha,
@@ -790,6 +794,13 @@ HWYBLAS_API double hwyblas_kernel_timer_read(int* launches);
  * a DMMA issue-rate loop; the FP64 roofline denominator. No counterpart in
  * the reference. */
 HWYBLAS_API double hwyblas_fp64_peak_tflops(void);
+/* Test hook for the bounded waits: sets how many times each CTA of the LU
+ * panel's cooperative pivot exchange (panels of more than 16 x 1024 rows)
+ * polls for its peers before it gives up, sets the timeout status (reported
+ * as cudaErrorLaunchTimeout by hwyblas_last_cuda_error) and returns; 0
+ * restores the default of 2^26. Applies to the current device; returns the
+ * previous limit. No counterpart in the reference. */
+HWYBLAS_API unsigned int hwyblas_set_leaf_wait_limit(unsigned int polls);
 
 /* IDAMAX that allocates no memory: for callers that must not allocate
  * device memory during a call (a cudaMalloc/cudaFree synchronizes the whole

@@ -502,25 +502,59 @@ def test_zpotrf_device_misaligned_and_errors(hb, orc):
 
 
 @pytest.mark.parametrize("p", ["z", "c"])
-def test_complex_split_chunks_bitexact(hb, orc, p):
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.3 - 0.2j])
+def test_complex_split_chunks_bitexact(hb, orc, p, beta):
     """Few output tiles and many KC chunks: the chunks run in parallel and
-    merge in order, which must give the sequential result (GEMM with a
-    general beta, and HERK on a triangle)."""
+    merge in order, which must give the sequential result. The first chunk's
+    merge stores (beta 0), adds (beta 1) or applies a general beta."""
     dtype = np.complex128 if p == "z" else np.complex64
     rng = np.random.default_rng(41)
     m, n, k = 100, 70, 3000
     a, b, c = crand(rng, m, k, dtype), crand(rng, k, n, dtype), crand(rng, m, n, dtype)
     c1, c2 = c.copy(order="F"), c.copy(order="F")
-    hb.zgemm(p, "N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, 0.3 - 0.2j, c1, m)
-    assert orc.zgemm("N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, 0.3 - 0.2j, c2, m) == 0
+    hb.zgemm(p, "N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, beta, c1, m)
+    assert orc.zgemm("N", "N", m, n, k, 0.5 - 1.0j, a, m, b, k, beta, c2, m) == 0
     assert same_bits(creal(c1), creal(c2))
-    for uplo in ("L", "U"):
-        h = crand(rng, 64, 4096, dtype)
-        d = crand(rng, 64, 64, dtype)
-        d1, d2 = d.copy(order="F"), d.copy(order="F")
-        hb.zherk(p, uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d1, 64)
-        assert orc.zherk(uplo, "N", 64, 4096, -1.0, h, 64, 1.0, d2, 64) == 0
-        assert same_bits(creal(d1), creal(d2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "C"])
+@pytest.mark.parametrize("beta", [0.0, 0.5, 1.0])
+def test_complex_split_chunks_herk_bitexact(hb, orc, p, uplo, trans, beta):
+    """HERK on a 64 x 64 triangle with k = 4096: the split's first chunk
+    applies beta on the crossing tiles, the later chunks add with beta 1."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    rng = np.random.default_rng(42)
+    n, k = 64, 4096
+    h = crand(rng, n, k, dtype) if trans == "N" else crand(rng, k, n, dtype)
+    ldh = h.shape[0]
+    d = crand(rng, n, n, dtype)
+    d1, d2 = d.copy(order="F"), d.copy(order="F")
+    hb.zherk(p, uplo, trans, n, k, -1.0, h, ldh, beta, d1, n)
+    assert orc.zherk(uplo, trans, n, k, -1.0, h, ldh, beta, d2, n) == 0
+    assert same_bits(creal(d1), creal(d2))
+
+
+@pytest.mark.parametrize("p", ["z", "c"])
+@pytest.mark.parametrize("recursive", [False, True])
+@pytest.mark.parametrize("m", [7000, 8700])
+def test_zgetrf_tall_panels_bitexact(hb, orc, p, recursive, m):
+    """Narrow panels over many CTAs of 512 rows: m = 7000 runs the cluster
+    variant with 14 CTAs exchanging candidates through distributed shared
+    memory, m = 8700 (17 CTAs, beyond the 16-CTA cluster) the cooperative
+    variant with polled global slots."""
+    dtype = np.complex128 if p == "z" else np.complex64
+    n = 20
+    rng = np.random.default_rng(m + n)
+    a = crand(rng, m, n, dtype)
+    a1, a2 = a.copy(order="F"), a.copy(order="F")
+    p1, p2 = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    i1 = hb.zgetrf(p, m, n, a1, m, p1, recursive=recursive)
+    i2 = orc.zgetrf(m, n, a2, m, p2, recursive=recursive)
+    assert i1 == i2 == 0
+    assert np.array_equal(p1, p2)
+    assert same_bits(creal(a1), creal(a2))
 
 
 @pytest.mark.parametrize("p", ["z", "c"])
