@@ -6,10 +6,12 @@ mixed against plain.
 
 Headline (`value`): DGEMM M = N = K = 8192, column-major NN, C = A B, with
 A and B entries u * 2^e (u uniform[-1, 1], e uniform in {-8..8}, seeded), on
-the emulated-FP64 path (Ozaki INT8 slices on tcgen05, slice count chosen
-automatically) - 2 * 8192^3 useful FP64 flops per step. "FP64-accurate": its
-normwise error against a double-double product of 64 sampled columns must not
-exceed the plain FP64 path's error on the same inputs (both are reported).
+the emulated-FP64 path (Ozaki INT8 slices on tcgen05, slice count chosen from
+the inputs' exponent spread) - 2 * 8192^3 useful FP64 flops per step.
+"FP64-accurate": its normwise error against a double-double product of 64
+sampled columns must not exceed the plain FP64 path's error on the same
+inputs (both are reported; the tests hold the double-double product to 1 ulp
+of the exact one).
 
 value  : device-timed, inputs resident in HBM, CUDA events on the library's
          stream, max over ranks; whole-job TFLOP/s (sum over ranks).
@@ -17,8 +19,13 @@ e2e    : the same product through the public C ABI with pinned HOST buffers
          (A, B copied in and C copied out inside the timed region).
 plain  : the plain FP64 tensor-pipe DGEMM (bit-identical to the reference)
          on the same inputs, and its error.
+auto_slices: the automatic slice count at exponent spreads 0, 8 and 30.
+config1: dgemm NN 1024^3, alpha 1.5, beta 0.5 (device, C ABI with host
+         buffers, and the CPU path single-threaded on the same inputs).
+config2: dtrsm L/L/N/U 4096 x 512 and dgetrf 4096, with the LU residual
+         ratio and ipiv / bit equality against the CPU path.
 batched: 10,000 problems, n log-uniform in [8, 512], dgetrf + dgetrs + dgemm
-         each, batched persistent launches against a per-problem loop.
+         each, batched persistent launches against the per-problem loop.
 widened: throughput of the routines beyond the hot path (dtrmm, dsymm,
          dsyr2k, dgemmtr, dtrtri, dgetri at n = 8192; zgemm, cgemm at 4096).
 dgesv  : n = 16384, A = H1 diag(s) H2 (H1, H2 products of 4 Householder
@@ -30,7 +37,8 @@ Replicas only: every rank runs its own problems (weak scaling).
 
 --impl reference times the reference's CPU implementation of the path on this
 host's cores (the oracle port of the reference's DGEMM with its per-element
-order, all threads) on a bounded column sample of the same workload.
+order, all threads): --warmup untimed and --steps timed steps, each one
+bounded column sample of the same workload, plus a single-threaded figure.
 """
 import argparse
 import datetime
@@ -65,7 +73,10 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-dgesv", action="store_true")
-    p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--no-sweep", action="store_true",
+                   help="skip the slice sweep and the automatic slice count per spread")
+    p.add_argument("--no-small", action="store_true",
+                   help="skip the dgemm 1024 / dtrsm 4096x512 / dgetrf 4096 configurations")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-widened", action="store_true",
                    help="skip the throughput of the routines beyond the hot path")
@@ -185,7 +196,7 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle port of the reference's hot path on host threads.
+# CPU baseline: the reference's CPU implementation of the path on host cores.
 
 def cpu_threads():
     try:
@@ -199,25 +210,79 @@ def spread_matrix(rng, rows, cols, spread):
     return np.asfortranarray(rng.uniform(-1, 1, (rows, cols)) * np.exp2(e))
 
 
-def cpu_dgemm_sample(n, cols, steps, threads):
-    """TFLOP/s of the reference's DGEMM order (oracle port) on an n x cols x n
-    slice of the workload (a bounded sample: cols of the n output columns)."""
-    from tests.oracle_lib import Oracle
-    orc = Oracle()
-    orc.set_threads(threads)
-    rng = np.random.default_rng(7)
-    a = spread_matrix(rng, n, n, SPREAD)
-    b = spread_matrix(rng, n, cols, SPREAD)
-    c = np.zeros((n, cols), order="F")
-    orc.dgemm("N", "N", n, cols, n, 1.0, a, n, b, n, 0.0, c, n)  # warm-up
-    best = float("inf")
+class CpuPath:
+    """The reference's CPU hot path: the oracle port of its DGEMM / DTRSM /
+    DGETRF with the reference's per-element order (kind "port")."""
+
+    def __init__(self):
+        from tests.oracle_lib import Oracle
+        self.orc = Oracle()
+        self.kind = "port"
+        self.threads = 1
+
+    def set_threads(self, n):
+        self.threads = int(n)
+        self.orc.set_threads(self.threads)
+
+    def dgemm(self, *args):
+        return self.orc.dgemm(*args)
+
+    def dtrsm(self, *args):
+        return self.orc.dtrsm(*args)
+
+    def dgetrf(self, *args):
+        return self.orc.dgetrf(*args)
+
+
+class DgemmSample:
+    """One step of the CPU baseline: C = A B with A n x n and B n x cols, the
+    first `cols` columns of the n = 8192 workload's product (a bounded sample:
+    every column costs the same, so its TFLOP/s is the whole product's)."""
+
+    def __init__(self, cpu, n, cols):
+        rng = np.random.default_rng(7)
+        self.cpu, self.n, self.cols = cpu, n, cols
+        self.a = spread_matrix(rng, n, n, SPREAD)
+        self.b = spread_matrix(rng, n, cols, SPREAD)
+        self.c = np.zeros((n, cols), order="F")
+        self.flops = 2.0 * n * cols * n
+
+    def __call__(self):
+        n = self.n
+        self.cpu.dgemm("N", "N", n, self.cols, n, 1.0, self.a, n, self.b, n, 0.0, self.c, n)
+
+    def describe(self):
+        return (f"dgemm NN {self.n}x{self.cols}x{self.n} (the first {self.cols} of the "
+                f"{self.n} output columns) per step")
+
+
+def cpu_sample_cols(n, threads):
+    """Output columns of one CPU step: one 96-column block of C (the CPU
+    path's unit of parallel work) per thread."""
+    return min(n, 96 * threads)
+
+
+def cpu_steps(fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        orc.dgemm("N", "N", n, cols, n, 1.0, a, n, b, n, 0.0, c, n)
-        best = min(best, time.perf_counter() - t0)
-    flops = 2.0 * n * cols * n
-    return flops / best / 1e12, (f"dgemm NN {n}x{cols}x{n} (1/{n // cols} of the output "
-                                 f"columns), best of {steps}")
+        fn()
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_single_thread(cpu, n):
+    """The single-threaded figure (the reference is single-threaded by
+    design): best of 3 on a 32-column sample."""
+    prev = cpu.threads
+    cpu.set_threads(1)
+    smp = DgemmSample(cpu, n, 32)
+    best = min(cpu_steps(smp, 3, 1))
+    cpu.set_threads(prev)
+    return {"value": smp.flops / best / 1e12, "unit": "TFLOP/s", "cores": 1,
+            "sample": smp.describe() + ", best of 3"}
 
 
 def workload_name(n):
@@ -225,27 +290,40 @@ def workload_name(n):
             f"e~U{{-{SPREAD}..{SPREAD}}}), FP64-accurate")
 
 
+def workload_config(n):
+    return {"workload": workload_name(n),
+            "l2": f"inputs (2 x {8 * n * n >> 20} MiB FP64) larger than L2"}
+
+
 def run_reference(args):
+    """The reference arm: the reference's CPU implementation of the path, all
+    host threads, `--warmup` untimed and `--steps` timed steps, each one
+    bounded sample of the workload; ms_per_step is the measured step."""
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
+    cpu = CpuPath()
     threads = cpu_threads()
+    cpu.set_threads(threads)
     n = args.n
-    cols = max(64, n // 8)
-    steps = max(1, min(args.steps, 3))
-    tf, sample = cpu_dgemm_sample(n, cols, steps, threads)
+    smp = DgemmSample(cpu, n, cpu_sample_cols(n, threads))
+    times = cpu_steps(smp, args.steps, args.warmup)
+    ms = 1e3 * sum(times) / len(times)
+    tf = smp.flops / (ms * 1e-3) / 1e12
+    single = cpu_single_thread(cpu, n)
     line = {
         "impl": "reference", "metric": METRIC, "value": tf, "unit": "TFLOP/s",
-        "n_gpus": args.gpus, "steps": steps, "warmup": 1, "higher_is_better": True,
-        "ms_per_step": 2.0 * n ** 3 / (tf * 1e12) * 1e3, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "ms_per_step": ms, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": workload_name(n), "parallelism": "host threads"},
-        "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+        "config": workload_config(n),
+        "parallelism": f"{threads} host threads (column blocks of C)",
+        "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": cpu.kind,
+                         "sample": smp.describe(), "single_thread": single},
         "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "the reference's Highway BLAS does not build here (Highway absent); "
-                "this is the oracle port of its hot path with the same per-element order",
+        "note": "the reference's Highway BLAS does not build here (Highway absent); this "
+                "is the oracle port of its hot path with the same per-element order",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -364,8 +442,7 @@ def run_dgemm(args, torch, hb, stream, dist, world, rank, local):
         "dmma_kernel_ms_per_launch": dm_ms / max(1, dm_launches),
     }
 
-    # Slice sweep S = 3..8 (one warm and one timed call each) and the wider
-    # exponent spread.
+    # Slice sweep S = 3..8 (one warm and one timed call each).
     if not args.no_sweep and rank == 0:
         sweep = {}
         for s in range(3, 9):
@@ -376,16 +453,6 @@ def run_dgemm(args, torch, hb, stream, dist, world, rank, local):
             sweep[str(s)] = {"tflops": flops / (t * 1e-3) / 1e12,
                              "err": normwise_error(torch, hb, A, B, C, n, cols)}
         out["sweep"] = sweep
-        g30 = torch.Generator(device="cuda").manual_seed(99)
-        A30 = device_spread(torch, n, 30, g30)
-        B30 = device_spread(torch, n, 30, g30)
-        torch.cuda.synchronize()
-        s30 = hb.dgemm_emulated("N", "N", n, n, n, 1.0, A30, n, B30, n, 0.0, C, n, 0)
-        e30 = normwise_error(torch, hb, A30, B30, C, n, cols)
-        hb.dgemm("N", "N", n, n, n, 1.0, A30, n, B30, n, 0.0, Cp, n)
-        p30 = normwise_error(torch, hb, A30, B30, Cp, n, cols)
-        out["spread30"] = {"slices": s30, "err_emulated": e30, "err_plain": p30}
-        del A30, B30
 
     # End to end through the C ABI with pinned host buffers: A, B in, C out
     # (beta = 0: C is not read).
@@ -498,11 +565,11 @@ def run_solvers(args, torch, hb, stream):
     return res
 
 
-def run_batched(args, torch, hb, count=10000, loop_sample=300):
+def run_batched(args, torch, hb, count=10000):
     """Config 5: `count` problems, n log-uniform in [8, 512], each dgetrf +
     dgetrs (nrhs uniform in 1..16) + dgemm (n x n x n), FP64 and FP32: the
     batched persistent launches against a per-problem loop of the
-    single-problem routines (timed on a sample, scaled to the batch)."""
+    single-problem routines over the same problems."""
     rng = np.random.default_rng(2024)
     ns = np.exp(rng.uniform(np.log(8), np.log(512), count)).astype(int).clip(8, 512)
     rhs = rng.integers(1, 17, count)
@@ -548,11 +615,8 @@ def run_batched(args, torch, hb, count=10000, loop_sample=300):
         t_batched = times[-1]
         entry = {"batched_ms": t_batched * 1e3, "tflops": flops / t_batched / 1e12}
         if prec == "d":
-            # The per-problem loop on a sample of the same problems.
-            idx = rng.choice(count, loop_sample, replace=False)
-            A.copy_(A0)
-            torch.cuda.synchronize()
-
+            # The per-problem loop of the single-problem routines over all
+            # `count` problems (each call returns when its result is ready).
             def loop(ids):
                 for i in ids:
                     n, r = nl[i], rl[i]
@@ -560,18 +624,16 @@ def run_batched(args, torch, hb, count=10000, loop_sample=300):
                     hb.dgetrs("N", n, r, va[i], n, vp[i], vb[i], n)
                     hb.dgemm("N", "N", n, n, n, 1.0, v1[i], n, v2[i], n, 0.0, v3[i], n)
 
-            loop(idx[:10])  # warm-up
+            loop(range(10))  # warm-up
             A.copy_(A0)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            loop(idx)
+            loop(range(count))
             torch.cuda.synchronize()
             t_loop = time.perf_counter() - t0
-            frac = float(np.sum(ns[idx] ** 3)) / float(np.sum(ns ** 3))
-            entry["loop_ms_estimate"] = t_loop / frac * 1e3
-            entry["loop_sample"] = f"{loop_sample} problems ({100 * frac:.1f} % of the n^3 work)"
-            entry["speedup_vs_loop"] = entry["loop_ms_estimate"] / entry["batched_ms"]
-            # getrf alone, batched vs loop on the same sample.
+            entry["loop_ms"] = t_loop * 1e3
+            entry["speedup_vs_loop"] = entry["loop_ms"] / entry["batched_ms"]
+            # getrf alone, batched against the loop, same problems.
             A.copy_(A0)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -581,12 +643,12 @@ def run_batched(args, torch, hb, count=10000, loop_sample=300):
             A.copy_(A0)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            for i in idx:
+            for i in range(count):
                 hb.dgetrf(nl[i], nl[i], va[i], nl[i], vp[i])
             torch.cuda.synchronize()
-            t_gl = (time.perf_counter() - t0) / frac
+            t_gl = time.perf_counter() - t0
             entry["getrf_batched_ms"] = t_gb * 1e3
-            entry["getrf_loop_ms_estimate"] = t_gl * 1e3
+            entry["getrf_loop_ms"] = t_gl * 1e3
             entry["getrf_speedup_vs_loop"] = t_gl / t_gb
         out["fp64" if prec == "d" else "fp32"] = entry
         del A0, A, B, G1, G2, G3, P
@@ -671,6 +733,193 @@ def run_widened(torch, hb, stream):
     return out
 
 
+def run_auto_slices(torch, hb, stream, n):
+    """The automatic slice count on the headline's shape at three exponent
+    spreads: the count chosen, its throughput, and its error next to the
+    plain FP64 path's (both against the double-double product)."""
+    out = {}
+    flops = 2.0 * n ** 3
+    C = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    Cp = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    cols = list(range(0, n, max(1, n // 64)))[:64]
+    for spread in (0, 8, 30):
+        g = torch.Generator(device="cuda").manual_seed(99 + spread)
+        A = device_spread(torch, n, spread, g)
+        B = device_spread(torch, n, spread, g)
+        torch.cuda.synchronize()
+        used = [0]
+
+        def one():
+            used[0] = hb.dgemm_emulated("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n, 0)
+        one()
+        t = timed(torch, stream, one, 2)
+        e = normwise_error(torch, hb, A, B, C, n, cols)
+        hb.dgemm("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, Cp, n)
+        pe = normwise_error(torch, hb, A, B, Cp, n, cols)
+        out[f"spread{spread}"] = {"slices": used[0], "tflops": flops / (t * 1e-3) / 1e12,
+                                  "err_emulated": e, "err_plain": pe,
+                                  "fp64_accurate": bool(e <= pe)}
+        del A, B
+    return out
+
+
+def run_small_configs(torch, hb, stream, cpu, fp64_peak):
+    """dgemm NN 1024^3 (alpha 1.5, beta 0.5), dtrsm L/L/N/U 4096 x 512 and
+    dgetrf 4096, entries U[-1, 1]: device-timed TFLOP/s with the fraction of
+    the FP64 tensor-pipe peak, the C-ABI time with host buffers, and the CPU
+    path single-threaded on the same inputs with bit equality (and ipiv
+    equality and the LU residual ratio ||PA - LU||_1 / (n ||A||_1 eps))."""
+    rng = np.random.default_rng(2025)
+    res = {}
+
+    def dev(x):
+        return torch.from_numpy(np.asfortranarray(x).ravel(order="F").copy()).cuda()
+
+    def host(t, rows, cols):
+        return np.asfortranarray(t.cpu().numpy().reshape(cols, rows).T)
+
+    def roof(tflops):
+        return {"bound": "tensor", "achieved": tflops, "peak": fp64_peak,
+                "unit": "TFLOP/s (FP64)", "frac": tflops / fp64_peak,
+                "peak_source": "measured DMMA issue rate (hwyblas_fp64_peak_tflops)"}
+
+    def cpu_time(fn, reps):
+        cpu.set_threads(1)
+        best = min(cpu_steps(fn, reps, 0))
+        cpu.set_threads(cpu_threads())
+        return best
+
+    # Config 1: dgemm.
+    n = 1024
+    a, b, c = (rng.uniform(-1, 1, (n, n)) for _ in range(3))
+    a, b, c = np.asfortranarray(a), np.asfortranarray(b), np.asfortranarray(c)
+    flops = 2.0 * n ** 3
+    A, B, C0 = dev(a), dev(b), dev(c)
+    Cw = C0.clone()
+    gemm = lambda: hb.dgemm("N", "N", n, n, n, 1.5, A, n, B, n, 0.5, Cw, n)
+    for _ in range(3):
+        gemm()
+    ms = timed(torch, stream, gemm, 50)
+    Cw.copy_(C0)
+    torch.cuda.synchronize()
+    gemm()
+    c_gpu = host(Cw, n, n)
+    hc = c.copy(order="F")
+    t0 = time.perf_counter()
+    for _ in range(10):
+        hc[:] = c
+        hb.dgemm("N", "N", n, n, n, 1.5, a, n, b, n, 0.5, hc, n)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / 10
+    entry = {"workload": "dgemm NN M=N=K=1024, alpha 1.5, beta 0.5, U[-1,1]",
+             "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+             "e2e": {"ms": e2e_ms, "tflops": flops / (e2e_ms * 1e-3) / 1e12,
+                     "h2d_bytes": 3 * 8 * n * n, "d2h_bytes": 8 * n * n}}
+    entry["roofline"] = roof(entry["tflops"])
+    if cpu is not None:
+        cc = c.copy(order="F")
+        cpu.dgemm("N", "N", n, n, n, 1.5, a, n, b, n, 0.5, cc, n)
+        entry["bit_identical_to_cpu"] = bool(np.array_equal(cc.view(np.uint64),
+                                                            c_gpu.view(np.uint64)))
+        cw = c.copy(order="F")
+
+        def cpu_gemm():
+            cw[:] = c
+            cpu.dgemm("N", "N", n, n, n, 1.5, a, n, b, n, 0.5, cw, n)
+        t = cpu_time(cpu_gemm, 3)
+        entry["cpu"] = {"ms": t * 1e3, "tflops": flops / t / 1e12, "cores": 1,
+                        "kind": cpu.kind}
+    res["config1"] = entry
+
+    # Config 2a: dtrsm L/L/N/U, M = 4096, N = 512 (m n ka flops). As
+    # configured, the unit lower triangle's entries are U[-1, 1] and the
+    # solution overflows; the reference tests' scaled variant (off-diagonal
+    # times 1/ka) is the well-posed one that the bits are compared on.
+    m, nr = 4096, 512
+    t_raw = np.asfortranarray(rng.uniform(-1, 1, (m, m)))
+    bb = np.asfortranarray(rng.uniform(-1, 1, (m, nr)))
+    t_scaled = np.asfortranarray(t_raw / m)
+    flops = float(m) * nr * m
+    out2 = {}
+    for label, tri in (("configured", t_raw), ("scaled", t_scaled)):
+        T, B0 = dev(tri), dev(bb)
+        Bw = B0.clone()
+        trsm = lambda: hb.dtrsm("L", "L", "N", "U", m, nr, 1.0, T, m, Bw, m)
+        for _ in range(2):
+            Bw.copy_(B0)
+            torch.cuda.synchronize()
+            trsm()
+        times = []
+        for _ in range(5):
+            Bw.copy_(B0)
+            torch.cuda.synchronize()
+            times.append(timed(torch, stream, trsm, 1))
+        ms = min(times)
+        e = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+        e["roofline"] = roof(e["tflops"])
+        if cpu is not None:
+            bw = bb.copy(order="F")
+            cpu.dtrsm("L", "L", "N", "U", m, nr, 1.0, tri, m, bw, m)
+            if label == "scaled":
+                e["bit_identical_to_cpu"] = bool(np.array_equal(
+                    bw.view(np.uint64), host(Bw, m, nr).view(np.uint64)))
+                cw = bb.copy(order="F")
+
+                def cpu_trsm():
+                    cw[:] = bb
+                    cpu.dtrsm("L", "L", "N", "U", m, nr, 1.0, tri, m, cw, m)
+                t = cpu_time(cpu_trsm, 2)
+                e["cpu"] = {"ms": t * 1e3, "tflops": flops / t / 1e12, "cores": 1,
+                            "kind": cpu.kind}
+        out2["dtrsm_" + label] = e
+    out2["dtrsm_workload"] = ("dtrsm side=L uplo=L trans=N diag=U, M=4096 N=512; "
+                              "configured: off-diagonal U[-1,1]; scaled: times 1/4096")
+
+    # Config 2b: dgetrf n = 4096.
+    n = 4096
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    flops = 2.0 / 3.0 * n ** 3
+    A0 = dev(a)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    times = []
+    for it in range(4):
+        Aw = A0.clone()
+        torch.cuda.synchronize()
+        times.append(timed(torch, stream, lambda: hb.dgetrf(n, n, Aw, n, ipiv), 1))
+    ms = min(times[1:])
+    lu = Aw.view(n, n).t()  # lu[i, j] = LU(i, j)
+    L = torch.tril(lu, -1) + torch.eye(n, dtype=torch.float64, device="cuda")
+    U = torch.triu(lu)
+    piv = ipiv.cpu().numpy()
+    perm = np.arange(n)
+    for i in range(n):
+        j = piv[i] - 1
+        perm[i], perm[j] = perm[j], perm[i]
+    Am = A0.view(n, n).t()
+    PA = Am[torch.from_numpy(perm).cuda()]
+    eps = np.finfo(np.float64).eps / 2
+    norm1 = lambda x: float(x.abs().sum(dim=0).max().item())
+    ratio = norm1(L @ U - PA) / n / norm1(Am) / eps
+    e = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "lu_residual_ratio": ratio,
+         "ratio_definition": "||P L U - A||_1 / (n ||A||_1 eps), eps = 2^-53 (LAPACK xGET01)"}
+    e["roofline"] = roof(e["tflops"])
+    if cpu is not None:
+        aw = a.copy(order="F")
+        pw = np.zeros(n, np.int32)
+        cpu.set_threads(1)
+        t0 = time.perf_counter()
+        cpu.dgetrf(n, n, aw, n, pw)
+        t = time.perf_counter() - t0
+        cpu.set_threads(cpu_threads())
+        e["ipiv_equal_to_cpu"] = bool(np.array_equal(pw, piv))
+        e["bit_identical_to_cpu"] = bool(np.array_equal(
+            aw.view(np.uint64), host(Aw, n, n).view(np.uint64)))
+        e["cpu"] = {"ms": t * 1e3, "tflops": flops / t / 1e12, "cores": 1, "kind": cpu.kind}
+    out2["dgetrf"] = e
+    out2["dgetrf_workload"] = "dgetrf n=4096, U[-1,1], partial pivoting (2/3 n^3 flops)"
+    res["config2"] = out2
+    return res
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -703,11 +952,24 @@ def run_ours(args):
     dm_achieved = 2.0 * n ** 3 / (dm_ms * 1e-3) / 1e12 if dm_ms > 0 else None
 
     cpu = None
+    cpu_path = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_path = CpuPath()
         threads = cpu_threads()
-        tf, sample = cpu_dgemm_sample(n, max(64, n // 8), 3, threads)
-        cpu = {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-               "sample": sample}
+        cpu_path.set_threads(threads)
+        smp = DgemmSample(cpu_path, n, cpu_sample_cols(n, threads))
+        times = cpu_steps(smp, 3, 1)
+        tf = smp.flops / (sum(times) / len(times)) / 1e12
+        cpu = {"value": tf, "unit": "TFLOP/s", "cores": threads, "kind": cpu_path.kind,
+               "sample": smp.describe() + ", mean of 3",
+               "single_thread": cpu_single_thread(cpu_path, n)}
+
+    small = None
+    if rank == 0 and world == 1 and not args.no_small:
+        small = run_small_configs(torch, hb, stream, cpu_path, fp64_peak)
+    auto = None
+    if rank == 0 and world == 1 and not args.no_sweep:
+        auto = run_auto_slices(torch, hb, stream, n)
 
     solvers = None
     if rank == 0 and world == 1 and not args.no_dgesv:
@@ -728,10 +990,10 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int8 slices -> f64", "data": "synthetic (seeded)",
-            "config": {"workload": workload_name(n), "path": "emulated FP64 (Ozaki INT8 "
-                       "slices on tcgen05), slices chosen automatically",
-                       "slices": S, "parallelism": f"replicas x{world}",
-                       "l2": "inputs (2 x 512 MiB FP64) larger than L2"},
+            "config": workload_config(n),
+            "path": "emulated FP64 (Ozaki INT8 slices on tcgen05), slice count chosen "
+                    "from the inputs' exponent spread",
+            "slices": S, "parallelism": f"replicas x{world}",
             "fp64_accurate": d["fp64_accurate"],
             "error": {"emulated": d["err_emulated"], "plain": d["err_plain"],
                       "measure": "normwise ||C - AB||_F / (||A||_F ||B||_F) on 64 columns "
@@ -760,7 +1022,11 @@ def run_ours(args):
         }
         if "sweep" in d:
             line["slice_sweep"] = d["sweep"]
-            line["spread30"] = d["spread30"]
+        if auto is not None:
+            line["auto_slices"] = auto
+        if small is not None:
+            line["config1"] = small["config1"]
+            line["config2"] = small["config2"]
         if solvers is not None:
             line["solvers"] = solvers
         if batched is not None:

@@ -14,7 +14,7 @@ from tests.oracle_lib import rand, same_bits
 
 pytestmark = pytest.mark.gpu
 
-CUDA_ERROR_LAUNCH_TIMEOUT = 6
+CUDA_ERROR_LAUNCH_TIMEOUT = 702  # cudaErrorLaunchTimeout
 DEFAULT_POLLS = 1 << 26
 
 
