@@ -933,8 +933,9 @@ def run_ours(args):
     d = run_dgemm(args, torch, hb, stream, dist, world, rank, local)
 
     peaks, peak_kind = measured_peaks()
-    int8_peak = 2.0 * float(peaks.get("bf16_tflops", FALLBACK_BF16_TFLOPS))
+    int8_inferred = 2.0 * float(peaks.get("bf16_tflops", FALLBACK_BF16_TFLOPS))
     fp64_peak = float(lib.hwyblas_fp64_peak_tflops())
+    int8_peak = float(lib.hwyblas_int8_peak_tops())
     S = d["slices"]
     # Dominant kernel: the slice-product GEMM. Algorithmic work = INT8
     # multiply-adds of all S(S+1)/2 slice products, 2 n^3 ops each, spread
@@ -1008,8 +1009,11 @@ def run_ours(args):
                          "traffic_unit": "bytes per launch (DRAM, ncu)",
                          "kernel": "OzakiGemmKernel (slice products, "
                                    f"{d['ozaki_launches_per_step']:.0f} launches per step)",
-                         "peak_source": f"2 x bf16_tflops of {peak_kind} MEASURED_PEAKS "
-                                        "(INT8 dense rate = 2 x bf16)"},
+                         "peak_source": "measured tcgen05.mma kind::i8 issue rate "
+                                        "(hwyblas_int8_peak_tops)",
+                         "peak_inferred": int8_inferred,
+                         "peak_inferred_source": f"2 x bf16_tflops of {peak_kind} "
+                                                 "MEASURED_PEAKS"},
             "roofline_plain": {"bound": "tensor", "achieved": dm_achieved,
                                "peak": fp64_peak, "unit": "TFLOP/s (FP64)",
                                "frac": dm_achieved / fp64_peak if dm_achieved else None,

@@ -76,6 +76,36 @@ __device__ __forceinline__ void PrefetchTmap(const CUtensorMap* map) {
                : "memory");
 }
 
+// tcgen05 (5th-generation tensor core) helpers.
+//
+// Shared-memory matrix descriptor of a K-major, swizzled operand tile whose
+// rows are kb_bytes long (128, 64 or 32): leading byte offset 16 B (unused
+// with swizzling), stride byte offset = 8 rows, descriptor version 1.
+__device__ __forceinline__ uint64_t SmemDesc(uint32_t addr, int kb_bytes) {
+  const uint64_t layout = kb_bytes == 128 ? 2 : (kb_bytes == 64 ? 4 : 6);
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (1ull << 16) |
+         (static_cast<uint64_t>((8 * kb_bytes) >> 4) << 32) | (1ull << 46) |
+         (layout << 61);
+}
+
+__device__ __forceinline__ void MmaI8(uint32_t d_tmem, uint64_t a_desc,
+                                      uint64_t b_desc, uint32_t idesc,
+                                      uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void MmaCommit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+      ::"r"(SmemAddr(bar))
+      : "memory");
+}
+
+
 // Grid barrier for cooperative launches: `counter` is zeroed before the
 // launch; barrier number `gen` (1, 2, ...) completes when all `nblocks`
 // blocks have arrived `gen` times. Bounded; false on timeout.

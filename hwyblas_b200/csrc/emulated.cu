@@ -217,31 +217,6 @@ __global__ void __launch_bounds__(512)
 // ---------------------------------------------------------------------------
 // tcgen05 helpers.
 
-__device__ __forceinline__ uint64_t SmemDesc(uint32_t addr, int kb_bytes) {
-  // K-major, swizzled: LBO 16 B (unused), SBO = 8 rows, version 1.
-  const uint64_t layout = kb_bytes == 128 ? 2 : (kb_bytes == 64 ? 4 : 6);
-  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (1ull << 16) |
-         (static_cast<uint64_t>((8 * kb_bytes) >> 4) << 32) | (1ull << 46) |
-         (layout << 61);
-}
-
-__device__ __forceinline__ void MmaI8(uint32_t d_tmem, uint64_t a_desc,
-                                      uint64_t b_desc, uint32_t idesc,
-                                      uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void MmaCommit(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-      ::"r"(SmemAddr(bar))
-      : "memory");
-}
-
 __device__ __forceinline__ void TmemLoad32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,"

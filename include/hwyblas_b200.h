@@ -794,6 +794,11 @@ HWYBLAS_API double hwyblas_kernel_timer_read(int* launches);
  * a DMMA issue-rate loop; the FP64 roofline denominator. No counterpart in
  * the reference. */
 HWYBLAS_API double hwyblas_fp64_peak_tflops(void);
+/* Measured INT8 throughput of the current device's 5th-generation tensor
+ * cores (TOPS), from a tcgen05.mma kind::i8 issue loop on every SM; the
+ * roofline denominator of the emulated GEMM's slice products. No counterpart
+ * in the reference. */
+HWYBLAS_API double hwyblas_int8_peak_tops(void);
 /* Test hook for the bounded waits: sets how many times each CTA of the LU
  * panel's cooperative pivot exchange (panels of more than 16 x 1024 rows)
  * polls for its peers before it gives up, sets the timeout status (reported
