@@ -18,7 +18,7 @@ __all__ = [
     "dgetrf2", "dgetrs", "dgesv", "slaswp", "sgetrf", "sgetrf2", "sgetrs", "sgesv",
     "dpotrf", "dpotrf2", "dpotrs", "dposv", "ssyrk", "spotrf", "spotrf2", "spotrs",
     "sposv", "cblas_dgemm", "cblas_sgemm", "cblas_dtrsm", "cblas_strsm", "cblas_idamax",
-    "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref",
+    "ErrorCapture", "launch_count", "set_stream", "dgemm_emulated", "dgemm_ddref", "dresidual_dd",
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
     "KERNEL_LU_LEAF", "getrf_batched", "getrs_batched", "gemm_batched",
@@ -48,7 +48,7 @@ from ._api import (  # noqa: E402  (needs lib())
     dgesv, slaswp, sgetrf, sgetrf2, sgetrs, sgesv, dpotrf, dpotrf2, dpotrs, dposv,
     ssyrk, spotrf, spotrf2, spotrs, sposv,
     cblas_dgemm, cblas_sgemm, cblas_dtrsm, cblas_strsm, cblas_idamax, ErrorCapture, launch_count, set_stream,
-    dgemm_emulated, dgemm_ddref, idamax_noalloc, dgesv_mixed, dposv_mixed,
+    dgemm_emulated, dgemm_ddref, dresidual_dd, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
     KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,
     trsm_batched, symm, syr2k, gemmtr, trmm, cblas_level3, getri, trtri, gerfs, zgemm, ztrsm, zgetrf, zlaswp, zgetrs, zgesv,

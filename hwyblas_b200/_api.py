@@ -362,6 +362,12 @@ def dgemm_ddref(transa, transb, m, k, a, lda, b, ldb, n, cols, out, ldo):
                               _ptr(out), _i(ldo))
 
 
+def dresidual_dd(n, nrhs, a, lda, x, ldx, b, ldb, r, ldr):
+    """r = b - A x with extra precision (double-double accumulation)."""
+    lib().hwyblas_dresidual_dd(_i(n), _i(nrhs), _ptr(a), _i(lda), _ptr(x), _i(ldx),
+                               _ptr(b), _i(ldb), _ptr(r), _i(ldr))
+
+
 def dgesv_mixed(n, nrhs, a, lda, ipiv, b, ldb, x, ldx):
     """Mixed-precision solve (DSGESV semantics). Returns (info, iter)."""
     info, it = ctypes.c_int(0), ctypes.c_int(0)

@@ -2219,6 +2219,38 @@ HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
   hb::Finish("DGEMM_DDREF");
 }
 
+HWYBLAS_API void hwyblas_dresidual_dd(const hwyblas_int* n_p, const hwyblas_int* nrhs_p,
+                                      const double* a, const hwyblas_int* lda_p,
+                                      const double* x, const hwyblas_int* ldx_p,
+                                      const double* b, const hwyblas_int* ldb_p, double* r,
+                                      const hwyblas_int* ldr_p) {
+  const int n = *n_p, nrhs = *nrhs_p, lda = *lda_p, ldx = *ldx_p, ldb = *ldb_p,
+            ldr = *ldr_p;
+  int info = 0;
+  if (n < 0) info = 1;
+  else if (nrhs < 0) info = 2;
+  else if (lda < std::max(1, n)) info = 4;
+  else if (ldx < std::max(1, n)) info = 6;
+  else if (ldb < std::max(1, n)) info = 8;
+  else if (ldr < std::max(1, n)) info = 10;
+  if (info != 0) {
+    hb::ReportError("DRESIDUAL_DD", info);
+    return;
+  }
+  if (n == 0 || nrhs == 0) return;
+  hb::Staged<double> sa, sx, sb, sr;
+  if (!sa.In(a, lda, n, n, hb::kWsStageA, true)) return;
+  if (!sx.In(x, ldx, n, nrhs, hb::kWsStageX, true)) return;
+  if (!sb.In(b, ldb, n, nrhs, hb::kWsStageB, true)) return;
+  if (!sr.In(r, ldr, n, nrhs, hb::kWsStageC, false)) return;
+  double* part = static_cast<double*>(
+      hb::Workspace(hb::kWsResidual, hb::ResidualDdPartBytes(n, nrhs)));
+  if (part == nullptr) return;
+  hb::ResidualDd(n, nrhs, sa.dev, sa.ld, sb.dev, sb.ld, sx.dev, sx.ld, sr.dev, sr.ld, part);
+  sr.Out();
+  hb::Finish("DRESIDUAL_DD");
+}
+
 HWYBLAS_API void hwyblas_set_stream(void* stream) {
   hb::Context& c = Ctx();
   c.stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : c.own_stream;

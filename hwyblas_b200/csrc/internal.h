@@ -97,7 +97,8 @@ enum WorkspaceSlot : int {
   kWsSplitK = 29,      // per-chunk accumulators of a split DMMA GEMM
   kWsZFactor = 30,     // aligned copy of a complex matrix being factored
   kWsZFactorB = 31,    // aligned copy of the right-hand sides of its solve
-  kNumWorkspaceSlots = 32
+  kWsResidual = 32,    // hwyblas_dresidual_dd partial sums
+  kNumWorkspaceSlots = 33
 };
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
@@ -294,6 +295,14 @@ void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,
 // Host-side wait-timeout check: returns true (and reports) if any kernel on
 // the context set the timeout flag since the last check. Synchronises.
 bool CheckDeviceStatus(const char* what);
+
+// r := b - A x (A n x n, x, b, r n x nrhs, device) with extra precision:
+// double-double accumulation of exactly split products, rounded once. part:
+// ResidualDdPartBytes(n, nrhs) bytes of device scratch.
+void ResidualDd(int n, int nrhs, const double* a, long long lda, const double* b,
+                long long ldb, const double* x, long long ldx, double* r, long long ldr,
+                double* part);
+size_t ResidualDdPartBytes(int n, int nrhs);
 
 // Mixed-precision solvers (LAPACK DSGESV / DSPOSV semantics) on device data;
 // the trailing updates of the factorization use `slices` INT8 slices. Return

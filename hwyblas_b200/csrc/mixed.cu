@@ -13,6 +13,11 @@
 // the FP64 path ran (-2 non-finite A, -3 factorization breakdown, -31 no
 // convergence).
 //
+// The residual of the refinement is extra-precise (double-double accumulation
+// of exactly split products, rounded once), so x converges to the solution of
+// A x = b to about the last bit rather than to the FP64 residual's
+// cond(A) eps.
+//
 // Factorization (right-looking, block nb):
 //   LU        panel (pivot search and diagonal block) in FP64 by the
 //             recursive LU, U12 by an FP64 triangular solve, and the
@@ -144,6 +149,74 @@ __global__ void ResidualFinishKernel(int n, int nrhs, int chunks,
   for (int c = 0; c < chunks; ++c)
     s += part[(static_cast<long long>(c) * nrhs + q) * n + i];
   r[i + q * ldr] = b[i + q * ldb] - s;
+}
+
+// Residual with extra precision (few right-hand sides at a time): every
+// product a(i, k) x(k, q) is split exactly into p = fl(a x) and
+// e = fma(a, x, -p); the p are summed in double-double (TwoSum, Knuth) and the
+// e in FP64, per chunk of kResK columns. part_hi / part_lo are [c][q][i].
+__global__ void __launch_bounds__(kResRows)
+    ResidualDdPartialKernel(int n, int nrhs, const double* a, long long lda,
+                            const double* x, long long ldx, double* part_hi,
+                            double* part_lo) {
+  __shared__ double sx[kResRhs][kResK];
+  const int k0 = blockIdx.y * kResK, kc = min(kResK, n - k0);
+  for (int idx = threadIdx.x; idx < kResRhs * kResK; idx += kResRows) {
+    const int q = idx / kResK, k = idx % kResK;
+    sx[q][k] = (q < nrhs && k < kc) ? x[k0 + k + q * ldx] : 0.0;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * kResRows + threadIdx.x;
+  if (i >= n) return;
+  double hi[kResRhs], lo[kResRhs];
+#pragma unroll
+  for (int q = 0; q < kResRhs; ++q) hi[q] = lo[q] = 0.0;
+  const double* ai = a + i + static_cast<long long>(k0) * lda;
+  for (int k = 0; k < kc; ++k) {
+    const double v = ai[static_cast<long long>(k) * lda];
+#pragma unroll
+    for (int q = 0; q < kResRhs; ++q) {
+      if (q < nrhs) {
+        const double p = v * sx[q][k];
+        const double pe = fma(v, sx[q][k], -p);
+        const double s = hi[q] + p;
+        const double bb = s - hi[q];
+        const double e = (hi[q] - (s - bb)) + (p - bb);
+        hi[q] = s;
+        lo[q] += e + pe;
+      }
+    }
+  }
+  const long long off = static_cast<long long>(blockIdx.y) * nrhs * n;
+#pragma unroll
+  for (int q = 0; q < kResRhs; ++q) {
+    if (q < nrhs) {
+      part_hi[off + static_cast<long long>(q) * n + i] = hi[q];
+      part_lo[off + static_cast<long long>(q) * n + i] = lo[q];
+    }
+  }
+}
+
+// r(i, q) = b(i, q) - sum of the chunks (in chunk order), in double-double,
+// rounded once.
+__global__ void ResidualDdFinishKernel(int n, int nrhs, int chunks,
+                                       const double* part_hi, const double* part_lo,
+                                       const double* b, long long ldb, double* r,
+                                       long long ldr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.y;
+  if (i >= n || q >= nrhs) return;
+  double hi = b[i + q * ldb], lo = 0.0;
+  for (int c = 0; c < chunks; ++c) {
+    const long long at = (static_cast<long long>(c) * nrhs + q) * n + i;
+    const double p = -part_hi[at];
+    const double s = hi + p;
+    const double bb = s - hi;
+    const double e = (hi - (s - bb)) + (p - bb);
+    hi = s;
+    lo += e - part_lo[at];
+  }
+  r[i + q * ldr] = hi + lo;
 }
 
 __global__ void AxpyMatrixKernel(int n, int nrhs, const double* d, long long ldd,
@@ -719,7 +792,7 @@ bool AllocBuffers(int n, int nrhs, bool sym, MixedBuffers* bf) {
   const size_t inv_elems = nblk * kTb * kTb;
   const size_t r_elems = static_cast<size_t>(bf->ldr) * nrhs;
   const size_t part_elems =
-      std::max(chunks * std::min(nrhs, kResRhs) * n, rowparts * n);
+      std::max(2 * chunks * std::min(nrhs, kResRhs) * n, rowparts * n);
   const size_t norm_elems = 1 + 3 * static_cast<size_t>(nrhs);
   // Chained solves launch at most num_sms / ceil(nblk / kChainSlots) chains
   // of nblk flags, which is at most max(nblk, kChainSlots * num_sms); the
@@ -795,6 +868,36 @@ void Residual(int n, int nrhs, const double* a, long long lda, const double* b,
   CountLaunch(2);
   LaunchFailed("mixed residual");
 }
+
+}  // namespace
+
+// r := b - A x with extra precision: each entry is the exact value up to a
+// relative error of about n eps^2 |A| |x| / |r|, then rounded once. Groups of
+// kResRhs right-hand sides; `part` holds 2 chunks kResRhs n doubles.
+void ResidualDd(int n, int nrhs, const double* a, long long lda, const double* b,
+                long long ldb, const double* x, long long ldx, double* r, long long ldr,
+                double* part) {
+  cudaStream_t st = Ctx().stream;
+  const int chunks = (n + kResK - 1) / kResK;
+  for (int q0 = 0; q0 < nrhs; q0 += kResRhs) {
+    const int g = std::min(kResRhs, nrhs - q0);
+    double* ph = part;
+    double* pl = part + static_cast<size_t>(chunks) * g * n;
+    ResidualDdPartialKernel<<<dim3((n + kResRows - 1) / kResRows, chunks), kResRows, 0, st>>>(
+        n, g, a, lda, x + q0 * ldx, ldx, ph, pl);
+    ResidualDdFinishKernel<<<dim3((n + 255) / 256, g), 256, 0, st>>>(
+        n, g, chunks, ph, pl, b + q0 * ldb, ldb, r + q0 * ldr, ldr);
+    CountLaunch(2);
+    if (LaunchFailed("extra-precise residual")) return;
+  }
+}
+
+size_t ResidualDdPartBytes(int n, int nrhs) {
+  const size_t chunks = (n + kResK - 1) / kResK;
+  return sizeof(double) * 2 * chunks * std::min(nrhs, kResRhs) * static_cast<size_t>(n);
+}
+
+namespace {
 
 // Column max-norms of `count` n x nrhs matrices into host arrays (waits for
 // the stream); norms[c][q] = max_i |m_c(i, q)|.
@@ -1118,15 +1221,25 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
   std::vector<char> settled_col(nrhs, 0);
   const double* mats[3] = {x, bf.r, bf.d};
   const long long lds[3] = {ldx, bf.ldr, bf.ldr};
+  // The residual is extra-precise (ResidualDd), so the corrections converge
+  // to the solution of A x = b itself rather than stalling at the FP64
+  // residual's noise (cond(A) eps). For few right-hand sides it costs what
+  // the FP64 GEMV costs (both read A once); for many, the FP64 DMMA residual
+  // runs until the FP64 tests pass and the extra-precise one then polishes.
+  bool extra = nrhs < kResRhs;
   for (int it = 0; it < kItMax; ++it) {
-    Residual(n, nrhs, a, lda, b, ldb, x, ldx, bf);
+    if (extra) {
+      ResidualDd(n, nrhs, a, lda, b, ldb, x, ldx, bf.r, bf.ldr, bf.part);
+    } else {
+      Residual(n, nrhs, a, lda, b, ldb, x, ldx, bf);
+    }
     MixedSolve(lu, n, nrhs, bf, bf.r, bf.ldr, bf.d, bf.ldr);
     if (!ColumnNorms(n, nrhs, 3, mats, lds, bf, &nm)) return -kItMax - 1;
     AxpyMatrixKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(n, nrhs, bf.d, bf.ldr,
                                                                   x, ldx);
     CountLaunch();
     // A column is done once it has met both tests; later corrections only
-    // move it within the noise of the FP64 residual.
+    // move it within the last bit.
     bool done = true;
     for (int q = 0; q < nrhs; ++q) {
       const double xn = nm[0][q], rn = nm[1][q], dn = nm[2][q];
@@ -1136,7 +1249,12 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
       if (!settled_col[q]) done = false;
       dprev[q] = dn;
     }
-    if (done) return it + 1;
+    if (done && extra) return it + 1;
+    if (done) {
+      extra = true;
+      std::fill(settled_col.begin(), settled_col.end(), 0);
+      std::fill(dprev.begin(), dprev.end(), INFINITY);
+    }
   }
   return -kItMax - 1;
 }

@@ -689,6 +689,19 @@ HWYBLAS_API void hwyblas_dgemm_ddref(const char* transa, const char* transb,
                                      const hwyblas_int* n,
                                      const hwyblas_int* cols, double* out,
                                      const hwyblas_int* ldo);
+/* R = B - A X (A n x n; X, B, R n x nrhs; column-major) with extra
+ * precision: every product is split exactly into its rounded value and
+ * error, the products are summed in double-double and each entry is rounded
+ * once, so its error is about n eps^2 |A| |X| rather than n eps |A| |X|. The
+ * residual of the mixed solvers' refinement, and the yardstick against which
+ * the solvers' forward errors are stated. Invalid arguments are reported
+ * with their positions (1, 2, 4, 6, 8, 10). No counterpart in the
+ * reference. */
+HWYBLAS_API void hwyblas_dresidual_dd(const hwyblas_int* n, const hwyblas_int* nrhs,
+                                      const double* a, const hwyblas_int* lda,
+                                      const double* x, const hwyblas_int* ldx,
+                                      const double* b, const hwyblas_int* ldb, double* r,
+                                      const hwyblas_int* ldr);
 
 /* Mixed-precision solve of A X = B (LAPACK DSGESV semantics; the reference
  * has no mixed-precision solver, README.md:81). The LU's trailing updates run

@@ -211,3 +211,76 @@ def test_mixed_quick_returns_and_invalid(hb):
                           ("DGESV_MIXED", 7), ("DGESV_MIXED", 9), ("DPOSV_MIXED", 1),
                           ("DPOSV_MIXED", 5), ("DPOSV_MIXED", 9)]
     assert np.all(x == 7.0)
+
+
+# ---------------------------------------------------------------------------
+# The extra-precise residual and the solvers at the configuration's own size.
+
+@pytest.mark.parametrize("n,nrhs", [(700, 1), (1500, 3), (900, 20)])
+def test_dresidual_dd_matches_exact(hb, n, nrhs):
+    """b - A x with b = fl(A x): the residual is all cancellation. The
+    extra-precise residual is within a few n eps^2 |A||x| of the exact one
+    (computed on the CPU, tests/exact_ref.py), far below the n eps |A||x| an
+    FP64 residual can reach."""
+    from tests.exact_ref import exact_residual
+    rng = np.random.default_rng(n + nrhs)
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n))))
+    x = np.asfortranarray(rng.uniform(-1, 1, (n, nrhs)))
+    b = np.asfortranarray(a @ x)
+    r = np.zeros((n, nrhs), order="F")
+    hb.dresidual_dd(n, nrhs, a, n, x, n, b, n, r, n)
+    absax = np.abs(a) @ np.abs(x)
+    rows = np.arange(0, n, 7)
+    for q in range(0, nrhs, max(1, nrhs // 3)):
+        exact = exact_residual(a[rows], x[:, q], b[rows, q])
+        bound = 8 * n * EPS * EPS * absax[rows, q] + np.spacing(np.abs(exact))
+        assert np.all(np.abs(r[rows, q] - exact) <= bound)
+        # An FP64 residual misses by far more than this bound.
+        assert np.max(np.abs((b[rows, q] - a[rows] @ x[:, q]) - exact) / bound) > 10
+
+
+def solve_to_last_bit(hb, orc, a, lu, ipiv, b, x0):
+    """The solution of A x = b to about the last bit: x0 refined twice with
+    the extra-precise residual and the oracle's FP64 LU factors."""
+    n, nrhs = b.shape
+    x = x0.copy(order="F")
+    r = np.zeros((n, nrhs), order="F")
+    for _ in range(2):
+        hb.dresidual_dd(n, nrhs, a, n, x, n, b, n, r, n)
+        d = r.copy(order="F")
+        assert orc.dgetrs("N", n, nrhs, lu, n, ipiv, d, n) == 0
+        x += d
+    return x
+
+
+def test_dgesv_mixed_config4_n8192(hb, orc):
+    """The configuration's case at n = 8192, cond 1e6, nrhs 1 and 64: the
+    mixed solver meets DSGESV's backward criterion and its forward error,
+    against the solution of A x = b to the last bit, is at most the oracle
+    dgesv's (the reference's FP64 LU order) on the same system."""
+    import os
+    orc.set_threads(os.cpu_count() or 1)
+    rng = np.random.default_rng(8192)
+    n = 8192
+    a = householder_matrix(rng, n, 1e6)
+    lu = a.copy(order="F")
+    ipiv = np.zeros(n, np.int32)
+    assert orc.dgetrf(n, n, lu, n, ipiv) == 0
+    anrm = np.abs(a).sum(axis=1).max()
+    for nrhs in (1, 64):
+        xt = rng.uniform(-1, 1, (n, nrhs))
+        b = np.asfortranarray(a @ xt)
+        xp = b.copy(order="F")
+        assert orc.dgetrs("N", n, nrhs, lu, n, ipiv, xp, n) == 0
+        xm = np.zeros((n, nrhs), order="F")
+        a_in = a.copy(order="F")
+        info, it = hb.dgesv_mixed(n, nrhs, a_in, n, np.zeros(n, np.int32), b, n, xm, n)
+        assert info == 0 and it > 0, (info, it)
+        assert same_bits(a_in, a)
+        xs = solve_to_last_bit(hb, orc, a, lu, ipiv, b, xm)
+        e_mixed, e_plain = fwd_err(xm, xs), fwd_err(xp, xs)
+        assert e_mixed <= e_plain, (nrhs, e_mixed, e_plain)
+        r = np.zeros((n, nrhs), order="F")
+        hb.dresidual_dd(n, nrhs, a, n, xm, n, b, n, r, n)
+        for q in range(nrhs):
+            assert np.abs(r[:, q]).max() <= np.abs(xm[:, q]).max() * anrm * EPS * np.sqrt(n)
