@@ -493,9 +493,10 @@ def householder_device(torch, n, cond, seed):
 
 
 def solve_to_last_bit(torch, hb, n, nrhs, A, lu, ipiv, Bm, x0):
-    """The solution of A x = b to about the last bit: x0 refined twice with
-    the extra-precise residual (hwyblas_dresidual_dd) and the plain FP64 LU
-    factors (bit-identical to the reference's). Column-major flat tensors."""
+    """The solution of A x = b to about the last bit: x0 (the plain FP64
+    solution) refined twice with the extra-precise residual
+    (hwyblas_dresidual_dd) and the plain FP64 LU factors (bit-identical to the
+    reference's). Column-major flat tensors."""
     x = x0.clone()
     r = torch.empty_like(x)
     for _ in range(2):
@@ -511,7 +512,8 @@ def run_solvers(args, torch, hb, stream):
     errors are stated against the solution of A x = b to the last bit."""
     n = args.gesv_n
     res = {"n": n, "fwd_err": "||x - x*||_F / ||x*||_F, x* = the solution of A x = b to "
-                              "the last bit (two steps of extra-precise refinement)"}
+                              "the last bit (the plain solution after two steps of "
+                              "extra-precise refinement)"}
     gesv_flops = lambda nrhs: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * nrhs
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
     cases = [(1e6, 1), (1e6, 64), (1e2, 1), (1e10, 1)]
@@ -549,7 +551,7 @@ def run_solvers(args, torch, hb, stream):
                          "solves_per_s": 1.0 / best, "info": info}
             if it is not None:
                 out[kind]["iterations"] = it
-        xs = solve_to_last_bit(torch, hb, n, nrhs, A, lu, piv, Bm, sols["mixed"])
+        xs = solve_to_last_bit(torch, hb, n, nrhs, A, lu, piv, Bm, sols["plain"])
         for kind in ("plain", "mixed"):
             out[kind]["fwd_err"] = float((torch.linalg.norm(sols[kind] - xs) /
                                           torch.linalg.norm(xs)).item())
@@ -589,7 +591,7 @@ def run_solvers(args, torch, hb, stream):
     # factorization serves the two correction steps).
     lu = A.clone()
     hb.dgetrf(n, n, lu, n, ipiv)
-    xs = solve_to_last_bit(torch, hb, n, 1, A, lu, ipiv, Bm, sols["mixed"])
+    xs = solve_to_last_bit(torch, hb, n, 1, A, lu, ipiv, Bm, sols["plain"])
     for kind in ("plain", "mixed"):
         out[kind]["fwd_err"] = float((torch.linalg.norm(sols[kind] - xs) /
                                       torch.linalg.norm(xs)).item())

@@ -60,7 +60,8 @@ struct WorkspaceBuf {
 
 struct ThreadState {
   Context ctx;
-  WorkspaceBuf ws[kNumWorkspaceSlots];
+  WorkspaceBuf ws[2][kNumWorkspaceSlots];  // [bank][slot]
+  SideStream side;
   bool initialized = false;
   ~ThreadState() {
     // Device memory is released with the process; freeing here could run
@@ -99,10 +100,26 @@ Context& Ctx() {
   return t_state.ctx;
 }
 
+SideStream& Side() {
+  ThreadState& st = t_state;
+  Init(st);
+  SideStream& s = st.side;
+  if (!s.ok && s.stream == nullptr) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    s.ok = cudaStreamCreateWithPriority(&s.stream, cudaStreamNonBlocking, greatest) ==
+               cudaSuccess &&
+           cudaEventCreateWithFlags(&s.to_side, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&s.to_main, cudaEventDisableTiming) == cudaSuccess;
+    if (!s.ok) cudaGetLastError();
+  }
+  return s;
+}
+
 void* Workspace(int slot, size_t bytes) {
   ThreadState& st = t_state;
   Init(st);
-  WorkspaceBuf& w = st.ws[slot];
+  WorkspaceBuf& w = st.ws[st.ctx.ws_bank][slot];
   if (bytes == 0) bytes = 256;
   if (w.bytes < bytes) {
     if (w.ptr != nullptr) {

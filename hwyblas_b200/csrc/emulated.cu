@@ -241,6 +241,7 @@ struct OzakiParams {
   long long ldc;
   double* w;  // FP64 partial sums of the first pass (m x n, leading dim m)
   int* timeout_flag;
+  int lower_only;  // skip the tiles strictly above the diagonal of C
 };
 
 // Tile of this CTA in groups of 16 tile rows: consecutive CTAs walk down a
@@ -286,6 +287,9 @@ __global__ void __launch_bounds__(kEThreads, 1)
   constexpr int kNA = Cfg::kNA;
   int m0, n0;
   TileOrigin(p.m, p.n, &m0, &n0);
+  // A product whose lower triangle alone is wanted (a symmetric rank-k
+  // update): tiles strictly above the diagonal return before any set-up.
+  if (p.lower_only && n0 >= m0 + kEBM) return;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024 - (SmemAddr(smem_raw) & 1023)) & 1023);
@@ -739,7 +743,7 @@ int OzakiMaxK(int S) { return static_cast<int>((2147483647LL / (S * 16384LL)) / 
 // inputs were not finite, or slices == 0 found no S <= 8 as accurate as it).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite, int ws_set) {
+                  bool check_finite, int ws_set, bool lower_only) {
   const int ws_emul = ws_set ? kWsEmul2 : kWsEmul;
   const int ws_acc = ws_set ? kWsEmulAcc2 : kWsEmulAcc;
   const int ws_w = ws_set ? kWsEmulW2 : kWsEmulW;
@@ -824,6 +828,7 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                                                             static_cast<size_t>(m) * n))
                 : nullptr;
   p.timeout_flag = ctx.dev_status;
+  p.lower_only = lower_only ? 1 : 0;
   for (int k0 = 0; k0 < k; k0 += kchunk) {
     const int kc = std::min(kchunk, k - k0);
     SplitDispatch(S, a.sub(0, k0), m, kc, row_exp, slices_a, kp, st);

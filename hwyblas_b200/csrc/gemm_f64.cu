@@ -766,6 +766,17 @@ const T* Canonical(View<T> x, int rows, int cols, int slot, long long* ld_out) {
 template const double* Canonical(View<double>, int, int, int, long long*);
 template const float* Canonical(View<float>, int, int, int, long long*);
 
+// Bytes of the per-chunk partial sums a DMMA GEMM of m x n x k takes when it
+// splits over its KC chunks (few tiles, a long k), 0 when it runs unsplit.
+size_t DgemmSplitBytes(int m, int n, int k) {
+  const long long tiles =
+      static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+  const int nchunks = (k + 255) / 256;
+  const size_t pbytes = sizeof(double) * static_cast<size_t>(nchunks) * m * n;
+  return (nchunks >= 2 && tiles * 2 <= Ctx().num_sms && pbytes <= (size_t(1) << 31)) ? pbytes
+                                                                                     : 0;
+}
+
 void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
            double beta, double* c, int ldc, Part part, Tri tri) {
   Context& ctx = Ctx();
@@ -849,8 +860,8 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   // chunks of one tile run on different SMs, and a second kernel merges them
   // in order. Every chain and merge is the unsplit kernel's.
   const int nchunks = (k + 255) / 256;
-  const size_t pbytes = sizeof(double) * static_cast<size_t>(nchunks) * m * n;
-  if (nchunks >= 2 && tiles * 2 <= ctx.num_sms && pbytes <= (size_t(1) << 31)) {
+  const size_t pbytes = DgemmSplitBytes(m, n, k);
+  if (pbytes > 0) {
     double* partial = static_cast<double*>(Workspace(kWsSplitK, pbytes));
     if (partial != nullptr) {
       p.partial = partial;

@@ -57,7 +57,22 @@ struct Context {
   // that must stop after a failure, e.g. Cholesky's non-positive minor).
   const int* guard = nullptr;
   int last_error = 0;
+  // Workspace bank of the work being enqueued: 0 on the context's stream, 1
+  // on the side stream (see OnSide), so that the two streams never share a
+  // scratch buffer.
+  int ws_bank = 0;
 };
+
+// The calling thread's second stream (highest priority) with two events, for
+// look-ahead: work that a later step needs first runs there while the
+// context's stream does the bulk of the current step. ok is false if the
+// stream could not be created (callers then stay on one stream).
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t to_side = nullptr, to_main = nullptr;
+  bool ok = false;
+};
+SideStream& Side();
 
 // The calling thread's context on the current device (created on first use).
 Context& Ctx();
@@ -98,8 +113,32 @@ enum WorkspaceSlot : int {
   kWsZFactor = 30,     // aligned copy of a complex matrix being factored
   kWsZFactorB = 31,    // aligned copy of the right-hand sides of its solve
   kWsResidual = 32,    // hwyblas_dresidual_dd partial sums
-  kNumWorkspaceSlots = 33
+  kWsMixedInv = 33,    // mixed Cholesky: the inverse of a diagonal block
+  kNumWorkspaceSlots = 34
 };
+
+// Makes `to` wait for the work enqueued on `from` so far.
+inline void StreamAfter(cudaEvent_t ev, cudaStream_t from, cudaStream_t to) {
+  if (from == to) return;
+  cudaEventRecord(ev, from);
+  cudaStreamWaitEvent(to, ev, 0);
+}
+
+// Enqueues f's work on the side stream with the second workspace bank.
+template <typename F>
+void OnSide(F f) {
+  Context& ctx = Ctx();
+  SideStream& side = Side();
+  const cudaStream_t saved = ctx.stream;
+  const int bank = ctx.ws_bank;
+  if (side.ok) {
+    ctx.stream = side.stream;
+    ctx.ws_bank = 1;
+  }
+  f();
+  ctx.stream = saved;
+  ctx.ws_bank = bank;
+}
 
 // Records a CUDA error on the context and prints it; returns true if `e` is
 // an error.
@@ -135,6 +174,9 @@ void KernelTimerStop(cudaEvent_t start, cudaStream_t stream);
 // multiplied, so every chain is the reference's.
 void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
            double beta, double* c, int ldc, Part part = kAll, Tri tri = kTriNone);
+// Bytes of the partial sums Dgemm takes from kWsSplitK when it splits an
+// m x n x k product over its KC chunks (0 when it does not split).
+size_t DgemmSplitBytes(int m, int n, int k);
 // FP32 (chunks of 384), FFMA on the CUDA cores.
 void Sgemm(int m, int n, int k, float alpha, View<float> a, View<float> b,
            float beta, float* c, int ldc, Part part = kAll, Tri tri = kTriNone);
@@ -283,10 +325,11 @@ void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
 // synchronization (callers whose inputs are known finite, or that detect a
 // non-finite result themselves). ws_set 1 takes a second set of workspace
 // slots, for a call that runs concurrently with another one on a second
-// stream.
+// stream. lower_only: only C's lower triangle is wanted (tiles of C strictly
+// above its diagonal are skipped; the diagonal tiles are computed whole).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite = true, int ws_set = 0);
+                  bool check_finite = true, int ws_set = 0, bool lower_only = false);
 int OzakiMaxK(int S);
 // out(:, jj) = op(A) op(B)(:, cols[jj]) in double-double (error reference).
 void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,

@@ -51,6 +51,17 @@ void Getrf2(int m, int n, T* a, int lda, int* ipiv, int* info) {
   GetrfRec<T>(m, n, a, lda, ipiv, info, 0);
 }
 
+// Blocked LU with a look-ahead of one panel. The reference's sequence of
+// calls per panel j (getrf.cc:243-276) is kept, and so is every element's
+// arithmetic; only the order of calls that touch disjoint columns changes:
+// on the side stream, panel j's interchanges, triangular solve and update
+// are applied to the next panel's columns first and the next panel is
+// factored, while the context's stream applies them to the columns left of
+// the panel and to the rest of the trailing matrix. Events order the
+// streams: the side stream's step j waits for the context stream's step
+// j - 1 (which updated the next panel's columns), and the context stream's
+// step j waits for the side stream's panel j. Splitting the triangular solve
+// and the update by columns leaves every element's operations unchanged.
 template <typename T>
 void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info) {
   if (m == 0 || n == 0) return;
@@ -60,22 +71,41 @@ void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info) {
     GetrfRec<T>(m, n, a, lda, ipiv, info, 0);
     return;
   }
+  Context& ctx = Ctx();
+  SideStream& side = Side();
+  const cudaStream_t main = ctx.stream;
+  const cudaStream_t look = side.ok ? side.stream : main;
+  // The trailing work of panel j on columns [c0, c0 + nc).
+  const auto update = [&](int j, int jb, int c0, int nc) {
+    Laswp<T>(nc, At(a, lda, 0, c0), lda, j + 1, j + jb, ipiv, 1);
+    TrsmFull<T>(true, true, false, true, jb, nc, T(1), At(a, lda, j, j), lda,
+                At(a, lda, j, c0), lda);
+    if (j + jb < m) {
+      GemmFull<T>(false, false, m - j - jb, nc, jb, T(-1), At(a, lda, j + jb, j), lda,
+                  At(a, lda, j, c0), lda, T(1), At(a, lda, j + jb, c0), lda);
+    }
+  };
+  StreamAfter(side.to_side, main, look);
+  OnSide([&] { GetrfRec<T>(m, std::min(nb, mn), a, lda, ipiv, info, 0); });
   for (int j = 0; j < mn; j += nb) {
     const int jb = std::min(mn - j, nb);
-    GetrfRec<T>(m - j, jb, At(a, lda, j, j), lda, ipiv + j, info, j);
-    AdjustPivots(ipiv, j, std::min(m, j + jb), j);
-    Laswp<T>(j, a, lda, j + 1, j + jb, ipiv, 1);
-    if (j + jb < n) {
-      Laswp<T>(n - j - jb, At(a, lda, 0, j + jb), lda, j + 1, j + jb, ipiv, 1);
-      TrsmFull<T>(true, true, false, true, jb, n - j - jb, T(1), At(a, lda, j, j),
-                  lda, At(a, lda, j, j + jb), lda);
-      if (j + jb < m) {
-        GemmFull<T>(false, false, m - j - jb, n - j - jb, jb, T(-1),
-                    At(a, lda, j + jb, j), lda, At(a, lda, j, j + jb), lda, T(1),
-                    At(a, lda, j + jb, j + jb), lda);
-      }
+    const int right = n - j - jb;               // columns right of the panel
+    const int next = std::min(nb, right);       // the next panel's columns
+    const int jb2 = std::min(mn - j - jb, nb);  // the next panel's width
+    StreamAfter(side.to_side, main, look);
+    OnSide([&] { AdjustPivots(ipiv, j, std::min(m, j + jb), j); });
+    StreamAfter(side.to_main, look, main);
+    if (next > 0) {
+      OnSide([&] {
+        update(j, jb, j + jb, next);
+        if (jb2 > 0) GetrfRec<T>(m - j - jb, jb2, At(a, lda, j + jb, j + jb), lda,
+                                 ipiv + j + jb, info, j + jb);
+      });
     }
+    Laswp<T>(j, a, lda, j + 1, j + jb, ipiv, 1);
+    if (right > next) update(j, jb, j + jb + next, right - next);
   }
+  StreamAfter(side.to_main, look, main);
 }
 
 template <typename T>
@@ -138,6 +168,16 @@ void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0) {
   ctx.guard = saved;
 }
 
+// Blocked Cholesky (potrf.cc:160-197) with a look-ahead of one block. Step j
+// updates and factors the diagonal block (SYRK, POTRF2), then updates and
+// solves the block beside it (GEMM, TRSM). The GEMM and TRSM act on each row
+// (lower; each column, upper) of that block independently, so they are split:
+// on the side stream, the part that the next diagonal block reads (its jb
+// rows) is done first and the next diagonal block is updated and factored;
+// the context's stream does the rest. The side stream's step j waits for
+// the context stream's step j - 1; the context stream's step j waits for
+// the side stream's diagonal block j. Every element's operations are the
+// reference's.
 template <typename T>
 void Potrf(bool upper, int n, T* a, int lda, int* info) {
   if (n == 0) return;
@@ -149,32 +189,69 @@ void Potrf(bool upper, int n, T* a, int lda, int* info) {
   Context& ctx = Ctx();
   const int* saved = ctx.guard;
   ctx.guard = info;
+  SideStream& side = Side();
+  const cudaStream_t main = ctx.stream;
+  const cudaStream_t look = side.ok ? side.stream : main;
+  // The split GEMMs' partial buffers at their largest, reserved before the
+  // first launch (growing one in the loop would synchronize the device).
+  size_t bytes_main = 0, bytes_side = 0;
+  for (int j = nb; j < n; j += nb) {
+    const int jb = std::min(nb, n - j), rest = n - j - jb, next = std::min(nb, rest);
+    const auto split = [&](int rows) {
+      return upper ? DgemmSplitBytes(jb, rows, j) : DgemmSplitBytes(rows, jb, j);
+    };
+    bytes_side = std::max(bytes_side, split(next));
+    if (rest > next) bytes_main = std::max(bytes_main, split(rest - next));
+  }
+  if (sizeof(T) == 8) {
+    if (bytes_main > 0) Workspace(kWsSplitK, bytes_main);
+    if (bytes_side > 0) OnSide([&] { Workspace(kWsSplitK, bytes_side); });
+  }
+  // Diagonal block j: its update by the finished columns, then POTRF2.
+  const auto diag = [&](int j, int jb) {
+    if (upper) {
+      SyrkFull<T>(false, true, jb, j, T(-1), At(a, lda, 0, j), lda, 1.0, At(a, lda, j, j),
+                  lda);
+      Potrf2Rec<T>(true, jb, At(a, lda, j, j), lda, info, j);
+    } else {
+      SyrkFull<T>(true, false, jb, j, T(-1), At(a, lda, j, 0), lda, 1.0, At(a, lda, j, j),
+                  lda);
+      Potrf2Rec<T>(false, jb, At(a, lda, j, j), lda, info, j);
+    }
+  };
+  // Block j's off-diagonal part, restricted to rows (lower; columns, upper)
+  // [r0, r0 + nr).
+  const auto beside = [&](int j, int jb, int r0, int nr) {
+    if (upper) {
+      if (j > 0)
+        GemmFull<T>(true, false, jb, nr, j, T(-1), At(a, lda, 0, j), lda, At(a, lda, 0, r0),
+                    lda, 1.0, At(a, lda, j, r0), lda);
+      TrsmFull<T>(true, false, true, false, jb, nr, 1.0, At(a, lda, j, j), lda,
+                  At(a, lda, j, r0), lda);
+    } else {
+      if (j > 0)
+        GemmFull<T>(false, true, nr, jb, j, -1.0, At(a, lda, r0, 0), lda, At(a, lda, j, 0),
+                    lda, 1.0, At(a, lda, r0, j), lda);
+      TrsmFull<T>(false, true, true, false, nr, jb, 1.0, At(a, lda, j, j), lda,
+                  At(a, lda, r0, j), lda);
+    }
+  };
+  StreamAfter(side.to_side, main, look);
+  OnSide([&] { diag(0, nb); });
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
-    if (upper) {
-      SyrkFull<T>(false, true, jb, j, T(-1), At(a, lda, 0, j), lda, 1.0,
-               At(a, lda, j, j), lda);
-      Potrf2Rec<T>(true, jb, At(a, lda, j, j), lda, info, j);
-      if (j + jb < n) {
-        GemmFull<T>(true, false, jb, n - j - jb, j, T(-1), At(a, lda, 0, j),
-                         lda, At(a, lda, 0, j + jb), lda, 1.0,
-                         At(a, lda, j, j + jb), lda);
-        TrsmFull<T>(true, false, true, false, jb, n - j - jb, 1.0,
-                         At(a, lda, j, j), lda, At(a, lda, j, j + jb), lda);
-      }
-    } else {
-      SyrkFull<T>(true, false, jb, j, T(-1), At(a, lda, j, 0), lda, 1.0,
-               At(a, lda, j, j), lda);
-      Potrf2Rec<T>(false, jb, At(a, lda, j, j), lda, info, j);
-      if (j + jb < n) {
-        GemmFull<T>(false, true, n - j - jb, jb, j, -1.0,
-                         At(a, lda, j + jb, 0), lda, At(a, lda, j, 0), lda, 1.0,
-                         At(a, lda, j + jb, j), lda);
-        TrsmFull<T>(false, true, true, false, n - j - jb, jb, 1.0,
-                         At(a, lda, j, j), lda, At(a, lda, j + jb, j), lda);
-      }
-    }
+    const int rest = n - j - jb;
+    if (rest <= 0) break;
+    const int next = std::min(nb, rest);
+    StreamAfter(side.to_side, main, look);
+    StreamAfter(side.to_main, look, main);
+    OnSide([&] {
+      beside(j, jb, j + jb, next);
+      diag(j + jb, next);
+    });
+    if (rest > next) beside(j, jb, j + jb + next, rest - next);
   }
+  StreamAfter(side.to_main, look, main);
   ctx.guard = saved;
 }
 

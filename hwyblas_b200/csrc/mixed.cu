@@ -23,8 +23,8 @@
 //             recursive LU, U12 by an FP64 triangular solve, and the
 //             trailing update A22 -= L21 U12 as an Ozaki GEMM with few INT8
 //             slices on tcgen05 (integer-exact products, FP64 recombination).
-//   Cholesky  diagonal block in FP64, L21 by an FP64 triangular solve,
-//             A22 -= L21 L21^T as an Ozaki GEMM.
+//   Cholesky  diagonal block factored and inverted in FP64, L21 = A21 L11^-T
+//             and A22 -= L21 L21^T (lower triangle) as Ozaki GEMMs.
 // The factors stay in FP64 storage; their accuracy is that of the slices
 // (about 8*S - 1 significant bits), which sets the refinement's contraction.
 //
@@ -1173,28 +1173,85 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
   signal(la.to_main, look, main);
 }
 
-// Right-looking lower Cholesky of w (full symmetric storage) with FP64
-// diagonal blocks and Ozaki trailing updates; then L^T is mirrored into the
-// upper triangle for the backward solve.
-void MixedPotrf(int n, double* w, long long ldw, int* info, int slices) {
+__global__ void SetIdentityKernel(int n, double* x, long long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i < n) x[i + j * ldx] = (i == j) ? 1.0 : 0.0;
+}
+
+// Right-looking lower Cholesky of w (full symmetric storage; the lower
+// triangle is read and factored, the upper one receives L^T at the end) with
+// a look-ahead of one block column, like the LU:
+//
+//   look (high priority): update the next block column with the current L21,
+//     factor its diagonal block in FP64 (the recursive POTRF2), invert that
+//     block in FP64 (the chained triangular solve of L11 X = I), then form
+//     the block column below it as L21 = A21 L11^-T, an Ozaki GEMM (in
+//     place: the slicing reads A21 before the product writes it);
+//   main: the rest of the trailing update, A22 -= L21 L21^T, an Ozaki GEMM
+//     that skips the tiles above the diagonal (only the lower triangle is
+//     wanted).
+//
+// The streams touch disjoint block columns; events order them as the data
+// flow requires (main's update waits for the L21 it reads; look's next
+// block column waits for main's previous update). FP64 runs only in the
+// diagonal blocks; every flop outside them is on the INT8 tensor cores.
+void MixedPotrf(int n, double* w, long long ldw, int* info, int slices, MixedBuffers& bf) {
+  Context& ctx = Ctx();
   const int nb = MixedBlock(n);
   const int lw = static_cast<int>(ldw);
+  const cudaStream_t main = ctx.stream;
+  Lookahead& la = GetLookahead();
+  const cudaStream_t look = la.ok ? la.stream : main;
+  auto signal = [&](cudaEvent_t ev, cudaStream_t from, cudaStream_t to) {
+    if (from == to) return;
+    cudaEventRecord(ev, from);
+    cudaStreamWaitEvent(to, ev, 0);
+  };
+  double* xinv = static_cast<double*>(
+      Workspace(kWsMixedInv, sizeof(double) * static_cast<size_t>(nb) * nb));
+  if (xinv == nullptr) return;
+  // Diagonal block at j (jb columns): FP64 factor and inverse, then the
+  // block column below it, rows [j + jb, n).
+  const auto panel = [&](int j, int jb) {
+    PotrfPanel(false, jb, At(w, ldw, j, j), lw, info, j);
+    const int below = n - j - jb;
+    if (below <= 0) return;
+    InvertDiagBlocks(jb, At(w, ldw, j, j), ldw, true, false, bf.inv_lo);
+    SetIdentityKernel<<<dim3((jb + 255) / 256, jb), 256, 0, ctx.stream>>>(jb, xinv, nb);
+    CountLaunch();
+    if (!ChainTrsv(true, jb, jb, At(w, ldw, j, j), ldw, bf.inv_lo, xinv, nb,
+                   bf.flags + bf.flag_stride))
+      TrsmFull<double>(true, true, false, false, jb, jb, 1.0, At(w, ldw, j, j), lw, xinv, nb);
+    DgemmEmulated(below, jb, jb, 1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
+                  ColMajor<double>(xinv, nb, true), 0.0, At(w, ldw, j + jb, j), lw, slices,
+                  false, 1);
+  };
+  signal(la.to_look, main, look);
+  OnStream(look, [&] { panel(0, std::min(nb, n)); });
   for (int j = 0; j < n; j += nb) {
     const int jb = std::min(nb, n - j);
-    PotrfPanel(false, jb, At(w, ldw, j, j), lw, info, j);
-    if (j + jb < n) {
-      const int rest = n - j - jb;
-      Context& ctx = Ctx();
-      const int* saved = ctx.guard;
-      ctx.guard = info;
-      TrsmFull<double>(false, true, true, false, rest, jb, 1.0, At(w, ldw, j, j), lw,
-                       At(w, ldw, j + jb, j), lw);
-      ctx.guard = saved;
-      DgemmEmulated(rest, rest, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
+    const int rest = n - j - jb;
+    if (rest <= 0) break;
+    const int next = std::min(nb, rest);
+    signal(la.to_main, look, main);  // L21 of block j
+    signal(la.to_look, main, look);  // main's previous update
+    OnStream(look, [&] {
+      // The next block column: rows [j + jb, n), columns [j + jb, + next).
+      DgemmEmulated(rest, next, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
                     ColMajor<double>(At(w, ldw, j + jb, j), ldw, true), 1.0,
-                    At(w, ldw, j + jb, j + jb), lw, slices, false);
+                    At(w, ldw, j + jb, j + jb), lw, slices, false, 1);
+      panel(j + jb, next);
+    });
+    if (rest > next) {
+      const int r2 = rest - next;
+      const double* l21 = At(w, ldw, j + jb + next, j);
+      DgemmEmulated(r2, r2, jb, -1.0, ColMajor<double>(l21, ldw),
+                    ColMajor<double>(l21, ldw, true), 1.0,
+                    At(w, ldw, j + jb + next, j + jb + next), lw, slices, false, 0, true);
     }
   }
+  signal(la.to_main, look, main);
   const dim3 grid((n + 31) / 32, (n + 31) / 32);
   // Upper triangle := transpose of the lower one (in place is safe: each
   // tile reads only the lower triangle and writes only the upper one).
@@ -1225,7 +1282,8 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
   // to the solution of A x = b itself rather than stalling at the FP64
   // residual's noise (cond(A) eps). For few right-hand sides it costs what
   // the FP64 GEMV costs (both read A once); for many, the FP64 DMMA residual
-  // runs until the FP64 tests pass and the extra-precise one then polishes.
+  // runs until every column meets the backward criterion and the
+  // extra-precise one then finishes.
   bool extra = nrhs < kResRhs;
   for (int it = 0; it < kItMax; ++it) {
     if (extra) {
@@ -1238,19 +1296,25 @@ int Refine(bool lu, int n, int nrhs, const double* a, long long lda, const doubl
     AxpyMatrixKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(n, nrhs, bf.d, bf.ldr,
                                                                   x, ldx);
     CountLaunch();
-    // A column is done once it has met both tests; later corrections only
-    // move it within the last bit.
-    bool done = true;
+    // A column is done once it meets the backward criterion and its
+    // correction has settled: it moved x by at most an ulp, it no longer
+    // halves (the corrections have reached the residual's noise), or, at the
+    // observed rate of contraction dn / dprev, the next one would move x by
+    // less than half an ulp. Later corrections only move it within the last
+    // bit.
+    bool done = true, backward_all = true;
     for (int q = 0; q < nrhs; ++q) {
       const double xn = nm[0][q], rn = nm[1][q], dn = nm[2][q];
       const bool backward = rn <= xn * cte;  // false on NaN
-      const bool settled = dn <= 0x1p-52 * xn || dn > 0.5 * dprev[q];
+      const bool settled = dn <= 0x1p-52 * xn || dn > 0.5 * dprev[q] ||
+                           (std::isfinite(dprev[q]) && (dn / dprev[q]) * dn <= 0x1p-53 * xn);
       if (backward && settled) settled_col[q] = 1;
       if (!settled_col[q]) done = false;
+      if (!backward) backward_all = false;
       dprev[q] = dn;
     }
-    if (done && extra) return it + 1;
-    if (done) {
+    if (extra && done) return it + 1;
+    if (!extra && backward_all) {
       extra = true;
       std::fill(settled_col.begin(), settled_col.end(), 0);
       std::fill(dprev.begin(), dprev.end(), INFINITY);
@@ -1328,7 +1392,7 @@ int DposvMixed(bool upper, int n, int nrhs, double* a, int lda, const double* b,
   } else {
     cudaMemsetAsync(dinfo, 0, sizeof(int), st);
     Copy2D(n, n, bf.afull, bf.ldw, bf.w, bf.ldw);
-    MixedPotrf(n, bf.w, bf.ldw, dinfo, slices);
+    MixedPotrf(n, bf.w, bf.ldw, dinfo, slices, bf);
     int finfo = 0;
     cudaMemcpyAsync(&finfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (Failed(cudaStreamSynchronize(st), "mixed potrf")) return -1;

@@ -240,8 +240,9 @@ def test_dresidual_dd_matches_exact(hb, n, nrhs):
 
 
 def solve_to_last_bit(hb, orc, a, lu, ipiv, b, x0):
-    """The solution of A x = b to about the last bit: x0 refined twice with
-    the extra-precise residual and the oracle's FP64 LU factors."""
+    """The solution of A x = b to about the last bit: x0 (the oracle's own
+    solution, independent of the solver under test) refined twice with the
+    extra-precise residual and the oracle's FP64 LU factors."""
     n, nrhs = b.shape
     x = x0.copy(order="F")
     r = np.zeros((n, nrhs), order="F")
@@ -277,7 +278,7 @@ def test_dgesv_mixed_config4_n8192(hb, orc):
         info, it = hb.dgesv_mixed(n, nrhs, a_in, n, np.zeros(n, np.int32), b, n, xm, n)
         assert info == 0 and it > 0, (info, it)
         assert same_bits(a_in, a)
-        xs = solve_to_last_bit(hb, orc, a, lu, ipiv, b, xm)
+        xs = solve_to_last_bit(hb, orc, a, lu, ipiv, b, xp)
         e_mixed, e_plain = fwd_err(xm, xs), fwd_err(xp, xs)
         assert e_mixed <= e_plain, (nrhs, e_mixed, e_plain)
         r = np.zeros((n, nrhs), order="F")
