@@ -128,6 +128,7 @@ PROTOTYPES = {
     "hwyblas_set_leaf_wait_limit": (ctypes.c_uint, [ctypes.c_uint]),
     "hwyblas_int8_peak_tops": (D, []),
     "hwyblas_dresidual_dd": (None, [PI, PI, P, PI, P, PI, P, PI, P, PI]),
+    "hwyblas_batched_set_config": (I, [I]),
     "hwyblas_launch_count": (ctypes.c_uint64, []),
     "hwyblas_kernel_timer": (None, [I]),
     "hwyblas_kernel_timer_read": (D, [PI]),

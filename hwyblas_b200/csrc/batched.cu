@@ -14,6 +14,7 @@
 // conventions of its single-problem routines with arrays of sizes, leading
 // dimensions and device pointers.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -83,6 +84,131 @@ __device__ void CtaGemm(int m, int n, int k, T alpha, Mat<T> a, Mat<T> b, T beta
       }
     }
     if (k > 0) c(i, j) = cv;
+  }
+  __syncthreads();
+}
+
+// The same product on the FP64 tensor pipe: the CTA's WM x WN warps walk C in
+// tiles of (16 WM) x (8 NB WN); each warp computes a 16 x 8 NB block with NB
+// mma.sync.m16n8k8.f64 per k8 step. The MMA accumulates its 8 products in
+// ascending k as a chain of correctly rounded FMAs starting from the
+// accumulator, so chaining the MMAs over k and restarting every KC = 256
+// gives every element the reference's chain; zero padding past k adds +0.
+// Each 256-deep chunk is merged into C exactly as CtaGemm merges it. Operand k-blocks of 32 are staged in shared memory with
+// rows padded to a stride of 8 (mod 32) words, which makes every fragment
+// load conflict free; the next block is fetched into registers while the
+// current one is multiplied.
+constexpr int kDmmaKb = 32;
+
+__device__ __forceinline__ void BatchDmma(double (&d)[4], double a0, double a1, double a2,
+                                          double a3, double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+template <int WM, int WN, int NB>
+struct DmmaTile {
+  static constexpr int kTM = 16 * WM, kTN = 8 * NB * WN;
+  static constexpr int kThreads = 32 * WM * WN;
+  static constexpr int kSA = kTM + 4, kSB = kTN + 4;  // row strides (doubles)
+  static constexpr int kLoadA = kDmmaKb * kTM / kThreads;  // elements per thread
+  static constexpr int kLoadB = kDmmaKb * kTN / kThreads;
+};
+
+template <int WM, int WN, int NB>
+__device__ void CtaGemmDmma(int m, int n, int k, double alpha, Mat<double> a, Mat<double> b,
+                            double beta, Mat<double> c, double* sA, double* sB) {
+  using Cfg = DmmaTile<WM, WN, NB>;
+  constexpr int TM = Cfg::kTM, TN = Cfg::kTN, SA = Cfg::kSA, SB = Cfg::kSB;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int wm = warp % WM, wn = warp / WM;
+  const int g = lane >> 2, t = lane & 3;
+  // Operand loads: along the contiguous index of each operand.
+  const bool a_rows = a.rs == 1;  // A(i, q) contiguous in i
+  const bool b_rows = b.rs == 1;  // B(q, j) contiguous in q
+  for (int m0 = 0; m0 < m; m0 += TM) {
+    for (int n0 = 0; n0 < n; n0 += TN) {
+      double acc[NB][4];
+      double ra[Cfg::kLoadA], rb[Cfg::kLoadB];
+      const auto fetch = [&](int kb0) {
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadA; ++l) {
+          const int idx = threadIdx.x + l * Cfg::kThreads;
+          const int i = a_rows ? idx % TM : idx / kDmmaKb;
+          const int q = a_rows ? idx / TM : idx % kDmmaKb;
+          ra[l] = (m0 + i < m && kb0 + q < k) ? a(m0 + i, kb0 + q) : 0.0;
+        }
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadB; ++l) {
+          const int idx = threadIdx.x + l * Cfg::kThreads;
+          const int q = b_rows ? idx % kDmmaKb : idx / TN;
+          const int j = b_rows ? idx / kDmmaKb : idx % TN;
+          rb[l] = (n0 + j < n && kb0 + q < k) ? b(kb0 + q, n0 + j) : 0.0;
+        }
+      };
+      const auto stash = [&]() {
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadA; ++l) {
+          const int idx = threadIdx.x + l * Cfg::kThreads;
+          const int i = a_rows ? idx % TM : idx / kDmmaKb;
+          const int q = a_rows ? idx / TM : idx % kDmmaKb;
+          sA[q * SA + i] = ra[l];
+        }
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadB; ++l) {
+          const int idx = threadIdx.x + l * Cfg::kThreads;
+          const int q = b_rows ? idx % kDmmaKb : idx / TN;
+          const int j = b_rows ? idx / kDmmaKb : idx % TN;
+          sB[q * SB + j] = rb[l];
+        }
+      };
+      fetch(0);
+      for (int pc = 0; pc < k; pc += 256) {
+        const int pe = min(k, pc + 256);
+#pragma unroll
+        for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc[nb][e] = 0.0;
+        for (int kb0 = pc; kb0 < pe; kb0 += kDmmaKb) {
+          __syncthreads();  // the previous block's fragments are read
+          stash();
+          __syncthreads();
+          if (kb0 + kDmmaKb < k) fetch(kb0 + kDmmaKb);
+          const int steps = (min(pe, kb0 + kDmmaKb) - kb0 + 7) / 8;
+          for (int ks = 0; ks < steps; ++ks) {
+            const double* pa = sA + (ks * 8 + t) * SA + wm * 16 + g;
+            const double a0 = pa[0], a1 = pa[8], a2 = pa[4 * SA], a3 = pa[4 * SA + 8];
+#pragma unroll
+            for (int nb = 0; nb < NB; ++nb) {
+              const double* pb = sB + (ks * 8 + t) * SB + wn * 8 * NB + nb * 8 + g;
+              BatchDmma(acc[nb], a0, a1, a2, a3, pb[0], pb[4 * SB]);
+            }
+          }
+        }
+        // Merge the chunk into C (CtaGemm's rules; each element is read and
+        // written by its own thread only).
+#pragma unroll
+        for (int nb = 0; nb < NB; ++nb) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int i = m0 + wm * 16 + g + (e >> 1) * 8;
+            const int j = n0 + wn * 8 * NB + nb * 8 + 2 * t + (e & 1);
+            if (i >= m || j >= n) continue;
+            const double r = alpha * acc[nb][e];
+            if (pc != 0 || beta == 1.0) {
+              c(i, j) = r + c(i, j);
+            } else if (beta == 0.0) {
+              c(i, j) = r;
+            } else {
+              c(i, j) = fma(c(i, j), beta, r);
+            }
+          }
+        }
+      }
+    }
   }
   __syncthreads();
 }
@@ -588,6 +714,41 @@ __global__ void __launch_bounds__(256) BatchedGemmKernel(BatchArgs<T> p) {
   }
 }
 
+// FP64 batched GEMM on the tensor pipe (CtaGemmDmma) for problems with m and n
+// of at least 16; smaller ones take the per-element chains of CtaGemm.
+template <int WM, int WN, int NB>
+__global__ void __launch_bounds__(DmmaTile<WM, WN, NB>::kThreads,
+                                  512 / DmmaTile<WM, WN, NB>::kThreads)
+    BatchedGemmDmmaKernel(BatchArgs<double> p) {
+  using Cfg = DmmaTile<WM, WN, NB>;
+  __shared__ double sA[kDmmaKb * Cfg::kSA];
+  __shared__ double sB[kDmmaKb * Cfg::kSB];
+  __shared__ int slot;
+  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+    const long long la = p.lda[id], lb = p.ldb[id];
+    const Mat<double> a = (p.flags & 1) ? Mat<double>{p.a[id], la, 1} : Col(p.a[id], la);
+    const Mat<double> b = (p.flags & 2) ? Mat<double>{p.b[id], lb, 1} : Col(p.b[id], lb);
+    const int m = p.m[id], n = p.n[id], k = p.k[id];
+    if (m == 0 || n == 0) continue;
+    const Mat<double> c = Col(p.c[id], p.ldc[id]);
+    if (k == 0 || p.alpha == 0.0) {
+      if (p.beta != 1.0) {
+        for (int idx = threadIdx.x; idx < m * n; idx += blockDim.x) {
+          const int i = idx % m, j = idx / m;
+          c(i, j) = (p.beta == 0.0) ? 0.0 : c(i, j) * p.beta;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    if (m < 16 || n < 16) {
+      CtaGemm<double>(m, n, k, p.alpha, a, b, p.beta, c);
+    } else {
+      CtaGemmDmma<WM, WN, NB>(m, n, k, p.alpha, a, b, p.beta, c, sA, sB);
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -682,12 +843,33 @@ struct Layout {
 
 enum BatchKind { kBatchGetrf = 0, kBatchGetrs = 1, kBatchGemm = 2, kBatchTrsm = 3 };
 
+// A launch configuration of the autotuner: the threads per CTA of the
+// per-element kernels (64, 128, 256), or a tile shape of the FP64 tensor-pipe
+// GEMM (kDmma32: 32 x 32 tiles, 4 warps; kDmma64: 64 x 64 tiles, 8 warps).
+constexpr int kDmma32 = 1001, kDmma64 = 1002;
+
+int ThreadsOf(int config) {
+  return config == kDmma32 ? DmmaTile<2, 2, 2>::kThreads
+         : config == kDmma64 ? DmmaTile<4, 2, 4>::kThreads : config;
+}
+
 template <typename T>
-void* KernelOf(int kind) {
+void* KernelOf(int kind, int config) {
   if (kind == kBatchGetrf) return reinterpret_cast<void*>(BatchedGetrfKernel<T>);
   if (kind == kBatchGetrs) return reinterpret_cast<void*>(BatchedGetrsKernel<T>);
   if (kind == kBatchTrsm) return reinterpret_cast<void*>(BatchedTrsmKernel<T>);
+  if (sizeof(T) == 8 && config == kDmma32)
+    return reinterpret_cast<void*>(BatchedGemmDmmaKernel<2, 2, 2>);
+  if (sizeof(T) == 8 && config == kDmma64)
+    return reinterpret_cast<void*>(BatchedGemmDmmaKernel<4, 2, 4>);
   return reinterpret_cast<void*>(BatchedGemmKernel<T>);
+}
+
+// The configurations the autotuner times for a routine and type.
+template <typename T>
+std::vector<int> Candidates(int kind) {
+  if (sizeof(T) == 8 && kind == kBatchGemm) return {64, 128, 256, kDmma32, kDmma64};
+  return {64, 128, 256};
 }
 
 // Threads per CTA for a batch: the autotuner's choice for the batch's size
@@ -708,7 +890,7 @@ namespace {
 
 // Graphs of recent batch shapes (per host thread).
 struct GraphKey {
-  int kind, bytes, count, threads, grid;
+  int kind, bytes, count, config, grid;
   void* dev;
   void* host;
   size_t total;
@@ -716,7 +898,7 @@ struct GraphKey {
   int flags, lanes;
   cudaStream_t stream;
   bool operator==(const GraphKey& o) const {
-    return kind == o.kind && bytes == o.bytes && count == o.count && threads == o.threads &&
+    return kind == o.kind && bytes == o.bytes && count == o.count && config == o.config &&
            grid == o.grid && dev == o.dev && host == o.host && total == o.total &&
            alpha == o.alpha && beta == o.beta && flags == o.flags && lanes == o.lanes &&
            stream == o.stream;
@@ -753,9 +935,10 @@ double WorkOf(int kind, const HostBatch<T>& bt, int i) {
 // kernel with `threads` threads a CTA. Problem info lands in dev_info (if
 // non-null) on return of the stream.
 template <typename T>
-bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info,
+bool LaunchBatch(int kind, const HostBatch<T>& bt, int config, int** dev_info,
                  bool use_graph) {
   Context& ctx = Ctx();
+  const int threads = ThreadsOf(config);
   const int count = bt.count;
   const Layout L(count);
   uint8_t* host = static_cast<uint8_t*>(t_stage.Get(L.total));
@@ -805,7 +988,7 @@ bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info,
   args.beta = bt.beta;
   args.flags = bt.flags;
   args.lanes = sizeof(T) == 8 ? RefLanesDouble() : 2 * RefLanesDouble();
-  void* fn = KernelOf<T>(kind);
+  void* fn = KernelOf<T>(kind, config);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0);
   const int grid = std::max(1, std::min(count, ctx.num_sms * std::max(per_sm, 1)));
@@ -815,7 +998,7 @@ bool LaunchBatch(int kind, const HostBatch<T>& bt, int threads, int** dev_info,
   // same batch shape comes again (same workspace, staging buffer and kernel
   // arguments); the legacy default stream cannot be captured.
   if (use_graph && ctx.stream != nullptr) {
-    GraphKey key{kind, static_cast<int>(sizeof(T)), count, threads, grid, dev, host,
+    GraphKey key{kind, static_cast<int>(sizeof(T)), count, config, grid, dev, host,
                  L.total, static_cast<double>(args.alpha), static_cast<double>(args.beta),
                  args.flags, args.lanes, ctx.stream};
     for (auto& e : t_graphs) {
@@ -872,12 +1055,22 @@ __global__ void FillRandomKernel(double* x, long long count, unsigned seed, doub
   }
 }
 
-// The autotuner: threads per CTA in {64, 128, 256} for (routine, type, size
-// bucket), timed on 96 synthetic problems of the bucket's representative
-// size (results do not depend on the choice: every problem's arithmetic is
-// the same whichever threads run it).
+// The autotuner: for (routine, type, size bucket), the launch configuration
+// (threads per CTA in {64, 128, 256}; for the FP64 GEMM also the tensor-pipe
+// kernel with 32 x 32 or 64 x 64 tiles) that runs 96 synthetic problems of
+// the bucket's representative size fastest (results do not depend on the
+// choice: every problem's arithmetic is the same whichever configuration
+// runs it).
+// A configuration set by hwyblas_batched_set_config (0: the autotuner's).
+std::atomic<int> g_forced_config{0};
+
 template <typename T>
-int TunedThreads(int kind, int median_m, int median_n) {
+int TunedConfig(int kind, int median_m, int median_n) {
+  const int forced = g_forced_config.load(std::memory_order_relaxed);
+  if (forced != 0) {
+    for (int c : Candidates<T>(kind))
+      if (c == forced) return c;
+  }
   static std::mutex mu;
   static std::map<TuneKey, int> cache;
   int bucket = 0;
@@ -935,17 +1128,17 @@ int TunedThreads(int kind, int median_m, int median_n) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int threads : {64, 128, 256}) {
-      LaunchBatch(kind, bt, threads, nullptr, false);  // warm-up
+    for (int config : Candidates<T>(kind)) {
+      LaunchBatch(kind, bt, config, nullptr, false);  // warm-up
       cudaEventRecord(e0, ctx.stream);
-      LaunchBatch(kind, bt, threads, nullptr, false);
+      LaunchBatch(kind, bt, config, nullptr, false);
       cudaEventRecord(e1, ctx.stream);
       cudaEventSynchronize(e1);
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best_ms) {
         best_ms = ms;
-        best = threads;
+        best = config;
       }
     }
     cudaEventDestroy(e0);
@@ -979,9 +1172,9 @@ namespace {
 template <typename T>
 void RunBatch(int kind, const HostBatch<T>& bt, int* info_out, const char* name) {
   if (bt.count == 0) return;
-  const int threads = TunedThreads<T>(kind, Median(bt.m), bt.n.empty() ? 0 : Median(bt.n));
+  const int config = TunedConfig<T>(kind, Median(bt.m), bt.n.empty() ? 0 : Median(bt.n));
   int* dev_info = nullptr;
-  if (!LaunchBatch(kind, bt, threads, &dev_info, true)) return;
+  if (!LaunchBatch(kind, bt, config, &dev_info, true)) return;
   LaunchFailed(name);
   if (info_out != nullptr) {
     Failed(cudaMemcpyAsync(info_out, dev_info, sizeof(int) * bt.count,
@@ -1158,6 +1351,10 @@ void GemmBatched(char transa, char transb, const int* m, const int* n, const int
 }  // namespace hb
 
 extern "C" {
+
+HWYBLAS_API int hwyblas_batched_set_config(int config) {
+  return hb::g_forced_config.exchange(config);
+}
 
 HWYBLAS_API void hwyblas_dgetrf_batched(const hwyblas_int* n, double* const* a,
                                         const hwyblas_int* lda, hwyblas_int* const* ipiv,

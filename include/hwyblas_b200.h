@@ -733,6 +733,15 @@ HWYBLAS_API void hwyblas_dposv_mixed(const char* uplo, const hwyblas_int* n,
  * reference's hwyblas_set_ilaenv (lapack.h:74-80), a tuning knob. */
 HWYBLAS_API int hwyblas_set_mixed_slices(int slices);
 
+/* Test hook of the batched routines: forces the launch configuration that
+ * the autotuner would otherwise choose per routine, type and size bucket
+ * (64, 128 or 256 threads per CTA; for hwyblas_dgemm_batched also 1001, the
+ * FP64 tensor-pipe kernel with 32 x 32 tiles, or 1002, with 64 x 64 tiles).
+ * A configuration that the routine does not have is ignored; 0 restores the
+ * autotuner. Results do not depend on the configuration. Returns the
+ * previous setting. No counterpart in the reference. */
+HWYBLAS_API int hwyblas_batched_set_config(int config);
+
 /* Batched LU, LU solve and GEMM over `count` independent problems of
  * uneven sizes (no counterpart in the reference, which solves one problem a
  * call). Arrays of sizes, leading dimensions and INFO are host memory; the

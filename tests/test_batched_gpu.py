@@ -135,6 +135,48 @@ def test_gemm_batched_matches_single(hb, cuda, ta, tb, alpha, beta):
             assert same_bits(got, want), (prec, i, dims[i], first_diff(got, want))
 
 
+@pytest.mark.parametrize("config", [64, 256, 1001, 1002])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.5])
+def test_dgemm_batched_every_config_matches_single(hb, cuda, config, ta, tb, beta):
+    """Each launch configuration the autotuner chooses from (the per-element
+    kernel at two thread counts, the FP64 tensor-pipe kernel with 32 x 32 and
+    64 x 64 tiles) gives every problem the single dgemm's bits: ragged sizes
+    below and across the tiles, k across several 256-deep chunks."""
+    torch = cuda
+    rng = np.random.default_rng(config + ord(ta) + ord(tb) + int(10 * beta))
+    dims = [(16, 16, 8), (17, 31, 5), (15, 40, 9), (64, 64, 256), (65, 63, 257), (96, 130, 600),
+            (200, 17, 513), (33, 200, 31), (512, 96, 40)]
+    m = [d[0] for d in dims]
+    n = [d[1] for d in dims]
+    k = [d[2] for d in dims]
+    lda = [(kk if ta != "N" else mm) + 1 for mm, kk in zip(m, k)]
+    ldb = [(nn if tb != "N" else kk) + 3 for nn, kk in zip(n, k)]
+    ldc = [mm + 2 for mm in m]
+    ea = [la * (mm if ta != "N" else kk) for la, mm, kk in zip(lda, m, k)]
+    eb = [lb * (kk if tb != "N" else nn) for lb, nn, kk in zip(ldb, n, k)]
+    ec = [lc * nn for lc, nn in zip(ldc, n)]
+    _, A = carve(torch, ea, torch.float64)
+    _, B = carve(torch, eb, torch.float64)
+    _, C = carve(torch, ec, torch.float64)
+    for v in A + B + C:
+        v.copy_(torch.from_numpy(rng.uniform(-1, 1, v.numel())))
+    C0 = [v.clone() for v in C]
+    torch.cuda.synchronize()
+    lib = hb.lib()
+    prev = lib.hwyblas_batched_set_config(config)
+    try:
+        hb.gemm_batched(ta, tb, m, n, k, 1.5, A, lda, B, ldb, beta, C, ldc)
+    finally:
+        lib.hwyblas_batched_set_config(prev)
+    for i in range(len(dims)):
+        c1 = C0[i].clone()
+        torch.cuda.synchronize()
+        hb.dgemm(ta, tb, m[i], n[i], k[i], 1.5, A[i], lda[i], B[i], ldb[i], beta, c1, ldc[i])
+        got, want = C[i].cpu().numpy(), c1.cpu().numpy()
+        assert same_bits(got, want), (config, i, dims[i], first_diff(got, want))
+
+
 def test_batched_invalid_arguments(hb, cuda):
     torch = cuda
     a = torch.zeros(16, dtype=torch.float64, device="cuda")
