@@ -803,7 +803,7 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
                                               slot_bytes);
   args.timeout_flag = ctx.dev_status;
   cudaEvent_t t0 = KernelTimerStart(kFamilyLuLeaf, ctx.stream);
-  if (wide || (P > 1 && P <= max_cluster)) {
+  if (wide || (P > 1 && P <= max_cluster && !ctx.side_leaf)) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P);
     cfg.blockDim = dim3(kLeafThreads);

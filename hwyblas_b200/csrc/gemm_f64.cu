@@ -866,8 +866,8 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
     if (partial != nullptr) {
       p.partial = partial;
       p.nchunks = nchunks;
-      const unsigned grid =
-          static_cast<unsigned>(std::min<long long>(tiles * nchunks, ctx.num_sms));
+      const int sms = ctx.sm_cap > 0 ? std::min(ctx.sm_cap, ctx.num_sms) : ctx.num_sms;
+      const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles * nchunks, sms));
       cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
       if (tri_kind == 0) {
         DgemmDmmaKernel<0, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
@@ -889,8 +889,8 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   // take 128 of each thread's registers). Measured against a variant whose
   // producer is lane 0 of warp 0 (8 warps): dgemm n = 8192 32.9 vs 27.5
   // TFLOP/s, getrf n = 16384 418 vs 440 ms.
-  const unsigned grid =
-      static_cast<unsigned>(std::min<long long>(tiles, ctx.num_sms));
+  const int sms = ctx.sm_cap > 0 ? std::min(ctx.sm_cap, ctx.num_sms) : ctx.num_sms;
+  const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles, sms));
   cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
   if (tri_kind == 0) {
     DgemmDmmaKernel<0, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);

@@ -61,6 +61,13 @@ struct Context {
   // on the side stream (see OnSide), so that the two streams never share a
   // scratch buffer.
   int ws_bank = 0;
+  // If nonzero, the persistent FP64 GEMM launches at most this many CTAs,
+  // leaving the other SMs to the side stream's work (look-ahead).
+  int sm_cap = 0;
+  // Set while the side stream factors panels beside a capped GEMM: the LU
+  // leaf then takes its cooperative variant, whose CTAs can run on any free
+  // SMs (a 16-CTA cluster needs 16 free SMs of one GPC).
+  bool side_leaf = false;
 };
 
 // The calling thread's second stream (highest priority) with two events, for

@@ -17,6 +17,10 @@
 namespace hb {
 
 namespace {
+// SMs left to the side stream while the context stream's persistent GEMMs
+// run (look-ahead): enough for a 16-CTA panel leaf and its small kernels.
+constexpr int kSideSms = 20;
+
 template <typename T>
 T* At(T* a, int lda, int i, int j) {
   return a + i + static_cast<long long>(j) * lda;
@@ -75,6 +79,9 @@ void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info) {
   SideStream& side = Side();
   const cudaStream_t main = ctx.stream;
   const cudaStream_t look = side.ok ? side.stream : main;
+  // The context stream's persistent GEMMs leave kSideSms SMs free, so that
+  // the side stream's panel runs beside them rather than after them.
+  const int cap = side.ok ? std::max(1, ctx.num_sms - kSideSms) : 0;
   // The trailing work of panel j on columns [c0, c0 + nc).
   const auto update = [&](int j, int jb, int c0, int nc) {
     Laswp<T>(nc, At(a, lda, 0, c0), lda, j + 1, j + jb, ipiv, 1);
@@ -97,13 +104,19 @@ void Getrf(int m, int n, T* a, int lda, int* ipiv, int* info) {
     StreamAfter(side.to_main, look, main);
     if (next > 0) {
       OnSide([&] {
+        ctx.side_leaf = side.ok;
         update(j, jb, j + jb, next);
         if (jb2 > 0) GetrfRec<T>(m - j - jb, jb2, At(a, lda, j + jb, j + jb), lda,
                                  ipiv + j + jb, info, j + jb);
+        ctx.side_leaf = false;
       });
     }
     Laswp<T>(j, a, lda, j + 1, j + jb, ipiv, 1);
-    if (right > next) update(j, jb, j + jb + next, right - next);
+    if (right > next) {
+      ctx.sm_cap = cap;
+      update(j, jb, j + jb + next, right - next);
+      ctx.sm_cap = 0;
+    }
   }
   StreamAfter(side.to_main, look, main);
 }
@@ -192,6 +205,7 @@ void Potrf(bool upper, int n, T* a, int lda, int* info) {
   SideStream& side = Side();
   const cudaStream_t main = ctx.stream;
   const cudaStream_t look = side.ok ? side.stream : main;
+  const int cap = side.ok ? std::max(1, ctx.num_sms - kSideSms) : 0;
   // The split GEMMs' partial buffers at their largest, reserved before the
   // first launch (growing one in the loop would synchronize the device).
   size_t bytes_main = 0, bytes_side = 0;
@@ -249,7 +263,11 @@ void Potrf(bool upper, int n, T* a, int lda, int* info) {
       beside(j, jb, j + jb, next);
       diag(j + jb, next);
     });
-    if (rest > next) beside(j, jb, j + jb + next, rest - next);
+    if (rest > next) {
+      ctx.sm_cap = cap;
+      beside(j, jb, j + jb + next, rest - next);
+      ctx.sm_cap = 0;
+    }
   }
   StreamAfter(side.to_main, look, main);
   ctx.guard = saved;
