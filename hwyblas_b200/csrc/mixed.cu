@@ -1060,6 +1060,12 @@ int MixedBlock(int n) { return n >= 8192 ? 1024 : (n >= 4096 ? 512 : 256); }
 
 // A high-priority stream of the calling thread for the look-ahead panel
 // work, and two events to order it against the context's stream.
+__global__ void SetIdentityKernel(int n, double* x, long long ldx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i < n) x[i + j * ldx] = (i == j) ? 1.0 : 0.0;
+}
+
 struct Lookahead {
   cudaStream_t stream = nullptr;
   cudaEvent_t to_look = nullptr, to_main = nullptr;
@@ -1114,22 +1120,31 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
   // of two buffers by panel parity (look writes panel j+1's while main may
   // still read panel j's).
   const auto l11_inv = [&](int j) { return ((j / nb) & 1) ? bf.inv_up : bf.inv_lo; };
+  // The inverse of panel j's unit lower diagonal block L11 (nb x nb, in one
+  // of two buffers by panel parity), formed in FP64 by the chained solve of
+  // L11 X = I with the inverted 64 x 64 diagonal blocks.
+  double* xinv = static_cast<double*>(
+      Workspace(kWsMixedInv, sizeof(double) * 2 * static_cast<size_t>(nb) * nb));
+  if (xinv == nullptr) return;
+  const auto l11_full_inv = [&](int j) { return xinv + ((j / nb) & 1) * static_cast<size_t>(nb) * nb; };
   const auto invert = [&](int j, int jb) {
-    if (j + jb < n) InvertDiagBlocks(jb, At(w, ldw, j, j), ldw, true, true, l11_inv(j));
+    if (j + jb >= n) return;
+    InvertDiagBlocks(jb, At(w, ldw, j, j), ldw, true, true, l11_inv(j));
+    double* x = l11_full_inv(j);
+    SetIdentityKernel<<<dim3((jb + 255) / 256, jb), 256, 0, Ctx().stream>>>(jb, x, nb);
+    CountLaunch();
+    if (!ChainTrsv(true, jb, jb, At(w, ldw, j, j), ldw, l11_inv(j), x, nb,
+                   bf.flags + bf.flag_stride))
+      TrsmFull<double>(true, true, false, true, jb, jb, 1.0, At(w, ldw, j, j), lw, x, nb);
   };
   const auto update = [&](int j, int jb, int c0, int nc, int ws_set) {
-    // Columns [c0, c0 + nc) of the trailing matrix: U12 by an FP64
-    // triangular solve, then A22 -= L21 U12 on the INT8 tensor cores. The
-    // next panel's columns (look, ws_set 1) take the chained solve, whose
-    // 64 chains of 16 columns run in one launch with a short critical path;
-    // the wide rest (main) takes the recursive solve, whose large DMMA
-    // GEMMs do the bulk of the flops at a higher rate.
+    // Columns [c0, c0 + nc) of the trailing matrix, both products on the
+    // INT8 tensor cores: U12 = L11^{-1} A12 (in place: the slicing reads A12
+    // before the product writes it), then A22 -= L21 U12.
     const int rest = n - j - jb;
-    if (ws_set == 0 ||
-        !ChainTrsv(true, jb, nc, At(w, ldw, j, j), ldw, l11_inv(j), At(w, ldw, j, c0), ldw,
-                   bf.flags + ws_set * bf.flag_stride))
-      TrsmFull<double>(true, true, false, true, jb, nc, 1.0, At(w, ldw, j, j), lw,
-                       At(w, ldw, j, c0), lw);
+    DgemmEmulated(jb, nc, jb, 1.0, ColMajor<double>(l11_full_inv(j), nb),
+                  ColMajor<double>(At(w, ldw, j, c0), ldw), 0.0, At(w, ldw, j, c0), lw,
+                  slices, false, ws_set);
     DgemmEmulated(rest, nc, jb, -1.0, ColMajor<double>(At(w, ldw, j + jb, j), ldw),
                   ColMajor<double>(At(w, ldw, j, c0), ldw), 1.0, At(w, ldw, j + jb, c0), lw,
                   slices, false, ws_set);
@@ -1171,12 +1186,6 @@ void MixedGetrf(int n, double* w, long long ldw, int* ipiv, int* info, int slice
     });
   }
   signal(la.to_main, look, main);
-}
-
-__global__ void SetIdentityKernel(int n, double* x, long long ldx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (i < n) x[i + j * ldx] = (i == j) ? 1.0 : 0.0;
 }
 
 // Right-looking lower Cholesky of w (full symmetric storage; the lower

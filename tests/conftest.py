@@ -29,6 +29,17 @@ def ref_drivers():
 
 
 @pytest.fixture(scope="session")
+def refblas():
+    """The reference library itself, compiled against the Highway-API shim
+    (oracle/_ref/libhwyblas_ref.so), if built."""
+    from tests import oracle_lib
+    lib = oracle_lib.load_refblas()
+    if lib is None:
+        pytest.skip("oracle/_ref/libhwyblas_ref.so not built (needs the reference sources)")
+    return lib
+
+
+@pytest.fixture(scope="session")
 def hb():
     import hwyblas_b200
     hwyblas_b200.lib()

@@ -442,3 +442,79 @@ def first_diff(x, y):
         return None
     i = idx[0]
     return f"{idx.size} differ; first at flat {i}: {x[i]!r} vs {y[i]!r}"
+
+
+# ---------------------------------------------------------------------------
+# The reference library itself (oracle/_ref/libhwyblas_ref.so): every source
+# of the reference compiled unmodified against the Highway-API shim. Built
+# only where the reference's sources were present.
+
+REFBLAS_LIB = os.path.join(ORACLE_DIR, "_ref", "libhwyblas_ref.so")
+
+
+class RefBlas:
+    """The reference's own Fortran-convention entry points (all arguments by
+    pointer), with the Oracle class's calling style for the tests."""
+
+    def __init__(self):
+        self.lib = ctypes.CDLL(REFBLAS_LIB)
+
+    @staticmethod
+    def _i(v):
+        return ctypes.byref(ctypes.c_int(int(v)))
+
+    @staticmethod
+    def _d(v, single=False):
+        return ctypes.byref(ctypes.c_float(v) if single else ctypes.c_double(v))
+
+    def _info_call(self, fn, *args):
+        info = ctypes.c_int(0)
+        fn(*args, ctypes.byref(info))
+        return info.value
+
+    def dgemm(self, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, single=False):
+        fn = self.lib.sgemm_ if single else self.lib.dgemm_
+        i, d = self._i, self._d
+        fn(_b(ta), _b(tb), i(m), i(n), i(k), d(alpha, single), ptr(a), i(lda), ptr(b), i(ldb),
+           d(beta, single), ptr(c), i(ldc))
+
+    def dtrsm(self, side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+        i, d = self._i, self._d
+        self.lib.dtrsm_(_b(side), _b(uplo), _b(trans), _b(diag), i(m), i(n), d(alpha),
+                        ptr(a), i(lda), ptr(b), i(ldb))
+
+    def dsyrk(self, uplo, trans, n, k, alpha, a, lda, beta, c, ldc):
+        i, d = self._i, self._d
+        self.lib.dsyrk_(_b(uplo), _b(trans), i(n), i(k), d(alpha), ptr(a), i(lda), d(beta),
+                        ptr(c), i(ldc))
+
+    def dtrmm(self, side, uplo, trans, diag, m, n, alpha, a, lda, b, ldb):
+        i, d = self._i, self._d
+        self.lib.dtrmm_(_b(side), _b(uplo), _b(trans), _b(diag), i(m), i(n), d(alpha),
+                        ptr(a), i(lda), ptr(b), i(ldb))
+
+    def idamax(self, n, x, incx):
+        self.lib.idamax_.restype = ctypes.c_int
+        return self.lib.idamax_(self._i(n), ptr(x), self._i(incx))
+
+    def dgetrf(self, m, n, a, lda, ipiv):
+        i = self._i
+        return self._info_call(self.lib.dgetrf_, i(m), i(n), ptr(a), i(lda), ptr(ipiv))
+
+    def dgetrs(self, trans, n, nrhs, a, lda, ipiv, b, ldb):
+        i = self._i
+        return self._info_call(self.lib.dgetrs_, _b(trans), i(n), i(nrhs), ptr(a), i(lda),
+                               ptr(ipiv), ptr(b), i(ldb))
+
+    def dpotrf(self, uplo, n, a, lda):
+        i = self._i
+        return self._info_call(self.lib.dpotrf_, _b(uplo), i(n), ptr(a), i(lda))
+
+    def dpotrs(self, uplo, n, nrhs, a, lda, b, ldb):
+        i = self._i
+        return self._info_call(self.lib.dpotrs_, _b(uplo), i(n), i(nrhs), ptr(a), i(lda),
+                               ptr(b), i(ldb))
+
+
+def load_refblas():
+    return RefBlas() if os.path.exists(REFBLAS_LIB) else None
