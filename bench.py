@@ -273,16 +273,45 @@ def cpu_steps(fn, steps, warmup):
     return times
 
 
+class RefLibrary:
+    """The reference library itself (oracle/_ref/libhwyblas_ref.so: its own
+    sources compiled against this repository's Highway-API shim), when it
+    was built; single-threaded like the reference."""
+
+    def __init__(self):
+        from tests.oracle_lib import load_refblas
+        self.ref = load_refblas()
+        self.kind = "reference"
+
+    def dgemm(self, *args):
+        return self.ref.dgemm(*args)
+
+
 def cpu_single_thread(cpu, n):
     """The single-threaded figure (the reference is single-threaded by
-    design): best of 3 on a 32-column sample."""
+    design): best of 3 on a 32-column sample, with the port and, where it
+    was built, with the reference library itself."""
     prev = cpu.threads
     cpu.set_threads(1)
     smp = DgemmSample(cpu, n, 32)
     best = min(cpu_steps(smp, 3, 1))
     cpu.set_threads(prev)
-    return {"value": smp.flops / best / 1e12, "unit": "TFLOP/s", "cores": 1,
-            "sample": smp.describe() + ", best of 3"}
+    out = {"value": smp.flops / best / 1e12, "unit": "TFLOP/s", "cores": 1,
+           "sample": smp.describe() + ", best of 3", "kind": cpu.kind}
+    lib = RefLibrary()
+    if lib.ref is not None:
+        smp_r = DgemmSample(lib, n, 32)
+        best_r = min(cpu_steps(smp_r, 3, 1))
+        smp_r()
+        smp()
+        out["reference_library"] = {
+            "value": smp_r.flops / best_r / 1e12, "unit": "TFLOP/s", "cores": 1,
+            "bit_identical_to_port": bool(np.array_equal(smp_r.c.view(np.uint64),
+                                                         smp.c.view(np.uint64))),
+            "note": "the reference's own sources compiled against this repository's "
+                    "portable Highway-API shim (slower than a Highway build; the port, "
+                    "bit-identical to it, is the timed baseline)"}
+    return out
 
 
 def workload_name(n):
