@@ -843,10 +843,13 @@ HWYBLAS_API unsigned int hwyblas_set_leaf_wait_limit(unsigned int polls);
  * accessible from the current device (each also reported through the error
  * handler as IDAMAX_NOALLOC), or a positive cudaError_t.
  * The scratch is a static array in the library's device code, one per
- * device. The first call on a device sets it up (looks up its address and
- * zeroes it on `stream`); make that call before capturing a stream. All
- * calls on a device share the array: calls that overlap in time (unordered
- * streams, or several host threads at once) race on it. */
+ * device. Every call looks its address up (this allocates nothing); the
+ * first call that sees an address on a device (the first on that device,
+ * or the first after its context was created again, as after
+ * cudaDeviceReset) zeroes the array on `stream`: make that call before
+ * capturing a stream. All calls on a device share the array: calls that
+ * overlap in time (unordered streams, or several host threads at once) race
+ * on it. */
 HWYBLAS_API int hwyblas_idamax_noalloc(int n, const double* x, int incx,
                                        int* result, void* stream);
 
