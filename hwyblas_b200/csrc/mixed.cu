@@ -107,89 +107,48 @@ __global__ void ColAbsMaxKernel(int n, int nrhs, const double* x, long long ldx,
   if (threadIdx.x % 32 == 0) atomicMax(out + q, bits);
 }
 
-// Residual, few right-hand sides: part[c][q][i] = sum over k in chunk c of
-// a(i, k) * x(k, q). One thread per row; the x chunk is staged in shared
-// memory.
-__global__ void __launch_bounds__(kResRows)
-    ResidualPartialKernel(int n, int nrhs, const double* a, long long lda,
-                          const double* x, long long ldx, double* part) {
-  __shared__ double sx[kResRhs][kResK];
-  const int k0 = blockIdx.y * kResK, kc = min(kResK, n - k0);
-  for (int idx = threadIdx.x; idx < kResRhs * kResK; idx += kResRows) {
-    const int q = idx / kResK, k = idx % kResK;
-    sx[q][k] = (q < nrhs && k < kc) ? x[k0 + k + q * ldx] : 0.0;
-  }
-  __syncthreads();
-  const int i = blockIdx.x * kResRows + threadIdx.x;
-  if (i >= n) return;
-  double acc[kResRhs];
-#pragma unroll
-  for (int q = 0; q < kResRhs; ++q) acc[q] = 0.0;
-  const double* ai = a + i + static_cast<long long>(k0) * lda;
-  for (int k = 0; k < kc; ++k) {
-    const double v = ai[static_cast<long long>(k) * lda];
-#pragma unroll
-    for (int q = 0; q < kResRhs; ++q)
-      if (q < nrhs) acc[q] = fma(v, sx[q][k], acc[q]);
-  }
-  double* out = part + static_cast<long long>(blockIdx.y) * nrhs * n;
-#pragma unroll
-  for (int q = 0; q < kResRhs; ++q)
-    if (q < nrhs) out[static_cast<long long>(q) * n + i] = acc[q];
-}
-
-// r(i, q) = b(i, q) - sum over chunks (in chunk order).
-__global__ void ResidualFinishKernel(int n, int nrhs, int chunks,
-                                     const double* part, const double* b,
-                                     long long ldb, double* r, long long ldr) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int q = blockIdx.y;
-  if (i >= n || q >= nrhs) return;
-  double s = 0.0;
-  for (int c = 0; c < chunks; ++c)
-    s += part[(static_cast<long long>(c) * nrhs + q) * n + i];
-  r[i + q * ldr] = b[i + q * ldb] - s;
-}
-
 // Residual with extra precision (few right-hand sides at a time): every
 // product a(i, k) x(k, q) is split exactly into p = fl(a x) and
 // e = fma(a, x, -p); the p are summed in double-double (TwoSum, Knuth) and the
 // e in FP64, per chunk of kResK columns. part_hi / part_lo are [c][q][i].
+// R right-hand sides per instantiation (1, 2, 4, 8 or 16; nrhs <= R), so
+// that a few right-hand sides do not issue the arithmetic of sixteen.
+template <int R>
 __global__ void __launch_bounds__(kResRows)
     ResidualDdPartialKernel(int n, int nrhs, const double* a, long long lda,
                             const double* x, long long ldx, double* part_hi,
                             double* part_lo) {
-  __shared__ double sx[kResRhs][kResK];
+  __shared__ double sx[R][kResK];
   const int k0 = blockIdx.y * kResK, kc = min(kResK, n - k0);
-  for (int idx = threadIdx.x; idx < kResRhs * kResK; idx += kResRows) {
+  for (int idx = threadIdx.x; idx < R * kResK; idx += kResRows) {
     const int q = idx / kResK, k = idx % kResK;
     sx[q][k] = (q < nrhs && k < kc) ? x[k0 + k + q * ldx] : 0.0;
   }
   __syncthreads();
   const int i = blockIdx.x * kResRows + threadIdx.x;
   if (i >= n) return;
-  double hi[kResRhs], lo[kResRhs];
+  double hi[R], lo[R];
 #pragma unroll
-  for (int q = 0; q < kResRhs; ++q) hi[q] = lo[q] = 0.0;
+  for (int q = 0; q < R; ++q) hi[q] = lo[q] = 0.0;
   const double* ai = a + i + static_cast<long long>(k0) * lda;
   for (int k = 0; k < kc; ++k) {
     const double v = ai[static_cast<long long>(k) * lda];
 #pragma unroll
-    for (int q = 0; q < kResRhs; ++q) {
-      if (q < nrhs) {
-        const double p = v * sx[q][k];
-        const double pe = fma(v, sx[q][k], -p);
-        const double s = hi[q] + p;
-        const double bb = s - hi[q];
-        const double e = (hi[q] - (s - bb)) + (p - bb);
-        hi[q] = s;
-        lo[q] += e + pe;
-      }
+    for (int q = 0; q < R; ++q) {
+      // Columns q >= nrhs multiply zeros: their sums stay zero and are not
+      // stored.
+      const double p = v * sx[q][k];
+      const double pe = fma(v, sx[q][k], -p);
+      const double s = hi[q] + p;
+      const double bb = s - hi[q];
+      const double e = (hi[q] - (s - bb)) + (p - bb);
+      hi[q] = s;
+      lo[q] += e + pe;
     }
   }
   const long long off = static_cast<long long>(blockIdx.y) * nrhs * n;
 #pragma unroll
-  for (int q = 0; q < kResRhs; ++q) {
+  for (int q = 0; q < R; ++q) {
     if (q < nrhs) {
       part_hi[off + static_cast<long long>(q) * n + i] = hi[q];
       part_lo[off + static_cast<long long>(q) * n + i] = lo[q];
@@ -849,24 +808,13 @@ double InfNorm(int n, const double* a, long long lda, MixedBuffers& bf) {
   return BitsToDouble(bits);
 }
 
-// r := b - A x (FP64). Many right-hand sides go through the DMMA GEMM; few
-// through a split-k GEMV whose partial sums are added in a fixed order.
+// r := b - A x in FP64 through the DMMA GEMM (the refinement's first phase
+// for 16 or more right-hand sides).
 void Residual(int n, int nrhs, const double* a, long long lda, const double* b,
               long long ldb, const double* x, long long ldx, MixedBuffers& bf) {
-  cudaStream_t st = Ctx().stream;
-  if (nrhs >= kResRhs) {
-    Copy2D(n, nrhs, b, ldb, bf.r, bf.ldr);
-    Dgemm(n, nrhs, n, -1.0, ColMajor(a, lda), ColMajor(x, ldx), 1.0, bf.r,
-          static_cast<int>(bf.ldr), kAll);
-    return;
-  }
-  const int chunks = (n + kResK - 1) / kResK;
-  ResidualPartialKernel<<<dim3((n + kResRows - 1) / kResRows, chunks), kResRows, 0, st>>>(
-      n, nrhs, a, lda, x, ldx, bf.part);
-  ResidualFinishKernel<<<dim3((n + 255) / 256, nrhs), 256, 0, st>>>(
-      n, nrhs, chunks, bf.part, b, ldb, bf.r, bf.ldr);
-  CountLaunch(2);
-  LaunchFailed("mixed residual");
+  Copy2D(n, nrhs, b, ldb, bf.r, bf.ldr);
+  Dgemm(n, nrhs, n, -1.0, ColMajor(a, lda), ColMajor(x, ldx), 1.0, bf.r,
+        static_cast<int>(bf.ldr), kAll);
 }
 
 }  // namespace
@@ -883,8 +831,19 @@ void ResidualDd(int n, int nrhs, const double* a, long long lda, const double* b
     const int g = std::min(kResRhs, nrhs - q0);
     double* ph = part;
     double* pl = part + static_cast<size_t>(chunks) * g * n;
-    ResidualDdPartialKernel<<<dim3((n + kResRows - 1) / kResRows, chunks), kResRows, 0, st>>>(
-        n, g, a, lda, x + q0 * ldx, ldx, ph, pl);
+    const dim3 grid((n + kResRows - 1) / kResRows, chunks);
+    const double* xq = x + q0 * ldx;
+    if (g == 1) {
+      ResidualDdPartialKernel<1><<<grid, kResRows, 0, st>>>(n, g, a, lda, xq, ldx, ph, pl);
+    } else if (g == 2) {
+      ResidualDdPartialKernel<2><<<grid, kResRows, 0, st>>>(n, g, a, lda, xq, ldx, ph, pl);
+    } else if (g <= 4) {
+      ResidualDdPartialKernel<4><<<grid, kResRows, 0, st>>>(n, g, a, lda, xq, ldx, ph, pl);
+    } else if (g <= 8) {
+      ResidualDdPartialKernel<8><<<grid, kResRows, 0, st>>>(n, g, a, lda, xq, ldx, ph, pl);
+    } else {
+      ResidualDdPartialKernel<16><<<grid, kResRows, 0, st>>>(n, g, a, lda, xq, ldx, ph, pl);
+    }
     ResidualDdFinishKernel<<<dim3((n + 255) / 256, g), 256, 0, st>>>(
         n, g, chunks, ph, pl, b + q0 * ldb, ldb, r + q0 * ldr, ldr);
     CountLaunch(2);
