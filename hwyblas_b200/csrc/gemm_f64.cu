@@ -308,26 +308,6 @@ __global__ void __maxnreg__(168)
         continue;
       if (kSplit && kt_lo >= kt_hi) continue;
     }
-    // The next tile's C into L2 while this tile computes: with a short k
-    // (the LU's rank-64 updates) the C loads at tile start would otherwise
-    // wait on HBM. Each of the 256 consumer threads touches two of the
-    // tile's 128-byte lines (8 lines a column, 64 columns).
-    if constexpr (!kTri && !kSplit) {
-      const int wn_next = w + gridDim.x;
-      if (p.beta != 0.0 && wn_next < num_work) {
-        int pm0, pn0;
-        TileOrigin(wn_next, tiles_m, tiles_n, &pm0, &pn0);
-        const int tid = threadIdx.x;  // consumers are warps 0..7
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int line = tid + h * 256;
-          const int i = pm0 + (line % 8) * 16, j = pn0 + line / 8;
-          if (i < p.m && j < p.n && !SkipTile(p, pm0, pn0)) {
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(p.c + i + static_cast<long long>(j) * p.ldc));
-          }
-        }
-      }
-    }
     // Element e of MMA (mb, nb) is C(row0 + mb*16 + (e >> 1),
     // col0 + nb*8 + (e & 1 ? ccol1 : ccol0)).
     const int row0 = m0 + wm * 32 + 2 * cg, col0 = n0 + wn * 32;
