@@ -45,13 +45,7 @@ constexpr int kABoxBytes = 16 * kBK * 8;
 constexpr int kTileBBytes = kBN * kBK * 8;
 constexpr int kStageBytes = kTileABytes + kTileBBytes;
 constexpr int kKtPerChunk = 256 / kBK;  // k-slices per reference KC chunk
-constexpr int kSmemBytes = kStages * kStageBytes + (2 * kStages + 4) * 8 + 1024;
-// With C staged in shared memory (GemmParams::c_smem): two 128 x 64 FP64 C
-// tiles after the ring and a 1 KB barrier area.
-constexpr int kCTileBytes = kBM * kBN * 8;
-constexpr int kCBufOffset = kStages * kStageBytes + 1024;
-constexpr int kSmemBytesC = kCBufOffset + 2 * kCTileBytes + 1024;
-static_assert(kSmemBytesC <= 227 * 1024, "C tiles exceed shared memory");
+constexpr int kSmemBytes = kStages * kStageBytes + 2 * kStages * 8 + 1024;
 
 struct GemmParams {
   int m, n, k;
@@ -66,11 +60,6 @@ struct GemmParams {
   int nchunks;
   int* timeout_flag;
   const int* guard;
-  // C tiles come into shared memory by TMA (tm_c), double-buffered, while
-  // the previous tile computes: a short k (the LU's rank-64 updates) would
-  // otherwise wait on C at every tile. Only for a plain product (no
-  // triangular operand or part, no split, beta != 0).
-  int c_smem;
 };
 
 // k range [*kb, *ke) that the reference multiplies for C(i, j) when an
@@ -177,7 +166,6 @@ __device__ __forceinline__ void Dmma(double (&d)[4], const double (&a)[4],
 // tile boundaries (kt = -1: the current tile's slices are not yet known).
 struct Producer {
   int tile, kt, kt_hi, gs;
-  int ct;  // tiles whose C has been requested (c_smem)
 };
 
 // The k-slices [*lo, *hi) of work item w (a tile, or a tile's chunk when
@@ -204,8 +192,7 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
                                           int tiles_m, int tiles_n, int kt_total,
                                           uint8_t* smem, uint64_t* full,
                                           uint64_t* empty, const CUtensorMap* tm_a,
-                                          const CUtensorMap* tm_b, const CUtensorMap* tm_c,
-                                          uint64_t* c_full, uint64_t* c_empty) {
+                                          const CUtensorMap* tm_b) {
   const int num_tiles = tiles_m * tiles_n;
   const int num_work = kSplit ? num_tiles * p.nchunks : num_tiles;
   int m0 = 0, n0 = 0;
@@ -229,17 +216,6 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
     if constexpr (kTri || kSplit) pr.kt = -1;
   }
   if (pr.tile >= num_work) return true;
-  if constexpr (!kTri && !kSplit) {
-    if (p.c_smem && pr.kt == 0) {
-      // First slice of a tile: its C into buffer ct % 2, once the consumers
-      // have read what the tile two back left there.
-      const int b = pr.ct & 1, use = pr.ct >> 1;
-      if (use > 0 && !MbarWait(&c_empty[b], (use - 1) & 1, p.timeout_flag)) return false;
-      MbarArriveExpectTx(&c_full[b], kCTileBytes);
-      TmaLoad2d(smem + kCBufOffset + b * kCTileBytes, tm_c, m0, n0, &c_full[b]);
-      ++pr.ct;
-    }
-  }
   const int s = pr.gs % kStages, round = pr.gs / kStages;
   if (round > 0 && !MbarWait(&empty[s], (round - 1) & 1, p.timeout_flag)) return false;
   uint8_t* st = smem + s * kStageBytes;
@@ -271,8 +247,7 @@ __device__ __forceinline__ bool IssueNext(Producer& pr, const GemmParams& p,
 template <int kTriKind, bool kSplit>
 __global__ void __maxnreg__(168)
     DgemmDmmaKernel(const __grid_constant__ CUtensorMap tm_a,
-                    const __grid_constant__ CUtensorMap tm_b,
-                    const __grid_constant__ CUtensorMap tm_c, GemmParams p) {
+                    const __grid_constant__ CUtensorMap tm_b, GemmParams p) {
   // kTriKind: 0 no triangular operand, 1 op(A) triangular, 2 op(B).
   constexpr bool kTri = kTriKind != 0, kTriA = kTriKind == 1, kTriB = kTriKind == 2;
   if (p.guard != nullptr && *p.guard != 0) return;
@@ -288,17 +263,11 @@ __global__ void __maxnreg__(168)
   uint8_t* smem = smem_raw + ((1024 - (SmemAddr(smem_raw) & 1023)) & 1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* c_full = empty + kStages;  // [2], used when p.c_smem
-  uint64_t* c_empty = c_full + 2;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       MbarInit(&full[s], 1);
       MbarInit(&empty[s], kConsumerWarps);
-    }
-    for (int b = 0; b < 2; ++b) {
-      MbarInit(&c_full[b], 1);
-      MbarInit(&c_empty[b], kConsumerWarps);
     }
     FenceBarrierInit();
   }
@@ -309,11 +278,10 @@ __global__ void __maxnreg__(168)
     if (lane == 0) {
       PrefetchTmap(&tm_a);
       PrefetchTmap(&tm_b);
-      if (p.c_smem) PrefetchTmap(&tm_c);
-      Producer pr{static_cast<int>(blockIdx.x), (kTri || kSplit) ? -1 : 0, 0, 0, 0};
+      Producer pr{static_cast<int>(blockIdx.x), (kTri || kSplit) ? -1 : 0, 0, 0};
       while (pr.tile < num_work) {
         if (!IssueNext<kTri, kSplit>(pr, p, tiles_m, tiles_n, kt_total, smem, full, empty,
-                                     &tm_a, &tm_b, &tm_c, c_full, c_empty))
+                                     &tm_a, &tm_b))
           return;
       }
     }
@@ -329,7 +297,6 @@ __global__ void __maxnreg__(168)
   const int ccol1 = 2 * ((2 * t + 1) & 3) + ((2 * t + 1) >> 2);
   const int bcol = 2 * (g & 3) + (g >> 2);  // tile column of this lane's B
   int gs = 0;
-  int ct = 0;  // tiles of this CTA so far (c_smem buffer ct % 2)
   for (int w = blockIdx.x; w < num_work; w += gridDim.x) {
     int m0, n0, kt_lo = 0, kt_hi = kt_total;
     if constexpr (!kTri && !kSplit) {
@@ -363,8 +330,8 @@ __global__ void __maxnreg__(168)
           if (inside) in_part |= 1u << bit;
           if (inside && p.part != kAll && InCrossingTile(p.part, p.m, p.n, i, j))
             crossing |= 1u << bit;
-          cacc[mb][nb][e] = (!kSplit && !p.c_smem && inside && p.beta != 0.0)
-                                ? p.c[i + j * p.ldc] : 0.0;
+          cacc[mb][nb][e] =
+              (!kSplit && inside && p.beta != 0.0) ? p.c[i + j * p.ldc] : 0.0;
         }
     // kTri: k ranges of the 16-row blocks [xb, xe) (op(A) triangular), and the
     // union [ub, ue) and intersection [ib, ie) of the ranges of the 8-column
@@ -530,36 +497,9 @@ __global__ void __maxnreg__(168)
       if (lane == 0) MbarArrive(&empty[s]);
 
       // End of a reference KC chunk: merge into the running C value.
-      if (!kSplit && ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_hi)) {
-        if constexpr (!kTri) {
-          if (p.c_smem && kt / kKtPerChunk == 0) {
-            // The tile's C from its shared-memory buffer (column-major,
-            // 128 rows), then the buffer back to the producer.
-            const int b = ct & 1;
-            if (!MbarWait(&c_full[b], (ct >> 1) & 1, p.timeout_flag)) return;
-            const double* sc =
-                reinterpret_cast<const double*>(smem + kCBufOffset + b * kCTileBytes);
-#pragma unroll
-            for (int mb = 0; mb < 2; ++mb)
-#pragma unroll
-              for (int nb = 0; nb < 4; ++nb)
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  const int il = row0 - m0 + mb * 16 + (e >> 1);
-                  const int jl = col0 - n0 + nb * 8 + ((e & 1) ? ccol1 : ccol0);
-                  cacc[mb][nb][e] = sc[il + jl * kBM];
-                }
-            // As for the ring: the generic reads are ordered before the
-            // buffer's refill by TMA (the async proxy).
-            __syncwarp();
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (lane == 0) MbarArrive(&c_empty[b]);
-          }
-        }
+      if (!kSplit && ((kt + 1) % kKtPerChunk == 0 || kt + 1 == kt_hi))
         merge(kt / kKtPerChunk);
-      }
     }
-    if (p.c_smem) ++ct;
 
     // Epilogue: write C, or the chunk's raw accumulators.
     const long long pbase =
@@ -898,20 +838,14 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   p.nchunks = 1;
   p.timeout_flag = ctx.dev_status;
   p.guard = ctx.guard;
-  p.c_smem = 0;
   const long long tiles =
       static_cast<long long>((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
   static bool configured = false;
-  static bool c_smem_ok = false;
   if (!configured) {
     const auto set = [](const void* f) {
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     };
-    c_smem_ok = cudaFuncSetAttribute(reinterpret_cast<const void*>(DgemmDmmaKernel<0, false>),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kSmemBytesC) == cudaSuccess;
-    cudaGetLastError();
-    if (!c_smem_ok) set(reinterpret_cast<const void*>(DgemmDmmaKernel<0, false>));
+    set(reinterpret_cast<const void*>(DgemmDmmaKernel<0, false>));
     set(reinterpret_cast<const void*>(DgemmDmmaKernel<1, false>));
     set(reinterpret_cast<const void*>(DgemmDmmaKernel<2, false>));
     set(reinterpret_cast<const void*>(DgemmDmmaKernel<0, true>));
@@ -936,11 +870,11 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles * nchunks, sms));
       cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
       if (tri_kind == 0) {
-        DgemmDmmaKernel<0, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, ma, p);
+        DgemmDmmaKernel<0, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
       } else if (tri_kind == 1) {
-        DgemmDmmaKernel<1, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, ma, p);
+        DgemmDmmaKernel<1, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
       } else {
-        DgemmDmmaKernel<2, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, ma, p);
+        DgemmDmmaKernel<2, true><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
       }
       KernelTimerStop(t0, ctx.stream);
       const long long total = static_cast<long long>(m) * n;
@@ -951,15 +885,6 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       return;
     }
   }
-  // C through shared memory: a plain product with beta != 0 whose C is a
-  // valid TMA operand (16-byte aligned base and leading dimension).
-  CUtensorMap mc;
-  if (c_smem_ok && tri_kind == 0 && part == kAll && beta != 0.0 &&
-      TmaReady(c, ldc, 8) &&
-      MakeTensorMap2d(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, c, m, n, ldc, kBM, kBN,
-                      CU_TENSOR_MAP_SWIZZLE_NONE)) {
-    p.c_smem = 1;
-  }
   // Persistent grid: one CTA per SM (the accumulators and the prefetched C
   // take 128 of each thread's registers). Measured against a variant whose
   // producer is lane 0 of warp 0 (8 warps): dgemm n = 8192 32.9 vs 27.5
@@ -968,12 +893,11 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
   const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles, sms));
   cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
   if (tri_kind == 0) {
-    DgemmDmmaKernel<0, false><<<grid, kThreads, p.c_smem ? kSmemBytesC : kSmemBytes,
-                                ctx.stream>>>(ma, mb, p.c_smem ? mc : ma, p);
+    DgemmDmmaKernel<0, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   } else if (tri_kind == 1) {
-    DgemmDmmaKernel<1, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, ma, p);
+    DgemmDmmaKernel<1, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   } else {
-    DgemmDmmaKernel<2, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, ma, p);
+    DgemmDmmaKernel<2, false><<<grid, kThreads, kSmemBytes, ctx.stream>>>(ma, mb, p);
   }
   KernelTimerStop(t0, ctx.stream);
   CountLaunch();
