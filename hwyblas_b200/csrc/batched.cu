@@ -213,6 +213,160 @@ __device__ void CtaGemmDmma(int m, int n, int k, double alpha, Mat<double> a, Ma
   __syncthreads();
 }
 
+// The same per-element chains with register tiles: the CTA's Threads threads
+// form a 16 x (Threads / 16) grid, each computing a 4 x 4 block of C; k-blocks
+// of 16 of A and B are staged in shared memory (the next one fetched into
+// registers while the current one is used) and each element's FMA chain runs
+// over q in ascending order, restarted every KC, exactly as in CtaGemm.
+template <typename T, int Threads>
+struct RegTile {
+  static constexpr int kTM = 64, kTN = 4 * (Threads / 16), kKb = 16;
+  static constexpr int kSA = kTM + 4, kSB = kTN + 4;  // row strides (elements)
+  static constexpr int kLoadA = kKb * kTM / Threads, kLoadB = kKb * kTN / Threads;
+};
+
+template <typename T>
+__device__ __forceinline__ void Load4(const T* p, T (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    const double2 x = *reinterpret_cast<const double2*>(p);
+    const double2 y = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+  }
+}
+
+template <typename T, int Threads>
+__device__ void CtaGemmReg(int m, int n, int k, T alpha, Mat<T> a, Mat<T> b, T beta,
+                           Mat<T> c, T* sA, T* sB) {
+  using Cfg = RegTile<T, Threads>;
+  constexpr int KC = Kc<T>::value, TM = Cfg::kTM, TN = Cfg::kTN, KB = Cfg::kKb;
+  constexpr int SA = Cfg::kSA, SB = Cfg::kSB;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const bool a_rows = a.rs == 1;  // A(i, q) contiguous in i
+  const bool b_rows = b.rs == 1;  // B(q, j) contiguous in q
+  for (int m0 = 0; m0 < m; m0 += TM) {
+    for (int n0 = 0; n0 < n; n0 += TN) {
+      T acc[4][4];
+      T ra[Cfg::kLoadA], rb[Cfg::kLoadB];
+      const auto fetch = [&](int kb0) {
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadA; ++l) {
+          const int idx = threadIdx.x + l * Threads;
+          const int i = a_rows ? idx % TM : idx / KB;
+          const int q = a_rows ? idx / TM : idx % KB;
+          ra[l] = (m0 + i < m && kb0 + q < k) ? a(m0 + i, kb0 + q) : T(0);
+        }
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadB; ++l) {
+          const int idx = threadIdx.x + l * Threads;
+          const int q = b_rows ? idx % KB : idx / TN;
+          const int j = b_rows ? idx / KB : idx % TN;
+          rb[l] = (n0 + j < n && kb0 + q < k) ? b(kb0 + q, n0 + j) : T(0);
+        }
+      };
+      const auto stash = [&]() {
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadA; ++l) {
+          const int idx = threadIdx.x + l * Threads;
+          const int i = a_rows ? idx % TM : idx / KB;
+          const int q = a_rows ? idx / TM : idx % KB;
+          sA[q * SA + i] = ra[l];
+        }
+#pragma unroll
+        for (int l = 0; l < Cfg::kLoadB; ++l) {
+          const int idx = threadIdx.x + l * Threads;
+          const int q = b_rows ? idx % KB : idx / TN;
+          const int j = b_rows ? idx / KB : idx % TN;
+          sB[q * SB + j] = rb[l];
+        }
+      };
+      fetch(0);
+      for (int pc = 0; pc < k; pc += KC) {
+        const int pe = min(k, pc + KC);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) acc[r][s] = T(0);
+        for (int kb0 = pc; kb0 < pe; kb0 += KB) {
+          __syncthreads();  // the previous block is read
+          stash();
+          __syncthreads();
+          if (kb0 + KB < k) fetch(kb0 + KB);
+          const int steps = min(pe, kb0 + KB) - kb0;
+          for (int q = 0; q < steps; ++q) {
+            T av[4], bv[4];
+            Load4(sA + q * SA + 4 * tx, av);
+            Load4(sB + q * SB + 4 * ty, bv);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+              for (int s = 0; s < 4; ++s) acc[r][s] = fma(av[r], bv[s], acc[r][s]);
+          }
+        }
+        // Merge the chunk into C (CtaGemm's rules; each element is read and
+        // written by its own thread only).
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            const int i = m0 + 4 * tx + r, j = n0 + 4 * ty + s;
+            if (i >= m || j >= n) continue;
+            const T v = alpha * acc[r][s];
+            if (pc != 0 || beta == T(1)) {
+              c(i, j) = v + c(i, j);
+            } else if (beta == T(0)) {
+              c(i, j) = v;
+            } else {
+              c(i, j) = fma(c(i, j), beta, v);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// The GEMM a batched factorization or solve calls for its updates: the
+// per-element chains (any type, any CTA size) or, in FP64, the tensor-pipe
+// tiles for blocks of at least 16 x 16 (the CTA has the tile's warps). Both
+// give every element the same bits.
+template <typename T>
+struct ElemGemm {
+  __device__ void operator()(int m, int n, int k, T alpha, Mat<T> a, Mat<T> b, T beta,
+                             Mat<T> c) const {
+    CtaGemm<T>(m, n, k, alpha, a, b, beta, c);
+  }
+};
+
+template <typename T, int Threads>
+struct RegGemm {
+  T* sA;
+  T* sB;
+  __device__ void operator()(int m, int n, int k, T alpha, Mat<T> a, Mat<T> b, T beta,
+                             Mat<T> c) const {
+    if (m < 16 || n < 16)
+      CtaGemm<T>(m, n, k, alpha, a, b, beta, c);
+    else
+      CtaGemmReg<T, Threads>(m, n, k, alpha, a, b, beta, c, sA, sB);
+  }
+};
+
+template <int WM, int WN, int NB>
+struct TileGemm {
+  double* sA;
+  double* sB;
+  __device__ void operator()(int m, int n, int k, double alpha, Mat<double> a,
+                             Mat<double> b, double beta, Mat<double> c) const {
+    if (m < 16 || n < 16)
+      CtaGemm<double>(m, n, k, alpha, a, b, beta, c);
+    else
+      CtaGemmDmma<WM, WN, NB>(m, n, k, alpha, a, b, beta, c, sA, sB);
+  }
+};
+
 // Row interchanges k1..k2 (1-based, increasing) of ncols columns.
 template <typename T>
 __device__ void CtaLaswp(int ncols, Mat<T> a, int k1, int k2, const int* ipiv) {
@@ -305,9 +459,9 @@ __device__ void CtaTrsmBase(Mat<T> t, bool lower, bool unit, int r, int other, T
 // Left-side triangular solve op(T) X = B (op(T) is `tri`, r x r; X is r x
 // other, column-major ld ldb) by the reference's recursion, emulated with an
 // explicit stack: top half, GEMM update, bottom half (lower; upper mirrored).
-template <typename T>
+template <typename T, typename G>
 __device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other, T* b,
-                            long long ldb, T (*st)[33], T* sinv) {
+                            long long ldb, T (*st)[33], T* sinv, const G& gemm) {
   if (r <= 0 || other <= 0) return;
   int s_off[8], s_r[8], s_ph[8];
   int sp = 0;
@@ -338,8 +492,8 @@ __device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other,
         s_r[sp] = r1;
         s_ph[sp] = 0;
       } else {
-        CtaGemm<T>(r2, other, r1, T(-1), tri.sub(off + r1, off), Col(b + off, ldb), T(1),
-                   Col(b + off + r1, ldb));
+        gemm(r2, other, r1, T(-1), tri.sub(off + r1, off), Col(b + off, ldb), T(1),
+             Col(b + off + r1, ldb));
         ++sp;
         s_off[sp] = off + r1;
         s_r[sp] = r2;
@@ -352,8 +506,8 @@ __device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other,
         s_r[sp] = r2;
         s_ph[sp] = 0;
       } else {
-        CtaGemm<T>(r1, other, r2, T(-1), tri.sub(off, off + r1), Col(b + off + r1, ldb),
-                   T(1), Col(b + off, ldb));
+        gemm(r1, other, r2, T(-1), tri.sub(off, off + r1), Col(b + off + r1, ldb), T(1),
+             Col(b + off, ldb));
         ++sp;
         s_off[sp] = off;
         s_r[sp] = r1;
@@ -366,9 +520,9 @@ __device__ void CtaTrsmLeft(Mat<T> tri, bool lower, bool unit, int r, int other,
 // Right-side triangular solve X op(T) = B (X is other x r, column-major ld
 // ldb), the reference's recursion for the right side: lower solves the
 // trailing block first, upper the leading one.
-template <typename T>
+template <typename T, typename G>
 __device__ void CtaTrsmRight(Mat<T> tri, bool lower, bool unit, int r, int other, T* b,
-                             long long ldb, T (*st)[33], T* sinv) {
+                             long long ldb, T (*st)[33], T* sinv, const G& gemm) {
   if (r <= 0 || other <= 0) return;
   int s_off[8], s_r[8], s_ph[8];
   int sp = 0;
@@ -397,11 +551,11 @@ __device__ void CtaTrsmRight(Mat<T> tri, bool lower, bool unit, int r, int other
       s_ph[sp] = 0;
     } else {
       if (lower) {
-        CtaGemm<T>(other, r1, r2, T(-1), Col(b + (off + r1) * ldb, ldb),
-                   tri.sub(off + r1, off), T(1), Col(b + off * ldb, ldb));
+        gemm(other, r1, r2, T(-1), Col(b + (off + r1) * ldb, ldb), tri.sub(off + r1, off),
+             T(1), Col(b + off * ldb, ldb));
       } else {
-        CtaGemm<T>(other, r2, r1, T(-1), Col(b + off * ldb, ldb), tri.sub(off, off + r1),
-                   T(1), Col(b + (off + r1) * ldb, ldb));
+        gemm(other, r2, r1, T(-1), Col(b + off * ldb, ldb), tri.sub(off, off + r1), T(1),
+             Col(b + (off + r1) * ldb, ldb));
       }
       ++sp;
       s_off[sp] = first_trailing ? off : off + r1;
@@ -507,9 +661,9 @@ __device__ void CtaLeaf(int m, int n, Mat<T> a, int* ipiv, int* info, int col0, 
 // block's pivots in ipiv (block-relative, 1-based) and col0 its first global
 // column (for INFO). Recursion emulated with an explicit stack; frames sit
 // on the block's diagonal at offset off.
-template <typename T>
+template <typename T, typename G>
 __device__ void CtaGetrfRec(int m, int n, Mat<T> a, int* ipiv, int* info, int col0,
-                            int lanes, LuShared<T>& sh) {
+                            int lanes, LuShared<T>& sh, const G& gemm) {
   int s_m[12], s_n[12], s_off[12], s_ph[12];
   int sp = 0;
   s_m[0] = m;
@@ -540,9 +694,8 @@ __device__ void CtaGetrfRec(int m, int n, Mat<T> a, int* ipiv, int* info, int co
       s_ph[sp] = 0;
     } else if (ph == 1) {
       CtaLaswp(n2, fa.sub(0, n1), 1, n1, fp);
-      CtaTrsmLeft(fa, true, true, n1, n2, &fa(0, n1), fa.cs, sh.st, sh.sinv);
-      CtaGemm<T>(fm - n1, n2, n1, T(-1), fa.sub(n1, 0), fa.sub(0, n1), T(1),
-                 fa.sub(n1, n1));
+      CtaTrsmLeft(fa, true, true, n1, n2, &fa(0, n1), fa.cs, sh.st, sh.sinv, gemm);
+      gemm(fm - n1, n2, n1, T(-1), fa.sub(n1, 0), fa.sub(0, n1), T(1), fa.sub(n1, n1));
       ++sp;
       s_m[sp] = fm - n1;
       s_n[sp] = n2;
@@ -558,46 +711,46 @@ __device__ void CtaGetrfRec(int m, int n, Mat<T> a, int* ipiv, int* info, int co
 }
 
 // The reference's blocked LU (Getrf, nb = 64) of an n x n matrix.
-template <typename T>
+template <typename T, typename G>
 __device__ void CtaGetrf(int n, Mat<T> a, int* ipiv, int* info, int lanes,
-                         LuShared<T>& sh) {
+                         LuShared<T>& sh, const G& gemm) {
   constexpr int nb = 64;
   if (n == 0) return;
   if (nb >= n) {
-    CtaGetrfRec(n, n, a, ipiv, info, 0, lanes, sh);
+    CtaGetrfRec(n, n, a, ipiv, info, 0, lanes, sh, gemm);
     return;
   }
   for (int j = 0; j < n; j += nb) {
     const int jb = min(n - j, nb);
-    CtaGetrfRec(n - j, jb, a.sub(j, j), ipiv + j, info, j, lanes, sh);
+    CtaGetrfRec(n - j, jb, a.sub(j, j), ipiv + j, info, j, lanes, sh, gemm);
     for (int i = j + threadIdx.x; i < j + jb; i += blockDim.x) ipiv[i] += j;
     __syncthreads();
     CtaLaswp(j, a, j + 1, j + jb, ipiv);
     if (j + jb < n) {
       CtaLaswp(n - j - jb, a.sub(0, j + jb), j + 1, j + jb, ipiv);
       CtaTrsmLeft(a.sub(j, j), true, true, jb, n - j - jb, &a(j, j + jb), a.cs, sh.st,
-                  sh.sinv);
-      CtaGemm<T>(n - j - jb, n - j - jb, jb, T(-1), a.sub(j + jb, j), a.sub(j, j + jb),
-                 T(1), a.sub(j + jb, j + jb));
+                  sh.sinv, gemm);
+      gemm(n - j - jb, n - j - jb, jb, T(-1), a.sub(j + jb, j), a.sub(j, j + jb), T(1),
+           a.sub(j + jb, j + jb));
     }
   }
 }
 
 // The reference's Getrs: solve op(A) X = B with the LU factors.
-template <typename T>
+template <typename T, typename G>
 __device__ void CtaGetrs(bool trans, int n, int nrhs, Mat<T> a, const int* ipiv, T* b,
-                         long long ldb, LuShared<T>& sh) {
+                         long long ldb, LuShared<T>& sh, const G& gemm) {
   if (n == 0 || nrhs == 0) return;
   const Mat<T> bm = Col(b, ldb);
   if (!trans) {
     CtaLaswp(nrhs, bm, 1, n, ipiv);
-    CtaTrsmLeft(a, true, true, n, nrhs, b, ldb, sh.st, sh.sinv);
-    CtaTrsmLeft(a, false, false, n, nrhs, b, ldb, sh.st, sh.sinv);
+    CtaTrsmLeft(a, true, true, n, nrhs, b, ldb, sh.st, sh.sinv, gemm);
+    CtaTrsmLeft(a, false, false, n, nrhs, b, ldb, sh.st, sh.sinv, gemm);
   } else {
     // op(T) = T^T: the transposed view, upper <-> lower.
     const Mat<T> at = {a.p, a.cs, a.rs};
-    CtaTrsmLeft(at, true, false, n, nrhs, b, ldb, sh.st, sh.sinv);
-    CtaTrsmLeft(at, false, true, n, nrhs, b, ldb, sh.st, sh.sinv);
+    CtaTrsmLeft(at, true, false, n, nrhs, b, ldb, sh.st, sh.sinv, gemm);
+    CtaTrsmLeft(at, false, true, n, nrhs, b, ldb, sh.st, sh.sinv, gemm);
     CtaLaswpBack(nrhs, bm, 1, n, ipiv);
   }
 }
@@ -636,35 +789,33 @@ __device__ __forceinline__ int NextProblem(const BatchArgs<T>& p, int* slot) {
   return q < p.count ? p.order[q] : -1;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) BatchedGetrfKernel(BatchArgs<T> p) {
-  __shared__ LuShared<T> sh;
-  __shared__ int slot;
-  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+// The three queue loops, each with the GEMM its updates use.
+template <typename T, typename G>
+__device__ void GetrfProblems(const BatchArgs<T>& p, const G& gemm, LuShared<T>& sh,
+                              int* slot) {
+  for (int id = NextProblem(p, slot); id >= 0; id = NextProblem(p, slot)) {
     if (threadIdx.x == 0) p.info[id] = 0;
     __syncthreads();
-    CtaGetrf(p.m[id], Col(p.a[id], p.lda[id]), p.ipiv[id], &p.info[id], p.lanes, sh);
+    CtaGetrf(p.m[id], Col(p.a[id], p.lda[id]), p.ipiv[id], &p.info[id], p.lanes, sh, gemm);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) BatchedGetrsKernel(BatchArgs<T> p) {
-  __shared__ LuShared<T> sh;
-  __shared__ int slot;
-  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+template <typename T, typename G>
+__device__ void GetrsProblems(const BatchArgs<T>& p, const G& gemm, LuShared<T>& sh,
+                              int* slot) {
+  for (int id = NextProblem(p, slot); id >= 0; id = NextProblem(p, slot)) {
     CtaGetrs(p.flags != 0, p.m[id], p.n[id], Col(p.a[id], p.lda[id]), p.ipiv[id], p.b[id],
-             p.ldb[id], sh);
+             p.ldb[id], sh, gemm);
   }
 }
 
 // TRSM (src/trsm.cc:137-180): B := alpha*B first (alpha != 1; B zeroed for
 // alpha == 0), then the recursion on op(A). flags: bit 0 right side, bit 1
 // lower, bit 2 transposed, bit 3 unit diagonal.
-template <typename T>
-__global__ void __launch_bounds__(256) BatchedTrsmKernel(BatchArgs<T> p) {
-  __shared__ LuShared<T> sh;
-  __shared__ int slot;
-  for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
+template <typename T, typename G>
+__device__ void TrsmProblems(const BatchArgs<T>& p, const G& gemm, LuShared<T>& sh,
+                             int* slot) {
+  for (int id = NextProblem(p, slot); id >= 0; id = NextProblem(p, slot)) {
     const int m = p.m[id], n = p.n[id];
     if (m == 0 || n == 0) continue;
     const bool right = p.flags & 1, lower = p.flags & 2, trans = p.flags & 4,
@@ -683,14 +834,50 @@ __global__ void __launch_bounds__(256) BatchedTrsmKernel(BatchArgs<T> p) {
     const Mat<T> tri = trans ? Mat<T>{p.a[id], la, 1} : Col(p.a[id], la);
     const bool op_lower = trans ? !lower : lower;
     if (right)
-      CtaTrsmRight(tri, op_lower, unit, n, m, b, ldb, sh.st, sh.sinv);
+      CtaTrsmRight(tri, op_lower, unit, n, m, b, ldb, sh.st, sh.sinv, gemm);
     else
-      CtaTrsmLeft(tri, op_lower, unit, m, n, b, ldb, sh.st, sh.sinv);
+      CtaTrsmLeft(tri, op_lower, unit, m, n, b, ldb, sh.st, sh.sinv, gemm);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) BatchedGemmKernel(BatchArgs<T> p) {
+enum BatchKindDev { kDevGetrf = 0, kDevGetrs = 1, kDevTrsm = 3 };
+
+template <int Kind, typename T, typename G>
+__device__ __forceinline__ void RunProblems(const BatchArgs<T>& p, const G& gemm,
+                                            LuShared<T>& sh, int* slot) {
+  if (Kind == kDevGetrf) GetrfProblems(p, gemm, sh, slot);
+  else if (Kind == kDevGetrs) GetrsProblems(p, gemm, sh, slot);
+  else TrsmProblems(p, gemm, sh, slot);
+}
+
+// Per-element updates (any CTA size up to 256).
+template <int Kind, typename T, int Threads, int MinBlocks = 1>
+__global__ void __launch_bounds__(Threads, MinBlocks) BatchedLuKernel(BatchArgs<T> p) {
+  using Cfg = RegTile<T, Threads>;
+  __shared__ LuShared<T> sh;
+  __shared__ __align__(16) T sA[Cfg::kKb * Cfg::kSA];
+  __shared__ __align__(16) T sB[Cfg::kKb * Cfg::kSB];
+  __shared__ int slot;
+  RunProblems<Kind>(p, RegGemm<T, Threads>{sA, sB}, sh, &slot);
+}
+
+// FP64 updates on the tensor pipe (the CTA has the tile's WM x WN warps).
+template <int Kind, int WM, int WN, int NB, int MinBlocks = 1>
+__global__ void __launch_bounds__(DmmaTile<WM, WN, NB>::kThreads, MinBlocks)
+    BatchedLuDmmaKernel(BatchArgs<double> p) {
+  using Cfg = DmmaTile<WM, WN, NB>;
+  __shared__ LuShared<double> sh;
+  __shared__ double sA[kDmmaKb * Cfg::kSA];
+  __shared__ double sB[kDmmaKb * Cfg::kSB];
+  __shared__ int slot;
+  RunProblems<Kind>(p, TileGemm<WM, WN, NB>{sA, sB}, sh, &slot);
+}
+
+template <typename T, int Threads>
+__global__ void __launch_bounds__(Threads, 512 / Threads) BatchedGemmKernel(BatchArgs<T> p) {
+  using Cfg = RegTile<T, Threads>;
+  __shared__ __align__(16) T sA[Cfg::kKb * Cfg::kSA];
+  __shared__ __align__(16) T sB[Cfg::kKb * Cfg::kSB];
   __shared__ int slot;
   for (int id = NextProblem(p, &slot); id >= 0; id = NextProblem(p, &slot)) {
     const long long la = p.lda[id], lb = p.ldb[id];
@@ -710,7 +897,7 @@ __global__ void __launch_bounds__(256) BatchedGemmKernel(BatchArgs<T> p) {
       __syncthreads();
       continue;
     }
-    CtaGemm<T>(m, n, k, p.alpha, a, b, p.beta, Col(p.c[id], p.ldc[id]));
+    RegGemm<T, Threads>{sA, sB}(m, n, k, p.alpha, a, b, p.beta, Col(p.c[id], p.ldc[id]));
   }
 }
 
@@ -844,32 +1031,56 @@ struct Layout {
 enum BatchKind { kBatchGetrf = 0, kBatchGetrs = 1, kBatchGemm = 2, kBatchTrsm = 3 };
 
 // A launch configuration of the autotuner: the threads per CTA of the
-// per-element kernels (64, 128, 256), or a tile shape of the FP64 tensor-pipe
-// GEMM (kDmma32: 32 x 32 tiles, 4 warps; kDmma64: 64 x 64 tiles, 8 warps).
-constexpr int kDmma32 = 1001, kDmma64 = 1002;
+// register-tiled FMA kernels (64, 128, 256; kDense128: 128 threads with
+// registers capped for six CTAs an SM), or a tile shape of the FP64
+// tensor-pipe GEMM that the routine's products use (kDmma32: 32 x 32 tiles,
+// 4 warps; kDmma64: 64 x 64 tiles, 8 warps).
+constexpr int kDmma32 = 1001, kDmma64 = 1002, kDense128 = 1128;
 
 int ThreadsOf(int config) {
-  return config == kDmma32 ? DmmaTile<2, 2, 2>::kThreads
-         : config == kDmma64 ? DmmaTile<4, 2, 4>::kThreads : config;
+  return config == kDmma32     ? DmmaTile<2, 2, 2>::kThreads
+         : config == kDmma64   ? DmmaTile<4, 2, 4>::kThreads
+         : config == kDense128 ? 128
+                               : config;
+}
+
+template <int Kind, typename T>
+void* LuKernelOf(int config) {
+  if constexpr (sizeof(T) == 8) {
+    if (config == kDmma32) return reinterpret_cast<void*>(BatchedLuDmmaKernel<Kind, 2, 2, 2, 4>);
+    if (config == kDmma64) return reinterpret_cast<void*>(BatchedLuDmmaKernel<Kind, 4, 2, 4, 3>);
+  }
+  if (config == 64) return reinterpret_cast<void*>(BatchedLuKernel<Kind, T, 64, 8>);
+  if (config == 128) return reinterpret_cast<void*>(BatchedLuKernel<Kind, T, 128, 4>);
+  if (config == kDense128) return reinterpret_cast<void*>(BatchedLuKernel<Kind, T, 128, 6>);
+  return reinterpret_cast<void*>(BatchedLuKernel<Kind, T, 256, 3>);
 }
 
 template <typename T>
 void* KernelOf(int kind, int config) {
-  if (kind == kBatchGetrf) return reinterpret_cast<void*>(BatchedGetrfKernel<T>);
-  if (kind == kBatchGetrs) return reinterpret_cast<void*>(BatchedGetrsKernel<T>);
-  if (kind == kBatchTrsm) return reinterpret_cast<void*>(BatchedTrsmKernel<T>);
+  if (kind == kBatchGetrf) return LuKernelOf<kDevGetrf, T>(config);
+  if (kind == kBatchGetrs) return LuKernelOf<kDevGetrs, T>(config);
+  if (kind == kBatchTrsm) return LuKernelOf<kDevTrsm, T>(config);
   if (sizeof(T) == 8 && config == kDmma32)
     return reinterpret_cast<void*>(BatchedGemmDmmaKernel<2, 2, 2>);
   if (sizeof(T) == 8 && config == kDmma64)
     return reinterpret_cast<void*>(BatchedGemmDmmaKernel<4, 2, 4>);
-  return reinterpret_cast<void*>(BatchedGemmKernel<T>);
+  if (config == 64) return reinterpret_cast<void*>(BatchedGemmKernel<T, 64>);
+  if (config == 128) return reinterpret_cast<void*>(BatchedGemmKernel<T, 128>);
+  return reinterpret_cast<void*>(BatchedGemmKernel<T, 256>);
 }
 
-// The configurations the autotuner times for a routine and type.
+// The configurations the autotuner times for a routine and type: in FP64
+// every routine also has the tensor-pipe variants for its products.
 template <typename T>
 std::vector<int> Candidates(int kind) {
-  if (sizeof(T) == 8 && kind == kBatchGemm) return {64, 128, 256, kDmma32, kDmma64};
-  return {64, 128, 256};
+  std::vector<int> c = {64, 128, 256};
+  if (kind != kBatchGemm) c.push_back(kDense128);
+  if (sizeof(T) == 8) {
+    c.push_back(kDmma32);
+    c.push_back(kDmma64);
+  }
+  return c;
 }
 
 // Threads per CTA for a batch: the autotuner's choice for the batch's size
@@ -1056,9 +1267,8 @@ __global__ void FillRandomKernel(double* x, long long count, unsigned seed, doub
 }
 
 // The autotuner: for (routine, type, size bucket), the launch configuration
-// (threads per CTA in {64, 128, 256}; for the FP64 GEMM also the tensor-pipe
-// kernel with 32 x 32 or 64 x 64 tiles) that runs 96 synthetic problems of
-// the bucket's representative size fastest (results do not depend on the
+// (Candidates above) that runs a few waves of synthetic problems
+// of the bucket's representative size fastest (results do not depend on the
 // choice: every problem's arithmetic is the same whichever configuration
 // runs it).
 // A configuration set by hwyblas_batched_set_config (0: the autotuner's).
@@ -1083,8 +1293,12 @@ int TunedConfig(int kind, int median_m, int median_n) {
   }
   const int nn = std::min(512, std::max(8, 3 << std::max(0, bucket - 1)));
   const int rhs = kind == kBatchGemm ? nn : std::max(1, std::min(16, median_n));
-  const int S = 96;
   Context& ctx = Ctx();
+  // Enough problems to fill every SM a few times over (throughput, not the
+  // latency of one problem), within 512 MB of matrices.
+  const size_t per = sizeof(T) * static_cast<size_t>(nn) * nn;
+  const int S = static_cast<int>(std::max<size_t>(
+      96, std::min<size_t>(3 * static_cast<size_t>(ctx.num_sms), (size_t(512) << 20) / per)));
   const size_t mat = static_cast<size_t>(nn) * nn;
   T *A = nullptr, *B = nullptr, *C = nullptr;
   int* P = nullptr;
@@ -1161,6 +1375,26 @@ int Median(std::vector<int> v) {
   return v[v.size() / 2];
 }
 
+// The size that splits the batch's work in half: problems at least this
+// large hold half of it. The batch's time follows these problems, so the
+// autotuner measures at this size rather than at the median count.
+template <typename T>
+int WorkMedian(int kind, const HostBatch<T>& bt) {
+  std::vector<std::pair<int, double>> w(bt.count);
+  double total = 0.0;
+  for (int i = 0; i < bt.count; ++i) {
+    w[i] = {bt.m[i], WorkOf(kind, bt, i)};
+    total += w[i].second;
+  }
+  std::sort(w.begin(), w.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  double acc = 0.0;
+  for (const auto& e : w) {
+    acc += e.second;
+    if (acc >= 0.5 * total) return e.first;
+  }
+  return w.empty() ? 0 : w.back().first;
+}
+
 }  // namespace
 }  // namespace hb
 
@@ -1172,7 +1406,7 @@ namespace {
 template <typename T>
 void RunBatch(int kind, const HostBatch<T>& bt, int* info_out, const char* name) {
   if (bt.count == 0) return;
-  const int config = TunedConfig<T>(kind, Median(bt.m), bt.n.empty() ? 0 : Median(bt.n));
+  const int config = TunedConfig<T>(kind, WorkMedian(kind, bt), bt.n.empty() ? 0 : Median(bt.n));
   int* dev_info = nullptr;
   if (!LaunchBatch(kind, bt, config, &dev_info, true)) return;
   LaunchFailed(name);

@@ -735,8 +735,10 @@ HWYBLAS_API int hwyblas_set_mixed_slices(int slices);
 
 /* Test hook of the batched routines: forces the launch configuration that
  * the autotuner would otherwise choose per routine, type and size bucket
- * (64, 128 or 256 threads per CTA; for hwyblas_dgemm_batched also 1001, the
- * FP64 tensor-pipe kernel with 32 x 32 tiles, or 1002, with 64 x 64 tiles).
+ * (64, 128 or 256 threads per CTA of the register-tiled FMA kernels; 1128,
+ * 128 threads with six CTAs an SM, for the LU, solve and TRSM; in FP64 also
+ * 1001 and 1002, whose products run on the tensor pipe in 32 x 32 and
+ * 64 x 64 tiles).
  * A configuration that the routine does not have is ignored; 0 restores the
  * autotuner. Results do not depend on the configuration. Returns the
  * previous setting. No counterpart in the reference. */

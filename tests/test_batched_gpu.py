@@ -249,3 +249,119 @@ def test_batched_repeated_shape_replays(hb, cuda):
             assert hb.dgetrf(n, n, a1, n, p1) == info[i]
             assert same_bits(mats[i].cpu().numpy(), a1.cpu().numpy()), (rep, i)
             assert np.array_equal(pivs[i].cpu().numpy(), p1.cpu().numpy())
+
+
+@pytest.mark.parametrize("config", [64, 128, 256, 1128, 1001, 1002])
+def test_lu_batched_every_config_matches_single(hb, cuda, config):
+    """The batched LU, its solve and TRSM under each launch configuration:
+    with 1001 and 1002 their trailing updates and TRSM products run on the
+    FP64 tensor pipe (32 x 32 and 64 x 64 tiles) and every problem must still
+    come out as the single routines give it."""
+    torch = cuda
+    rng = np.random.default_rng(config)
+    ns = [1, 16, 17, 33, 64, 65, 100, 129, 200, 300, 512]
+    nrhs = [1, 3, 16, 5, 33, 2, 40, 7, 16, 64, 20]
+    _, mats = carve(torch, [n * n for n in ns], torch.float64)
+    _, pivs = carve(torch, ns, torch.int32)
+    _, rhs = carve(torch, [n * r for n, r in zip(ns, nrhs)], torch.float64)
+    host = [rng.uniform(-1, 1, n * n) for n in ns]
+    for i, n in enumerate(ns):
+        mats[i].copy_(torch.from_numpy(host[i]))
+        rhs[i].copy_(torch.from_numpy(rng.uniform(-1, 1, n * nrhs[i])))
+    b0 = [r.clone() for r in rhs]
+    torch.cuda.synchronize()
+    lib = hb.lib()
+    prev = lib.hwyblas_batched_set_config(config)
+    try:
+        info = hb.getrf_batched(ns, mats, ns, pivs)
+        for trans in ("N", "T"):
+            for i in range(len(ns)):
+                rhs[i].copy_(b0[i])
+            torch.cuda.synchronize()
+            assert hb.getrs_batched(trans, ns, nrhs, mats, ns, pivs, rhs, ns) == 0
+            for i, n in enumerate(ns):
+                x = b0[i].clone()
+                torch.cuda.synchronize()
+                hb.dgetrs(trans, n, nrhs[i], mats[i], n, pivs[i], x, n)
+                got, want = rhs[i].cpu().numpy(), x.cpu().numpy()
+                assert same_bits(got, want), (config, trans, i, n, first_diff(got, want))
+        for side, uplo, tr, diag in (("L", "L", "N", "U"), ("R", "U", "T", "N")):
+            tri = [m.clone() for m in mats]
+            for i in range(len(ns)):
+                rhs[i].copy_(b0[i])
+            torch.cuda.synchronize()
+            mm = ns if side == "L" else nrhs
+            nn = nrhs if side == "L" else ns
+            # B is n x nrhs (left) or nrhs x n (right), both stored in rhs[i].
+            hb.trsm_batched(side, uplo, tr, diag, mm, nn, 0.5, tri, ns, rhs, mm)
+            for i, n in enumerate(ns):
+                x = b0[i].clone()
+                torch.cuda.synchronize()
+                hb.dtrsm(side, uplo, tr, diag, mm[i], nn[i], 0.5, tri[i], n, x, mm[i])
+                got, want = rhs[i].cpu().numpy(), x.cpu().numpy()
+                assert same_bits(got, want), (config, side, i, n, first_diff(got, want))
+    finally:
+        lib.hwyblas_batched_set_config(prev)
+    for i, n in enumerate(ns):
+        a1 = torch.from_numpy(host[i]).cuda()
+        p1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        assert hb.dgetrf(n, n, a1, n, p1) == info[i]
+        assert same_bits(mats[i].cpu().numpy(), a1.cpu().numpy()), (config, i, n)
+        assert np.array_equal(pivs[i].cpu().numpy(), p1.cpu().numpy())
+
+
+@pytest.mark.parametrize("config", [64, 128, 256, 1128])
+def test_single_precision_batched_every_config(hb, orc, cuda, config):
+    """FP32 under each register-tiled configuration: the LU against the
+    oracle's sgetrf, the solve against sgetrs and the GEMM against sgemm,
+    bit for bit (chains restarted every 384 in single precision)."""
+    torch = cuda
+    rng = np.random.default_rng(100 + config)
+    ns = [1, 16, 17, 64, 65, 130, 257, 400]
+    nrhs = [2, 16, 1, 64, 3, 17, 9, 40]
+    _, mats = carve(torch, [n * n for n in ns], torch.float32)
+    _, pivs = carve(torch, ns, torch.int32)
+    _, rhs = carve(torch, [n * r for n, r in zip(ns, nrhs)], torch.float32)
+    host = [rng.uniform(-1, 1, n * n).astype(np.float32) for n in ns]
+    for i, n in enumerate(ns):
+        mats[i].copy_(torch.from_numpy(host[i]))
+        rhs[i].copy_(torch.from_numpy(rng.uniform(-1, 1, n * nrhs[i]).astype(np.float32)))
+    b0 = [r.clone() for r in rhs]
+    dims = [(16, 16, 7), (64, 70, 384), (65, 33, 385), (200, 130, 800), (17, 300, 50)]
+    m = [d[0] for d in dims]
+    n = [d[1] for d in dims]
+    k = [d[2] for d in dims]
+    _, A = carve(torch, [mm * kk for mm, kk in zip(m, k)], torch.float32)
+    _, B = carve(torch, [kk * nn for kk, nn in zip(k, n)], torch.float32)
+    _, C = carve(torch, [mm * nn for mm, nn in zip(m, n)], torch.float32)
+    for v in A + B + C:
+        v.copy_(torch.from_numpy(rng.uniform(-1, 1, v.numel()).astype(np.float32)))
+    C0 = [v.clone() for v in C]
+    torch.cuda.synchronize()
+    lib = hb.lib()
+    prev = lib.hwyblas_batched_set_config(config)
+    try:
+        info = hb.getrf_batched(ns, mats, ns, pivs, precision="s")
+        assert hb.getrs_batched("N", ns, nrhs, mats, ns, pivs, rhs, ns, precision="s") == 0
+        hb.gemm_batched("N", "N", m, n, k, 1.25, A, m, B, k, 0.5, C, m, precision="s")
+    finally:
+        lib.hwyblas_batched_set_config(prev)
+    for i, nn in enumerate(ns):
+        a = np.asfortranarray(host[i].reshape(nn, nn).T)
+        p = np.zeros(nn, np.int32)
+        assert orc.sgetrf(nn, nn, a, nn, p) == info[i]
+        got = mats[i].cpu().numpy().reshape(nn, nn).T
+        assert np.array_equal(pivs[i].cpu().numpy(), p), (config, i, nn)
+        assert same_bits(got, a), (config, i, nn, first_diff(got, a))
+        x = b0[i].clone()
+        torch.cuda.synchronize()
+        hb.sgetrs("N", nn, nrhs[i], mats[i], nn, pivs[i], x, nn)
+        got, want = rhs[i].cpu().numpy(), x.cpu().numpy()
+        assert same_bits(got, want), (config, i, nn, first_diff(got, want))
+    for i in range(len(dims)):
+        c1 = C0[i].clone()
+        torch.cuda.synchronize()
+        hb.sgemm("N", "N", m[i], n[i], k[i], 1.25, A[i], m[i], B[i], k[i], 0.5, c1, m[i])
+        got, want = C[i].cpu().numpy(), c1.cpu().numpy()
+        assert same_bits(got, want), (config, i, dims[i], first_diff(got, want))
