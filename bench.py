@@ -85,12 +85,12 @@ def parse():
                    help="with --case: per-kernel device time of the call (CUPTI activity "
                         "records through torch.profiler)")
     p.add_argument("--case", default=None,
-                   choices=["leaf", "getrf", "gesv", "gesv-mixed", "trtri", "getri", "trmm",
-                            "zgemm", "zgetrf", "zpotrf"],
+                   choices=["leaf", "getrf", "gesv", "gesv-mixed", "potrf", "posv-mixed",
+                            "trtri", "getri", "trmm", "zgemm", "zgetrf", "zpotrf"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
-                        "leaf on a gesv-n x 16 panel, plain dgetrf, or mixed dgesv at "
-                        "gesv-n; dtrtri, dgetri, dtrmm or zgemm at n; each after one "
-                        "warm-up call")
+                        "leaf on a gesv-n x 16 panel, plain dgetrf / dgesv / dpotrf, or "
+                        "mixed dgesv / dposv at gesv-n; dtrtri, dgetri, dtrmm, zgemm, "
+                        "zgetrf or zpotrf at n; each after one warm-up call")
     return p.parse_args()
 
 
@@ -1144,6 +1144,18 @@ def run_case(args):
     elif args.case == "leaf":
         a0 = torch.rand(n * 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         call = lambda a: hb.dgetrf2(n, 16, a, n, ipiv)
+    elif args.case in ("potrf", "posv-mixed"):
+        # SPD A = G G^T / n + 1e-3 I, G Gaussian (the dposv configuration).
+        gm = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+        a0 = torch.addmm(torch.eye(n, dtype=torch.float64, device="cuda"), gm, gm.T,
+                         beta=1e-3, alpha=1.0 / n).contiguous().view(-1)
+        del gm
+        b = torch.rand(n * args.nrhs, dtype=torch.float64, device="cuda", generator=g)
+        x = torch.zeros_like(b)
+        if args.case == "potrf":
+            call = lambda a: hb.dpotrf("L", n, a, n)
+        else:
+            call = lambda a: hb.dposv_mixed("L", n, args.nrhs, a, n, b, n, x, n)
     else:
         a0 = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         b = torch.rand(n * args.nrhs, dtype=torch.float64, device="cuda", generator=g)

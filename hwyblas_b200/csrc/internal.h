@@ -242,6 +242,11 @@ void PotrfPanel(bool upper, int n, double* a, int lda, int* info, int col0);
 // right-looking over leaf-wide sub-panels, not the reference's recursion;
 // pivots relative to the panel's first row; *info set at the first zero pivot.
 void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col0);
+// Lower Cholesky of an n x n diagonal block for the mixed solver
+// (mixed_panel.cu): right-looking over 32-column sub-panels; the upper
+// triangle is scratch; *info as PotrfPanel sets it; `arrivals` is one device
+// word of scratch for this stream.
+void CholBlock(int n, double* a, int lda, int* info, int col0, unsigned int* arrivals);
 template <typename T>
 void Potrf2(bool upper, int n, T* a, int lda, int* info);
 template <typename T>

@@ -19,10 +19,11 @@
 // cond(A) eps.
 //
 // Factorization (right-looking, block nb):
-//   LU        panel (pivot search and diagonal block) in FP64 by the
-//             recursive LU, U12 by an FP64 triangular solve, and the
-//             trailing update A22 -= L21 U12 as an Ozaki GEMM with few INT8
-//             slices on tcgen05 (integer-exact products, FP64 recombination).
+//   LU        panel (pivot search, diagonal block, in-panel updates) in
+//             FP64; the inverse of the panel's unit L11 in FP64; then
+//             U12 = L11^-1 A12 and the trailing update A22 -= L21 U12 as
+//             Ozaki GEMMs with few INT8 slices on tcgen05 (integer-exact
+//             products, FP64 recombination).
 //   Cholesky  diagonal block factored and inverted in FP64, L21 = A21 L11^-T
 //             and A22 -= L21 L21^T (lower triangle) as Ozaki GEMMs.
 // The factors stay in FP64 storage; their accuracy is that of the slices
@@ -728,7 +729,7 @@ struct MixedBuffers {
   double* part = nullptr;   // residual and norm partial sums
   int* perm = nullptr;      // LU row permutation
   unsigned long long* norms = nullptr;  // [0] ||A||, then ||x||, ||r|| columns
-  unsigned int* barrier = nullptr;
+  unsigned int* barrier = nullptr;  // [0]: grid barrier; [32]: Cholesky arrivals
   unsigned int* flags = nullptr;  // per-position ready flags of the chained solve
   size_t flag_stride = 0;         // flags of a second, concurrent chained solve
 };
@@ -1182,7 +1183,7 @@ void MixedPotrf(int n, double* w, long long ldw, int* info, int slices, MixedBuf
   // Diagonal block at j (jb columns): FP64 factor and inverse, then the
   // block column below it, rows [j + jb, n).
   const auto panel = [&](int j, int jb) {
-    PotrfPanel(false, jb, At(w, ldw, j, j), lw, info, j);
+    CholBlock(jb, At(w, ldw, j, j), lw, info, j, bf.barrier + 32);
     const int below = n - j - jb;
     if (below <= 0) return;
     InvertDiagBlocks(jb, At(w, ldw, j, j), ldw, true, false, bf.inv_lo);

@@ -118,14 +118,17 @@ __global__ void __launch_bounds__(256)
 constexpr int kRkM = 128, kRkN = 32, kRkK = 32;
 constexpr int kRkLda = kRkM + 4;  // conflict-free A fragments
 constexpr int kRkLdb = kRkK + 4;  // conflict-free B fragments
+// With lower_only, tiles wholly above C's diagonal are skipped.
 __global__ void __launch_bounds__(256)
     PanelRankUpdateKernel(int m, int n, int kw, const double* a, long long lda,
-                          const double* b, long long ldb, double* c, long long ldc) {
+                          const double* b, long long ldb, double* c, long long ldc,
+                          bool lower_only) {
   __shared__ __align__(16) double sa[kRkK * kRkLda];  // sa[k * kRkLda + row] = -A
   __shared__ __align__(16) double sb[kRkN * kRkLdb];  // sb[col * kRkLdb + k] = B
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int g = lane >> 2, t = lane & 3;
   const int r0 = blockIdx.x * kRkM, c0 = blockIdx.y * kRkN;
+  if (lower_only && c0 >= r0 + kRkM) return;
   for (int idx = tid; idx < kRkK * kRkM; idx += 256) {
     const int k = idx / kRkM, r = idx % kRkM;
     sa[k * kRkLda + r] = (k < kw && r0 + r < m) ? -a[r0 + r + k * lda] : 0.0;
@@ -174,6 +177,101 @@ __global__ void __launch_bounds__(256)
       const int rr = row + (e >> 1) * 8, cc = col + (e & 1);
       if (rr < m && cc < n) c[rr + cc * ldc] = d[j][e];
     }
+  }
+}
+
+// Cholesky of one 32-column sub-panel of a diagonal block (the mixed
+// dposv's FP64 diagonal blocks; a stable Cholesky is all that is needed, not
+// the reference's recursive order). The sub-panel is m rows x w columns
+// (w <= 32) at a, its top w x w block on the diagonal. Every CTA factors
+// that block in shared memory (one warp, right-looking), then solves its 128
+// rows below it, X L11^T = A21, one row per thread with the row in
+// registers. It stores L21 in place and, transposed, into the strip to the
+// right of the diagonal block (rows 0..w, columns w..m), where the rank-w
+// update reads it as its right operand. L11 overwrites the block that every
+// CTA reads first, so the last CTA to have read it (an arrival counter,
+// zero between launches) stores it: no CTA waits for another. A pivot that
+// is not positive records INFO (global column col0 + j + 1, the first one
+// only) and is replaced by 1 so that what follows stays finite; kernels see
+// a recorded INFO and do nothing.
+constexpr int kChRows = 128;
+__global__ void __launch_bounds__(kChRows)
+    CholSubPanelKernel(int m, int w, double* a, long long lda, int* info, int col0,
+                       unsigned int* arrivals) {
+  __shared__ double s_l[32][33];
+  __shared__ double s_x[32][kChRows + 1];
+  __shared__ int s_bad;
+  __shared__ bool s_last;
+  if (*info != 0) return;
+  const int tid = threadIdx.x, lane = tid % 32;
+  for (int idx = tid; idx < 32 * 32; idx += kChRows) {
+    const int i = idx % 32, j = idx / 32;
+    s_l[i][j] = (i < w && j <= i) ? a[i + j * lda] : 0.0;
+  }
+  if (tid == 0) s_bad = -1;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(arrivals, 1u) == gridDim.x - 1;
+    if (s_last) *arrivals = 0u;  // every CTA has arrived: reset for the next launch
+  }
+  if (tid < 32) {
+    for (int j = 0; j < w; ++j) {
+      const double d = s_l[j][j];
+      const bool ok = d > 0.0;  // false on NaN
+      const double l = ok ? sqrt(d) : 1.0;
+      if (!ok && lane == 0 && s_bad < 0) s_bad = j;
+      __syncwarp();
+      const double lij = (lane > j && lane < w) ? s_l[lane][j] / l : 0.0;
+      if (lane == j) s_l[j][j] = l;
+      if (lane > j && lane < w) s_l[lane][j] = lij;
+      __syncwarp();
+      // Trailing columns of the block: s_l[i][k] -= l_ij l_kj, j < k <= i.
+      for (int k = j + 1; k < w; ++k) {
+        const double lkj = s_l[k][j];
+        if (lane >= k && lane < w) s_l[lane][k] = fma(-lij, lkj, s_l[lane][k]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (s_last) {
+    if (tid == 0 && s_bad >= 0) *info = col0 + s_bad + 1;
+    for (int idx = tid; idx < 32 * 32; idx += kChRows) {
+      const int i = idx % 32, j = idx / 32;
+      if (i < w && j <= i) a[i + j * lda] = s_l[i][j];
+    }
+  }
+  // Rows below: x_j = (a_j - sum_{k<j} x_k l_jk) / l_jj.
+  const int r = w + static_cast<int>(blockIdx.x) * kChRows + tid;
+  if (r < m) {
+    double x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = j < w ? a[r + j * lda] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < w) {
+        double acc = x[j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) acc = fma(-x[k], s_l[j][k], acc);
+        x[j] = acc / s_l[j][j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < w) {
+        a[r + j * lda] = x[j];
+        s_x[j][tid] = x[j];
+      }
+    }
+  }
+  __syncthreads();
+  // The transposed strip: rows 0..w, columns w + blockIdx.x * 128 + i.
+  const int rows = min(kChRows, m - w - static_cast<int>(blockIdx.x) * kChRows);
+  for (int idx = tid; idx < 32 * kChRows; idx += kChRows) {
+    const int j = idx % 32, i = idx / 32;
+    if (j < w && i < rows)
+      a[j + (w + static_cast<long long>(blockIdx.x) * kChRows + i) * lda] = s_x[j][i];
   }
 }
 
@@ -727,10 +825,10 @@ PanelSide& GetPanelSide() {
 }
 
 void RankUpdate(int mr, int nr, int w, const double* l21, const double* u12, double* a22,
-                int lda, cudaStream_t st) {
+                int lda, cudaStream_t st, bool lower_only = false) {
   if (mr <= 0 || nr <= 0) return;
   PanelRankUpdateKernel<<<dim3((mr + kRkM - 1) / kRkM, (nr + kRkN - 1) / kRkN), 256, 0, st>>>(
-      mr, nr, w, l21, lda, u12, lda, a22, lda);
+      mr, nr, w, l21, lda, u12, lda, a22, lda, lower_only);
   CountLaunch();
   LaunchFailed("mixed panel update");
 }
@@ -791,6 +889,27 @@ void MixedPanel(int m, int nc, double* a, int lda, int* ipiv, int* info, int col
   PanelPivotOffsetKernel<<<(mn + 255) / 256, 256, 0, st>>>(mn, ib, ipiv);
   CountLaunch();
   LaunchFailed("mixed panel pivots");
+}
+
+// Lower Cholesky of an n x n diagonal block, right-looking over 32-column
+// sub-panels: the sub-panel kernel, then the rank-32 update of the block's
+// lower trailing part. The block's upper triangle is scratch (it receives
+// the transposed panels); *info as PotrfPanel sets it; `arrivals` is one
+// device word of scratch for this stream.
+void CholBlock(int n, double* a, int lda, int* info, int col0, unsigned int* arrivals) {
+  const cudaStream_t st = Ctx().stream;
+  cudaMemsetAsync(arrivals, 0, sizeof(unsigned int), st);
+  for (int c = 0; c < n; c += 32) {
+    const int w = std::min(32, n - c), m = n - c, below = m - w;
+    const int grid = std::max(1, (below + kChRows - 1) / kChRows);
+    CholSubPanelKernel<<<grid, kChRows, 0, st>>>(m, w, At(a, lda, c, c), lda, info,
+                                                 col0 + c, arrivals);
+    CountLaunch();
+    LaunchFailed("mixed cholesky panel");
+    if (below > 0)
+      RankUpdate(below, below, w, At(a, lda, c + w, c), At(a, lda, c, c + w),
+                 At(a, lda, c + w, c + w), lda, st, true);
+  }
 }
 
 }  // namespace hb

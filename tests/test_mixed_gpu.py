@@ -133,6 +133,24 @@ def test_dposv_mixed_accuracy(hb, orc, uplo, n, nrhs):
     assert fwd_err(x, xt) <= 4.0 * fwd_err(x2, xt) + 1e-15
 
 
+@pytest.mark.parametrize("n", [4500, 8200])
+def test_dposv_mixed_many_blocks(hb, n):
+    """Several diagonal blocks of 512 / 1024 columns with a ragged last one:
+    each factored in FP64 by 32-column sub-panels, the blocks below and the
+    trailing matrix on INT8. The refined solution must be at least as
+    accurate as LAPACK's FP64 solve."""
+    rng = np.random.default_rng(n)
+    a = spd_matrix(rng, n)
+    xt = rng.uniform(-1, 1, (n, 2))
+    b = np.asfortranarray(a @ xt)
+    x = np.zeros((n, 2), order="F")
+    info, it = hb.dposv_mixed("L", n, 2, a.copy(order="F"), n, b, n, x, n)
+    assert info == 0 and 1 <= it <= 10, (info, it)
+    check_backward(a, x, b, n)
+    ref = np.linalg.solve(a, b)
+    assert fwd_err(x, xt) <= fwd_err(ref, xt) + 1e-15, (fwd_err(x, xt), fwd_err(ref, xt))
+
+
 @pytest.mark.parametrize("slices", [3, 4, 5])
 def test_dgesv_mixed_slice_counts(hb, slices):
     n = 500
