@@ -526,20 +526,6 @@ struct ChainCursor {
   }
 };
 
-__device__ __forceinline__ void CpAsync16(double* dst, const double* src, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
-               :
-               : "r"(SmemAddr(dst)), "l"(src), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void CpAsyncCommit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void CpAsyncWait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // One m16n8k8 FP64 product chain over k = 0..63: d += A(16 x 64) B(64 x 8),
 // A column-major with stride kChainLd starting at row `row`, B stored by
 // column (b[col * kChainLd + k]).

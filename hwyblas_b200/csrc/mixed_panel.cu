@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(256)
 // dposv's FP64 diagonal blocks; a stable Cholesky is all that is needed, not
 // the reference's recursive order). The sub-panel is m rows x w columns
 // (w <= 32) at a, its top w x w block on the diagonal. Every CTA factors
-// that block in shared memory (one warp, right-looking), then solves its 128
+// that block in registers (one warp, left-looking), then solves its 128
 // rows below it, X L11^T = A21, one row per thread with the row in
 // registers. It stores L21 in place and, transposed, into the strip to the
 // right of the diagonal block (rows 0..w, columns w..m), where the rank-w
@@ -200,6 +200,7 @@ __global__ void __launch_bounds__(kChRows)
                        unsigned int* arrivals) {
   __shared__ double s_l[32][33];
   __shared__ double s_x[32][kChRows + 1];
+  __shared__ double s_rinv[32];
   __shared__ int s_bad;
   __shared__ bool s_last;
   if (*info != 0) return;
@@ -208,7 +209,6 @@ __global__ void __launch_bounds__(kChRows)
     const int i = idx % 32, j = idx / 32;
     s_l[i][j] = (i < w && j <= i) ? a[i + j * lda] : 0.0;
   }
-  if (tid == 0) s_bad = -1;
   __syncthreads();
   if (tid == 0) {
     __threadfence();
@@ -216,23 +216,32 @@ __global__ void __launch_bounds__(kChRows)
     if (s_last) *arrivals = 0u;  // every CTA has arrived: reset for the next launch
   }
   if (tid < 32) {
-    for (int j = 0; j < w; ++j) {
-      const double d = s_l[j][j];
-      const bool ok = d > 0.0;  // false on NaN
-      const double l = ok ? sqrt(d) : 1.0;
-      if (!ok && lane == 0 && s_bad < 0) s_bad = j;
-      __syncwarp();
-      const double lij = (lane > j && lane < w) ? s_l[lane][j] / l : 0.0;
-      if (lane == j) s_l[j][j] = l;
-      if (lane > j && lane < w) s_l[lane][j] = lij;
-      __syncwarp();
-      // Trailing columns of the block: s_l[i][k] -= l_ij l_kj, j < k <= i.
-      for (int k = j + 1; k < w; ++k) {
-        const double lkj = s_l[k][j];
-        if (lane >= k && lane < w) s_l[lane][k] = fma(-lij, lkj, s_l[lane][k]);
+    // Warp 0, lane i holding row i in registers; left-looking:
+    // l_ij = (a_ij - sum_{k<j} l_ik l_jk) / l_jj, row j's entries by shuffle.
+    double row[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) row[k] = s_l[lane][k];
+    int bad = -1;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < w) {
+        double acc = row[j];
+#pragma unroll
+        for (int k = 0; k < j; ++k)
+          acc = fma(-row[k], __shfl_sync(0xffffffffu, row[k], j), acc);
+        const double d = __shfl_sync(0xffffffffu, acc, j);
+        const bool ok = d > 0.0;  // false on NaN
+        if (!ok && bad < 0) bad = j;
+        const double l = ok ? sqrt(d) : 1.0;
+        if (lane == j) row[j] = l;
+        else if (lane > j) row[j] = acc / l;
       }
-      __syncwarp();
     }
+#pragma unroll
+    for (int k = 0; k < 32; ++k) s_l[lane][k] = (lane < w && k <= lane) ? row[k] : 0.0;
+    __syncwarp();
+    if (lane < w) s_rinv[lane] = 1.0 / s_l[lane][lane];
+    if (lane == 0) s_bad = bad;
   }
   __syncthreads();
   if (s_last) {
@@ -254,7 +263,7 @@ __global__ void __launch_bounds__(kChRows)
         double acc = x[j];
 #pragma unroll
         for (int k = 0; k < j; ++k) acc = fma(-x[k], s_l[j][k], acc);
-        x[j] = acc / s_l[j][j];
+        x[j] = acc * s_rinv[j];
       }
     }
 #pragma unroll

@@ -51,6 +51,30 @@ def test_dgemm_alpha_beta_special(hb, orc, alpha, beta, k):
     run_gemm(hb, orc, "N", "T", 37, 23, k, alpha, beta, pad=2, seed=1000 + k)
 
 
+@pytest.mark.parametrize("m,n,k,pad,alpha,beta", [
+    (2000, 1500, 64, 0, -1.0, 1.0),   # the LU's trailing update
+    (1999, 1501, 33, 1, 1.5, 0.5),    # ragged tiles, odd k
+    (4097, 1100, 1, 1, 0.7, -0.3),
+    (1000, 4160, 64, 2, 1.0, 0.0),    # beta 0: C not read (poisoned)
+    (640, 700, 17, 0, 0.0, 1.0),
+    (3001, 2500, 64, 0, -1.0, 1.0),   # odd leading dimension: the tile kernel
+])
+def test_dgemm_short_k(hb, orc, m, n, k, pad, alpha, beta):
+    """k <= 64 (one reference chunk) on the short-product kernel: persistent
+    CTAs over 64 x 64 tiles with the next tile's operands prefetched; the
+    same chains and merges as the reference."""
+    run_gemm(hb, orc, "N", "N", m, n, k, alpha, beta, pad=pad, seed=m + n + k)
+
+
+def test_dgemm_short_k_special_values(hb, orc):
+    def special(a, b, c):
+        a[5, 3] = np.inf
+        b[3, 40] = np.nan
+        c[100, 7] = -np.inf
+        a[70, 0] = -0.0
+    run_gemm(hb, orc, "N", "N", 1500, 1200, 64, -1.0, 1.0, seed=9, special=special)
+
+
 def test_dgemm_config_1024(hb, orc):
     """M=N=K=1024 NN, alpha=1.5, beta=0.5 (the reference-runnable config)."""
     run_gemm(hb, orc, "N", "N", 1024, 1024, 1024, 1.5, 0.5, seed=1)
