@@ -577,11 +577,15 @@ __global__ void __launch_bounds__(256) DgemmSplitMergeKernel(GemmParams p) {
 // 12 for the tile kernel; every variant gave the same bits.) Operand rows
 // are padded to 68 doubles and C's to 66, which makes every fragment and
 // accumulator access conflict free. Canonical operands only (column-major,
-// 16-byte aligned base and leading dimension), full C, no triangular operand.
+// 16-byte aligned base and leading dimension), no triangular operand; a
+// triangular C part (SYRK) skips the tiles outside it and merges with the
+// reference's crossing-tile rule.
 constexpr int kSkM = 64, kSkN = 32, kSkK = 64;
 constexpr int kSkLdAB = kSkK + 4;   // shared row stride of A and B (doubles)
+constexpr int kSkLdBt = kSkN + 4;   // of a transposed B (k rows of 32)
 constexpr int kSkLdC = kSkM + 2;    // shared row stride of C
-constexpr int kSkSmemBytes = (kSkK * kSkLdAB + kSkN * kSkLdAB + kSkN * kSkLdC) * 8;
+constexpr int kSkSizeB = kSkK * kSkLdBt;  // >= kSkN * kSkLdAB
+constexpr int kSkSmemBytes = (kSkK * kSkLdAB + kSkSizeB + kSkN * kSkLdC) * 8;
 constexpr int kSkThreads = 128;
 constexpr int kSkPerSm = 3;
 
@@ -596,14 +600,17 @@ __device__ __forceinline__ void ShortKTile(int tile, int tiles_m, int tiles_n, i
   *n0 = (in_group / gm) * kSkN;
 }
 
+// kTA / kTB: op(A) = A^T (A(i, q) at a[q + i lda]) / op(B) = B^T; shared
+// memory keeps each operand's contiguous index contiguous.
+template <bool kTA, bool kTB, bool kPart>
 __global__ void __launch_bounds__(kSkThreads, kSkPerSm)
     DgemmShortKKernel(GemmParams p, const double* __restrict__ a, long long lda,
                       const double* __restrict__ b, long long ldb) {
   if (p.guard != nullptr && *p.guard != 0) return;
   extern __shared__ __align__(16) double sk_smem[];
-  double* sA = sk_smem;                   // sA[q][i] = A(m0 + i, q)
-  double* sB = sA + kSkK * kSkLdAB;       // sB[j][q] = B(q, n0 + j)
-  double* sC = sB + kSkN * kSkLdAB;       // sC[j][i] = C(m0 + i, n0 + j)
+  double* sA = sk_smem;                   // sA[q][i] (kTA: sA[i][q]) = op(A)(m0 + i, q)
+  double* sB = sA + kSkK * kSkLdAB;       // sB[j][q] (kTB: sB[q][j]) = op(B)(q, n0 + j)
+  double* sC = sB + kSkSizeB;             // sC[j][i] = C(m0 + i, n0 + j)
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp % 2, wn = warp / 2;  // warp tile: rows 32 wm, columns 16 wn
@@ -614,20 +621,37 @@ __global__ void __launch_bounds__(kSkThreads, kSkPerSm)
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     int m0, n0;
     ShortKTile(tile, tiles_m, tiles_n, &m0, &n0);
+    if (kPart &&
+        ((p.part == kLower && m0 + kSkM - 1 < n0) || (p.part == kUpper && m0 > n0 + kSkN - 1)))
+      continue;  // wholly outside C's part
     __syncthreads();  // the previous tile's reads are done
     // 16-byte chunks (two doubles along the contiguous index); chunks past
     // the matrices' edges read only their valid doubles and are zero-filled.
     for (int ch = tid; ch < kSkK * kSkM / 2; ch += kSkThreads) {
-      const int q = ch / (kSkM / 2), r2 = (ch % (kSkM / 2)) * 2;
-      const int rows = min(2, p.m - m0 - r2);
-      const bool ok = q < k && rows > 0;
-      CpAsync16(sA + q * kSkLdAB + r2, ok ? a + (m0 + r2) + q * lda : a, ok ? rows * 8 : 0);
+      if (!kTA) {
+        const int q = ch / (kSkM / 2), r2 = (ch % (kSkM / 2)) * 2;
+        const int rows = min(2, p.m - m0 - r2);
+        const bool ok = q < k && rows > 0;
+        CpAsync16(sA + q * kSkLdAB + r2, ok ? a + (m0 + r2) + q * lda : a, ok ? rows * 8 : 0);
+      } else {
+        const int i = ch / (kSkK / 2), q2 = (ch % (kSkK / 2)) * 2;
+        const int qs = min(2, k - q2);
+        const bool ok = m0 + i < p.m && qs > 0;
+        CpAsync16(sA + i * kSkLdAB + q2, ok ? a + q2 + (m0 + i) * lda : a, ok ? qs * 8 : 0);
+      }
     }
     for (int ch = tid; ch < kSkN * kSkK / 2; ch += kSkThreads) {
-      const int j = ch / (kSkK / 2), q2 = (ch % (kSkK / 2)) * 2;
-      const int qs = min(2, k - q2);
-      const bool ok = n0 + j < p.n && qs > 0;
-      CpAsync16(sB + j * kSkLdAB + q2, ok ? b + q2 + (n0 + j) * ldb : b, ok ? qs * 8 : 0);
+      if (!kTB) {
+        const int j = ch / (kSkK / 2), q2 = (ch % (kSkK / 2)) * 2;
+        const int qs = min(2, k - q2);
+        const bool ok = n0 + j < p.n && qs > 0;
+        CpAsync16(sB + j * kSkLdAB + q2, ok ? b + q2 + (n0 + j) * ldb : b, ok ? qs * 8 : 0);
+      } else {
+        const int q = ch / (kSkN / 2), j2 = (ch % (kSkN / 2)) * 2;
+        const int cols = min(2, p.n - n0 - j2);
+        const bool ok = q < k && cols > 0;
+        CpAsync16(sB + q * kSkLdBt + j2, ok ? b + (n0 + j2) + q * ldb : b, ok ? cols * 8 : 0);
+      }
     }
     if (read_c) {
       for (int ch = tid; ch < kSkN * kSkM / 2; ch += kSkThreads) {
@@ -653,17 +677,33 @@ __global__ void __launch_bounds__(kSkThreads, kSkPerSm)
       double af[2][4], bf[2][2];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
-        const double* pa = sA + (ks * 8 + t4) * kSkLdAB + wm * 32 + i * 16 + g;
-        af[i][0] = pa[0];
-        af[i][1] = pa[8];
-        af[i][2] = pa[4 * kSkLdAB];
-        af[i][3] = pa[4 * kSkLdAB + 8];
+        const int row = wm * 32 + i * 16 + g, q = ks * 8 + t4;
+        if (!kTA) {
+          const double* pa = sA + q * kSkLdAB + row;
+          af[i][0] = pa[0];
+          af[i][1] = pa[8];
+          af[i][2] = pa[4 * kSkLdAB];
+          af[i][3] = pa[4 * kSkLdAB + 8];
+        } else {
+          const double* pa = sA + row * kSkLdAB + q;
+          af[i][0] = pa[0];
+          af[i][1] = pa[8 * kSkLdAB];
+          af[i][2] = pa[4];
+          af[i][3] = pa[8 * kSkLdAB + 4];
+        }
       }
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const double* pb = sB + (wn * 16 + j * 8 + g) * kSkLdAB + ks * 8 + t4;
-        bf[j][0] = pb[0];
-        bf[j][1] = pb[4];
+        const int col = wn * 16 + j * 8 + g, q = ks * 8 + t4;
+        if (!kTB) {
+          const double* pb = sB + col * kSkLdAB + q;
+          bf[j][0] = pb[0];
+          bf[j][1] = pb[4];
+        } else {
+          const double* pb = sB + q * kSkLdBt + col;
+          bf[j][0] = pb[0];
+          bf[j][1] = pb[4 * kSkLdBt];
+        }
       }
 #pragma unroll
       for (int i = 0; i < 2; ++i)
@@ -686,11 +726,26 @@ __global__ void __launch_bounds__(kSkThreads, kSkPerSm)
         for (int e = 0; e < 4; ++e) {
           const int r = wm * 32 + i * 16 + g + (e >> 1) * 8;
           const int c = wn * 16 + j * 8 + 2 * t4 + (e & 1);
-          if (m0 + r < p.m && n0 + c < p.n) {
+          if (!kPart && m0 + r < p.m && n0 + c < p.n) {
             const double v = p.alpha * acc[i][j][e];
             const double cin = sC[c * kSkLdC + r];
             p.c[(m0 + r) + static_cast<long long>(n0 + c) * p.ldc] =
                 p.beta == 1.0 ? v + cin : p.beta == 0.0 ? v : fma(cin, p.beta, v);
+          } else if (kPart && InPart(p, m0 + r, n0 + c)) {
+            const double v = p.alpha * acc[i][j][e];
+            const double cin = sC[c * kSkLdC + r];
+            double cv;
+            if (p.beta == 1.0) {
+              cv = v + cin;
+            } else if (p.beta == 0.0) {
+              cv = v;
+            } else if (InCrossingTile(p.part, p.m, p.n, m0 + r, n0 + c)) {
+              const double bc = p.beta * cin;
+              cv = v + bc;
+            } else {
+              cv = fma(cin, p.beta, v);
+            }
+            p.c[(m0 + r) + static_cast<long long>(n0 + c) * p.ldc] = cv;
           }
         }
   }
@@ -946,12 +1001,21 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
       return;
     }
   }
-  if (k <= kSkK && part == kAll && tri == kTriNone && !a.trans() && !b.trans() &&
-      TmaReady(a.data, a.ld(), 8) && TmaReady(b.data, b.ld(), 8) && TmaReady(c, ldc, 8)) {
+  if (k <= kSkK && tri == kTriNone && TmaReady(a.data, a.ld(), 8) &&
+      TmaReady(b.data, b.ld(), 8) && TmaReady(c, ldc, 8)) {
     static bool sk_configured = false;
     if (!sk_configured) {
-      cudaFuncSetAttribute(reinterpret_cast<const void*>(DgemmShortKKernel),
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, kSkSmemBytes);
+      const auto set = [](const void* f) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSkSmemBytes);
+      };
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<false, false, false>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<false, true, false>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<true, false, false>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<true, true, false>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<false, false, true>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<false, true, true>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<true, false, true>));
+      set(reinterpret_cast<const void*>(DgemmShortKKernel<true, true, true>));
       sk_configured = true;
     }
     GemmParams p;
@@ -973,8 +1037,21 @@ void Dgemm(int m, int n, int k, double alpha, View<double> a, View<double> b,
     const int sms = ctx.sm_cap > 0 ? std::min(ctx.sm_cap, ctx.num_sms) : ctx.num_sms;
     const unsigned grid = static_cast<unsigned>(std::min<long long>(tiles, kSkPerSm * sms));
     cudaEvent_t t0 = KernelTimerStart(kFamilyDmmaGemm, ctx.stream);
-    DgemmShortKKernel<<<grid, kSkThreads, kSkSmemBytes, ctx.stream>>>(p, a.data, a.ld(),
-                                                                      b.data, b.ld());
+    const auto launch = [&](auto kernel) {
+      kernel<<<grid, kSkThreads, kSkSmemBytes, ctx.stream>>>(p, a.data, a.ld(), b.data, b.ld());
+    };
+    const bool ta = a.trans(), tb = b.trans();
+    if (part == kAll) {
+      if (!ta && !tb) launch(DgemmShortKKernel<false, false, false>);
+      else if (!ta) launch(DgemmShortKKernel<false, true, false>);
+      else if (!tb) launch(DgemmShortKKernel<true, false, false>);
+      else launch(DgemmShortKKernel<true, true, false>);
+    } else {
+      if (!ta && !tb) launch(DgemmShortKKernel<false, false, true>);
+      else if (!ta) launch(DgemmShortKKernel<false, true, true>);
+      else if (!tb) launch(DgemmShortKKernel<true, false, true>);
+      else launch(DgemmShortKKernel<true, true, true>);
+    }
     KernelTimerStop(t0, ctx.stream);
     CountLaunch();
     LaunchFailed("dgemm short k");
