@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -2106,15 +2107,42 @@ HWYBLAS_API hwyblas_int hwyblas_dgemm_emulated(
   }
   if (!sc.In(c, ldc, m, n, hb::kWsStageC, beta != 0.0)) return -1;
   int used = 0;
+  long long copied = 0;  // columns of a host C already queued back
   if (!compute) {
     hb::ScaleMatrix<double>(m, n, beta, sc.dev, sc.ld, hb::kAll);
   } else {
+    // A host C large enough for a few waves of tiles per block goes back in
+    // column blocks on the side stream, each while the next is computed.
+    hb::SideStream& side = hb::Side();
+    int col_blocks = 1;
+    std::function<void(int, int)> done;
+    if (sc.host && side.ok) {
+      const long long tiles = static_cast<long long>((m + 127) / 128) * ((n + 127) / 128);
+      col_blocks = static_cast<int>(
+          std::min<long long>(4, tiles / (6LL * hb::Ctx().num_sms)));
+      done = [&](int n0, int nb) {
+        cudaEventRecord(side.to_side, hb::Ctx().stream);
+        cudaStreamWaitEvent(side.stream, side.to_side, 0);
+        if (!hb::Failed(cudaMemcpy2DAsync(c + static_cast<long long>(n0) * ldc,
+                                          sizeof(double) * ldc,
+                                          sc.dev + static_cast<long long>(n0) * sc.ld,
+                                          sizeof(double) * sc.ld, sizeof(double) * m, nb,
+                                          cudaMemcpyDeviceToHost, side.stream),
+                        "copy out"))
+          copied += nb;
+      };
+    }
     // slices == 0: chosen from the inputs' exponent spread (emulated.cu).
     used = hb::DgemmEmulated(m, n, k, alpha, hb::ColMajor<double>(sa.dev, sa.ld, ta),
                              hb::ColMajor<double>(sb.dev, sb.ld, tb), beta, sc.dev,
-                             sc.ld, slices);
+                             sc.ld, slices, true, 0, false, col_blocks,
+                             col_blocks > 1 ? &done : nullptr);
+    if (copied > 0) {
+      cudaEventRecord(side.to_main, side.stream);
+      cudaStreamWaitEvent(hb::Ctx().stream, side.to_main, 0);
+    }
   }
-  sc.Out();
+  if (copied != n) sc.Out();
   hb::Finish("DGEMM_EMULATED");
   return used;
 }

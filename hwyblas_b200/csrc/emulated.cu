@@ -37,6 +37,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <functional>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -242,6 +243,10 @@ struct OzakiParams {
   double* w;  // FP64 partial sums of the first pass (m x n, leading dim m)
   int* timeout_flag;
   int lower_only;  // skip the tiles strictly above the diagonal of C
+  // op(B)'s slice rows: slice sl of column j (of this launch's n) is row
+  // sl * b_rows + b_off + j of the slice array (a launch over a block of C's
+  // columns reads its columns of the whole array).
+  int b_rows, b_off;
 };
 
 // Tile of this CTA in groups of 16 tile rows: consecutive CTAs walk down a
@@ -331,7 +336,7 @@ __global__ void __launch_bounds__(kEThreads, 1)
         for (int sl = 0; sl < kNA; ++sl) {
           TmaLoad2d(st + sl * Cfg::kATile, &tm_a, kb * KB, sl * p.m + m0, &full[s]);
           TmaLoad2d(st + kNA * Cfg::kATile + sl * Cfg::kBTile, &tm_b, kb * KB,
-                    sl * p.n + n0, &full[s]);
+                    sl * p.b_rows + p.b_off + n0, &full[s]);
         }
       }
     }
@@ -743,7 +748,8 @@ int OzakiMaxK(int S) { return static_cast<int>((2147483647LL / (S * 16384LL)) / 
 // inputs were not finite, or slices == 0 found no S <= 8 as accurate as it).
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite, int ws_set, bool lower_only) {
+                  bool check_finite, int ws_set, bool lower_only, int col_blocks,
+                  const std::function<void(int, int)>* block_done) {
   const int ws_emul = ws_set ? kWsEmul2 : kWsEmul;
   const int ws_acc = ws_set ? kWsEmulAcc2 : kWsEmulAcc;
   const int ws_w = ws_set ? kWsEmulW2 : kWsEmulW;
@@ -829,6 +835,49 @@ int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                 : nullptr;
   p.timeout_flag = ctx.dev_status;
   p.lower_only = lower_only ? 1 : 0;
+  p.b_rows = n;
+  p.b_off = 0;
+  // Column blocks (one k chunk, a full C): the products run block by block
+  // and block_done(first column, columns) is called as each block's
+  // launches are queued, so that the caller can move the block while the
+  // next one is computed. Each element's arithmetic is the same as unblocked.
+  const int blocks =
+      (col_blocks > 1 && block_done != nullptr && kchunk == k && !lower_only) ? col_blocks : 1;
+  if (blocks > 1) {
+    SplitDispatch(S, a, m, k, row_exp, slices_a, kp, st);
+    SplitDispatch(S, bt, n, k, col_exp, slices_b, kp, st);
+    PassMaps single, high, low;
+    bool ok;
+    if (S <= 4) {
+      ok = MakePassMaps(&single, slices_a, slices_b, k, m, n, S, kp, KbSingle(S));
+    } else {
+      ok = MakePassMaps(&high, slices_a, slices_b, k, m, n, S, kp, kKbHigh) &&
+           MakePassMaps(&low, slices_a, slices_b, k, m, n, S, kp, kKbLow);
+    }
+    if (!ok) {
+      Failed(cudaErrorInvalidValue, "ozaki tensor map");
+      return -1;
+    }
+    p.k = k;
+    p.beta = beta;
+    // Block widths: multiples of the tile width, as even as possible.
+    const int tiles_n = (n + kEBN - 1) / kEBN;
+    for (int blk = 0, t0 = 0; blk < blocks; ++blk) {
+      const int t1 = static_cast<int>(static_cast<long long>(tiles_n) * (blk + 1) / blocks);
+      const int n0 = t0 * kEBN, nb = std::min(n, t1 * kEBN) - n0;
+      t0 = t1;
+      if (nb <= 0) continue;
+      OzakiParams q = p;
+      q.n = nb;
+      q.col_exp = col_exp + n0;
+      q.c = c + static_cast<long long>(n0) * ldc;
+      q.w = p.w ? p.w + static_cast<long long>(n0) * m : nullptr;
+      q.b_off = n0;
+      if (!GemmDispatch(S, single, high, low, q, st)) return -1;
+      (*block_done)(n0, nb);
+    }
+    return S;
+  }
   for (int k0 = 0; k0 < k; k0 += kchunk) {
     const int kc = std::min(kchunk, k - k0);
     SplitDispatch(S, a.sub(0, k0), m, kc, row_exp, slices_a, kp, st);

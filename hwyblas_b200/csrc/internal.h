@@ -9,6 +9,7 @@
 
 #include <atomic>
 #include <cstddef>
+#include <functional>
 #include <cstdint>
 
 namespace hb {
@@ -339,9 +340,15 @@ void GemmFull(bool ta, bool tb, int m, int n, int k, T alpha, const T* a,
 // slots, for a call that runs concurrently with another one on a second
 // stream. lower_only: only C's lower triangle is wanted (tiles of C strictly
 // above its diagonal are skipped; the diagonal tiles are computed whole).
+// col_blocks > 1 with block_done (a full C and k within one chunk): the
+// products run in that many column blocks of C and block_done(first column,
+// columns) is called on the host as each block's launches are queued on the
+// stream, e.g. to queue that block's copy to the host.
 int DgemmEmulated(int m, int n, int k, double alpha, View<double> a,
                   View<double> b, double beta, double* c, int ldc, int slices,
-                  bool check_finite = true, int ws_set = 0, bool lower_only = false);
+                  bool check_finite = true, int ws_set = 0, bool lower_only = false,
+                  int col_blocks = 1,
+                  const std::function<void(int, int)>* block_done = nullptr);
 int OzakiMaxK(int S);
 // out(:, jj) = op(A) op(B)(:, cols[jj]) in double-double (error reference).
 void DgemmDoubleDouble(int m, int ncols, int k, View<double> a, View<double> b,

@@ -272,3 +272,25 @@ def test_auto_slices_too_wide_runs_plain(hb):
     assert hb.dgemm_emulated("N", "N", m, n, k, 1.5, a, m, b, k, 0.5, c1, m, 0) == 0
     hb.dgemm("N", "N", m, n, k, 1.5, a, m, b, k, 0.5, c2, m)
     assert same_bits(c1, c2)
+
+
+@pytest.mark.parametrize("slices,beta", [(0, 0.0), (5, 0.5), (8, 1.0)])
+def test_host_c_column_blocks_match_device(hb, cuda, slices, beta):
+    """A large host C goes back to the host in column blocks while the next
+    block is computed; every element must equal the device-pointer call's
+    (same slices, same products), including a ragged last block."""
+    torch = cuda
+    rng = np.random.default_rng(slices + 7)
+    m, n, k = 6000, 6150, 512
+    a = np.asfortranarray(rng.uniform(-1, 1, (m, k)) * np.exp2(rng.integers(-8, 9, (m, k))))
+    b = np.asfortranarray(rng.uniform(-1, 1, (k, n)) * np.exp2(rng.integers(-8, 9, (k, n))))
+    c0 = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    c_host = c0.copy(order="F")
+    used_h = hb.dgemm_emulated("N", "N", m, n, k, 1.25, a, m, b, k, beta, c_host, m, slices)
+    da = torch.from_numpy(a.T.copy()).cuda()  # column-major m x k as a k x m row-major block
+    db = torch.from_numpy(b.T.copy()).cuda()
+    dc = torch.from_numpy(c0.T.copy()).cuda()
+    torch.cuda.synchronize()
+    used_d = hb.dgemm_emulated("N", "N", m, n, k, 1.25, da, m, db, k, beta, dc, m, slices)
+    assert used_h == used_d > 0
+    assert same_bits(c_host, dc.cpu().numpy().T)
