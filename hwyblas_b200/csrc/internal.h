@@ -122,7 +122,8 @@ enum WorkspaceSlot : int {
   kWsZFactorB = 31,    // aligned copy of the right-hand sides of its solve
   kWsResidual = 32,    // hwyblas_dresidual_dd partial sums
   kWsMixedInv = 33,    // mixed Cholesky: the inverse of a diagonal block
-  kNumWorkspaceSlots = 34
+  kWsTrsmBarrier = 34, // cooperative TRSM: its grid barrier counter
+  kNumWorkspaceSlots = 35
 };
 
 // Makes `to` wait for the work enqueued on `from` so far.

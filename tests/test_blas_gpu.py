@@ -221,6 +221,36 @@ def test_dtrsm_bitexact(hb, orc, side, uplo, trans, diag, m):
         assert not np.isnan(x1[:m]).any()
 
 
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+@pytest.mark.parametrize("r,few", [(64, 1), (500, 3), (512, 16), (1100, 2), (613, 16),
+                                   (700, 40), (512, 64)])
+def test_dtrsm_few_rhs_cooperative(hb, orc, side, uplo, trans, diag, r, few):
+    """Few right-hand sides (at most 64): each subtree of at most 512 rows of
+    the recursion runs in one cooperative launch (base solves and updates
+    with grid barriers between them; right-side updates computed
+    transposed). Bits must equal the oracle's, subtree sizes that are not
+    powers of two and problems above one subtree included."""
+    rng = np.random.default_rng(r * 31 + few + ord(side) + ord(uplo) * 3 + ord(trans) * 5)
+    m, n = (r, few) if side == "L" else (few, r)
+    ka = r
+    lda = ka + 3
+    a = rand(rng, lda, ka)
+    a[:ka, :ka] = a[:ka, :ka] / ka + np.diag(1.5 + rng.uniform(0, 1, ka))
+    tri = np.tril(np.ones((ka, ka), bool)) if uplo == "L" else np.triu(np.ones((ka, ka), bool))
+    if diag == "U":
+        np.fill_diagonal(tri, False)
+    a[:ka, :ka][~tri] = np.nan
+    b = rand(rng, m + 2, n)
+    x1, x2 = b.copy(order="F"), b.copy(order="F")
+    hb.dtrsm(side, uplo, trans, diag, m, n, 1.0, a, lda, x1, m + 2)
+    orc.dtrsm(side, uplo, trans, diag, m, n, 1.0, a, lda, x2, m + 2)
+    assert same_bits(x1, x2), first_diff(x1, x2)
+    assert not np.isnan(x1[:m]).any()
+
+
 def test_dtrsm_config_4096x512(hb, orc):
     """side=L uplo=L trans=N diag=U, M=4096 N=512, U[-1,1] entries (scaled
     off-diagonal, as tests/level3_test.cc:491-494, so that X stays finite)."""

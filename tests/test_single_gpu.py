@@ -44,6 +44,25 @@ def test_strsm_bitexact(hb, orc, side, uplo, trans, diag, m):
         assert not np.isnan(x1[:m]).any()
 
 
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("r,few", [(500, 3), (900, 16)])
+def test_strsm_few_rhs_cooperative(hb, orc, side, uplo, trans, r, few):
+    """The cooperative subtree path in single precision (chains restarted
+    every 384)."""
+    rng = np.random.default_rng(r + few + ord(side) + ord(uplo) + ord(trans))
+    m, n = (r, few) if side == "L" else (few, r)
+    ka = r
+    a = rand(rng, ka, ka, np.float32)
+    a = (a / ka + np.diag(1.5 + rng.uniform(0, 1, ka))).astype(np.float32, order="F")
+    b = rand(rng, m, n, np.float32)
+    x1, x2 = b.copy(order="F"), b.copy(order="F")
+    hb.strsm(side, uplo, trans, "N", m, n, 1.0, a, ka, x1, m)
+    orc.strsm(side, uplo, trans, "N", m, n, np.float32(1.0), a, ka, x2, m)
+    assert same_bits(x1, x2), first_diff(x1, x2)
+
+
 def test_strsm_alpha_zero_and_invalid(hb):
     a = np.full(9, np.nan, np.float32)
     b = np.ones(6, np.float32)
