@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(128)
 }
 
 // Cooperative TRSM of a subtree of the recursion (at most kTcRows rows of
-// the triangle, at most kTcOther right-hand sides): all of its base solves
+// the triangle, at most TcOther right-hand sides): all of its base solves
 // and updates in one launch, in TrsmRec's order, with a bounded grid barrier
 // after each step; below that size the recursion is a chain of small
 // dependent launches. (n = 16384, one right-hand side: 22 -> 12 ms a
@@ -266,7 +266,11 @@ __global__ void __launch_bounds__(128)
 // restarted every KC and merged in order (alpha -1, beta 1), as the GEMM
 // kernels compute it. X is read and written through L2 only: its rows
 // change owner between steps.
-constexpr int kTcRows = 512, kTcOther = 64, kTcThreads = 256;
+constexpr int kTcRows = 512, kTcThreads = 256;
+// Right-hand sides of the cooperative path: up to 64 on the staged FMA
+// chains; in FP64 up to 1024, with the updates on the tensor pipe from 32.
+template <typename T>
+constexpr int TcOther() { return sizeof(T) == 8 ? 1024 : 64; }
 
 template <typename T>
 struct KcOf {
@@ -334,6 +338,87 @@ __device__ void CoopUpdate(int mm, int nn, int kk, View<T> a, View<T> bv, View<T
       __stcg(cij, cv);
     }
   }
+}
+
+// The same update on the FP64 tensor pipe for many right-hand sides: blocks
+// of 32 x 32 of C, the CTA's 8 warps one 16 x 8 tile each, k staged in
+// 64-deep chunks (A and B padded to 36 doubles a row, conflict-free
+// fragments) and each tile's m16n8k8 chain restarted every KC = 256 and
+// merged in order: every element's chain and merges are CoopUpdate's.
+constexpr int kTcDmmaB = 32, kTcDmmaKb = 64, kTcDmmaLd = kTcDmmaB + 4;
+__device__ void CoopUpdateDmma(int mm, int nn, int kk, View<double> a, View<double> bv,
+                               View<double> cv_, double* sa, double* sb) {
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = warp % 2, wc = warp / 2;  // tile rows 16 wr, columns 8 wc
+  const int rgroups = (mm + kTcDmmaB - 1) / kTcDmmaB;
+  const int items = rgroups * ((nn + kTcDmmaB - 1) / kTcDmmaB);
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int i0 = (item % rgroups) * kTcDmmaB, j0 = (item / rgroups) * kTcDmmaB;
+    // This thread's four elements (the m16n8 accumulator layout) and their C.
+    double cv[4], acc[4] = {0.0, 0.0, 0.0, 0.0};
+    bool in[4];
+    double* cp[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = i0 + wr * 16 + g + (e >> 1) * 8, j = j0 + wc * 8 + 2 * t + (e & 1);
+      in[e] = i < mm && j < nn;
+      cp[e] = const_cast<double*>(cv_.data) + i * cv_.rs + j * cv_.cs;
+      cv[e] = in[e] ? __ldcg(cp[e]) : 0.0;
+    }
+    for (int k0 = 0; k0 < kk; k0 += kTcDmmaKb) {
+      __syncthreads();  // the previous chunk's fragments are read
+      // sa[q * 36 + il] = A(i0 + il, k0 + q); sb[q * 36 + jl] = B(k0 + q, j0 + jl)
+      for (int idx = threadIdx.x; idx < kTcDmmaKb * kTcDmmaB; idx += blockDim.x) {
+        const int l = idx % kTcDmmaB, q = idx / kTcDmmaB;
+        const bool kq = k0 + q < kk;
+        sa[q * kTcDmmaLd + l] = (kq && i0 + l < mm)
+                                    ? __ldcg(a.data + (i0 + l) * a.rs + (k0 + q) * a.cs)
+                                    : 0.0;
+        sb[q * kTcDmmaLd + l] = (kq && j0 + l < nn)
+                                    ? __ldcg(bv.data + (k0 + q) * bv.rs + (j0 + l) * bv.cs)
+                                    : 0.0;
+      }
+      __syncthreads();
+      const int steps = (min(kTcDmmaKb, kk - k0) + 7) / 8;
+      for (int ks = 0; ks < steps; ++ks) {
+        const double* pa = sa + (ks * 8 + t) * kTcDmmaLd + wr * 16 + g;
+        const double* pb = sb + (ks * 8 + t) * kTcDmmaLd + wc * 8 + g;
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+            "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+            : "+d"(acc[0]), "+d"(acc[1]), "+d"(acc[2]), "+d"(acc[3])
+            : "d"(pa[0]), "d"(pa[8]), "d"(pa[4 * kTcDmmaLd]), "d"(pa[4 * kTcDmmaLd + 8]),
+              "d"(pb[0]), "d"(pb[4 * kTcDmmaLd]));
+      }
+      // End of a KC chunk (or of k): merge alpha * acc = -acc, restart.
+      if ((k0 + kTcDmmaKb) % 256 == 0 || k0 + kTcDmmaKb >= kk) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double r = -1.0 * acc[e];
+          cv[e] = r + cv[e];
+          acc[e] = 0.0;
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (in[e]) __stcg(cp[e], cv[e]);
+  }
+}
+
+// The update of a cooperative step: the tensor-pipe tiles in FP64 when the
+// right-hand sides fill them, else the staged FMA chains.
+template <typename T>
+__device__ __forceinline__ void CoopStep(int mm, int nn, int kk, View<T> a, View<T> bv,
+                                         View<T> c, T* sa, T* sb) {
+  if constexpr (sizeof(T) == 8) {
+    if (nn >= kTcDmmaB) {
+      CoopUpdateDmma(mm, nn, kk, a, bv, c, sa, sb);
+      return;
+    }
+  }
+  CoopUpdate(mm, nn, kk, a, bv, c, sa, sb);
 }
 
 template <typename T>
@@ -408,9 +493,9 @@ __global__ void __launch_bounds__(kTcThreads) TrsmCoopKernel(TrsmCoopArgs<T> p) 
         T* b1 = p.b + off;
         T* b2 = p.b + off + r1;
         if (p.lower)
-          CoopUpdate(r2, p.other, r1, toff, col(b1, p.ldb), col(b2, p.ldb), sa, sb);
+          CoopStep(r2, p.other, r1, toff, col(b1, p.ldb), col(b2, p.ldb), sa, sb);
         else
-          CoopUpdate(r1, p.other, r2, toff, col(b2, p.ldb), col(b1, p.ldb), sa, sb);
+          CoopStep(r1, p.other, r2, toff, col(b2, p.ldb), col(b1, p.ldb), sa, sb);
       } else {
         // X op(T) = B: the update C -= X_k toff, computed transposed,
         // C^T -= toff^T X_k^T (each product's factors swap, which leaves
@@ -422,9 +507,9 @@ __global__ void __launch_bounds__(kTcThreads) TrsmCoopKernel(TrsmCoopArgs<T> p) 
         tt.rs = toff.cs;
         tt.cs = toff.rs;
         if (p.lower)
-          CoopUpdate(r1, p.other, r2, tt, row(b2, p.ldb), row(b1, p.ldb), sa, sb);
+          CoopStep(r1, p.other, r2, tt, row(b2, p.ldb), row(b1, p.ldb), sa, sb);
         else
-          CoopUpdate(r2, p.other, r1, tt, row(b1, p.ldb), row(b2, p.ldb), sa, sb);
+          CoopStep(r2, p.other, r1, tt, row(b1, p.ldb), row(b2, p.ldb), sa, sb);
       }
       if (!GridBarrier(p.barrier, gridDim.x, ++gen, p.timeout_flag)) return;
     }
@@ -458,8 +543,10 @@ bool TrsmCoop(bool left, View<T> tri, bool lower, bool unit, int r, int other, T
   if (occ <= 0) return false;
   // One CTA per block of the largest update, at most one an SM (fewer CTAs
   // make cheaper barriers).
-  const int blocks = ((r - 32 + kTcRowsCta - 1) / kTcRowsCta) *
-                     ((other + kTcColsCta - 1) / kTcColsCta);
+  const int blocks =
+      (sizeof(T) == 8 && other >= kTcDmmaB)
+          ? ((r - 32 + kTcDmmaB - 1) / kTcDmmaB) * ((other + kTcDmmaB - 1) / kTcDmmaB)
+          : ((r - 32 + kTcRowsCta - 1) / kTcRowsCta) * ((other + kTcColsCta - 1) / kTcColsCta);
   const int grid = std::max(1, std::min(blocks, std::min(ctx.num_sms, ctx.num_sms * occ)));
   unsigned int* bar = static_cast<unsigned int*>(Workspace(kWsTrsmBarrier, 256));
   if (bar == nullptr) return false;
@@ -509,7 +596,7 @@ void TrsmRec(bool left, View<T> tri, bool lower, bool unit, int r, int other,
     TrsmSolve<T>(left, tri, lower, unit, r, other, b, ldb);
     return;
   }
-  if (r <= kTcRows && other <= kTcOther &&
+  if (r <= kTcRows && other <= TcOther<T>() &&
       TrsmCoop<T>(left, tri, lower, unit, r, other, b, ldb))
     return;
   const int r1 = std::max(32, (r / 2) / 32 * 32);

@@ -226,13 +226,15 @@ def test_dtrsm_bitexact(hb, orc, side, uplo, trans, diag, m):
 @pytest.mark.parametrize("trans", ["N", "T"])
 @pytest.mark.parametrize("diag", ["N", "U"])
 @pytest.mark.parametrize("r,few", [(64, 1), (500, 3), (512, 16), (1100, 2), (613, 16),
-                                   (700, 40), (512, 64)])
+                                   (700, 40), (512, 64), (500, 100), (1100, 512),
+                                   (512, 1024)])
 def test_dtrsm_few_rhs_cooperative(hb, orc, side, uplo, trans, diag, r, few):
-    """Few right-hand sides (at most 64): each subtree of at most 512 rows of
+    """Up to 1024 right-hand sides: each subtree of at most 512 rows of
     the recursion runs in one cooperative launch (base solves and updates
     with grid barriers between them; right-side updates computed
-    transposed). Bits must equal the oracle's, subtree sizes that are not
-    powers of two and problems above one subtree included."""
+    transposed; from 32 right-hand sides the updates on the FP64 tensor
+    pipe). Bits must equal the oracle's, subtree sizes that are not powers
+    of two and problems above one subtree included."""
     rng = np.random.default_rng(r * 31 + few + ord(side) + ord(uplo) * 3 + ord(trans) * 5)
     m, n = (r, few) if side == "L" else (few, r)
     ka = r
