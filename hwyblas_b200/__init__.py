@@ -22,7 +22,7 @@ __all__ = [
     "idamax_noalloc", "dgesv_mixed", "dposv_mixed", "set_mixed_slices",
     "kernel_timer", "kernel_timer_read", "KERNEL_DMMA_GEMM", "KERNEL_OZAKI_GEMM",
     "KERNEL_LU_LEAF", "getrf_batched", "getrs_batched", "gemm_batched",
-    "trsm_batched", "symm", "syr2k", "gemmtr", "trmm", "cblas_level3", "getri", "trtri", "gerfs", "zgemm", "ztrsm", "zgetrf", "zlaswp", "zgetrs", "zgesv",
+    "trsm_batched", "int_array", "ptr_array", "symm", "syr2k", "gemmtr", "trmm", "cblas_level3", "getri", "trtri", "gerfs", "zgemm", "ztrsm", "zgetrf", "zlaswp", "zgetrs", "zgesv",
     "zpotrf", "zpotrs", "zposv", "zherk",
 ]
 
@@ -51,7 +51,7 @@ from ._api import (  # noqa: E402  (needs lib())
     dgemm_emulated, dgemm_ddref, dresidual_dd, idamax_noalloc, dgesv_mixed, dposv_mixed,
     set_mixed_slices, kernel_timer, kernel_timer_read, KERNEL_DMMA_GEMM,
     KERNEL_OZAKI_GEMM, KERNEL_LU_LEAF, getrf_batched, getrs_batched, gemm_batched,
-    trsm_batched, symm, syr2k, gemmtr, trmm, cblas_level3, getri, trtri, gerfs, zgemm, ztrsm, zgetrf, zlaswp, zgetrs, zgesv,
+    trsm_batched, int_array, ptr_array, symm, syr2k, gemmtr, trmm, cblas_level3, getri, trtri, gerfs, zgemm, ztrsm, zgetrf, zlaswp, zgetrs, zgesv,
     zpotrf, zpotrs, zposv, zherk,
     CblasRowMajor, CblasColMajor, CblasNoTrans, CblasTrans, CblasConjTrans,
     CblasUpper, CblasLower, CblasNonUnit, CblasUnit, CblasLeft, CblasRight,

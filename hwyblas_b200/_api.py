@@ -392,11 +392,26 @@ def set_mixed_slices(slices):
 
 
 def _ints(vals):
+    if isinstance(vals, ctypes.Array):
+        return vals
     return (ctypes.c_int * max(1, len(vals)))(*[int(v) for v in vals])
 
 
 def _ptrs(objs):
+    if isinstance(objs, ctypes.Array):
+        return objs
     return (ctypes.c_void_p * max(1, len(objs)))(*[_ptr(o) for o in objs])
+
+
+def int_array(vals):
+    """A C int array for the batched calls (a caller repeating a batch
+    builds its arguments once, as a C caller keeps its arrays)."""
+    return _ints(list(vals))
+
+
+def ptr_array(objs):
+    """A C array of device pointers for the batched calls."""
+    return _ptrs(list(objs))
 
 
 def getrf_batched(n, a, lda, ipiv, precision="d"):
