@@ -322,6 +322,10 @@ constexpr int kLeafThreads = 512;
 constexpr int kLeafMaxRows = 1024;  // rows per CTA
 constexpr int kLeafMaxP = 64;       // CTAs per panel (m <= 65536)
 constexpr int kLeafMaxCluster = 16; // CTAs of the cluster variant (m <= 16384)
+// On the look-ahead stream, beside the capped trailing GEMM, a cluster of at
+// most this many CTAs still finds its SMs in one GPC; larger panels take
+// the cooperative variant.
+constexpr int kLeafSideCluster = 8;
 constexpr int kLeafW = 16;
 
 // Polls of the cooperative leaf's candidate exchange before a CTA gives up
@@ -803,7 +807,7 @@ void GetrfLeaf(int m, int n, T* a, int lda, int* ipiv, int* info, int info_base,
                                               slot_bytes);
   args.timeout_flag = ctx.dev_status;
   cudaEvent_t t0 = KernelTimerStart(kFamilyLuLeaf, ctx.stream);
-  if (wide || (P > 1 && P <= max_cluster && !ctx.side_leaf)) {
+  if (wide || (P > 1 && P <= max_cluster && (!ctx.side_leaf || P <= kLeafSideCluster))) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P);
     cfg.blockDim = dim3(kLeafThreads);
