@@ -536,13 +536,27 @@ def solve_to_last_bit(torch, hb, n, nrhs, A, lu, ipiv, Bm, x0):
     return x
 
 
+def backward_error(torch, Mt, X, Bm):
+    """Normwise backward error max_q ||b - A x||_inf / (||A||_inf ||x||_inf +
+    ||b||_inf) of the columns x (rows of X) against b (rows of Bm), A = Mt^T
+    given as the column-major data Mt (FP64 torch arithmetic, outside the
+    product path)."""
+    R = (Mt.t() @ X.t()).t() - Bm
+    anorm = Mt.abs().sum(dim=0).max()
+    num = R.abs().max(dim=1).values
+    den = anorm * X.abs().max(dim=1).values + Bm.abs().max(dim=1).values
+    return float((num / den).max().item())
+
+
 def run_solvers(args, torch, hb, stream):
     """dgesv and dposv at n = args.gesv_n: plain FP64 against mixed. Forward
     errors are stated against the solution of A x = b to the last bit."""
     n = args.gesv_n
     res = {"n": n, "fwd_err": "||x - x*||_F / ||x*||_F, x* = the solution of A x = b to "
                               "the last bit (the plain solution after two steps of "
-                              "extra-precise refinement)"}
+                              "extra-precise refinement)",
+           "bwd_err": "max over columns of ||b - A x||_inf / (||A||_inf ||x||_inf + "
+                      "||b||_inf)"}
     gesv_flops = lambda nrhs: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * nrhs
     ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
     cases = [(1e6, 1), (1e6, 64), (1e2, 1), (1e10, 1)]
@@ -584,6 +598,7 @@ def run_solvers(args, torch, hb, stream):
         for kind in ("plain", "mixed"):
             out[kind]["fwd_err"] = float((torch.linalg.norm(sols[kind] - xs) /
                                           torch.linalg.norm(xs)).item())
+            out[kind]["bwd_err"] = backward_error(torch, M, sols[kind], Bm)
         out["speedup"] = out["plain"]["ms"] / out["mixed"]["ms"]
         out["mixed_err_le_plain"] = bool(out["mixed"]["fwd_err"] <= out["plain"]["fwd_err"])
         res[f"dgesv_cond{cond:g}_nrhs{nrhs}"] = out
@@ -624,6 +639,7 @@ def run_solvers(args, torch, hb, stream):
     for kind in ("plain", "mixed"):
         out[kind]["fwd_err"] = float((torch.linalg.norm(sols[kind] - xs) /
                                       torch.linalg.norm(xs)).item())
+        out[kind]["bwd_err"] = backward_error(torch, S, sols[kind], Bm)
     out["speedup"] = out["plain"]["ms"] / out["mixed"]["ms"]
     out["mixed_err_le_plain"] = bool(out["mixed"]["fwd_err"] <= out["plain"]["fwd_err"])
     res["dposv_spd_nrhs1"] = out
