@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1084,8 +1085,8 @@ std::vector<int> Candidates(int kind) {
 }
 
 // Threads per CTA for a batch: the autotuner's choice for the batch's size
-// bucket (the median problem's log2 size), measured once per process on a
-// synthetic sample of that size (see Autotune below).
+// bucket (the log2 of the size that splits the batch's work in half),
+// measured once per process on a sample of the batch (TunedConfig below).
 struct TuneKey {
   int kind, bytes, bucket;
   bool operator<(const TuneKey& o) const {
@@ -1251,31 +1252,43 @@ bool LaunchBatch(int kind, const HostBatch<T>& bt, int config, int** dev_info,
   return true;
 }
 
-__global__ void FillRandomKernel(double* x, long long count, unsigned seed, double diag,
-                                 int n) {
+// Uniform values in [-1, 1) from a hash of the index.
+template <typename T>
+__global__ void FillRandomKernel(T* x, long long count, unsigned seed) {
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
        i < count; i += static_cast<long long>(gridDim.x) * blockDim.x) {
     unsigned h = static_cast<unsigned>(i) * 2654435761u ^ seed;
     h ^= h >> 15;
     h *= 2246822519u;
     h ^= h >> 13;
-    double v = (h & 0xffffff) / 8388608.0 - 1.0;
-    const long long e = i % (static_cast<long long>(n) * n);
-    if (e % (n + 1) == 0) v += diag;
-    x[i] = v;
+    x[i] = static_cast<T>((h & 0xffffff) / 8388608.0 - 1.0);
+  }
+}
+
+// Adds dim[p] to the diagonal of the dim[p] x dim[p] matrix at base + off[p]
+// (leading dimension dim[p]): a triangular factor that stays well conditioned.
+template <typename T>
+__global__ void BoostDiagonalKernel(T* base, const long long* off, const int* dim, int count) {
+  for (int p = blockIdx.x; p < count; p += gridDim.x) {
+    T* a = base + off[p];
+    const int d = dim[p];
+    for (int j = threadIdx.x; j < d; j += blockDim.x)
+      a[j + static_cast<long long>(j) * d] += static_cast<T>(d);
   }
 }
 
 // The autotuner: for (routine, type, size bucket), the launch configuration
-// (Candidates above) that runs a few waves of synthetic problems
-// of the bucket's representative size fastest (results do not depend on the
-// choice: every problem's arithmetic is the same whichever configuration
-// runs it).
+// (Candidates above) that runs a replica of the batch itself fastest: the
+// batch's own problem sizes (all of them, or every stride-th in largest-first
+// order for a batch too large to copy), on synthetic operands with tight
+// leading dimensions. Results do not depend on
+// the choice: every problem's arithmetic is the same whichever configuration
+// runs it.
 // A configuration set by hwyblas_batched_set_config (0: the autotuner's).
 std::atomic<int> g_forced_config{0};
 
 template <typename T>
-int TunedConfig(int kind, int median_m, int median_n) {
+int TunedConfig(int kind, const HostBatch<T>& real, int work_median) {
   const int forced = g_forced_config.load(std::memory_order_relaxed);
   if (forced != 0) {
     for (int c : Candidates<T>(kind))
@@ -1284,95 +1297,184 @@ int TunedConfig(int kind, int median_m, int median_n) {
   static std::mutex mu;
   static std::map<TuneKey, int> cache;
   int bucket = 0;
-  while ((2 << bucket) <= std::max(1, median_m)) ++bucket;
+  while ((2 << bucket) <= std::max(1, work_median)) ++bucket;
   const TuneKey key{kind, static_cast<int>(sizeof(T)), bucket};
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
   }
-  const int nn = std::min(512, std::max(8, 3 << std::max(0, bucket - 1)));
-  const int rhs = kind == kBatchGemm ? nn : std::max(1, std::min(16, median_n));
+  // Per-problem operand shapes with tight leading dimensions: A (rows x
+  // cols), B and C (rows x n), and the pivot vector.
+  struct Shape {
+    int m, n, k, ra, ca, rb, cb, rc, cc, piv;
+  };
+  const bool right = kind == kBatchTrsm && (real.flags & 1);
+  auto shape_of = [&](int i) {
+    Shape s{};
+    s.m = real.m[i];
+    s.n = real.n.empty() ? 0 : real.n[i];
+    s.k = real.k.empty() ? 0 : real.k[i];
+    if (kind == kBatchGemm) {
+      const bool ta = real.flags & 1, tb = real.flags & 2;
+      s.ra = ta ? s.k : s.m, s.ca = ta ? s.m : s.k;
+      s.rb = tb ? s.n : s.k, s.cb = tb ? s.k : s.n;
+      s.rc = s.m, s.cc = s.n;
+    } else {
+      const int t = right ? s.n : s.m;
+      s.ra = t, s.ca = t;
+      if (kind != kBatchGetrf) s.rb = s.m, s.cb = s.n;
+      if (kind != kBatchTrsm) s.piv = s.m;
+    }
+    return s;
+  };
+  auto round_up = [](size_t x) { return (x + 31) / 32 * 32; };  // 256-byte starts
+  std::vector<int> order(real.count);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<double> work(real.count);
+  size_t total = 0;
+  for (int i = 0; i < real.count; ++i) {
+    work[i] = WorkOf(kind, real, i);
+    const Shape s = shape_of(i);
+    total += sizeof(T) * (round_up(size_t(s.ra) * s.ca) + round_up(size_t(s.rb) * s.cb) +
+                          round_up(size_t(s.rc) * s.cc));
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return work[x] > work[y]; });
+  // The whole batch when its operands fit a quarter of the free memory (at
+  // most 16 GB): a batch's time is the larger of the throughput bound and
+  // the latency of its largest problem on one CTA, and a thinned sample
+  // shifts that balance (it keeps the largest problem but not the work
+  // around it). Beyond that, every stride-th problem.
+  size_t free_bytes = 0, total_bytes = 0;
+  if (cudaMemGetInfo(&free_bytes, &total_bytes) != cudaSuccess) free_bytes = size_t(4) << 30;
+  const size_t budget = std::max<size_t>(size_t(256) << 20,
+                                         std::min<size_t>(free_bytes / 4, size_t(16) << 30));
+  const size_t stride = std::max<size_t>(1, (total + budget - 1) / budget);
+  std::vector<Shape> sample;
+  for (size_t q = 0; q < order.size(); q += stride) sample.push_back(shape_of(order[q]));
+  const int S = static_cast<int>(sample.size());
+  std::vector<long long> off_a(S), off_b(S), off_c(S), off_p(S);
+  std::vector<int> dim_a(S);
+  size_t na = 0, nb = 0, nc = 0, np = 0;
+  for (int i = 0; i < S; ++i) {
+    const Shape& s = sample[i];
+    off_a[i] = static_cast<long long>(na), na += round_up(size_t(s.ra) * s.ca);
+    off_b[i] = static_cast<long long>(nb), nb += round_up(size_t(s.rb) * s.cb);
+    off_c[i] = static_cast<long long>(nc), nc += round_up(size_t(s.rc) * s.cc);
+    off_p[i] = static_cast<long long>(np), np += round_up(size_t(s.piv));
+    dim_a[i] = s.ra;
+  }
   Context& ctx = Ctx();
-  // Enough problems to fill every SM a few times over (throughput, not the
-  // latency of one problem), within 512 MB of matrices.
-  const size_t per = sizeof(T) * static_cast<size_t>(nn) * nn;
-  const int S = static_cast<int>(std::max<size_t>(
-      96, std::min<size_t>(3 * static_cast<size_t>(ctx.num_sms), (size_t(512) << 20) / per)));
-  const size_t mat = static_cast<size_t>(nn) * nn;
   T *A = nullptr, *B = nullptr, *C = nullptr;
   int* P = nullptr;
+  long long* d_off = nullptr;
+  int* d_dim = nullptr;
   int best = 256;
-  if (cudaMalloc(&A, sizeof(T) * mat * S) == cudaSuccess &&
-      cudaMalloc(&B, sizeof(T) * static_cast<size_t>(nn) * rhs * S) == cudaSuccess &&
-      cudaMalloc(&C, sizeof(T) * static_cast<size_t>(nn) * rhs * S) == cudaSuccess &&
-      cudaMalloc(&P, sizeof(int) * nn * S) == cudaSuccess) {
+  if (cudaMalloc(&A, sizeof(T) * std::max<size_t>(na, 1)) == cudaSuccess &&
+      cudaMalloc(&B, sizeof(T) * std::max<size_t>(nb, 1)) == cudaSuccess &&
+      cudaMalloc(&C, sizeof(T) * std::max<size_t>(nc, 1)) == cudaSuccess &&
+      cudaMalloc(&P, sizeof(int) * std::max<size_t>(np, 1)) == cudaSuccess &&
+      cudaMalloc(&d_off, sizeof(long long) * S) == cudaSuccess &&
+      cudaMalloc(&d_dim, sizeof(int) * S) == cudaSuccess) {
     HostBatch<T> bt;
     bt.count = S;
+    bt.alpha = real.alpha;
+    bt.beta = real.beta;
+    bt.flags = real.flags;
     for (int i = 0; i < S; ++i) {
-      bt.m.push_back(nn);
-      bt.n.push_back(rhs);
-      bt.k.push_back(nn);
-      bt.lda.push_back(nn);
-      bt.ldb.push_back(nn);
-      bt.ldc.push_back(nn);
-      bt.a.push_back(A + mat * i);
-      bt.b.push_back(B + static_cast<size_t>(nn) * rhs * i);
-      bt.c.push_back(C + static_cast<size_t>(nn) * rhs * i);
-      bt.ipiv.push_back(P + nn * i);
+      const Shape& s = sample[i];
+      bt.m.push_back(s.m);
+      if (!real.n.empty()) bt.n.push_back(s.n);
+      if (!real.k.empty()) bt.k.push_back(s.k);
+      bt.lda.push_back(std::max(1, s.ra));
+      bt.a.push_back(A + off_a[i]);
+      if (!real.b.empty()) {
+        bt.ldb.push_back(std::max(1, s.rb));
+        bt.b.push_back(B + off_b[i]);
+      }
+      if (!real.c.empty()) {
+        bt.ldc.push_back(std::max(1, s.rc));
+        bt.c.push_back(C + off_c[i]);
+      }
+      if (!real.ipiv.empty()) bt.ipiv.push_back(P + off_p[i]);
     }
-    bt.alpha = T(1);
-    bt.beta = T(0);
-    if (sizeof(T) == 8) {
-      FillRandomKernel<<<256, 256, 0, ctx.stream>>>(reinterpret_cast<double*>(A),
-                                                    static_cast<long long>(mat * S), 7u,
-                                                    nn, nn);
-    } else {
-      cudaMemsetAsync(A, 0, sizeof(T) * mat * S, ctx.stream);
-    }
-    cudaMemsetAsync(B, 0, sizeof(T) * static_cast<size_t>(nn) * rhs * S, ctx.stream);
-    cudaMemsetAsync(P, 0, sizeof(int) * nn * S, ctx.stream);
     if (kind == kBatchGetrs) {
       // Valid pivots for the solve: the identity.
-      std::vector<int> ident(static_cast<size_t>(nn) * S);
-      for (size_t i = 0; i < ident.size(); ++i) ident[i] = static_cast<int>(i % nn) + 1;
+      std::vector<int> ident(std::max<size_t>(np, 1), 1);
+      for (int i = 0; i < S; ++i)
+        for (int r = 0; r < sample[i].piv; ++r) ident[off_p[i] + r] = r + 1;
       cudaMemcpy(P, ident.data(), sizeof(int) * ident.size(), cudaMemcpyHostToDevice);
     }
+    // A once (the solves and products only read it; the LU refills it below).
+    FillRandomKernel<<<1024, 256, 0, ctx.stream>>>(A, static_cast<long long>(na), 7u);
+    if (kind == kBatchGetrs || kind == kBatchTrsm) {
+      cudaMemcpyAsync(d_off, off_a.data(), sizeof(long long) * S, cudaMemcpyHostToDevice,
+                      ctx.stream);
+      cudaMemcpyAsync(d_dim, dim_a.data(), sizeof(int) * S, cudaMemcpyHostToDevice,
+                      ctx.stream);
+      BoostDiagonalKernel<<<std::min(S, 4096), 256, 0, ctx.stream>>>(A, d_off, d_dim, S);
+    }
+    FillRandomKernel<<<1024, 256, 0, ctx.stream>>>(C, static_cast<long long>(nc), 11u);
+    // Fresh operands before every run: the LU and the solves work in place,
+    // and a factored matrix pivots differently from a random one.
+    auto refill = [&]() {
+      if (kind == kBatchGetrf)
+        FillRandomKernel<<<1024, 256, 0, ctx.stream>>>(A, static_cast<long long>(na), 7u);
+      if (kind != kBatchGetrf)
+        FillRandomKernel<<<1024, 256, 0, ctx.stream>>>(B, static_cast<long long>(nb), 9u);
+    };
+    const std::vector<int> configs = Candidates<T>(kind);
+    for (int config : configs) {  // untimed: first launches of every kernel
+      refill();
+      LaunchBatch(kind, bt, config, nullptr, false);
+    }
+    cudaStreamSynchronize(ctx.stream);
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int config : Candidates<T>(kind)) {
-      LaunchBatch(kind, bt, config, nullptr, false);  // warm-up
-      cudaEventRecord(e0, ctx.stream);
-      LaunchBatch(kind, bt, config, nullptr, false);
-      cudaEventRecord(e1, ctx.stream);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = config;
+    std::vector<float> times(configs.size(), 1e30f);
+    for (int rep = 0; rep < 2; ++rep) {
+      for (size_t c = 0; c < configs.size(); ++c) {
+        refill();
+        cudaEventRecord(e0, ctx.stream);
+        LaunchBatch(kind, bt, configs[c], nullptr, false);
+        cudaEventRecord(e1, ctx.stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        times[c] = std::min(times[c], ms);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = configs[c];
+        }
       }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // HWYBLAS_TUNE_LOG=1: one line per tuning on stderr (routine, type size,
+    // bucket, sample size, each configuration's time, the choice).
+    const char* log = getenv("HWYBLAS_TUNE_LOG");
+    if (log != nullptr && log[0] != '\0' && log[0] != '0') {
+      std::fprintf(stderr, "hwyblas tune: kind %d bytes %d bucket %d sample %d/%d:", kind,
+                   static_cast<int>(sizeof(T)), bucket, S, real.count);
+      for (size_t c = 0; c < configs.size(); ++c)
+        std::fprintf(stderr, " %d=%.3fms", configs[c], times[c]);
+      std::fprintf(stderr, " -> %d\n", best);
+    }
   }
   cudaStreamSynchronize(ctx.stream);
   cudaFree(A);
   cudaFree(B);
   cudaFree(C);
   cudaFree(P);
+  cudaFree(d_off);
+  cudaFree(d_dim);
   cudaGetLastError();
   std::lock_guard<std::mutex> lock(mu);
   cache[key] = best;
   return best;
-}
-
-int Median(std::vector<int> v) {
-  if (v.empty()) return 0;
-  std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
-  return v[v.size() / 2];
 }
 
 // The size that splits the batch's work in half: problems at least this
@@ -1406,7 +1508,7 @@ namespace {
 template <typename T>
 void RunBatch(int kind, const HostBatch<T>& bt, int* info_out, const char* name) {
   if (bt.count == 0) return;
-  const int config = TunedConfig<T>(kind, WorkMedian(kind, bt), bt.n.empty() ? 0 : Median(bt.n));
+  const int config = TunedConfig<T>(kind, bt, WorkMedian(kind, bt));
   int* dev_info = nullptr;
   if (!LaunchBatch(kind, bt, config, &dev_info, true)) return;
   LaunchFailed(name);

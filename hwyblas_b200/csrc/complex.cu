@@ -138,6 +138,37 @@ __device__ __forceinline__ void ZMergeElement(const ZParams<R>& p, int i, int j,
   }
 }
 
+// One m16n8k8 FP64 MMA: d += a b (a: rows g, g + 8 at k t, t + 4; b: k t,
+// t + 4 at column g), the 8 products added in ascending k.
+__device__ __forceinline__ void DmmaStep(double (&d)[4], const double (&a)[4],
+                                         const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// The end of a KC chunk for element (i, j): ab = (rr - ii, ir + ri), then
+// alpha * ab as the reference's complex product, stored to the chunk's
+// partial buffer (split launches) or merged into C.
+template <typename R>
+__device__ __forceinline__ void ZChunkResult(const ZParams<R>& p, int i, int j, bool first,
+                                             R rr, R ir, R ri, R ii) {
+  if (i >= p.m || j >= p.n) return;
+  const R ab_re = Sub(rr, ii);
+  const R ab_im = Add(ir, ri);
+  const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
+  const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
+  if (p.partial != nullptr) {
+    R* pe = p.partial + 2 * ((static_cast<long long>(blockIdx.z) * p.n + j) * p.m + i);
+    pe[0] = t_re;
+    pe[1] = t_im;
+  } else {
+    ZMergeElement(p, i, j, first, t_re, t_im);
+  }
+}
+
 template <typename R>
 struct Vec2;
 template <>
@@ -257,21 +288,129 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const int i = m0 + tx + 16 * r, j = n0 + ty + 16 * q;
-          const R ab_re = Sub(rr[r][q], ii[r][q]);
-          const R ab_im = Add(ir[r][q], ri[r][q]);
+          ZChunkResult(p, m0 + tx + 16 * r, n0 + ty + 16 * q, first, rr[r][q], ir[r][q],
+                       ri[r][q], ii[r][q]);
           rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
-          if (i >= p.m || j >= p.n) continue;
-          const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
-          const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
-          if (split) {
-            R* pe = p.partial + 2 * ((static_cast<long long>(blockIdx.z) * p.n + j) * p.m + i);
-            pe[0] = t_re;
-            pe[1] = t_im;
-          } else {
-            ZMergeElement(p, i, j, first, t_re, t_im);
-          }
         }
+    }
+  }
+}
+
+// The FP64 complex GEMM on the FP64 tensor pipe. Each of the four real
+// chains of an element (rr, ir, ri, ii) is a `mma.sync.m16n8k8.f64` chain
+// over k, which accumulates its products in ascending k exactly as the
+// reference's fma chain does; chains restart at every KC chunk, whose end
+// goes through the same combine and merge (ZChunkResult). The CTA computes a
+// 64 x 64 complex tile with 8 warps of 32 x 16 (2 x 2 fragments of 16 x 8,
+// four chains each); k-slices of 16 stream through two shared buffers with
+// cp.async, complex elements interleaved, rows padded to 66 elements so that
+// the 16-byte fragment loads of a quarter warp (rows g, k rows t) fall in
+// distinct banks. Zero-filled k beyond the end adds fma(0, 0, acc) = acc: a
+// chain started at +0 never holds -0.
+constexpr int kZdLd = kZK == 16 ? 66 : 0;
+constexpr int kZdSmemBytes = 2 * 2 * kZK * kZdLd * 16;
+
+__global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  extern __shared__ __align__(16) unsigned char zsmem[];
+  double2* sa = reinterpret_cast<double2*>(zsmem);  // [2][kZK][kZdLd]
+  double2* sb = sa + 2 * kZK * kZdLd;               // [2][kZK][kZdLd]
+  const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
+  if (p.part == 1 && min(m0 + kZM, p.m) - 1 < n0) return;
+  if (p.part == 2 && m0 > min(n0 + kZN, p.n) - 1) return;
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const int g = lane / 4, t = lane % 4;
+  const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+  // acc[chain][mt][nt][r]: chains rr, ir, ri, ii; fragment rows g (+8),
+  // columns 2t (+1).
+  double acc[4][2][2][4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[c][a][b][r] = 0.0;
+  const bool split = p.partial != nullptr;
+  const int kbeg = split ? blockIdx.z * kZChunk : 0;
+  const int kend = split ? min(p.k, kbeg + kZChunk) : p.k;
+  const bool a_rows = p.a.rs == 1, b_k = p.b.rs == 1;
+  const auto issue = [&](int k0, int buf) {
+    double2* da = sa + buf * kZK * kZdLd;
+    double2* db = sb + buf * kZK * kZdLd;
+    for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
+      const int kk = a_rows ? idx / kZM : idx % kZK, mm = a_rows ? idx % kZM : idx / kZK;
+      const int gi = m0 + mm, gk = k0 + kk;
+      const bool ok = gi < p.m && gk < p.k;
+      const double* src = ok ? p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs) : p.a.data;
+      CpAsyncElem<double>(da + kk * kZdLd + mm, src, ok);
+    }
+    for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
+      const int kk = b_k ? idx % kZK : idx / kZN, nn = b_k ? idx / kZK : idx % kZN;
+      const int gj = n0 + nn, gk = k0 + kk;
+      const bool ok = gj < p.n && gk < p.k;
+      const double* src = ok ? p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs) : p.b.data;
+      CpAsyncElem<double>(db + kk * kZdLd + nn, src, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const double sa_sign = p.a.conj ? -1.0 : 1.0, sb_sign = p.b.conj ? -1.0 : 1.0;
+  issue(kbeg, 0);
+  int buf = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += kZK, buf ^= 1) {
+    if (k0 + kZK < kend) {
+      issue(k0 + kZK, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const double2* ca = sa + buf * kZK * kZdLd;
+    const double2* cb = sb + buf * kZK * kZdLd;
+    const int steps = (min(kZK, kend - k0) + 7) / 8;
+    for (int ks = 0; ks < steps; ++ks) {
+      double ar[2][4], ai[2][4], br[2][2], bi[2][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const double2* pa = ca + (ks * 8 + t) * kZdLd + wm + a * 16 + g;
+        const double2 v0 = pa[0], v1 = pa[8], v2 = pa[4 * kZdLd], v3 = pa[4 * kZdLd + 8];
+        ar[a][0] = v0.x, ar[a][1] = v1.x, ar[a][2] = v2.x, ar[a][3] = v3.x;
+        ai[a][0] = Mul(v0.y, sa_sign), ai[a][1] = Mul(v1.y, sa_sign);
+        ai[a][2] = Mul(v2.y, sa_sign), ai[a][3] = Mul(v3.y, sa_sign);
+      }
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const double2* pb = cb + (ks * 8 + t) * kZdLd + wn + b * 8 + g;
+        const double2 w0 = pb[0], w1 = pb[4 * kZdLd];
+        br[b][0] = w0.x, br[b][1] = w1.x;
+        bi[b][0] = Mul(w0.y, sb_sign), bi[b][1] = Mul(w1.y, sb_sign);
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          DmmaStep(acc[0][a][b], ar[a], br[b]);
+          DmmaStep(acc[1][a][b], ai[a], br[b]);
+          DmmaStep(acc[2][a][b], ar[a], bi[b]);
+          DmmaStep(acc[3][a][b], ai[a], bi[b]);
+        }
+    }
+    __syncthreads();
+    if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= kend) {
+      const bool first = k0 < kZChunk;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int i = m0 + wm + a * 16 + g + (r >= 2 ? 8 : 0);
+            const int j = n0 + wn + b * 8 + 2 * t + (r & 1);
+            ZChunkResult(p, i, j, first, acc[0][a][b][r], acc[1][a][b][r], acc[2][a][b][r],
+                         acc[3][a][b][r]);
+            acc[0][a][b][r] = acc[1][a][b][r] = acc[2][a][b][r] = acc[3][a][b][r] = 0.0;
+          }
     }
   }
 }
@@ -950,12 +1089,22 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   p.tmr = lanes;
   p.tnr = RefLanesDouble() == 8 ? 6 : 3;
   const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
+  // FP64 runs the four chains on the tensor pipe, FP32 on the CUDA cores.
+  void* fn;
+  int smem;
+  if constexpr (sizeof(R) == 8) {
+    fn = reinterpret_cast<void*>(ZgemmDmmaKernel);
+    smem = kZdSmemBytes;
+  } else {
+    fn = reinterpret_cast<void*>(ZgemmKernel<R>);
+    smem = ZSmemBytes<R>();
+  }
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(ZgemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         ZSmemBytes<R>());
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     configured = true;
   }
+  void* args[] = {&p};
   // Few tiles and several KC chunks: the chunks run in parallel (each one's
   // alpha * ab does not depend on C) and are merged in order afterwards,
   // which gives the same C as merging them one after another.
@@ -966,7 +1115,7 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   if (nchunks >= 2 && tiles * 2 <= Ctx().num_sms && pbytes <= (size_t(1) << 30)) {
     p.partial = static_cast<R*>(Workspace(kWsSplitK, pbytes));
     if (p.partial == nullptr) return;
-    ZgemmKernel<R><<<dim3(grid.x, grid.y, nchunks), 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
+    cudaLaunchKernel(fn, dim3(grid.x, grid.y, nchunks), 256, args, smem, Ctx().stream);
     CountLaunch();
     if (LaunchFailed("complex gemm (split)")) return;
     const long long total = static_cast<long long>(m) * n;
@@ -976,7 +1125,7 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
     LaunchFailed("complex gemm split merge");
     return;
   }
-  ZgemmKernel<R><<<grid, 256, ZSmemBytes<R>(), Ctx().stream>>>(p);
+  cudaLaunchKernel(fn, grid, 256, args, smem, Ctx().stream);
   CountLaunch();
   LaunchFailed("complex gemm");
 }
