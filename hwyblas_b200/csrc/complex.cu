@@ -149,23 +149,76 @@ __device__ __forceinline__ void DmmaStep(double (&d)[4], const double (&a)[4],
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// The end of a KC chunk for element (i, j): ab = (rr - ii, ir + ri), then
-// alpha * ab as the reference's complex product, stored to the chunk's
-// partial buffer (split launches) or merged into C.
-template <typename R>
-__device__ __forceinline__ void ZChunkResult(const ZParams<R>& p, int i, int j, bool first,
-                                             R rr, R ir, R ri, R ii) {
-  if (i >= p.m || j >= p.n) return;
-  const R ab_re = Sub(rr, ii);
-  const R ab_im = Add(ir, ri);
-  const R t_re = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
-  const R t_im = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
+// The end of a KC chunk for a thread's N elements (ei[e], ej[e]): ab =
+// (rr - ii, ir + ri), t = alpha * ab as the reference's complex product,
+// then t to the chunk's partial buffer (split launches) or merged into C as
+// ZMergeElement does. Plain tiles load all of their C elements before the
+// first store, so the loads overlap; HERK tiles go element by element.
+template <typename R, int N>
+__device__ __forceinline__ void ZChunkTile(const ZParams<R>& p, const int (&ei)[N],
+                                           const int (&ej)[N], bool first, const R (&rr)[N],
+                                           const R (&ir)[N], const R (&ri)[N],
+                                           const R (&ii)[N]) {
+  R tr[N], ti[N];
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    const R ab_re = Sub(rr[e], ii[e]);
+    const R ab_im = Add(ir[e], ri[e]);
+    tr[e] = Sub(Mul(ab_re, p.alpha_re), Mul(ab_im, p.alpha_im));
+    ti[e] = Add(Mul(ab_im, p.alpha_re), Mul(ab_re, p.alpha_im));
+  }
   if (p.partial != nullptr) {
-    R* pe = p.partial + 2 * ((static_cast<long long>(blockIdx.z) * p.n + j) * p.m + i);
-    pe[0] = t_re;
-    pe[1] = t_im;
-  } else {
-    ZMergeElement(p, i, j, first, t_re, t_im);
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+      if (ei[e] >= p.m || ej[e] >= p.n) continue;
+      R* pe = p.partial +
+              2 * ((static_cast<long long>(blockIdx.z) * p.n + ej[e]) * p.m + ei[e]);
+      pe[0] = tr[e];
+      pe[1] = ti[e];
+    }
+    return;
+  }
+  if (p.part != 0) {
+#pragma unroll
+    for (int e = 0; e < N; ++e)
+      if (ei[e] < p.m && ej[e] < p.n) ZMergeElement(p, ei[e], ej[e], first, tr[e], ti[e]);
+    return;
+  }
+  const bool beta_zero = (p.beta_re == R(0) && p.beta_im == R(0));
+  const bool beta_one = (p.beta_re == R(1) && p.beta_im == R(0));
+  if (first && beta_zero) {
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+      if (ei[e] >= p.m || ej[e] >= p.n) continue;
+      R* ce = p.c + 2 * (ei[e] + ej[e] * p.ldc);
+      ce[0] = tr[e];
+      ce[1] = ti[e];
+    }
+    return;
+  }
+  R c0[N], c1[N];
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    c0[e] = c1[e] = R(0);
+    if (ei[e] < p.m && ej[e] < p.n) {
+      const R* ce = p.c + 2 * (ei[e] + ej[e] * p.ldc);
+      c0[e] = ce[0];
+      c1[e] = ce[1];
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < N; ++e) {
+    if (ei[e] >= p.m || ej[e] >= p.n) continue;
+    R* ce = p.c + 2 * (ei[e] + ej[e] * p.ldc);
+    if (!first || beta_one) {
+      ce[0] = Add(tr[e], c0[e]);
+      ce[1] = Add(ti[e], c1[e]);
+    } else {
+      const R b_re = Sub(Mul(c0[e], p.beta_re), Mul(c1[e], p.beta_im));
+      const R b_im = Add(Mul(c1[e], p.beta_re), Mul(c0[e], p.beta_im));
+      ce[0] = Add(tr[e], b_re);
+      ce[1] = Add(ti[e], b_im);
+    }
   }
 }
 
@@ -284,14 +337,18 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
     __syncthreads();
     if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= kend) {
       const bool first = k0 < kZChunk;
+      int ei[16], ej[16];
+      R vrr[16], vir[16], vri[16], vii[16];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          ZChunkResult(p, m0 + tx + 16 * r, n0 + ty + 16 * q, first, rr[r][q], ir[r][q],
-                       ri[r][q], ii[r][q]);
+          const int e = 4 * r + q;
+          ei[e] = m0 + tx + 16 * r, ej[e] = n0 + ty + 16 * q;
+          vrr[e] = rr[r][q], vir[e] = ir[r][q], vri[e] = ri[r][q], vii[e] = ii[r][q];
           rr[r][q] = ir[r][q] = ri[r][q] = ii[r][q] = R(0);
         }
+      ZChunkTile(p, ei, ej, first, vrr, vir, vri, vii);
     }
   }
 }
@@ -300,21 +357,23 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
 // chains of an element (rr, ir, ri, ii) is a `mma.sync.m16n8k8.f64` chain
 // over k, which accumulates its products in ascending k exactly as the
 // reference's fma chain does; chains restart at every KC chunk, whose end
-// goes through the same combine and merge (ZChunkResult). The CTA computes a
+// goes through the same combine and merge (ZChunkTile). The CTA computes a
 // 64 x 64 complex tile with 8 warps of 32 x 16 (2 x 2 fragments of 16 x 8,
-// four chains each); k-slices of 16 stream through two shared buffers with
-// cp.async, complex elements interleaved, rows padded to 66 elements so that
-// the 16-byte fragment loads of a quarter warp (rows g, k rows t) fall in
-// distinct banks. Zero-filled k beyond the end adds fma(0, 0, acc) = acc: a
-// chain started at +0 never holds -0.
-constexpr int kZdLd = kZK == 16 ? 66 : 0;
-constexpr int kZdSmemBytes = 2 * 2 * kZK * kZdLd * 16;
+// four chains each); k-slices of 16 stream through three shared buffers with
+// cp.async (two slices in flight while one is multiplied), complex elements
+// interleaved, rows padded to 66 elements so that the 16-byte fragment loads
+// of a quarter warp (rows g, k rows t) fall in distinct banks. Zero-filled k
+// beyond the end adds fma(0, 0, acc) = acc: a chain started at +0 never
+// holds -0.
+constexpr int kZdLd = 66, kZdStages = 3;
+constexpr int kZdSmemBytes = kZdStages * 2 * kZK * kZdLd * 16;
 
+template <bool kConjA, bool kConjB>
 __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
   if (p.guard != nullptr && *p.guard != 0) return;
   extern __shared__ __align__(16) unsigned char zsmem[];
-  double2* sa = reinterpret_cast<double2*>(zsmem);  // [2][kZK][kZdLd]
-  double2* sb = sa + 2 * kZK * kZdLd;               // [2][kZK][kZdLd]
+  double2* sa = reinterpret_cast<double2*>(zsmem);  // [stages][kZK][kZdLd]
+  double2* sb = sa + kZdStages * kZK * kZdLd;       // [stages][kZK][kZdLd]
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * kZN;
   if (p.part == 1 && min(m0 + kZM, p.m) - 1 < n0) return;
   if (p.part == 2 && m0 > min(n0 + kZN, p.n) - 1) return;
@@ -336,55 +395,63 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
   const int kbeg = split ? blockIdx.z * kZChunk : 0;
   const int kend = split ? min(p.k, kbeg + kZChunk) : p.k;
   const bool a_rows = p.a.rs == 1, b_k = p.b.rs == 1;
+  // Issues slice k0 into buffer buf (nothing past kend), always committing a
+  // group so that the wait counts stay uniform.
   const auto issue = [&](int k0, int buf) {
-    double2* da = sa + buf * kZK * kZdLd;
-    double2* db = sb + buf * kZK * kZdLd;
-    for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
-      const int kk = a_rows ? idx / kZM : idx % kZK, mm = a_rows ? idx % kZM : idx / kZK;
-      const int gi = m0 + mm, gk = k0 + kk;
-      const bool ok = gi < p.m && gk < p.k;
-      const double* src = ok ? p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs) : p.a.data;
-      CpAsyncElem<double>(da + kk * kZdLd + mm, src, ok);
-    }
-    for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
-      const int kk = b_k ? idx % kZK : idx / kZN, nn = b_k ? idx / kZK : idx % kZN;
-      const int gj = n0 + nn, gk = k0 + kk;
-      const bool ok = gj < p.n && gk < p.k;
-      const double* src = ok ? p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs) : p.b.data;
-      CpAsyncElem<double>(db + kk * kZdLd + nn, src, ok);
+    if (k0 < kend) {
+      double2* da = sa + buf * kZK * kZdLd;
+      double2* db = sb + buf * kZK * kZdLd;
+      for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
+        const int kk = a_rows ? idx / kZM : idx % kZK, mm = a_rows ? idx % kZM : idx / kZK;
+        const int gi = m0 + mm, gk = k0 + kk;
+        const bool ok = gi < p.m && gk < p.k;
+        const double* src = ok ? p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs) : p.a.data;
+        CpAsyncElem<double>(da + kk * kZdLd + mm, src, ok);
+      }
+      for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
+        const int kk = b_k ? idx % kZK : idx / kZN, nn = b_k ? idx / kZK : idx % kZN;
+        const int gj = n0 + nn, gk = k0 + kk;
+        const bool ok = gj < p.n && gk < p.k;
+        const double* src = ok ? p.b.data + 2 * (gk * p.b.rs + gj * p.b.cs) : p.b.data;
+        CpAsyncElem<double>(db + kk * kZdLd + nn, src, ok);
+      }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  const double sa_sign = p.a.conj ? -1.0 : 1.0, sb_sign = p.b.conj ? -1.0 : 1.0;
   issue(kbeg, 0);
+  issue(kbeg + kZK, 1);
   int buf = 0;
-  for (int k0 = kbeg; k0 < kend; k0 += kZK, buf ^= 1) {
-    if (k0 + kZK < kend) {
-      issue(k0 + kZK, buf ^ 1);
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-    }
+  for (int k0 = kbeg; k0 < kend; k0 += kZK, buf = buf == kZdStages - 1 ? 0 : buf + 1) {
+    // This slice's group is the oldest but one; after the barrier every
+    // thread is done with the previous slice, whose buffer takes slice + 2.
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
     __syncthreads();
+    issue(k0 + 2 * kZK, buf == 0 ? kZdStages - 1 : buf - 1);
     const double2* ca = sa + buf * kZK * kZdLd;
     const double2* cb = sb + buf * kZK * kZdLd;
     const int steps = (min(kZK, kend - k0) + 7) / 8;
-    for (int ks = 0; ks < steps; ++ks) {
+#pragma unroll
+    for (int ks = 0; ks < kZK / 8; ++ks) {
+      if (ks >= steps) break;
       double ar[2][4], ai[2][4], br[2][2], bi[2][2];
 #pragma unroll
       for (int a = 0; a < 2; ++a) {
         const double2* pa = ca + (ks * 8 + t) * kZdLd + wm + a * 16 + g;
         const double2 v0 = pa[0], v1 = pa[8], v2 = pa[4 * kZdLd], v3 = pa[4 * kZdLd + 8];
         ar[a][0] = v0.x, ar[a][1] = v1.x, ar[a][2] = v2.x, ar[a][3] = v3.x;
-        ai[a][0] = Mul(v0.y, sa_sign), ai[a][1] = Mul(v1.y, sa_sign);
-        ai[a][2] = Mul(v2.y, sa_sign), ai[a][3] = Mul(v3.y, sa_sign);
+        ai[a][0] = v0.y, ai[a][1] = v1.y, ai[a][2] = v2.y, ai[a][3] = v3.y;
+        if constexpr (kConjA) {
+#pragma unroll
+          for (int r = 0; r < 4; ++r) ai[a][r] = Mul(ai[a][r], -1.0);
+        }
       }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const double2* pb = cb + (ks * 8 + t) * kZdLd + wn + b * 8 + g;
         const double2 w0 = pb[0], w1 = pb[4 * kZdLd];
         br[b][0] = w0.x, br[b][1] = w1.x;
-        bi[b][0] = Mul(w0.y, sb_sign), bi[b][1] = Mul(w1.y, sb_sign);
+        bi[b][0] = w0.y, bi[b][1] = w1.y;
+        if constexpr (kConjB) bi[b][0] = Mul(bi[b][0], -1.0), bi[b][1] = Mul(bi[b][1], -1.0);
       }
 #pragma unroll
       for (int a = 0; a < 2; ++a)
@@ -396,23 +463,27 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
           DmmaStep(acc[3][a][b], ai[a], bi[b]);
         }
     }
-    __syncthreads();
     if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= kend) {
       const bool first = k0 < kZChunk;
+      int ei[16], ej[16];
+      double vrr[16], vir[16], vri[16], vii[16];
 #pragma unroll
       for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
           for (int r = 0; r < 4; ++r) {
-            const int i = m0 + wm + a * 16 + g + (r >= 2 ? 8 : 0);
-            const int j = n0 + wn + b * 8 + 2 * t + (r & 1);
-            ZChunkResult(p, i, j, first, acc[0][a][b][r], acc[1][a][b][r], acc[2][a][b][r],
-                         acc[3][a][b][r]);
+            const int e = 8 * a + 4 * b + r;
+            ei[e] = m0 + wm + a * 16 + g + (r >= 2 ? 8 : 0);
+            ej[e] = n0 + wn + b * 8 + 2 * t + (r & 1);
+            vrr[e] = acc[0][a][b][r], vir[e] = acc[1][a][b][r];
+            vri[e] = acc[2][a][b][r], vii[e] = acc[3][a][b][r];
             acc[0][a][b][r] = acc[1][a][b][r] = acc[2][a][b][r] = acc[3][a][b][r] = 0.0;
           }
+      ZChunkTile(p, ei, ej, first, vrr, vir, vri, vii);
     }
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 // The in-order merge of a split complex GEMM: per element, chunk 0 with the
@@ -1093,17 +1164,16 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   void* fn;
   int smem;
   if constexpr (sizeof(R) == 8) {
-    fn = reinterpret_cast<void*>(ZgemmDmmaKernel);
+    fn = a.conj ? (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<true, true>)
+                          : reinterpret_cast<void*>(ZgemmDmmaKernel<true, false>))
+                : (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<false, true>)
+                          : reinterpret_cast<void*>(ZgemmDmmaKernel<false, false>));
     smem = kZdSmemBytes;
   } else {
     fn = reinterpret_cast<void*>(ZgemmKernel<R>);
     smem = ZSmemBytes<R>();
   }
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    configured = true;
-  }
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   void* args[] = {&p};
   // Few tiles and several KC chunks: the chunks run in parallel (each one's
   // alpha * ab does not depend on C) and are merged in order afterwards,
