@@ -358,18 +358,21 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
 // over k, which accumulates its products in ascending k exactly as the
 // reference's fma chain does; chains restart at every KC chunk, whose end
 // goes through the same combine and merge (ZChunkTile). The CTA computes a
-// 64 x 64 complex tile with 8 warps of 32 x 16 (2 x 2 fragments of 16 x 8,
-// four chains each); k-slices of 16 stream through three shared buffers with
+// 64 x 64 complex tile with 512 / kFa threads: warps of 16 kFa x 16
+// elements (kFa x 2 fragments of 16 x 8, four chains each; kFa = 1 keeps
+// 16 warps an SM under 128 registers, which measured faster than 8 warps of
+// 32 x 16); k-slices of 16 stream through three shared buffers with
 // cp.async (two slices in flight while one is multiplied), complex elements
 // interleaved, rows padded to 66 elements so that the 16-byte fragment loads
 // of a quarter warp (rows g, k rows t) fall in distinct banks. Zero-filled k
 // beyond the end adds fma(0, 0, acc) = acc: a chain started at +0 never
 // holds -0.
-constexpr int kZdLd = 66, kZdStages = 3;
+constexpr int kZdLd = 66, kZdStages = 3, kZdFa = 1;
 constexpr int kZdSmemBytes = kZdStages * 2 * kZK * kZdLd * 16;
 
-template <bool kConjA, bool kConjB>
-__global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
+template <int kFa, bool kConjA, bool kConjB>
+__global__ void __launch_bounds__(512 / kFa, 1) ZgemmDmmaKernel(ZParams<double> p) {
+  constexpr int kThreads = 512 / kFa;
   if (p.guard != nullptr && *p.guard != 0) return;
   extern __shared__ __align__(16) unsigned char zsmem[];
   double2* sa = reinterpret_cast<double2*>(zsmem);  // [stages][kZK][kZdLd]
@@ -379,14 +382,15 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
   if (p.part == 2 && m0 > min(n0 + kZN, p.n) - 1) return;
   const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
   const int g = lane / 4, t = lane % 4;
-  const int wm = (warp % 2) * 32, wn = (warp / 2) * 16;
+  constexpr int kWarpsM = 4 / kFa;  // warps along m; 4 along n
+  const int wm = (warp % kWarpsM) * 16 * kFa, wn = (warp / kWarpsM) * 16;
   // acc[chain][mt][nt][r]: chains rr, ir, ri, ii; fragment rows g (+8),
   // columns 2t (+1).
-  double acc[4][2][2][4];
+  double acc[4][kFa][2][4];
 #pragma unroll
   for (int c = 0; c < 4; ++c)
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < kFa; ++a)
 #pragma unroll
       for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -401,14 +405,14 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
     if (k0 < kend) {
       double2* da = sa + buf * kZK * kZdLd;
       double2* db = sb + buf * kZK * kZdLd;
-      for (int idx = threadIdx.x; idx < kZK * kZM; idx += 256) {
+      for (int idx = threadIdx.x; idx < kZK * kZM; idx += kThreads) {
         const int kk = a_rows ? idx / kZM : idx % kZK, mm = a_rows ? idx % kZM : idx / kZK;
         const int gi = m0 + mm, gk = k0 + kk;
         const bool ok = gi < p.m && gk < p.k;
         const double* src = ok ? p.a.data + 2 * (gi * p.a.rs + gk * p.a.cs) : p.a.data;
         CpAsyncElem<double>(da + kk * kZdLd + mm, src, ok);
       }
-      for (int idx = threadIdx.x; idx < kZK * kZN; idx += 256) {
+      for (int idx = threadIdx.x; idx < kZK * kZN; idx += kThreads) {
         const int kk = b_k ? idx % kZK : idx / kZN, nn = b_k ? idx / kZK : idx % kZN;
         const int gj = n0 + nn, gk = k0 + kk;
         const bool ok = gj < p.n && gk < p.k;
@@ -433,9 +437,9 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
 #pragma unroll
     for (int ks = 0; ks < kZK / 8; ++ks) {
       if (ks >= steps) break;
-      double ar[2][4], ai[2][4], br[2][2], bi[2][2];
+      double ar[kFa][4], ai[kFa][4], br[2][2], bi[2][2];
 #pragma unroll
-      for (int a = 0; a < 2; ++a) {
+      for (int a = 0; a < kFa; ++a) {
         const double2* pa = ca + (ks * 8 + t) * kZdLd + wm + a * 16 + g;
         const double2 v0 = pa[0], v1 = pa[8], v2 = pa[4 * kZdLd], v3 = pa[4 * kZdLd + 8];
         ar[a][0] = v0.x, ar[a][1] = v1.x, ar[a][2] = v2.x, ar[a][3] = v3.x;
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
         if constexpr (kConjB) bi[b][0] = Mul(bi[b][0], -1.0), bi[b][1] = Mul(bi[b][1], -1.0);
       }
 #pragma unroll
-      for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < kFa; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
           DmmaStep(acc[0][a][b], ar[a], br[b]);
@@ -465,10 +469,10 @@ __global__ void __launch_bounds__(256, 1) ZgemmDmmaKernel(ZParams<double> p) {
     }
     if ((k0 + kZK) % kZChunk == 0 || k0 + kZK >= kend) {
       const bool first = k0 < kZChunk;
-      int ei[16], ej[16];
-      double vrr[16], vir[16], vri[16], vii[16];
+      int ei[8 * kFa], ej[8 * kFa];
+      double vrr[8 * kFa], vir[8 * kFa], vri[8 * kFa], vii[8 * kFa];
 #pragma unroll
-      for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < kFa; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -1162,12 +1166,13 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   const dim3 grid((m + kZM - 1) / kZM, (n + kZN - 1) / kZN);
   // FP64 runs the four chains on the tensor pipe, FP32 on the CUDA cores.
   void* fn;
-  int smem;
+  int smem, threads = 256;
   if constexpr (sizeof(R) == 8) {
-    fn = a.conj ? (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<true, true>)
-                          : reinterpret_cast<void*>(ZgemmDmmaKernel<true, false>))
-                : (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<false, true>)
-                          : reinterpret_cast<void*>(ZgemmDmmaKernel<false, false>));
+    fn = a.conj ? (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<kZdFa, true, true>)
+                          : reinterpret_cast<void*>(ZgemmDmmaKernel<kZdFa, true, false>))
+                : (b.conj ? reinterpret_cast<void*>(ZgemmDmmaKernel<kZdFa, false, true>)
+                          : reinterpret_cast<void*>(ZgemmDmmaKernel<kZdFa, false, false>));
+    threads = 512 / kZdFa;
     smem = kZdSmemBytes;
   } else {
     fn = reinterpret_cast<void*>(ZgemmKernel<R>);
@@ -1185,7 +1190,7 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
   if (nchunks >= 2 && tiles * 2 <= Ctx().num_sms && pbytes <= (size_t(1) << 30)) {
     p.partial = static_cast<R*>(Workspace(kWsSplitK, pbytes));
     if (p.partial == nullptr) return;
-    cudaLaunchKernel(fn, dim3(grid.x, grid.y, nchunks), 256, args, smem, Ctx().stream);
+    cudaLaunchKernel(fn, dim3(grid.x, grid.y, nchunks), threads, args, smem, Ctx().stream);
     CountLaunch();
     if (LaunchFailed("complex gemm (split)")) return;
     const long long total = static_cast<long long>(m) * n;
@@ -1195,7 +1200,7 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
     LaunchFailed("complex gemm split merge");
     return;
   }
-  cudaLaunchKernel(fn, grid, 256, args, smem, Ctx().stream);
+  cudaLaunchKernel(fn, grid, threads, args, smem, Ctx().stream);
   CountLaunch();
   LaunchFailed("complex gemm");
 }
