@@ -251,12 +251,13 @@ __device__ __forceinline__ void CpAsyncElem(void* smem_dst, const R* src, bool v
 // One CTA: a 64 x 64 complex tile, 4 x 4 elements per thread (rows
 // tx + 16 r, columns ty + 16 q). The k-slices of 16 stream through two
 // shared-memory buffers with cp.async (complex elements stay interleaved, so
-// one shared load gives both parts; conjugation is applied after the load),
-// the next slice in flight while this one is multiplied. A chunk ends on a
-// slice boundary (256 is a multiple of 16), where the thread merges its
-// chunk into C in memory: the running value stays in C itself.
-template <typename R>
-__global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
+// one shared load gives both parts; conjugation, chosen at compile time, is
+// applied after the load), the next slice in flight while this one is
+// multiplied; two CTAs an SM. A chunk ends on a slice boundary (256 is a
+// multiple of 16), where the thread merges its chunk into C in memory: the
+// running value stays in C itself. FP32 only: FP64 runs ZgemmDmmaKernel.
+template <typename R, bool kConjA, bool kConjB>
+__global__ void __launch_bounds__(256, 2) ZgemmKernel(ZParams<R> p) {
   if (p.guard != nullptr && *p.guard != 0) return;
   using V = typename Vec2<R>::type;
   extern __shared__ __align__(16) unsigned char zsmem[];
@@ -298,7 +299,6 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  const R sa_sign = p.a.conj ? R(-1) : R(1), sb_sign = p.b.conj ? R(-1) : R(1);
   issue(kbeg, 0);
   int buf = 0;
   for (int k0 = kbeg; k0 < kend; k0 += kZK, buf ^= 1) {
@@ -320,9 +320,9 @@ __global__ void __launch_bounds__(256, 1) ZgemmKernel(ZParams<R> p) {
         const V va = ca[kk * kZM + tx + 16 * r];
         const V vb = cb[kk * kZN + ty + 16 * r];
         ar[r] = va.x;
-        ai[r] = Mul(va.y, sa_sign);
+        ai[r] = kConjA ? Mul(va.y, R(-1)) : va.y;
         br[r] = vb.x;
-        bi[r] = Mul(vb.y, sb_sign);
+        bi[r] = kConjB ? Mul(vb.y, R(-1)) : vb.y;
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r)
@@ -1175,7 +1175,10 @@ void ZgemmViews(int m, int n, int k, const R* alpha, ZView<R> a, ZView<R> b, con
     threads = 512 / kZdFa;
     smem = kZdSmemBytes;
   } else {
-    fn = reinterpret_cast<void*>(ZgemmKernel<R>);
+    fn = a.conj ? (b.conj ? reinterpret_cast<void*>(ZgemmKernel<R, true, true>)
+                          : reinterpret_cast<void*>(ZgemmKernel<R, true, false>))
+                : (b.conj ? reinterpret_cast<void*>(ZgemmKernel<R, false, true>)
+                          : reinterpret_cast<void*>(ZgemmKernel<R, false, false>));
     smem = ZSmemBytes<R>();
   }
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
