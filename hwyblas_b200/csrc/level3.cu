@@ -574,6 +574,153 @@ bool TrsmCoop(bool left, View<T> tri, bool lower, bool unit, int r, int other, T
   return true;
 }
 
+// Left-side FP64 TRSM subtree (at most kTcRows rows) with many right-hand
+// sides: the columns of X are independent, so each CTA owns kTsCols of them
+// and walks the whole recursion for those columns alone, with block
+// barriers only (no grid barrier, no cooperative launch). Base solves are
+// the base kernel's code (one thread a column); an update C -= A X of the
+// CTA's columns gives each warp 16-row strips of C and runs the element's
+// m16n8k8 chain over k, restarted every KC = 256 and merged in order (alpha
+// -1, beta 1): every element's FMA chain and merges are those of the
+// cooperative kernel's updates, so X comes out the same.
+constexpr int kTsCols = 8;       // right-hand sides a CTA owns: one n8 fragment
+constexpr int kTsMinOther = 256;  // the column-owned path from this many
+// ... and from this many rows: a shallower subtree is a short chain of
+// launches already, and the LU's 64-row panel solves over thousands of
+// columns measured slower column-owned (dgesv n = 16384 251 -> 278 ms).
+constexpr int kTsMinRows = 256;
+
+// C (mm x w) -= A (mm x kk) X (kk x w); X and C column-major with leading
+// dimension ld, A a strided view. Fragments come from L2 four k8 steps at a
+// time (zero past kk, mm and w: fma(0, 0, acc) = acc for a chain started at
+// +0).
+__device__ void ColsUpdate(int mm, int kk, View<double> a, const double* x, double* c,
+                           long long ld, int w) {
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int g = lane >> 2, t = lane & 3;
+  const int warps = blockDim.x / 32;
+  for (int i0 = warp * 16; i0 < mm; i0 += warps * 16) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, cv[4];
+    bool in[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = i0 + g + (e >> 1) * 8, j = 2 * t + (e & 1);
+      in[e] = i < mm && j < w;
+      cv[e] = in[e] ? __ldcg(c + i + j * ld) : 0.0;
+    }
+    const int ra = i0 + g, rb = i0 + g + 8;
+    for (int k0 = 0; k0 < kk; k0 += 32) {
+      double fa[4][4], fb[4][2];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int q0 = k0 + 8 * s + t, q1 = q0 + 4;
+        fa[s][0] = (ra < mm && q0 < kk) ? __ldcg(a.data + ra * a.rs + q0 * a.cs) : 0.0;
+        fa[s][1] = (rb < mm && q0 < kk) ? __ldcg(a.data + rb * a.rs + q0 * a.cs) : 0.0;
+        fa[s][2] = (ra < mm && q1 < kk) ? __ldcg(a.data + ra * a.rs + q1 * a.cs) : 0.0;
+        fa[s][3] = (rb < mm && q1 < kk) ? __ldcg(a.data + rb * a.rs + q1 * a.cs) : 0.0;
+        fb[s][0] = (g < w && q0 < kk) ? __ldcg(x + q0 + g * ld) : 0.0;
+        fb[s][1] = (g < w && q1 < kk) ? __ldcg(x + q1 + g * ld) : 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+            "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+            : "+d"(acc[0]), "+d"(acc[1]), "+d"(acc[2]), "+d"(acc[3])
+            : "d"(fa[s][0]), "d"(fa[s][1]), "d"(fa[s][2]), "d"(fa[s][3]), "d"(fb[s][0]),
+              "d"(fb[s][1]));
+      }
+      // End of a KC chunk (or of k): merge alpha * acc = -acc, restart.
+      if ((k0 + 32) % 256 == 0 || k0 + 32 >= kk) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double r = -1.0 * acc[e];
+          cv[e] = r + cv[e];
+          acc[e] = 0.0;
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = i0 + g + (e >> 1) * 8, j = 2 * t + (e & 1);
+      if (in[e]) __stcg(c + i + j * ld, cv[e]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTcThreads) TrsmColsKernel(TrsmCoopArgs<double> p) {
+  if (p.guard != nullptr && *p.guard != 0) return;
+  __shared__ double st[32][33];
+  __shared__ double sinv[32];
+  const int j0 = blockIdx.x * kTsCols;
+  const int w = min(kTsCols, p.other - j0);
+  if (w <= 0) return;
+  double* xb = p.b + static_cast<long long>(j0) * p.ldb;  // this CTA's columns
+  // Which half TrsmRec solves first: t11 for left-lower.
+  const bool first11 = p.lower != 0;
+  int s_off[8], s_r[8], s_ph[8];
+  int sp = 0;
+  s_off[0] = 0;
+  s_r[0] = p.r;
+  s_ph[0] = 0;
+  while (sp >= 0) {
+    const int off = s_off[sp], rr = s_r[sp];
+    if (rr <= 32) {
+      // T X = B as X^T T^T = B^T: rows of X^T are B's columns.
+      View<double> t = SubView(p.tri, off, off);
+      const long long rs = t.rs;
+      t.rs = t.cs;
+      t.cs = rs;
+      const int lo = !p.lower;
+      LoadBaseTriangle(t, lo, p.unit, rr, st, sinv);
+      if (threadIdx.x < w)
+        BaseSolveRow<double, true>(st, sinv, lo, p.unit, rr,
+                                   xb + off + threadIdx.x * p.ldb, 1);
+      --sp;
+      __syncthreads();
+      continue;
+    }
+    const int r1 = max(32, (rr / 2) / 32 * 32), r2 = rr - r1;
+    const int ph = s_ph[sp]++;
+    if (ph == 2) {
+      --sp;
+      continue;
+    }
+    if (ph == 1) {
+      if (p.lower)
+        ColsUpdate(r2, r1, SubView(p.tri, off + r1, off), xb + off, xb + off + r1, p.ldb, w);
+      else
+        ColsUpdate(r1, r2, SubView(p.tri, off, off + r1), xb + off + r1, xb + off, p.ldb, w);
+      __syncthreads();
+    }
+    // ph 0: the first half; ph 1: the second.
+    const bool take11 = (ph == 0) == first11;
+    ++sp;
+    s_off[sp] = take11 ? off : off + r1;
+    s_r[sp] = take11 ? r1 : r2;
+    s_ph[sp] = 0;
+  }
+}
+
+bool TrsmCols(View<double> tri, bool lower, bool unit, int r, int other, double* b, int ldb) {
+  Context& ctx = Ctx();
+  TrsmCoopArgs<double> a;
+  a.tri = tri;
+  a.left = 1;
+  a.lower = lower ? 1 : 0;
+  a.unit = unit ? 1 : 0;
+  a.r = r;
+  a.other = other;
+  a.b = b;
+  a.ldb = ldb;
+  a.barrier = nullptr;
+  a.timeout_flag = ctx.dev_status;
+  a.guard = ctx.guard;
+  TrsmColsKernel<<<(other + kTsCols - 1) / kTsCols, kTcThreads, 0, ctx.stream>>>(a);
+  CountLaunch();
+  return !LaunchFailed("trsm column-owned");
+}
+
 template <typename T>
 void LaunchGemm(int m, int n, int k, T alpha, View<T> a, View<T> b, T beta,
                 T* c, int ldc);
@@ -595,6 +742,12 @@ void TrsmRec(bool left, View<T> tri, bool lower, bool unit, int r, int other,
   if (r <= 32) {
     TrsmSolve<T>(left, tri, lower, unit, r, other, b, ldb);
     return;
+  }
+  if constexpr (sizeof(T) == 8) {
+    if (left && r <= kTcRows && r >= kTsMinRows && other >= kTsMinOther) {
+      TrsmCols(tri, lower, unit, r, other, b, ldb);
+      return;
+    }
   }
   if (r <= kTcRows && other <= TcOther<T>() &&
       TrsmCoop<T>(left, tri, lower, unit, r, other, b, ldb))

@@ -253,6 +253,34 @@ def test_dtrsm_few_rhs_cooperative(hb, orc, side, uplo, trans, diag, r, few):
     assert not np.isnan(x1[:m]).any()
 
 
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+@pytest.mark.parametrize("r,many", [(500, 300), (1300, 257), (512, 1500)])
+def test_dtrsm_many_rhs_column_owned(hb, orc, uplo, trans, diag, r, many):
+    """Left side, at least 256 right-hand sides: each subtree of at most 512
+    rows runs with the columns of X split among CTAs (8 a CTA, the last one
+    ragged), each walking the whole recursion for its own columns. A 500-row
+    upper subtree has a 276-deep update (a KC restart inside it). Bits must
+    equal the oracle's."""
+    rng = np.random.default_rng(r * 7 + many + ord(uplo) * 3 + ord(trans) * 5 + ord(diag))
+    m, n = r, many
+    lda = r + 3
+    a = rand(rng, lda, r)
+    a[:r, :r] = a[:r, :r] / r + np.diag(1.5 + rng.uniform(0, 1, r))
+    tri = np.tril(np.ones((r, r), bool)) if uplo == "L" else np.triu(np.ones((r, r), bool))
+    if diag == "U":
+        np.fill_diagonal(tri, False)
+    a[:r, :r][~tri] = np.nan
+    b = rand(rng, m + 2, n)
+    for alpha in (1.0, -0.5):
+        x1, x2 = b.copy(order="F"), b.copy(order="F")
+        hb.dtrsm("L", uplo, trans, diag, m, n, alpha, a, lda, x1, m + 2)
+        orc.dtrsm("L", uplo, trans, diag, m, n, alpha, a, lda, x2, m + 2)
+        assert same_bits(x1, x2), first_diff(x1, x2)
+        assert not np.isnan(x1[:m]).any()
+
+
 def test_dtrsm_config_4096x512(hb, orc):
     """side=L uplo=L trans=N diag=U, M=4096 N=512, U[-1,1] entries (scaled
     off-diagonal, as tests/level3_test.cc:491-494, so that X stays finite)."""
