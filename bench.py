@@ -86,7 +86,7 @@ def parse():
                         "records through torch.profiler)")
     p.add_argument("--case", default=None,
                    choices=["leaf", "getrf", "gesv", "gesv-mixed", "potrf", "posv-mixed",
-                            "trtri", "getri", "trmm", "zgemm", "zgetrf", "zpotrf"],
+                            "trtri", "getri", "trmm", "zgemm", "zgetrf", "zpotrf", "trsm"],
                    help="run one call of a hot-path piece and exit (for profilers): the LU "
                         "leaf on a gesv-n x 16 panel, plain dgetrf / dgesv / dpotrf, or "
                         "mixed dgesv / dposv at gesv-n; dtrtri, dgetri, dtrmm, zgemm, "
@@ -1163,6 +1163,12 @@ def run_case(args):
         else:
             c = torch.zeros_like(a0)
             call = lambda a: hb.zgemm("z", "N", "N", n, n, n, 1.0, a, n, other, n, 0.0, c, n)
+    elif args.case == "trsm":
+        # dtrsm L/L/N/U, n x nrhs (the configured 4096 x 512 with --gesv-n 4096
+        # --nrhs 512): the triangle is fixed, B is the operand solved in place.
+        tri = torch.rand(n * n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        a0 = torch.rand(n * args.nrhs, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        call = lambda x: hb.dtrsm("L", "L", "N", "U", n, args.nrhs, 1.0, tri, n, x, n)
     elif args.case == "leaf":
         a0 = torch.rand(n * 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         call = lambda a: hb.dgetrf2(n, 16, a, n, ipiv)
